@@ -1,0 +1,299 @@
+"""Benchmark: node-steps/s of the explicit meshfree step on the 1M-node Taylor bar.
+
+Workload: copper Taylor bar D = 6.4 mm, L = 32.4 mm on a 0.1 mm jittered
+lattice (1,042,925 nodes), linear-basis RKPM, cubic B-spline box support
+2.0 h, direct nodal integration, J2 with linear hardening, v0 = 227 m/s
+into a rigid wall, fixed CFL-0.5 step.  A "step" is one explicit step of
+the whole bar (force, return mapping, central-difference update).  The
+inputs (shape-function stacks, ~4 GB) are far larger than L2 (126 MB), so
+no L2 flush is needed between steps.
+
+`value` = node-steps/s of the mixed-precision path (the headline form),
+`fp64_value` the plain FP64 drop-in; both device-timed with CUDA events on
+the library's stream.  `e2e` drives the same job through the public C ABI
+from host buffers: model upload, step-0 search and shapes, K steps with the
+per-step scalars MAIN writes (energies, reaction force) read back to the
+host every step, and the end-state download, all inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: replicas only (one independent bar per rank), weak scaling.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-steps/s, 1M-node Taylor bar: mixed+learned vs plain FP64 at <=1e-3 err"
+UNIT = "node-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--h", type=float, default=0.1e-3, help="lattice spacing (m)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=0, help="CPU baseline sample steps (0 = auto)")
+    return ap.parse_args()
+
+
+def dist_setup(n):
+    rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        return rank, world, dist
+    return rank, world, None
+
+
+def max_over_ranks(v, dist):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (SM clock and throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["unsampled"])
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        dev = os.environ.get("LOCAL_RANK", "0")
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9 or parts[0] != dev:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=smax, reasons=sorted(reasons),
+                    samples=len(sm))
+
+
+def measured_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def kernel_bytes(n, nnz, mixed):
+    """Algorithmic bytes per launch of each per-step kernel (every array
+    touched once; neighbour data counted once per owning node)."""
+    g = 12 if mixed else 24          # three gradient components per CSR entry
+    t = 36 if mixed else 72          # T_i (3x3) per node
+    defgrad = nnz * (4 + g) + n * (8 + 48 + 24 + 144)           # col + grad; rowptr, u and du, sum grad, F/G0 out
+    stress = n * (144 + 192 + 16 + 8 + 8 + 8 + 2 + t)           # F/G0, sigma+eps rw, eps_p rw, eq, wvel, vol, mat, T
+    force = nnz * (4 + g) + n * (8 + t + 3 + 24 + 24 + 48 + 48 + 24 + 48 + 48 + 24)  # trow + grad^T; T, fixity,
+    return dict(defgrad=defgrad, stress=stress, force=force)     # mass, fint, fext rw, vel rw, acl, dsp rw, tot rw, pr
+
+
+def survey_step_bytes(k, mixed):
+    """Whole-step algorithmic bytes per node-step: 36k + 600 (FP64), 20k + 484 (mixed)."""
+    return (20 * k + 484) if mixed else (36 * k + 600)
+
+
+def run_ours(args, rank, world, dist):
+    import taylor_b200
+    from taylor_b200 import _lib, cases, mega
+    case = cases.taylor_bar(h=args.h, seed=1 + rank)
+    n = case["n"]
+    p = _lib.params(**cases.param_kwargs(case))
+    m = mega.Mega(case, p)
+    t0 = time.perf_counter()
+    info = m.search_and_shapes(download=False)
+    step0_s = time.perf_counter() - t0
+    nnz = info["nnz"]
+    kmean = nnz / n
+    # the CFL step from the neighbour lists (host-side, once)
+    nb = m.search_and_shapes(download=True)
+    dt = cases.stable_dt(case, nb["gn"], nb["gstart"], nb["gstack"])
+    del nb
+    res = {}
+    for mode in ("fp64", "mixed"):
+        m.step(args.warmup, dt, mode=mode)
+        barrier(dist)
+        clk = Clocks()
+        clk.start()
+        l0 = m.kernel_launches()
+        ms = m.step_timed(args.steps, dt, mode=mode)
+        launches = m.kernel_launches() - l0
+        clocks = clk.stop()
+        ms = max_over_ranks(ms, dist)
+        kt = m.kernel_times(max(3, args.steps // 2), dt, mode=mode)
+        res[mode] = dict(ms=ms, clocks=clocks, launches=launches, kt=[float(x) for x in kt])
+    s = m.scalars()
+    dev_bytes = m.device_bytes()
+    m.close()
+
+    # end to end through the public API from host buffers
+    barrier(dist)
+    t0 = time.perf_counter()
+    e = mega.Mega(case, p)
+    e.search_and_shapes()
+    d2h = 0
+    for _ in range(args.steps):
+        e.step(1, dt, mode="mixed")
+        sc = e.scalars()           # ENERGY_INFO.OUT / TOTAL_FORCE.OUT / TIME.OUT of MAIN, every step
+        d2h += 8 * 12
+    xend = e.download(_lib.F_COO_CURRENT)
+    epend = e.download(_lib.F_EPS)
+    d2h += xend.nbytes + epend.nbytes
+    e.close()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    h2d = sum(np.asarray(case[k]).nbytes for k in ("coo", "win", "vol", "mass", "ebc", "vinit", "props", "mat_type",
+                                                     "body_id", "sm_len"))
+    peak, peak_kind = measured_peak()
+    out = dict(case=case, n=n, nnz=nnz, kmean=kmean, dt=dt, res=res, step0_s=step0_s, e2e_s=e2e_s, h2d=h2d,
+               d2h=d2h, peak=peak, peak_kind=peak_kind, scalars=s, dev_bytes=dev_bytes)
+    return out
+
+
+def cpu_baseline(case, steps, nthreads):
+    from oracle import oracle as O
+    from taylor_b200 import cases
+    p = O.params(**cases.param_kwargs(case))
+    r = O.Run(case, p, nthreads=nthreads)
+    dt = cases.stable_dt(case, r.nb["gn"], r.nb["gstart"], r.nb["gstack"])
+    r.step(1, dt)
+    t0 = time.perf_counter()
+    r.step(steps, dt)
+    el = time.perf_counter() - t0
+    return case["n"] * steps / el, el
+
+
+def main():
+    args = parse()
+    rank, world, dist = dist_setup(args.gpus)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from taylor_b200 import cases
+        case = cases.taylor_bar(h=args.h, seed=1)
+        nthreads = os.cpu_count() or 1
+        steps = args.cpu_steps or max(1, min(args.steps, 10))
+        for _ in range(0):
+            pass
+        val, el = cpu_baseline(case, steps, nthreads)
+        line = dict(metric=METRIC, value=val, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=1e3 * el / steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+                    dtype="f64", data="synthetic", impl="reference",
+                    config=dict(workload=f"taylor_bar_1M h={args.h*1e3:.3g}mm n={case['n']}", nodes=case["n"],
+                                sample=f"{steps} explicit steps after step 0 (reference arm: C++ OpenMP "
+                                       f"restatement of MEGA, the Fortran reference cannot be compiled here)"),
+                    cpu_baseline=dict(value=val, unit=UNIT, cores=nthreads, kind="port",
+                                      sample=f"{steps} steps of the {case['n']}-node bar"),
+                    e2e=dict(value=val, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+        print(json.dumps(line))
+        return
+
+    r = run_ours(args, rank, world, dist)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    n, nnz, K = r["n"], r["nnz"], args.steps
+    mix, f64 = r["res"]["mixed"], r["res"]["fp64"]
+    value = world * n * K / (mix["ms"] / 1e3)
+    fp64_value = world * n * K / (f64["ms"] / 1e3)
+    # roofline of the dominant kernel (mixed path, the headline)
+    kb = kernel_bytes(n, nnz, mixed=True)
+    names = ["defgrad", "stress", "force"]
+    kt = mix["kt"]
+    dom = int(np.argmax(kt))
+    achieved = kb[names[dom]] / (kt[dom] / 1e3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = prof.get(f"mixed_{names[dom]}_bytes_per_launch")
+    except Exception:
+        pass
+    roof = dict(bound="hbm", kernel=f"k_{names[dom]} (mixed)", achieved=achieved, peak=r["peak"], unit="GB/s",
+                frac=achieved / r["peak"], traffic=traffic, peak_source=r["peak_kind"],
+                all_kernels={nm: dict(ms=kt[i], gbs=kb[nm] / (kt[i] / 1e3) / 1e9,
+                                      frac=kb[nm] / (kt[i] / 1e3) / 1e9 / r["peak"]) for i, nm in enumerate(names)},
+                fp64_kernels={nm: dict(ms=f64["kt"][i],
+                                       gbs=kernel_bytes(n, nnz, False)[nm] / (f64["kt"][i] / 1e3) / 1e9)
+                              for i, nm in enumerate(names)},
+                step_bytes_per_node_survey=dict(fp64=survey_step_bytes(nnz / n, False),
+                                                mixed=survey_step_bytes(nnz / n, True)))
+    cpu = None
+    if not args.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        steps = args.cpu_steps or 5
+        val, el = cpu_baseline(r["case"], steps, nthreads)
+        cpu = dict(value=val, unit=UNIT, cores=nthreads, kind="port",
+                   sample=f"{steps} explicit steps of the same {n}-node bar after step 0, C++ OpenMP restatement "
+                          f"of MEGA with per-thread FINT_TEMP buffers (the Fortran reference cannot be compiled here)")
+    e2e_val = world * n * K / r["e2e_s"]
+    line = dict(
+        metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=K, warmup=args.warmup,
+        ms_per_step=mix["ms"] / K, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32+f64",
+        data="synthetic (seeded jittered lattice, config 2 geometry and material)",
+        config=dict(workload=f"taylor_bar_1M h={args.h*1e3:.3g}mm", nodes=n, nnz=nnz, mean_neighbours=nnz / n,
+                    dt=r["dt"], parallelism=f"replicas{world}", l2="inputs larger than L2 (no flush needed)",
+                    step0_search_shapes_s=r["step0_s"], device_bytes=r["dev_bytes"]),
+        fp64_value=fp64_value, fp64_ms_per_step=f64["ms"] / K, mixed_over_fp64=value / fp64_value,
+        roofline=roof, cpu_baseline=cpu,
+        e2e=dict(value=e2e_val, unit=UNIT, h2d_bytes_per_step=r["h2d"] / K, d2h_bytes_per_step=r["d2h"] / K,
+                 note="model upload + step 0 + K steps with per-step scalar readback + end-state download"),
+        gpu_launches=mix["launches"], clocks=mix["clocks"], clocks_fp64=f64["clocks"],
+        newton_iters_last_step=r["scalars"]["newton_iters"], plastic_nodes_last_step=r["scalars"]["plastic_nodes"])
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,271 @@
+/*
+ * mega_gpu.h -- C ABI of the B200 explicit meshfree step (libmega_gpu.so).
+ *
+ * The library replaces the hot path of MEGA (Meshfree Explicit Galerkin
+ * Analysis, XieZhengTing/Taylor): the bin neighbour search, the RK shape
+ * function build, the nodal-integration internal force with Hughes-Winget
+ * rotation and von Mises return mapping, the displacement interpolation,
+ * the central-difference update and the peridynamic force.
+ *
+ * Conventions (they mirror gfortran's defaults, so an ISO_C_BINDING
+ * interface block binds every entry point without wrappers):
+ *   - arrays are host pointers to Fortran column-major storage: (3,N) is
+ *     xyz-interleaved per node, (6,N) is Voigt (xx,yy,zz,yz,xz,xy) per node,
+ *     (30,N) material properties, (20,N) state variables;
+ *   - LOGICAL is int32_t (0 / 1); INTEGER is int32_t; DOUBLE PRECISION is double;
+ *   - neighbour lists (GN, GSTART, GSTACK) are 1-based like the reference;
+ *   - every entry returns int: 0 = success, >0 = bitmask of MEGA_ST_* raised
+ *     by the device, <0 = MEGA_ERR_* (CUDA or argument error).  Kernels never
+ *     trap; the caller maps a nonzero status onto EXIT_PROGRAM.
+ * One context owns one CUDA stream and all device buffers; calls on one
+ * context are not re-entrant.  The host arrays are never freed or resized.
+ */
+#ifndef MEGA_GPU_H
+#define MEGA_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status bits (device status word, OR-ed by kernels) ----------------- */
+#define MEGA_ST_NEWTON_CAP      0x0001 /* return mapping hit its iteration cap
+                                          (CONSTITUTE_VONMISES.F90:115-119) */
+#define MEGA_ST_SINGULAR_MOMENT 0x0002 /* RK moment matrix determinant is 0 or
+                                          not finite (INVERSE.F90:185-223) */
+#define MEGA_ST_BIN_OVERFLOW    0x0004 /* >= 1000 nodes in one bin
+                                          (BIN_SEARCH.F90:48-51) */
+#define MEGA_ST_CAND_OVERFLOW   0x0008 /* > 10000 candidates for one node
+                                          (BIN_SEARCH.F90:117-120) */
+#define MEGA_ST_NONFINITE       0x0010 /* NaN/Inf in a force or stress */
+#define MEGA_ST_BAD_MATERIAL    0x0020 /* material type not on this path
+                                          (CONSTITUTION.F90:79-83) */
+#define MEGA_ST_STACK_OVERFLOW  0x0040 /* neighbour stack larger than the
+                                          caller's DIM_NN_LIST */
+#define MEGA_ST_SINGULAR_SHAPE  0x0080 /* PD shape tensor K not invertible
+                                          (INVERSE.F90:41-45) */
+
+/* ---- API errors (negative return codes) --------------------------------- */
+#define MEGA_ERR_CUDA     (-1)
+#define MEGA_ERR_ARG      (-2)
+#define MEGA_ERR_HANDLE   (-3)
+#define MEGA_ERR_STATE    (-4)  /* call out of order (e.g. step before search) */
+#define MEGA_ERR_NOMEM    (-5)
+#define MEGA_ERR_UNSUPPORTED (-6)
+
+/* ---- precision / physics modes for the resident stepper ----------------- */
+#define MEGA_MODE_FP64    0  /* plain FP64 drop-in */
+#define MEGA_MODE_MIXED   1  /* FP32 gradients, stress, strain and force
+                                accumulation; FP64 moment inverse, positions,
+                                displacements, time integration and return-
+                                mapping residual */
+#define MEGA_FLAG_INTERP_EACH_STEP 0x100 /* accumulate the physical displacement
+                                            every step as HANDELER.F90:114-139
+                                            and MAIN.F90:377-386 do, instead of
+                                            evaluating it when downloaded */
+#define MEGA_FLAG_LEARNED_GUESS    0x200 /* rate-dependent return mapping starts
+                                            Newton from the surrogate network */
+
+/* ---- material types handled by the fused force kernel ------------------- */
+#define MEGA_MAT_ELASTIC      1  /* CONSTITUTION.F90:48-52 */
+#define MEGA_MAT_VONMISES     2  /* CONSTITUTE_VONMISES.F90:21-158 */
+#define MEGA_MAT_VM_RATE      7  /* power-law rate-dependent J2 (no reference
+                                    counterpart): sigma_y = A + B*ep^n *
+                                    (1 + C*ln(max(epdot,epdot0)/epdot0));
+                                    PROPS(4..8) = A, B, n, C, epdot0 */
+
+/* ---- fields for mega_download / mega_upload ----------------------------- */
+enum mega_field {
+  MEGA_F_COO_CURRENT = 0, /* (3,N) x = X + physical total displacement       */
+  MEGA_F_DSP         = 1, /* (3N) generalised displacement increment (LOCAL_DSP) */
+  MEGA_F_DSP_TOT     = 2, /* (3N) generalised total displacement             */
+  MEGA_F_VEL         = 3, /* (3N) generalised velocity                       */
+  MEGA_F_ACL         = 4, /* (3N) generalised acceleration                   */
+  MEGA_F_FINT        = 5, /* (3N) internal force                             */
+  MEGA_F_FEXT        = 6, /* (3N) external force                             */
+  MEGA_F_STRESS      = 7, /* (6,N) Cauchy stress                             */
+  MEGA_F_STRAIN      = 8, /* (6,N) strain                                    */
+  MEGA_F_EPS         = 9, /* (N) equivalent plastic strain, STATE(3,:)       */
+  MEGA_F_STRAIN_EQ   = 10,/* (N) GSTRAIN_EQ                                  */
+  MEGA_F_WAVE_VEL    = 11,/* (N) GMAX_WVEL                                   */
+  MEGA_F_DSP_TOT_PHY = 12,/* (3N) physical total displacement                */
+  MEGA_F_PRFORCE     = 13,/* (3,N) reaction force on fixed DOFs              */
+  MEGA_F_NEWTON_IT   = 14 /* (N) Newton iterations of the last step (int32 stored as double) */
+};
+
+/* Scalars reported by mega_scalars (energies are those MAIN.F90:524-555 writes). */
+typedef struct mega_scalars_t {
+  double time;            /* simulated time after the last step               */
+  double int_energy;      /* internal work (LOCAL_INT_WORK, finite strain)    */
+  double kin_energy;      /* 0.5 m v^2                                        */
+  double ext_energy;      /* accumulated 0.5 (fext + fext_prev) dsp           */
+  double total_force[6];  /* reaction sums for bodies 1 and 2 (TOTAL_FORCE)   */
+  int64_t steps;          /* explicit steps taken                             */
+  int64_t newton_iters;   /* total return-mapping Newton iterations, last step*/
+  int64_t plastic_nodes;  /* nodes that returned plastically, last step       */
+} mega_scalars_t;
+
+/* Hot-path switches of the reference's CONTROL module (CONTROL.F90:27-95)
+ * plus the values PRE_CONTROL derives from the model.  Passed once. */
+typedef struct mega_params {
+  int32_t rk_degree;       /* RK_DEGREE; only 1 (linear basis) is live        */
+  int32_t rk_cont;         /* RK_CONT; 3 = cubic B-spline (KERNEL.F90:57-71)   */
+  int32_t rk_impl;         /* RK_IMPL; read, no effect on the live path        */
+  int32_t itype_int;       /* ITYPE_INT; 0 = direct nodal integration         */
+  int32_t ql;              /* QL (logical): quasi-linear moment regularisation */
+  int32_t lagrangian;      /* LLAGRANGIAN (logical); only 1 is on this path    */
+  int32_t finite_strain;   /* LFINITE_STRAIN (logical)                         */
+  int32_t shsup;           /* SHSUP (logical): 1 = ellipsoidal support         */
+  int32_t peridynamics;    /* PERIDYNAMICS (logical)                          */
+  int32_t inv3_exact;      /* 0 = reproduce INV3 as written (det^2 * A^-1,
+                              INVERSE.F90:119-152); 1 = true 3x3 inverse      */
+  int32_t newton_max_iter; /* return-mapping iteration cap; 20 in the reference */
+  int32_t reserved0;
+  double  ql_coef;         /* QL_COEF                                         */
+  double  ql_len;          /* QL_LEN                                          */
+  double  gravity[3];      /* IGRAVITY                                        */
+  double  dist_max[3];     /* GXDIST_MAX, GYDIST_MAX, GZDIST_MAX              */
+  double  newton_rtol;     /* rate-dependent law: relative residual tolerance */
+} mega_params;
+
+/* Fill p with the reference's defaults for the Taylor-bar deck
+ * (Control.dat: RK 1/3/0, QL on 0.001, DNI, Lagrangian, finite strain). */
+void mega_params_default(mega_params* p);
+
+/* ======================================================================== */
+/* Stateless drop-ins (copy in, compute on the GPU, copy out, synchronous)  */
+/* ======================================================================== */
+
+/* GET_BINS + SOFT_SEARCH (BIN_SEARCH.F90:2-64, 153-328) with the bin
+ * geometry HANDELER computes at LINIT (HANDELER.F90:187-250).
+ *   coo (3,n), win (3,n), sm_len (6,n), dist_max[3];
+ *   out: gn(n), gstart(n), gstack(dim_nn_list) (1-based), *gmaxn, ijk (3,n)
+ *   (GIJKSPC), *nnz.  The neighbour order is BIN_INODE's: cells IX-outer /
+ *   IZ-inner, node index order inside a cell. */
+int mega_bin_search(int32_t n, const double* coo, const double* win,
+                    const double* sm_len, const double* dist_max,
+                    int32_t itype_int, int32_t shsup,
+                    int32_t* gn, int32_t* gstart, int32_t* gstack,
+                    int64_t dim_nn_list, int32_t* gmaxn, int32_t* ijk,
+                    int64_t* nnz);
+
+/* RK1 for every node (RK.f90:16-453 via FINT.F90:404-408): shape functions
+ * and gradients at X_i for the neighbours in (gn, gstart, gstack).
+ *   ebc_nodes (n) logical; out: shp (nnz), dshp (3,nnz). */
+int mega_rk_shapes(const mega_params* p, int32_t n, const double* coo,
+                   const double* win, const int32_t* ebc_nodes,
+                   const int32_t* gn, const int32_t* gstart,
+                   const int32_t* gstack, int64_t nnz,
+                   double* shp, double* dshp);
+
+/* HUGHES_WINGET (HUGHES_WINGET.F90:16-81) for n independent nodes.
+ *   lmat (3,3,n) column-major; out: rot (3,3,n), strain (6,n), d (6,n). */
+int mega_hughes_winget(const mega_params* p, int32_t n, const double* lmat,
+                       double* rot, double* strain, double* d);
+
+/* ROTATE_TENSOR (ROTATE_TENSOR.F90:21-87) for n nodes: v <- R v R^T. */
+int mega_rotate_tensor(int32_t n, const double* rot, double* vtensor);
+
+/* CONSTITUTION (CONSTITUTION.F90:18-89) for n nodes:
+ *   stress_pred (6,n), mat_type (n), props (30,n), dlt; state (20,n) in/out;
+ *   out: stress (6,n), iters (n) Newton iterations used (may be NULL). */
+int mega_constitution(const mega_params* p, int32_t n,
+                      const double* stress_pred, const int32_t* mat_type,
+                      const double* props, double dlt, double* state,
+                      double* stress, int32_t* iters);
+
+/* CONSTRUCT_FINT (FINT.F90:16-25) with the reference's argument meaning,
+ * Lagrangian DNI path.  When linit != 0 the shape functions are computed
+ * (RK1) and written to gstack_shp / gstack_dshp; otherwise they are read.
+ * In/out arrays follow FINT.F90: gstress, gstrain (6,n), gstate (20,n).
+ * Outputs: fint, fext (3n), gmax_wvel (n), gstrain_eq (n), *gint_work
+ * (accumulated, as GINT_WORK is). */
+int mega_construct_fint(const mega_params* p, int32_t n,
+                        const double* gcoo, const double* gwin,
+                        const double* gvol, const double* gprop,
+                        const int32_t* gmat_type, const int32_t* gebc_nodes,
+                        const double* bodyforce,
+                        double* gstate, double* gstress, double* gstrain,
+                        const double* gdinc, const double* gdinc_tot,
+                        const int32_t* gn, const int32_t* gstart,
+                        const int32_t* gstack, int64_t nnz,
+                        double* gstack_shp, double* gstack_dshp,
+                        int32_t linit, double dlt,
+                        double* fint, double* fext,
+                        double* gmax_wvel, double* gstrain_eq,
+                        double* gint_work);
+
+/* CONSTRUCT_FINT_PD (FINT_PD.F90:16-759), correspondence peridynamics,
+ * Lagrangian path.  At linit != 0 the influence functions and K^-1 are built
+ * (UDFM_SHAPE_TENSOR, RK.f90:579-726) into gstack_shp and ginvk (3,3,n).
+ * gcoo_current (3,n) are the current coordinates. */
+int mega_construct_fint_pd(const mega_params* p, int32_t n,
+                           const double* gcoo, const double* gcoo_current,
+                           const double* gwin, const double* gvol,
+                           const double* gprop, const int32_t* gmat_type,
+                           double* gstate, double* gstress, double* gstrain,
+                           const double* gdinc,
+                           const int32_t* gn, const int32_t* gstart,
+                           const int32_t* gstack, int64_t nnz,
+                           double* gstack_shp, double* ginvk,
+                           int32_t linit, double dlt,
+                           double* fint, double* gmax_wvel, double* gint_work);
+
+/* ======================================================================== */
+/* Resident context: the whole MAIN.F90:304-658 loop on the device          */
+/* ======================================================================== */
+
+/* Upload the model and create a context.  Arrays as in MAIN.F90:146-221:
+ *   coo (3,n), win (3,n) normalised windows, vol (n), mass (3n), ebc (3,n)
+ *   fixity codes (0 free, 1 fixed), vinit (3,n), props (30,n), mat_type (n),
+ *   body_id (n), bodyforce (3,n) (may be NULL), sm_len (6,n).
+ * Velocity starts at vinit except on fixed DOFs (STATE_INIT.f90:97-105). */
+int mega_gpu_init(const mega_params* p, int32_t n, const double* coo,
+                  const double* win, const double* vol, const double* mass,
+                  const int32_t* ebc, const double* vinit, const double* props,
+                  const int32_t* mat_type, const int32_t* body_id,
+                  const double* bodyforce, const double* sm_len,
+                  int64_t* handle);
+
+/* Step 0 (LINIT): neighbour search and RK shapes on the device.  Optional
+ * downloads (any pointer may be NULL): gn, gstart, gstack (1-based; gstack
+ * sized dim_nn_list), shp (nnz), dshp (3,nnz). *nnz and *gmaxn returned. */
+int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart,
+                           int32_t* gstack, int64_t dim_nn_list,
+                           double* shp, double* dshp, int64_t* nnz,
+                           int32_t* gmaxn);
+
+/* Advance nsteps explicit steps of size dt (IAUTO_TS = 0 semantics) in
+ * mode (MEGA_MODE_* | MEGA_FLAG_*).  Device resident; the step sequence is
+ * captured in a CUDA graph.  Returns the accumulated device status. */
+int mega_step_resident(int64_t h, int32_t nsteps, double dt, int32_t mode);
+
+/* As mega_step_resident, and time the stepping with CUDA events recorded on
+ * the context's stream: *ms = device milliseconds for the nsteps. */
+int mega_step_timed(int64_t h, int32_t nsteps, double dt, int32_t mode,
+                    float* ms);
+
+/* Time one launch of each per-step kernel averaged over reps launches on the
+ * context stream (state is advanced reps times): out_ms[0] = stress/force
+ * kernel, out_ms[1] = force-gather/integrator kernel. */
+int mega_kernel_times(int64_t h, int32_t reps, double dt, int32_t mode,
+                      float* out_ms);
+
+/* Copy a field (enum mega_field) to host memory (sizes in the enum). */
+int mega_download(int64_t h, int32_t field, double* dst);
+/* Replace a field from host memory (DSP_TOT, VEL, ACL, STRESS, STRAIN, EPS). */
+int mega_upload(int64_t h, int32_t field, const double* src);
+int mega_get_scalars(int64_t h, mega_scalars_t* out);
+/* Device bytes held by the context. */
+int64_t mega_device_bytes(int64_t h);
+/* Number of kernels launched by the context since creation. */
+int64_t mega_kernel_launches(int64_t h);
+
+const char* mega_status_string(int32_t status);
+int mega_gpu_finalize(int64_t h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MEGA_GPU_H */

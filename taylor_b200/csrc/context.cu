@@ -1,0 +1,1091 @@
+// context.cu -- the C ABI of libmega_gpu.so: resident context (the whole
+// MAIN.F90:304-658 time loop on the device, captured in CUDA graphs) and the
+// copy-in/copy-out drop-ins for the reference's subroutines.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <set>
+#include <vector>
+#include "mega_internal.cuh"
+
+namespace mega {
+
+static thread_local char g_err[512] = {0};
+void record_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  snprintf(g_err, sizeof(g_err), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+}
+const char* last_error_text() { return g_err; }
+
+namespace {
+
+__global__ void k_fill_f32(int64_t m, const double* __restrict__ a, float* __restrict__ b) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < m) b[i] = (float)a[i];
+}
+__global__ void k_gather_pos(int64_t m, const int64_t* __restrict__ pos, const double* __restrict__ src,
+                             double* __restrict__ dst) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e < m) dst[e] = src[pos[e]];
+}
+// row sums of the stored gradients: sum_J grad0 phi_iJ (FP64 of the values
+// as stored, so the split sum of k_defgrad is exact in exact arithmetic)
+template <typename G>
+__global__ void k_rowsum3(int32_t n, const int64_t* __restrict__ rowptr, const G* __restrict__ gx,
+                          const G* __restrict__ gy, const G* __restrict__ gz, double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int64_t p = rowptr[i]; p < rowptr[i + 1]; ++p) {
+    a += (double)gx[p]; b += (double)gy[p]; c += (double)gz[p];
+  }
+  out[3 * i] = a; out[3 * i + 1] = b; out[3 * i + 2] = c;
+}
+__global__ void k_hw(int32_t n, const double* __restrict__ lmat, double* __restrict__ rot,
+                     double* __restrict__ strain, double* __restrict__ d, int exact) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double L[3][3], R[3][3], s6[6], d6[6];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) L[r][c] = lmat[9 * i + 3 * c + r];
+  hughes_winget(L, R, s6, d6, exact != 0);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) rot[9 * i + 3 * c + r] = R[r][c];
+  for (int k = 0; k < 6; ++k) { strain[6 * i + k] = s6[k]; d[6 * i + k] = d6[k]; }
+}
+__global__ void k_rotate(int32_t n, const double* __restrict__ rot, double* __restrict__ v) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double R[3][3], s[6];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) R[r][c] = rot[9 * i + 3 * c + r];
+  for (int k = 0; k < 6; ++k) s[k] = v[6 * i + k];
+  rotate_tensor(R, s);
+  for (int k = 0; k < 6; ++k) v[6 * i + k] = s[k];
+}
+__global__ void k_constitution(int32_t n, const double* __restrict__ spred, const int32_t* __restrict__ mat,
+                               const double* __restrict__ props, double dlt, int maxit, double rtol,
+                               double* __restrict__ state, double* __restrict__ stress, int32_t* __restrict__ iters,
+                               unsigned* __restrict__ status) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* pr = props + 30 * i;
+  NodeMat m;
+  m.type = mat[i]; m.nu = pr[0]; m.E = pr[1]; m.rho = pr[2]; m.sig0 = pr[3]; m.B = pr[4]; m.C = pr[5];
+  m.p7 = pr[6]; m.p8 = pr[7]; m.lam = pr[27]; m.mu = pr[28]; m.l2m = pr[29];
+  double sp[6], out[6];
+  for (int k = 0; k < 6; ++k) sp[k] = spred[6 * i + k];
+  double ep = state[20 * i + 2];
+  bool cap = false;
+  int it = 0;
+  if (m.type == MEGA_MAT_ELASTIC) {
+    for (int k = 0; k < 6; ++k) out[k] = sp[k];
+  } else if (m.type == MEGA_MAT_VONMISES) {
+    it = von_mises(sp, ep, m, maxit, out, cap);
+  } else if (m.type == MEGA_MAT_VM_RATE) {
+    double dg, ftr;
+    it = vm_rate(sp, ep, m, dlt, rtol, maxit, -1.0, out, cap, dg, ftr);
+  } else {
+    atomicOr(status, (unsigned)MEGA_ST_BAD_MATERIAL);
+    for (int k = 0; k < 6; ++k) out[k] = sp[k];
+  }
+  if (cap) atomicOr(status, (unsigned)MEGA_ST_NEWTON_CAP);
+  state[20 * i + 2] = ep;
+  for (int k = 0; k < 6; ++k) stress[6 * i + k] = out[k];
+  if (iters) iters[i] = it;
+}
+
+inline unsigned grid_for(int64_t work, int block) { return (unsigned)((work + block - 1) / block); }
+
+}  // namespace
+
+// ------------------------------------------------------------- context
+struct Ctx {
+  mega_params p{};
+  int32_t n = 0;
+  cudaStream_t s = nullptr;
+  DevPool pool;      // model + state
+  DevPool nbpool;    // neighbour structure and shapes
+  DevPool mixpool;   // float copies for the mixed mode
+  // model
+  double *coo = nullptr, *win = nullptr, *vol = nullptr, *mass = nullptr, *sm_len = nullptr;
+  double* bodyforce = nullptr;
+  int8_t *ebc = nullptr, *body_id = nullptr;
+  int32_t* ebc_nodes = nullptr;
+  uint16_t* matidx = nullptr;
+  MatEntry* mats = nullptr;
+  bool has_body = false;
+  // neighbours and shapes
+  DevCSR csr;
+  DevCSR* dcsr = nullptr;  // device copy read by the force kernel
+  bool searched = false;
+  double *shp = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *sdphi = nullptr;
+  double *tgx = nullptr, *tgy = nullptr, *tgz = nullptr, *tshp = nullptr;
+  float *fgx = nullptr, *fgy = nullptr, *fgz = nullptr, *ftgx = nullptr, *ftgy = nullptr, *ftgz = nullptr;
+  double* sdphi32 = nullptr;
+  bool mixed_ready = false;
+  // state
+  double *dsp = nullptr, *dsp_tot = nullptr, *dsp_tot_phy = nullptr, *vel = nullptr, *acl = nullptr;
+  double *fint = nullptr, *fext = nullptr, *prforce = nullptr, *stress = nullptr, *strain = nullptr;
+  double *eps = nullptr, *strain_eq = nullptr, *wvel = nullptr, *fg = nullptr, *scratch3 = nullptr;
+  void* tmat = nullptr;
+  int32_t* iters = nullptr;
+  StepAccum* acc = nullptr;
+  unsigned* status = nullptr;
+  bool phy_valid = true;
+  double time = 0.0;
+  int64_t steps = 0;
+  int64_t launches = 0;
+  // graph cache
+  cudaGraphExec_t gexec = nullptr;
+  int g_mode = -1;
+  double g_dt = 0.0;
+  int g_len = 0;
+  ~Ctx() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+static std::mutex g_ctx_mu;
+static std::set<Ctx*> g_ctxs;
+
+static Ctx* get_ctx(int64_t h) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  Ctx* c = reinterpret_cast<Ctx*>(h);
+  return g_ctxs.count(c) ? c : nullptr;
+}
+
+static int read_status(Ctx* c, bool reset) {
+  unsigned st = 0;
+  MEGA_TRY(cudaMemcpyAsync(&st, c->status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  if (reset && st) MEGA_TRY(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->s));
+  return (int)st;
+}
+
+static int ensure_mixed(Ctx* c) {
+  if (c->mixed_ready) return 0;
+  const int64_t nnz = c->csr.nnz;
+  MEGA_ALLOC(c->mixpool, c->fgx, nnz);
+  MEGA_ALLOC(c->mixpool, c->fgy, nnz);
+  MEGA_ALLOC(c->mixpool, c->fgz, nnz);
+  MEGA_ALLOC(c->mixpool, c->ftgx, nnz);
+  MEGA_ALLOC(c->mixpool, c->ftgy, nnz);
+  MEGA_ALLOC(c->mixpool, c->ftgz, nnz);
+  MEGA_ALLOC(c->mixpool, c->sdphi32, 3 * (int64_t)c->n);
+  const unsigned g = grid_for(nnz, 256);
+  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->gx, c->fgx);
+  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->gy, c->fgy);
+  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->gz, c->fgz);
+  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->tgx, c->ftgx);
+  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->tgy, c->ftgy);
+  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->tgz, c->ftgz);
+  k_rowsum3<float><<<grid_for(c->n, 256), 256, 0, c->s>>>(c->n, c->csr.rowptr, c->fgx, c->fgy, c->fgz, c->sdphi32);
+  MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  c->mixed_ready = true;
+  return 0;
+}
+
+static StressArgs stress_args(Ctx* c, double dt, int mode) {
+  StressArgs a{};
+  a.n = c->n; a.fg = c->fg; a.matidx = c->matidx; a.mats = c->mats; a.vol = c->vol;
+  a.stress = c->stress; a.strain = c->strain; a.eps = c->eps; a.strain_eq = c->strain_eq; a.wvel = c->wvel;
+  a.tmat = c->tmat; a.bodyforce = c->bodyforce;
+  a.grav[0] = c->p.gravity[0]; a.grav[1] = c->p.gravity[1]; a.grav[2] = c->p.gravity[2];
+  a.has_body = c->has_body; a.inv3_exact = c->p.inv3_exact; a.finite_strain = c->p.finite_strain;
+  a.maxit = c->p.newton_max_iter; a.rtol = c->p.newton_rtol; a.dt = dt; a.iters = c->iters;
+  a.mlp_guess = nullptr; a.rate_samples = nullptr; a.acc = c->acc; a.status = c->status;
+  (void)mode;
+  return a;
+}
+
+static ForceArgs force_args(Ctx* c, double dt, int mode, int predict) {
+  const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
+  ForceArgs f{};
+  f.n = c->n; f.csr = nullptr;
+  f.tgx = mixed ? (const void*)c->ftgx : (const void*)c->tgx;
+  f.tgy = mixed ? (const void*)c->ftgy : (const void*)c->tgy;
+  f.tgz = mixed ? (const void*)c->ftgz : (const void*)c->tgz;
+  f.tshp = c->tshp; f.tmat = c->tmat; f.has_body = c->has_body; f.integrate = 1; f.predict = predict;
+  f.ebc = c->ebc; f.mass = c->mass; f.matidx = c->matidx; f.mats = c->mats; f.body_id = c->body_id;
+  f.fint = c->fint; f.fext = c->fext; f.vel = c->vel; f.acl = c->acl; f.dsp = c->dsp; f.dsp_tot = c->dsp_tot;
+  f.prforce = c->prforce; f.dt = dt; f.acc = c->acc; f.status = c->status;
+  return f;
+}
+
+// The force kernel reads the CSC through a device-visible copy of DevCSR.
+static DevCSR* dev_csr_copy(Ctx* c) { return c->dcsr; }
+
+static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) {
+  const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
+  const bool interp = (mode & MEGA_FLAG_INTERP_EACH_STEP) != 0;
+  if (ev) MEGA_TRY(cudaEventRecord(ev[0], c->s));
+  int r = launch_defgrad(c->s, mixed, interp, c->n, c->csr, mixed ? (const void*)c->fgx : (const void*)c->gx,
+                         mixed ? (const void*)c->fgy : (const void*)c->gy,
+                         mixed ? (const void*)c->fgz : (const void*)c->gz, c->dsp, c->dsp_tot,
+                         mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc);
+  if (r) return r;
+  if (ev) MEGA_TRY(cudaEventRecord(ev[1], c->s));
+  r = launch_stress(c->s, mixed, stress_args(c, dt, mode));
+  if (r) return r;
+  if (ev) MEGA_TRY(cudaEventRecord(ev[2], c->s));
+  ForceArgs f = force_args(c, dt, mode, predict);
+  f.csr = dev_csr_copy(c);
+  if (!f.csr) return MEGA_ERR_NOMEM;
+  r = launch_force(c->s, mixed, f);
+  if (r) return r;
+  if (ev) MEGA_TRY(cudaEventRecord(ev[3], c->s));
+  c->launches += 3;
+  return 0;
+}
+
+static int graph_for(Ctx* c, double dt, int mode, int len) {
+  if (c->gexec && c->g_mode == mode && c->g_dt == dt && c->g_len == len) return 0;
+  if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+  if (!dev_csr_copy(c)) return MEGA_ERR_NOMEM;
+  cudaGraph_t g = nullptr;
+  MEGA_TRY(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
+  const int64_t before = c->launches;
+  int r = 0;
+  for (int k = 0; k < len && !r; ++k) r = step_once(c, dt, mode, 1, nullptr);
+  cudaError_t e = cudaStreamEndCapture(c->s, &g);
+  c->launches = before;
+  if (r) { if (g) cudaGraphDestroy(g); return r; }
+  if (e != cudaSuccess) { record_cuda_error(e, "cudaStreamEndCapture", __FILE__, __LINE__); return MEGA_ERR_CUDA; }
+  e = cudaGraphInstantiate(&c->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { record_cuda_error(e, "cudaGraphInstantiate", __FILE__, __LINE__); return MEGA_ERR_CUDA; }
+  c->g_mode = mode; c->g_dt = dt; c->g_len = len;
+  return 0;
+}
+
+static int run_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
+  if (!c->searched) return MEGA_ERR_STATE;
+  if (nsteps <= 0) return 0;
+  const int prec = mode & 0xff;
+  if (prec != MEGA_MODE_FP64 && prec != MEGA_MODE_MIXED) return MEGA_ERR_ARG;
+  if (prec == MEGA_MODE_MIXED) { int r = ensure_mixed(c); if (r) return r; }
+  if (!(mode & MEGA_FLAG_INTERP_EACH_STEP)) c->phy_valid = false;
+  int r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
+  if (r) return r;
+  c->launches += 1;
+  int32_t rem = nsteps - 1;
+  const int len = 16;
+  if (rem >= len) {
+    r = graph_for(c, dt, mode, len);
+    if (r) return r;
+    while (rem >= len) {
+      MEGA_TRY(cudaGraphLaunch(c->gexec, c->s));
+      c->launches += 3 * len;
+      rem -= len;
+    }
+  }
+  for (; rem > 0 && !r; --rem) r = step_once(c, dt, mode, 1, nullptr);
+  if (r) return r;
+  r = step_once(c, dt, mode, 0, nullptr);
+  if (r) return r;
+  for (int32_t k = 0; k < nsteps; ++k) c->time = c->time + dt;  // TIME = TIME + DLT
+  c->steps += nsteps;
+  return 0;
+}
+
+// Host-side deduplication of PROPS(30,N) into a small table.
+static int build_materials(Ctx* c, const double* props, const int32_t* mat_type) {
+  std::map<std::vector<double>, uint16_t> tab;
+  std::vector<uint16_t> idx(c->n);
+  std::vector<MatEntry> ents;
+  int64_t prev = -1;
+  for (int32_t i = 0; i < c->n; ++i) {
+    // fast path: same PROPS row and type as the previous node
+    if (prev >= 0 && mat_type[i] == mat_type[prev] &&
+        std::memcmp(props + 30 * (size_t)i, props + 30 * (size_t)prev, 30 * sizeof(double)) == 0) {
+      idx[i] = idx[prev];
+      prev = i;
+      continue;
+    }
+    prev = i;
+    std::vector<double> key(props + 30 * (size_t)i, props + 30 * (size_t)i + 30);
+    key.push_back((double)mat_type[i]);
+    auto it = tab.find(key);
+    if (it == tab.end()) {
+      if (ents.size() >= 65535) return MEGA_ERR_UNSUPPORTED;
+      MatEntry e{};
+      const double* pr = props + 30 * (size_t)i;
+      e.type = mat_type[i];
+      e.nu = pr[0]; e.E = pr[1]; e.rho = pr[2]; e.sig0 = pr[3]; e.B = pr[4]; e.C = pr[5];
+      e.p7 = pr[6]; e.p8 = pr[7]; e.damp = pr[20]; e.lam = pr[27]; e.mu = pr[28]; e.l2m = pr[29];
+      uint16_t id = (uint16_t)ents.size();
+      ents.push_back(e);
+      it = tab.emplace(key, id).first;
+    }
+    idx[i] = it->second;
+  }
+  MEGA_ALLOC(c->pool, c->matidx, c->n);
+  MEGA_ALLOC(c->pool, c->mats, ents.size());
+  MEGA_TRY(cudaMemcpyAsync(c->matidx, idx.data(), sizeof(uint16_t) * c->n, cudaMemcpyHostToDevice, c->s));
+  MEGA_TRY(cudaMemcpyAsync(c->mats, ents.data(), sizeof(MatEntry) * ents.size(), cudaMemcpyHostToDevice, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  return 0;
+}
+
+template <typename T>
+static int upload(cudaStream_t s, T* d, const T* h, size_t count) {
+  MEGA_TRY(cudaMemcpyAsync(d, h, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+  return 0;
+}
+
+// Device CSR from the reference's 1-based (GN, GSTART, GSTACK); rows are
+// re-packed contiguously in node order.  hpos[k] = 0-based GSTACK position
+// of packed entry k (for writing per-entry values back).
+static int csr_from_host(cudaStream_t s, int32_t n, const int32_t* gn, const int32_t* gstart,
+                         const int32_t* gstack, int64_t nnz_cap, DevPool& pool, DevCSR& csr,
+                         std::vector<int64_t>& hpos) {
+  std::vector<int64_t> rp(n + 1, 0);
+  for (int32_t i = 0; i < n; ++i) {
+    if (gn[i] < 0) return MEGA_ERR_ARG;
+    rp[i + 1] = rp[i] + gn[i];
+  }
+  const int64_t nnz = rp[n];
+  std::vector<int32_t> col(nnz);
+  hpos.resize(nnz);
+  for (int32_t i = 0; i < n; ++i) {
+    const int64_t s0 = (int64_t)gstart[i] - 1;
+    if (gn[i] > 0 && (s0 < 0 || s0 + gn[i] > nnz_cap)) return MEGA_ERR_ARG;
+    for (int32_t k = 0; k < gn[i]; ++k) {
+      const int32_t j = gstack[s0 + k] - 1;
+      if (j < 0 || j >= n) return MEGA_ERR_ARG;
+      col[rp[i] + k] = j;
+      hpos[rp[i] + k] = s0 + k;
+    }
+  }
+  csr.n = n;
+  csr.nnz = nnz;
+  csr.gmaxn = 0;
+  for (int32_t i = 0; i < n; ++i) csr.gmaxn = std::max(csr.gmaxn, gn[i]);
+  MEGA_ALLOC(pool, csr.rowptr, n + 1);
+  MEGA_ALLOC(pool, csr.col, nnz);
+  int r = upload(s, csr.rowptr, rp.data(), n + 1);
+  if (r) return r;
+  return upload(s, csr.col, col.data(), nnz);
+}
+
+static int make_stream(cudaStream_t* s) {
+  MEGA_TRY(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
+  return 0;
+}
+
+struct StreamGuard {
+  cudaStream_t s = nullptr;
+  ~StreamGuard() { if (s) cudaStreamDestroy(s); }
+};
+
+}  // namespace mega
+
+using namespace mega;
+
+extern "C" {
+
+void mega_params_default(mega_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->rk_degree = 1;
+  p->rk_cont = 3;
+  p->rk_impl = 0;
+  p->itype_int = 0;
+  p->ql = 1;
+  p->lagrangian = 1;
+  p->finite_strain = 1;
+  p->shsup = 0;
+  p->peridynamics = 0;
+  p->inv3_exact = 0;
+  p->newton_max_iter = 20;
+  p->ql_coef = 0.001;
+  p->ql_len = 0.0;
+  p->newton_rtol = 1e-10;
+}
+
+const char* mega_status_string(int32_t st) {
+  static thread_local char buf[768];
+  if (st == 0) return "ok";
+  if (st < 0) {
+    const char* w = st == MEGA_ERR_CUDA ? "CUDA error" : st == MEGA_ERR_ARG ? "invalid argument"
+                  : st == MEGA_ERR_HANDLE ? "invalid handle" : st == MEGA_ERR_STATE ? "call out of order"
+                  : st == MEGA_ERR_NOMEM ? "device allocation failed"
+                  : st == MEGA_ERR_UNSUPPORTED ? "configuration not supported on this path" : "error";
+    snprintf(buf, sizeof(buf), "%s%s%s", w, last_error_text()[0] ? ": " : "", last_error_text());
+    return buf;
+  }
+  buf[0] = 0;
+  struct { int bit; const char* t; } tab[] = {
+      {MEGA_ST_NEWTON_CAP, "PLASTICITY MATERIAL MODEL DID NOT CONVERGE"},
+      {MEGA_ST_SINGULAR_MOMENT, "singular RK moment matrix"},
+      {MEGA_ST_BIN_OVERFLOW, "(NODES_IN_BIN(M).GE.MAX_NEIGH)"},
+      {MEGA_ST_CAND_OVERFLOW, "IP.GT.10000"},
+      {MEGA_ST_NONFINITE, "non-finite force or stress"},
+      {MEGA_ST_BAD_MATERIAL, "INVALID MATERIAL TYPE IN SUBROUTINE CONSTITUTION"},
+      {MEGA_ST_STACK_OVERFLOW, "neighbour stack larger than DIM_NN_LIST"},
+      {MEGA_ST_SINGULAR_SHAPE, "PROBLEM INVERTING MATRIX"}};
+  for (auto& t : tab)
+    if (st & t.bit) {
+      if (buf[0]) strncat(buf, "; ", sizeof(buf) - strlen(buf) - 1);
+      strncat(buf, t.t, sizeof(buf) - strlen(buf) - 1);
+    }
+  return buf;
+}
+
+int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const double* win, const double* vol,
+                  const double* mass, const int32_t* ebc, const double* vinit, const double* props,
+                  const int32_t* mat_type, const int32_t* body_id, const double* bodyforce,
+                  const double* sm_len, int64_t* handle) {
+  if (!p || n <= 0 || !coo || !win || !vol || !mass || !ebc || !vinit || !props || !mat_type || !sm_len || !handle)
+    return MEGA_ERR_ARG;
+  if (p->lagrangian != 1 || p->peridynamics != 0) return MEGA_ERR_UNSUPPORTED;
+  for (int64_t m = 0; m < 3 * (int64_t)n; ++m)
+    if (ebc[m] != 0 && ebc[m] != 1) return MEGA_ERR_UNSUPPORTED;  // prescribed-velocity fixity (code 2)
+  Ctx* c = new Ctx();
+  c->p = *p;
+  c->n = n;
+  int r = make_stream(&c->s);
+  const int64_t n3 = 3 * (int64_t)n;
+  auto fail = [&](int code) { delete c; return code; };
+  if (r) return fail(r);
+#define CA(ptr, cnt) do { if (c->pool.alloc(&(ptr), (size_t)(cnt))) return fail(MEGA_ERR_NOMEM); } while (0)
+  CA(c->coo, n3); CA(c->win, n3); CA(c->vol, n); CA(c->mass, n3); CA(c->sm_len, 6 * (int64_t)n);
+  CA(c->ebc, n3); CA(c->body_id, n); CA(c->ebc_nodes, n);
+  CA(c->dsp, n3); CA(c->dsp_tot, n3); CA(c->dsp_tot_phy, n3); CA(c->vel, n3); CA(c->acl, n3);
+  CA(c->fint, n3); CA(c->fext, n3); CA(c->prforce, n3); CA(c->scratch3, n3);
+  CA(c->stress, 6 * (int64_t)n); CA(c->strain, 6 * (int64_t)n); CA(c->eps, n); CA(c->strain_eq, n);
+  CA(c->wvel, n); CA(c->fg, 18 * (int64_t)n); CA(c->iters, n); CA(c->acc, 1); CA(c->status, 1);
+  {
+    double* t = nullptr;
+    CA(t, 12 * (int64_t)n);
+    c->tmat = t;
+  }
+  c->has_body = p->gravity[0] != 0.0 || p->gravity[1] != 0.0 || p->gravity[2] != 0.0;
+  if (bodyforce) {
+    for (int64_t m = 0; m < n3 && !c->has_body; ++m) c->has_body = bodyforce[m] != 0.0;
+    if (c->has_body) {
+      CA(c->bodyforce, n3);
+      if (upload(c->s, c->bodyforce, bodyforce, n3)) return fail(MEGA_ERR_CUDA);
+    }
+  }
+#undef CA
+  std::vector<int8_t> hebc(n3), hbody(n);
+  std::vector<int32_t> hen(n, 0);
+  std::vector<double> v0(n3);
+  for (int32_t i = 0; i < n; ++i) {
+    hbody[i] = (int8_t)(body_id ? body_id[i] : 1);
+    for (int j = 0; j < 3; ++j) {
+      const int64_t m = 3 * (int64_t)i + j;
+      hebc[m] = (int8_t)ebc[m];
+      if (ebc[m] == 1) { v0[m] = 0.0; hen[i] = 1; }  // STATE_INIT.f90:97-105
+      else v0[m] = vinit[m];
+    }
+  }
+  if (upload(c->s, c->coo, coo, n3) || upload(c->s, c->win, win, n3) || upload(c->s, c->vol, vol, n) ||
+      upload(c->s, c->mass, mass, n3) || upload(c->s, c->sm_len, sm_len, 6 * (size_t)n) ||
+      upload(c->s, c->ebc, hebc.data(), n3) || upload(c->s, c->body_id, hbody.data(), n) ||
+      upload(c->s, c->ebc_nodes, hen.data(), n) || upload(c->s, c->vel, v0.data(), n3))
+    return fail(MEGA_ERR_CUDA);
+  cudaMemsetAsync(c->dsp, 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->dsp_tot, 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->dsp_tot_phy, 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->acl, 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->fint, 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->fext, 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->prforce, 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->stress, 0, sizeof(double) * 6 * n, c->s);
+  cudaMemsetAsync(c->strain, 0, sizeof(double) * 6 * n, c->s);
+  cudaMemsetAsync(c->eps, 0, sizeof(double) * n, c->s);
+  cudaMemsetAsync(c->strain_eq, 0, sizeof(double) * n, c->s);
+  cudaMemsetAsync(c->wvel, 0, sizeof(double) * n, c->s);
+  cudaMemsetAsync(c->acc, 0, sizeof(StepAccum), c->s);
+  cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->s);
+  cudaMemsetAsync(c->tmat, 0, sizeof(double) * 12 * n, c->s);
+  if (cudaStreamSynchronize(c->s) != cudaSuccess) return fail(MEGA_ERR_CUDA);
+  r = build_materials(c, props, mat_type);
+  if (r) return fail(r);
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    g_ctxs.insert(c);
+  }
+  *handle = reinterpret_cast<int64_t>(c);
+  return 0;
+}
+
+int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gstack, int64_t dim_nn_list,
+                           double* shp, double* dshp, int64_t* nnz, int32_t* gmaxn) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (c->searched) {
+    c->nbpool.free_all();
+    c->mixpool.free_all();
+    c->mixed_ready = false;
+    c->csr = DevCSR();
+    c->dcsr = nullptr;
+    c->searched = false;
+    if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+  }
+  int r = bin_search(c->s, c->n, c->coo, c->win, c->sm_len, c->p.dist_max, c->p.itype_int, c->p.shsup, c->status,
+                     c->csr, nullptr, c->nbpool, nullptr);
+  if (r) return r;
+  r = build_transpose(c->s, c->csr, c->nbpool);
+  if (r) return r;
+  const int64_t nnz_ = c->csr.nnz;
+  MEGA_ALLOC(c->nbpool, c->shp, nnz_);
+  MEGA_ALLOC(c->nbpool, c->gx, nnz_);
+  MEGA_ALLOC(c->nbpool, c->gy, nnz_);
+  MEGA_ALLOC(c->nbpool, c->gz, nnz_);
+  MEGA_ALLOC(c->nbpool, c->tgx, nnz_);
+  MEGA_ALLOC(c->nbpool, c->tgy, nnz_);
+  MEGA_ALLOC(c->nbpool, c->tgz, nnz_);
+  MEGA_ALLOC(c->nbpool, c->sdphi, 3 * (int64_t)c->n);
+  if (c->has_body) MEGA_ALLOC(c->nbpool, c->tshp, nnz_);
+  r = rk_shapes(c->s, c->p, c->n, c->coo, c->win, c->ebc_nodes, c->csr, c->shp, c->gx, c->gy, c->gz, c->status);
+  if (r) return r;
+  const unsigned g = grid_for(nnz_, 256);
+  k_gather_pos<<<g, 256, 0, c->s>>>(nnz_, c->csr.tpos, c->gx, c->tgx);
+  k_gather_pos<<<g, 256, 0, c->s>>>(nnz_, c->csr.tpos, c->gy, c->tgy);
+  k_gather_pos<<<g, 256, 0, c->s>>>(nnz_, c->csr.tpos, c->gz, c->tgz);
+  if (c->has_body) k_gather_pos<<<g, 256, 0, c->s>>>(nnz_, c->csr.tpos, c->shp, c->tshp);
+  k_rowsum3<double><<<grid_for(c->n, 256), 256, 0, c->s>>>(c->n, c->csr.rowptr, c->gx, c->gy, c->gz, c->sdphi);
+  MEGA_CHECK_LAUNCH();
+  MEGA_ALLOC(c->nbpool, c->dcsr, 1);
+  MEGA_TRY(cudaMemcpyAsync(c->dcsr, &c->csr, sizeof(DevCSR), cudaMemcpyHostToDevice, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  c->searched = true;
+  if (nnz) *nnz = nnz_;
+  if (gmaxn) *gmaxn = c->csr.gmaxn;
+  // optional downloads in the reference's layout
+  std::vector<int64_t> rp;
+  if (gn || gstart || gstack || shp || dshp) {
+    rp.resize(c->n + 1);
+    MEGA_TRY(cudaMemcpyAsync(rp.data(), c->csr.rowptr, sizeof(int64_t) * (c->n + 1), cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+  }
+  int st = 0;
+  if (gn || gstart) {
+    for (int32_t i = 0; i < c->n; ++i) {
+      if (gn) gn[i] = (int32_t)(rp[i + 1] - rp[i]);
+      if (gstart) gstart[i] = (int32_t)(rp[i] + 1);
+    }
+  }
+  if (gstack) {
+    if (nnz_ > dim_nn_list) st |= MEGA_ST_STACK_OVERFLOW;
+    else {
+      MEGA_TRY(cudaMemcpyAsync(gstack, c->csr.col, sizeof(int32_t) * nnz_, cudaMemcpyDeviceToHost, c->s));
+      MEGA_TRY(cudaStreamSynchronize(c->s));
+      for (int64_t k = 0; k < nnz_; ++k) gstack[k] += 1;
+    }
+  }
+  if (shp) MEGA_TRY(cudaMemcpyAsync(shp, c->shp, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, c->s));
+  if (dshp) {
+    std::vector<double> a(nnz_), b(nnz_), d(nnz_);
+    MEGA_TRY(cudaMemcpyAsync(a.data(), c->gx, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaMemcpyAsync(b.data(), c->gy, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaMemcpyAsync(d.data(), c->gz, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    for (int64_t k = 0; k < nnz_; ++k) { dshp[3 * k] = a[k]; dshp[3 * k + 1] = b[k]; dshp[3 * k + 2] = d[k]; }
+  }
+  int ds = read_status(c, true);
+  if (ds < 0) return ds;
+  return st | ds;
+}
+
+int mega_step_resident(int64_t h, int32_t nsteps, double dt, int32_t mode) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  int r = run_steps(c, nsteps, dt, mode);
+  if (r) return r;
+  return read_status(c, true);
+}
+
+int mega_step_timed(int64_t h, int32_t nsteps, double dt, int32_t mode, float* ms) {
+  Ctx* c = get_ctx(h);
+  if (!c || !ms) return c ? MEGA_ERR_ARG : MEGA_ERR_HANDLE;
+  if (c->searched && (mode & 0xff) == MEGA_MODE_MIXED) { int r = ensure_mixed(c); if (r) return r; }
+  if (c->searched && nsteps > 16) { int r = graph_for(c, dt, mode, 16); if (r) return r; }
+  cudaEvent_t e0, e1;
+  MEGA_TRY(cudaEventCreate(&e0));
+  MEGA_TRY(cudaEventCreate(&e1));
+  MEGA_TRY(cudaEventRecord(e0, c->s));
+  int r = run_steps(c, nsteps, dt, mode);
+  if (!r) {
+    cudaEventRecord(e1, c->s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r) return r;
+  return read_status(c, true);
+}
+
+int mega_kernel_times(int64_t h, int32_t reps, double dt, int32_t mode, float* out_ms) {
+  Ctx* c = get_ctx(h);
+  if (!c || !out_ms || reps <= 0) return c ? MEGA_ERR_ARG : MEGA_ERR_HANDLE;
+  if (!c->searched) return MEGA_ERR_STATE;
+  if ((mode & 0xff) == MEGA_MODE_MIXED) { int r = ensure_mixed(c); if (r) return r; }
+  if (!(mode & MEGA_FLAG_INTERP_EACH_STEP)) c->phy_valid = false;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) MEGA_TRY(cudaEventCreate(&e));
+  double acc[3] = {0, 0, 0};
+  int r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
+  for (int32_t k = 0; k < reps && !r; ++k) {
+    r = step_once(c, dt, mode, k < reps - 1 ? 1 : 0, ev);
+    if (r) break;
+    cudaEventSynchronize(ev[3]);
+    float t;
+    for (int q = 0; q < 3; ++q) {
+      cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+      acc[q] += t;
+    }
+    c->time = c->time + dt;
+    c->steps += 1;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (r) return r;
+  for (int q = 0; q < 3; ++q) out_ms[q] = (float)(acc[q] / reps);
+  return read_status(c, true);
+}
+
+int mega_download(int64_t h, int32_t field, double* dst) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (!dst) return MEGA_ERR_ARG;
+  const int64_t n = c->n, n3 = 3 * n;
+  const double* src = nullptr;
+  int64_t cnt = 0;
+  switch (field) {
+    case MEGA_F_DSP: src = c->dsp; cnt = n3; break;
+    case MEGA_F_DSP_TOT: src = c->dsp_tot; cnt = n3; break;
+    case MEGA_F_VEL: src = c->vel; cnt = n3; break;
+    case MEGA_F_ACL: src = c->acl; cnt = n3; break;
+    case MEGA_F_FINT: src = c->fint; cnt = n3; break;
+    case MEGA_F_FEXT: src = c->fext; cnt = n3; break;
+    case MEGA_F_STRESS: src = c->stress; cnt = 6 * n; break;
+    case MEGA_F_STRAIN: src = c->strain; cnt = 6 * n; break;
+    case MEGA_F_EPS: src = c->eps; cnt = n; break;
+    case MEGA_F_STRAIN_EQ: src = c->strain_eq; cnt = n; break;
+    case MEGA_F_WAVE_VEL: src = c->wvel; cnt = n; break;
+    case MEGA_F_PRFORCE: src = c->prforce; cnt = n3; break;
+    case MEGA_F_NEWTON_IT: {
+      std::vector<int32_t> it(n);
+      MEGA_TRY(cudaMemcpyAsync(it.data(), c->iters, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c->s));
+      MEGA_TRY(cudaStreamSynchronize(c->s));
+      for (int64_t i = 0; i < n; ++i) dst[i] = it[i];
+      return 0;
+    }
+    case MEGA_F_DSP_TOT_PHY:
+    case MEGA_F_COO_CURRENT: {
+      const double* phy = c->dsp_tot_phy;
+      if (!c->phy_valid) {
+        if (!c->searched) return MEGA_ERR_STATE;
+        int r = launch_interp(c->s, c->n, c->csr, c->shp, c->dsp_tot, nullptr, c->scratch3);
+        if (r) return r;
+        phy = c->scratch3;
+      }
+      std::vector<double> a(n3);
+      MEGA_TRY(cudaMemcpyAsync(a.data(), phy, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->s));
+      if (field == MEGA_F_COO_CURRENT) {
+        std::vector<double> x(n3);
+        MEGA_TRY(cudaMemcpyAsync(x.data(), c->coo, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->s));
+        MEGA_TRY(cudaStreamSynchronize(c->s));
+        for (int64_t m = 0; m < n3; ++m) dst[m] = x[m] + a[m];  // MAIN.F90:382-386
+      } else {
+        MEGA_TRY(cudaStreamSynchronize(c->s));
+        std::memcpy(dst, a.data(), sizeof(double) * n3);
+      }
+      return 0;
+    }
+    default: return MEGA_ERR_ARG;
+  }
+  MEGA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  return 0;
+}
+
+int mega_upload(int64_t h, int32_t field, const double* src) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (!src) return MEGA_ERR_ARG;
+  const int64_t n = c->n, n3 = 3 * n;
+  double* dst = nullptr;
+  int64_t cnt = 0;
+  switch (field) {
+    case MEGA_F_DSP: dst = c->dsp; cnt = n3; break;
+    case MEGA_F_DSP_TOT: dst = c->dsp_tot; cnt = n3; c->phy_valid = false; break;
+    case MEGA_F_VEL: dst = c->vel; cnt = n3; break;
+    case MEGA_F_ACL: dst = c->acl; cnt = n3; break;
+    case MEGA_F_FEXT: dst = c->fext; cnt = n3; break;
+    case MEGA_F_STRESS: dst = c->stress; cnt = 6 * n; break;
+    case MEGA_F_STRAIN: dst = c->strain; cnt = 6 * n; break;
+    case MEGA_F_EPS: dst = c->eps; cnt = n; break;
+    default: return MEGA_ERR_ARG;
+  }
+  MEGA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyHostToDevice, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  return 0;
+}
+
+int mega_get_scalars(int64_t h, mega_scalars_t* out) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (!out) return MEGA_ERR_ARG;
+  StepAccum a;
+  MEGA_TRY(cudaMemcpyAsync(&a, c->acc, sizeof(a), cudaMemcpyDeviceToHost, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  out->time = c->time;
+  out->int_energy = a.int_work;
+  out->kin_energy = a.ke;
+  out->ext_energy = a.ee;
+  for (int k = 0; k < 6; ++k) out->total_force[k] = a.total_force[k];
+  out->steps = c->steps;
+  out->newton_iters = (int64_t)a.newton_iters;
+  out->plastic_nodes = (int64_t)a.plastic;
+  return 0;
+}
+
+int64_t mega_device_bytes(int64_t h) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  return c->pool.bytes + c->nbpool.bytes + c->mixpool.bytes;
+}
+
+int64_t mega_kernel_launches(int64_t h) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  return c->launches;
+}
+
+int mega_gpu_finalize(int64_t h) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    g_ctxs.erase(c);
+  }
+  cudaStreamSynchronize(c->s);
+  delete c;
+  return 0;
+}
+
+// ------------------------------------------------ stateless drop-ins
+int mega_bin_search(int32_t n, const double* coo, const double* win, const double* sm_len, const double* dist_max,
+                    int32_t itype_int, int32_t shsup, int32_t* gn, int32_t* gstart, int32_t* gstack,
+                    int64_t dim_nn_list, int32_t* gmaxn, int32_t* ijk, int64_t* nnz) {
+  if (n <= 0 || !coo || !win || !sm_len || !dist_max || !gn || !gstart || !gstack || !gmaxn) return MEGA_ERR_ARG;
+  StreamGuard sg;
+  int r = make_stream(&sg.s);
+  if (r) return r;
+  cudaStream_t s = sg.s;
+  DevPool pool;
+  double *dc, *dw, *ds;
+  int32_t* dijk = nullptr;
+  unsigned* st;
+  MEGA_ALLOC(pool, dc, 3 * (int64_t)n);
+  MEGA_ALLOC(pool, dw, 3 * (int64_t)n);
+  MEGA_ALLOC(pool, ds, 6 * (int64_t)n);
+  MEGA_ALLOC(pool, st, 1);
+  if (ijk) MEGA_ALLOC(pool, dijk, 3 * (int64_t)n);
+  if ((r = upload(s, dc, coo, 3 * (size_t)n)) || (r = upload(s, dw, win, 3 * (size_t)n)) ||
+      (r = upload(s, ds, sm_len, 6 * (size_t)n)))
+    return r;
+  MEGA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
+  DevCSR csr;
+  r = bin_search(s, n, dc, dw, ds, dist_max, itype_int, shsup, st, csr, dijk, pool, nullptr);
+  if (r) return r;
+  std::vector<int64_t> rp(n + 1);
+  MEGA_TRY(cudaMemcpyAsync(rp.data(), csr.rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+  unsigned hst = 0;
+  MEGA_TRY(cudaMemcpyAsync(&hst, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  if (ijk) MEGA_TRY(cudaMemcpyAsync(ijk, dijk, sizeof(int32_t) * 3 * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaStreamSynchronize(s));
+  for (int32_t i = 0; i < n; ++i) {
+    gn[i] = (int32_t)(rp[i + 1] - rp[i]);
+    gstart[i] = (int32_t)(rp[i] + 1);
+  }
+  *gmaxn = csr.gmaxn;
+  if (nnz) *nnz = csr.nnz;
+  if (csr.nnz > dim_nn_list) return (int)(hst | MEGA_ST_STACK_OVERFLOW);
+  MEGA_TRY(cudaMemcpyAsync(gstack, csr.col, sizeof(int32_t) * csr.nnz, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaStreamSynchronize(s));
+  for (int64_t k = 0; k < csr.nnz; ++k) gstack[k] += 1;
+  return (int)hst;
+}
+
+int mega_rk_shapes(const mega_params* p, int32_t n, const double* coo, const double* win, const int32_t* ebc_nodes,
+                   const int32_t* gn, const int32_t* gstart, const int32_t* gstack, int64_t nnz, double* shp,
+                   double* dshp) {
+  if (!p || n <= 0 || !coo || !win || !gn || !gstart || !gstack || !shp || !dshp) return MEGA_ERR_ARG;
+  StreamGuard sg;
+  int r = make_stream(&sg.s);
+  if (r) return r;
+  cudaStream_t s = sg.s;
+  DevPool pool;
+  DevCSR csr;
+  std::vector<int64_t> hpos;
+  r = csr_from_host(s, n, gn, gstart, gstack, nnz, pool, csr, hpos);
+  if (r) return r;
+  double *dc, *dw, *dshp0, *dgx, *dgy, *dgz;
+  int32_t* den = nullptr;
+  unsigned* st;
+  MEGA_ALLOC(pool, dc, 3 * (int64_t)n);
+  MEGA_ALLOC(pool, dw, 3 * (int64_t)n);
+  MEGA_ALLOC(pool, st, 1);
+  if (ebc_nodes) MEGA_ALLOC(pool, den, n);
+  MEGA_ALLOC(pool, dshp0, csr.nnz);
+  MEGA_ALLOC(pool, dgx, csr.nnz);
+  MEGA_ALLOC(pool, dgy, csr.nnz);
+  MEGA_ALLOC(pool, dgz, csr.nnz);
+  if ((r = upload(s, dc, coo, 3 * (size_t)n)) || (r = upload(s, dw, win, 3 * (size_t)n))) return r;
+  if (ebc_nodes && (r = upload(s, den, ebc_nodes, (size_t)n))) return r;
+  MEGA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
+  r = rk_shapes(s, *p, n, dc, dw, den, csr, dshp0, dgx, dgy, dgz, st);
+  if (r) return r;
+  std::vector<double> a(csr.nnz), b(csr.nnz), d(csr.nnz), e(csr.nnz);
+  unsigned hst = 0;
+  MEGA_TRY(cudaMemcpyAsync(a.data(), dshp0, sizeof(double) * csr.nnz, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(b.data(), dgx, sizeof(double) * csr.nnz, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(d.data(), dgy, sizeof(double) * csr.nnz, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(e.data(), dgz, sizeof(double) * csr.nnz, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(&hst, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaStreamSynchronize(s));
+  for (int64_t k = 0; k < csr.nnz; ++k) {
+    const int64_t q = hpos[k];
+    shp[q] = a[k];
+    dshp[3 * q] = b[k]; dshp[3 * q + 1] = d[k]; dshp[3 * q + 2] = e[k];
+  }
+  return (int)hst;
+}
+
+int mega_hughes_winget(const mega_params* p, int32_t n, const double* lmat, double* rot, double* strain, double* d) {
+  if (!p || n <= 0 || !lmat || !rot || !strain || !d) return MEGA_ERR_ARG;
+  StreamGuard sg;
+  int r = make_stream(&sg.s);
+  if (r) return r;
+  DevPool pool;
+  double *dl, *dr, *ds, *dd;
+  MEGA_ALLOC(pool, dl, 9 * (int64_t)n);
+  MEGA_ALLOC(pool, dr, 9 * (int64_t)n);
+  MEGA_ALLOC(pool, ds, 6 * (int64_t)n);
+  MEGA_ALLOC(pool, dd, 6 * (int64_t)n);
+  if ((r = upload(sg.s, dl, lmat, 9 * (size_t)n))) return r;
+  k_hw<<<grid_for(n, 128), 128, 0, sg.s>>>(n, dl, dr, ds, dd, p->inv3_exact);
+  MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaMemcpyAsync(rot, dr, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, sg.s));
+  MEGA_TRY(cudaMemcpyAsync(strain, ds, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, sg.s));
+  MEGA_TRY(cudaMemcpyAsync(d, dd, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, sg.s));
+  MEGA_TRY(cudaStreamSynchronize(sg.s));
+  return 0;
+}
+
+int mega_rotate_tensor(int32_t n, const double* rot, double* vtensor) {
+  if (n <= 0 || !rot || !vtensor) return MEGA_ERR_ARG;
+  StreamGuard sg;
+  int r = make_stream(&sg.s);
+  if (r) return r;
+  DevPool pool;
+  double *dr, *dv;
+  MEGA_ALLOC(pool, dr, 9 * (int64_t)n);
+  MEGA_ALLOC(pool, dv, 6 * (int64_t)n);
+  if ((r = upload(sg.s, dr, rot, 9 * (size_t)n)) || (r = upload(sg.s, dv, vtensor, 6 * (size_t)n))) return r;
+  k_rotate<<<grid_for(n, 128), 128, 0, sg.s>>>(n, dr, dv);
+  MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaMemcpyAsync(vtensor, dv, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, sg.s));
+  MEGA_TRY(cudaStreamSynchronize(sg.s));
+  return 0;
+}
+
+int mega_constitution(const mega_params* p, int32_t n, const double* stress_pred, const int32_t* mat_type,
+                      const double* props, double dlt, double* state, double* stress, int32_t* iters) {
+  if (!p || n <= 0 || !stress_pred || !mat_type || !props || !state || !stress) return MEGA_ERR_ARG;
+  StreamGuard sg;
+  int r = make_stream(&sg.s);
+  if (r) return r;
+  DevPool pool;
+  double *dp, *dprop, *dst, *dsig;
+  int32_t *dm, *dit = nullptr;
+  unsigned* st;
+  MEGA_ALLOC(pool, dp, 6 * (int64_t)n);
+  MEGA_ALLOC(pool, dprop, 30 * (int64_t)n);
+  MEGA_ALLOC(pool, dst, 20 * (int64_t)n);
+  MEGA_ALLOC(pool, dsig, 6 * (int64_t)n);
+  MEGA_ALLOC(pool, dm, n);
+  MEGA_ALLOC(pool, st, 1);
+  if (iters) MEGA_ALLOC(pool, dit, n);
+  if ((r = upload(sg.s, dp, stress_pred, 6 * (size_t)n)) || (r = upload(sg.s, dprop, props, 30 * (size_t)n)) ||
+      (r = upload(sg.s, dst, state, 20 * (size_t)n)) || (r = upload(sg.s, dm, mat_type, (size_t)n)))
+    return r;
+  MEGA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), sg.s));
+  k_constitution<<<grid_for(n, 128), 128, 0, sg.s>>>(n, dp, dm, dprop, dlt, p->newton_max_iter, p->newton_rtol, dst,
+                                                     dsig, dit, st);
+  MEGA_CHECK_LAUNCH();
+  unsigned hst = 0;
+  MEGA_TRY(cudaMemcpyAsync(state, dst, sizeof(double) * 20 * n, cudaMemcpyDeviceToHost, sg.s));
+  MEGA_TRY(cudaMemcpyAsync(stress, dsig, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, sg.s));
+  if (iters) MEGA_TRY(cudaMemcpyAsync(iters, dit, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, sg.s));
+  MEGA_TRY(cudaMemcpyAsync(&hst, st, sizeof(unsigned), cudaMemcpyDeviceToHost, sg.s));
+  MEGA_TRY(cudaStreamSynchronize(sg.s));
+  return (int)hst;
+}
+
+int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, const double* gwin, const double* gvol,
+                        const double* gprop, const int32_t* gmat_type, const int32_t* gebc_nodes,
+                        const double* bodyforce, double* gstate, double* gstress, double* gstrain,
+                        const double* gdinc, const double* gdinc_tot, const int32_t* gn, const int32_t* gstart,
+                        const int32_t* gstack, int64_t nnz, double* gstack_shp, double* gstack_dshp,
+                        int32_t linit, double dlt, double* fint, double* fext, double* gmax_wvel,
+                        double* gstrain_eq, double* gint_work) {
+  if (!p || n <= 0 || !gcoo || !gwin || !gvol || !gprop || !gmat_type || !gstate || !gstress || !gstrain ||
+      !gdinc || !gdinc_tot || !gn || !gstart || !gstack || !gstack_shp || !gstack_dshp || !fint || !fext ||
+      !gmax_wvel || !gstrain_eq || !gint_work)
+    return MEGA_ERR_ARG;
+  if (p->lagrangian != 1) return MEGA_ERR_UNSUPPORTED;
+  StreamGuard sg;
+  int r = make_stream(&sg.s);
+  if (r) return r;
+  cudaStream_t s = sg.s;
+  DevPool pool;
+  DevCSR csr;
+  std::vector<int64_t> hpos;
+  r = csr_from_host(s, n, gn, gstart, gstack, nnz, pool, csr, hpos);
+  if (r) return r;
+  r = build_transpose(s, csr, pool);
+  if (r) return r;
+  const int64_t n3 = 3 * (int64_t)n, m = csr.nnz;
+  double *dc, *dw, *dv, *dsh, *dgx, *dgy, *dgz, *tgx, *tgy, *tgz, *tsh = nullptr, *sd, *ddsp, *dtot, *dsig, *deps6,
+         *dep, *deq, *dwv, *dfg, *dT, *dfi, *dfe, *dbf = nullptr;
+  int32_t* den = nullptr;
+  uint16_t* midx;
+  StepAccum* acc;
+  unsigned* st;
+  MEGA_ALLOC(pool, dc, n3); MEGA_ALLOC(pool, dw, n3); MEGA_ALLOC(pool, dv, n);
+  MEGA_ALLOC(pool, dsh, m); MEGA_ALLOC(pool, dgx, m); MEGA_ALLOC(pool, dgy, m); MEGA_ALLOC(pool, dgz, m);
+  MEGA_ALLOC(pool, tgx, m); MEGA_ALLOC(pool, tgy, m); MEGA_ALLOC(pool, tgz, m);
+  MEGA_ALLOC(pool, sd, n3); MEGA_ALLOC(pool, ddsp, n3); MEGA_ALLOC(pool, dtot, n3);
+  MEGA_ALLOC(pool, dsig, 6 * (int64_t)n); MEGA_ALLOC(pool, deps6, 6 * (int64_t)n); MEGA_ALLOC(pool, dep, n);
+  MEGA_ALLOC(pool, deq, n); MEGA_ALLOC(pool, dwv, n); MEGA_ALLOC(pool, dfg, 18 * (int64_t)n);
+  MEGA_ALLOC(pool, dT, 12 * (int64_t)n); MEGA_ALLOC(pool, dfi, n3); MEGA_ALLOC(pool, dfe, n3);
+  MEGA_ALLOC(pool, midx, n); MEGA_ALLOC(pool, acc, 1); MEGA_ALLOC(pool, st, 1);
+  bool has_body = p->gravity[0] != 0.0 || p->gravity[1] != 0.0 || p->gravity[2] != 0.0;
+  if (bodyforce)
+    for (int64_t k = 0; k < n3 && !has_body; ++k) has_body = bodyforce[k] != 0.0;
+  if (has_body) {
+    MEGA_ALLOC(pool, tsh, m);
+    if (bodyforce) { MEGA_ALLOC(pool, dbf, n3); if ((r = upload(s, dbf, bodyforce, n3))) return r; }
+  }
+  if (gebc_nodes) { MEGA_ALLOC(pool, den, n); if ((r = upload(s, den, gebc_nodes, (size_t)n))) return r; }
+  // material table (per call)
+  std::map<std::vector<double>, uint16_t> tab;
+  std::vector<uint16_t> hidx(n);
+  std::vector<MatEntry> ents;
+  for (int32_t i = 0; i < n; ++i) {
+    std::vector<double> key(gprop + 30 * (size_t)i, gprop + 30 * (size_t)i + 30);
+    key.push_back(gmat_type[i]);
+    auto it = tab.find(key);
+    if (it == tab.end()) {
+      if (ents.size() >= 65535) return MEGA_ERR_UNSUPPORTED;
+      const double* pr = gprop + 30 * (size_t)i;
+      MatEntry e{};
+      e.type = gmat_type[i]; e.nu = pr[0]; e.E = pr[1]; e.rho = pr[2]; e.sig0 = pr[3]; e.B = pr[4]; e.C = pr[5];
+      e.p7 = pr[6]; e.p8 = pr[7]; e.damp = pr[20]; e.lam = pr[27]; e.mu = pr[28]; e.l2m = pr[29];
+      it = tab.emplace(key, (uint16_t)ents.size()).first;
+      ents.push_back(e);
+    }
+    hidx[i] = it->second;
+  }
+  MatEntry* dmat;
+  MEGA_ALLOC(pool, dmat, ents.size());
+  std::vector<double> hs(n), hsig(6 * (size_t)n), heps(6 * (size_t)n);
+  for (int32_t i = 0; i < n; ++i) hs[i] = gstate[20 * (size_t)i + 2];
+  if ((r = upload(s, dc, gcoo, n3)) || (r = upload(s, dw, gwin, n3)) || (r = upload(s, dv, gvol, (size_t)n)) ||
+      (r = upload(s, ddsp, gdinc, n3)) || (r = upload(s, dtot, gdinc_tot, n3)) ||
+      (r = upload(s, dsig, gstress, 6 * (size_t)n)) || (r = upload(s, deps6, gstrain, 6 * (size_t)n)) ||
+      (r = upload(s, dep, hs.data(), (size_t)n)) || (r = upload(s, midx, hidx.data(), (size_t)n)) ||
+      (r = upload(s, dmat, ents.data(), ents.size())))
+    return r;
+  MEGA_TRY(cudaMemsetAsync(acc, 0, sizeof(StepAccum), s));
+  MEGA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
+  if (linit) {
+    r = rk_shapes(s, *p, n, dc, dw, den, csr, dsh, dgx, dgy, dgz, st);
+    if (r) return r;
+  } else {
+    std::vector<double> a(m), b(m), d(m), e(m);
+    for (int64_t k = 0; k < m; ++k) {
+      const int64_t q = hpos[k];
+      a[k] = gstack_shp[q];
+      b[k] = gstack_dshp[3 * q]; d[k] = gstack_dshp[3 * q + 1]; e[k] = gstack_dshp[3 * q + 2];
+    }
+    if ((r = upload(s, dsh, a.data(), m)) || (r = upload(s, dgx, b.data(), m)) || (r = upload(s, dgy, d.data(), m)) ||
+        (r = upload(s, dgz, e.data(), m)))
+      return r;
+    MEGA_TRY(cudaStreamSynchronize(s));
+  }
+  const unsigned g = grid_for(m, 256);
+  k_gather_pos<<<g, 256, 0, s>>>(m, csr.tpos, dgx, tgx);
+  k_gather_pos<<<g, 256, 0, s>>>(m, csr.tpos, dgy, tgy);
+  k_gather_pos<<<g, 256, 0, s>>>(m, csr.tpos, dgz, tgz);
+  if (has_body) k_gather_pos<<<g, 256, 0, s>>>(m, csr.tpos, dsh, tsh);
+  k_rowsum3<double><<<grid_for(n, 256), 256, 0, s>>>(n, csr.rowptr, dgx, dgy, dgz, sd);
+  MEGA_CHECK_LAUNCH();
+  r = launch_defgrad(s, false, false, n, csr, dgx, dgy, dgz, ddsp, dtot, sd, dsh, nullptr, dfg, acc);
+  if (r) return r;
+  StressArgs a{};
+  a.n = n; a.fg = dfg; a.matidx = midx; a.mats = dmat; a.vol = dv; a.stress = dsig; a.strain = deps6; a.eps = dep;
+  a.strain_eq = deq; a.wvel = dwv; a.tmat = dT; a.bodyforce = dbf;
+  a.grav[0] = p->gravity[0]; a.grav[1] = p->gravity[1]; a.grav[2] = p->gravity[2];
+  a.has_body = has_body; a.inv3_exact = p->inv3_exact; a.finite_strain = p->finite_strain;
+  a.maxit = p->newton_max_iter; a.rtol = p->newton_rtol; a.dt = dlt; a.acc = acc; a.status = st;
+  r = launch_stress(s, false, a);
+  if (r) return r;
+  DevCSR* dcsr;
+  MEGA_ALLOC(pool, dcsr, 1);
+  if ((r = upload(s, dcsr, &csr, 1))) return r;
+  ForceArgs f{};
+  f.n = n; f.csr = dcsr; f.tgx = tgx; f.tgy = tgy; f.tgz = tgz; f.tshp = tsh; f.tmat = dT; f.has_body = has_body;
+  f.integrate = 0; f.predict = 0; f.fint = dfi; f.fext = dfe; f.acc = acc; f.status = st;
+  r = launch_force(s, false, f);
+  if (r) return r;
+  StepAccum hacc;
+  unsigned hst = 0;
+  MEGA_TRY(cudaMemcpyAsync(fint, dfi, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(fext, dfe, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(gstress, dsig, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(gstrain, deps6, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(hs.data(), dep, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(gmax_wvel, dwv, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(gstrain_eq, deq, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(&hacc, acc, sizeof(hacc), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(&hst, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  if (linit) {
+    std::vector<double> a2(m), b(m), d(m), e(m);
+    MEGA_TRY(cudaMemcpyAsync(a2.data(), dsh, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    MEGA_TRY(cudaMemcpyAsync(b.data(), dgx, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    MEGA_TRY(cudaMemcpyAsync(d.data(), dgy, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    MEGA_TRY(cudaMemcpyAsync(e.data(), dgz, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    MEGA_TRY(cudaStreamSynchronize(s));
+    for (int64_t k = 0; k < m; ++k) {
+      const int64_t q = hpos[k];
+      gstack_shp[q] = a2[k];
+      gstack_dshp[3 * q] = b[k]; gstack_dshp[3 * q + 1] = d[k]; gstack_dshp[3 * q + 2] = e[k];
+    }
+  }
+  MEGA_TRY(cudaStreamSynchronize(s));
+  for (int32_t i = 0; i < n; ++i) gstate[20 * (size_t)i + 2] = hs[i];
+  *gint_work += hacc.int_work;
+  return (int)hst;
+}
+
+int mega_construct_fint_pd(const mega_params* p, int32_t n, const double* gcoo, const double* gcoo_current,
+                           const double* gwin, const double* gvol, const double* gprop, const int32_t* gmat_type,
+                           double* gstate, double* gstress, double* gstrain, const double* gdinc, const int32_t* gn,
+                           const int32_t* gstart, const int32_t* gstack, int64_t nnz, double* gstack_shp,
+                           double* ginvk, int32_t linit, double dlt, double* fint, double* gmax_wvel,
+                           double* gint_work) {
+  return MEGA_ERR_UNSUPPORTED;
+}
+
+}  // extern "C"

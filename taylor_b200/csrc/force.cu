@@ -1,0 +1,501 @@
+// force.cu -- the per-step internal force of CONSTRUCT_FINT (FINT.F90:
+// 259-1247) and the central-difference update of MAIN.F90:348-488.
+//
+// One explicit step is three kernels:
+//   k_defgrad  (row gather, 4 lanes per node): F = I + sum_J u_J (x) grad0 phi_iJ
+//              and G0 = sum_J du_J (x) grad0 phi_iJ (FINT.F90:363-376, 673-679)
+//              written as sum_J (u_J - u_i)(x)g + u_i (x) sum_J g so the
+//              rigid part does not cancel in float;
+//   k_stress   (thread per node): |det F|, INV3, L = G0 INV3(F) (the push-
+//              forward of FINT.F90:380-391 applied once to the 3x3 instead
+//              of per neighbour), Hughes-Winget, rotation of sigma and eps,
+//              elastic predictor, return mapping, state write-back, wave
+//              speed and internal work (FINT.F90:758-870); it emits
+//              T_i = V_i J_i sigma_i INV3(F_i)^T so that the scattered force
+//              f_J += B(grad phi_iJ)^T sigma_i V_i J_i (FINT.F90:999-1116)
+//              becomes T_i grad0 phi_iJ;
+//   k_force    (column gather over the transposed list, 4 lanes per node):
+//              f_J = sum_{i: J in N(i)} T_i grad0 phi_iJ -- no atomics, a
+//              fixed summation order, no FINT_TEMP(NCORES,3,N) buffers --
+//              fused with the fixity / acceleration / corrector of MAIN.F90:
+//              432-488, the energy sums of MAIN.F90:524-555 and the next
+//              step's predictor (MAIN.F90:353-355).
+// FP64 (drop-in) and mixed (float gradients / stress / force arithmetic,
+// double moment inverse, positions, integration and return-mapping
+// residual) instantiate the same templates.
+#include "mega_internal.cuh"
+
+namespace mega {
+namespace {
+
+constexpr int kGroup = 4;  // lanes per node in the gathers
+
+__device__ __forceinline__ NodeMat to_nodemat(const MatEntry& e) {
+  NodeMat m;
+  m.type = e.type; m.nu = e.nu; m.E = e.E; m.rho = e.rho; m.sig0 = e.sig0; m.B = e.B; m.C = e.C;
+  m.lam = e.lam; m.mu = e.mu; m.l2m = e.l2m; m.p7 = e.p7; m.p8 = e.p8;
+  return m;
+}
+
+template <typename G, typename A, bool INTERP>
+__global__ void __launch_bounds__(256) k_defgrad(int32_t n, const int64_t* __restrict__ rowptr,
+                                                 const int32_t* __restrict__ col, const G* __restrict__ gx,
+                                                 const G* __restrict__ gy, const G* __restrict__ gz,
+                                                 const double* __restrict__ dsp,
+                                                 const double* __restrict__ dsp_tot,
+                                                 const double* __restrict__ sdphi,
+                                                 const double* __restrict__ shp,
+                                                 double* __restrict__ dsp_tot_phy, double* __restrict__ fg,
+                                                 StepAccum* __restrict__ acc) {
+  if (acc && blockIdx.x == 0 && threadIdx.x == 0) {  // per-step counters of the stress kernel
+    acc->newton_iters = 0ull;
+    acc->plastic = 0ull;
+  }
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kGroup;
+  const int q = threadIdx.x & (kGroup - 1);
+  const unsigned gmask = 0xFu << (threadIdx.x & 28);
+  if (i >= n) return;
+  const double ui0 = dsp_tot[3 * i], ui1 = dsp_tot[3 * i + 1], ui2 = dsp_tot[3 * i + 2];
+  const double di0 = dsp[3 * i], di1 = dsp[3 * i + 1], di2 = dsp[3 * i + 2];
+  A F[9], L[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) { F[k] = A(0); L[k] = A(0); }
+  double ph0 = 0.0, ph1 = 0.0, ph2 = 0.0;
+  const int64_t p1 = rowptr[i + 1];
+  for (int64_t p = rowptr[i] + q; p < p1; p += kGroup) {
+    const int64_t j = col[p];
+    const A g0 = (A)gx[p], g1 = (A)gy[p], g2 = (A)gz[p];
+    const A u0 = (A)(dsp_tot[3 * j] - ui0), u1 = (A)(dsp_tot[3 * j + 1] - ui1), u2 = (A)(dsp_tot[3 * j + 2] - ui2);
+    const double dj0 = dsp[3 * j], dj1 = dsp[3 * j + 1], dj2 = dsp[3 * j + 2];
+    const A d0 = (A)(dj0 - di0), d1 = (A)(dj1 - di1), d2 = (A)(dj2 - di2);
+    F[0] += u0 * g0; F[1] += u0 * g1; F[2] += u0 * g2;
+    F[3] += u1 * g0; F[4] += u1 * g1; F[5] += u1 * g2;
+    F[6] += u2 * g0; F[7] += u2 * g1; F[8] += u2 * g2;
+    L[0] += d0 * g0; L[1] += d0 * g1; L[2] += d0 * g2;
+    L[3] += d1 * g0; L[4] += d1 * g1; L[5] += d1 * g2;
+    L[6] += d2 * g0; L[7] += d2 * g1; L[8] += d2 * g2;
+    if (INTERP) {
+      const double s = shp[p];
+      ph0 += s * dj0; ph1 += s * dj1; ph2 += s * dj2;
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < kGroup; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      F[k] += __shfl_xor_sync(gmask, F[k], o);
+      L[k] += __shfl_xor_sync(gmask, L[k], o);
+    }
+    if (INTERP) {
+      ph0 += __shfl_xor_sync(gmask, ph0, o);
+      ph1 += __shfl_xor_sync(gmask, ph1, o);
+      ph2 += __shfl_xor_sync(gmask, ph2, o);
+    }
+  }
+  if (q == 0) {
+    const double s0 = sdphi[3 * i], s1 = sdphi[3 * i + 1], s2 = sdphi[3 * i + 2];
+    const double ui[3] = {ui0, ui1, ui2}, di[3] = {di0, di1, di2}, sd[3] = {s0, s1, s2};
+    double* o = fg + 18 * i;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        o[3 * k + l] = (k == l ? 1.0 : 0.0) + ((double)F[3 * k + l] + ui[k] * sd[l]);
+        o[9 + 3 * k + l] = (double)L[3 * k + l] + di[k] * sd[l];
+      }
+    if (INTERP) {
+      dsp_tot_phy[3 * i] += ph0;
+      dsp_tot_phy[3 * i + 1] += ph1;
+      dsp_tot_phy[3 * i + 2] += ph2;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* sm) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sm[wid] = v;
+  __syncthreads();
+  T r = T(0);
+  if (wid == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? sm[lane] : T(0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  }
+  return r;  // valid in thread 0
+}
+
+// T = arithmetic of kinematics / rotation / predictor, TS = storage of T_i
+template <typename T, typename TS>
+__global__ void __launch_bounds__(256) k_stress(StressArgs a) {
+  __shared__ double smd[32];
+  __shared__ unsigned long long smu[32];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.acc->ke = 0.0;  // the force kernel of this step accumulates it afresh
+  }
+  double work = 0.0;
+  unsigned long long nit = 0, npl = 0;
+  unsigned st = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* fgi = a.fg + 18 * i;
+    const MatEntry me = a.mats[a.matidx[i]];
+    const NodeMat m = to_nodemat(me);
+    const double vol = a.vol[i];
+    T Fm[3][3], G0[3][3], IF[3][3], L[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) { Fm[k][l] = (T)fgi[3 * k + l]; G0[k][l] = (T)fgi[9 + 3 * k + l]; }
+    double det = 1.0;
+    T sig[6], eps6[6], dstr[6], D[6];
+    double sold[6], eold[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      sold[k] = a.stress[6 * i + k];
+      eold[k] = a.strain[6 * i + k];
+      sig[k] = (T)sold[k];
+      eps6[k] = (T)eold[k];
+      D[k] = T(0);
+    }
+    if (a.finite_strain) {
+      // |det F| and the push-forward in double for F (FP64 positions path)
+      double Fd[3][3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) Fd[k][l] = fgi[3 * k + l];
+      det = det_abs(Fd);
+      double IFd[3][3];
+      inv3(Fd, IFd, a.inv3_exact != 0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) IF[k][l] = (T)IFd[k][l];
+      mm3(G0, IF, L);
+      T R[3][3];
+      hughes_winget(L, R, dstr, D, a.inv3_exact != 0);
+      rotate_tensor(R, sig);
+      rotate_tensor(R, eps6);
+    } else {
+      // FINT.F90:772-783 small strain: engineering shear, no rotation, DET = 1
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) IF[k][l] = (k == l) ? T(1) : T(0);
+      dstr[0] = G0[0][0]; dstr[1] = G0[1][1]; dstr[2] = G0[2][2];
+      dstr[3] = G0[2][1] + G0[1][2]; dstr[4] = G0[2][0] + G0[0][2]; dstr[5] = G0[1][0] + G0[0][1];
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) eps6[k] = eps6[k] + dstr[k];
+    // elastic predictor with FORM_CMAT (FINT_FUNCTIONS.F90:252-288)
+    const T lam = (T)me.lam, mu = (T)me.mu, l2m = (T)me.l2m;
+    double spred[6];
+    spred[0] = (double)(sig[0] + (l2m * dstr[0] + lam * dstr[1] + lam * dstr[2]));
+    spred[1] = (double)(sig[1] + (lam * dstr[0] + l2m * dstr[1] + lam * dstr[2]));
+    spred[2] = (double)(sig[2] + (lam * dstr[0] + lam * dstr[1] + l2m * dstr[2]));
+    spred[3] = (double)(sig[3] + mu * dstr[3]);
+    spred[4] = (double)(sig[4] + mu * dstr[4]);
+    spred[5] = (double)(sig[5] + mu * dstr[5]);
+    double snew[6];
+    double ep = a.eps[i];
+    int it = 0;
+    bool cap = false;
+    if (m.type == MEGA_MAT_ELASTIC) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) snew[k] = spred[k];
+    } else if (m.type == MEGA_MAT_VONMISES) {
+      it = von_mises(spred, ep, m, a.maxit, snew, cap);
+    } else if (m.type == MEGA_MAT_VM_RATE) {
+      double dg = 0.0, ftr = 0.0;
+      const double g0 = a.mlp_guess ? (double)a.mlp_guess[i] : -1.0;
+      it = vm_rate(spred, ep, m, a.dt, a.rtol, a.maxit, g0, snew, cap, dg, ftr);
+    } else {
+      st |= MEGA_ST_BAD_MATERIAL;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) snew[k] = spred[k];
+    }
+    if (cap) st |= MEGA_ST_NEWTON_CAP;
+    nit += (unsigned long long)it;
+    npl += (it > 0) ? 1ull : 0ull;
+    if (a.iters) a.iters[i] = it;
+    double sinc[6], einc[6], enew[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      enew[k] = (double)eps6[k];
+      sinc[k] = snew[k] - sold[k];
+      einc[k] = enew[k] - eold[k];
+      a.stress[6 * i + k] = snew[k];
+      a.strain[6 * i + k] = enew[k];
+    }
+    a.eps[i] = ep;
+    const double eq = enew[0] * enew[0] + enew[1] * enew[1] + enew[2] * enew[2] +
+                      2.0 * (enew[3] * enew[3] + enew[4] * enew[4] + enew[5] * enew[5]);
+    a.strain_eq[i] = sqrt(eq * 2.0 / 3.0);
+    if (a.finite_strain) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) work += 0.5 * (double)D[k] * (2.0 * snew[k] - sinc[k]) * vol * det;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) work += 0.5 * einc[k] * sinc[k] * vol * det;
+    }
+    double bulk = m.E / (3.0 * (1.0 - 2.0 * m.nu)), shear = m.E / (2.0 * (1.0 + m.nu));
+    if (m.type > 1) estimate_moduli(sinc, einc, shear, bulk);
+    const double pmod = bulk + 4.0 * shear / 3.0;
+    a.wvel[i] = sqrt(fmax(pmod, shear) / m.rho);
+    // T_i = V J sigma IF^T: f_J(k) = sum_m T(k,m) grad0 phi_iJ(m)
+    const T vj = (T)(vol * det);
+    T S[3][3];
+    T sn[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sn[k] = (T)snew[k];
+    v2t(sn, S);
+    TS* to = (TS*)a.tmat + 12 * i;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int mm = 0; mm < 3; ++mm)
+        to[3 * k + mm] = (TS)(vj * (S[k][0] * IF[mm][0] + S[k][1] * IF[mm][1] + S[k][2] * IF[mm][2]));
+    if (a.has_body) {
+      const double rvj = m.rho * vol * det;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double b = (a.bodyforce ? a.bodyforce[3 * i + k] : 0.0) + a.grav[k];
+        to[9 + k] = (TS)(b * rvj);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      if (!isfinite(snew[k])) st |= MEGA_ST_NONFINITE;
+  }
+  const double wsum = block_sum(work, smd);
+  const unsigned long long it_sum = block_sum(nit, smu);
+  const unsigned long long pl_sum = block_sum(npl, smu);
+  if (threadIdx.x == 0) {
+    if (wsum != 0.0) atomicAdd(&a.acc->int_work, wsum);
+    if (it_sum) atomicAdd(&a.acc->newton_iters, it_sum);
+    if (pl_sum) atomicAdd(&a.acc->plastic, pl_sum);
+  }
+  if (st) atomicOr(a.status, st);
+}
+
+// G = storage of grad phi, TS = storage of T_i, A = accumulation
+template <typename G, typename TS, typename A>
+__global__ void __launch_bounds__(256) k_force(ForceArgs a) {
+  __shared__ double smd[32];
+  const int64_t* __restrict__ colptr = a.csr->colptr;
+  const int32_t* __restrict__ trow = a.csr->trow;
+  const G* __restrict__ tgx = (const G*)a.tgx;
+  const G* __restrict__ tgy = (const G*)a.tgy;
+  const G* __restrict__ tgz = (const G*)a.tgz;
+  const TS* __restrict__ tm = (const TS*)a.tmat;
+  const int q = threadIdx.x & (kGroup - 1);
+  const unsigned gmask = 0xFu << (threadIdx.x & 28);
+  double ke = 0.0, ee = 0.0, tf[6] = {0, 0, 0, 0, 0, 0};
+  unsigned st = 0;
+  const int64_t groups = ((int64_t)gridDim.x * blockDim.x) / kGroup;
+  // every lane of a group runs the same iterations, so group shuffles are safe
+  for (int64_t J = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kGroup; J < a.n; J += groups) {
+    A f0 = A(0), f1 = A(0), f2 = A(0);
+    double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+    const int64_t c1 = colptr[J + 1];
+    for (int64_t e = colptr[J] + q; e < c1; e += kGroup) {
+      const int64_t i = trow[e];
+      const A g0 = (A)tgx[e], g1 = (A)tgy[e], g2 = (A)tgz[e];
+      const TS* t = tm + 12 * i;
+      f0 += (A)t[0] * g0 + (A)t[1] * g1 + (A)t[2] * g2;
+      f1 += (A)t[3] * g0 + (A)t[4] * g1 + (A)t[5] * g2;
+      f2 += (A)t[6] * g0 + (A)t[7] * g1 + (A)t[8] * g2;
+      if (a.has_body) {
+        const double s = a.tshp[e];
+        e0 += s * (double)t[9]; e1 += s * (double)t[10]; e2 += s * (double)t[11];
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < kGroup; o <<= 1) {
+      f0 += __shfl_xor_sync(gmask, f0, o);
+      f1 += __shfl_xor_sync(gmask, f1, o);
+      f2 += __shfl_xor_sync(gmask, f2, o);
+      if (a.has_body) {
+        e0 += __shfl_xor_sync(gmask, e0, o);
+        e1 += __shfl_xor_sync(gmask, e1, o);
+        e2 += __shfl_xor_sync(gmask, e2, o);
+      }
+    }
+    if (q < 3) {
+      const int64_t m = 3 * J + q;
+      const double fi = (double)(q == 0 ? f0 : (q == 1 ? f1 : f2));
+      double fe = (q == 0 ? e0 : (q == 1 ? e1 : e2));
+      if (!isfinite(fi)) st |= MEGA_ST_NONFINITE;
+      if (!a.integrate) {
+        a.fint[m] = fi;
+        a.fext[m] = fe;
+      } else {
+        const double mass = a.mass[m];
+        const double fe_old = a.fext[m];
+        double v = a.vel[m], acc, pr;
+        if (a.ebc[m] == 1) {  // MAIN.F90:438-445
+          v = 0.0;
+          acc = 0.0;
+          pr = -fi;
+          fe = -fi;
+        } else {  // MAIN.F90:472-481
+          const double mpdc = a.mats[a.matidx[J]].damp * mass;
+          acc = (fe - fi - mpdc * v) / (mass + 0.5 * a.dt * mpdc);
+          v = v + 0.5 * a.dt * acc;
+          pr = 0.0;
+        }
+        const double d_old = a.dsp[m];
+        ee += 0.5 * (fe + fe_old) * d_old;
+        ke += 0.5 * mass * v * v;
+        const int b = a.body_id ? a.body_id[J] : 1;
+        if (b == 1) tf[q] += pr;
+        else if (b == 2) tf[3 + q] += pr;
+        a.fint[m] = fi;
+        a.fext[m] = fe;
+        a.acl[m] = acc;
+        a.prforce[m] = pr;
+        if (a.predict) {  // MAIN.F90:353-355 of the next step
+          const double d = a.dt * v + a.dt * a.dt * 0.5 * acc;
+          a.dsp[m] = d;
+          a.dsp_tot[m] = a.dsp_tot[m] + d;
+          v = v + a.dt * 0.5 * acc;
+        }
+        a.vel[m] = v;
+      }
+    }
+  }
+  if (a.integrate) {
+    const double ks = block_sum(ke, smd);
+    const double es = block_sum(ee, smd);
+    double ts[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ts[k] = block_sum(tf[k], smd);
+    if (threadIdx.x == 0) {
+      atomicAdd(&a.acc->ke, ks);
+      if (es != 0.0) atomicAdd(&a.acc->ee, es);
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+        if (ts[k] != 0.0) atomicAdd(&a.acc->total_force[k], ts[k]);
+    }
+  }
+  if (st) atomicOr(a.status, st);
+}
+
+__global__ void k_predict(int64_t n3, double* __restrict__ dsp, double* __restrict__ dsp_tot,
+                          double* __restrict__ vel, const double* __restrict__ acl, double dt) {
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (m >= n3) return;
+  const double v = vel[m], a = acl[m];
+  const double d = dt * v + dt * dt * 0.5 * a;
+  dsp[m] = d;
+  dsp_tot[m] = dsp_tot[m] + d;
+  vel[m] = v + dt * 0.5 * a;
+}
+
+__global__ void k_interp(int32_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                         const double* __restrict__ shp, const double* __restrict__ val,
+                         const double* __restrict__ base, double* __restrict__ out) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kGroup;
+  const int q = threadIdx.x & (kGroup - 1);
+  const unsigned gmask = 0xFu << (threadIdx.x & 28);
+  if (i >= n) return;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t p = rowptr[i] + q; p < rowptr[i + 1]; p += kGroup) {
+    const int64_t j = col[p];
+    const double w = shp[p];
+    s0 += w * val[3 * j]; s1 += w * val[3 * j + 1]; s2 += w * val[3 * j + 2];
+  }
+#pragma unroll
+  for (int o = 1; o < kGroup; o <<= 1) {
+    s0 += __shfl_xor_sync(gmask, s0, o);
+    s1 += __shfl_xor_sync(gmask, s1, o);
+    s2 += __shfl_xor_sync(gmask, s2, o);
+  }
+  if (q == 0) {
+    out[3 * i] = (base ? base[3 * i] : 0.0) + s0;
+    out[3 * i + 1] = (base ? base[3 * i + 1] : 0.0) + s1;
+    out[3 * i + 2] = (base ? base[3 * i + 2] : 0.0) + s2;
+  }
+}
+
+inline unsigned grid_for(int64_t work, int block) { return (unsigned)((work + block - 1) / block); }
+
+}  // namespace
+
+int device_sm_count() {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+int launch_defgrad(cudaStream_t s, bool mixed, bool interp, int32_t n, const DevCSR& csr, const void* gx,
+                   const void* gy, const void* gz, const double* dsp, const double* dsp_tot,
+                   const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc) {
+  const int block = 256;
+  const unsigned grid = grid_for((int64_t)n * kGroup, block);
+  if (mixed) {
+    if (interp)
+      k_defgrad<float, float, true><<<grid, block, 0, s>>>(n, csr.rowptr, csr.col, (const float*)gx,
+                                                           (const float*)gy, (const float*)gz, dsp, dsp_tot,
+                                                           sdphi, shp, dsp_tot_phy, fg, acc);
+    else
+      k_defgrad<float, float, false><<<grid, block, 0, s>>>(n, csr.rowptr, csr.col, (const float*)gx,
+                                                            (const float*)gy, (const float*)gz, dsp, dsp_tot,
+                                                            sdphi, shp, dsp_tot_phy, fg, acc);
+  } else {
+    if (interp)
+      k_defgrad<double, double, true><<<grid, block, 0, s>>>(n, csr.rowptr, csr.col, (const double*)gx,
+                                                             (const double*)gy, (const double*)gz, dsp,
+                                                             dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
+    else
+      k_defgrad<double, double, false><<<grid, block, 0, s>>>(n, csr.rowptr, csr.col, (const double*)gx,
+                                                              (const double*)gy, (const double*)gz, dsp,
+                                                              dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
+  }
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int launch_stress(cudaStream_t s, bool mixed, const StressArgs& a) {
+  const int block = 256;
+  const int64_t need = grid_for(a.n, block);
+  const unsigned grid = (unsigned)std::min<int64_t>(need, (int64_t)device_sm_count() * 8);
+  if (mixed) k_stress<float, float><<<grid > 0 ? grid : 1, block, 0, s>>>(a);
+  else k_stress<double, double><<<grid > 0 ? grid : 1, block, 0, s>>>(a);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int launch_force(cudaStream_t s, bool mixed, const ForceArgs& a) {
+  const int block = 256;
+  const int64_t need = grid_for((int64_t)a.n * kGroup, block);
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)device_sm_count() * 8));
+  if (mixed) k_force<float, float, float><<<grid, block, 0, s>>>(a);
+  else k_force<double, double, double><<<grid, block, 0, s>>>(a);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int launch_predict(cudaStream_t s, int64_t n3, double* dsp, double* dsp_tot, double* vel, const double* acl,
+                   double dt) {
+  if (n3 <= 0) return 0;
+  k_predict<<<grid_for(n3, 256), 256, 0, s>>>(n3, dsp, dsp_tot, vel, acl, dt);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int launch_interp(cudaStream_t s, int32_t n, const DevCSR& csr, const double* shp, const double* val,
+                  const double* base, double* out) {
+  k_interp<<<grid_for((int64_t)n * kGroup, 256), 256, 0, s>>>(n, csr.rowptr, csr.col, shp, val, base, out);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+}  // namespace mega

@@ -1,0 +1,189 @@
+// mega_internal.cuh -- host-side plumbing shared by the library's .cu files:
+// device allocation tracking, error capture, the resident context and the
+// launchers each translation unit exports.
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "mega_device.cuh"
+
+namespace mega {
+
+constexpr int kMaxBinCount = 1000;     // MAX_NEIGH, HANDELER.F90:245
+constexpr int kMaxCandidates = 10000;  // INODE(10000), BIN_SEARCH.F90:80
+
+void record_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+const char* last_error_text();
+
+#define MEGA_TRY(x)                                                   \
+  do {                                                                \
+    cudaError_t e_ = (x);                                             \
+    if (e_ != cudaSuccess) {                                          \
+      ::mega::record_cuda_error(e_, #x, __FILE__, __LINE__);          \
+      return MEGA_ERR_CUDA;                                           \
+    }                                                                 \
+  } while (0)
+
+#define MEGA_CHECK_LAUNCH() MEGA_TRY(cudaGetLastError())
+
+// Device allocations owned by one object; freed together.
+struct DevPool {
+  std::vector<void*> ptrs;
+  int64_t bytes = 0;
+  template <typename T>
+  int alloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      record_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
+      *p = nullptr;
+      return MEGA_ERR_NOMEM;
+    }
+    ptrs.push_back((void*)*p);
+    bytes += (int64_t)(count * sizeof(T));
+    return 0;
+  }
+  void release(void* p) {
+    for (size_t k = 0; k < ptrs.size(); ++k)
+      if (ptrs[k] == p) { cudaFree(p); ptrs.erase(ptrs.begin() + k); return; }
+  }
+  void free_all() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+    bytes = 0;
+  }
+  ~DevPool() { free_all(); }
+};
+
+#define MEGA_ALLOC(pool, ptr, count)                  \
+  do {                                                \
+    int r_ = (pool).alloc(&(ptr), (size_t)(count));   \
+    if (r_) return r_;                                \
+  } while (0)
+
+// Compressed neighbour structure on the device.  CSR rows are the
+// reference's GSTACK rows (0-based); the CSC view lists, for every node J,
+// the rows i whose list contains J (ascending i) and the CSR position of
+// that entry, which is how values stored per CSR entry are transposed.
+struct DevCSR {
+  int32_t n = 0;
+  int64_t nnz = 0;
+  int32_t gmaxn = 0;
+  int64_t* rowptr = nullptr;  // n + 1
+  int32_t* col = nullptr;     // nnz
+  int64_t* colptr = nullptr;  // n + 1
+  int32_t* trow = nullptr;    // nnz
+  int64_t* tpos = nullptr;    // nnz
+};
+
+// Bin geometry of HANDELER.F90:187-243 (doubles: xmin,ymin,zmin,xbin,ybin,zbin)
+struct BinGeom {
+  double g[6];
+  int32_t nx, ny, nz;
+};
+
+// ---------------- launchers (search.cu)
+// Exclusive scan of m int32 counts into int64 offsets (off[m] = total).
+int scan_counts(cudaStream_t s, const int32_t* cnt, int64_t* off, int64_t m, DevPool& scratch);
+// Bin search into csr (rowptr/col, gmaxn) with the reference's ordering.
+// ijk (3,n) 1-based may be null.  status is a device word (OR-ed).
+int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, const double* sm_len,
+               const double dist_max[3], int32_t itype_int, int32_t shsup, unsigned* status,
+               DevCSR& csr, int32_t* ijk, DevPool& pool, BinGeom* geom_out);
+// Build the CSC view of csr.
+int build_transpose(cudaStream_t s, DevCSR& csr, DevPool& pool);
+
+// ---------------- launchers (rk.cu)
+int rk_shapes(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
+              const int32_t* ebc_nodes, const DevCSR& csr, double* shp, double* gx, double* gy, double* gz,
+              unsigned* status);
+
+// Per-material constants, deduplicated from PROPS(30,N) at init.
+struct MatEntry {
+  int32_t type;
+  int32_t pad;
+  double nu, E, rho, sig0, B, C, p7, p8, lam, mu, l2m, damp;
+};
+
+// Reductions the step kernels accumulate on the device.
+struct StepAccum {
+  double int_work;        // GINT_WORK, accumulated over calls (FINT.F90:1232)
+  double ke;              // kinetic energy of the last step
+  double ee;              // accumulated external energy (MAIN.F90:539)
+  double total_force[6];  // TOTAL_FORCE(3,2), running sum (MAIN.F90:485)
+  unsigned long long newton_iters;  // last step
+  unsigned long long plastic;       // last step
+  double pad[4];
+};
+
+// ---------------- launchers (force.cu)
+struct StressArgs {
+  int32_t n;
+  const double* fg;          // 18 per node: F (row-major 3x3), G0 (3x3)
+  const uint16_t* matidx;
+  const MatEntry* mats;
+  const double* vol;
+  double* stress;            // (6,n)
+  double* strain;            // (6,n)
+  double* eps;               // (n)
+  double* strain_eq;         // (n)
+  double* wvel;              // (n)
+  void* tmat;                // 12 per node (double or float)
+  const double* bodyforce;   // (3,n) or null
+  double grav[3];
+  int has_body;
+  int inv3_exact;
+  int finite_strain;
+  int maxit;
+  double rtol;
+  double dt;
+  int32_t* iters;            // per-node Newton passes (or null)
+  const float* mlp_guess;    // per-node Newton start for the rate law (or null)
+  float* rate_samples;       // logging of (features, dg) for the surrogate (or null)
+  StepAccum* acc;
+  unsigned* status;
+};
+int launch_defgrad(cudaStream_t s, bool mixed, bool interp, int32_t n, const DevCSR& csr, const void* gx,
+                   const void* gy, const void* gz, const double* dsp, const double* dsp_tot,
+                   const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg,
+                   StepAccum* acc);
+int launch_stress(cudaStream_t s, bool mixed, const StressArgs& a);
+struct ForceArgs {
+  int32_t n;
+  const DevCSR* csr;
+  const void* tgx;
+  const void* tgy;
+  const void* tgz;
+  const double* tshp;   // transposed shape values (body force) or null
+  const void* tmat;
+  int has_body;
+  int integrate;        // 0: only fint / fext (CONSTRUCT_FINT drop-in)
+  int predict;          // fuse the next step's predictor
+  const int8_t* ebc;
+  const double* mass;
+  const uint16_t* matidx;
+  const MatEntry* mats;
+  const int8_t* body_id;
+  double* fint;
+  double* fext;
+  double* vel;
+  double* acl;
+  double* dsp;
+  double* dsp_tot;
+  double* prforce;
+  double dt;
+  StepAccum* acc;
+  unsigned* status;
+};
+int launch_force(cudaStream_t s, bool mixed, const ForceArgs& a);
+int launch_predict(cudaStream_t s, int64_t n3, double* dsp, double* dsp_tot, double* vel, const double* acl,
+                   double dt);
+// out[3i+k] = base[3i+k] + sum_J shp_iJ * val[3J+k]
+int launch_interp(cudaStream_t s, int32_t n, const DevCSR& csr, const double* shp, const double* val,
+                  const double* base, double* out);
+int device_sm_count();
+
+}  // namespace mega

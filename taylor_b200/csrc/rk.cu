@@ -1,0 +1,211 @@
+// rk.cu -- reproducing-kernel shape functions, one warp per node, FP64.
+//
+// Restates RK1 (RK.f90:16-453) for DEG = 1: per neighbour the linear basis
+// H = (1, X-X_J), the box cubic B-spline kernel phi = w(|dx|/a)w(|dy|/a)
+// w(|dz|/a) (or the spherical one with SHSUP) with its gradient, the
+// singular-kernel modification for EBC neighbours (RK.f90:217-228); the
+// moment matrix M and its x/y/z derivatives (RK.f90:231-242), the
+// quasi-linear term (RK.f90:251-303), the cofactor inverse (M44INV), the
+// correction vectors b = e1 M^-1 and b_,x = -e1 M^-1 M_,x M^-1
+// (RK.f90:311-342), and finally phi_J = (b.H~)phi, grad phi_J =
+// (b_,x.H~ + b.H_,x)phi + (b.H~)phi_,x (RK.f90:346-405).
+// Lanes stride the neighbour list and accumulate the 4 symmetric 4x4
+// matrices; a butterfly reduction leaves the sums in every lane, each lane
+// inverts redundantly (no shared memory), then the lanes write their own
+// entries (coalesced SoA stores).
+#include "mega_internal.cuh"
+
+namespace mega {
+namespace {
+
+struct EntryK {
+  double H[4];
+  double phi, px, py, pz;
+};
+
+// RK.f90:123-230 for one neighbour
+__device__ __forceinline__ void rk_entry(const double xi[3], const double xj[3], const double aj[3], bool ebc_j,
+                                         int shsup, EntryK& e) {
+  const double dx = xi[0] - xj[0], dy = xi[1] - xj[1], dz = xi[2] - xj[2];
+  e.H[0] = 1.0; e.H[1] = dx; e.H[2] = dy; e.H[3] = dz;
+  const double nx = dx / aj[0], ny = dy / aj[1], nz = dz / aj[2];
+  if (shsup) {
+    const double dia = sqrt(nx * nx + ny * ny + nz * nz);
+    double k, kx;
+    bspline3(dia, k, kx);
+    double drdx = 0.0, drdy = 0.0, drdz = 0.0;
+    if (!(dia <= 1.0e-13)) {
+      drdx = dx / (aj[0] * aj[0]) / dia;
+      drdy = dy / (aj[1] * aj[1]) / dia;
+      drdz = dz / (aj[2] * aj[2]) / dia;
+    }
+    e.phi = k; e.px = kx * drdx; e.py = kx * drdy; e.pz = kx * drdz;
+  } else {
+    double kx, kxx, ky, kyy, kz, kzz;
+    bspline3(fabs(nx), kx, kxx);
+    bspline3(fabs(ny), ky, kyy);
+    bspline3(fabs(nz), kz, kzz);
+    double phi = kx * ky * kz;
+    // RK.f90:183-205: every axis divides by GWIN(1,II) (kept as written)
+    const double drdx = (nx == 0.0) ? 0.0 : (nx >= 0.0 ? 1.0 / aj[0] : -1.0 / aj[0]);
+    const double drdy = (ny == 0.0) ? 0.0 : (ny >= 0.0 ? 1.0 / aj[0] : -1.0 / aj[0]);
+    const double drdz = (nz == 0.0) ? 0.0 : (nz >= 0.0 ? 1.0 / aj[0] : -1.0 / aj[0]);
+    double px = kxx * ky * kz * drdx;
+    double py = kx * kyy * kz * drdy;
+    double pz = kx * ky * kzz * drdz;
+    if (ebc_j) {
+      const double wm = 1.0 / (sqrt(nx * nx + ny * ny + nz * nz) + (double)1.0e-15f);
+      const double w3 = phi * wm * wm * wm;
+      px = px * wm - w3 * nx / aj[0];
+      py = py * wm - w3 * ny / aj[1];
+      pz = pz * wm - w3 * nz / aj[2];
+      phi = phi * wm;
+    }
+    e.phi = phi; e.px = px; e.py = py; e.pz = pz;
+  }
+}
+
+// packed symmetric 4x4: (00,01,02,03,11,12,13,22,23,33)
+__device__ __forceinline__ int sidx(int j, int k) {
+  if (j > k) { int t = j; j = k; k = t; }
+  return j == 0 ? k : (j == 1 ? 3 + k : (j == 2 ? 5 + k : 9));
+}
+
+__global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __restrict__ coo,
+                                                   const double* __restrict__ win,
+                                                   const int32_t* __restrict__ ebc_nodes,
+                                                   const int64_t* __restrict__ rowptr,
+                                                   const int32_t* __restrict__ col, int ql, double ql_coef,
+                                                   double ql_len, int shsup, double* __restrict__ shp,
+                                                   double* __restrict__ gx, double* __restrict__ gy,
+                                                   double* __restrict__ gz, unsigned* __restrict__ status) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const double xi[3] = {coo[3 * i], coo[3 * i + 1], coo[3 * i + 2]};
+  const int64_t p0 = rowptr[i], p1 = rowptr[i + 1];
+  double M[10], Mx[10], My[10], Mz[10], psum = 0.0;
+#pragma unroll
+  for (int k = 0; k < 10; ++k) { M[k] = 0.0; Mx[k] = 0.0; My[k] = 0.0; Mz[k] = 0.0; }
+  for (int64_t p = p0 + lane; p < p1; p += 32) {
+    const int64_t j = col[p];
+    const double xj[3] = {coo[3 * j], coo[3 * j + 1], coo[3 * j + 2]};
+    const double aj[3] = {win[3 * j], win[3 * j + 1], win[3 * j + 2]};
+    EntryK e;
+    rk_entry(xi, xj, aj, ebc_nodes && ebc_nodes[j], shsup, e);
+    psum += e.phi;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = a; b < 4; ++b) {
+        const int q = sidx(a, b);
+        const double hh = e.H[a] * e.H[b];
+        M[q] += hh * e.phi;
+        // (Hd H^T + H Hd^T) phi with Hd = unit vector of the axis
+        Mx[q] += hh * e.px + ((a == 1 ? e.H[b] : 0.0) + (b == 1 ? e.H[a] : 0.0)) * e.phi;
+        My[q] += hh * e.py + ((a == 2 ? e.H[b] : 0.0) + (b == 2 ? e.H[a] : 0.0)) * e.phi;
+        Mz[q] += hh * e.pz + ((a == 3 ? e.H[b] : 0.0) + (b == 3 ? e.H[a] : 0.0)) * e.phi;
+      }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    psum += __shfl_xor_sync(0xffffffffu, psum, o);
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      M[k] += __shfl_xor_sync(0xffffffffu, M[k], o);
+      Mx[k] += __shfl_xor_sync(0xffffffffu, Mx[k], o);
+      My[k] += __shfl_xor_sync(0xffffffffu, My[k], o);
+      Mz[k] += __shfl_xor_sync(0xffffffffu, Mz[k], o);
+    }
+  }
+  double Mf[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) Mf[a][b] = M[sidx(a, b)];
+  double Hs[4] = {0.0, 0.0, 0.0, 0.0};
+  if (ql) {
+    // RK.f90:253-301: the six points X +- QL_LEN e_d, differences evaluated
+    // in floating point as the reference does
+    double d[6][3];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) { d[m][0] = 0.0; d[m][1] = 0.0; d[m][2] = 0.0; }
+    d[0][0] = xi[0] - (xi[0] + ql_len); d[1][0] = xi[0] - (xi[0] - ql_len);
+    d[2][1] = xi[1] - (xi[1] + ql_len); d[3][1] = xi[1] - (xi[1] - ql_len);
+    d[4][2] = xi[2] - (xi[2] + ql_len); d[5][2] = xi[2] - (xi[2] - ql_len);
+    double Ms[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) Ms[a][b] = 0.0;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      const double H[4] = {1.0, d[m][0], d[m][1], d[m][2]};
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) Ms[a][b] += H[a] * H[b];
+      Hs[0] += 1.0; Hs[1] += d[m][0]; Hs[2] += d[m][1]; Hs[3] += d[m][2];
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) Mf[a][b] = Mf[a][b] + Ms[a][b] * psum * ql_coef;
+  }
+  double Mi[4][4];
+  const double det = m44inv(Mf, Mi);
+  if (lane == 0 && (!isfinite(det) || det == 0.0)) atomicOr(status, (unsigned)MEGA_ST_SINGULAR_MOMENT);
+  double B[4], BX[4], BY[4], BZ[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) B[k] = Mi[0][k];
+  // b_,d = -(b M_,d) M^-1
+  double t[4];
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd) {
+    const double* Md = dd == 0 ? Mx : (dd == 1 ? My : Mz);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) s += B[q] * Md[sidx(q, k)];
+      t[k] = -s;
+    }
+    double* out = dd == 0 ? BX : (dd == 1 ? BY : BZ);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out[k] = t[0] * Mi[0][k] + t[1] * Mi[1][k] + t[2] * Mi[2][k] + t[3] * Mi[3][k];
+  }
+  for (int64_t p = p0 + lane; p < p1; p += 32) {
+    const int64_t j = col[p];
+    const double xj[3] = {coo[3 * j], coo[3 * j + 1], coo[3 * j + 2]};
+    const double aj[3] = {win[3 * j], win[3 * j + 1], win[3 * j + 2]};
+    EntryK e;
+    rk_entry(xi, xj, aj, ebc_nodes && ebc_nodes[j], shsup, e);
+    double H[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) H[k] = ql ? e.H[k] + Hs[k] * ql_coef : e.H[k];
+    const double C = B[0] * H[0] + B[1] * H[1] + B[2] * H[2] + B[3] * H[3];
+    const double CX = BX[0] * H[0] + BX[1] * H[1] + BX[2] * H[2] + BX[3] * H[3] + B[1];
+    const double CY = BY[0] * H[0] + BY[1] * H[1] + BY[2] * H[2] + BY[3] * H[3] + B[2];
+    const double CZ = BZ[0] * H[0] + BZ[1] * H[1] + BZ[2] * H[2] + BZ[3] * H[3] + B[3];
+    shp[p] = C * e.phi;
+    gx[p] = CX * e.phi + C * e.px;
+    gy[p] = CY * e.phi + C * e.py;
+    gz[p] = CZ * e.phi + C * e.pz;
+  }
+}
+
+}  // namespace
+
+int rk_shapes(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
+              const int32_t* ebc_nodes, const DevCSR& csr, double* shp, double* gx, double* gy, double* gz,
+              unsigned* status) {
+  if (p.rk_degree != 1 || p.rk_cont != 3) return MEGA_ERR_UNSUPPORTED;
+  const int block = 128;
+  const unsigned grid = (unsigned)(((int64_t)n * 32 + block - 1) / block);
+  k_rk_shapes<<<grid, block, 0, s>>>(n, coo, win, ebc_nodes, csr.rowptr, csr.col, p.ql, p.ql_coef, p.ql_len,
+                                     p.shsup, shp, gx, gy, gz, status);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+}  // namespace mega

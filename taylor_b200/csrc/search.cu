@@ -1,0 +1,443 @@
+// search.cu -- sort-by-cell neighbour search, bit-exact with BIN_SEARCH.
+//
+// Replaces GET_BINS / BIN_INODE / SOFT_SEARCH (BIN_SEARCH.F90:2-328) and
+// the LINIT bin geometry of HANDELER.F90:187-250:
+//   1. bounding box and bin size (block reductions; max/min are exact);
+//   2. cell of each node, FLOOR((X-XMIN)/XBIN)+1 clamped (BIN_SEARCH.F90:28-41);
+//   3. counting sort by cell: histogram, exclusive scan, scatter, then a
+//      per-cell sort by node id so every cell lists its nodes in index order
+//      like NODELIST_IN_BIN does (BIN_SEARCH.F90:45-54);
+//   4. warp-per-node candidate filter over the 27 cells in BIN_INODE order
+//      (IX outer, IZ inner, BIN_SEARCH.F90:105-127), ballot + popc compaction
+//      so the output rows keep the reference's order exactly;
+//   5. count pass -> scan -> fill pass.
+// Every floating-point operation of the test uses __d*_rn intrinsics, so no
+// FMA contraction can change a comparison: the lists are bit-exact.
+#include "mega_internal.cuh"
+
+namespace mega {
+
+namespace {
+
+__device__ __forceinline__ void atomic_max_int(int32_t* a, int32_t v) { atomicMax(a, v); }
+
+// ---- 1. bounding box / bin size partials: 9 values per block:
+// [xbin, ybin, zbin, xmax, ymax, zmax, -xmin, -ymin, -zmin] as maxima
+__global__ void k_bbox_partial(int32_t n, const double* __restrict__ coo, const double* __restrict__ win,
+                               double d0, double d1, double d2, double* __restrict__ part) {
+  __shared__ double sm[9][32];
+  double v[9];
+  v[0] = 0.0; v[1] = 0.0; v[2] = 0.0;
+  v[3] = -INFINITY; v[4] = -INFINITY; v[5] = -INFINITY;
+  v[6] = -INFINITY; v[7] = -INFINITY; v[8] = -INFINITY;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double w0 = win[3 * i], w1 = win[3 * i + 1], w2 = win[3 * i + 2];
+    v[0] = fmax(v[0], fmax(w0, __dadd_rn(w0, d0)));
+    v[1] = fmax(v[1], fmax(w1, __dadd_rn(w1, d1)));
+    v[2] = fmax(v[2], fmax(w2, __dadd_rn(w2, d2)));
+    const double x0 = coo[3 * i], x1 = coo[3 * i + 1], x2 = coo[3 * i + 2];
+    v[3] = fmax(v[3], x0); v[4] = fmax(v[4], x1); v[5] = fmax(v[5], x2);
+    v[6] = fmax(v[6], -x0); v[7] = fmax(v[7], -x1); v[8] = fmax(v[8], -x2);
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] = fmax(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) sm[k][wid] = v[k];
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      double a = (lane < nw) ? sm[k][lane] : (k < 3 ? 0.0 : -INFINITY);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+      if (lane == 0) part[9 * blockIdx.x + k] = a;
+    }
+  }
+}
+
+// HANDELER.F90:221-243 in one thread, with the same IEEE operations.
+__global__ void k_bbox_final(int nb, const double* __restrict__ part, double* __restrict__ geom,
+                             int32_t* __restrict__ dims) {
+  double v[9];
+  for (int k = 0; k < 9; ++k) v[k] = part[k];
+  for (int b = 1; b < nb; ++b)
+    for (int k = 0; k < 9; ++k) v[k] = fmax(v[k], part[9 * b + k]);
+  const double xbin = v[0], ybin = v[1], zbin = v[2];
+  const double xmin = __dsub_rn(-v[6], __dmul_rn(xbin, 10.0));
+  const double ymin = __dsub_rn(-v[7], __dmul_rn(ybin, 10.0));
+  const double zmin = __dsub_rn(-v[8], __dmul_rn(zbin, 10.0));
+  const double xmax = __dadd_rn(v[3], __dmul_rn(xbin, 10.0));
+  const double ymax = __dadd_rn(v[4], __dmul_rn(ybin, 10.0));
+  const double zmax = __dadd_rn(v[5], __dmul_rn(zbin, 10.0));
+  geom[0] = xmin; geom[1] = ymin; geom[2] = zmin;
+  geom[3] = xbin; geom[4] = ybin; geom[5] = zbin;
+  dims[0] = (int32_t)ceil(__ddiv_rn(__dsub_rn(xmax, xmin), xbin));
+  dims[1] = (int32_t)ceil(__ddiv_rn(__dsub_rn(ymax, ymin), ybin));
+  dims[2] = (int32_t)ceil(__ddiv_rn(__dsub_rn(zmax, zmin), zbin));
+}
+
+__device__ __forceinline__ int32_t bin_of(double x, double xmin, double bin, int32_t nb) {
+  int32_t c = (int32_t)floor(__ddiv_rn(__dsub_rn(x, xmin), bin)) + 1;
+  c = max(1, c);
+  return min(c, nb);
+}
+
+// ---- 2. cell per node, histogram
+__global__ void k_cell_assign(int32_t n, const double* __restrict__ coo, const double* __restrict__ geom,
+                              int32_t nx, int32_t ny, int32_t nz, int32_t* __restrict__ cell,
+                              int32_t* __restrict__ cnt, int32_t* __restrict__ ijk) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t a = bin_of(coo[3 * i], geom[0], geom[3], nx);
+  const int32_t b = bin_of(coo[3 * i + 1], geom[1], geom[4], ny);
+  const int32_t c = bin_of(coo[3 * i + 2], geom[2], geom[5], nz);
+  const int32_t m = (c - 1) * nx * ny + (b - 1) * nx + (a - 1);
+  cell[i] = m;
+  atomicAdd(&cnt[m], 1);
+  if (ijk) { ijk[3 * i] = a; ijk[3 * i + 1] = b; ijk[3 * i + 2] = c; }
+}
+
+// ---- 3. scatter into cells, then restore index order inside each cell
+__global__ void k_cell_scatter(int32_t n, const int32_t* __restrict__ cell, const int64_t* __restrict__ cstart,
+                               int32_t* __restrict__ fill, int32_t* __restrict__ sorted) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t m = cell[i];
+  const int32_t k = atomicAdd(&fill[m], 1);
+  sorted[cstart[m] + k] = (int32_t)i;
+}
+
+__global__ void k_cell_sort(int64_t nbins, const int64_t* __restrict__ cstart, int32_t* __restrict__ sorted,
+                            unsigned* __restrict__ status) {
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (m >= nbins) return;
+  const int64_t s = cstart[m], e = cstart[m + 1];
+  if (e - s >= kMaxBinCount) atomicOr(status, (unsigned)MEGA_ST_BIN_OVERFLOW);
+  for (int64_t a = s + 1; a < e; ++a) {  // insertion sort (cells hold few nodes)
+    const int32_t v = sorted[a];
+    int64_t b = a - 1;
+    while (b >= s && sorted[b] > v) { sorted[b + 1] = sorted[b]; --b; }
+    sorted[b + 1] = v;
+  }
+}
+
+// SOFT_SEARCH acceptance test (BIN_SEARCH.F90:235-293), exact arithmetic.
+__device__ __forceinline__ bool accept(const double xi[3], const double xj[3], const double wj[3],
+                                       const double sl[6], int mmax, int shsup) {
+  for (int m = 0; m < mmax; ++m) {
+    double px = xj[0], py = xj[1], pz = xj[2];
+    if (m == 1) px = __dadd_rn(xj[0], sl[0]);
+    else if (m == 2) px = __dsub_rn(xj[0], sl[1]);
+    else if (m == 3) py = __dadd_rn(xj[1], sl[2]);
+    else if (m == 4) py = __dsub_rn(xj[1], sl[3]);
+    else if (m == 5) pz = __dadd_rn(xj[2], sl[4]);
+    else if (m == 6) pz = __dsub_rn(xj[2], sl[5]);
+    const double dx = fabs(__dsub_rn(px, xi[0]));
+    const double dy = fabs(__dsub_rn(py, xi[1]));
+    const double dz = fabs(__dsub_rn(pz, xi[2]));
+    if (shsup) {
+      const double a = __ddiv_rn(dx, wj[0]), b = __ddiv_rn(dy, wj[1]), c = __ddiv_rn(dz, wj[2]);
+      const double s = __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c));
+      if (__dsqrt_rn(s) < 1.0) return true;
+    } else {
+      if (__ddiv_rn(dx, wj[0]) < 1.0 && __ddiv_rn(dy, wj[1]) < 1.0 && __ddiv_rn(dz, wj[2]) < 1.0) return true;
+    }
+  }
+  return false;
+}
+
+// ---- 4/5. warp per node; FILL = false counts, FILL = true writes the row.
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_soft_search(
+    int32_t n, const double* __restrict__ coo, const double* __restrict__ win, const double* __restrict__ sm_len,
+    const int32_t* __restrict__ cell, int32_t nx, int32_t ny, int32_t nz, const int64_t* __restrict__ cstart,
+    const int32_t* __restrict__ sorted, int mmax, int shsup, int32_t* __restrict__ gn,
+    const int64_t* __restrict__ rowptr, int32_t* __restrict__ col, int32_t* __restrict__ gmaxn,
+    unsigned* __restrict__ status) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;  // whole warp leaves together
+  const double xi[3] = {coo[3 * i], coo[3 * i + 1], coo[3 * i + 2]};
+  double sl[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) sl[k] = sm_len[6 * i + k];
+  const int32_t m0 = cell[i];
+  const int32_t is = m0 % nx + 1, js = (m0 / nx) % ny + 1, ks = m0 / (nx * ny) + 1;
+  const int32_t i0 = max(is - 1, 1), i1 = min(is + 1, nx);
+  const int32_t j0 = max(js - 1, 1), j1 = min(js + 1, ny);
+  const int32_t k0 = max(ks - 1, 1), k1 = min(ks + 1, nz);
+  const unsigned lt = (1u << lane) - 1u;
+  int32_t count = 0;
+  int64_t ncand = 0;
+  int64_t base = FILL ? rowptr[i] : 0;
+  for (int32_t ix = i0; ix <= i1; ++ix)
+    for (int32_t iy = j0; iy <= j1; ++iy)
+      for (int32_t iz = k0; iz <= k1; ++iz) {
+        const int64_t m = (int64_t)(iz - 1) * nx * ny + (int64_t)(iy - 1) * nx + (ix - 1);
+        const int64_t p0 = cstart[m], p1 = cstart[m + 1];
+        ncand += p1 - p0;
+        for (int64_t q = p0; q < p1; q += 32) {
+          const int64_t p = q + lane;
+          bool add = false;
+          int32_t j = 0;
+          if (p < p1) {
+            j = sorted[p];
+            const double xj[3] = {coo[3 * (int64_t)j], coo[3 * (int64_t)j + 1], coo[3 * (int64_t)j + 2]};
+            const double wj[3] = {win[3 * (int64_t)j], win[3 * (int64_t)j + 1], win[3 * (int64_t)j + 2]};
+            add = accept(xi, xj, wj, sl, mmax, shsup);
+          }
+          const unsigned b = __ballot_sync(0xffffffffu, add);
+          if (FILL && add) col[base + count + __popc(b & lt)] = j;
+          count += __popc(b);
+        }
+      }
+  if (lane == 0) {
+    if (!FILL) {
+      gn[i] = count;
+      atomic_max_int(gmaxn, count);
+      if (ncand > kMaxCandidates) atomicOr(status, (unsigned)MEGA_ST_CAND_OVERFLOW);
+    }
+  }
+}
+
+// ---- scan helpers
+constexpr int kScanBlock = 1024;
+
+__global__ void k_scan_block_sums(int64_t m, const int32_t* __restrict__ cnt, int64_t* __restrict__ bsum) {
+  __shared__ int64_t sm[32];
+  const int64_t i = blockIdx.x * (int64_t)kScanBlock + threadIdx.x;
+  int64_t v = (i < m) ? cnt[i] : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int64_t a = sm[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = a;
+  }
+}
+
+// single block: exclusive scan of nb block sums in place, total at [nb]
+__global__ void k_scan_bsums(int64_t nb, int64_t* __restrict__ bsum) {
+  __shared__ int64_t carry_s;
+  __shared__ int64_t wsum[32];
+  if (threadIdx.x == 0) carry_s = 0;
+  __syncthreads();
+  for (int64_t b0 = 0; b0 < nb; b0 += kScanBlock) {
+    const int64_t b = b0 + threadIdx.x;
+    const int64_t v = (b < nb) ? bsum[b] : 0;
+    int64_t x = v;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int64_t w = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      wsum[lane] = w;
+    }
+    __syncthreads();
+    const int64_t incl = x + (wid > 0 ? wsum[wid - 1] : 0);
+    const int64_t carry = carry_s;
+    if (b < nb) bsum[b] = carry + incl - v;
+    __syncthreads();
+    if (threadIdx.x == kScanBlock - 1) carry_s = carry + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bsum[nb] = carry_s;
+}
+
+__global__ void k_scan_apply(int64_t m, const int32_t* __restrict__ cnt, const int64_t* __restrict__ bsum,
+                             int64_t* __restrict__ off) {
+  __shared__ int64_t wsum[32];
+  const int64_t i = blockIdx.x * (int64_t)kScanBlock + threadIdx.x;
+  const int64_t v = (i < m) ? cnt[i] : 0;
+  int64_t x = v;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int64_t w = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  const int64_t incl = x + (wid > 0 ? wsum[wid - 1] : 0);
+  if (i < m) off[i] = bsum[blockIdx.x] + incl - v;
+  if (i == m - 1) off[m] = bsum[blockIdx.x] + incl;
+}
+
+// ---- transpose (CSC) helpers
+__global__ void k_col_count(int64_t nnz, const int32_t* __restrict__ col, int32_t* __restrict__ ccnt) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p < nnz) atomicAdd(&ccnt[col[p]], 1);
+}
+__global__ void k_col_scatter(int32_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                              const int64_t* __restrict__ colptr, int32_t* __restrict__ cfill,
+                              int64_t* __restrict__ tpos, int32_t* __restrict__ trow) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  for (int64_t p = rowptr[i] + lane; p < rowptr[i + 1]; p += 32) {
+    const int32_t j = col[p];
+    const int64_t e = colptr[j] + atomicAdd(&cfill[j], 1);
+    tpos[e] = p;
+    trow[e] = (int32_t)i;
+  }
+}
+// order each column by CSR position (equivalently by row, rows being
+// contiguous and ascending), so the CSC sums are deterministic
+__global__ void k_col_sort(int32_t n, const int64_t* __restrict__ colptr, int64_t* __restrict__ tpos,
+                           int32_t* __restrict__ trow) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int64_t s = colptr[j], e = colptr[j + 1];
+  for (int64_t a = s + 1; a < e; ++a) {
+    const int64_t v = tpos[a];
+    const int32_t r = trow[a];
+    int64_t b = a - 1;
+    while (b >= s && tpos[b] > v) { tpos[b + 1] = tpos[b]; trow[b + 1] = trow[b]; --b; }
+    tpos[b + 1] = v;
+    trow[b + 1] = r;
+  }
+}
+
+inline unsigned grid_for(int64_t work, int block) { return (unsigned)((work + block - 1) / block); }
+
+}  // namespace
+
+int scan_counts(cudaStream_t s, const int32_t* cnt, int64_t* off, int64_t m, DevPool& scratch) {
+  if (m <= 0) {
+    MEGA_TRY(cudaMemsetAsync(off, 0, sizeof(int64_t), s));
+    return 0;
+  }
+  const int64_t nb = (m + kScanBlock - 1) / kScanBlock;
+  int64_t* bsum = nullptr;
+  MEGA_ALLOC(scratch, bsum, nb + 1);
+  k_scan_block_sums<<<(unsigned)nb, kScanBlock, 0, s>>>(m, cnt, bsum);
+  MEGA_CHECK_LAUNCH();
+  k_scan_bsums<<<1, kScanBlock, 0, s>>>(nb, bsum);
+  MEGA_CHECK_LAUNCH();
+  k_scan_apply<<<(unsigned)nb, kScanBlock, 0, s>>>(m, cnt, bsum, off);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, const double* sm_len,
+               const double dist_max[3], int32_t itype_int, int32_t shsup, unsigned* status, DevCSR& csr,
+               int32_t* ijk, DevPool& pool, BinGeom* geom_out) {
+  DevPool scratch;  // freed on return
+  csr.n = n;
+  const int nbb = 148 * 2;
+  double* part = nullptr;
+  double* geom = nullptr;
+  int32_t* dims = nullptr;
+  MEGA_ALLOC(scratch, part, 9 * nbb);
+  MEGA_ALLOC(scratch, geom, 6);
+  MEGA_ALLOC(scratch, dims, 3);
+  k_bbox_partial<<<nbb, 256, 0, s>>>(n, coo, win, dist_max[0], dist_max[1], dist_max[2], part);
+  MEGA_CHECK_LAUNCH();
+  k_bbox_final<<<1, 1, 0, s>>>(nbb, part, geom, dims);
+  MEGA_CHECK_LAUNCH();
+  BinGeom bg;
+  MEGA_TRY(cudaMemcpyAsync(bg.g, geom, sizeof(double) * 6, cudaMemcpyDeviceToHost, s));
+  int32_t hd[3];
+  MEGA_TRY(cudaMemcpyAsync(hd, dims, sizeof(hd), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaStreamSynchronize(s));
+  bg.nx = hd[0]; bg.ny = hd[1]; bg.nz = hd[2];
+  if (geom_out) *geom_out = bg;
+  const int64_t nbins = (int64_t)bg.nx * bg.ny * bg.nz;
+  if (bg.nx <= 0 || bg.ny <= 0 || bg.nz <= 0 || nbins > INT32_MAX) return MEGA_ERR_UNSUPPORTED;
+
+  int32_t *cell = nullptr, *cnt = nullptr, *fill = nullptr, *sorted = nullptr, *gn = nullptr;
+  int64_t* cstart = nullptr;
+  MEGA_ALLOC(scratch, cell, n);
+  MEGA_ALLOC(scratch, cnt, nbins);
+  MEGA_ALLOC(scratch, fill, nbins);
+  MEGA_ALLOC(scratch, cstart, nbins + 1);
+  MEGA_ALLOC(scratch, sorted, n);
+  MEGA_ALLOC(scratch, gn, n);
+  MEGA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * nbins, s));
+  MEGA_TRY(cudaMemsetAsync(fill, 0, sizeof(int32_t) * nbins, s));
+  k_cell_assign<<<grid_for(n, 256), 256, 0, s>>>(n, coo, geom, bg.nx, bg.ny, bg.nz, cell, cnt, ijk);
+  MEGA_CHECK_LAUNCH();
+  int r = scan_counts(s, cnt, cstart, nbins, scratch);
+  if (r) return r;
+  k_cell_scatter<<<grid_for(n, 256), 256, 0, s>>>(n, cell, cstart, fill, sorted);
+  MEGA_CHECK_LAUNCH();
+  k_cell_sort<<<grid_for(nbins, 256), 256, 0, s>>>(nbins, cstart, sorted, status);
+  MEGA_CHECK_LAUNCH();
+
+  const int mmax = (itype_int == 0) ? 1 : 7;  // BIN_SEARCH.F90:204-208
+  int32_t* gmaxn = nullptr;
+  MEGA_ALLOC(scratch, gmaxn, 1);
+  MEGA_TRY(cudaMemsetAsync(gmaxn, 0, sizeof(int32_t), s));
+  MEGA_ALLOC(pool, csr.rowptr, (int64_t)n + 1);
+  const unsigned gw = grid_for((int64_t)n * 32, 256);
+  k_soft_search<false><<<gw, 256, 0, s>>>(n, coo, win, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax,
+                                          shsup, gn, nullptr, nullptr, gmaxn, status);
+  MEGA_CHECK_LAUNCH();
+  r = scan_counts(s, gn, csr.rowptr, n, scratch);
+  if (r) return r;
+  int64_t nnz = 0;
+  MEGA_TRY(cudaMemcpyAsync(&nnz, csr.rowptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(&csr.gmaxn, gmaxn, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaStreamSynchronize(s));
+  csr.nnz = nnz;
+  MEGA_ALLOC(pool, csr.col, nnz);
+  k_soft_search<true><<<gw, 256, 0, s>>>(n, coo, win, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax,
+                                         shsup, gn, csr.rowptr, csr.col, gmaxn, status);
+  MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int build_transpose(cudaStream_t s, DevCSR& csr, DevPool& pool) {
+  DevPool scratch;
+  const int32_t n = csr.n;
+  int32_t *ccnt = nullptr, *cfill = nullptr;
+  MEGA_ALLOC(scratch, ccnt, n);
+  MEGA_ALLOC(scratch, cfill, n);
+  MEGA_ALLOC(pool, csr.colptr, (int64_t)n + 1);
+  MEGA_ALLOC(pool, csr.trow, csr.nnz);
+  MEGA_ALLOC(pool, csr.tpos, csr.nnz);
+  MEGA_TRY(cudaMemsetAsync(ccnt, 0, sizeof(int32_t) * n, s));
+  MEGA_TRY(cudaMemsetAsync(cfill, 0, sizeof(int32_t) * n, s));
+  k_col_count<<<grid_for(csr.nnz, 256), 256, 0, s>>>(csr.nnz, csr.col, ccnt);
+  MEGA_CHECK_LAUNCH();
+  int r = scan_counts(s, ccnt, csr.colptr, n, scratch);
+  if (r) return r;
+  k_col_scatter<<<grid_for((int64_t)n * 32, 256), 256, 0, s>>>(n, csr.rowptr, csr.col, csr.colptr, cfill, csr.tpos,
+                                                              csr.trow);
+  MEGA_CHECK_LAUNCH();
+  k_col_sort<<<grid_for(n, 128), 128, 0, s>>>(n, csr.colptr, csr.tpos, csr.trow);
+  MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+}  // namespace mega

@@ -1,0 +1,233 @@
+"""Host-side mirror of MEGA's hot-path interface over libmega_gpu.so.
+
+Function names and argument meanings follow the reference's subroutines:
+  bin_search        GET_BINS + SOFT_SEARCH      (BIN_SEARCH.F90:2-328)
+  rk_shapes         RK1 over all nodes           (RK.f90:16-453, FINT.F90:404-408)
+  hughes_winget     HUGHES_WINGET                (HUGHES_WINGET.F90:16-81)
+  rotate_tensor     ROTATE_TENSOR                (ROTATE_TENSOR.F90:21-87)
+  constitution      CONSTITUTION                 (CONSTITUTION.F90:18-89)
+  construct_fint    CONSTRUCT_FINT               (FINT.F90:16-1336)
+  construct_fint_pd CONSTRUCT_FINT_PD            (FINT_PD.F90:16-759)
+  Mega              the MAIN.F90:304-658 time loop, device resident.
+Errors are raised as MegaError with the reference's message, the way
+EXIT_PROGRAM would stop the Fortran program.  Neighbour lists are 1-based.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ptr
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def bin_search(coo, win, sm_len, dist_max, itype_int=0, shsup=False, dim_nn_list=None):
+    """Neighbour lists of every node (GN, GSTART, GSTACK 1-based, GMAXN, GIJKSPC)."""
+    coo, win, sm_len = _f64(coo), _f64(win), _f64(sm_len)
+    dist_max = _f64(dist_max)
+    n = len(coo)
+    gn = np.zeros(n, np.int32)
+    gstart = np.zeros(n, np.int32)
+    ijk = np.zeros((n, 3), np.int32)
+    gmaxn = C.c_int32(0)
+    nnz = C.c_int64(0)
+    cap = int(dim_nn_list) if dim_nn_list else n * 128
+    while True:
+        gstack = np.zeros(cap, np.int32)
+        st = _lib.lib().mega_bin_search(n, ptr(coo), ptr(win), ptr(sm_len), ptr(dist_max), int(itype_int),
+                                        int(bool(shsup)), ptr(gn), ptr(gstart), ptr(gstack), cap,
+                                        C.byref(gmaxn), ptr(ijk), C.byref(nnz))
+        if st > 0 and (st & _lib.ST_STACK_OVERFLOW) and not dim_nn_list:
+            cap = int(nnz.value)
+            continue
+        check(st, "bin_search")
+        break
+    return dict(gn=gn, gstart=gstart, gstack=gstack[: nnz.value].copy(), gmaxn=gmaxn.value, ijk=ijk,
+                nnz=int(nnz.value))
+
+
+def rk_shapes(params, coo, win, ebc_nodes, gn, gstart, gstack):
+    """GSTACK_SHP (nnz) and GSTACK_DSHP (nnz,3) from RK1 at every node."""
+    coo, win = _f64(coo), _f64(win)
+    gn, gstart, gstack = _i32(gn), _i32(gstart), _i32(gstack)
+    n = len(coo)
+    nnz = len(gstack)
+    shp = np.zeros(nnz)
+    dshp = np.zeros((nnz, 3))
+    en = None if ebc_nodes is None else _i32(ebc_nodes)
+    st = _lib.lib().mega_rk_shapes(C.byref(params), n, ptr(coo), ptr(win), ptr(en), ptr(gn), ptr(gstart),
+                                   ptr(gstack), nnz, ptr(shp), ptr(dshp))
+    check(st, "rk_shapes")
+    return shp, dshp
+
+
+def hughes_winget(params, lmat):
+    """lmat (n,3,3) -> rot (n,3,3), strain (n,6), d (n,6)."""
+    lm = np.ascontiguousarray(np.transpose(_f64(lmat), (0, 2, 1)))  # column-major per node
+    n = len(lm)
+    rot = np.zeros((n, 3, 3))
+    strain = np.zeros((n, 6))
+    d = np.zeros((n, 6))
+    check(_lib.lib().mega_hughes_winget(C.byref(params), n, ptr(lm), ptr(rot), ptr(strain), ptr(d)),
+          "hughes_winget")
+    return np.transpose(rot, (0, 2, 1)).copy(), strain, d
+
+
+def rotate_tensor(rot, v):
+    r = np.ascontiguousarray(np.transpose(_f64(rot), (0, 2, 1)))
+    v = _f64(v).copy()
+    check(_lib.lib().mega_rotate_tensor(len(v), ptr(r), ptr(v)), "rotate_tensor")
+    return v
+
+
+def constitution(params, stress_pred, mat_type, props, dlt, state, allow_status=False):
+    """Returns (stress (n,6), state (n,20), iterations (n), status)."""
+    sp = _f64(stress_pred)
+    n = len(sp)
+    state = _f64(state).copy()
+    stress = np.zeros((n, 6))
+    it = np.zeros(n, np.int32)
+    st = _lib.lib().mega_constitution(C.byref(params), n, ptr(sp), ptr(_i32(mat_type)), ptr(_f64(props)),
+                                      float(dlt), ptr(state), ptr(stress), ptr(it))
+    check(st, "constitution", allow_status)
+    return stress, state, it, st
+
+
+def construct_fint(params, coo, win, vol, props, mat_type, ebc_nodes, state, stress, strain, dinc, dinc_tot,
+                   gn, gstart, gstack, shp, dshp, linit, dlt, bodyforce=None, gint_work=0.0, allow_status=False):
+    """CONSTRUCT_FINT: returns a dict with fint, fext (3N), stress, strain,
+    state, gmax_wvel, gstrain_eq, gint_work and (linit) the shape stacks."""
+    n = len(coo)
+    state, stress, strain = _f64(state).copy(), _f64(stress).copy(), _f64(strain).copy()
+    shp, dshp = _f64(shp).copy(), _f64(dshp).copy()
+    fint = np.zeros(3 * n)
+    fext = np.zeros(3 * n)
+    wv = np.zeros(n)
+    seq = np.zeros(n)
+    gw = C.c_double(gint_work)
+    en = None if ebc_nodes is None else _i32(ebc_nodes)
+    st = _lib.lib().mega_construct_fint(
+        C.byref(params), n, ptr(_f64(coo)), ptr(_f64(win)), ptr(_f64(vol)), ptr(_f64(props)), ptr(_i32(mat_type)),
+        ptr(en), ptr(None if bodyforce is None else _f64(bodyforce)), ptr(state), ptr(stress), ptr(strain),
+        ptr(_f64(dinc)), ptr(_f64(dinc_tot)), ptr(_i32(gn)), ptr(_i32(gstart)), ptr(_i32(gstack)), len(gstack),
+        ptr(shp), ptr(dshp), int(bool(linit)), float(dlt), ptr(fint), ptr(fext), ptr(wv), ptr(seq), C.byref(gw))
+    check(st, "construct_fint", allow_status)
+    return dict(fint=fint, fext=fext, stress=stress, strain=strain, state=state, gmax_wvel=wv, gstrain_eq=seq,
+                gint_work=gw.value, shp=shp, dshp=dshp, status=st)
+
+
+class Mega:
+    """Device-resident model: the MAIN.F90 time loop on the GPU.
+
+    Construct from a case dict (taylor_b200.cases), call search_and_shapes()
+    once (LINIT), then step(nsteps, dt, mode)."""
+
+    def __init__(self, case, params):
+        self.case = case
+        self.n = int(case["n"])
+        self.params = params
+        h = C.c_int64(0)
+        bf = case.get("bodyforce")
+        check(_lib.lib().mega_gpu_init(
+            C.byref(params), self.n, ptr(_f64(case["coo"])), ptr(_f64(case["win"])), ptr(_f64(case["vol"])),
+            ptr(_f64(case["mass"])), ptr(_i32(case["ebc"])), ptr(_f64(case["vinit"])), ptr(_f64(case["props"])),
+            ptr(_i32(case["mat_type"])), ptr(_i32(case["body_id"])), ptr(None if bf is None else _f64(bf)),
+            ptr(_f64(case["sm_len"])), C.byref(h)), "mega_gpu_init")
+        self.h = h.value
+        self.nnz = 0
+
+    def search_and_shapes(self, download=False, allow_status=False):
+        nnz = C.c_int64(0)
+        gmaxn = C.c_int32(0)
+        L = _lib.lib()
+        if not download:
+            st = L.mega_search_and_shapes(self.h, None, None, None, 0, None, None, C.byref(nnz), C.byref(gmaxn))
+            check(st, "search_and_shapes", allow_status)
+            self.nnz, self.gmaxn = nnz.value, gmaxn.value
+            return dict(nnz=self.nnz, gmaxn=self.gmaxn, status=st)
+        # first pass learns nnz, second downloads (the device search is cheap)
+        st = L.mega_search_and_shapes(self.h, None, None, None, 0, None, None, C.byref(nnz), C.byref(gmaxn))
+        check(st, "search_and_shapes", allow_status)
+        m = nnz.value
+        gn = np.zeros(self.n, np.int32)
+        gstart = np.zeros(self.n, np.int32)
+        gstack = np.zeros(m, np.int32)
+        shp = np.zeros(m)
+        dshp = np.zeros((m, 3))
+        st = L.mega_search_and_shapes(self.h, ptr(gn), ptr(gstart), ptr(gstack), m, ptr(shp), ptr(dshp),
+                                      C.byref(nnz), C.byref(gmaxn))
+        check(st, "search_and_shapes", allow_status)
+        self.nnz, self.gmaxn = nnz.value, gmaxn.value
+        return dict(gn=gn, gstart=gstart, gstack=gstack, shp=shp, dshp=dshp, nnz=m, gmaxn=gmaxn.value, status=st)
+
+    @staticmethod
+    def mode_bits(mode="fp64", interp_each_step=False, learned=False):
+        b = {"fp64": _lib.MODE_FP64, "mixed": _lib.MODE_MIXED}[mode]
+        if interp_each_step:
+            b |= _lib.FLAG_INTERP_EACH_STEP
+        if learned:
+            b |= _lib.FLAG_LEARNED_GUESS
+        return b
+
+    def step(self, nsteps, dt, mode="fp64", interp_each_step=False, allow_status=False):
+        st = _lib.lib().mega_step_resident(self.h, int(nsteps), float(dt),
+                                           self.mode_bits(mode, interp_each_step))
+        return check(st, "step", allow_status)
+
+    def step_timed(self, nsteps, dt, mode="fp64", interp_each_step=False):
+        ms = C.c_float(0.0)
+        st = _lib.lib().mega_step_timed(self.h, int(nsteps), float(dt), self.mode_bits(mode, interp_each_step),
+                                        C.byref(ms))
+        check(st, "step_timed")
+        return ms.value
+
+    def kernel_times(self, reps, dt, mode="fp64"):
+        out = np.zeros(3, np.float32)
+        check(_lib.lib().mega_kernel_times(self.h, int(reps), float(dt), self.mode_bits(mode), ptr(out)),
+              "kernel_times")
+        return out
+
+    _SIZES = {0: 3, 1: 3, 2: 3, 3: 3, 4: 3, 5: 3, 6: 3, 7: 6, 8: 6, 9: 1, 10: 1, 11: 1, 12: 3, 13: 3, 14: 1}
+
+    def download(self, field):
+        k = self._SIZES[field]
+        out = np.zeros(self.n * k)
+        check(_lib.lib().mega_download(self.h, int(field), ptr(out)), "download")
+        return out.reshape(self.n, k) if k > 1 else out
+
+    def upload(self, field, arr):
+        check(_lib.lib().mega_upload(self.h, int(field), ptr(_f64(arr).ravel())), "upload")
+
+    def scalars(self):
+        s = _lib.MegaScalars()
+        check(_lib.lib().mega_get_scalars(self.h, C.byref(s)), "scalars")
+        return dict(time=s.time, int_energy=s.int_energy, kin_energy=s.kin_energy, ext_energy=s.ext_energy,
+                    total_force=list(s.total_force), steps=s.steps, newton_iters=s.newton_iters,
+                    plastic_nodes=s.plastic_nodes)
+
+    def device_bytes(self):
+        return int(_lib.lib().mega_device_bytes(self.h))
+
+    def kernel_launches(self):
+        return int(_lib.lib().mega_kernel_launches(self.h))
+
+    def close(self):
+        if self.h:
+            _lib.lib().mega_gpu_finalize(self.h)
+            self.h = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,108 @@
+"""Generate tests/golden/case_a.npz from the reference's sample deck.
+
+Golden case A is the reference's own input: Taylor_bar.k (1,950 nodes,
+1,536 hexahedra, node sets BAR and WALL) with the Control.dat deck.  This
+script runs where the reference tree is mounted (it is not needed, and not
+run, on a GPU box) and restates the pre-processing that turns the mesh into
+the arrays the hot path consumes:
+  *NODE / *ELEMENT_SOLID / *SET_NODE_LIST fixed-width reads  PRE_MODEL.F90:149-231
+  raw nodal windows = max element extent per axis            PRE_MODEL_ADIAL.F90:64-153
+  nodal volumes = 1/8 of each adjacent hex (GET_VOL2)         PRE_MODEL_VOLUMES.F90:70-117,
+                                                             PRE_MODEL_VOL2.F90:36-52
+  the deck values the hot path uses (window 2.75, QL, props, v0, fixity, dt)
+                                                             Control.dat, READ.F90:354-511
+Usage: python tests/golden/make_case_a.py [reference_dir]
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def read_k(path):
+    lines = open(path).read().splitlines()
+    nodes, elems, sets = {}, [], {}
+    i = 0
+    while i < len(lines):
+        t = lines[i].strip()
+        if t == "*NODE":
+            i += 2  # comment line follows the card (PRE_MODEL.F90:156)
+            while i < len(lines) and not lines[i].startswith("*"):
+                ln = lines[i]
+                if ln.startswith("$") or not ln.strip():
+                    i += 1
+                    continue
+                nid = int(ln[0:8])
+                nodes[nid] = (float(ln[8:24]), float(ln[24:40]), float(ln[40:56]))
+                i += 1
+            continue
+        if t == "*ELEMENT_SOLID":
+            i += 1
+            while i < len(lines) and not lines[i].startswith("*"):
+                ln = lines[i]
+                if ln.strip() and not ln.startswith("$"):
+                    elems.append([int(ln[8 * k:8 * k + 8]) for k in range(2, 10)])
+                i += 1
+            continue
+        if t == "*SET_NODE_LIST":
+            sid = int(lines[i + 1].split()[0])
+            i += 2
+            ids = []
+            while i < len(lines) and not lines[i].startswith("*"):
+                ln = lines[i]
+                for k in range(8):
+                    f = ln[10 * k:10 * k + 10].strip()
+                    if f:
+                        v = int(f)
+                        if v != 0:
+                            ids.append(v)
+                i += 1
+            sets[sid] = np.array(ids, np.int32)
+            continue
+        i += 1
+    n = max(nodes)
+    coo = np.zeros((n, 3))
+    for k, v in nodes.items():
+        coo[k - 1] = v
+    return coo, np.array(elems, np.int32) - 1, sets
+
+
+def det_abs(a):
+    return abs(a[0, 0] * (a[1, 1] * a[2, 2] - a[2, 1] * a[1, 2]) + a[0, 1] * (a[2, 0] * a[1, 2] - a[1, 0] * a[2, 2])
+               + a[0, 2] * (a[1, 0] * a[2, 1] - a[2, 0] * a[1, 1]))
+
+
+def windows_and_volumes(coo, elems):
+    n = len(coo)
+    adial = np.zeros((n, 3))
+    vol = np.zeros(n)
+    for el in elems:
+        xe = coo[el]                      # (8,3)
+        ext = xe.max(0) - xe.min(0)       # max |x_k - x_j| over the element's nodes
+        for k in el:
+            adial[k] = np.maximum(adial[k], ext)
+        # GET_VOL2: columns X7-X1; X2-X1 | X5-X1 | X4-X1; X3-X6 | X6-X8 | X8-X3
+        x = xe
+        A = np.stack([x[6] - x[0], x[1] - x[0], x[2] - x[5]], axis=1)
+        B = np.stack([x[6] - x[0], x[4] - x[0], x[5] - x[7]], axis=1)
+        Cm = np.stack([x[6] - x[0], x[3] - x[0], x[7] - x[2]], axis=1)
+        dvol = (det_abs(A) + det_abs(B) + det_abs(Cm)) / 6.0
+        vol[el] += 0.125 * dvol
+    return adial, vol
+
+
+def main(ref=None):
+    ref = ref or "/root/reference"
+    coo, elems, sets = read_k(os.path.join(ref, "Taylor_bar.k"))
+    win_raw, vol = windows_and_volumes(coo, elems)
+    out = os.path.join(HERE, "case_a.npz")
+    np.savez_compressed(out, coo=coo, win_raw=win_raw, vol=vol, bar=sets[1], wall=sets[2],
+                        norm_win=2.75, v0=373.0, dt=0.78363e-07, time_end=5.5e-05, ql_coef=0.001,
+                        props=np.array([0.3, 78.2e9, 2700.0, 0.29e9, 125.0, 0.1]), mat_type=2)
+    print("wrote", out, "nodes", len(coo), "elements", len(elems), "wall", len(sets[2]))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else None)
