@@ -262,6 +262,29 @@ int64_t mega_device_bytes(int64_t h);
 /* Number of kernels launched by the context since creation. */
 int64_t mega_kernel_launches(int64_t h);
 
+/* ======================================================================== */
+/* Bond-based peridynamics (no reference counterpart: the reference's        */
+/* FINT_PD is correspondence-based).  Prototype microelastic brittle model  */
+/* (Silling & Askari 2005) with bond breaking, resident on the device.      */
+/* ======================================================================== */
+
+/* coo (3,n) reference positions, vol (n), vinit (3,n), fixed (n) particles
+ * that keep their velocity (may be NULL); spherical horizon; micromodulus
+ * c; critical stretch s_c; density rho; broken0 (nnz) initial broken flags
+ * per neighbour-list entry (may be NULL; the list is the SOFT_SEARCH
+ * ellipsoidal-support list with window = horizon, as mega_bin_search(...,
+ * shsup = 1) returns it).  *nbonds = list entries (self included). */
+int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double* vinit,
+                  const int32_t* fixed, double horizon, double micromodulus, double s_c,
+                  double rho, const uint8_t* broken0, int64_t* handle, int64_t* nbonds);
+/* nsteps of velocity-Verlet (float force, double positions); *ms device time
+ * of the call when ms is not NULL. */
+int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms);
+/* what: 0 displacement (3,n), 1 velocity, 2 acceleration, 3 broken flags (nnz);
+ * *nbroken = bond copies broken so far (each bond breaks at both ends). */
+int mega_pmb_download(int64_t h, int32_t what, double* dst, int64_t* nbroken);
+int mega_pmb_finalize(int64_t h);
+
 const char* mega_status_string(int32_t status);
 int mega_gpu_finalize(int64_t h);
 

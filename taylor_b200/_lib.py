@@ -80,6 +80,10 @@ SIGNATURES = {
     "mega_get_scalars": (I32, [I64, C.POINTER(MegaScalars)]),
     "mega_device_bytes": (I64, [I64]),
     "mega_kernel_launches": (I64, [I64]),
+    "mega_pmb_init": (I32, [I32, P, P, P, P, D, D, D, D, P, C.POINTER(I64), C.POINTER(I64)]),
+    "mega_pmb_step": (I32, [I64, I32, D, C.POINTER(F32)]),
+    "mega_pmb_download": (I32, [I64, I32, P, C.POINTER(I64)]),
+    "mega_pmb_finalize": (I32, [I64]),
     "mega_status_string": (C.c_char_p, [I32]),
     "mega_gpu_finalize": (I32, [I64]),
 }

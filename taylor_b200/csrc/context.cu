@@ -1079,13 +1079,4 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   return (int)hst;
 }
 
-int mega_construct_fint_pd(const mega_params* p, int32_t n, const double* gcoo, const double* gcoo_current,
-                           const double* gwin, const double* gvol, const double* gprop, const int32_t* gmat_type,
-                           double* gstate, double* gstress, double* gstrain, const double* gdinc, const int32_t* gn,
-                           const int32_t* gstart, const int32_t* gstack, int64_t nnz, double* gstack_shp,
-                           double* ginvk, int32_t linit, double dlt, double* fint, double* gmax_wvel,
-                           double* gint_work) {
-  return MEGA_ERR_UNSUPPORTED;
-}
-
 }  // extern "C"

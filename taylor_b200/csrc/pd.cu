@@ -1,0 +1,706 @@
+// pd.cu -- peridynamic forces.
+//
+// 1. Correspondence ("non-ordinary state-based") peridynamics of
+//    CONSTRUCT_FINT_PD (FINT_PD.F90:214-684), Lagrangian, HODIV = .FALSE.:
+//    influence w_iJ = box cubic spline, K_i = sum_J xi xi^T w V_J and its
+//    full-pivot inverse (UDFM_SHAPE_TENSOR, RK.f90:579-726); per step
+//    F = S K^-1 with S = sum_J (x_J - x_i) xi^T w V_J (DFM_SHAPE_TENSOR,
+//    RK.f90:730-807), L = (sum_J (du_J - du_i) xi^T w V_J) K^-1 F^-1, the
+//    same Hughes-Winget / return mapping as the RKPM path, P = J sigma F^-T
+//    and the pair forces FINT3 = P K^-1 (X_i - X_J):
+//       f_J -= FINT3 V_i w V_J,   f_i += FINT3 V_J w V_i   (FINT_PD.F90:629-655).
+//    With A_i = P_i K_i^-1 the force on node k is
+//       f_k = V_k [ A_k s_k - sum_{i: k in N(i)} A_i (X_i - X_k) w_ik V_i ],
+//    s_k = sum_J (X_k - X_J) w_kJ V_J (static), gathered over the transposed
+//    list without atomics.
+// 2. Bond-based prototype-microelastic-brittle peridynamics (no reference
+//    counterpart; Silling & Askari 2005): f_i = sum_j c s mu (y_j - y_i)/|.|
+//    V_j, a bond breaks for good when its stretch exceeds s_c.  Each bond is
+//    evaluated from both ends with bitwise-identical arithmetic, so both
+//    copies break in the same step.  Float force arithmetic, double
+//    positions and velocity-Verlet integration.
+#include <mutex>
+#include <set>
+#include "mega_internal.cuh"
+
+namespace mega {
+namespace {
+
+constexpr int kG = 4;
+
+__device__ __forceinline__ double box_w(double r) {
+  double w, dw;
+  bspline3(fabs(r), w, dw);
+  return w;
+}
+
+// UDFM_SHAPE_TENSOR: influence functions, K^-1 (column-major (3,3,n)) and s_i
+__global__ void k_pd_shape(int32_t n, const double* __restrict__ X, const double* __restrict__ win,
+                           const double* __restrict__ vol, const int64_t* __restrict__ rowptr,
+                           const int32_t* __restrict__ col, double* __restrict__ shp, double* __restrict__ ginvk,
+                           double* __restrict__ svec, unsigned* __restrict__ status) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kG;
+  const int q = threadIdx.x & (kG - 1);
+  const unsigned gm = 0xFu << (threadIdx.x & 28);
+  if (i >= n) return;
+  const double xi0 = X[3 * i], xi1 = X[3 * i + 1], xi2 = X[3 * i + 2];
+  double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, s[3] = {0, 0, 0};
+  for (int64_t p = rowptr[i] + q; p < rowptr[i + 1]; p += kG) {
+    const int64_t j = col[p];
+    const double h0 = -(xi0 - X[3 * j]), h1 = -(xi1 - X[3 * j + 1]), h2 = -(xi2 - X[3 * j + 2]);
+    const double w = box_w(h0 / win[3 * j]) * box_w(h1 / win[3 * j + 1]) * box_w(h2 / win[3 * j + 2]);
+    const double vw = w * vol[j];
+    K[0] += h0 * h0 * vw; K[1] += h0 * h1 * vw; K[2] += h0 * h2 * vw;
+    K[4] += h1 * h1 * vw; K[5] += h1 * h2 * vw; K[8] += h2 * h2 * vw;
+    s[0] -= h0 * vw; s[1] -= h1 * vw; s[2] -= h2 * vw;
+    shp[p] = w;
+  }
+#pragma unroll
+  for (int o = 1; o < kG; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) K[k] += __shfl_xor_sync(gm, K[k], o);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s[k] += __shfl_xor_sync(gm, s[k], o);
+  }
+  if (q == 0) {
+    double A[3][3] = {{K[0], K[1], K[2]}, {K[1], K[4], K[5]}, {K[2], K[5], K[8]}}, R[3][3];
+    if (!inverse3_gj(A, R)) atomicOr(status, (unsigned)MEGA_ST_SINGULAR_SHAPE);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) ginvk[9 * i + 3 * b + a] = R[a][b];
+    svec[3 * i] = s[0]; svec[3 * i + 1] = s[1]; svec[3 * i + 2] = s[2];
+  }
+}
+
+// static s_k when the influence functions come from the caller
+__global__ void k_pd_svec(int32_t n, const double* __restrict__ X, const double* __restrict__ vol,
+                          const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                          const double* __restrict__ shp, double* __restrict__ svec) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int64_t p = rowptr[i]; p < rowptr[i + 1]; ++p) {
+    const int64_t j = col[p];
+    const double vw = shp[p] * vol[j];
+    s0 += (X[3 * i] - X[3 * j]) * vw; s1 += (X[3 * i + 1] - X[3 * j + 1]) * vw; s2 += (X[3 * i + 2] - X[3 * j + 2]) * vw;
+  }
+  svec[3 * i] = s0; svec[3 * i + 1] = s1; svec[3 * i + 2] = s2;
+}
+
+// DFM_SHAPE_TENSOR twice: S (current coordinates) and the increment tensor
+__global__ void k_pd_defgrad(int32_t n, const double* __restrict__ X, const double* __restrict__ xc,
+                             const double* __restrict__ du, const double* __restrict__ vol,
+                             const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                             const double* __restrict__ shp, double* __restrict__ fg) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kG;
+  const int q = threadIdx.x & (kG - 1);
+  const unsigned gm = 0xFu << (threadIdx.x & 28);
+  if (i >= n) return;
+  double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const double X0[3] = {X[3 * i], X[3 * i + 1], X[3 * i + 2]};
+  const double x0[3] = {xc[3 * i], xc[3 * i + 1], xc[3 * i + 2]};
+  const double d0[3] = {du[3 * i], du[3 * i + 1], du[3 * i + 2]};
+  for (int64_t p = rowptr[i] + q; p < rowptr[i + 1]; p += kG) {
+    const int64_t j = col[p];
+    const double vw = shp[p] * vol[j];
+    const double h[3] = {X[3 * j] - X0[0], X[3 * j + 1] - X0[1], X[3 * j + 2] - X0[2]};
+    const double hs[3] = {xc[3 * j] - x0[0], xc[3 * j + 1] - x0[1], xc[3 * j + 2] - x0[2]};
+    const double hd[3] = {du[3 * j] - d0[0], du[3 * j + 1] - d0[1], du[3 * j + 2] - d0[2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        S[3 * a + b] += hs[a] * h[b] * vw;
+        L[3 * a + b] += hd[a] * h[b] * vw;
+      }
+  }
+#pragma unroll
+  for (int o = 1; o < kG; o <<= 1)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      S[k] += __shfl_xor_sync(gm, S[k], o);
+      L[k] += __shfl_xor_sync(gm, L[k], o);
+    }
+  if (q == 0)
+    for (int k = 0; k < 9; ++k) { fg[18 * i + k] = S[k]; fg[18 * i + 9 + k] = L[k]; }
+}
+
+struct PdStressArgs {
+  int32_t n;
+  const double* fg;
+  const double* ginvk;
+  const uint16_t* matidx;
+  const MatEntry* mats;
+  double* stress;
+  double* strain;
+  double* eps;
+  double* wvel;
+  double* amat;  // 9 per node, row-major A_i = P_i K_i^-1
+  int linit;
+  int inv3_exact;
+  int maxit;
+  double rtol;
+  double dt;
+  unsigned* status;
+};
+
+__global__ void k_pd_stress(PdStressArgs a) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const double* g = a.fg + 18 * i;
+  double Ki[3][3], F[3][3], IF[3][3], Ld[3][3], L[3][3], t[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) { Ki[r][c] = a.ginvk[9 * i + 3 * c + r]; Ld[r][c] = g[9 + 3 * r + c]; }
+  double det = 1.0;
+  unsigned st = 0;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) IF[r][c] = (r == c) ? 1.0 : 0.0;
+  if (!a.linit) {
+    double S[3][3];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) S[r][c] = g[3 * r + c];
+    mm3(S, Ki, F);
+    det = det_abs(F);
+    if (!inverse3_gj(F, IF)) st |= MEGA_ST_SINGULAR_SHAPE;
+  }
+  mm3(Ld, Ki, t);
+  if (!a.linit) mm3(t, IF, L);
+  else
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) L[r][c] = t[r][c];
+  double R[3][3], dstr[6], D[6], sig[6], e6[6], sold[6];
+  hughes_winget(L, R, dstr, D, a.inv3_exact != 0);
+  for (int k = 0; k < 6; ++k) { sold[k] = a.stress[6 * i + k]; sig[k] = sold[k]; e6[k] = a.strain[6 * i + k]; }
+  rotate_tensor(R, sig);
+  rotate_tensor(R, e6);
+  for (int k = 0; k < 6; ++k) e6[k] += dstr[k];
+  const MatEntry me = a.mats[a.matidx[i]];
+  NodeMat m;
+  m.type = me.type; m.nu = me.nu; m.E = me.E; m.rho = me.rho; m.sig0 = me.sig0; m.B = me.B; m.C = me.C;
+  m.lam = me.lam; m.mu = me.mu; m.l2m = me.l2m; m.p7 = me.p7; m.p8 = me.p8;
+  double sp[6];
+  sp[0] = sig[0] + (me.l2m * dstr[0] + me.lam * dstr[1] + me.lam * dstr[2]);
+  sp[1] = sig[1] + (me.lam * dstr[0] + me.l2m * dstr[1] + me.lam * dstr[2]);
+  sp[2] = sig[2] + (me.lam * dstr[0] + me.lam * dstr[1] + me.l2m * dstr[2]);
+  sp[3] = sig[3] + me.mu * dstr[3];
+  sp[4] = sig[4] + me.mu * dstr[4];
+  sp[5] = sig[5] + me.mu * dstr[5];
+  double sn[6];
+  double ep = a.eps[i];
+  bool cap = false;
+  if (m.type == MEGA_MAT_ELASTIC) {
+    for (int k = 0; k < 6; ++k) sn[k] = sp[k];
+  } else if (m.type == MEGA_MAT_VONMISES) {
+    von_mises(sp, ep, m, a.maxit, sn, cap);
+  } else if (m.type == MEGA_MAT_VM_RATE) {
+    double dg, ftr;
+    vm_rate(sp, ep, m, a.dt, a.rtol, a.maxit, -1.0, sn, cap, dg, ftr);
+  } else {
+    st |= MEGA_ST_BAD_MATERIAL;
+    for (int k = 0; k < 6; ++k) sn[k] = sp[k];
+  }
+  if (cap) st |= MEGA_ST_NEWTON_CAP;
+  double sinc[6], einc[6];
+  for (int k = 0; k < 6; ++k) {
+    sinc[k] = sn[k] - sold[k];
+    einc[k] = e6[k] - sold[k];  // FINT_PD.F90:509 subtracts the old STRESS (kept as written)
+    a.stress[6 * i + k] = sn[k];
+    a.strain[6 * i + k] = e6[k];
+  }
+  a.eps[i] = ep;
+  double bulk = m.E / (3.0 * (1.0 - 2.0 * m.nu)), shear = m.E / (2.0 * (1.0 + m.nu));
+  if (m.type > 1) estimate_moduli(sinc, einc, shear, bulk);
+  double wv = sqrt(fmax(bulk + 4.0 * shear / 3.0, shear) / m.rho);
+  if (m.type == 3) wv = wv / 0.15;
+  a.wvel[i] = wv;
+  // P = det sigma IF^T ; A = P K^-1
+  double Sg[3][3], P[3][3], A[3][3];
+  v2t(sn, Sg);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) P[r][c] = det * (Sg[r][0] * IF[c][0] + Sg[r][1] * IF[c][1] + Sg[r][2] * IF[c][2]);
+  mm3(P, Ki, A);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) a.amat[9 * i + 3 * r + c] = A[r][c];
+  for (int k = 0; k < 6; ++k)
+    if (!isfinite(sn[k])) st |= MEGA_ST_NONFINITE;
+  if (st) atomicOr(a.status, st);
+}
+
+__global__ void k_pd_force(int32_t n, const double* __restrict__ X, const double* __restrict__ vol,
+                           const int64_t* __restrict__ colptr, const int32_t* __restrict__ trow,
+                           const int64_t* __restrict__ tpos, const double* __restrict__ shp,
+                           const double* __restrict__ amat, const double* __restrict__ svec,
+                           double* __restrict__ fint) {
+  const int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kG;
+  const int q = threadIdx.x & (kG - 1);
+  const unsigned gm = 0xFu << (threadIdx.x & 28);
+  if (k >= n) return;
+  const double xk0 = X[3 * k], xk1 = X[3 * k + 1], xk2 = X[3 * k + 2];
+  double f0 = 0, f1 = 0, f2 = 0;
+  for (int64_t e = colptr[k] + q; e < colptr[k + 1]; e += kG) {
+    const int64_t i = trow[e];
+    const double w = shp[tpos[e]] * vol[i];
+    const double d0 = (X[3 * i] - xk0) * w, d1 = (X[3 * i + 1] - xk1) * w, d2 = (X[3 * i + 2] - xk2) * w;
+    const double* A = amat + 9 * i;
+    f0 -= A[0] * d0 + A[1] * d1 + A[2] * d2;
+    f1 -= A[3] * d0 + A[4] * d1 + A[5] * d2;
+    f2 -= A[6] * d0 + A[7] * d1 + A[8] * d2;
+  }
+#pragma unroll
+  for (int o = 1; o < kG; o <<= 1) {
+    f0 += __shfl_xor_sync(gm, f0, o);
+    f1 += __shfl_xor_sync(gm, f1, o);
+    f2 += __shfl_xor_sync(gm, f2, o);
+  }
+  if (q == 0) {
+    const double* A = amat + 9 * k;
+    const double s0 = svec[3 * k], s1 = svec[3 * k + 1], s2 = svec[3 * k + 2];
+    const double vk = vol[k];
+    fint[3 * k] = vk * (A[0] * s0 + A[1] * s1 + A[2] * s2 + f0);
+    fint[3 * k + 1] = vk * (A[3] * s0 + A[4] * s1 + A[5] * s2 + f1);
+    fint[3 * k + 2] = vk * (A[6] * s0 + A[7] * s1 + A[8] * s2 + f2);
+  }
+}
+
+// ------------------------------------------------------------------ PMB
+// Bond-based force density and velocity-Verlet, one group of 4 lanes per
+// particle.  u_in is read, u_out written (double buffered: the kernel reads
+// every neighbour's displacement of this step while it advances its own).
+struct PmbArgs {
+  int32_t n;
+  const int64_t* rowptr;
+  const int32_t* col;
+  const float* xi;        // 3 per bond: X_j - X_i (float; static)
+  const float* l0;        // |xi| per bond
+  uint32_t* broken;       // bit per bond
+  const double* vol;
+  const double* u_in;
+  double* u_out;
+  double* vel;
+  double* acl;
+  const int8_t* fixed;    // 1: prescribed velocity (kept)
+  double c;               // micromodulus
+  double s_c;             // critical stretch
+  double inv_rho;
+  double dt;
+  unsigned long long* nbroken;
+};
+
+__global__ void __launch_bounds__(256) k_pmb_step(PmbArgs a) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kG;
+  const int q = threadIdx.x & (kG - 1);
+  const unsigned gm = 0xFu << (threadIdx.x & 28);
+  if (i >= a.n) return;
+  const double ui0 = a.u_in[3 * i], ui1 = a.u_in[3 * i + 1], ui2 = a.u_in[3 * i + 2];
+  float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+  unsigned nb = 0;
+  const float c = (float)a.c, sc = (float)a.s_c;
+  for (int64_t p = a.rowptr[i] + q; p < a.rowptr[i + 1]; p += kG) {
+    const float L0 = a.l0[p];
+    if (L0 == 0.f) continue;  // the particle itself
+    const uint32_t word = a.broken[p >> 5], bit = 1u << (p & 31);
+    if (word & bit) continue;
+    const int64_t j = a.col[p];
+    const float d0 = (float)(a.u_in[3 * j] - ui0), d1 = (float)(a.u_in[3 * j + 1] - ui1),
+                d2 = (float)(a.u_in[3 * j + 2] - ui2);
+    const float x0 = a.xi[3 * p], x1 = a.xi[3 * p + 1], x2 = a.xi[3 * p + 2];
+    // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|))
+    const float e0 = x0 + d0, e1 = x1 + d1, e2 = x2 + d2;
+    const float l = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+    const float num = 2.f * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
+    const float s = num / (L0 * (l + L0));
+    if (s > sc) {
+      atomicOr(&a.broken[p >> 5], bit);
+      ++nb;
+      continue;
+    }
+    const float w = c * s * (float)a.vol[j] / l;
+    f0 += w * e0; f1 += w * e1; f2 += w * e2;
+  }
+#pragma unroll
+  for (int o = 1; o < kG; o <<= 1) {
+    f0 += __shfl_xor_sync(gm, f0, o);
+    f1 += __shfl_xor_sync(gm, f1, o);
+    f2 += __shfl_xor_sync(gm, f2, o);
+    nb += __shfl_xor_sync(gm, nb, o);
+  }
+  if (q < 3) {
+    const int64_t m = 3 * i + q;
+    const double f = (double)(q == 0 ? f0 : (q == 1 ? f1 : f2));
+    double v = a.vel[m];
+    const double aold = a.acl[m];
+    double u = a.u_in[m];
+    if (a.fixed && a.fixed[i]) {
+      u = u + a.dt * v;
+    } else {
+      const double anew = f * a.inv_rho;
+      v = v + 0.5 * a.dt * (aold + anew);            // corrector of this step
+      a.acl[m] = anew;
+      u = u + a.dt * v + 0.5 * a.dt * a.dt * anew;    // predictor of the next
+      a.vel[m] = v;
+    }
+    a.u_out[m] = u;
+  }
+  if (q == 0 && nb && a.nbroken) atomicAdd(a.nbroken, (unsigned long long)nb);
+}
+
+__global__ void k_pmb_geometry(int32_t n, const double* __restrict__ X, const int64_t* __restrict__ rowptr,
+                               const int32_t* __restrict__ col, float* __restrict__ xi, float* __restrict__ l0) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kG;
+  const int q = threadIdx.x & (kG - 1);
+  if (i >= n) return;
+  for (int64_t p = rowptr[i] + q; p < rowptr[i + 1]; p += kG) {
+    const int64_t j = col[p];
+    const double a0 = X[3 * j] - X[3 * i], a1 = X[3 * j + 1] - X[3 * i + 1], a2 = X[3 * j + 2] - X[3 * i + 2];
+    xi[3 * p] = (float)a0; xi[3 * p + 1] = (float)a1; xi[3 * p + 2] = (float)a2;
+    l0[p] = (j == i) ? 0.f : (float)sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+  }
+}
+
+// predictor of the first step: u1 = u0 + dt v0 + dt^2/2 a0
+__global__ void k_pmb_first(int64_t n3, double* __restrict__ u, const double* __restrict__ vel,
+                            const double* __restrict__ acl, double dt) {
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (m < n3) u[m] = u[m] + dt * vel[m] + 0.5 * dt * dt * acl[m];
+}
+
+inline unsigned gridg(int64_t n) { return (unsigned)((n * kG + 255) / 256); }
+
+}  // namespace
+
+// launchers used by the C ABI (context.cu / pmb ABI below)
+int pd_shape(cudaStream_t s, int32_t n, const double* X, const double* win, const double* vol, const DevCSR& csr,
+             double* shp, double* ginvk, double* svec, unsigned* status) {
+  k_pd_shape<<<gridg(n), 256, 0, s>>>(n, X, win, vol, csr.rowptr, csr.col, shp, ginvk, svec, status);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+int pd_svec(cudaStream_t s, int32_t n, const double* X, const double* vol, const DevCSR& csr, const double* shp,
+            double* svec) {
+  k_pd_svec<<<(n + 127) / 128, 128, 0, s>>>(n, X, vol, csr.rowptr, csr.col, shp, svec);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+int pd_step(cudaStream_t s, int32_t n, const double* X, const double* xc, const double* du, const double* vol,
+            const DevCSR& csr, const double* shp, const double* ginvk, const double* svec, const uint16_t* matidx,
+            const MatEntry* mats, double* stress, double* strain, double* eps, double* wvel, double* fg,
+            double* amat, double* fint, int linit, const mega_params& p, double dt, unsigned* status) {
+  k_pd_defgrad<<<gridg(n), 256, 0, s>>>(n, X, xc, du, vol, csr.rowptr, csr.col, shp, fg);
+  MEGA_CHECK_LAUNCH();
+  PdStressArgs a{};
+  a.n = n; a.fg = fg; a.ginvk = ginvk; a.matidx = matidx; a.mats = mats; a.stress = stress; a.strain = strain;
+  a.eps = eps; a.wvel = wvel; a.amat = amat; a.linit = linit; a.inv3_exact = p.inv3_exact;
+  a.maxit = p.newton_max_iter; a.rtol = p.newton_rtol; a.dt = dt; a.status = status;
+  k_pd_stress<<<(n + 127) / 128, 128, 0, s>>>(a);
+  MEGA_CHECK_LAUNCH();
+  k_pd_force<<<gridg(n), 256, 0, s>>>(n, X, vol, csr.colptr, csr.trow, csr.tpos, shp, amat, svec, fint);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+// ------------------------------------------------- resident PMB context
+struct PmbCtx {
+  int32_t n = 0;
+  cudaStream_t s = nullptr;
+  DevPool pool;
+  DevCSR csr;
+  double *X = nullptr, *vol = nullptr, *u[2] = {nullptr, nullptr}, *vel = nullptr, *acl = nullptr;
+  float *xi = nullptr, *l0 = nullptr;
+  uint32_t* broken = nullptr;
+  int8_t* fixed = nullptr;
+  unsigned long long* nbroken = nullptr;
+  unsigned* status = nullptr;
+  double c = 0, s_c = 0, rho = 1;
+  int cur = 0;
+  int64_t steps = 0;
+  cudaGraphExec_t g = nullptr;
+  double g_dt = 0;
+  ~PmbCtx() {
+    if (g) cudaGraphExecDestroy(g);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+static PmbArgs pmb_args(PmbCtx* c, double dt) {
+  PmbArgs a{};
+  a.n = c->n; a.rowptr = c->csr.rowptr; a.col = c->csr.col; a.xi = c->xi; a.l0 = c->l0; a.broken = c->broken;
+  a.vol = c->vol; a.u_in = c->u[c->cur]; a.u_out = c->u[1 - c->cur]; a.vel = c->vel; a.acl = c->acl;
+  a.fixed = c->fixed; a.c = c->c; a.s_c = c->s_c; a.inv_rho = 1.0 / c->rho; a.dt = dt; a.nbroken = c->nbroken;
+  return a;
+}
+
+}  // namespace mega
+
+using namespace mega;
+
+extern "C" {
+
+int mega_construct_fint_pd(const mega_params* p, int32_t n, const double* gcoo, const double* gcoo_current,
+                           const double* gwin, const double* gvol, const double* gprop, const int32_t* gmat_type,
+                           double* gstate, double* gstress, double* gstrain, const double* gdinc, const int32_t* gn,
+                           const int32_t* gstart, const int32_t* gstack, int64_t nnz, double* gstack_shp,
+                           double* ginvk, int32_t linit, double dlt, double* fint, double* gmax_wvel,
+                           double* gint_work) {
+  (void)gint_work;
+  if (!p || n <= 0 || !gcoo || !gcoo_current || !gwin || !gvol || !gprop || !gmat_type || !gstate || !gstress ||
+      !gstrain || !gdinc || !gn || !gstart || !gstack || !gstack_shp || !ginvk || !fint || !gmax_wvel)
+    return MEGA_ERR_ARG;
+  cudaStream_t s;
+  MEGA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct SG { cudaStream_t s; ~SG() { cudaStreamDestroy(s); } } sg{s};
+  DevPool pool;
+  // CSR in the caller's row order (1-based GSTART/GSTACK)
+  std::vector<int64_t> rp(n + 1, 0), hpos;
+  for (int32_t i = 0; i < n; ++i) rp[i + 1] = rp[i] + gn[i];
+  const int64_t m = rp[n];
+  std::vector<int32_t> colh(m);
+  hpos.resize(m);
+  for (int32_t i = 0; i < n; ++i)
+    for (int32_t k = 0; k < gn[i]; ++k) {
+      const int64_t q = (int64_t)gstart[i] - 1 + k;
+      if (q < 0 || q >= nnz || gstack[q] < 1 || gstack[q] > n) return MEGA_ERR_ARG;
+      colh[rp[i] + k] = gstack[q] - 1;
+      hpos[rp[i] + k] = q;
+    }
+  DevCSR csr;
+  csr.n = n; csr.nnz = m;
+  MEGA_ALLOC(pool, csr.rowptr, n + 1);
+  MEGA_ALLOC(pool, csr.col, m);
+  MEGA_TRY(cudaMemcpyAsync(csr.rowptr, rp.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(csr.col, colh.data(), sizeof(int32_t) * m, cudaMemcpyHostToDevice, s));
+  int r = build_transpose(s, csr, pool);
+  if (r) return r;
+  const int64_t n3 = 3 * (int64_t)n;
+  double *X, *xc, *w, *v, *du, *shp, *ik, *sv, *sig, *eps6, *ep, *wv, *fg, *am, *fi;
+  uint16_t* midx;
+  MatEntry* dm;
+  unsigned* st;
+  MEGA_ALLOC(pool, X, n3); MEGA_ALLOC(pool, xc, n3); MEGA_ALLOC(pool, w, n3); MEGA_ALLOC(pool, v, n);
+  MEGA_ALLOC(pool, du, n3); MEGA_ALLOC(pool, shp, m); MEGA_ALLOC(pool, ik, 9 * (int64_t)n);
+  MEGA_ALLOC(pool, sv, n3); MEGA_ALLOC(pool, sig, 6 * (int64_t)n); MEGA_ALLOC(pool, eps6, 6 * (int64_t)n);
+  MEGA_ALLOC(pool, ep, n); MEGA_ALLOC(pool, wv, n); MEGA_ALLOC(pool, fg, 18 * (int64_t)n);
+  MEGA_ALLOC(pool, am, 9 * (int64_t)n); MEGA_ALLOC(pool, fi, n3); MEGA_ALLOC(pool, midx, n); MEGA_ALLOC(pool, st, 1);
+  // material table
+  std::vector<MatEntry> ents;
+  std::vector<uint16_t> idx(n);
+  for (int32_t i = 0; i < n; ++i) {
+    const double* pr = gprop + 30 * (size_t)i;
+    int found = -1;
+    for (size_t e = 0; e < ents.size() && found < 0; ++e) {
+      const MatEntry& q = ents[e];
+      if (q.type == gmat_type[i] && q.nu == pr[0] && q.E == pr[1] && q.rho == pr[2] && q.sig0 == pr[3] &&
+          q.B == pr[4] && q.C == pr[5] && q.p7 == pr[6] && q.p8 == pr[7] && q.lam == pr[27] && q.mu == pr[28] &&
+          q.l2m == pr[29])
+        found = (int)e;
+    }
+    if (found < 0) {
+      if (ents.size() >= 1024) return MEGA_ERR_UNSUPPORTED;
+      MatEntry q{};
+      q.type = gmat_type[i]; q.nu = pr[0]; q.E = pr[1]; q.rho = pr[2]; q.sig0 = pr[3]; q.B = pr[4]; q.C = pr[5];
+      q.p7 = pr[6]; q.p8 = pr[7]; q.damp = pr[20]; q.lam = pr[27]; q.mu = pr[28]; q.l2m = pr[29];
+      found = (int)ents.size();
+      ents.push_back(q);
+    }
+    idx[i] = (uint16_t)found;
+  }
+  MEGA_ALLOC(pool, dm, ents.size());
+  std::vector<double> hep(n);
+  for (int32_t i = 0; i < n; ++i) hep[i] = gstate[20 * (size_t)i + 2];
+  MEGA_TRY(cudaMemcpyAsync(X, gcoo, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(xc, gcoo_current, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(w, gwin, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(v, gvol, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(du, gdinc, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(sig, gstress, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(eps6, gstrain, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(ep, hep.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(midx, idx.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemcpyAsync(dm, ents.data(), sizeof(MatEntry) * ents.size(), cudaMemcpyHostToDevice, s));
+  MEGA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
+  if (linit) {
+    r = pd_shape(s, n, X, w, v, csr, shp, ik, sv, st);
+    if (r) return r;
+  } else {
+    std::vector<double> hs(m);
+    for (int64_t k = 0; k < m; ++k) hs[k] = gstack_shp[hpos[k]];
+    MEGA_TRY(cudaMemcpyAsync(shp, hs.data(), sizeof(double) * m, cudaMemcpyHostToDevice, s));
+    MEGA_TRY(cudaMemcpyAsync(ik, ginvk, sizeof(double) * 9 * n, cudaMemcpyHostToDevice, s));
+    MEGA_TRY(cudaStreamSynchronize(s));
+    r = pd_svec(s, n, X, v, csr, shp, sv);
+    if (r) return r;
+  }
+  r = pd_step(s, n, X, xc, du, v, csr, shp, ik, sv, midx, dm, sig, eps6, ep, wv, fg, am, fi, linit, *p, dlt, st);
+  if (r) return r;
+  unsigned hst = 0;
+  MEGA_TRY(cudaMemcpyAsync(fint, fi, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(gstress, sig, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(gstrain, eps6, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(hep.data(), ep, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(gmax_wvel, wv, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(&hst, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  std::vector<double> hs(m);
+  if (linit) {
+    MEGA_TRY(cudaMemcpyAsync(hs.data(), shp, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    MEGA_TRY(cudaMemcpyAsync(ginvk, ik, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, s));
+  }
+  MEGA_TRY(cudaStreamSynchronize(s));
+  if (linit)
+    for (int64_t k = 0; k < m; ++k) gstack_shp[hpos[k]] = hs[k];
+  for (int32_t i = 0; i < n; ++i) gstate[20 * (size_t)i + 2] = hep[i];
+  return (int)hst;
+}
+
+static std::mutex g_pmb_mu;
+static std::set<PmbCtx*> g_pmbs;
+static PmbCtx* get_pmb(int64_t h) {
+  std::lock_guard<std::mutex> lk(g_pmb_mu);
+  PmbCtx* c = reinterpret_cast<PmbCtx*>(h);
+  return g_pmbs.count(c) ? c : nullptr;
+}
+
+int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double* vinit, const int32_t* fixed,
+                  double horizon, double micromodulus, double s_c, double rho, const uint8_t* broken0,
+                  int64_t* handle, int64_t* nbonds) {
+  if (n <= 0 || !coo || !vol || !vinit || !handle || !(horizon > 0) || !(rho > 0)) return MEGA_ERR_ARG;
+  PmbCtx* c = new PmbCtx();
+  auto fail = [&](int code) { delete c; return code; };
+  c->n = n; c->c = micromodulus; c->s_c = s_c; c->rho = rho;
+  if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) return fail(MEGA_ERR_CUDA);
+  const int64_t n3 = 3 * (int64_t)n;
+#define PA(ptr, cnt) do { if (c->pool.alloc(&(ptr), (size_t)(cnt))) return fail(MEGA_ERR_NOMEM); } while (0)
+  double *win = nullptr, *sml = nullptr;
+  PA(c->X, n3); PA(c->vol, n); PA(c->u[0], n3); PA(c->u[1], n3); PA(c->vel, n3); PA(c->acl, n3);
+  PA(c->fixed, n); PA(c->nbroken, 1); PA(c->status, 1);
+  DevPool tmp;
+  if (tmp.alloc(&win, n3) || tmp.alloc(&sml, 6 * (int64_t)n)) return fail(MEGA_ERR_NOMEM);
+  std::vector<double> hw(n3, horizon);
+  std::vector<int8_t> hf(n, 0);
+  if (fixed)
+    for (int32_t i = 0; i < n; ++i) hf[i] = (int8_t)(fixed[i] != 0);
+  cudaMemcpyAsync(c->X, coo, sizeof(double) * n3, cudaMemcpyHostToDevice, c->s);
+  cudaMemcpyAsync(c->vol, vol, sizeof(double) * n, cudaMemcpyHostToDevice, c->s);
+  cudaMemcpyAsync(c->vel, vinit, sizeof(double) * n3, cudaMemcpyHostToDevice, c->s);
+  cudaMemcpyAsync(c->fixed, hf.data(), n, cudaMemcpyHostToDevice, c->s);
+  cudaMemcpyAsync(win, hw.data(), sizeof(double) * n3, cudaMemcpyHostToDevice, c->s);
+  cudaMemsetAsync(sml, 0, sizeof(double) * 6 * n, c->s);
+  cudaMemsetAsync(c->u[0], 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->u[1], 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->acl, 0, sizeof(double) * n3, c->s);
+  cudaMemsetAsync(c->nbroken, 0, sizeof(unsigned long long), c->s);
+  cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->s);
+  const double dmax[3] = {0.0, 0.0, 0.0};
+  // spherical horizon: the ellipsoidal support test of SOFT_SEARCH (SHSUP)
+  int r = bin_search(c->s, n, c->X, win, sml, dmax, 0, 1, c->status, c->csr, nullptr, c->pool, nullptr);
+  if (r) return fail(r);
+  const int64_t m = c->csr.nnz;
+  PA(c->xi, 3 * m); PA(c->l0, m); PA(c->broken, (m + 31) / 32);
+#undef PA
+  k_pmb_geometry<<<gridg(n), 256, 0, c->s>>>(n, c->X, c->csr.rowptr, c->csr.col, c->xi, c->l0);
+  cudaMemsetAsync(c->broken, 0, sizeof(uint32_t) * ((m + 31) / 32), c->s);
+  if (broken0) {
+    std::vector<uint32_t> bits((m + 31) / 32, 0);
+    for (int64_t p = 0; p < m; ++p)
+      if (broken0[p]) bits[p >> 5] |= 1u << (p & 31);
+    cudaMemcpyAsync(c->broken, bits.data(), sizeof(uint32_t) * bits.size(), cudaMemcpyHostToDevice, c->s);
+  }
+  if (cudaStreamSynchronize(c->s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return fail(MEGA_ERR_CUDA);
+  if (nbonds) *nbonds = m;
+  {
+    std::lock_guard<std::mutex> lk(g_pmb_mu);
+    g_pmbs.insert(c);
+  }
+  *handle = reinterpret_cast<int64_t>(c);
+  return 0;
+}
+
+// nsteps of velocity-Verlet: the first step starts from a = 0 like the
+// reference's STATE_INIT (the predictor of step 1 is u = dt v).
+int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms) {
+  PmbCtx* c = get_pmb(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ms) {
+    MEGA_TRY(cudaEventCreate(&e0));
+    MEGA_TRY(cudaEventCreate(&e1));
+    MEGA_TRY(cudaEventRecord(e0, c->s));
+  }
+  if (c->steps == 0) {
+    const int64_t n3 = 3 * (int64_t)c->n;
+    k_pmb_first<<<(unsigned)((n3 + 255) / 256), 256, 0, c->s>>>(n3, c->u[c->cur], c->vel, c->acl, dt);
+    MEGA_CHECK_LAUNCH();
+  }
+  int done = 0;
+  // graph of two steps (the ping-pong buffers return to where they started)
+  if (nsteps >= 2 && (c->g == nullptr || c->g_dt != dt)) {
+    if (c->g) { cudaGraphExecDestroy(c->g); c->g = nullptr; }
+    cudaGraph_t gr;
+    MEGA_TRY(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < 2; ++k) {
+      PmbArgs a = pmb_args(c, dt);
+      k_pmb_step<<<gridg(c->n), 256, 0, c->s>>>(a);
+      c->cur = 1 - c->cur;
+    }
+    cudaError_t e = cudaStreamEndCapture(c->s, &gr);
+    if (e != cudaSuccess) { record_cuda_error(e, "capture", __FILE__, __LINE__); return MEGA_ERR_CUDA; }
+    e = cudaGraphInstantiate(&c->g, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) { record_cuda_error(e, "instantiate", __FILE__, __LINE__); return MEGA_ERR_CUDA; }
+    c->g_dt = dt;
+  }
+  while (nsteps - done >= 2) {
+    MEGA_TRY(cudaGraphLaunch(c->g, c->s));
+    done += 2;
+  }
+  for (; done < nsteps; ++done) {
+    PmbArgs a = pmb_args(c, dt);
+    k_pmb_step<<<gridg(c->n), 256, 0, c->s>>>(a);
+    MEGA_CHECK_LAUNCH();
+    c->cur = 1 - c->cur;
+  }
+  c->steps += nsteps;
+  if (ms) {
+    MEGA_TRY(cudaEventRecord(e1, c->s));
+    MEGA_TRY(cudaEventSynchronize(e1));
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  return 0;
+}
+
+// what = 0: displacement u (3n), 1: velocity (3n), 2: acceleration (3n),
+// 3: broken-bond flags (nnz, as double 0/1).  *nbroken = bonds broken so far.
+int mega_pmb_download(int64_t h, int32_t what, double* dst, int64_t* nbroken) {
+  PmbCtx* c = get_pmb(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  const int64_t n3 = 3 * (int64_t)c->n;
+  if (nbroken) {
+    unsigned long long v = 0;
+    MEGA_TRY(cudaMemcpy(&v, c->nbroken, sizeof(v), cudaMemcpyDeviceToHost));
+    *nbroken = (int64_t)v;
+  }
+  if (!dst) return 0;
+  if (what == 0) MEGA_TRY(cudaMemcpy(dst, c->u[c->cur], sizeof(double) * n3, cudaMemcpyDeviceToHost));
+  else if (what == 1) MEGA_TRY(cudaMemcpy(dst, c->vel, sizeof(double) * n3, cudaMemcpyDeviceToHost));
+  else if (what == 2) MEGA_TRY(cudaMemcpy(dst, c->acl, sizeof(double) * n3, cudaMemcpyDeviceToHost));
+  else if (what == 3) {
+    const int64_t m = c->csr.nnz;
+    std::vector<uint32_t> bits((m + 31) / 32);
+    MEGA_TRY(cudaMemcpy(bits.data(), c->broken, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost));
+    for (int64_t p = 0; p < m; ++p) dst[p] = (bits[p >> 5] >> (p & 31)) & 1u;
+  } else return MEGA_ERR_ARG;
+  return 0;
+}
+
+int mega_pmb_finalize(int64_t h) {
+  PmbCtx* c = get_pmb(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  {
+    std::lock_guard<std::mutex> lk(g_pmb_mu);
+    g_pmbs.erase(c);
+  }
+  delete c;
+  return 0;
+}
+
+}  // extern "C"
