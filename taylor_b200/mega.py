@@ -231,3 +231,66 @@ class Mega:
             self.close()
         except Exception:
             pass
+
+
+def construct_fint_pd(params, coo, coo_current, win, vol, props, mat_type, state, stress, strain, dinc, gn, gstart,
+                      gstack, shp, ginvk, linit, dlt, allow_status=False):
+    """CONSTRUCT_FINT_PD (correspondence peridynamics).  ginvk is (n,3,3)
+    row-major here; returns fint (3N), stress, strain, state, gmax_wvel and
+    (linit) the influence functions and K^-1."""
+    n = len(coo)
+    state, stress, strain = _f64(state).copy(), _f64(stress).copy(), _f64(strain).copy()
+    shp = _f64(shp).copy()
+    ik = np.ascontiguousarray(np.transpose(_f64(ginvk), (0, 2, 1)))  # column-major (3,3,n)
+    fint = np.zeros(3 * n)
+    wv = np.zeros(n)
+    gw = C.c_double(0.0)
+    st = _lib.lib().mega_construct_fint_pd(
+        C.byref(params), n, ptr(_f64(coo)), ptr(_f64(coo_current)), ptr(_f64(win)), ptr(_f64(vol)),
+        ptr(_f64(props)), ptr(_i32(mat_type)), ptr(state), ptr(stress), ptr(strain), ptr(_f64(dinc)), ptr(_i32(gn)),
+        ptr(_i32(gstart)), ptr(_i32(gstack)), len(gstack), ptr(shp), ptr(ik), int(bool(linit)), float(dlt), ptr(fint),
+        ptr(wv), C.byref(gw))
+    check(st, "construct_fint_pd", allow_status)
+    return dict(fint=fint, stress=stress, strain=strain, state=state, gmax_wvel=wv, shp=shp,
+                ginvk=np.transpose(ik, (0, 2, 1)).copy(), status=st)
+
+
+class Pmb:
+    """Bond-based PMB peridynamics, device resident (no reference
+    counterpart).  case from taylor_b200.cases.pd_plate."""
+
+    def __init__(self, case, broken0=None, fixed=None):
+        self.case = case
+        self.n = int(case["n"])
+        h = C.c_int64(0)
+        nb = C.c_int64(0)
+        b0 = None if broken0 is None else np.ascontiguousarray(broken0, dtype=np.uint8)
+        fx = None if fixed is None else _i32(fixed)
+        check(_lib.lib().mega_pmb_init(self.n, ptr(_f64(case["coo"])), ptr(_f64(case["vol"])),
+                                       ptr(_f64(case["vinit"])), ptr(fx), float(case["delta"]), float(case["c"]),
+                                       float(case["s_c"]), float(case["rho"]), ptr(b0), C.byref(h), C.byref(nb)),
+              "pmb_init")
+        self.h, self.nnz = h.value, nb.value
+
+    def step(self, nsteps, dt, timed=False):
+        ms = C.c_float(0.0)
+        check(_lib.lib().mega_pmb_step(self.h, int(nsteps), float(dt), C.byref(ms) if timed else None), "pmb_step")
+        return ms.value
+
+    def download(self, what):
+        m = self.nnz if what == 3 else 3 * self.n
+        out = np.zeros(m)
+        nbk = C.c_int64(0)
+        check(_lib.lib().mega_pmb_download(self.h, int(what), ptr(out), C.byref(nbk)), "pmb_download")
+        return out, nbk.value
+
+    def close(self):
+        if self.h:
+            _lib.lib().mega_pmb_finalize(self.h)
+            self.h = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
