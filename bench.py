@@ -22,9 +22,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -45,6 +43,7 @@ def parse():
     ap.add_argument("--h", type=float, default=0.1e-3, help="lattice spacing (m)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=0, help="CPU baseline sample steps (0 = auto)")
+    ap.add_argument("--modes", default="fp64,mixed", help="order in which the precision modes run")
     return ap.parse_args()
 
 
@@ -76,49 +75,52 @@ def barrier(dist):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (SM clock and throttle reasons)."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled during the timed region: NVML
+    from a background thread every 2 ms (the region can be tens of ms)."""
+    HW_SLOW, SW_POWER, HW_THERMAL, SW_THERMAL = 0x8, 0x4, 0x40, 0x20
 
     def __init__(self):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.p = None
+        import threading
+        self.samples, self.reasons, self.smax = [], 0, None
+        self.stop_evt = threading.Event()
+        self.t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(int(os.environ.get("LOCAL_RANK", 0)))
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_evt.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                self.reasons |= int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def start(self):
-        try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.p = None
+        import threading
+        if self.nv is not None:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
 
     def stop(self):
-        if self.p is None:
-            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["unsampled"])
-        self.p.terminate()
-        try:
-            self.p.wait(5)
-        except Exception:
-            self.p.kill()
-        self.f.flush()
-        dev = os.environ.get("LOCAL_RANK", "0")
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.f.name):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9 or parts[0] != dev:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        os.unlink(self.f.name)
-        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=smax, reasons=sorted(reasons),
-                    samples=len(sm))
+        if self.t is None:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["unsampled"], samples=0)
+        self.stop_evt.set()
+        self.t.join()
+        names = []
+        for bit, nm in ((self.HW_SLOW, "hw_slowdown"), (self.HW_THERMAL, "hw_thermal_slowdown"),
+                        (self.SW_THERMAL, "sw_thermal_slowdown"), (self.SW_POWER, "sw_power_cap")):
+            if self.reasons & bit:
+                names.append(nm)
+        return dict(sm_mhz=statistics.median(self.samples) if self.samples else None, sm_max_mhz=self.smax,
+                    reasons=names, samples=len(self.samples))
 
 
 def measured_peak():
@@ -161,7 +163,7 @@ def run_ours(args, rank, world, dist):
     dt = cases.stable_dt(case, nb["gn"], nb["gstart"], nb["gstack"])
     del nb
     res = {}
-    for mode in ("fp64", "mixed"):
+    for mode in args.modes.split(","):
         m.step(args.warmup, dt, mode=mode)
         barrier(dist)
         clk = Clocks()
