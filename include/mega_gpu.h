@@ -150,6 +150,29 @@ int mega_bin_search(int32_t n, const double* coo, const double* win,
                     int64_t dim_nn_list, int32_t* gmaxn, int32_t* ijk,
                     int64_t* nnz);
 
+/* No counterpart in the reference: the same search as mega_bin_search for
+ * callers that cannot allocate GPU memory when they search (their device
+ * memory belongs to another allocator or arena, or allocation is not allowed
+ * in their loop).  It allocates nothing: inputs and outputs are device
+ * pointers the caller owns -- d_coo (3,n), d_win (3,n), d_sm_len (6,n);
+ * out d_gn (n), d_gstart (n), d_gstack (dim_nn_list) 1-based, d_ijk (3,n)
+ * or NULL -- and every temporary lives in one fixed 48 MiB __device__ array
+ * compiled into the library, held by every GPU that loads it until exit.
+ * Problems that do not fit (about 12 bytes per bin plus 20 per node, e.g.
+ * 1.04 M nodes in 0.32 M bins fit) are rejected with MEGA_ERR_UNSUPPORTED
+ * and a message.  dist_max, *gmaxn and *nnz are host memory; stream is a
+ * cudaStream_t (NULL = default stream); the call returns after the work on
+ * that stream finished.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress), so make it before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race, serialise them.  When nnz
+ * exceeds dim_nn_list, GN/GSTART are written, GSTACK is not, and
+ * MEGA_ST_STACK_OVERFLOW is returned. */
+int mega_bin_search_noalloc(int32_t n, const double* d_coo, const double* d_win,
+                            const double* d_sm_len, const double* dist_max,
+                            int32_t itype_int, int32_t shsup, int32_t* d_gn,
+                            int32_t* d_gstart, int32_t* d_gstack, int64_t dim_nn_list,
+                            int32_t* d_ijk, int32_t* gmaxn, int64_t* nnz, void* stream);
+
 /* RK1 for every node (RK.f90:16-453 via FINT.F90:404-408): shape functions
  * and gradients at X_i for the neighbours in (gn, gstart, gstack).
  *   ebc_nodes (n) logical; out: shp (nnz), dshp (3,nnz). */

@@ -62,6 +62,8 @@ PP = C.POINTER(MegaParams)
 SIGNATURES = {
     "mega_params_default": (None, [PP]),
     "mega_bin_search": (I32, [I32, P, P, P, P, I32, I32, P, P, P, I64, P, P, P]),
+    "mega_bin_search_noalloc": (I32, [I32, P, P, P, P, I32, I32, P, P, P, I64, P, C.POINTER(I32),
+                                      C.POINTER(I64), P]),
     "mega_rk_shapes": (I32, [PP, I32, P, P, P, P, P, P, I64, P, P]),
     "mega_hughes_winget": (I32, [PP, I32, P, P, P, P]),
     "mega_rotate_tensor": (I32, [I32, P, P]),

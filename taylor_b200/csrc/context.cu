@@ -17,6 +17,7 @@ void record_cuda_error(cudaError_t e, const char* what, const char* file, int li
   snprintf(g_err, sizeof(g_err), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
 }
 const char* last_error_text() { return g_err; }
+void record_error_text(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
 
 namespace {
 

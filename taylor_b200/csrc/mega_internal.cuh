@@ -16,6 +16,7 @@ constexpr int kMaxCandidates = 10000;  // INODE(10000), BIN_SEARCH.F90:80
 
 void record_cuda_error(cudaError_t e, const char* what, const char* file, int line);
 const char* last_error_text();
+void record_error_text(const char* msg);
 
 #define MEGA_TRY(x)                                                   \
   do {                                                                \

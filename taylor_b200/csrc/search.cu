@@ -13,6 +13,8 @@
 //   5. count pass -> scan -> fill pass.
 // Every floating-point operation of the test uses __d*_rn intrinsics, so no
 // FMA contraction can change a comparison: the lists are bit-exact.
+#include <algorithm>
+#include <mutex>
 #include "mega_internal.cuh"
 
 namespace mega {
@@ -441,3 +443,204 @@ int build_transpose(cudaStream_t s, DevCSR& csr, DevPool& pool) {
 }
 
 }  // namespace mega
+
+// ===========================================================================
+// Neighbour search that allocates nothing.
+//
+// Some callers cannot call cudaMalloc at the moment they need a neighbour
+// list: a host code whose GPU memory is owned by another allocator (a
+// framework's caching pool, a Fortran code that maps one arena at start-up),
+// a real-time loop where an allocation's implicit synchronisation is not
+// allowed, or a process that has hit its device-memory quota.  This variant
+// takes its inputs and outputs in device memory the caller already owns and
+// takes every temporary (bounding-box partials, bin histogram and offsets,
+// cell-sorted node list, row offsets) from one fixed array that is part of
+// the library image.
+//
+// The array is a file-scope __device__ object of kNoAllocScratchBytes; every
+// GPU that loads the library holds it until the process exits.  Host code
+// cannot use the symbol g_noalloc_scratch as a device address (on the host it
+// names a stand-in object), so the first call on each device looks the
+// address up with cudaGetSymbolAddress while that device is current and
+// caches it; make that first call before any stream capture.  All calls
+// share the array and it keeps the previous call's contents: the counters
+// that must start at zero are cleared on every call.  Calls whose work
+// overlaps on the GPU (other streams, other host threads) race on the array,
+// so serialise them.
+// ===========================================================================
+
+namespace mega {
+
+constexpr int64_t kNoAllocScratchBytes = 48ll << 20;  // 48 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[256] = {nullptr};
+
+// set-up, once per device, with that device current
+int noalloc_scratch_address(void** out) {
+  int dev = 0;
+  MEGA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return MEGA_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    MEGA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    if (!p) return MEGA_ERR_CUDA;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return 0;
+}
+
+// bump allocator over the fixed array (256-byte aligned slices)
+struct Carve {
+  unsigned char* base;
+  int64_t used = 0;
+  template <typename T>
+  T* take(int64_t count) {
+    T* p = (T*)(base + used);
+    used += ((count * (int64_t)sizeof(T) + 255) / 256) * 256;
+    return p;
+  }
+};
+
+int64_t scan_scratch_count(int64_t m) { return (m + kScanBlock - 1) / kScanBlock + 1; }
+
+int scan_counts_into(cudaStream_t s, const int32_t* cnt, int64_t* off, int64_t m, int64_t* bsum) {
+  if (m <= 0) {
+    MEGA_TRY(cudaMemsetAsync(off, 0, sizeof(int64_t), s));
+    return 0;
+  }
+  const int64_t nb = (m + kScanBlock - 1) / kScanBlock;
+  k_scan_block_sums<<<(unsigned)nb, kScanBlock, 0, s>>>(m, cnt, bsum);
+  MEGA_CHECK_LAUNCH();
+  k_scan_bsums<<<1, kScanBlock, 0, s>>>(nb, bsum);
+  MEGA_CHECK_LAUNCH();
+  k_scan_apply<<<(unsigned)nb, kScanBlock, 0, s>>>(m, cnt, bsum, off);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+// 0-based device CSR -> the reference's GN / GSTART / GSTACK (1-based)
+__global__ void k_noalloc_fortran(int32_t n, const int64_t* __restrict__ rowptr, int32_t* __restrict__ gn,
+                                  int32_t* __restrict__ gstart) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  gn[i] = (int32_t)(rowptr[i + 1] - rowptr[i]);
+  gstart[i] = (int32_t)(rowptr[i] + 1);
+}
+__global__ void k_noalloc_plus_one(int64_t m, int32_t* __restrict__ v) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p < m) v[p] += 1;
+}
+
+// scratch bytes for n nodes and nbins bins (each slice rounded to 256 B)
+int64_t noalloc_bytes(int64_t n, int64_t nbins, int nbb) {
+  auto r = [](int64_t b) { return ((b + 255) / 256) * 256; };
+  return r(9 * 8 * (int64_t)nbb) + r(6 * 8) + r(3 * 4) + r(4) + r(4) + r(4 * n) + r(4 * n) + r(4 * n) +
+         r(8 * (n + 1)) + r(4 * nbins) + r(4 * nbins) + r(8 * (nbins + 1)) +
+         r(8 * scan_scratch_count(std::max<int64_t>(nbins, n)));
+}
+
+}  // namespace
+}  // namespace mega
+
+extern "C" int mega_bin_search_noalloc(int32_t n, const double* d_coo, const double* d_win,
+                                       const double* d_sm_len, const double* dist_max, int32_t itype_int,
+                                       int32_t shsup, int32_t* d_gn, int32_t* d_gstart, int32_t* d_gstack,
+                                       int64_t dim_nn_list, int32_t* d_ijk, int32_t* gmaxn, int64_t* nnz,
+                                       void* stream) {
+  using namespace mega;
+  if (n <= 0 || !d_coo || !d_win || !d_sm_len || !dist_max || !d_gn || !d_gstart || !d_gstack || !gmaxn || !nnz)
+    return MEGA_ERR_ARG;
+  const int nbb = 148 * 2;
+  // reject before touching any input when the nodes alone exceed the array
+  if (noalloc_bytes(n, 1, nbb) > kNoAllocScratchBytes) {
+    char msg[256];
+    snprintf(msg, sizeof(msg),
+             "mega_bin_search_noalloc: %d nodes need more than its fixed %lld-byte scratch array", (int)n,
+             (long long)kNoAllocScratchBytes);
+    record_error_text(msg);
+    return MEGA_ERR_UNSUPPORTED;
+  }
+  void* base = nullptr;
+  int r = noalloc_scratch_address(&base);
+  if (r) return r;
+  cudaStream_t s = (cudaStream_t)stream;
+  Carve cv{(unsigned char*)base};
+  double* part = cv.take<double>(9 * nbb);
+  double* geom = cv.take<double>(6);
+  int32_t* dims = cv.take<int32_t>(3);
+  unsigned* status = cv.take<unsigned>(1);
+  int32_t* dmax = cv.take<int32_t>(1);
+  int32_t* cell = cv.take<int32_t>(n);
+  int32_t* sorted = cv.take<int32_t>(n);
+  int32_t* gnw = cv.take<int32_t>(n);
+  int64_t* rowptr = cv.take<int64_t>((int64_t)n + 1);
+  const int64_t head = cv.used;
+  k_bbox_partial<<<nbb, 256, 0, s>>>(n, d_coo, d_win, dist_max[0], dist_max[1], dist_max[2], part);
+  MEGA_CHECK_LAUNCH();
+  k_bbox_final<<<1, 1, 0, s>>>(nbb, part, geom, dims);
+  MEGA_CHECK_LAUNCH();
+  int32_t hd[3];
+  MEGA_TRY(cudaMemcpyAsync(hd, dims, sizeof(hd), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaStreamSynchronize(s));
+  const int64_t nbins = (int64_t)hd[0] * hd[1] * hd[2];
+  if (hd[0] <= 0 || hd[1] <= 0 || hd[2] <= 0 || nbins > INT32_MAX) return MEGA_ERR_UNSUPPORTED;
+  if (noalloc_bytes(n, nbins, nbb) > kNoAllocScratchBytes) {
+    char msg[256];
+    snprintf(msg, sizeof(msg),
+             "mega_bin_search_noalloc: %d nodes in %lld bins need %lld bytes of scratch, the fixed array has %lld",
+             (int)n, (long long)nbins, (long long)noalloc_bytes(n, nbins, nbb), (long long)kNoAllocScratchBytes);
+    record_error_text(msg);
+    return MEGA_ERR_UNSUPPORTED;
+  }
+  cv.used = head;
+  int32_t* cnt = cv.take<int32_t>(nbins);
+  int32_t* fill = cv.take<int32_t>(nbins);
+  int64_t* cstart = cv.take<int64_t>(nbins + 1);
+  int64_t* bsum = cv.take<int64_t>(scan_scratch_count(std::max<int64_t>(nbins, n)));
+  // the array keeps the previous call's contents: clear the counters
+  MEGA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * nbins, s));
+  MEGA_TRY(cudaMemsetAsync(fill, 0, sizeof(int32_t) * nbins, s));
+  MEGA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned), s));
+  MEGA_TRY(cudaMemsetAsync(dmax, 0, sizeof(int32_t), s));
+  k_cell_assign<<<grid_for(n, 256), 256, 0, s>>>(n, d_coo, geom, hd[0], hd[1], hd[2], cell, cnt, d_ijk);
+  MEGA_CHECK_LAUNCH();
+  r = scan_counts_into(s, cnt, cstart, nbins, bsum);
+  if (r) return r;
+  k_cell_scatter<<<grid_for(n, 256), 256, 0, s>>>(n, cell, cstart, fill, sorted);
+  MEGA_CHECK_LAUNCH();
+  k_cell_sort<<<grid_for(nbins, 256), 256, 0, s>>>(nbins, cstart, sorted, status);
+  MEGA_CHECK_LAUNCH();
+  const int mmax = (itype_int == 0) ? 1 : 7;  // BIN_SEARCH.F90:204-208
+  const unsigned gw = grid_for((int64_t)n * 32, 256);
+  k_soft_search<false><<<gw, 256, 0, s>>>(n, d_coo, d_win, d_sm_len, cell, hd[0], hd[1], hd[2], cstart, sorted,
+                                          mmax, shsup, gnw, nullptr, nullptr, dmax, status);
+  MEGA_CHECK_LAUNCH();
+  r = scan_counts_into(s, gnw, rowptr, n, bsum);
+  if (r) return r;
+  int64_t total = 0;
+  unsigned hst = 0;
+  MEGA_TRY(cudaMemcpyAsync(&total, rowptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(gmaxn, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(&hst, status, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaStreamSynchronize(s));
+  *nnz = total;
+  k_noalloc_fortran<<<grid_for(n, 256), 256, 0, s>>>(n, rowptr, d_gn, d_gstart);
+  MEGA_CHECK_LAUNCH();
+  if (total > dim_nn_list) {  // the caller's GSTACK is too small: lists not written
+    MEGA_TRY(cudaStreamSynchronize(s));
+    return (int)(hst | MEGA_ST_STACK_OVERFLOW);
+  }
+  k_soft_search<true><<<gw, 256, 0, s>>>(n, d_coo, d_win, d_sm_len, cell, hd[0], hd[1], hd[2], cstart, sorted,
+                                         mmax, shsup, gnw, rowptr, d_gstack, dmax, status);
+  MEGA_CHECK_LAUNCH();
+  k_noalloc_plus_one<<<grid_for(total, 256), 256, 0, s>>>(total, d_gstack);
+  MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaStreamSynchronize(s));
+  return (int)hst;
+}
