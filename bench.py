@@ -44,6 +44,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=0, help="CPU baseline sample steps (0 = auto)")
     ap.add_argument("--modes", default="fp64,mixed", help="order in which the precision modes run")
+    ap.add_argument("--full-steps", type=int, default=2000,
+                    help="steps of the accuracy runs (FP64 vs mixed end states); 0 skips them")
+    ap.add_argument("--rate-h", type=float, default=0.08e-3,
+                    help="lattice spacing of the rate-dependent bar of the learned-start runs; 0 skips them")
+    ap.add_argument("--rate-steps", type=int, default=2000, help="steps of the rate-dependent runs")
     return ap.parse_args()
 
 
@@ -197,9 +202,113 @@ def run_ours(args, rank, world, dist):
     h2d = sum(np.asarray(case[k]).nbytes for k in ("coo", "win", "vol", "mass", "ebc", "vinit", "props", "mat_type",
                                                      "body_id", "sm_len"))
     peak, peak_kind = measured_peak()
+    acc = accuracy(case, p, dt, args.full_steps) if args.full_steps > 0 else None
+    lrn = learned_runs(args, rank) if args.rate_h > 0 else None
     out = dict(case=case, n=n, nnz=nnz, kmean=kmean, dt=dt, res=res, step0_s=step0_s, e2e_s=e2e_s, h2d=h2d,
-               d2h=d2h, peak=peak, peak_kind=peak_kind, scalars=s, dev_bytes=dev_bytes)
+               d2h=d2h, peak=peak, peak_kind=peak_kind, scalars=s, dev_bytes=dev_bytes, accuracy=acc, learned=lrn)
     return out
+
+
+STATE_FIELDS = (1, 2, 3, 4, 6, 7, 8, 9)  # dsp, dsp_tot, vel, acl, fext, stress, strain, eps
+
+
+def accuracy(case, p, dt, steps):
+    """FP64 and mixed runs of `steps` steps from impact: end-state length,
+    mushroom radius and peak plastic strain, and (from the FP64 end state)
+    the relative L2 difference of one step's nodal forces."""
+    from taylor_b200 import _lib, cases, mega
+    m = mega.Mega(case, p)
+    m.search_and_shapes()
+    m.step(steps, dt, mode="fp64")
+    ref = cases.bar_metrics(case, m.download(_lib.F_COO_CURRENT), m.download(_lib.F_EPS))
+    state = {f: m.download(f) for f in STATE_FIELDS}
+    m.step(1, dt, mode="fp64")
+    f64 = m.download(_lib.F_FINT)
+    for f, v in state.items():
+        m.upload(f, v)
+    m.step(1, dt, mode="mixed")
+    f32 = m.download(_lib.F_FINT)
+    m.close()
+    del state
+    q = mega.Mega(case, p)
+    q.search_and_shapes()
+    q.step(steps, dt, mode="mixed")
+    mix = cases.bar_metrics(case, q.download(_lib.F_COO_CURRENT), q.download(_lib.F_EPS))
+    q.close()
+    rel = {k: abs(mix[k] - ref[k]) / abs(ref[k]) for k in ref}
+    return dict(steps=steps, fp64=ref, mixed=mix, mixed_rel_err=rel,
+                force_rel_l2_one_step=float(np.linalg.norm(f32 - f64) / np.linalg.norm(f64)))
+
+
+RATE_LAW = (90e6, 292e6, 0.31, 0.025, 1.0)  # A, B, n, C, epsdot0 of the power-law rate-dependent hardening
+
+
+def learned_runs(args, rank):
+    """Rate-dependent bar: plain FP64, plain mixed and mixed + learned start
+    from impact for the same steps.  The learned context logs return-mapping
+    samples during the first quarter (plain Newton), trains the network on
+    them on the device, then continues with the learned start; the other
+    two run plain throughout.  Times cover the last three quarters."""
+    from taylor_b200 import _lib, cases, mega
+    case = cases.taylor_bar(h=args.rate_h, rate_law=RATE_LAW, seed=7 + rank)
+    n = case["n"]
+    p = _lib.params(**cases.param_kwargs(case, newton_max_iter=60, newton_rtol=1e-10))
+    total = args.rate_steps
+    first = total // 4
+    rest = total - first
+    runs = {}
+    dt = None
+    for name, mode, learn in (("fp64", "fp64", False), ("mixed", "mixed", False), ("mixed_learned", "mixed", True)):
+        m = mega.Mega(case, p)
+        m.search_and_shapes()
+        if dt is None:
+            nb = m.search_and_shapes(download=True)
+            dt = cases.stable_dt(case, nb["gn"], nb["gstart"], nb["gstack"])
+            del nb
+        info = {}
+        if learn:
+            m.log_rate_samples(cap=10_000_000, stride=4, seed=3)
+        m.step(first, dt, mode=mode)
+        if learn:
+            t0 = time.perf_counter()
+            th, loss = m.train_surrogate(mega.mlp_init(5), epochs=6, batch=8192, lr=2e-3, seed=9)
+            info.update(train_s=time.perf_counter() - t0, samples=int(min(10_000_000, _held_count(m))),
+                        loss_first_epoch=float(loss[0]), loss_last_epoch=float(loss[-1]))
+            m.log_rate_samples(0)
+            del th
+        s0 = m.scalars()
+        clk = Clocks()
+        clk.start()
+        ms = m.step_timed(rest, dt, mode=mode, learned=learn)
+        info["clocks"] = clk.stop()
+        s1 = m.scalars()
+        it = s1["newton_iters_total"] - s0["newton_iters_total"]
+        pl = s1["plastic_nodes_total"] - s0["plastic_nodes_total"]
+        kt = m.kernel_times(3, dt, mode=mode, learned=learn)
+        end = cases.bar_metrics(case, m.download(_lib.F_COO_CURRENT), m.download(_lib.F_EPS))
+        m.close()
+        info.update(ms_per_step=ms / rest, node_steps_per_s=n * rest / (ms / 1e3), newton_iters=int(it),
+                    plastic_updates=int(pl), iters_per_plastic_update=it / max(pl, 1),
+                    stress_kernel_ms=float(kt[1]), end_state=end)
+        runs[name] = info
+    ref = runs["fp64"]["end_state"]
+    for name in ("mixed", "mixed_learned"):
+        e = runs[name]["end_state"]
+        runs[name]["rel_err_vs_fp64"] = {k: abs(e[k] - ref[k]) / abs(ref[k]) for k in ref}
+    return dict(workload=f"rate-dependent taylor_bar h={args.rate_h*1e3:.3g}mm", nodes=n, dt=dt, steps=total,
+                timed_steps=rest, rate_law=dict(A=RATE_LAW[0], B=RATE_LAW[1], n=RATE_LAW[2], C=RATE_LAW[3],
+                                                epsdot0=RATE_LAW[4]), newton_rtol=1e-10, runs=runs,
+                mixed_learned_over_fp64=runs["fp64"]["ms_per_step"] / runs["mixed_learned"]["ms_per_step"],
+                iteration_reduction=1.0 - runs["mixed_learned"]["iters_per_plastic_update"]
+                / runs["mixed"]["iters_per_plastic_update"])
+
+
+def _held_count(m):
+    import ctypes as C
+    from taylor_b200 import _lib
+    k = C.c_int64(0)
+    _lib.check(_lib.lib().mega_rate_samples(m.h, None, 0, C.byref(k)), "rate_samples")
+    return k.value
 
 
 def cpu_baseline(case, steps, nthreads):
@@ -246,7 +355,8 @@ def main():
             dist.destroy_process_group()
         return
     n, nnz, K = r["n"], r["nnz"], args.steps
-    mix, f64 = r["res"]["mixed"], r["res"]["fp64"]
+    mix = r["res"].get("mixed") or r["res"]["fp64"]
+    f64 = r["res"].get("fp64") or mix
     value = world * n * K / (mix["ms"] / 1e3)
     fp64_value = world * n * K / (f64["ms"] / 1e3)
     # roofline of the dominant kernel (mixed path, the headline)
@@ -282,7 +392,7 @@ def main():
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=K, warmup=args.warmup,
         ms_per_step=mix["ms"] / K, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32+f64",
-        data="synthetic (seeded jittered lattice, config 2 geometry and material)",
+        data="synthetic (seeded jittered lattice of the 0.1 mm copper bar, random-free material data)",
         config=dict(workload=f"taylor_bar_1M h={args.h*1e3:.3g}mm", nodes=n, nnz=nnz, mean_neighbours=nnz / n,
                     dt=r["dt"], parallelism=f"replicas{world}", l2="inputs larger than L2 (no flush needed)",
                     step0_search_shapes_s=r["step0_s"], device_bytes=r["dev_bytes"]),
@@ -291,7 +401,8 @@ def main():
         e2e=dict(value=e2e_val, unit=UNIT, h2d_bytes_per_step=r["h2d"] / K, d2h_bytes_per_step=r["d2h"] / K,
                  note="model upload + step 0 + K steps with per-step scalar readback + end-state download"),
         gpu_launches=mix["launches"], clocks=mix["clocks"], clocks_fp64=f64["clocks"],
-        newton_iters_last_step=r["scalars"]["newton_iters"], plastic_nodes_last_step=r["scalars"]["plastic_nodes"])
+        newton_iters_last_step=r["scalars"]["newton_iters"], plastic_nodes_last_step=r["scalars"]["plastic_nodes"],
+        accuracy=r["accuracy"], learned=r["learned"])
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

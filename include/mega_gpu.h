@@ -104,6 +104,8 @@ typedef struct mega_scalars_t {
   int64_t steps;          /* explicit steps taken                             */
   int64_t newton_iters;   /* total return-mapping Newton iterations, last step*/
   int64_t plastic_nodes;  /* nodes that returned plastically, last step       */
+  int64_t newton_iters_total;  /* Newton iterations over all resident steps    */
+  int64_t plastic_nodes_total; /* plastic node updates over all resident steps */
 } mega_scalars_t;
 
 /* Hot-path switches of the reference's CONTROL module (CONTROL.F90:27-95)
@@ -286,6 +288,52 @@ int64_t mega_device_bytes(int64_t h);
 int64_t mega_kernel_launches(int64_t h);
 
 /* ======================================================================== */
+/* Surrogate start of the rate-dependent return mapping (material 7; no    */
+/* reference counterpart).  A 4 -> 64 -> 64 -> 1 tanh perceptron predicts   */
+/* the converged plastic multiplier as a fraction y of the perfectly        */
+/* plastic estimate f_trial / (2 mu); Newton then starts at                 */
+/* clamp(y, 0.02, 1) f_trial / (2 mu) instead of at the estimate itself,    */
+/* and converges to the same tolerance.  Parameters theta (4545 floats)     */
+/* packed [W1 (64x4), b1 (64), W2 (64x64), b2 (64), W3 (64), b3], weights   */
+/* row-major (output, input).  Features of a plastic node, with q the      */
+/* trial deviatoric norm, sy0 = A + B eps^n, f = q - sqrt(2/3) sy0:         */
+/*   x0 = ln(f / (sqrt(2/3) sy0)), x1 = eps^n,                              */
+/*   x2 = ln(max(sqrt(2/3) f / (2 mu dt), epsdot0) / epsdot0) / 10,          */
+/*   x3 = 1e3 sqrt(2/3) sy0 / (2 mu).                                       */
+/* ======================================================================== */
+
+/* Parameter count for the given hidden width (only 64 is built). */
+int mega_mlp_nparams(int32_t hidden);
+/* Mean-squared-error loss 0.5 mean (y - t)^2 over nb samples x (4,nb),
+ * t (nb) and its gradient (nparams floats) in FP32. */
+int mega_mlp_grad(int32_t hidden, const float* theta, int64_t nb, const float* x,
+                  const float* t, float* grad, float* loss);
+/* y (n) = network(x (4,n)); tensor_cores != 0 evaluates it as the learned
+ * stress kernel does (bf16 W2 on the tensor cores, fp32 accumulation). */
+int mega_mlp_eval(int32_t hidden, const float* theta, int64_t n, const float* x,
+                  float* y, int32_t tensor_cores);
+/* Mini-batch Adam (beta 0.9 / 0.999, eps 1e-8) on the device; theta in/out,
+ * loss_per_epoch (epochs) out (may be NULL). */
+int mega_mlp_train(int32_t hidden, float* theta, int64_t ns, const float* x,
+                   const float* t, int32_t epochs, int32_t batch, float lr,
+                   uint64_t seed, float* loss_per_epoch);
+/* Install theta (host) in the context; steps whose mode has
+ * MEGA_FLAG_LEARNED_GUESS then use it.  theta = NULL removes it. */
+int mega_set_surrogate(int64_t h, int32_t hidden, const float* theta);
+/* Log (features, y) of plastic rate-dependent nodes solved by plain Newton
+ * into a device buffer of cap samples: a node is sampled when a hash of its
+ * index and trial stress is 0 mod stride.  cap = 0 stops logging and frees
+ * the buffer. */
+int mega_log_rate_samples(int64_t h, int64_t cap, int32_t stride, uint32_t seed);
+/* Copy up to cap logged samples, 5 floats each (x0..x3, y), to out (host,
+ * may be NULL); *count = samples copied (or held, when out is NULL). */
+int mega_rate_samples(int64_t h, float* out, int64_t cap, int64_t* count);
+/* Train on the logged samples without leaving the device, starting from
+ * theta (host, in/out), then install the result as by mega_set_surrogate. */
+int mega_train_surrogate(int64_t h, float* theta, int32_t epochs, int32_t batch,
+                         float lr, uint64_t seed, float* loss_per_epoch);
+
+/* ======================================================================== */
 /* Bond-based peridynamics (no reference counterpart: the reference's        */
 /* FINT_PD is correspondence-based).  Prototype microelastic brittle model  */
 /* (Silling & Askari 2005) with bond breaking, resident on the device.      */
@@ -296,10 +344,12 @@ int64_t mega_kernel_launches(int64_t h);
  * c; critical stretch s_c; density rho; broken0 (nnz) initial broken flags
  * per neighbour-list entry (may be NULL; the list is the SOFT_SEARCH
  * ellipsoidal-support list with window = horizon, as mega_bin_search(...,
- * shsup = 1) returns it).  *nbonds = list entries (self included). */
+ * shsup = 1) returns it).  mode: MEGA_MODE_MIXED = float bond arithmetic,
+ * MEGA_MODE_FP64 = double.  *nbonds = list entries (self included). */
 int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double* vinit,
                   const int32_t* fixed, double horizon, double micromodulus, double s_c,
-                  double rho, const uint8_t* broken0, int64_t* handle, int64_t* nbonds);
+                  double rho, const uint8_t* broken0, int32_t mode, int64_t* handle,
+                  int64_t* nbonds);
 /* nsteps of velocity-Verlet (float force, double positions); *ms device time
  * of the call when ms is not NULL. */
 int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms);

@@ -51,6 +51,7 @@ class MegaScalars(C.Structure):
         ("time", C.c_double), ("int_energy", C.c_double), ("kin_energy", C.c_double),
         ("ext_energy", C.c_double), ("total_force", C.c_double * 6), ("steps", C.c_int64),
         ("newton_iters", C.c_int64), ("plastic_nodes", C.c_int64),
+        ("newton_iters_total", C.c_int64), ("plastic_nodes_total", C.c_int64),
     ]
 
 
@@ -82,10 +83,18 @@ SIGNATURES = {
     "mega_get_scalars": (I32, [I64, C.POINTER(MegaScalars)]),
     "mega_device_bytes": (I64, [I64]),
     "mega_kernel_launches": (I64, [I64]),
-    "mega_pmb_init": (I32, [I32, P, P, P, P, D, D, D, D, P, C.POINTER(I64), C.POINTER(I64)]),
+    "mega_pmb_init": (I32, [I32, P, P, P, P, D, D, D, D, P, I32, C.POINTER(I64), C.POINTER(I64)]),
     "mega_pmb_step": (I32, [I64, I32, D, C.POINTER(F32)]),
     "mega_pmb_download": (I32, [I64, I32, P, C.POINTER(I64)]),
     "mega_pmb_finalize": (I32, [I64]),
+    "mega_mlp_nparams": (I32, [I32]),
+    "mega_mlp_grad": (I32, [I32, P, I64, P, P, P, P]),
+    "mega_mlp_eval": (I32, [I32, P, I64, P, P, I32]),
+    "mega_mlp_train": (I32, [I32, P, I64, P, P, I32, I32, F32, C.c_uint64, P]),
+    "mega_set_surrogate": (I32, [I64, I32, P]),
+    "mega_log_rate_samples": (I32, [I64, I64, I32, C.c_uint32]),
+    "mega_rate_samples": (I32, [I64, P, I64, C.POINTER(I64)]),
+    "mega_train_surrogate": (I32, [I64, P, I32, I32, F32, C.c_uint64, P]),
     "mega_status_string": (C.c_char_p, [I32]),
     "mega_gpu_finalize": (I32, [I64]),
 }

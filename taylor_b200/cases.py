@@ -99,6 +99,17 @@ def taylor_bar(h=0.4e-3, R=3.2e-3, L=32.4e-3, jitter=0.05, seed=1, v0=227.0, E=1
         layer=k, R=R, L=L, v0=v0)
 
 
+def bar_metrics(case, coo_cur, eps):
+    """End-state measures of a Taylor test: bar length (z extent), mushroom
+    radius (largest radius of the wall layer) and peak equivalent plastic
+    strain."""
+    x = np.asarray(coo_cur).reshape(-1, 3)
+    w = case["wall"]
+    return dict(length=float(x[:, 2].max() - x[:, 2].min()),
+                radius=float(np.sqrt(x[w, 0] ** 2 + x[w, 1] ** 2).max()),
+                peak_eps=float(np.max(eps)))
+
+
 def param_kwargs(case, **over):
     """mega_params values for a case (Control.dat defaults: RK 1/3/0, QL 1
     0.001, DNI, Lagrangian finite strain, box support)."""
@@ -109,18 +120,27 @@ def param_kwargs(case, **over):
     return kw
 
 
-def stable_dt(case, gn, gstart, gstack, cfl=0.5):
+def stable_dt(case, gn, gstart, gstack, cfl=0.5, chunk=1 << 22):
     """Fixed step 0.5 * min_i(d_min,i / c_i) (the CFL rule of FINT.F90:
     1280-1311, commented out in the reference, evaluated once): d_min = the
-    nearest neighbour distance, c = sqrt(max(K + 4G/3, G) / rho)."""
+    nearest neighbour distance, c = sqrt(max(K + 4G/3, G) / rho).  Evaluated
+    over list chunks of `chunk` entries to bound host memory."""
     coo = case["coo"]
     n = case["n"]
-    rows = np.repeat(np.arange(n), gn)
-    cols = gstack - 1
-    d = np.linalg.norm(coo[cols] - coo[rows], axis=1)
-    d[cols == rows] = np.inf
+    gn = np.asarray(gn, np.int64)
+    ptr = np.zeros(n + 1, np.int64)
+    np.cumsum(gn, out=ptr[1:])
     dmin = np.full(n, np.inf)
-    np.minimum.at(dmin, rows, d)
+    r0 = 0
+    while r0 < n:
+        r1 = int(np.searchsorted(ptr, ptr[r0] + chunk, side="right")) - 1
+        r1 = min(n, max(r1, r0 + 1))
+        rows = np.repeat(np.arange(r0, r1), gn[r0:r1])
+        cols = np.asarray(gstack[ptr[r0]:ptr[r1]], np.int64) - 1
+        d = np.linalg.norm(coo[cols] - coo[rows], axis=1)
+        d[cols == rows] = np.inf
+        np.minimum.at(dmin, rows, d)
+        r0 = r1
     p = case["props"]
     E, nu, rho = p[:, 1], p[:, 0], p[:, 2]
     K = E / (3.0 * (1.0 - 2.0 * nu))

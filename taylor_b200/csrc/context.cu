@@ -9,6 +9,7 @@
 #include <set>
 #include <vector>
 #include "mega_internal.cuh"
+#include "tiled.cuh"
 
 namespace mega {
 
@@ -21,10 +22,6 @@ void record_error_text(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", m
 
 namespace {
 
-__global__ void k_fill_f32(int64_t m, const double* __restrict__ a, float* __restrict__ b) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < m) b[i] = (float)a[i];
-}
 __global__ void k_gather_pos(int64_t m, const int64_t* __restrict__ pos, const double* __restrict__ src,
                              double* __restrict__ dst) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -97,6 +94,56 @@ __global__ void k_constitution(int32_t n, const double* __restrict__ spred, cons
   if (iters) iters[i] = it;
 }
 
+// renumbering: new node r is old node perm[r]
+__global__ void k_iperm(int32_t n, const int32_t* __restrict__ perm, int32_t* __restrict__ iperm) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r < n) iperm[perm[r]] = (int32_t)r;
+}
+// dst[r*w + k] = src[perm[r]*w + k]  (gather = old -> new), element size es bytes
+__global__ void k_perm_gather(int32_t n, int w, int es, const int32_t* __restrict__ perm,
+                              const unsigned char* __restrict__ src, unsigned char* __restrict__ dst) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)n * w) return;
+  const int64_t r = t / w, k = t - r * w;
+  const unsigned char* a = src + ((int64_t)perm[r] * w + k) * es;
+  unsigned char* b = dst + t * es;
+  for (int q = 0; q < es; ++q) b[q] = a[q];
+}
+__global__ void k_newrow_len(int32_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ rowptr0,
+                             int32_t* __restrict__ len) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r < n) len[r] = (int32_t)(rowptr0[perm[r] + 1] - rowptr0[perm[r]]);
+}
+// warp per new row: copy the old row (same entry order), columns renumbered
+__global__ void k_permute_rows(int32_t n, const int32_t* __restrict__ perm, const int32_t* __restrict__ iperm,
+                               const int64_t* __restrict__ rowptr0, const int32_t* __restrict__ col0,
+                               const double* __restrict__ v0, const double* __restrict__ v1,
+                               const double* __restrict__ v2, const double* __restrict__ v3,
+                               const int64_t* __restrict__ rowptr1, int32_t* __restrict__ col1,
+                               double* __restrict__ w0, double* __restrict__ w1, double* __restrict__ w2,
+                               double* __restrict__ w3) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const int64_t a0 = rowptr0[perm[r]], len = rowptr0[perm[r] + 1] - a0, b0 = rowptr1[r];
+  for (int64_t k = lane; k < len; k += 32) {
+    col1[b0 + k] = iperm[col0[a0 + k]];
+    w0[b0 + k] = v0[a0 + k]; w1[b0 + k] = v1[a0 + k]; w2[b0 + k] = v2[a0 + k]; w3[b0 + k] = v3[a0 + k];
+  }
+}
+// row sums of the float-rounded packed gradients (the mixed path's sum_J g)
+__global__ void k_rowsum_pk32(int32_t n, const int64_t* __restrict__ rowptr, const float4* __restrict__ pk,
+                              double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int64_t p = rowptr[i]; p < rowptr[i + 1]; ++p) {
+    const float4 v = pk[p];
+    a += (double)v.x; b += (double)v.y; c += (double)v.z;
+  }
+  out[3 * i] = a; out[3 * i + 1] = b; out[3 * i + 2] = c;
+}
+
 inline unsigned grid_for(int64_t work, int block) { return (unsigned)((work + block - 1) / block); }
 
 }  // namespace
@@ -117,15 +164,14 @@ struct Ctx {
   uint16_t* matidx = nullptr;
   MatEntry* mats = nullptr;
   bool has_body = false;
-  // neighbours and shapes
+  // neighbours and shapes, in the renumbered (bin-cell) node order
   DevCSR csr;
-  DevCSR* dcsr = nullptr;  // device copy read by the force kernel
   bool searched = false;
-  double *shp = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *sdphi = nullptr;
-  double *tgx = nullptr, *tgy = nullptr, *tgz = nullptr, *tshp = nullptr;
-  float *fgx = nullptr, *fgy = nullptr, *fgz = nullptr, *ftgx = nullptr, *ftgy = nullptr, *ftgz = nullptr;
-  double* sdphi32 = nullptr;
-  bool mixed_ready = false;
+  int32_t* perm = nullptr;   // new node r = original node perm[r]
+  int32_t* iperm = nullptr;  // original node i = new node iperm[i]
+  TileSet rt, ct;            // row tiles (deformation gradient), column tiles (force)
+  double *shp = nullptr, *sdphi = nullptr, *sdphi32 = nullptr, *tshp = nullptr;
+  void *pk64 = nullptr, *tpk64 = nullptr, *pk32 = nullptr, *tpk32 = nullptr;
   // state
   double *dsp = nullptr, *dsp_tot = nullptr, *dsp_tot_phy = nullptr, *vel = nullptr, *acl = nullptr;
   double *fint = nullptr, *fext = nullptr, *prforce = nullptr, *stress = nullptr, *strain = nullptr;
@@ -138,6 +184,16 @@ struct Ctx {
   double time = 0.0;
   int64_t steps = 0;
   int64_t launches = 0;
+  // surrogate of the rate-dependent return mapping and its sample log
+  DevPool mlppool;
+  float* mlp_theta = nullptr;  // fp32 parameters (training copy)
+  uint16_t* mlp_w2 = nullptr;  // bf16 W2 for the tensor cores
+  float* mlp_small = nullptr;
+  bool mlp_on = false;
+  float* log_buf = nullptr;
+  unsigned long long* log_count = nullptr;
+  int64_t log_cap = 0;
+  uint32_t log_stride = 1, log_seed = 0;
   // graph cache
   cudaGraphExec_t gexec = nullptr;
   int g_mode = -1;
@@ -167,26 +223,7 @@ static int read_status(Ctx* c, bool reset) {
 }
 
 static int ensure_mixed(Ctx* c) {
-  if (c->mixed_ready) return 0;
-  const int64_t nnz = c->csr.nnz;
-  MEGA_ALLOC(c->mixpool, c->fgx, nnz);
-  MEGA_ALLOC(c->mixpool, c->fgy, nnz);
-  MEGA_ALLOC(c->mixpool, c->fgz, nnz);
-  MEGA_ALLOC(c->mixpool, c->ftgx, nnz);
-  MEGA_ALLOC(c->mixpool, c->ftgy, nnz);
-  MEGA_ALLOC(c->mixpool, c->ftgz, nnz);
-  MEGA_ALLOC(c->mixpool, c->sdphi32, 3 * (int64_t)c->n);
-  const unsigned g = grid_for(nnz, 256);
-  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->gx, c->fgx);
-  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->gy, c->fgy);
-  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->gz, c->fgz);
-  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->tgx, c->ftgx);
-  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->tgy, c->ftgy);
-  k_fill_f32<<<g, 256, 0, c->s>>>(nnz, c->tgz, c->ftgz);
-  k_rowsum3<float><<<grid_for(c->n, 256), 256, 0, c->s>>>(c->n, c->csr.rowptr, c->fgx, c->fgy, c->fgz, c->sdphi32);
-  MEGA_CHECK_LAUNCH();
-  MEGA_TRY(cudaStreamSynchronize(c->s));
-  c->mixed_ready = true;
+  (void)c;  // the float records are packed at search time
   return 0;
 }
 
@@ -198,45 +235,40 @@ static StressArgs stress_args(Ctx* c, double dt, int mode) {
   a.grav[0] = c->p.gravity[0]; a.grav[1] = c->p.gravity[1]; a.grav[2] = c->p.gravity[2];
   a.has_body = c->has_body; a.inv3_exact = c->p.inv3_exact; a.finite_strain = c->p.finite_strain;
   a.maxit = c->p.newton_max_iter; a.rtol = c->p.newton_rtol; a.dt = dt; a.iters = c->iters;
-  a.mlp_guess = nullptr; a.rate_samples = nullptr; a.acc = c->acc; a.status = c->status;
-  (void)mode;
+  a.acc = c->acc; a.status = c->status;
+  if ((mode & MEGA_FLAG_LEARNED_GUESS) && c->mlp_on) { a.mlp_w2 = c->mlp_w2; a.mlp_small = c->mlp_small; }
+  if (c->log_cap > 0) {
+    a.log_buf = c->log_buf; a.log_count = c->log_count; a.log_cap = c->log_cap;
+    a.log_stride = c->log_stride; a.log_seed = c->log_seed;
+  }
   return a;
 }
 
-static ForceArgs force_args(Ctx* c, double dt, int mode, int predict) {
+static TiledForceArgs force_args(Ctx* c, double dt, int mode, int predict) {
   const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
-  ForceArgs f{};
-  f.n = c->n; f.csr = nullptr;
-  f.tgx = mixed ? (const void*)c->ftgx : (const void*)c->tgx;
-  f.tgy = mixed ? (const void*)c->ftgy : (const void*)c->tgy;
-  f.tgz = mixed ? (const void*)c->ftgz : (const void*)c->tgz;
-  f.tshp = c->tshp; f.tmat = c->tmat; f.has_body = c->has_body; f.integrate = 1; f.predict = predict;
+  TiledForceArgs f{};
+  f.n = c->n; f.R = c->ct.R; f.ntiles = c->ct.ntiles; f.jmax = c->ct.jmax; f.maxcnt = c->ct.maxcnt;
+  f.jset = c->ct.jset; f.jcnt = c->ct.jcnt; f.colptr = c->csr.colptr;
+  f.pk = mixed ? c->tpk32 : c->tpk64;
+  f.tshp = c->tshp; f.tmat = c->tmat; f.has_body = c->has_body; f.predict = predict;
   f.ebc = c->ebc; f.mass = c->mass; f.matidx = c->matidx; f.mats = c->mats; f.body_id = c->body_id;
   f.fint = c->fint; f.fext = c->fext; f.vel = c->vel; f.acl = c->acl; f.dsp = c->dsp; f.dsp_tot = c->dsp_tot;
   f.prforce = c->prforce; f.dt = dt; f.acc = c->acc; f.status = c->status;
   return f;
 }
 
-// The force kernel reads the CSC through a device-visible copy of DevCSR.
-static DevCSR* dev_csr_copy(Ctx* c) { return c->dcsr; }
-
 static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) {
   const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
   const bool interp = (mode & MEGA_FLAG_INTERP_EACH_STEP) != 0;
   if (ev) MEGA_TRY(cudaEventRecord(ev[0], c->s));
-  int r = launch_defgrad(c->s, mixed, interp, c->n, c->csr, mixed ? (const void*)c->fgx : (const void*)c->gx,
-                         mixed ? (const void*)c->fgy : (const void*)c->gy,
-                         mixed ? (const void*)c->fgz : (const void*)c->gz, c->dsp, c->dsp_tot,
-                         mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc);
+  int r = launch_defgrad_tiled(c->s, mixed, interp, c->n, c->rt, c->csr.rowptr, mixed ? c->pk32 : c->pk64, c->dsp,
+                               c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc);
   if (r) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[1], c->s));
   r = launch_stress(c->s, mixed, stress_args(c, dt, mode));
   if (r) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[2], c->s));
-  ForceArgs f = force_args(c, dt, mode, predict);
-  f.csr = dev_csr_copy(c);
-  if (!f.csr) return MEGA_ERR_NOMEM;
-  r = launch_force(c->s, mixed, f);
+  r = launch_force_tiled(c->s, mixed, force_args(c, dt, mode, predict));
   if (r) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[3], c->s));
   c->launches += 3;
@@ -246,7 +278,6 @@ static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) 
 static int graph_for(Ctx* c, double dt, int mode, int len) {
   if (c->gexec && c->g_mode == mode && c->g_dt == dt && c->g_len == len) return 0;
   if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
-  if (!dev_csr_copy(c)) return MEGA_ERR_NOMEM;
   cudaGraph_t g = nullptr;
   MEGA_TRY(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
   const int64_t before = c->launches;
@@ -268,6 +299,7 @@ static int run_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
   if (nsteps <= 0) return 0;
   const int prec = mode & 0xff;
   if (prec != MEGA_MODE_FP64 && prec != MEGA_MODE_MIXED) return MEGA_ERR_ARG;
+  if ((mode & MEGA_FLAG_LEARNED_GUESS) && !c->mlp_on) return MEGA_ERR_STATE;
   if (prec == MEGA_MODE_MIXED) { int r = ensure_mixed(c); if (r) return r; }
   if (!(mode & MEGA_FLAG_INTERP_EACH_STEP)) c->phy_valid = false;
   int r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
@@ -516,80 +548,178 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   return 0;
 }
 
+// Gather every per-node array through map (dst[r] = src[map[r]]): perm moves
+// the original numbering to the bin-cell numbering, iperm moves it back.
+static int permute_nodes(Ctx* c, const int32_t* map) {
+  const int32_t n = c->n;
+  DevPool tp;
+  unsigned char* tmp = nullptr;
+  MEGA_ALLOC(tp, tmp, (int64_t)n * 48);
+  struct Arr { void* p; int w; int es; };
+  const Arr list[] = {
+      {c->coo, 3, 8}, {c->win, 3, 8}, {c->mass, 3, 8}, {c->dsp, 3, 8}, {c->dsp_tot, 3, 8}, {c->dsp_tot_phy, 3, 8},
+      {c->vel, 3, 8}, {c->acl, 3, 8}, {c->fint, 3, 8}, {c->fext, 3, 8}, {c->prforce, 3, 8}, {c->bodyforce, 3, 8},
+      {c->sm_len, 6, 8}, {c->stress, 6, 8}, {c->strain, 6, 8}, {c->vol, 1, 8}, {c->eps, 1, 8},
+      {c->strain_eq, 1, 8}, {c->wvel, 1, 8}, {c->ebc, 3, 1}, {c->body_id, 1, 1}, {c->ebc_nodes, 1, 4},
+      {c->iters, 1, 4}, {c->matidx, 1, 2}};
+  for (const Arr& a : list) {
+    if (!a.p) continue;
+    k_perm_gather<<<grid_for((int64_t)n * a.w, 256), 256, 0, c->s>>>(n, a.w, a.es, map, (const unsigned char*)a.p,
+                                                                       tmp);
+    MEGA_CHECK_LAUNCH();
+    MEGA_TRY(cudaMemcpyAsync(a.p, tmp, (size_t)n * a.w * a.es, cudaMemcpyDeviceToDevice, c->s));
+  }
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  return 0;
+}
+
 int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gstack, int64_t dim_nn_list,
                            double* shp, double* dshp, int64_t* nnz, int32_t* gmaxn) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
-  if (c->searched) {
+  const int32_t n = c->n;
+  if (c->searched) {  // back to the original numbering, then search afresh
+    int r = permute_nodes(c, c->iperm);
+    if (r) return r;
     c->nbpool.free_all();
     c->mixpool.free_all();
-    c->mixed_ready = false;
     c->csr = DevCSR();
-    c->dcsr = nullptr;
+    c->rt = TileSet();
+    c->ct = TileSet();
+    c->perm = c->iperm = nullptr;
+    c->shp = c->sdphi = c->sdphi32 = c->tshp = nullptr;
+    c->pk64 = c->tpk64 = c->pk32 = c->tpk32 = nullptr;
     c->searched = false;
     if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
   }
-  int r = bin_search(c->s, c->n, c->coo, c->win, c->sm_len, c->p.dist_max, c->p.itype_int, c->p.shsup, c->status,
-                     c->csr, nullptr, c->nbpool, nullptr);
+  // 1. search and shapes in the reference's numbering (what the caller may download)
+  DevPool tmp0;
+  DevCSR csr0;
+  MEGA_ALLOC(c->nbpool, c->perm, n);
+  MEGA_ALLOC(c->nbpool, c->iperm, n);
+  int r = bin_search(c->s, n, c->coo, c->win, c->sm_len, c->p.dist_max, c->p.itype_int, c->p.shsup, c->status, csr0,
+                     nullptr, tmp0, nullptr, c->perm);
   if (r) return r;
-  r = build_transpose(c->s, c->csr, c->nbpool);
+  const int64_t m = csr0.nnz;
+  double *shp0, *g0x, *g0y, *g0z;
+  MEGA_ALLOC(tmp0, shp0, m);
+  MEGA_ALLOC(tmp0, g0x, m);
+  MEGA_ALLOC(tmp0, g0y, m);
+  MEGA_ALLOC(tmp0, g0z, m);
+  r = rk_shapes(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr0, shp0, g0x, g0y, g0z, c->status);
   if (r) return r;
-  const int64_t nnz_ = c->csr.nnz;
-  MEGA_ALLOC(c->nbpool, c->shp, nnz_);
-  MEGA_ALLOC(c->nbpool, c->gx, nnz_);
-  MEGA_ALLOC(c->nbpool, c->gy, nnz_);
-  MEGA_ALLOC(c->nbpool, c->gz, nnz_);
-  MEGA_ALLOC(c->nbpool, c->tgx, nnz_);
-  MEGA_ALLOC(c->nbpool, c->tgy, nnz_);
-  MEGA_ALLOC(c->nbpool, c->tgz, nnz_);
-  MEGA_ALLOC(c->nbpool, c->sdphi, 3 * (int64_t)c->n);
-  if (c->has_body) MEGA_ALLOC(c->nbpool, c->tshp, nnz_);
-  r = rk_shapes(c->s, c->p, c->n, c->coo, c->win, c->ebc_nodes, c->csr, c->shp, c->gx, c->gy, c->gz, c->status);
-  if (r) return r;
-  const unsigned g = grid_for(nnz_, 256);
-  k_gather_pos<<<g, 256, 0, c->s>>>(nnz_, c->csr.tpos, c->gx, c->tgx);
-  k_gather_pos<<<g, 256, 0, c->s>>>(nnz_, c->csr.tpos, c->gy, c->tgy);
-  k_gather_pos<<<g, 256, 0, c->s>>>(nnz_, c->csr.tpos, c->gz, c->tgz);
-  if (c->has_body) k_gather_pos<<<g, 256, 0, c->s>>>(nnz_, c->csr.tpos, c->shp, c->tshp);
-  k_rowsum3<double><<<grid_for(c->n, 256), 256, 0, c->s>>>(c->n, c->csr.rowptr, c->gx, c->gy, c->gz, c->sdphi);
-  MEGA_CHECK_LAUNCH();
-  MEGA_ALLOC(c->nbpool, c->dcsr, 1);
-  MEGA_TRY(cudaMemcpyAsync(c->dcsr, &c->csr, sizeof(DevCSR), cudaMemcpyHostToDevice, c->s));
-  MEGA_TRY(cudaStreamSynchronize(c->s));
-  c->searched = true;
-  if (nnz) *nnz = nnz_;
-  if (gmaxn) *gmaxn = c->csr.gmaxn;
-  // optional downloads in the reference's layout
-  std::vector<int64_t> rp;
-  if (gn || gstart || gstack || shp || dshp) {
-    rp.resize(c->n + 1);
-    MEGA_TRY(cudaMemcpyAsync(rp.data(), c->csr.rowptr, sizeof(int64_t) * (c->n + 1), cudaMemcpyDeviceToHost, c->s));
-    MEGA_TRY(cudaStreamSynchronize(c->s));
-  }
   int st = 0;
-  if (gn || gstart) {
-    for (int32_t i = 0; i < c->n; ++i) {
+  if (gn || gstart || gstack || shp || dshp) {
+    std::vector<int64_t> rp(n + 1);
+    MEGA_TRY(cudaMemcpyAsync(rp.data(), csr0.rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    for (int32_t i = 0; i < n; ++i) {
       if (gn) gn[i] = (int32_t)(rp[i + 1] - rp[i]);
       if (gstart) gstart[i] = (int32_t)(rp[i] + 1);
     }
-  }
-  if (gstack) {
-    if (nnz_ > dim_nn_list) st |= MEGA_ST_STACK_OVERFLOW;
-    else {
-      MEGA_TRY(cudaMemcpyAsync(gstack, c->csr.col, sizeof(int32_t) * nnz_, cudaMemcpyDeviceToHost, c->s));
-      MEGA_TRY(cudaStreamSynchronize(c->s));
-      for (int64_t k = 0; k < nnz_; ++k) gstack[k] += 1;
+    if (gstack) {
+      if (m > dim_nn_list) st |= MEGA_ST_STACK_OVERFLOW;
+      else {
+        MEGA_TRY(cudaMemcpyAsync(gstack, csr0.col, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, c->s));
+        MEGA_TRY(cudaStreamSynchronize(c->s));
+        for (int64_t k = 0; k < m; ++k) gstack[k] += 1;
+      }
     }
-  }
-  if (shp) MEGA_TRY(cudaMemcpyAsync(shp, c->shp, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, c->s));
-  if (dshp) {
-    std::vector<double> a(nnz_), b(nnz_), d(nnz_);
-    MEGA_TRY(cudaMemcpyAsync(a.data(), c->gx, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, c->s));
-    MEGA_TRY(cudaMemcpyAsync(b.data(), c->gy, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, c->s));
-    MEGA_TRY(cudaMemcpyAsync(d.data(), c->gz, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, c->s));
+    if (shp) MEGA_TRY(cudaMemcpyAsync(shp, shp0, sizeof(double) * m, cudaMemcpyDeviceToHost, c->s));
+    if (dshp) {
+      std::vector<double> a(m), b(m), d(m);
+      MEGA_TRY(cudaMemcpyAsync(a.data(), g0x, sizeof(double) * m, cudaMemcpyDeviceToHost, c->s));
+      MEGA_TRY(cudaMemcpyAsync(b.data(), g0y, sizeof(double) * m, cudaMemcpyDeviceToHost, c->s));
+      MEGA_TRY(cudaMemcpyAsync(d.data(), g0z, sizeof(double) * m, cudaMemcpyDeviceToHost, c->s));
+      MEGA_TRY(cudaStreamSynchronize(c->s));
+      for (int64_t k = 0; k < m; ++k) { dshp[3 * k] = a[k]; dshp[3 * k + 1] = b[k]; dshp[3 * k + 2] = d[k]; }
+    }
     MEGA_TRY(cudaStreamSynchronize(c->s));
-    for (int64_t k = 0; k < nnz_; ++k) { dshp[3 * k] = a[k]; dshp[3 * k + 1] = b[k]; dshp[3 * k + 2] = d[k]; }
   }
+  // 2. renumber the nodes in bin-cell order (spatially compact rows and tiles)
+  k_iperm<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->perm, c->iperm);
+  MEGA_CHECK_LAUNCH();
+  r = permute_nodes(c, c->perm);
+  if (r) return r;
+  DevPool tmp1;
+  int32_t* len1;
+  MEGA_ALLOC(tmp1, len1, n);
+  c->csr.n = n;
+  c->csr.nnz = m;
+  c->csr.gmaxn = csr0.gmaxn;
+  MEGA_ALLOC(c->nbpool, c->csr.rowptr, (int64_t)n + 1);
+  MEGA_ALLOC(c->nbpool, c->csr.col, m);
+  MEGA_ALLOC(c->nbpool, c->shp, m);
+  double *g1x, *g1y, *g1z;
+  MEGA_ALLOC(tmp1, g1x, m);
+  MEGA_ALLOC(tmp1, g1y, m);
+  MEGA_ALLOC(tmp1, g1z, m);
+  k_newrow_len<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->perm, csr0.rowptr, len1);
+  MEGA_CHECK_LAUNCH();
+  r = scan_counts(c->s, len1, c->csr.rowptr, n, tmp1);
+  if (r) return r;
+  k_permute_rows<<<grid_for((int64_t)n * 32, 256), 256, 0, c->s>>>(n, c->perm, c->iperm, csr0.rowptr, csr0.col, shp0,
+                                                                    g0x, g0y, g0z, c->csr.rowptr, c->csr.col, c->shp,
+                                                                    g1x, g1y, g1z);
+  MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  tmp0.free_all();
+  // 3. transposed view, tiles, packed records
+  r = configure_tiled_kernels();
+  if (r) return r;
+  r = build_transpose(c->s, c->csr, c->nbpool);
+  if (r) return r;
+  r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->rt, c->nbpool, nullptr);
+  if (r) return r;
+  int32_t cmax = 0;
+  {
+    // the longest column bounds a column tile's set from below
+    std::vector<int64_t> cp(n + 1);
+    MEGA_TRY(cudaMemcpyAsync(cp.data(), c->csr.colptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    for (int32_t i = 0; i < n; ++i) cmax = std::max<int32_t>(cmax, (int32_t)(cp[i + 1] - cp[i]));
+  }
+  r = build_tiles(c->s, n, c->csr.colptr, c->csr.trow, m, cmax, c->ct, c->nbpool, nullptr);
+  if (r) return r;
+  {
+    double *a = nullptr, *b = nullptr;  // 4 doubles per entry
+    MEGA_ALLOC(c->nbpool, a, 4 * m);
+    MEGA_ALLOC(c->nbpool, b, 4 * m);
+    c->pk64 = a;
+    c->tpk64 = b;
+  }
+  {
+    float4 *a = nullptr, *b = nullptr;
+    MEGA_ALLOC(c->nbpool, a, m);
+    MEGA_ALLOC(c->nbpool, b, m);
+    c->pk32 = a;
+    c->tpk32 = b;
+  }
+  if ((r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, true, c->pk64)) ||
+      (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, true, c->tpk64)) ||
+      (r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, false, c->pk32)) ||
+      (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, false, c->tpk32)))
+    return r;
+  MEGA_ALLOC(c->nbpool, c->sdphi, 3 * (int64_t)n);
+  MEGA_ALLOC(c->nbpool, c->sdphi32, 3 * (int64_t)n);
+  k_rowsum3<double><<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, g1x, g1y, g1z, c->sdphi);
+  k_rowsum_pk32<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, (const float4*)c->pk32, c->sdphi32);
+  MEGA_CHECK_LAUNCH();
+  if (c->has_body) {
+    MEGA_ALLOC(c->nbpool, c->tshp, m);
+    k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->csr.tpos, c->shp, c->tshp);
+    MEGA_CHECK_LAUNCH();
+  }
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  // the per-step kernels read neither the transposed row ids nor the positions
+  c->nbpool.release(c->csr.trow);
+  c->nbpool.release(c->csr.tpos);
+  c->csr.trow = nullptr;
+  c->csr.tpos = nullptr;
+  tmp1.free_all();
+  c->searched = true;
+  if (nnz) *nnz = m;
+  if (gmaxn) *gmaxn = c->csr.gmaxn;
   int ds = read_status(c, true);
   if (ds < 0) return ds;
   return st | ds;
@@ -652,30 +782,49 @@ int mega_kernel_times(int64_t h, int32_t reps, double dt, int32_t mode, float* o
   return read_status(c, true);
 }
 
+// Device array in the renumbered order -> host array in the caller's order.
+static int download_nodes(Ctx* c, const void* src, int w, int es, void* dst) {
+  const int32_t n = c->n;
+  const size_t bytes = (size_t)n * w * es;
+  if (!c->searched) {
+    MEGA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    return 0;
+  }
+  DevPool tp;
+  unsigned char* tmp = nullptr;
+  MEGA_ALLOC(tp, tmp, bytes);
+  k_perm_gather<<<grid_for((int64_t)n * w, 256), 256, 0, c->s>>>(n, w, es, c->iperm, (const unsigned char*)src, tmp);
+  MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaMemcpyAsync(dst, tmp, bytes, cudaMemcpyDeviceToHost, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  return 0;
+}
+
 int mega_download(int64_t h, int32_t field, double* dst) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
   if (!dst) return MEGA_ERR_ARG;
   const int64_t n = c->n, n3 = 3 * n;
   const double* src = nullptr;
-  int64_t cnt = 0;
+  int w = 0;
   switch (field) {
-    case MEGA_F_DSP: src = c->dsp; cnt = n3; break;
-    case MEGA_F_DSP_TOT: src = c->dsp_tot; cnt = n3; break;
-    case MEGA_F_VEL: src = c->vel; cnt = n3; break;
-    case MEGA_F_ACL: src = c->acl; cnt = n3; break;
-    case MEGA_F_FINT: src = c->fint; cnt = n3; break;
-    case MEGA_F_FEXT: src = c->fext; cnt = n3; break;
-    case MEGA_F_STRESS: src = c->stress; cnt = 6 * n; break;
-    case MEGA_F_STRAIN: src = c->strain; cnt = 6 * n; break;
-    case MEGA_F_EPS: src = c->eps; cnt = n; break;
-    case MEGA_F_STRAIN_EQ: src = c->strain_eq; cnt = n; break;
-    case MEGA_F_WAVE_VEL: src = c->wvel; cnt = n; break;
-    case MEGA_F_PRFORCE: src = c->prforce; cnt = n3; break;
+    case MEGA_F_DSP: src = c->dsp; w = 3; break;
+    case MEGA_F_DSP_TOT: src = c->dsp_tot; w = 3; break;
+    case MEGA_F_VEL: src = c->vel; w = 3; break;
+    case MEGA_F_ACL: src = c->acl; w = 3; break;
+    case MEGA_F_FINT: src = c->fint; w = 3; break;
+    case MEGA_F_FEXT: src = c->fext; w = 3; break;
+    case MEGA_F_STRESS: src = c->stress; w = 6; break;
+    case MEGA_F_STRAIN: src = c->strain; w = 6; break;
+    case MEGA_F_EPS: src = c->eps; w = 1; break;
+    case MEGA_F_STRAIN_EQ: src = c->strain_eq; w = 1; break;
+    case MEGA_F_WAVE_VEL: src = c->wvel; w = 1; break;
+    case MEGA_F_PRFORCE: src = c->prforce; w = 3; break;
     case MEGA_F_NEWTON_IT: {
       std::vector<int32_t> it(n);
-      MEGA_TRY(cudaMemcpyAsync(it.data(), c->iters, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c->s));
-      MEGA_TRY(cudaStreamSynchronize(c->s));
+      int r = download_nodes(c, c->iters, 1, 4, it.data());
+      if (r) return r;
       for (int64_t i = 0; i < n; ++i) dst[i] = it[i];
       return 0;
     }
@@ -688,45 +837,51 @@ int mega_download(int64_t h, int32_t field, double* dst) {
         if (r) return r;
         phy = c->scratch3;
       }
-      std::vector<double> a(n3);
-      MEGA_TRY(cudaMemcpyAsync(a.data(), phy, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->s));
+      int r = download_nodes(c, phy, 3, 8, dst);
+      if (r) return r;
       if (field == MEGA_F_COO_CURRENT) {
         std::vector<double> x(n3);
-        MEGA_TRY(cudaMemcpyAsync(x.data(), c->coo, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->s));
-        MEGA_TRY(cudaStreamSynchronize(c->s));
-        for (int64_t m = 0; m < n3; ++m) dst[m] = x[m] + a[m];  // MAIN.F90:382-386
-      } else {
-        MEGA_TRY(cudaStreamSynchronize(c->s));
-        std::memcpy(dst, a.data(), sizeof(double) * n3);
+        r = download_nodes(c, c->coo, 3, 8, x.data());
+        if (r) return r;
+        for (int64_t k = 0; k < n3; ++k) dst[k] = x[k] + dst[k];  // MAIN.F90:382-386
       }
       return 0;
     }
     default: return MEGA_ERR_ARG;
   }
-  MEGA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->s));
-  MEGA_TRY(cudaStreamSynchronize(c->s));
-  return 0;
+  return download_nodes(c, src, w, 8, dst);
 }
 
 int mega_upload(int64_t h, int32_t field, const double* src) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
   if (!src) return MEGA_ERR_ARG;
-  const int64_t n = c->n, n3 = 3 * n;
+  const int32_t n = c->n;
   double* dst = nullptr;
-  int64_t cnt = 0;
+  int w = 0;
   switch (field) {
-    case MEGA_F_DSP: dst = c->dsp; cnt = n3; break;
-    case MEGA_F_DSP_TOT: dst = c->dsp_tot; cnt = n3; c->phy_valid = false; break;
-    case MEGA_F_VEL: dst = c->vel; cnt = n3; break;
-    case MEGA_F_ACL: dst = c->acl; cnt = n3; break;
-    case MEGA_F_FEXT: dst = c->fext; cnt = n3; break;
-    case MEGA_F_STRESS: dst = c->stress; cnt = 6 * n; break;
-    case MEGA_F_STRAIN: dst = c->strain; cnt = 6 * n; break;
-    case MEGA_F_EPS: dst = c->eps; cnt = n; break;
+    case MEGA_F_DSP: dst = c->dsp; w = 3; break;
+    case MEGA_F_DSP_TOT: dst = c->dsp_tot; w = 3; c->phy_valid = false; break;
+    case MEGA_F_VEL: dst = c->vel; w = 3; break;
+    case MEGA_F_ACL: dst = c->acl; w = 3; break;
+    case MEGA_F_FEXT: dst = c->fext; w = 3; break;
+    case MEGA_F_STRESS: dst = c->stress; w = 6; break;
+    case MEGA_F_STRAIN: dst = c->strain; w = 6; break;
+    case MEGA_F_EPS: dst = c->eps; w = 1; break;
     default: return MEGA_ERR_ARG;
   }
-  MEGA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyHostToDevice, c->s));
+  const size_t bytes = (size_t)n * w * sizeof(double);
+  if (!c->searched) {
+    MEGA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    return 0;
+  }
+  DevPool tp;
+  unsigned char* tmp = nullptr;
+  MEGA_ALLOC(tp, tmp, bytes);
+  MEGA_TRY(cudaMemcpyAsync(tmp, src, bytes, cudaMemcpyHostToDevice, c->s));
+  k_perm_gather<<<grid_for((int64_t)n * w, 256), 256, 0, c->s>>>(n, w, 8, c->perm, tmp, (unsigned char*)dst);
+  MEGA_CHECK_LAUNCH();
   MEGA_TRY(cudaStreamSynchronize(c->s));
   return 0;
 }
@@ -739,26 +894,122 @@ int mega_get_scalars(int64_t h, mega_scalars_t* out) {
   MEGA_TRY(cudaMemcpyAsync(&a, c->acc, sizeof(a), cudaMemcpyDeviceToHost, c->s));
   MEGA_TRY(cudaStreamSynchronize(c->s));
   out->time = c->time;
-  out->int_energy = a.int_work;
-  out->kin_energy = a.ke;
-  out->ext_energy = a.ee;
-  for (int k = 0; k < 6; ++k) out->total_force[k] = a.total_force[k];
+  out->int_energy = slot_sum(a.int_work);
+  out->kin_energy = slot_sum(a.ke);
+  out->ext_energy = slot_sum(a.ee);
+  for (int k = 0; k < 6; ++k) out->total_force[k] = slot_sum(a.tf[k]);
   out->steps = c->steps;
-  out->newton_iters = (int64_t)a.newton_iters;
-  out->plastic_nodes = (int64_t)a.plastic;
+  out->newton_iters = (int64_t)slot_sum(a.newton_iters);
+  out->plastic_nodes = (int64_t)slot_sum(a.plastic);
+  out->newton_iters_total = (int64_t)slot_sum(a.newton_total);
+  out->plastic_nodes_total = (int64_t)slot_sum(a.plastic_total);
   return 0;
 }
 
 int64_t mega_device_bytes(int64_t h) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
-  return c->pool.bytes + c->nbpool.bytes + c->mixpool.bytes;
+  return c->pool.bytes + c->nbpool.bytes + c->mixpool.bytes + c->mlppool.bytes;
 }
 
 int64_t mega_kernel_launches(int64_t h) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
   return c->launches;
+}
+
+static void drop_graph(Ctx* c) {
+  if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+  c->g_mode = -1;
+}
+
+int mega_set_surrogate(int64_t h, int32_t hidden, const float* theta) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  drop_graph(c);
+  if (!theta) { c->mlp_on = false; return 0; }
+  if (hidden != 64) return MEGA_ERR_UNSUPPORTED;
+  const int np = mlp_nparams();
+  if (!c->mlp_theta) {
+    MEGA_ALLOC(c->mlppool, c->mlp_theta, np);
+    MEGA_ALLOC(c->mlppool, c->mlp_w2, 64 * 64);
+    MEGA_ALLOC(c->mlppool, c->mlp_small, 4 * 64 + 3 * 64 + 1);
+  }
+  MEGA_TRY(cudaMemcpyAsync(c->mlp_theta, theta, sizeof(float) * np, cudaMemcpyHostToDevice, c->s));
+  int r = mlp_pack(c->s, c->mlp_theta, c->mlp_w2, c->mlp_small);
+  if (r) return r;
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  c->mlp_on = true;
+  return 0;
+}
+
+int mega_log_rate_samples(int64_t h, int64_t cap, int32_t stride, uint32_t seed) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (cap < 0 || stride <= 0) return MEGA_ERR_ARG;
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  drop_graph(c);
+  if (c->log_buf) { c->mlppool.release(c->log_buf); c->log_buf = nullptr; }
+  if (c->log_count) { c->mlppool.release(c->log_count); c->log_count = nullptr; }
+  c->log_cap = 0;
+  if (cap == 0) return 0;
+  MEGA_ALLOC(c->mlppool, c->log_buf, 5 * cap);
+  MEGA_ALLOC(c->mlppool, c->log_count, 1);
+  MEGA_TRY(cudaMemsetAsync(c->log_count, 0, sizeof(unsigned long long), c->s));
+  c->log_cap = cap;
+  c->log_stride = (uint32_t)stride;
+  c->log_seed = seed;
+  return 0;
+}
+
+int mega_rate_samples(int64_t h, float* out, int64_t cap, int64_t* count) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (!count || cap < 0) return MEGA_ERR_ARG;
+  if (c->log_cap == 0) { *count = 0; return 0; }
+  unsigned long long k = 0;
+  MEGA_TRY(cudaMemcpyAsync(&k, c->log_count, sizeof(k), cudaMemcpyDeviceToHost, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  const int64_t held = std::min<int64_t>((int64_t)k, c->log_cap);
+  *count = held;
+  if (out && held > 0) {
+    const int64_t m = std::min<int64_t>(held, cap);
+    MEGA_TRY(cudaMemcpyAsync(out, c->log_buf, sizeof(float) * 5 * m, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    *count = m;
+  }
+  return 0;
+}
+
+int mega_train_surrogate(int64_t h, float* theta, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                         float* loss_per_epoch) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (!theta || epochs <= 0 || batch <= 0) return MEGA_ERR_ARG;
+  if (c->log_cap == 0) return MEGA_ERR_STATE;
+  unsigned long long k = 0;
+  MEGA_TRY(cudaMemcpyAsync(&k, c->log_count, sizeof(k), cudaMemcpyDeviceToHost, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  const int64_t ns = std::min<int64_t>((int64_t)k, c->log_cap);
+  if (ns <= 0) return MEGA_ERR_STATE;
+  const int np = mlp_nparams();
+  if (!c->mlp_theta) {
+    MEGA_ALLOC(c->mlppool, c->mlp_theta, np);
+    MEGA_ALLOC(c->mlppool, c->mlp_w2, 64 * 64);
+    MEGA_ALLOC(c->mlppool, c->mlp_small, 4 * 64 + 3 * 64 + 1);
+  }
+  drop_graph(c);
+  MEGA_TRY(cudaMemcpyAsync(c->mlp_theta, theta, sizeof(float) * np, cudaMemcpyHostToDevice, c->s));
+  int r = mlp_train_dev(c->s, c->mlp_theta, ns, c->log_buf, 5, c->log_buf + 4, 5, epochs, batch, lr, seed,
+                        loss_per_epoch);
+  if (r) return r;
+  r = mlp_pack(c->s, c->mlp_theta, c->mlp_w2, c->mlp_small);
+  if (r) return r;
+  MEGA_TRY(cudaMemcpyAsync(theta, c->mlp_theta, sizeof(float) * np, cudaMemcpyDeviceToHost, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  c->mlp_on = true;
+  return 0;
 }
 
 int mega_gpu_finalize(int64_t h) {
@@ -1076,7 +1327,7 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   }
   MEGA_TRY(cudaStreamSynchronize(s));
   for (int32_t i = 0; i < n; ++i) gstate[20 * (size_t)i + 2] = hs[i];
-  *gint_work += hacc.int_work;
+  *gint_work += slot_sum(hacc.int_work);
   return (int)hst;
 }
 

@@ -24,6 +24,7 @@
 // double moment inverse, positions, integration and return-mapping
 // residual) instantiate the same templates.
 #include "mega_internal.cuh"
+#include "mlp_tc.cuh"
 
 namespace mega {
 namespace {
@@ -47,9 +48,9 @@ __global__ void __launch_bounds__(256) k_defgrad(int32_t n, const int64_t* __res
                                                  const double* __restrict__ shp,
                                                  double* __restrict__ dsp_tot_phy, double* __restrict__ fg,
                                                  StepAccum* __restrict__ acc) {
-  if (acc && blockIdx.x == 0 && threadIdx.x == 0) {  // per-step counters of the stress kernel
-    acc->newton_iters = 0ull;
-    acc->plastic = 0ull;
+  if (acc && blockIdx.x == 0 && threadIdx.x < kSlots) {  // per-step counters of the stress kernel
+    acc->newton_iters[threadIdx.x] = 0ull;
+    acc->plastic[threadIdx.x] = 0ull;
   }
   const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kGroup;
   const int q = threadIdx.x & (kGroup - 1);
@@ -128,157 +129,275 @@ __device__ __forceinline__ T block_sum(T v, T* sm) {
   return r;  // valid in thread 0
 }
 
+// State of one node between the trial part of the update (kinematics,
+// rotation, elastic predictor) and the rest (return mapping, write-back).
+template <typename T>
+struct Trial {
+  double spred[6], sold[6], eold[6];
+  T eps6[6], D[6], IF[3][3];
+  double det, vol;
+  MatEntry me;
+};
+
+// FINT.F90:363-794: |det F|, INV3(F), L = G0 INV3(F), Hughes-Winget, rotation
+// of sigma and eps, eps += dstrain, elastic predictor.
+template <typename T>
+__device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Trial<T>& w) {
+  const double* fgi = a.fg + 18 * i;
+  w.me = a.mats[a.matidx[i]];
+  w.vol = a.vol[i];
+  T G0[3][3], L[3][3], sig[6], dstr[6];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int l = 0; l < 3; ++l) G0[k][l] = (T)fgi[9 + 3 * k + l];
+  w.det = 1.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    w.sold[k] = a.stress[6 * i + k];
+    w.eold[k] = a.strain[6 * i + k];
+    sig[k] = (T)w.sold[k];
+    w.eps6[k] = (T)w.eold[k];
+    w.D[k] = T(0);
+  }
+  if (a.finite_strain) {
+    // |det F| and INV3 in double (F carries the FP64 displacement path)
+    double Fd[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) Fd[k][l] = fgi[3 * k + l];
+    w.det = det_abs(Fd);
+    double IFd[3][3];
+    inv3(Fd, IFd, a.inv3_exact != 0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) w.IF[k][l] = (T)IFd[k][l];
+    mm3(G0, w.IF, L);
+    T R[3][3];
+    hughes_winget(L, R, dstr, w.D, a.inv3_exact != 0);
+    rotate_tensor(R, sig);
+    rotate_tensor(R, w.eps6);
+  } else {
+    // FINT.F90:772-783 small strain: engineering shear, no rotation, DET = 1
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) w.IF[k][l] = (k == l) ? T(1) : T(0);
+    dstr[0] = G0[0][0]; dstr[1] = G0[1][1]; dstr[2] = G0[2][2];
+    dstr[3] = G0[2][1] + G0[1][2]; dstr[4] = G0[2][0] + G0[0][2]; dstr[5] = G0[1][0] + G0[0][1];
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) w.eps6[k] = w.eps6[k] + dstr[k];
+  // elastic predictor with FORM_CMAT (FINT_FUNCTIONS.F90:252-288)
+  const T lam = (T)w.me.lam, mu = (T)w.me.mu, l2m = (T)w.me.l2m;
+  w.spred[0] = (double)(sig[0] + (l2m * dstr[0] + lam * dstr[1] + lam * dstr[2]));
+  w.spred[1] = (double)(sig[1] + (lam * dstr[0] + l2m * dstr[1] + lam * dstr[2]));
+  w.spred[2] = (double)(sig[2] + (lam * dstr[0] + lam * dstr[1] + l2m * dstr[2]));
+  w.spred[3] = (double)(sig[3] + mu * dstr[3]);
+  w.spred[4] = (double)(sig[4] + mu * dstr[4]);
+  w.spred[5] = (double)(sig[5] + mu * dstr[5]);
+}
+
+// Inputs of the surrogate network for a rate-dependent node: with q the
+// trial deviatoric norm, sy0 = A + B eps0^n and f = q - sqrt(2/3) sy0,
+//   x0 = ln(f / (sqrt(2/3) sy0))            overstress
+//   x1 = eps0^n                             hardening state
+//   x2 = ln(max(sqrt(2/3) f/(2 mu)/dt, epsdot0)/epsdot0) / 10   rate
+//   x3 = 1e3 sqrt(2/3) sy0 / (2 mu)          yield-strain scale
+// The target is y = dgamma / (f / (2 mu)).  Returns f (<= 0: elastic).
+__device__ __forceinline__ double rate_features(const double spred[6], double eps0, const MatEntry& me, double dt,
+                                                float x[4], double& dgpp) {
+  const double mu = me.E / (2.0 * (1.0 + me.nu));
+  const double kk = spred[0] + spred[1] + spred[2];
+  const double d0 = spred[0] - kk / 3.0, d1 = spred[1] - kk / 3.0, d2 = spred[2] - kk / 3.0;
+  const double q = sqrt(d0 * d0 + d1 * d1 + d2 * d2 + 2.0 * (spred[3] * spred[3] + spred[4] * spred[4] +
+                                                             spred[5] * spred[5]));
+  const double s23 = sqrt(2.0 / 3.0);
+  const double epn = (eps0 > 0.0) ? pow(eps0, me.C) : 0.0;
+  const double sy0 = me.sig0 + me.B * epn;
+  const double f = q - s23 * sy0;
+  dgpp = f / (2.0 * mu);
+  x[0] = (float)log(fmax(f, 1e-30 * sy0) / (s23 * sy0));
+  x[1] = (float)epn;
+  x[2] = (float)(log(fmax(s23 * dgpp / dt, me.p8) / me.p8) / 10.0);
+  x[3] = (float)(1e3 * s23 * sy0 / (2.0 * mu));
+  return f;
+}
+
+// FINT.F90:797-870, 999-1116: return mapping (dg0 >= 0 starts the rate law's
+// Newton there), state write-back, strain_eq, internal work, wave speed, T_i.
+template <typename T, typename TS>
+__device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Trial<T>& w, double dg0, double& work,
+                                              unsigned long long& nit, unsigned long long& npl, unsigned& st) {
+  const NodeMat m = to_nodemat(w.me);
+  double snew[6];
+  double ep = a.eps[i];
+  const double ep0 = ep;
+  int it = 0;
+  bool cap = false;
+  if (m.type == MEGA_MAT_ELASTIC) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) snew[k] = w.spred[k];
+  } else if (m.type == MEGA_MAT_VONMISES) {
+    it = von_mises(w.spred, ep, m, a.maxit, snew, cap);
+  } else if (m.type == MEGA_MAT_VM_RATE) {
+    double dg = 0.0, ftr = 0.0;
+    const double g0 = (dg0 >= 0.0) ? dg0 : (a.mlp_guess ? (double)a.mlp_guess[i] : -1.0);
+    it = vm_rate(w.spred, ep, m, a.dt, a.rtol, a.maxit, g0, snew, cap, dg, ftr);
+    if (a.log_buf && it > 0) {  // sample (features, converged multiplier) for the surrogate
+      const uint64_t sb = (uint64_t)__double_as_longlong(w.spred[0]);
+      const uint32_t hsh = ((uint32_t)i * 2654435761u) ^ (uint32_t)(sb ^ (sb >> 29)) ^ a.log_seed;
+      if (hsh % a.log_stride == 0) {
+        float x[4];
+        double dgpp;
+        const double f = rate_features(w.spred, ep0, w.me, a.dt, x, dgpp);
+        if (f > 0.0) {
+          const unsigned long long k = atomicAdd(a.log_count, 1ull);
+          if ((int64_t)k < a.log_cap) {
+            float* o = a.log_buf + 5 * k;
+            o[0] = x[0]; o[1] = x[1]; o[2] = x[2]; o[3] = x[3];
+            o[4] = (float)(dg / dgpp);
+          }
+        }
+      }
+    }
+  } else {
+    st |= MEGA_ST_BAD_MATERIAL;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) snew[k] = w.spred[k];
+  }
+  if (cap) st |= MEGA_ST_NEWTON_CAP;
+  nit += (unsigned long long)it;
+  npl += (it > 0) ? 1ull : 0ull;
+  if (a.iters) a.iters[i] = it;
+  double sinc[6], einc[6], enew[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    enew[k] = (double)w.eps6[k];
+    sinc[k] = snew[k] - w.sold[k];
+    einc[k] = enew[k] - w.eold[k];
+    a.stress[6 * i + k] = snew[k];
+    a.strain[6 * i + k] = enew[k];
+  }
+  a.eps[i] = ep;
+  const double eq = enew[0] * enew[0] + enew[1] * enew[1] + enew[2] * enew[2] +
+                    2.0 * (enew[3] * enew[3] + enew[4] * enew[4] + enew[5] * enew[5]);
+  a.strain_eq[i] = sqrt(eq * 2.0 / 3.0);
+  if (a.finite_strain) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) work += 0.5 * (double)w.D[k] * (2.0 * snew[k] - sinc[k]) * w.vol * w.det;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) work += 0.5 * einc[k] * sinc[k] * w.vol * w.det;
+  }
+  double bulk = m.E / (3.0 * (1.0 - 2.0 * m.nu)), shear = m.E / (2.0 * (1.0 + m.nu));
+  if (m.type > 1) estimate_moduli(sinc, einc, shear, bulk);
+  const double pmod = bulk + 4.0 * shear / 3.0;
+  a.wvel[i] = sqrt(fmax(pmod, shear) / m.rho);
+  // T_i = V J sigma IF^T: f_J(k) = sum_m T(k,m) grad0 phi_iJ(m)
+  const T vj = (T)(w.vol * w.det);
+  T S[3][3];
+  T sn[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) sn[k] = (T)snew[k];
+  v2t(sn, S);
+  TS* to = (TS*)a.tmat + 12 * i;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int mm = 0; mm < 3; ++mm)
+      to[3 * k + mm] = (TS)(vj * (S[k][0] * w.IF[mm][0] + S[k][1] * w.IF[mm][1] + S[k][2] * w.IF[mm][2]));
+  if (a.has_body) {
+    const double rvj = m.rho * w.vol * w.det;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double b = (a.bodyforce ? a.bodyforce[3 * i + k] : 0.0) + a.grav[k];
+      to[9 + k] = (TS)(b * rvj);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+    if (!isfinite(snew[k])) st |= MEGA_ST_NONFINITE;
+}
+
+template <typename T>
+__device__ __forceinline__ void stress_reduce(const StressArgs& a, double work, unsigned long long nit,
+                                              unsigned long long npl, unsigned st, double* smd,
+                                              unsigned long long* smu) {
+  const double wsum = block_sum(work, smd);
+  const unsigned long long it_sum = block_sum(nit, smu);
+  const unsigned long long pl_sum = block_sum(npl, smu);
+  if (threadIdx.x == 0) {
+    const int sl = blockIdx.x % kSlots;
+    if (wsum != 0.0) atomicAdd(&a.acc->int_work[sl], wsum);
+    if (it_sum) { atomicAdd(&a.acc->newton_iters[sl], it_sum); atomicAdd(&a.acc->newton_total[sl], it_sum); }
+    if (pl_sum) { atomicAdd(&a.acc->plastic[sl], pl_sum); atomicAdd(&a.acc->plastic_total[sl], pl_sum); }
+  }
+  if (st) atomicOr(a.status, st);
+}
+
 // T = arithmetic of kinematics / rotation / predictor, TS = storage of T_i
 template <typename T, typename TS>
-__global__ void __launch_bounds__(256) k_stress(StressArgs a) {
+__global__ void __launch_bounds__(256, 2) k_stress(StressArgs a) {
   __shared__ double smd[32];
   __shared__ unsigned long long smu[32];
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    a.acc->ke = 0.0;  // the force kernel of this step accumulates it afresh
+  if (blockIdx.x == 0 && threadIdx.x < kSlots) {
+    a.acc->ke[threadIdx.x] = 0.0;  // the force kernel of this step accumulates it afresh
   }
   double work = 0.0;
   unsigned long long nit = 0, npl = 0;
   unsigned st = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double* fgi = a.fg + 18 * i;
-    const MatEntry me = a.mats[a.matidx[i]];
-    const NodeMat m = to_nodemat(me);
-    const double vol = a.vol[i];
-    T Fm[3][3], G0[3][3], IF[3][3], L[3][3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-#pragma unroll
-      for (int l = 0; l < 3; ++l) { Fm[k][l] = (T)fgi[3 * k + l]; G0[k][l] = (T)fgi[9 + 3 * k + l]; }
-    double det = 1.0;
-    T sig[6], eps6[6], dstr[6], D[6];
-    double sold[6], eold[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      sold[k] = a.stress[6 * i + k];
-      eold[k] = a.strain[6 * i + k];
-      sig[k] = (T)sold[k];
-      eps6[k] = (T)eold[k];
-      D[k] = T(0);
-    }
-    if (a.finite_strain) {
-      // |det F| and the push-forward in double for F (FP64 positions path)
-      double Fd[3][3];
-#pragma unroll
-      for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int l = 0; l < 3; ++l) Fd[k][l] = fgi[3 * k + l];
-      det = det_abs(Fd);
-      double IFd[3][3];
-      inv3(Fd, IFd, a.inv3_exact != 0);
-#pragma unroll
-      for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int l = 0; l < 3; ++l) IF[k][l] = (T)IFd[k][l];
-      mm3(G0, IF, L);
-      T R[3][3];
-      hughes_winget(L, R, dstr, D, a.inv3_exact != 0);
-      rotate_tensor(R, sig);
-      rotate_tensor(R, eps6);
-    } else {
-      // FINT.F90:772-783 small strain: engineering shear, no rotation, DET = 1
-#pragma unroll
-      for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int l = 0; l < 3; ++l) IF[k][l] = (k == l) ? T(1) : T(0);
-      dstr[0] = G0[0][0]; dstr[1] = G0[1][1]; dstr[2] = G0[2][2];
-      dstr[3] = G0[2][1] + G0[1][2]; dstr[4] = G0[2][0] + G0[0][2]; dstr[5] = G0[1][0] + G0[0][1];
-    }
-#pragma unroll
-    for (int k = 0; k < 6; ++k) eps6[k] = eps6[k] + dstr[k];
-    // elastic predictor with FORM_CMAT (FINT_FUNCTIONS.F90:252-288)
-    const T lam = (T)me.lam, mu = (T)me.mu, l2m = (T)me.l2m;
-    double spred[6];
-    spred[0] = (double)(sig[0] + (l2m * dstr[0] + lam * dstr[1] + lam * dstr[2]));
-    spred[1] = (double)(sig[1] + (lam * dstr[0] + l2m * dstr[1] + lam * dstr[2]));
-    spred[2] = (double)(sig[2] + (lam * dstr[0] + lam * dstr[1] + l2m * dstr[2]));
-    spred[3] = (double)(sig[3] + mu * dstr[3]);
-    spred[4] = (double)(sig[4] + mu * dstr[4]);
-    spred[5] = (double)(sig[5] + mu * dstr[5]);
-    double snew[6];
-    double ep = a.eps[i];
-    int it = 0;
-    bool cap = false;
-    if (m.type == MEGA_MAT_ELASTIC) {
-#pragma unroll
-      for (int k = 0; k < 6; ++k) snew[k] = spred[k];
-    } else if (m.type == MEGA_MAT_VONMISES) {
-      it = von_mises(spred, ep, m, a.maxit, snew, cap);
-    } else if (m.type == MEGA_MAT_VM_RATE) {
-      double dg = 0.0, ftr = 0.0;
-      const double g0 = a.mlp_guess ? (double)a.mlp_guess[i] : -1.0;
-      it = vm_rate(spred, ep, m, a.dt, a.rtol, a.maxit, g0, snew, cap, dg, ftr);
-    } else {
-      st |= MEGA_ST_BAD_MATERIAL;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) snew[k] = spred[k];
-    }
-    if (cap) st |= MEGA_ST_NEWTON_CAP;
-    nit += (unsigned long long)it;
-    npl += (it > 0) ? 1ull : 0ull;
-    if (a.iters) a.iters[i] = it;
-    double sinc[6], einc[6], enew[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      enew[k] = (double)eps6[k];
-      sinc[k] = snew[k] - sold[k];
-      einc[k] = enew[k] - eold[k];
-      a.stress[6 * i + k] = snew[k];
-      a.strain[6 * i + k] = enew[k];
-    }
-    a.eps[i] = ep;
-    const double eq = enew[0] * enew[0] + enew[1] * enew[1] + enew[2] * enew[2] +
-                      2.0 * (enew[3] * enew[3] + enew[4] * enew[4] + enew[5] * enew[5]);
-    a.strain_eq[i] = sqrt(eq * 2.0 / 3.0);
-    if (a.finite_strain) {
-#pragma unroll
-      for (int k = 0; k < 6; ++k) work += 0.5 * (double)D[k] * (2.0 * snew[k] - sinc[k]) * vol * det;
-    } else {
-#pragma unroll
-      for (int k = 0; k < 6; ++k) work += 0.5 * einc[k] * sinc[k] * vol * det;
-    }
-    double bulk = m.E / (3.0 * (1.0 - 2.0 * m.nu)), shear = m.E / (2.0 * (1.0 + m.nu));
-    if (m.type > 1) estimate_moduli(sinc, einc, shear, bulk);
-    const double pmod = bulk + 4.0 * shear / 3.0;
-    a.wvel[i] = sqrt(fmax(pmod, shear) / m.rho);
-    // T_i = V J sigma IF^T: f_J(k) = sum_m T(k,m) grad0 phi_iJ(m)
-    const T vj = (T)(vol * det);
-    T S[3][3];
-    T sn[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) sn[k] = (T)snew[k];
-    v2t(sn, S);
-    TS* to = (TS*)a.tmat + 12 * i;
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-#pragma unroll
-      for (int mm = 0; mm < 3; ++mm)
-        to[3 * k + mm] = (TS)(vj * (S[k][0] * IF[mm][0] + S[k][1] * IF[mm][1] + S[k][2] * IF[mm][2]));
-    if (a.has_body) {
-      const double rvj = m.rho * vol * det;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const double b = (a.bodyforce ? a.bodyforce[3 * i + k] : 0.0) + a.grav[k];
-        to[9 + k] = (TS)(b * rvj);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 6; ++k)
-      if (!isfinite(snew[k])) st |= MEGA_ST_NONFINITE;
+    Trial<T> w;
+    stress_trial(a, i, w);
+    stress_finish<T, TS>(a, i, w, -1.0, work, nit, npl, st);
   }
-  const double wsum = block_sum(work, smd);
-  const unsigned long long it_sum = block_sum(nit, smu);
-  const unsigned long long pl_sum = block_sum(npl, smu);
-  if (threadIdx.x == 0) {
-    if (wsum != 0.0) atomicAdd(&a.acc->int_work, wsum);
-    if (it_sum) atomicAdd(&a.acc->newton_iters, it_sum);
-    if (pl_sum) atomicAdd(&a.acc->plastic, pl_sum);
+  stress_reduce<T>(a, work, nit, npl, st, smd, smu);
+}
+
+// The learned start: a warp of 32 nodes evaluates the surrogate together
+// (the 64x64 layer on the tensor cores, mlp_tc.cuh) and each plastic
+// rate-dependent node starts its Newton iteration from
+// dgamma0 = clamp(y, 0.02, 1) f_trial / (2 mu).  The loop is warp-uniform.
+constexpr int kLearnBlock = 128;
+
+template <typename T, typename TS>
+__global__ void __launch_bounds__(kLearnBlock, 2) k_stress_learned(StressArgs a) {
+  __shared__ double smd[32];
+  __shared__ unsigned long long smu[32];
+  __shared__ __align__(16) MlpSmem net;
+  __shared__ __align__(16) uint16_t sH1[kLearnBlock * kMlpLd];
+  __shared__ float sOut[kLearnBlock];
+  if (blockIdx.x == 0 && threadIdx.x < kSlots) a.acc->ke[threadIdx.x] = 0.0;
+  mlp_load(net, a.mlp_w2, a.mlp_small);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint16_t* hw = sH1 + (wid * 32) * kMlpLd;
+  float* ow = sOut + wid * 32;
+  double work = 0.0;
+  unsigned long long nit = 0, npl = 0;
+  unsigned st = 0;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < a.n;
+       base += nwarps * 32) {
+    const int64_t i = base + lane;
+    const bool act = i < a.n;
+    Trial<T> w;
+    float x[4] = {0.f, 0.f, 0.f, 0.f};
+    double dgpp = 0.0, f = -1.0;
+    if (act) {
+      stress_trial(a, i, w);
+      if (w.me.type == MEGA_MAT_VM_RATE) f = rate_features(w.spred, a.eps[i], w.me, a.dt, x, dgpp);
+    }
+    const float y = warp_mlp(x, f > 0.0, net, hw, ow);
+    if (act) {
+      const double dg0 = f > 0.0 ? (double)fminf(fmaxf(y, 0.02f), 1.0f) * dgpp : -1.0;
+      stress_finish<T, TS>(a, i, w, dg0, work, nit, npl, st);
+    }
   }
-  if (st) atomicOr(a.status, st);
+  stress_reduce<T>(a, work, nit, npl, st, smd, smu);
 }
 
 // G = storage of grad phi, TS = storage of T_i, A = accumulation
@@ -374,11 +493,12 @@ __global__ void __launch_bounds__(256) k_force(ForceArgs a) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) ts[k] = block_sum(tf[k], smd);
     if (threadIdx.x == 0) {
-      atomicAdd(&a.acc->ke, ks);
-      if (es != 0.0) atomicAdd(&a.acc->ee, es);
+      const int sl = blockIdx.x % kSlots;
+      atomicAdd(&a.acc->ke[sl], ks);
+      if (es != 0.0) atomicAdd(&a.acc->ee[sl], es);
 #pragma unroll
       for (int k = 0; k < 6; ++k)
-        if (ts[k] != 0.0) atomicAdd(&a.acc->total_force[k], ts[k]);
+        if (ts[k] != 0.0) atomicAdd(&a.acc->tf[k][sl], ts[k]);
     }
   }
   if (st) atomicOr(a.status, st);
@@ -466,9 +586,16 @@ int launch_defgrad(cudaStream_t s, bool mixed, bool interp, int32_t n, const Dev
 int launch_stress(cudaStream_t s, bool mixed, const StressArgs& a) {
   const int block = 256;
   const int64_t need = grid_for(a.n, block);
-  const unsigned grid = (unsigned)std::min<int64_t>(need, (int64_t)device_sm_count() * 8);
-  if (mixed) k_stress<float, float><<<grid > 0 ? grid : 1, block, 0, s>>>(a);
-  else k_stress<double, double><<<grid > 0 ? grid : 1, block, 0, s>>>(a);
+  if (a.mlp_w2 && a.mlp_small) {  // learned start of the rate-dependent return mapping
+    const int64_t lneed = grid_for(a.n, kLearnBlock);
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(lneed, (int64_t)device_sm_count() * 8));
+    if (mixed) k_stress_learned<float, float><<<grid, kLearnBlock, 0, s>>>(a);
+    else k_stress_learned<double, double><<<grid, kLearnBlock, 0, s>>>(a);
+  } else {
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)device_sm_count() * 8));
+    if (mixed) k_stress<float, float><<<grid, block, 0, s>>>(a);
+    else k_stress<double, double><<<grid, block, 0, s>>>(a);
+  }
   MEGA_CHECK_LAUNCH();
   return 0;
 }

@@ -93,7 +93,7 @@ int scan_counts(cudaStream_t s, const int32_t* cnt, int64_t* off, int64_t m, Dev
 // ijk (3,n) 1-based may be null.  status is a device word (OR-ed).
 int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, const double* sm_len,
                const double dist_max[3], int32_t itype_int, int32_t shsup, unsigned* status,
-               DevCSR& csr, int32_t* ijk, DevPool& pool, BinGeom* geom_out);
+               DevCSR& csr, int32_t* ijk, DevPool& pool, BinGeom* geom_out, int32_t* cell_order = nullptr);
 // Build the CSC view of csr.
 int build_transpose(cudaStream_t s, DevCSR& csr, DevPool& pool);
 
@@ -109,16 +109,30 @@ struct MatEntry {
   double nu, E, rho, sig0, B, C, p7, p8, lam, mu, l2m, damp;
 };
 
-// Reductions the step kernels accumulate on the device.
+// Reductions the step kernels accumulate on the device.  Each quantity has
+// kSlots partial sums (a block adds into slot blockIdx % kSlots) so that
+// thousands of blocks do not serialise on one address; readers sum the slots.
+constexpr int kSlots = 64;
 struct StepAccum {
-  double int_work;        // GINT_WORK, accumulated over calls (FINT.F90:1232)
-  double ke;              // kinetic energy of the last step
-  double ee;              // accumulated external energy (MAIN.F90:539)
-  double total_force[6];  // TOTAL_FORCE(3,2), running sum (MAIN.F90:485)
-  unsigned long long newton_iters;  // last step
-  unsigned long long plastic;       // last step
-  double pad[4];
+  double int_work[kSlots];        // GINT_WORK, accumulated over calls (FINT.F90:1232)
+  double ke[kSlots];              // kinetic energy of the last step
+  double ee[kSlots];              // accumulated external energy (MAIN.F90:539)
+  double tf[6][kSlots];           // TOTAL_FORCE(3,2), running sum (MAIN.F90:485)
+  unsigned long long newton_iters[kSlots];  // last step
+  unsigned long long plastic[kSlots];       // last step
+  unsigned long long newton_total[kSlots];  // over all steps (never reset by a step)
+  unsigned long long plastic_total[kSlots];
 };
+inline double slot_sum(const double* v) {
+  double s = 0.0;
+  for (int k = 0; k < kSlots; ++k) s += v[k];
+  return s;
+}
+inline unsigned long long slot_sum(const unsigned long long* v) {
+  unsigned long long s = 0;
+  for (int k = 0; k < kSlots; ++k) s += v[k];
+  return s;
+}
 
 // ---------------- launchers (force.cu)
 struct StressArgs {
@@ -143,7 +157,13 @@ struct StressArgs {
   double dt;
   int32_t* iters;            // per-node Newton passes (or null)
   const float* mlp_guess;    // per-node Newton start for the rate law (or null)
-  float* rate_samples;       // logging of (features, dg) for the surrogate (or null)
+  const uint16_t* mlp_w2;    // surrogate network: W2 (64x64) as bf16 bits, or null
+  const float* mlp_small;    // W1 (64x4), b1, b2, W3, b3 as fp32, or null
+  float* log_buf;            // sample log: 5 floats (4 features, target) per sample, or null
+  unsigned long long* log_count;
+  int64_t log_cap;
+  uint32_t log_stride;
+  uint32_t log_seed;
   StepAccum* acc;
   unsigned* status;
 };
@@ -152,6 +172,12 @@ int launch_defgrad(cudaStream_t s, bool mixed, bool interp, int32_t n, const Dev
                    const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg,
                    StepAccum* acc);
 int launch_stress(cudaStream_t s, bool mixed, const StressArgs& a);
+
+// surrogate network of the rate-dependent return mapping (mlp.cu)
+int mlp_nparams();
+int mlp_pack(cudaStream_t s, const float* dtheta, uint16_t* w2, float* small);
+int mlp_train_dev(cudaStream_t s, float* dth, int64_t ns, const float* X, int xs, const float* T, int ts,
+                  int32_t epochs, int32_t batch, float lr, uint64_t seed, float* loss_host);
 struct ForceArgs {
   int32_t n;
   const DevCSR* csr;

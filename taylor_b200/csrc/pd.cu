@@ -273,6 +273,7 @@ struct PmbArgs {
   const float* l0;        // |xi| per bond
   uint32_t* broken;       // bit per bond
   const double* vol;
+  const double* X;        // reference positions (double-precision bond geometry)
   const double* u_in;
   double* u_out;
   double* vel;
@@ -285,35 +286,52 @@ struct PmbArgs {
   unsigned long long* nbroken;
 };
 
+// T = per-bond arithmetic: float (the mixed path: float bond geometry and
+// force, double accumulation of nothing but the integrator) or double (the
+// oracle's arithmetic, recomputed from X, for exact parity checks).
+template <typename T>
 __global__ void __launch_bounds__(256) k_pmb_step(PmbArgs a) {
   const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kG;
   const int q = threadIdx.x & (kG - 1);
   const unsigned gm = 0xFu << (threadIdx.x & 28);
   if (i >= a.n) return;
   const double ui0 = a.u_in[3 * i], ui1 = a.u_in[3 * i + 1], ui2 = a.u_in[3 * i + 2];
-  float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+  T f0 = T(0), f1 = T(0), f2 = T(0);
   unsigned nb = 0;
-  const float c = (float)a.c, sc = (float)a.s_c;
+  const T c = (T)a.c, sc = (T)a.s_c;
   for (int64_t p = a.rowptr[i] + q; p < a.rowptr[i + 1]; p += kG) {
-    const float L0 = a.l0[p];
-    if (L0 == 0.f) continue;  // the particle itself
+    const float L0f = a.l0[p];
+    if (L0f == 0.f) continue;  // the particle itself
     const uint32_t word = a.broken[p >> 5], bit = 1u << (p & 31);
     if (word & bit) continue;
     const int64_t j = a.col[p];
-    const float d0 = (float)(a.u_in[3 * j] - ui0), d1 = (float)(a.u_in[3 * j + 1] - ui1),
-                d2 = (float)(a.u_in[3 * j + 2] - ui2);
-    const float x0 = a.xi[3 * p], x1 = a.xi[3 * p + 1], x2 = a.xi[3 * p + 2];
-    // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|))
-    const float e0 = x0 + d0, e1 = x1 + d1, e2 = x2 + d2;
-    const float l = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
-    const float num = 2.f * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
-    const float s = num / (L0 * (l + L0));
+    T s, e0, e1, e2, l;
+    if (sizeof(T) == sizeof(double)) {
+      // the oracle's arithmetic: xi from X, eta = xi + (u_j - u_i), s = (|eta| - |xi|)/|xi|
+      const double x0 = a.X[3 * j] - a.X[3 * i], x1 = a.X[3 * j + 1] - a.X[3 * i + 1],
+                   x2 = a.X[3 * j + 2] - a.X[3 * i + 2];
+      e0 = (T)(x0 + (a.u_in[3 * j] - ui0));
+      e1 = (T)(x1 + (a.u_in[3 * j + 1] - ui1));
+      e2 = (T)(x2 + (a.u_in[3 * j + 2] - ui2));
+      const T L0 = (T)sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+      l = (T)sqrt((double)(e0 * e0 + e1 * e1 + e2 * e2));
+      s = (l - L0) / L0;
+    } else {
+      const T d0 = (T)(a.u_in[3 * j] - ui0), d1 = (T)(a.u_in[3 * j + 1] - ui1), d2 = (T)(a.u_in[3 * j + 2] - ui2);
+      const T x0 = (T)a.xi[3 * p], x1 = (T)a.xi[3 * p + 1], x2 = (T)a.xi[3 * p + 2];
+      const T L0 = (T)L0f;
+      // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|))
+      e0 = x0 + d0; e1 = x1 + d1; e2 = x2 + d2;
+      l = (T)sqrtf((float)(e0 * e0 + e1 * e1 + e2 * e2));
+      const T num = T(2) * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
+      s = num / (L0 * (l + L0));
+    }
     if (s > sc) {
       atomicOr(&a.broken[p >> 5], bit);
       ++nb;
       continue;
     }
-    const float w = c * s * (float)a.vol[j] / l;
+    const T w = c * s * (T)a.vol[j] / l;
     f0 += w * e0; f1 += w * e1; f2 += w * e2;
   }
 #pragma unroll
@@ -410,6 +428,7 @@ struct PmbCtx {
   unsigned long long* nbroken = nullptr;
   unsigned* status = nullptr;
   double c = 0, s_c = 0, rho = 1;
+  int f64 = 0;
   int cur = 0;
   int64_t steps = 0;
   cudaGraphExec_t g = nullptr;
@@ -423,7 +442,7 @@ struct PmbCtx {
 static PmbArgs pmb_args(PmbCtx* c, double dt) {
   PmbArgs a{};
   a.n = c->n; a.rowptr = c->csr.rowptr; a.col = c->csr.col; a.xi = c->xi; a.l0 = c->l0; a.broken = c->broken;
-  a.vol = c->vol; a.u_in = c->u[c->cur]; a.u_out = c->u[1 - c->cur]; a.vel = c->vel; a.acl = c->acl;
+  a.vol = c->vol; a.X = c->X; a.u_in = c->u[c->cur]; a.u_out = c->u[1 - c->cur]; a.vel = c->vel; a.acl = c->acl;
   a.fixed = c->fixed; a.c = c->c; a.s_c = c->s_c; a.inv_rho = 1.0 / c->rho; a.dt = dt; a.nbroken = c->nbroken;
   return a;
 }
@@ -559,11 +578,12 @@ static PmbCtx* get_pmb(int64_t h) {
 
 int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double* vinit, const int32_t* fixed,
                   double horizon, double micromodulus, double s_c, double rho, const uint8_t* broken0,
-                  int64_t* handle, int64_t* nbonds) {
+                  int32_t mode, int64_t* handle, int64_t* nbonds) {
   if (n <= 0 || !coo || !vol || !vinit || !handle || !(horizon > 0) || !(rho > 0)) return MEGA_ERR_ARG;
   PmbCtx* c = new PmbCtx();
   auto fail = [&](int code) { delete c; return code; };
   c->n = n; c->c = micromodulus; c->s_c = s_c; c->rho = rho;
+  c->f64 = ((mode & 0xff) == MEGA_MODE_FP64);
   if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) return fail(MEGA_ERR_CUDA);
   const int64_t n3 = 3 * (int64_t)n;
 #define PA(ptr, cnt) do { if (c->pool.alloc(&(ptr), (size_t)(cnt))) return fail(MEGA_ERR_NOMEM); } while (0)
@@ -636,7 +656,8 @@ int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms) {
     MEGA_TRY(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < 2; ++k) {
       PmbArgs a = pmb_args(c, dt);
-      k_pmb_step<<<gridg(c->n), 256, 0, c->s>>>(a);
+      if (c->f64) k_pmb_step<double><<<gridg(c->n), 256, 0, c->s>>>(a);
+      else k_pmb_step<float><<<gridg(c->n), 256, 0, c->s>>>(a);
       c->cur = 1 - c->cur;
     }
     cudaError_t e = cudaStreamEndCapture(c->s, &gr);
@@ -652,7 +673,8 @@ int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms) {
   }
   for (; done < nsteps; ++done) {
     PmbArgs a = pmb_args(c, dt);
-    k_pmb_step<<<gridg(c->n), 256, 0, c->s>>>(a);
+    if (c->f64) k_pmb_step<double><<<gridg(c->n), 256, 0, c->s>>>(a);
+    else k_pmb_step<float><<<gridg(c->n), 256, 0, c->s>>>(a);
     MEGA_CHECK_LAUNCH();
     c->cur = 1 - c->cur;
   }
@@ -680,7 +702,10 @@ int mega_pmb_download(int64_t h, int32_t what, double* dst, int64_t* nbroken) {
     *nbroken = (int64_t)v;
   }
   if (!dst) return 0;
-  if (what == 0) MEGA_TRY(cudaMemcpy(dst, c->u[c->cur], sizeof(double) * n3, cudaMemcpyDeviceToHost));
+  // after a step, u[cur] already holds the next step's predictor; the
+  // displacement of the last completed step is the one it started from
+  const double* ucur = c->steps > 0 ? c->u[1 - c->cur] : c->u[c->cur];
+  if (what == 0) MEGA_TRY(cudaMemcpy(dst, ucur, sizeof(double) * n3, cudaMemcpyDeviceToHost));
   else if (what == 1) MEGA_TRY(cudaMemcpy(dst, c->vel, sizeof(double) * n3, cudaMemcpyDeviceToHost));
   else if (what == 2) MEGA_TRY(cudaMemcpy(dst, c->acl, sizeof(double) * n3, cudaMemcpyDeviceToHost));
   else if (what == 3) {

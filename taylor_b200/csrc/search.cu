@@ -351,7 +351,7 @@ int scan_counts(cudaStream_t s, const int32_t* cnt, int64_t* off, int64_t m, Dev
 
 int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, const double* sm_len,
                const double dist_max[3], int32_t itype_int, int32_t shsup, unsigned* status, DevCSR& csr,
-               int32_t* ijk, DevPool& pool, BinGeom* geom_out) {
+               int32_t* ijk, DevPool& pool, BinGeom* geom_out, int32_t* cell_order) {
   DevPool scratch;  // freed on return
   csr.n = n;
   const int nbb = 148 * 2;
@@ -393,6 +393,8 @@ int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, 
   MEGA_CHECK_LAUNCH();
   k_cell_sort<<<grid_for(nbins, 256), 256, 0, s>>>(nbins, cstart, sorted, status);
   MEGA_CHECK_LAUNCH();
+  if (cell_order)  // nodes by bin cell (cell id order, index order inside a cell)
+    MEGA_TRY(cudaMemcpyAsync(cell_order, sorted, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
 
   const int mmax = (itype_int == 0) ? 1 : 7;  // BIN_SEARCH.F90:204-208
   int32_t* gmaxn = nullptr;

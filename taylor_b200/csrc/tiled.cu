@@ -1,0 +1,532 @@
+// tiled.cu -- shared-memory tiled gathers for the per-step kernels.
+//
+// The untiled gathers (force.cu) issue ten to thirteen scattered loads per
+// neighbour entry and run at the L1 throughput limit with HBM far from busy.
+// Here nodes are renumbered in bin-cell order (spatially compact), rows are
+// grouped into tiles of R consecutive nodes, and each tile's neighbour set
+// (the union of its rows, "J-set") is listed once.  Every neighbour entry
+// then carries its gradient and a 16-bit tile-local index in one 16-byte
+// (float) or 32-byte (double) record, and the neighbour data the tile needs
+// -- (u_tot, du) for the deformation gradient, T_i for the force -- is staged
+// in shared memory once per tile:
+//   k_defgrad_t  F = I + sum_J (u_J - u_i) (x) g + u_i (x) sum g,  G0 likewise
+//   k_force_t    f_J = sum_i T_i g^T_iJ, then the corrector / predictor
+// The summation order is fixed by the list order, so results are
+// deterministic, and identical in exact arithmetic to force.cu's.
+#include "mega_internal.cuh"
+#include "tiled.cuh"
+
+namespace mega {
+namespace {
+
+constexpr int kG = 4;  // lanes per row
+constexpr int kU = 4;  // records in flight per lane
+
+__device__ __forceinline__ unsigned hash_u32(unsigned x) {
+  x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+  return x;
+}
+
+// Block per tile: list the distinct neighbours of the tile's rows, sort them,
+// and give each entry its rank in that list.  HS hash slots in shared memory;
+// a tile with more than jmax distinct neighbours reports overflow.
+template <int HS>
+__global__ void __launch_bounds__(256) k_build_tiles(int32_t n, int32_t R, const int64_t* __restrict__ ptr,
+                                                     const int32_t* __restrict__ idx, int32_t jmax,
+                                                     int32_t* __restrict__ jset, int32_t* __restrict__ jcnt,
+                                                     uint16_t* __restrict__ lidx, int16_t* __restrict__ slot_tmp,
+                                                     int32_t* __restrict__ overflow) {
+  __shared__ int32_t keys[HS];
+  __shared__ int16_t rank[HS];
+  __shared__ int32_t sk[HS / 2];
+  __shared__ int32_t wsum[8];
+  __shared__ int32_t s_total, s_full;
+  const int tid = threadIdx.x;
+  const int64_t t = blockIdx.x;
+  const int64_t r0 = t * R, r1 = min((int64_t)n, r0 + R);
+  const int64_t p0 = ptr[r0], p1 = ptr[r1];
+  for (int s = tid; s < HS; s += blockDim.x) keys[s] = -1;
+  if (tid == 0) s_full = 0;
+  __syncthreads();
+  for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+    const int32_t j = idx[p];
+    unsigned h = hash_u32((unsigned)j) & (HS - 1);
+    int16_t slot = -1;
+    for (int probe = 0; probe < HS; ++probe) {  // bounded: a full table stops
+      const int32_t prev = atomicCAS(&keys[h], -1, j);
+      if (prev == -1 || prev == j) { slot = (int16_t)h; break; }
+      h = (h + 1) & (HS - 1);
+    }
+    if (slot < 0) s_full = 1;
+    slot_tmp[p] = slot;
+  }
+  __syncthreads();
+  // compaction of the occupied slots: each thread owns HS/256 consecutive slots
+  constexpr int PER = HS / 256;
+  int cnt = 0;
+  for (int k = 0; k < PER; ++k) cnt += (keys[tid * PER + k] != -1);
+  int x = cnt;
+  const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  if (tid == 0) {
+    int a = 0;
+    for (int w = 0; w < 8; ++w) { const int v = wsum[w]; wsum[w] = a; a += v; }
+    s_total = a;
+  }
+  __syncthreads();
+  const int total = s_total;
+  if (total > jmax || s_full) {  // the whole block leaves together
+    if (tid == 0) {
+      jcnt[t] = total;
+      atomicMax(overflow, s_full ? HS : total);
+    }
+    return;
+  }
+  int pos = wsum[wid] + x - cnt;
+  for (int k = 0; k < PER; ++k) {
+    const int32_t key = keys[tid * PER + k];
+    if (key != -1) sk[pos++] = key;
+  }
+  int np2 = 1;
+  while (np2 < total) np2 <<= 1;
+  for (int s = total + tid; s < np2; s += blockDim.x) sk[s] = INT32_MAX;
+  __syncthreads();
+  // bitonic sort of sk[0..np2)
+  for (int k = 2; k <= np2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < np2; i += blockDim.x) {
+        const int l = i ^ j;
+        if (l > i) {
+          const int32_t a = sk[i], b = sk[l];
+          const bool up = (i & k) == 0;
+          if ((a > b) == up) { sk[i] = b; sk[l] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  // rank of each slot = position of its key in the sorted list
+  for (int r = tid; r < total; r += blockDim.x) {
+    const int32_t key = sk[r];
+    unsigned h = hash_u32((unsigned)key) & (HS - 1);
+    for (int probe = 0; probe < HS; ++probe) {
+      if (keys[h] == key) { rank[h] = (int16_t)r; break; }
+      h = (h + 1) & (HS - 1);
+    }
+    jset[t * (int64_t)jmax + r] = key;
+  }
+  if (tid == 0) jcnt[t] = total;
+  __syncthreads();
+  for (int64_t p = p0 + tid; p < p1; p += blockDim.x) lidx[p] = (uint16_t)rank[slot_tmp[p]];
+}
+
+__global__ void k_pack_f32(int64_t m, const uint16_t* __restrict__ lidx, const double* __restrict__ gx,
+                           const double* __restrict__ gy, const double* __restrict__ gz,
+                           const int64_t* __restrict__ pos, float4* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= m) return;
+  const int64_t p = pos ? pos[e] : e;
+  out[e] = make_float4((float)gx[p], (float)gy[p], (float)gz[p], __int_as_float((int)lidx[e]));
+}
+
+__global__ void k_pack_f64(int64_t m, const uint16_t* __restrict__ lidx, const double* __restrict__ gx,
+                           const double* __restrict__ gy, const double* __restrict__ gz,
+                           const int64_t* __restrict__ pos, double2* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= m) return;
+  const int64_t p = pos ? pos[e] : e;
+  out[2 * e] = make_double2(gx[p], gy[p]);
+  out[2 * e + 1] = make_double2(gz[p], __longlong_as_double((long long)lidx[e]));
+}
+
+template <bool F64>
+__device__ __forceinline__ void load_entry(const void* pk, int64_t p, float& g0, float& g1, float& g2, int& l);
+template <>
+__device__ __forceinline__ void load_entry<false>(const void* pk, int64_t p, float& g0, float& g1, float& g2,
+                                                  int& l) {
+  const float4 v = __ldg((const float4*)pk + p);
+  g0 = v.x; g1 = v.y; g2 = v.z; l = __float_as_int(v.w);
+}
+__device__ __forceinline__ void load_entry64(const void* pk, int64_t p, double& g0, double& g1, double& g2, int& l) {
+  const double2 a = __ldg((const double2*)pk + 2 * p);
+  const double2 b = __ldg((const double2*)pk + 2 * p + 1);
+  g0 = a.x; g1 = a.y; g2 = b.x; l = (int)__double_as_longlong(b.y);
+}
+
+template <typename A, bool F64, bool INTERP>
+__global__ void __launch_bounds__(256) k_defgrad_t(int32_t n, int32_t R, int32_t jmax,
+                                                   const int64_t* __restrict__ rowptr, const void* __restrict__ pk,
+                                                   const int32_t* __restrict__ jset, const int32_t* __restrict__ jcnt,
+                                                   const double* __restrict__ dsp, const double* __restrict__ dsp_tot,
+                                                   const double* __restrict__ sdphi, const double* __restrict__ shp,
+                                                   double* __restrict__ dsp_tot_phy, double* __restrict__ fg,
+                                                   StepAccum* __restrict__ acc) {
+  extern __shared__ double sm[];
+  if (acc && blockIdx.x == 0 && threadIdx.x < kSlots) {
+    acc->newton_iters[threadIdx.x] = 0ull;
+    acc->plastic[threadIdx.x] = 0ull;
+  }
+  const int64_t t = blockIdx.x;
+  const int cnt = jcnt[t];
+  double* su = sm;             // 3 per local neighbour
+  double* sd = sm + 3 * cnt;
+  const int32_t* js = jset + t * (int64_t)jmax;
+  for (int l = threadIdx.x; l < cnt; l += blockDim.x) {
+    const int64_t g = js[l];
+    su[3 * l] = dsp_tot[3 * g]; su[3 * l + 1] = dsp_tot[3 * g + 1]; su[3 * l + 2] = dsp_tot[3 * g + 2];
+    sd[3 * l] = dsp[3 * g]; sd[3 * l + 1] = dsp[3 * g + 1]; sd[3 * l + 2] = dsp[3 * g + 2];
+  }
+  __syncthreads();
+  const int64_t i = t * R + threadIdx.x / kG;
+  const int q = threadIdx.x & (kG - 1);
+  const unsigned gmask = 0xFu << (threadIdx.x & 28);
+  if (threadIdx.x / kG >= R || i >= n) return;
+  const double ui0 = dsp_tot[3 * i], ui1 = dsp_tot[3 * i + 1], ui2 = dsp_tot[3 * i + 2];
+  const double di0 = dsp[3 * i], di1 = dsp[3 * i + 1], di2 = dsp[3 * i + 2];
+  A F[9], L[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) { F[k] = A(0); L[k] = A(0); }
+  double ph0 = 0.0, ph1 = 0.0, ph2 = 0.0;
+  const int64_t pend = rowptr[i + 1];
+  // One entry: F += (u_J - u_i) (x) g, L += (d_J - d_i) (x) g (+ phi d_J).
+  auto body = [&](int64_t p, A g0, A g1, A g2, int l) {
+    const A u0 = (A)(su[3 * l] - ui0), u1 = (A)(su[3 * l + 1] - ui1), u2 = (A)(su[3 * l + 2] - ui2);
+    const double dj0 = sd[3 * l], dj1 = sd[3 * l + 1], dj2 = sd[3 * l + 2];
+    const A d0 = (A)(dj0 - di0), d1 = (A)(dj1 - di1), d2 = (A)(dj2 - di2);
+    F[0] += u0 * g0; F[1] += u0 * g1; F[2] += u0 * g2;
+    F[3] += u1 * g0; F[4] += u1 * g1; F[5] += u1 * g2;
+    F[6] += u2 * g0; F[7] += u2 * g1; F[8] += u2 * g2;
+    L[0] += d0 * g0; L[1] += d0 * g1; L[2] += d0 * g2;
+    L[3] += d1 * g0; L[4] += d1 * g1; L[5] += d1 * g2;
+    L[6] += d2 * g0; L[7] += d2 * g1; L[8] += d2 * g2;
+    if (INTERP) {
+      const double s = shp[p];
+      ph0 += s * dj0; ph1 += s * dj1; ph2 += s * dj2;
+    }
+  };
+  // kU records in flight per lane before any is used (the loop is bound by
+  // DRAM latency otherwise); each lane still sums its entries in list order.
+  int64_t p = rowptr[i] + q;
+  if (F64) {
+    for (; p + (kU - 1) * kG < pend; p += kU * kG) {
+      double2 ra[kU], rb[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        ra[u] = __ldg((const double2*)pk + 2 * (p + u * kG));
+        rb[u] = __ldg((const double2*)pk + 2 * (p + u * kG) + 1);
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+        body(p + u * kG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y));
+    }
+  } else {
+    for (; p + (kU - 1) * kG < pend; p += kU * kG) {
+      float4 r[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) r[u] = __ldg((const float4*)pk + p + u * kG);
+#pragma unroll
+      for (int u = 0; u < kU; ++u) body(p + u * kG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w));
+    }
+  }
+  for (; p < pend; p += kG) {
+    if (F64) {
+      double a0, a1, a2;
+      int l;
+      load_entry64(pk, p, a0, a1, a2, l);
+      body(p, (A)a0, (A)a1, (A)a2, l);
+    } else {
+      float a0, a1, a2;
+      int l;
+      load_entry<false>(pk, p, a0, a1, a2, l);
+      body(p, (A)a0, (A)a1, (A)a2, l);
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < kG; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      F[k] += __shfl_xor_sync(gmask, F[k], o);
+      L[k] += __shfl_xor_sync(gmask, L[k], o);
+    }
+    if (INTERP) {
+      ph0 += __shfl_xor_sync(gmask, ph0, o);
+      ph1 += __shfl_xor_sync(gmask, ph1, o);
+      ph2 += __shfl_xor_sync(gmask, ph2, o);
+    }
+  }
+  if (q == 0) {
+    const double ui[3] = {ui0, ui1, ui2}, di[3] = {di0, di1, di2};
+    const double sd3[3] = {sdphi[3 * i], sdphi[3 * i + 1], sdphi[3 * i + 2]};
+    double* o = fg + 18 * i;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        o[3 * k + l] = (k == l ? 1.0 : 0.0) + ((double)F[3 * k + l] + ui[k] * sd3[l]);
+        o[9 + 3 * k + l] = (double)L[3 * k + l] + di[k] * sd3[l];
+      }
+    if (INTERP) {
+      dsp_tot_phy[3 * i] += ph0;
+      dsp_tot_phy[3 * i + 1] += ph1;
+      dsp_tot_phy[3 * i + 2] += ph2;
+    }
+  }
+}
+
+// TS = storage of T_i (float / double), A = accumulation, F64 = record width
+template <typename TS, typename A, bool F64>
+__global__ void __launch_bounds__(256) k_force_t(TiledForceArgs a) {
+  extern __shared__ double smx[];
+  __shared__ double red[8 * 8];
+  const int64_t t = blockIdx.x;
+  const int cnt = a.jcnt[t];
+  const int nv = a.has_body ? 12 : 9;
+  TS* sT = (TS*)smx;
+  const int32_t* js = a.jset + t * (int64_t)a.jmax;
+  const TS* tm = (const TS*)a.tmat;
+  for (int w = threadIdx.x; w < cnt * nv; w += blockDim.x) {
+    const int l = w / nv, k = w - l * nv;
+    sT[l * nv + k] = tm[12 * (int64_t)js[l] + k];
+  }
+  __syncthreads();
+  const int64_t J = t * a.R + threadIdx.x / kG;
+  const int q = threadIdx.x & (kG - 1);
+  const unsigned gmask = 0xFu << (threadIdx.x & 28);
+  double ke = 0.0, ee = 0.0, tf0 = 0.0, tf1 = 0.0, tf2 = 0.0, tf3 = 0.0, tf4 = 0.0, tf5 = 0.0;
+  unsigned st = 0;
+  if (threadIdx.x / kG < a.R && J < a.n) {
+    A f0 = A(0), f1 = A(0), f2 = A(0);
+    double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+    const int64_t c1 = a.colptr[J + 1];
+    auto body = [&](int64_t e, A g0, A g1, A g2, int l) {
+      const TS* T = sT + l * nv;
+      f0 += (A)T[0] * g0 + (A)T[1] * g1 + (A)T[2] * g2;
+      f1 += (A)T[3] * g0 + (A)T[4] * g1 + (A)T[5] * g2;
+      f2 += (A)T[6] * g0 + (A)T[7] * g1 + (A)T[8] * g2;
+      if (a.has_body) {
+        const double s = a.tshp[e];
+        e0 += s * (double)T[9]; e1 += s * (double)T[10]; e2 += s * (double)T[11];
+      }
+    };
+    int64_t e = a.colptr[J] + q;
+    if (F64) {
+      for (; e + (kU - 1) * kG < c1; e += kU * kG) {
+        double2 ra[kU], rb[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          ra[u] = __ldg((const double2*)a.pk + 2 * (e + u * kG));
+          rb[u] = __ldg((const double2*)a.pk + 2 * (e + u * kG) + 1);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+          body(e + u * kG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y));
+      }
+    } else {
+      for (; e + (kU - 1) * kG < c1; e += kU * kG) {
+        float4 r[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) r[u] = __ldg((const float4*)a.pk + e + u * kG);
+#pragma unroll
+        for (int u = 0; u < kU; ++u) body(e + u * kG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w));
+      }
+    }
+    for (; e < c1; e += kG) {
+      if (F64) {
+        double b0, b1, b2;
+        int l;
+        load_entry64(a.pk, e, b0, b1, b2, l);
+        body(e, (A)b0, (A)b1, (A)b2, l);
+      } else {
+        float b0, b1, b2;
+        int l;
+        load_entry<false>(a.pk, e, b0, b1, b2, l);
+        body(e, (A)b0, (A)b1, (A)b2, l);
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < kG; o <<= 1) {
+      f0 += __shfl_xor_sync(gmask, f0, o);
+      f1 += __shfl_xor_sync(gmask, f1, o);
+      f2 += __shfl_xor_sync(gmask, f2, o);
+      if (a.has_body) {
+        e0 += __shfl_xor_sync(gmask, e0, o);
+        e1 += __shfl_xor_sync(gmask, e1, o);
+        e2 += __shfl_xor_sync(gmask, e2, o);
+      }
+    }
+    if (q < 3) {
+      const int64_t m = 3 * J + q;
+      const double fi = (double)(q == 0 ? f0 : (q == 1 ? f1 : f2));
+      double fe = (q == 0 ? e0 : (q == 1 ? e1 : e2));
+      if (!isfinite(fi)) st |= MEGA_ST_NONFINITE;
+      const double mass = a.mass[m];
+      const double fe_old = a.fext[m];
+      double v = a.vel[m], acc, pr;
+      if (a.ebc[m] == 1) {  // MAIN.F90:438-445
+        v = 0.0;
+        acc = 0.0;
+        pr = -fi;
+        fe = -fi;
+      } else {  // MAIN.F90:472-481
+        const double mpdc = a.mats[a.matidx[J]].damp * mass;
+        acc = (fe - fi - mpdc * v) / (mass + 0.5 * a.dt * mpdc);
+        v = v + 0.5 * a.dt * acc;
+        pr = 0.0;
+      }
+      ee += 0.5 * (fe + fe_old) * a.dsp[m];
+      ke += 0.5 * mass * v * v;
+      const int b = a.body_id ? a.body_id[J] : 1;
+      if (b == 1) { if (q == 0) tf0 += pr; else if (q == 1) tf1 += pr; else tf2 += pr; }
+      else if (b == 2) { if (q == 0) tf3 += pr; else if (q == 1) tf4 += pr; else tf5 += pr; }
+      a.fint[m] = fi;
+      a.fext[m] = fe;
+      a.acl[m] = acc;
+      a.prforce[m] = pr;
+      if (a.predict) {  // MAIN.F90:353-355 of the next step
+        const double d = a.dt * v + a.dt * a.dt * 0.5 * acc;
+        a.dsp[m] = d;
+        a.dsp_tot[m] = a.dsp_tot[m] + d;
+        v = v + a.dt * 0.5 * acc;
+      }
+      a.vel[m] = v;
+    }
+  }
+  // one block reduction of the eight sums, then one atomic per sum into this block's slot
+  double v[8] = {ke, ee, tf0, tf1, tf2, tf3, tf4, tf5};
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) red[wid * 8 + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double tsum = 0.0;
+    for (int w = 0; w < nw; ++w) tsum += red[w * 8 + threadIdx.x];
+    const int sl = blockIdx.x % kSlots;
+    double* dst = threadIdx.x == 0 ? &a.acc->ke[sl] : (threadIdx.x == 1 ? &a.acc->ee[sl] : &a.acc->tf[threadIdx.x - 2][sl]);
+    if (tsum != 0.0) atomicAdd(dst, tsum);
+  }
+  if (st) atomicOr(a.status, st);
+}
+
+inline unsigned grid_for(int64_t work, int block) { return (unsigned)((work + block - 1) / block); }
+
+}  // namespace
+
+int build_tiles(cudaStream_t s, int32_t n, const int64_t* ptr, const int32_t* idx, int64_t nnz, int32_t gmaxn,
+                TileSet& ts, DevPool& pool, int32_t* maxcnt_out) {
+  constexpr int HS = 2048;
+  const int32_t jmax = HS / 2;
+  if (gmaxn > jmax) return MEGA_ERR_UNSUPPORTED;
+  DevPool scratch;
+  int16_t* slot_tmp = nullptr;
+  int32_t* ovf = nullptr;
+  MEGA_ALLOC(scratch, slot_tmp, nnz);
+  MEGA_ALLOC(scratch, ovf, 1);
+  for (int32_t R = 64; R >= 8; R >>= 1) {  // >= 8 keeps every block a whole warp
+    const int64_t ntiles = (n + R - 1) / R;
+    int32_t *jset = nullptr, *jcnt = nullptr;
+    uint16_t* lidx = nullptr;
+    DevPool trial;
+    MEGA_ALLOC(trial, jset, ntiles * jmax);
+    MEGA_ALLOC(trial, jcnt, ntiles);
+    MEGA_ALLOC(trial, lidx, nnz);
+    MEGA_TRY(cudaMemsetAsync(ovf, 0, sizeof(int32_t), s));
+    k_build_tiles<HS><<<(unsigned)ntiles, 256, 0, s>>>(n, R, ptr, idx, jmax, jset, jcnt, lidx, slot_tmp, ovf);
+    MEGA_CHECK_LAUNCH();
+    int32_t hovf = 0;
+    MEGA_TRY(cudaMemcpyAsync(&hovf, ovf, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    std::vector<int32_t> hc(ntiles);
+    MEGA_TRY(cudaMemcpyAsync(hc.data(), jcnt, sizeof(int32_t) * ntiles, cudaMemcpyDeviceToHost, s));
+    MEGA_TRY(cudaStreamSynchronize(s));
+    if (hovf) continue;  // too many distinct neighbours: halve the tile
+    int32_t mx = 0;
+    for (int32_t v : hc) mx = std::max(mx, v);
+    // keep the trial buffers: move ownership into the persistent pool
+    for (void* p : trial.ptrs) pool.ptrs.push_back(p);
+    pool.bytes += trial.bytes;
+    trial.ptrs.clear();
+    ts.R = R;
+    ts.ntiles = ntiles;
+    ts.jmax = jmax;
+    ts.maxcnt = mx;
+    ts.jset = jset;
+    ts.jcnt = jcnt;
+    ts.lidx = lidx;
+    if (maxcnt_out) *maxcnt_out = mx;
+    return 0;
+  }
+  return MEGA_ERR_UNSUPPORTED;
+}
+
+int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* gx, const double* gy,
+                 const double* gz, const int64_t* pos, bool f64, void* out) {
+  if (m <= 0) return 0;
+  if (f64) k_pack_f64<<<grid_for(m, 256), 256, 0, s>>>(m, lidx, gx, gy, gz, pos, (double2*)out);
+  else k_pack_f32<<<grid_for(m, 256), 256, 0, s>>>(m, lidx, gx, gy, gz, pos, (float4*)out);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+// Raise the dynamic shared-memory limit of the tiled kernels once (outside
+// any stream capture): a tile stages at most 1024 neighbours, 96 KB for the
+// double-precision T_i of the force kernel.
+int configure_tiled_kernels() {
+  static bool done = false;
+  if (done) return 0;
+  const int lim = 12 * 8 * 1024 + 1024;
+  MEGA_TRY(cudaFuncSetAttribute(k_defgrad_t<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  MEGA_TRY(cudaFuncSetAttribute(k_defgrad_t<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  MEGA_TRY(cudaFuncSetAttribute(k_defgrad_t<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  MEGA_TRY(cudaFuncSetAttribute(k_defgrad_t<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  MEGA_TRY(cudaFuncSetAttribute(k_force_t<float, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  MEGA_TRY(cudaFuncSetAttribute(k_force_t<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  done = true;
+  return 0;
+}
+
+int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
+                         const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
+                         const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc) {
+  const size_t smem = sizeof(double) * 6 * (size_t)ts.maxcnt;
+  const unsigned grid = (unsigned)ts.ntiles;
+  const int block = ts.R * kG;
+  if (mixed) {
+    auto k = interp ? k_defgrad_t<float, false, true> : k_defgrad_t<float, false, false>;
+    k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
+                                dsp_tot_phy, fg, acc);
+  } else {
+    auto k = interp ? k_defgrad_t<double, true, true> : k_defgrad_t<double, true, false>;
+    k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
+                                dsp_tot_phy, fg, acc);
+  }
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a) {
+  const int nv = a.has_body ? 12 : 9;
+  const size_t smem = (mixed ? sizeof(float) : sizeof(double)) * nv * (size_t)a.maxcnt;
+  const unsigned grid = (unsigned)a.ntiles;
+  const int block = a.R * kG;
+  if (mixed) {
+    auto k = k_force_t<float, float, false>;
+    k<<<grid, block, smem, s>>>(a);
+  } else {
+    auto k = k_force_t<double, double, true>;
+    k<<<grid, block, smem, s>>>(a);
+  }
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+}  // namespace mega

@@ -1,0 +1,62 @@
+// tiled.cuh -- tiles of consecutive rows (or columns) with their neighbour
+// sets, for the shared-memory staged gathers of tiled.cu.
+#pragma once
+#include "mega_internal.cuh"
+
+namespace mega {
+
+struct TileSet {
+  int32_t R = 0;           // rows (columns) per tile; the kernels run R*4 threads per tile
+  int64_t ntiles = 0;
+  int32_t jmax = 0;        // stride of jset per tile
+  int32_t maxcnt = 0;      // largest neighbour set of any tile
+  int32_t* jset = nullptr; // [ntiles][jmax] sorted node ids
+  int32_t* jcnt = nullptr; // [ntiles]
+  uint16_t* lidx = nullptr;  // per entry: rank of its neighbour in the tile's set
+};
+
+struct TiledForceArgs {
+  int32_t n;
+  int32_t R;
+  int64_t ntiles;
+  int32_t jmax;
+  int32_t maxcnt;
+  const int32_t* jset;
+  const int32_t* jcnt;
+  const int64_t* colptr;
+  const void* pk;         // packed transposed entries (gradient + local index)
+  const double* tshp;     // transposed shape values (body force) or null
+  const void* tmat;       // 12 values per node
+  int has_body;
+  int predict;
+  const int8_t* ebc;
+  const double* mass;
+  const uint16_t* matidx;
+  const MatEntry* mats;
+  const int8_t* body_id;
+  double* fint;
+  double* fext;
+  double* vel;
+  double* acl;
+  double* dsp;
+  double* dsp_tot;
+  double* prforce;
+  double dt;
+  StepAccum* acc;
+  unsigned* status;
+};
+
+// Tiles of R consecutive rows of (ptr, idx), R halved from 64 down to 8
+// until every tile's neighbour set fits jmax = 1024.
+int build_tiles(cudaStream_t s, int32_t n, const int64_t* ptr, const int32_t* idx, int64_t nnz, int32_t gmaxn,
+                TileSet& ts, DevPool& pool, int32_t* maxcnt_out);
+// out[e] = (g[pos[e]], lidx[e]) as float4 (f64 = false) or 2 x double2
+int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* gx, const double* gy,
+                 const double* gz, const int64_t* pos, bool f64, void* out);
+int configure_tiled_kernels();
+int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
+                         const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
+                         const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc);
+int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a);
+
+}  // namespace mega

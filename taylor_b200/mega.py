@@ -126,6 +126,56 @@ def construct_fint(params, coo, win, vol, props, mat_type, ebc_nodes, state, str
                 gint_work=gw.value, shp=shp, dshp=dshp, status=st)
 
 
+MLP_HIDDEN = 64
+
+
+def mlp_nparams(hidden=MLP_HIDDEN):
+    return int(check(_lib.lib().mega_mlp_nparams(int(hidden)), "mlp_nparams", allow_status=True))
+
+
+def mlp_init(seed=0, hidden=MLP_HIDDEN):
+    """Glorot-uniform weights, zero biases, in the packed parameter order."""
+    rng = np.random.default_rng(seed)
+    H = hidden
+    parts = []
+    for (o, i) in ((H, 4), (H, 0), (H, H), (H, 0), (1, H), (1, 0)):
+        if i == 0:
+            parts.append(np.zeros(o))
+        else:
+            a = np.sqrt(6.0 / (o + i))
+            parts.append(rng.uniform(-a, a, o * i))
+    return np.concatenate(parts).astype(np.float32)
+
+
+def mlp_grad(theta, x, t):
+    th = np.ascontiguousarray(theta, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    tt = np.ascontiguousarray(t, np.float32)
+    g = np.zeros_like(th)
+    loss = np.zeros(1, np.float32)
+    check(_lib.lib().mega_mlp_grad(MLP_HIDDEN, ptr(th), len(tt), ptr(xx), ptr(tt), ptr(g), ptr(loss)), "mlp_grad")
+    return float(loss[0]), g
+
+
+def mlp_eval(theta, x, tensor_cores=False):
+    th = np.ascontiguousarray(theta, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    y = np.zeros(len(xx), np.float32)
+    check(_lib.lib().mega_mlp_eval(MLP_HIDDEN, ptr(th), len(xx), ptr(xx), ptr(y), int(bool(tensor_cores))),
+          "mlp_eval")
+    return y
+
+
+def mlp_train(theta, x, t, epochs, batch=4096, lr=1e-3, seed=0):
+    th = np.array(theta, np.float32, copy=True)
+    xx = np.ascontiguousarray(x, np.float32)
+    tt = np.ascontiguousarray(t, np.float32)
+    loss = np.zeros(int(epochs), np.float32)
+    check(_lib.lib().mega_mlp_train(MLP_HIDDEN, ptr(th), len(tt), ptr(xx), ptr(tt), int(epochs), int(batch),
+                                    float(lr), int(seed), ptr(loss)), "mlp_train")
+    return th, loss
+
+
 class Mega:
     """Device-resident model: the MAIN.F90 time loop on the GPU.
 
@@ -179,23 +229,51 @@ class Mega:
             b |= _lib.FLAG_LEARNED_GUESS
         return b
 
-    def step(self, nsteps, dt, mode="fp64", interp_each_step=False, allow_status=False):
+    def step(self, nsteps, dt, mode="fp64", interp_each_step=False, allow_status=False, learned=False):
         st = _lib.lib().mega_step_resident(self.h, int(nsteps), float(dt),
-                                           self.mode_bits(mode, interp_each_step))
+                                           self.mode_bits(mode, interp_each_step, learned))
         return check(st, "step", allow_status)
 
-    def step_timed(self, nsteps, dt, mode="fp64", interp_each_step=False):
+    def step_timed(self, nsteps, dt, mode="fp64", interp_each_step=False, learned=False):
         ms = C.c_float(0.0)
-        st = _lib.lib().mega_step_timed(self.h, int(nsteps), float(dt), self.mode_bits(mode, interp_each_step),
-                                        C.byref(ms))
+        st = _lib.lib().mega_step_timed(self.h, int(nsteps), float(dt),
+                                        self.mode_bits(mode, interp_each_step, learned), C.byref(ms))
         check(st, "step_timed")
         return ms.value
 
-    def kernel_times(self, reps, dt, mode="fp64"):
+    def kernel_times(self, reps, dt, mode="fp64", learned=False):
         out = np.zeros(3, np.float32)
-        check(_lib.lib().mega_kernel_times(self.h, int(reps), float(dt), self.mode_bits(mode), ptr(out)),
-              "kernel_times")
+        check(_lib.lib().mega_kernel_times(self.h, int(reps), float(dt), self.mode_bits(mode, learned=learned),
+                                           ptr(out)), "kernel_times")
         return out
+
+    # -- surrogate start of the rate-dependent return mapping
+    def set_surrogate(self, theta):
+        th = None if theta is None else np.ascontiguousarray(theta, np.float32)
+        check(_lib.lib().mega_set_surrogate(self.h, MLP_HIDDEN, None if th is None else ptr(th)), "set_surrogate")
+
+    def log_rate_samples(self, cap, stride=1, seed=0):
+        check(_lib.lib().mega_log_rate_samples(self.h, int(cap), int(stride), int(seed)), "log_rate_samples")
+
+    def rate_samples(self, cap=None):
+        """Logged (x0..x3, y) rows, shape (m, 5)."""
+        held = C.c_int64(0)
+        check(_lib.lib().mega_rate_samples(self.h, None, 0, C.byref(held)), "rate_samples")
+        m = held.value if cap is None else min(held.value, int(cap))
+        out = np.zeros((max(m, 1), 5), np.float32)
+        got = C.c_int64(0)
+        if m:
+            check(_lib.lib().mega_rate_samples(self.h, ptr(out), m, C.byref(got)), "rate_samples")
+        return out[:got.value]
+
+    def train_surrogate(self, theta, epochs, batch=4096, lr=1e-3, seed=0):
+        """Adam on the logged samples without leaving the device; installs and
+        returns the trained parameters and the per-epoch mean loss."""
+        th = np.array(theta, np.float32, copy=True)
+        loss = np.zeros(int(epochs), np.float32)
+        check(_lib.lib().mega_train_surrogate(self.h, ptr(th), int(epochs), int(batch), float(lr), int(seed),
+                                              ptr(loss)), "train_surrogate")
+        return th, loss
 
     _SIZES = {0: 3, 1: 3, 2: 3, 3: 3, 4: 3, 5: 3, 6: 3, 7: 6, 8: 6, 9: 1, 10: 1, 11: 1, 12: 3, 13: 3, 14: 1}
 
@@ -213,7 +291,8 @@ class Mega:
         check(_lib.lib().mega_get_scalars(self.h, C.byref(s)), "scalars")
         return dict(time=s.time, int_energy=s.int_energy, kin_energy=s.kin_energy, ext_energy=s.ext_energy,
                     total_force=list(s.total_force), steps=s.steps, newton_iters=s.newton_iters,
-                    plastic_nodes=s.plastic_nodes)
+                    plastic_nodes=s.plastic_nodes, newton_iters_total=s.newton_iters_total,
+                    plastic_nodes_total=s.plastic_nodes_total)
 
     def device_bytes(self):
         return int(_lib.lib().mega_device_bytes(self.h))
@@ -259,7 +338,7 @@ class Pmb:
     """Bond-based PMB peridynamics, device resident (no reference
     counterpart).  case from taylor_b200.cases.pd_plate."""
 
-    def __init__(self, case, broken0=None, fixed=None):
+    def __init__(self, case, broken0=None, fixed=None, mode="mixed"):
         self.case = case
         self.n = int(case["n"])
         h = C.c_int64(0)
@@ -268,7 +347,9 @@ class Pmb:
         fx = None if fixed is None else _i32(fixed)
         check(_lib.lib().mega_pmb_init(self.n, ptr(_f64(case["coo"])), ptr(_f64(case["vol"])),
                                        ptr(_f64(case["vinit"])), ptr(fx), float(case["delta"]), float(case["c"]),
-                                       float(case["s_c"]), float(case["rho"]), ptr(b0), C.byref(h), C.byref(nb)),
+                                       float(case["s_c"]), float(case["rho"]), ptr(b0),
+                                       {"fp64": _lib.MODE_FP64, "mixed": _lib.MODE_MIXED}[mode], C.byref(h),
+                                       C.byref(nb)),
               "pmb_init")
         self.h, self.nnz = h.value, nb.value
 

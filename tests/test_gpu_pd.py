@@ -11,8 +11,9 @@ pytestmark = pytest.mark.gpu
 
 
 def _pd_case():
-    c = cases.taylor_bar(h=0.8e-3, L=10e-3, seed=4, norm_win=2.2)
-    return c
+    # millimetre units: INVERSE's absolute pivot test (D + 1 == 1,
+    # INVERSE.F90:41) would call the SI-unit shape tensors (~1e-16) singular
+    return cases.taylor_bar(h=0.8, R=3.2, L=10.0, seed=4, norm_win=2.2)
 
 
 def test_construct_fint_pd_matches_oracle():
@@ -27,7 +28,7 @@ def test_construct_fint_pd_matches_oracle():
     g0 = mega.construct_fint_pd(gp, c["coo"], c["coo"], c["win"], c["vol"], c["props"], c["mat_type"],
                                 np.zeros((n, 20)), np.zeros((n, 6)), np.zeros((n, 6)), z3, nb["gn"], nb["gstart"],
                                 nb["gstack"], np.zeros(nb["nnz"]), np.zeros((n, 3, 3)), True, 1e-8)
-    np.testing.assert_allclose(g0["shp"], shp_o, rtol=1e-14, atol=1e-16)
+    np.testing.assert_allclose(g0["shp"], shp_o, rtol=1e-14, atol=1e-15)
     np.testing.assert_allclose(g0["ginvk"], ik_o, rtol=1e-10)
     # a deformed, plastic state: affine stretch plus noise
     rng = np.random.default_rng(3)
@@ -63,7 +64,7 @@ def _oracle_pmb(case, nb, broken, nsteps, dt):
     return u, v
 
 
-def test_pmb_matches_oracle_and_breaks_bonds():
+def _plate_and_lists():
     c = cases.pd_plate(h=0.5e-3, nx=40, ny=40, nz=4, notch=6e-3, v_edge=20.0)
     nb = O.bin_search(c["coo"], c["win"], c["sm_len"], c["dist_max"], 0, 1)
     got_nb = mega.bin_search(c["coo"], c["win"], c["sm_len"], c["dist_max"], 0, 1)
@@ -71,7 +72,19 @@ def test_pmb_matches_oracle_and_breaks_bonds():
     broken0 = cases.notch_broken(c, nb["gn"], nb["gstart"], nb["gstack"])
     assert broken0.sum() > 0
     dt = 0.5 * c["h"] / np.sqrt(72e9 / c["rho"])
-    p = mega.Pmb(c, broken0)
+    return c, nb, broken0, dt
+
+
+def _pair_mismatch(nb, n, flags):
+    rows = np.repeat(np.arange(n), nb["gn"])
+    cols = nb["gstack"] - 1
+    key = {(int(i), int(j)): k for k, (i, j) in enumerate(zip(rows, cols))}
+    return sum(1 for k, (i, j) in enumerate(zip(rows, cols)) if flags[k] != flags[key[(int(j), int(i))]])
+
+
+def test_pmb_fp64_matches_oracle_exactly():
+    c, nb, broken0, dt = _plate_and_lists()
+    p = mega.Pmb(c, broken0, mode="fp64")
     assert p.nnz == nb["nnz"]
     nsteps = 300
     p.step(nsteps, dt)
@@ -79,15 +92,27 @@ def test_pmb_matches_oracle_and_breaks_bonds():
     flags, nbk = p.download(3)
     bo = broken0.copy()
     uo, vo = _oracle_pmb(c, nb, bo, nsteps, dt)
-    assert np.abs(u - uo).max() <= 2e-4 * np.abs(uo).max()
+    assert bo.sum() > broken0.sum()  # bonds broke during the run
+    np.testing.assert_array_equal(flags.astype(np.uint8), bo)
+    assert np.abs(u - uo).max() <= 1e-9 * np.abs(uo).max()
+    assert _pair_mismatch(nb, c["n"], flags) == 0  # both copies of a bond break together
+    p.close()
+
+
+def test_pmb_float_force_error_bound():
+    """Float bond arithmetic: displacement within 1 % of the FP64 oracle and
+    the broken-bond count within 3 % after 300 steps through fracture."""
+    c, nb, broken0, dt = _plate_and_lists()
+    p = mega.Pmb(c, broken0, mode="mixed")
+    nsteps = 300
+    p.step(nsteps, dt)
+    u, _ = p.download(0)
+    flags, nbk = p.download(3)
+    bo = broken0.copy()
+    uo, vo = _oracle_pmb(c, nb, bo, nsteps, dt)
+    assert np.abs(u - uo).max() <= 1e-2 * np.abs(uo).max()
     newly_gpu = int(flags.sum() - broken0.sum())
     newly_orc = int(bo.sum() - broken0.sum())
-    assert newly_orc > 0
-    assert abs(newly_gpu - newly_orc) <= max(4, 0.02 * newly_orc)
-    # both copies of a bond break together
-    rows = np.repeat(np.arange(c["n"]), nb["gn"])
-    cols = nb["gstack"] - 1
-    key = {(int(i), int(j)): k for k, (i, j) in enumerate(zip(rows, cols))}
-    mism = sum(1 for k, (i, j) in enumerate(zip(rows, cols)) if flags[k] != flags[key[(int(j), int(i))]])
-    assert mism == 0
+    assert abs(newly_gpu - newly_orc) <= max(4, 0.03 * newly_orc)
+    assert _pair_mismatch(nb, c["n"], flags) == 0
     p.close()
