@@ -44,11 +44,16 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=0, help="CPU baseline sample steps (0 = auto)")
     ap.add_argument("--modes", default="fp64,mixed", help="order in which the precision modes run")
-    ap.add_argument("--full-steps", type=int, default=2000,
+    ap.add_argument("--full-steps", type=int, default=600,
                     help="steps of the accuracy runs (FP64 vs mixed end states); 0 skips them")
     ap.add_argument("--rate-h", type=float, default=0.08e-3,
                     help="lattice spacing of the rate-dependent bar of the learned-start runs; 0 skips them")
-    ap.add_argument("--rate-steps", type=int, default=2000, help="steps of the rate-dependent runs")
+    ap.add_argument("--rate-steps", type=int, default=600, help="steps of the rate-dependent runs")
+    ap.add_argument("--pmb-nx", type=int, default=400,
+                    help="in-plane particles per side of the bond-based peridynamics plate; 0 skips it")
+    ap.add_argument("--pmb-steps", type=int, default=4000, help="steps of the peridynamics run")
+    ap.add_argument("--batch-bars", type=int, default=256, help="bars of the batched run; 0 skips it")
+    ap.add_argument("--batch-steps", type=int, default=64, help="timed steps of the batched and sequential runs")
     return ap.parse_args()
 
 
@@ -188,24 +193,45 @@ def run_ours(args, rank, world, dist):
     barrier(dist)
     t0 = time.perf_counter()
     e = mega.Mega(case, p)
+    t1 = time.perf_counter()
     e.search_and_shapes()
+    t2 = time.perf_counter()
     d2h = 0
     for _ in range(args.steps):
         e.step(1, dt, mode="mixed")
         sc = e.scalars()           # ENERGY_INFO.OUT / TOTAL_FORCE.OUT / TIME.OUT of MAIN, every step
         d2h += 8 * 12
+    t3 = time.perf_counter()
     xend = e.download(_lib.F_COO_CURRENT)
     epend = e.download(_lib.F_EPS)
     d2h += xend.nbytes + epend.nbytes
     e.close()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    t4 = time.perf_counter()
+    e2e_s = max_over_ranks(t4 - t0, dist)
+    e2e_parts = dict(upload_s=t1 - t0, search_shapes_s=t2 - t1, steps_s=t3 - t2, download_close_s=t4 - t3)
     h2d = sum(np.asarray(case[k]).nbytes for k in ("coo", "win", "vol", "mass", "ebc", "vinit", "props", "mat_type",
                                                      "body_id", "sm_len"))
     peak, peak_kind = measured_peak()
-    acc = accuracy(case, p, dt, args.full_steps) if args.full_steps > 0 else None
-    lrn = learned_runs(args, rank) if args.rate_h > 0 else None
+    acc = lrn = None
+    try:
+        acc = accuracy(case, p, dt, args.full_steps) if args.full_steps > 0 else None
+    except Exception as ex:  # reported in the JSON line, the timing above stands
+        acc = dict(error=str(ex))
+    try:
+        lrn = learned_runs(args, rank) if args.rate_h > 0 else None
+    except Exception as ex:
+        lrn = dict(error=str(ex))
+    try:
+        pmb = pmb_run(args) if args.pmb_nx > 0 else None
+    except Exception as ex:
+        pmb = dict(error=str(ex))
+    try:
+        batch = batch_run(args) if args.batch_bars > 0 else None
+    except Exception as ex:
+        batch = dict(error=str(ex))
     out = dict(case=case, n=n, nnz=nnz, kmean=kmean, dt=dt, res=res, step0_s=step0_s, e2e_s=e2e_s, h2d=h2d,
-               d2h=d2h, peak=peak, peak_kind=peak_kind, scalars=s, dev_bytes=dev_bytes, accuracy=acc, learned=lrn)
+               d2h=d2h, peak=peak, peak_kind=peak_kind, scalars=s, dev_bytes=dev_bytes, accuracy=acc, learned=lrn, pmb=pmb, batch=batch,
+               e2e_parts=e2e_parts)
     return out
 
 
@@ -244,22 +270,28 @@ RATE_LAW = (90e6, 292e6, 0.31, 0.025, 1.0)  # A, B, n, C, epsdot0 of the power-l
 
 
 def learned_runs(args, rank):
-    """Rate-dependent bar: plain FP64, plain mixed and mixed + learned start
-    from impact for the same steps.  The learned context logs return-mapping
-    samples during the first quarter (plain Newton), trains the network on
-    them on the device, then continues with the learned start; the other
-    two run plain throughout.  Times cover the last three quarters."""
+    """Rate-dependent bar: plain FP64, plain mixed, mixed with the textbook
+    Newton start (perfectly plastic estimate, Newton in dgamma) and mixed +
+    learned start, from impact for the same steps.  The plain solver starts
+    Newton in ln(dgamma) from the upper bound of the multiplier.  The learned
+    context logs return-mapping samples during the first quarter (plain
+    Newton), trains the network on them on the device, then continues with
+    the learned start; the others run plain throughout.  Times cover the last
+    three quarters."""
     from taylor_b200 import _lib, cases, mega
     case = cases.taylor_bar(h=args.rate_h, rate_law=RATE_LAW, seed=7 + rank)
     n = case["n"]
     p = _lib.params(**cases.param_kwargs(case, newton_max_iter=60, newton_rtol=1e-10))
+    p_textbook = _lib.params(**cases.param_kwargs(case, newton_max_iter=60, newton_rtol=1e-10, rate_solver=1))
     total = args.rate_steps
     first = total // 4
     rest = total - first
     runs = {}
     dt = None
-    for name, mode, learn in (("fp64", "fp64", False), ("mixed", "mixed", False), ("mixed_learned", "mixed", True)):
-        m = mega.Mega(case, p)
+    for name, mode, learn, pp in (("fp64", "fp64", False, p), ("mixed", "mixed", False, p),
+                                  ("mixed_textbook_newton", "mixed", False, p_textbook),
+                                  ("mixed_learned", "mixed", True, p)):
+        m = mega.Mega(case, pp)
         m.search_and_shapes()
         if dt is None:
             nb = m.search_and_shapes(download=True)
@@ -268,7 +300,7 @@ def learned_runs(args, rank):
         info = {}
         if learn:
             m.log_rate_samples(cap=10_000_000, stride=4, seed=3)
-        m.step(first, dt, mode=mode)
+        st_first = m.step(first, dt, mode=mode, allow_status=True)
         if learn:
             t0 = time.perf_counter()
             th, loss = m.train_surrogate(mega.mlp_init(5), epochs=6, batch=8192, lr=2e-3, seed=9)
@@ -279,12 +311,16 @@ def learned_runs(args, rank):
         s0 = m.scalars()
         clk = Clocks()
         clk.start()
-        ms = m.step_timed(rest, dt, mode=mode, learned=learn)
+        ms = m.step_timed(rest, dt, mode=mode, learned=learn, allow_status=True)
         info["clocks"] = clk.stop()
+        info["status"] = int(st_first | m.last_status)
         s1 = m.scalars()
         it = s1["newton_iters_total"] - s0["newton_iters_total"]
         pl = s1["plastic_nodes_total"] - s0["plastic_nodes_total"]
-        kt = m.kernel_times(3, dt, mode=mode, learned=learn)
+        try:
+            kt = m.kernel_times(3, dt, mode=mode, learned=learn)
+        except Exception:
+            kt = [float("nan")] * 3
         end = cases.bar_metrics(case, m.download(_lib.F_COO_CURRENT), m.download(_lib.F_EPS))
         m.close()
         info.update(ms_per_step=ms / rest, node_steps_per_s=n * rest / (ms / 1e3), newton_iters=int(it),
@@ -292,15 +328,104 @@ def learned_runs(args, rank):
                     stress_kernel_ms=float(kt[1]), end_state=end)
         runs[name] = info
     ref = runs["fp64"]["end_state"]
-    for name in ("mixed", "mixed_learned"):
+    for name in ("mixed", "mixed_textbook_newton", "mixed_learned"):
         e = runs[name]["end_state"]
         runs[name]["rel_err_vs_fp64"] = {k: abs(e[k] - ref[k]) / abs(ref[k]) for k in ref}
     return dict(workload=f"rate-dependent taylor_bar h={args.rate_h*1e3:.3g}mm", nodes=n, dt=dt, steps=total,
                 timed_steps=rest, rate_law=dict(A=RATE_LAW[0], B=RATE_LAW[1], n=RATE_LAW[2], C=RATE_LAW[3],
                                                 epsdot0=RATE_LAW[4]), newton_rtol=1e-10, runs=runs,
                 mixed_learned_over_fp64=runs["fp64"]["ms_per_step"] / runs["mixed_learned"]["ms_per_step"],
-                iteration_reduction=1.0 - runs["mixed_learned"]["iters_per_plastic_update"]
-                / runs["mixed"]["iters_per_plastic_update"])
+                iteration_reduction_vs_plain=1.0 - runs["mixed_learned"]["iters_per_plastic_update"]
+                / runs["mixed"]["iters_per_plastic_update"],
+                iteration_reduction_vs_textbook=1.0 - runs["mixed_learned"]["iters_per_plastic_update"]
+                / runs["mixed_textbook_newton"]["iters_per_plastic_update"])
+
+
+def pmb_run(args):
+    """Bond-based PMB plate (400 x 400 x 16 particles at 0.25 mm, horizon
+    3.015 h, pre-notch cut on the device): the mixed run (float bond force,
+    double positions) steps the whole job, the FP64 run a tenth of it."""
+    from taylor_b200 import cases, mega
+    nz = max(4, args.pmb_nx // 25)
+    case = cases.pd_plate(nx=args.pmb_nx, ny=args.pmb_nx, nz=nz, notch=20e-3 * args.pmb_nx / 400)
+    n = case["n"]
+    dt = 0.5 * case["h"] / np.sqrt(72e9 / case["rho"])
+    out = dict(workload=f"pmb plate {args.pmb_nx}x{args.pmb_nx}x{nz} h=0.25mm", particles=n, dt=dt)
+    peak, _ = measured_peak()
+    for mode, steps in (("mixed", args.pmb_steps), ("fp64", max(10, args.pmb_steps // 10))):
+        t0 = time.perf_counter()
+        p = mega.Pmb(case, None, mode=mode)
+        init_s = time.perf_counter() - t0
+        ncut = p.cut(*cases.notch_rect(case))
+        p.step(3, dt)
+        clk = Clocks()
+        clk.start()
+        ms = p.step(steps, dt, timed=True)
+        clocks = clk.stop()
+        _, nbroken = p.download(3)
+        bonds = p.nnz
+        # per step: bond column index and broken bit; per particle u in/out,
+        # velocity and acceleration read+write, X, volume, fixity
+        algo = bonds * (4 + 1 / 8) + n * (24 + 24 + 48 + 48 + 24 + 8 + 1)
+        gbs = algo / (ms / steps / 1e3) / 1e9
+        out[mode] = dict(steps=steps, ms_per_step=ms / steps, particle_steps_per_s=n * steps / (ms / 1e3),
+                         bonds=bonds, notch_bonds=ncut, broken_bond_entries=nbroken, init_s=init_s,
+                         roofline=dict(bound="hbm", achieved=gbs, peak=peak, unit="GB/s", frac=gbs / peak,
+                                       algorithmic_bytes_per_step=algo),
+                         clocks=clocks)
+        p.close()
+    return out
+
+
+def batch_run(args):
+    """Many bars of uneven size (spacing uniform in 0.15-0.6 mm, v0 in
+    100-300 m/s, sigma_y in 200-600 MPa, H = 100 MPa, one seed) stepped as
+    one context, every step one CUDA-graph replay over all bars, against the
+    same bars stepped one context after another.  Mixed precision; every
+    bar takes the smallest bar's stable step (0.5 x 0.9 h_min / c, 0.9 h the
+    closest two nodes of the +-5 % jittered lattice can be)."""
+    from taylor_b200 import _lib, cases, mega
+    b = cases.batch_bars(args.batch_bars)
+    n = b["n"]
+    p = _lib.params(**cases.param_kwargs(b, dist_max=tuple(float(v) for v in b["dist_max"].max(axis=0)),
+                                         ql_len=b["ql_len"]))
+    pr = b["props"][0]
+    E, nu, rho = pr[1], pr[0], pr[2]
+    K, G = E / (3.0 * (1.0 - 2.0 * nu)), E / (2.0 * (1.0 + nu))
+    dt = 0.5 * 0.9 * b["h"] / np.sqrt((K + 4.0 * G / 3.0) / rho)
+    K_steps = args.batch_steps
+    t0 = time.perf_counter()
+    m = mega.Mega(b, p)
+    m.set_instances(b["counts"], b["dist_max"])
+    m.set_precisions(fp64=False, mixed=True)
+    m.search_and_shapes()
+    init_s = time.perf_counter() - t0
+    m.step(3, dt, mode="mixed")
+    clk = Clocks()
+    clk.start()
+    ms = m.step_timed(K_steps, dt, mode="mixed")
+    clocks = clk.stop()
+    dev_bytes = m.device_bytes()
+    m.close()
+    seq_ms = 0.0
+    t0 = time.perf_counter()
+    for k, bar in enumerate(b["bars"]):
+        pk = _lib.params(**cases.param_kwargs(bar, dist_max=tuple(float(v) for v in b["dist_max"][k]),
+                                              ql_len=b["ql_len"]))
+        s = mega.Mega(bar, pk)
+        s.set_precisions(fp64=False, mixed=True)
+        s.search_and_shapes()
+        s.step(3, dt, mode="mixed")
+        seq_ms += s.step_timed(K_steps, dt, mode="mixed")
+        s.close()
+    seq_wall = time.perf_counter() - t0
+    return dict(workload=f"{args.batch_bars} Taylor bars, h in 0.15-0.6 mm", bars=args.batch_bars, nodes=n,
+                nodes_min=int(b["counts"].min()), nodes_max=int(b["counts"].max()), dt=dt, steps=K_steps,
+                batched=dict(ms_per_step=ms / K_steps, node_steps_per_s=n * K_steps / (ms / 1e3), init_s=init_s,
+                             device_bytes=dev_bytes, clocks=clocks),
+                sequential=dict(ms_per_step=seq_ms / K_steps, node_steps_per_s=n * K_steps / (seq_ms / 1e3),
+                                wall_s_with_init=seq_wall),
+                batched_over_sequential=seq_ms / ms)
 
 
 def _held_count(m):
@@ -399,10 +524,11 @@ def main():
         fp64_value=fp64_value, fp64_ms_per_step=f64["ms"] / K, mixed_over_fp64=value / fp64_value,
         roofline=roof, cpu_baseline=cpu,
         e2e=dict(value=e2e_val, unit=UNIT, h2d_bytes_per_step=r["h2d"] / K, d2h_bytes_per_step=r["d2h"] / K,
-                 note="model upload + step 0 + K steps with per-step scalar readback + end-state download"),
+                 note="model upload + step 0 + K steps with per-step scalar readback + end-state download",
+                 parts=r["e2e_parts"]),
         gpu_launches=mix["launches"], clocks=mix["clocks"], clocks_fp64=f64["clocks"],
         newton_iters_last_step=r["scalars"]["newton_iters"], plastic_nodes_last_step=r["scalars"]["plastic_nodes"],
-        accuracy=r["accuracy"], learned=r["learned"])
+        accuracy=r["accuracy"], learned=r["learned"], peridynamics=r["pmb"], batch=r["batch"])
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

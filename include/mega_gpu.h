@@ -123,7 +123,9 @@ typedef struct mega_params {
   int32_t inv3_exact;      /* 0 = reproduce INV3 as written (det^2 * A^-1,
                               INVERSE.F90:119-152); 1 = true 3x3 inverse      */
   int32_t newton_max_iter; /* return-mapping iteration cap; 20 in the reference */
-  int32_t reserved0;
+  int32_t rate_solver;      /* material 7 return mapping: 0 Newton in ln(dgamma) from
+                                the upper bound (default), 1 textbook: Newton in dgamma
+                                from the perfectly plastic estimate */
   double  ql_coef;         /* QL_COEF                                         */
   double  ql_len;          /* QL_LEN                                          */
   double  gravity[3];      /* IGRAVITY                                        */
@@ -253,6 +255,22 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo,
                   const double* bodyforce, const double* sm_len,
                   int64_t* handle);
 
+/* Declare that the context's n nodes are ninst independent instances (for
+ * example many bars stepped together), instance k owning the next
+ * inst_nodes[k] nodes.  Call before mega_search_and_shapes: each instance is
+ * then searched with its own bin grid (dist_max (3,ninst) its DIST_MAX, or
+ * NULL for the params' value) and sees no other instance's nodes, so
+ * instances may overlap in space; its lists equal those of a search of the
+ * instance alone.  The other params (QL length among them) are shared.
+ * Energies and reaction sums in mega_get_scalars are totals over all
+ * instances. */
+int mega_set_instances(int64_t h, int32_t ninst, const int32_t* inst_nodes, const double* dist_max);
+/* Precisions the context will step: mask bit 0 FP64, bit 1 mixed (default
+ * 3).  Call before mega_search_and_shapes; only the asked-for packed records
+ * are built (the FP64 records are 32 B per list entry, the mixed 16 B).
+ * Stepping a precision that was not built returns MEGA_ERR_STATE. */
+int mega_set_precisions(int64_t h, int32_t mask);
+
 /* Step 0 (LINIT): neighbour search and RK shapes on the device.  Optional
  * downloads (any pointer may be NULL): gn, gstart, gstack (1-based; gstack
  * sized dim_nn_list), shp (nnz), dshp (3,nnz). *nnz and *gmaxn returned. */
@@ -290,10 +308,11 @@ int64_t mega_kernel_launches(int64_t h);
 /* ======================================================================== */
 /* Surrogate start of the rate-dependent return mapping (material 7; no    */
 /* reference counterpart).  A 4 -> 64 -> 64 -> 1 tanh perceptron predicts   */
-/* the converged plastic multiplier as a fraction y of the perfectly        */
-/* plastic estimate f_trial / (2 mu); Newton then starts at                 */
-/* clamp(y, 0.02, 1) f_trial / (2 mu) instead of at the estimate itself,    */
-/* and converges to the same tolerance.  Parameters theta (4545 floats)     */
+/* the converged plastic multiplier as a fraction y of its upper bound     */
+/* ub = min(f / (2 mu), ((eps^n + f / (sqrt(2/3) B))^(1/n) - eps) /         */
+/* sqrt(2/3)), where the plain solver starts; the Newton iteration (in      */
+/* ln dgamma) then starts at clamp(y, 1e-3, 1) ub instead and converges to  */
+/* the same tolerance.  Parameters theta (4545 floats)                      */
 /* packed [W1 (64x4), b1 (64), W2 (64x64), b2 (64), W3 (64), b3], weights   */
 /* row-major (output, input).  Features of a plastic node, with q the      */
 /* trial deviatoric norm, sy0 = A + B eps^n, f = q - sqrt(2/3) sy0:         */
@@ -356,6 +375,10 @@ int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms);
 /* what: 0 displacement (3,n), 1 velocity, 2 acceleration, 3 broken flags (nnz);
  * *nbroken = bond copies broken so far (each bond breaks at both ends). */
 int mega_pmb_download(int64_t h, int32_t what, double* dst, int64_t* nbroken);
+/* Pre-crack on the device: break every bond whose reference segment crosses
+ * the rectangle corner + s edge_a + t edge_b (0 <= s, t <= 1), each a
+ * double[3]; *ncut = list entries newly broken (may be NULL). */
+int mega_pmb_cut(int64_t h, const double* corner, const double* edge_a, const double* edge_b, int64_t* ncut);
 int mega_pmb_finalize(int64_t h);
 
 const char* mega_status_string(int32_t status);

@@ -405,7 +405,7 @@ int von_mises(double stress[6], const double spred[6], double state[20], const d
 // |f| <= rtol * sqrt(2/3)*sigma_y.  Starts from dg0 (< 0: the elastic-
 // perfectly-plastic guess f_tr / (2 mu)).  Returns Newton passes.
 int vm_rate(double stress[6], const double spred[6], double state[20], const double* props,
-            double dt, double rtol, int maxit, double dg0, bool* capped, double* dg_out) {
+            double dt, double rtol, int maxit, int solver, double dg0, bool* capped, double* dg_out) {
   double poiss = props[0], young = props[1];
   double A = props[3], Bh = props[4], n = props[5], C = props[6], ed0 = props[7];
   double mu = shear_mod(young, poiss);
@@ -430,21 +430,67 @@ int vm_rate(double stress[6], const double spred[6], double state[20], const dou
   int iters = 0;
   double dg = 0.0;
   if (f0 > 0.0) {
-    double lo = 0.0, hi = tn / (2.0 * mu);
-    dg = (dg0 >= 0.0) ? dg0 : f0 / (2.0 * mu);
-    if (!(dg > lo && dg < hi)) dg = 0.5 * (lo + hi);
+    // f(dg) = tn - 2 mu dg - sqrt(2/3) sy(dg) decreases in dg.  Two upper
+    // bounds of the root (sy >= A + B (eps0 + sqrt(2/3) dg)^n because the
+    // rate factor is >= 1, and 2 mu dg >= 0): the perfectly plastic
+    // multiplier and the pure power-law one; start at the smaller.
+    // solver 1 (textbook, for comparison): Newton in dg from the perfectly
+    // plastic estimate, bracket [0, tn / (2 mu)], arithmetic bisection.
+    const bool textbook = solver == 1;
+    double hi = f0 / (2.0 * mu);
+    if (Bh > 0.0) {
+      const double epn0 = (eps0 > 0.0) ? std::pow(eps0, n) : 0.0;
+      const double pw = (std::pow(epn0 + f0 / (s23 * Bh), 1.0 / n) - eps0) / s23;
+      if (pw > 0.0 && pw < hi) hi = pw;
+    }
+    if (textbook) hi = tn / (2.0 * mu);
+    double lo = 0.0;
+    dg = (dg0 >= 0.0) ? dg0 : (textbook ? f0 / (2.0 * mu) : hi);
+    if (textbook ? !(dg > lo && dg < hi) : !(dg > lo && dg <= hi)) dg = textbook ? 0.5 * (lo + hi) : hi;
+    // Newton in y = ln(dg): f is concave in y, so from the right of the root
+    // the iterates decrease monotonically onto it; dg > 0 always.  The
+    // bracket guards the start from the left; outside it, bisect in y.
     bool conv = false;
-    for (int i = 1; i <= maxit; ++i) {
-      ++iters;
-      double ds;
-      double sy = sigy(dg, &ds);
-      double f = tn - 2.0 * mu * dg - s23 * sy;
-      if (std::fabs(f) <= rtol * s23 * sy) { conv = true; break; }
-      if (f > 0.0) lo = dg; else hi = dg;
-      double df = -2.0 * mu - s23 * ds;
-      double nd = dg - f / df;
-      if (!(nd > lo && nd < hi) || !std::isfinite(nd)) nd = 0.5 * (lo + hi);
-      dg = nd;
+    if (textbook) {
+      for (int i = 1; i <= maxit; ++i) {
+        ++iters;
+        double ds;
+        double sy = sigy(dg, &ds);
+        double f = tn - 2.0 * mu * dg - s23 * sy;
+        if (std::fabs(f) <= rtol * s23 * sy) { conv = true; break; }
+        if (f > 0.0) lo = dg; else hi = dg;
+        double df = -2.0 * mu - s23 * ds;
+        double nd = dg - f / df;
+        if (!(nd > lo && nd < hi) || !std::isfinite(nd)) nd = 0.5 * (lo + hi);
+        const bool stalled = std::fabs(nd - dg) <= 4.0e-16 * dg;  // below the rounding of dg
+        dg = nd;
+        if (stalled) { conv = true; break; }
+      }
+    } else {
+      // the iterate is y = ln(dg); ln(epsdot / epsdot0) = y - ythr, and
+      // eps^n = exp(n ln eps)
+      const double ythr = std::log(ed0 * dt / s23);
+      double y = std::log(dg), ylo = -INFINITY, yhi = std::log(hi);
+      for (int i = 1; i <= maxit; ++i) {
+        ++iters;
+        const double ep = eps0 + s23 * dg;
+        const double epn = std::exp(n * std::log(ep));
+        const double depn = n * epn / ep * s23;
+        double rate = 1.0, drate = 0.0;
+        if (y > ythr) { rate = 1.0 + C * (y - ythr); drate = C / dg; }
+        const double sy = A + Bh * epn * rate;
+        const double f = tn - 2.0 * mu * dg - s23 * sy;
+        if (std::fabs(f) <= rtol * s23 * sy) { conv = true; break; }
+        if (f > 0.0) ylo = y; else yhi = y;
+        const double df = -2.0 * mu - s23 * Bh * (depn * rate + epn * drate);
+        double yn = y + std::fmax(std::fmin(-f / (df * dg), 50.0), -50.0);
+        if (!(yn > ylo && yn < yhi) || !std::isfinite(yn))
+          yn = std::isfinite(ylo) ? 0.5 * (ylo + yhi) : yhi - 0.69314718055994530942;  // bisect in y
+        const bool stalled = std::fabs(yn - y) <= 4.0e-16;  // below the rounding of dg
+        y = yn;
+        dg = std::exp(y);
+        if (stalled) { conv = true; break; }
+      }
     }
     if (!conv && capped) *capped = true;
     for (int k = 0; k < 6; ++k) dev[k] = dev[k] - dg * 2.0 * mu * dev[k] / tn;
@@ -474,7 +520,7 @@ void estimate_moduli(const double sinc[6], const double einc[6], double& shear, 
 
 // CONSTITUTION.F90:46-85 dispatch.  status bits as in mega_gpu.h.
 int constitution(const double spred[6], int mat, const double* props, double dlt, double state[20],
-                 double stress[6], int maxit, double rtol, int* status, int* iters_out) {
+                 double stress[6], int maxit, double rtol, int* status, int* iters_out, int solver = 0) {
   int it = 0;
   bool capped = false;
   switch (mat) {
@@ -485,7 +531,7 @@ int constitution(const double spred[6], int mat, const double* props, double dlt
       it = von_mises(stress, spred, state, props, maxit, &capped);
       break;
     case MEGA_MAT_VM_RATE:
-      it = vm_rate(stress, spred, state, props, dlt, rtol, maxit, -1.0, &capped, nullptr);
+      it = vm_rate(stress, spred, state, props, dlt, rtol, maxit, solver, -1.0, &capped, nullptr);
       break;
     default:
       *status |= MEGA_ST_BAD_MATERIAL;
@@ -665,11 +711,11 @@ void orc_rotate_tensor(int n, const double* rot, double* v) {
 }
 
 int orc_constitution(int n, const double* spred, const int* mat, const double* props, double dlt,
-                     double* state, double* stress, int* iters, int maxit, double rtol) {
+                     double* state, double* stress, int* iters, int maxit, double rtol, int solver) {
   int status = 0;
   for (int i = 0; i < n; ++i)
     constitution(spred + 6 * (size_t)i, mat[i], props + 30 * (size_t)i, dlt, state + 20 * (size_t)i,
-                 stress + 6 * (size_t)i, maxit, rtol, &status, iters ? iters + i : nullptr);
+                 stress + 6 * (size_t)i, maxit, rtol, &status, iters ? iters + i : nullptr, solver);
   return status;
 }
 
@@ -677,12 +723,12 @@ int orc_constitution(int n, const double* spred, const int* mat, const double* p
 // guess enters here).  dg0 < 0 selects the plain start.
 int orc_vm_rate(int n, const double* spred, const double* props, double dt, double rtol,
                 int maxit, const double* dg0, double* state, double* stress, int* iters,
-                double* dg_out) {
+                double* dg_out, int solver) {
   int status = 0;
   for (int i = 0; i < n; ++i) {
     bool capped = false;
     int it = vm_rate(stress + 6 * (size_t)i, spred + 6 * (size_t)i, state + 20 * (size_t)i,
-                     props + 30 * (size_t)i, dt, rtol, maxit, dg0 ? dg0[i] : -1.0, &capped,
+                     props + 30 * (size_t)i, dt, rtol, maxit, solver, dg0 ? dg0[i] : -1.0, &capped,
                      dg_out ? dg_out + i : nullptr);
     if (iters) iters[i] = it;
     if (capped) status |= MEGA_ST_NEWTON_CAP;
@@ -799,7 +845,7 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
       }
       int it = 0;
       constitution(spred, gmat[i], lprop, dlt, lstate, lstress, p->newton_max_iter, p->newton_rtol,
-                   &status, &it);
+                   &status, &it, p->rate_solver);
       if (newton_iters) newton_iters[i] = it;
       for (int k = 0; k < 20; ++k) gstate[20 * (size_t)i + k] = lstate[k];   // FINT.F90:809-811
       double sinc[6], einc[6];
@@ -982,7 +1028,7 @@ int orc_construct_fint_pd(const mega_params* p, int n, const double* gcoo, const
         spred[r] = lstress[r] + v;
       }
       constitution(spred, gmat[i], lprop, dlt, lstate, lstress, p->newton_max_iter, p->newton_rtol,
-                   &status, nullptr);
+                   &status, nullptr, p->rate_solver);
       for (int k = 0; k < 20; ++k) gstate[20 * (size_t)i + k] = lstate[k];
       double sinc[6], einc[6];
       for (int k = 0; k < 6; ++k) {                                   // :505-518 (STRAIN_INC uses

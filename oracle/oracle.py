@@ -20,8 +20,8 @@ _SIG = {
     "orc_rk_shapes": (I32, [P, I32, P, P, P, P, P, P, P, P, I32]),
     "orc_hughes_winget": (None, [I32, P, P, P, P, I32]),
     "orc_rotate_tensor": (None, [I32, P, P]),
-    "orc_constitution": (I32, [I32, P, P, P, D, P, P, P, I32, D]),
-    "orc_vm_rate": (I32, [I32, P, P, D, D, I32, P, P, P, P, P]),
+    "orc_constitution": (I32, [I32, P, P, P, D, P, P, P, I32, D, I32]),
+    "orc_vm_rate": (I32, [I32, P, P, D, D, I32, P, P, P, P, P, I32]),
     "orc_construct_fint": (I32, [P, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, I32, D, P, P, P, P,
                                  P, I32, P]),
     "orc_interp": (None, [I32, P, P, P, P, P, P, I32]),
@@ -97,7 +97,7 @@ class Params(C.Structure):
         ("rk_degree", C.c_int32), ("rk_cont", C.c_int32), ("rk_impl", C.c_int32),
         ("itype_int", C.c_int32), ("ql", C.c_int32), ("lagrangian", C.c_int32),
         ("finite_strain", C.c_int32), ("shsup", C.c_int32), ("peridynamics", C.c_int32),
-        ("inv3_exact", C.c_int32), ("newton_max_iter", C.c_int32), ("reserved0", C.c_int32),
+        ("inv3_exact", C.c_int32), ("newton_max_iter", C.c_int32), ("rate_solver", C.c_int32),
         ("ql_coef", C.c_double), ("ql_len", C.c_double), ("gravity", C.c_double * 3),
         ("dist_max", C.c_double * 3), ("newton_rtol", C.c_double),
     ]
@@ -144,18 +144,18 @@ def rotate_tensor(rot, v):
     return v
 
 
-def constitution(spred, mat, props, dlt, state, maxit=20, rtol=1e-10):
+def constitution(spred, mat, props, dlt, state, maxit=20, rtol=1e-10, solver=0):
     spred = f64(spred)
     n = len(spred)
     state = f64(state).copy()
     stress = np.zeros((n, 6))
     it = np.zeros(n, np.int32)
     st = lib().orc_constitution(n, _p(spred), _p(i32(mat)), _p(f64(props)), float(dlt), _p(state), _p(stress),
-                                _p(it), maxit, rtol)
+                                _p(it), maxit, rtol, int(solver))
     return stress, state, it, st
 
 
-def vm_rate(spred, props, dt, state, dg0=None, rtol=1e-10, maxit=50):
+def vm_rate(spred, props, dt, state, dg0=None, rtol=1e-10, maxit=50, solver=0):
     spred = f64(spred)
     n = len(spred)
     state = f64(state).copy()
@@ -163,7 +163,8 @@ def vm_rate(spred, props, dt, state, dg0=None, rtol=1e-10, maxit=50):
     it = np.zeros(n, np.int32)
     dg = np.zeros(n)
     st = lib().orc_vm_rate(n, _p(spred), _p(f64(props)), float(dt), float(rtol), int(maxit),
-                           _p(None if dg0 is None else f64(dg0)), _p(state), _p(stress), _p(it), _p(dg))
+                           _p(None if dg0 is None else f64(dg0)), _p(state), _p(stress), _p(it), _p(dg),
+                           int(solver))
     return stress, state, it, dg, st
 
 

@@ -40,7 +40,7 @@ class MegaParams(C.Structure):
         ("rk_degree", C.c_int32), ("rk_cont", C.c_int32), ("rk_impl", C.c_int32),
         ("itype_int", C.c_int32), ("ql", C.c_int32), ("lagrangian", C.c_int32),
         ("finite_strain", C.c_int32), ("shsup", C.c_int32), ("peridynamics", C.c_int32),
-        ("inv3_exact", C.c_int32), ("newton_max_iter", C.c_int32), ("reserved0", C.c_int32),
+        ("inv3_exact", C.c_int32), ("newton_max_iter", C.c_int32), ("rate_solver", C.c_int32),
         ("ql_coef", C.c_double), ("ql_len", C.c_double), ("gravity", C.c_double * 3),
         ("dist_max", C.c_double * 3), ("newton_rtol", C.c_double),
     ]
@@ -75,6 +75,8 @@ SIGNATURES = {
                                      I32, D, P, P, P]),
     "mega_gpu_init": (I32, [PP, I32, P, P, P, P, P, P, P, P, P, P, P, C.POINTER(I64)]),
     "mega_search_and_shapes": (I32, [I64, P, P, P, I64, P, P, P, P]),
+    "mega_set_instances": (I32, [I64, I32, P, P]),
+    "mega_set_precisions": (I32, [I64, I32]),
     "mega_step_resident": (I32, [I64, I32, D, I32]),
     "mega_step_timed": (I32, [I64, I32, D, I32, C.POINTER(F32)]),
     "mega_kernel_times": (I32, [I64, I32, D, I32, P]),
@@ -86,6 +88,7 @@ SIGNATURES = {
     "mega_pmb_init": (I32, [I32, P, P, P, P, D, D, D, D, P, I32, C.POINTER(I64), C.POINTER(I64)]),
     "mega_pmb_step": (I32, [I64, I32, D, C.POINTER(F32)]),
     "mega_pmb_download": (I32, [I64, I32, P, C.POINTER(I64)]),
+    "mega_pmb_cut": (I32, [I64, P, P, P, C.POINTER(I64)]),
     "mega_pmb_finalize": (I32, [I64]),
     "mega_mlp_nparams": (I32, [I32]),
     "mega_mlp_grad": (I32, [I32, P, I64, P, P, P, P]),

@@ -110,6 +110,31 @@ def bar_metrics(case, coo_cur, eps):
                 peak_eps=float(np.max(eps)))
 
 
+def batch_bars(nbars=256, seed=5, h_range=(0.15e-3, 0.6e-3), v0_range=(100.0, 300.0), sy_range=(200e6, 600e6),
+               H=100e6, **bar):
+    """Many Taylor bars of uneven size stepped as one batch: instance k has
+    lattice spacing h_k, impact speed v0_k and yield stress sy_k drawn
+    uniformly from the ranges (one seed), linear hardening H.  The bars keep
+    their own coordinates (they overlap in space; each is searched alone).
+    Returns the concatenated case with `counts`, per-instance `dist_max`
+    (nbars, 3), `params` (h, v0, sy) and the instances themselves."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    hs = rng.uniform(*h_range, nbars)
+    v0s = rng.uniform(*v0_range, nbars)
+    sys_ = rng.uniform(*sy_range, nbars)
+    bars = [taylor_bar(h=float(hs[k]), v0=float(v0s[k]), sy=float(sys_[k]), H=H, seed=seed * 1000 + k, **bar)
+            for k in range(nbars)]
+    keys = ("coo", "win", "win_raw", "vol", "mass", "ebc", "vinit", "props", "mat_type", "body_id", "sm_len", "wall",
+            "layer")
+    out = {k: np.concatenate([b[k] for b in bars]) for k in keys}
+    out.update(name=f"batch_{nbars}_bars", n=int(sum(b["n"] for b in bars)), bodyforce=None,
+               counts=np.array([b["n"] for b in bars], np.int32),
+               dist_max=np.stack([b["dist_max"] for b in bars]),
+               ql_len=float(min(b["ql_len"] for b in bars)), params=np.stack([hs, v0s, sys_], axis=1), bars=bars,
+               h=float(hs.min()))
+    return out
+
+
 def param_kwargs(case, **over):
     """mega_params values for a case (Control.dat defaults: RK 1/3/0, QL 1
     0.001, DNI, Lagrangian finite strain, box support)."""
@@ -192,6 +217,15 @@ def notch_broken(case, gn, gstart, gstack):
     t = (case["ymid"] - yi) / np.where(yj != yi, yj - yi, 1.0)
     xc = coo[rows, 0] + t * (coo[cols, 0] - coo[rows, 0])
     return (cross & (xc < case["notch"])).astype(np.uint8)
+
+
+def notch_rect(case):
+    """The pre-notch of notch_broken as a cut rectangle (corner, edge a, edge
+    b) for the device cut: plane y = ymid, x up to the notch length, through
+    the whole thickness."""
+    zmax = float(np.max(case["coo"][:, 2]))
+    corner = np.array([-1.0, case["ymid"], -1.0])
+    return corner, np.array([case["notch"] + 1.0, 0.0, 0.0]), np.array([0.0, 0.0, zmax + 2.0])
 
 
 def case_a(npz):

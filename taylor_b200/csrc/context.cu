@@ -2,7 +2,10 @@
 // MAIN.F90:304-658 time loop on the device, captured in CUDA graphs) and the
 // copy-in/copy-out drop-ins for the reference's subroutines.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -63,7 +66,7 @@ __global__ void k_rotate(int32_t n, const double* __restrict__ rot, double* __re
   for (int k = 0; k < 6; ++k) v[6 * i + k] = s[k];
 }
 __global__ void k_constitution(int32_t n, const double* __restrict__ spred, const int32_t* __restrict__ mat,
-                               const double* __restrict__ props, double dlt, int maxit, double rtol,
+                               const double* __restrict__ props, double dlt, int maxit, int solver, double rtol,
                                double* __restrict__ state, double* __restrict__ stress, int32_t* __restrict__ iters,
                                unsigned* __restrict__ status) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -83,7 +86,7 @@ __global__ void k_constitution(int32_t n, const double* __restrict__ spred, cons
     it = von_mises(sp, ep, m, maxit, out, cap);
   } else if (m.type == MEGA_MAT_VM_RATE) {
     double dg, ftr;
-    it = vm_rate(sp, ep, m, dlt, rtol, maxit, -1.0, out, cap, dg, ftr);
+    it = vm_rate(sp, ep, m, dlt, rtol, maxit, solver, -1.0, out, cap, dg, ftr);
   } else {
     atomicOr(status, (unsigned)MEGA_ST_BAD_MATERIAL);
     for (int k = 0; k < 6; ++k) out[k] = sp[k];
@@ -184,6 +187,10 @@ struct Ctx {
   double time = 0.0;
   int64_t steps = 0;
   int64_t launches = 0;
+  // independent instances sharing the context (node ranges searched apart)
+  std::vector<int32_t> inst_off;  // ninst + 1 prefix offsets, empty = one instance
+  std::vector<double> inst_dmax;  // 3 per instance: DIST_MAX of its bin grid
+  int prec_mask = 3;              // bit 0: FP64 records built, bit 1: mixed records
   // surrogate of the rate-dependent return mapping and its sample log
   DevPool mlppool;
   float* mlp_theta = nullptr;  // fp32 parameters (training copy)
@@ -201,7 +208,36 @@ struct Ctx {
   int g_len = 0;
   ~Ctx() {
     if (gexec) cudaGraphExecDestroy(gexec);
-    if (s) cudaStreamDestroy(s);
+    // stream-ordered frees first, then the stream
+    mlppool.free_all();
+    mixpool.free_all();
+    nbpool.free_all();
+    pool.free_all();
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+};
+
+// Phase timing of the set-up entry points, printed to stderr when the
+// environment variable MEGA_TRACE is set (each mark synchronises the stream).
+struct PhaseTrace {
+  bool on;
+  cudaStream_t s;
+  const char* what;
+  std::chrono::steady_clock::time_point t0, t;
+  PhaseTrace(cudaStream_t st, const char* w) : on(std::getenv("MEGA_TRACE") != nullptr), s(st), what(w) {
+    t0 = t = std::chrono::steady_clock::now();
+  }
+  void mark(const char* phase) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[mega] %s %-24s %8.3f ms (total %8.3f ms)\n", what, phase,
+                 std::chrono::duration<double, std::milli>(now - t).count(),
+                 std::chrono::duration<double, std::milli>(now - t0).count());
+    t = now;
   }
 };
 
@@ -222,10 +258,10 @@ static int read_status(Ctx* c, bool reset) {
   return (int)st;
 }
 
-static int ensure_mixed(Ctx* c) {
-  (void)c;  // the float records are packed at search time
-  return 0;
-}
+// The records of a precision are packed at search time only when the
+// context's precision mask asks for them.
+static int ensure_mixed(Ctx* c) { return (c->prec_mask & 2) ? 0 : MEGA_ERR_STATE; }
+static int ensure_fp64(Ctx* c) { return (c->prec_mask & 1) ? 0 : MEGA_ERR_STATE; }
 
 static StressArgs stress_args(Ctx* c, double dt, int mode) {
   StressArgs a{};
@@ -234,7 +270,7 @@ static StressArgs stress_args(Ctx* c, double dt, int mode) {
   a.tmat = c->tmat; a.bodyforce = c->bodyforce;
   a.grav[0] = c->p.gravity[0]; a.grav[1] = c->p.gravity[1]; a.grav[2] = c->p.gravity[2];
   a.has_body = c->has_body; a.inv3_exact = c->p.inv3_exact; a.finite_strain = c->p.finite_strain;
-  a.maxit = c->p.newton_max_iter; a.rtol = c->p.newton_rtol; a.dt = dt; a.iters = c->iters;
+  a.maxit = c->p.newton_max_iter; a.rate_solver = c->p.rate_solver; a.rtol = c->p.newton_rtol; a.dt = dt; a.iters = c->iters;
   a.acc = c->acc; a.status = c->status;
   if ((mode & MEGA_FLAG_LEARNED_GUESS) && c->mlp_on) { a.mlp_w2 = c->mlp_w2; a.mlp_small = c->mlp_small; }
   if (c->log_cap > 0) {
@@ -300,7 +336,7 @@ static int run_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
   const int prec = mode & 0xff;
   if (prec != MEGA_MODE_FP64 && prec != MEGA_MODE_MIXED) return MEGA_ERR_ARG;
   if ((mode & MEGA_FLAG_LEARNED_GUESS) && !c->mlp_on) return MEGA_ERR_STATE;
-  if (prec == MEGA_MODE_MIXED) { int r = ensure_mixed(c); if (r) return r; }
+  { int r = (prec == MEGA_MODE_MIXED) ? ensure_mixed(c) : ensure_fp64(c); if (r) return r; }
   if (!(mode & MEGA_FLAG_INTERP_EACH_STEP)) c->phy_valid = false;
   int r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
   if (r) return r;
@@ -410,6 +446,36 @@ static int make_stream(cudaStream_t* s) {
   return 0;
 }
 
+// Contexts and their set-up temporaries allocate from the device's default
+// memory pool; with the release threshold at its maximum, memory a context
+// or a temporary frees stays in the pool and the next allocation reuses it
+// without a driver round trip (it returns to the driver at process exit).
+bool trace_on() {
+  static const bool on = std::getenv("MEGA_TRACE") != nullptr;
+  return on;
+}
+
+void trace_alloc(size_t bytes, double ms, bool ordered) {
+  if (ms > 5.0)
+    std::fprintf(stderr, "[mega] slow %s of %.1f MB: %.3f ms\n", ordered ? "cudaMallocAsync" : "cudaMalloc",
+                 bytes / 1048576.0, ms);
+}
+
+void retain_pool_memory() {
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(dev)) return;
+  cudaMemPool_t mp;
+  if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done.insert(dev);
+}
+
 struct StreamGuard {
   cudaStream_t s = nullptr;
   ~StreamGuard() { if (s) cudaStreamDestroy(s); }
@@ -484,6 +550,11 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   const int64_t n3 = 3 * (int64_t)n;
   auto fail = [&](int code) { delete c; return code; };
   if (r) return fail(r);
+  c->pool.bind(c->s);
+  c->nbpool.bind(c->s);
+  c->mixpool.bind(c->s);
+  c->mlppool.bind(c->s);
+  PhaseTrace tr(c->s, "gpu_init");
 #define CA(ptr, cnt) do { if (c->pool.alloc(&(ptr), (size_t)(cnt))) return fail(MEGA_ERR_NOMEM); } while (0)
   CA(c->coo, n3); CA(c->win, n3); CA(c->vol, n); CA(c->mass, n3); CA(c->sm_len, 6 * (int64_t)n);
   CA(c->ebc, n3); CA(c->body_id, n); CA(c->ebc_nodes, n);
@@ -505,6 +576,7 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
     }
   }
 #undef CA
+  tr.mark("allocate");
   std::vector<int8_t> hebc(n3), hbody(n);
   std::vector<int32_t> hen(n, 0);
   std::vector<double> v0(n3);
@@ -538,8 +610,10 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->s);
   cudaMemsetAsync(c->tmat, 0, sizeof(double) * 12 * n, c->s);
   if (cudaStreamSynchronize(c->s) != cudaSuccess) return fail(MEGA_ERR_CUDA);
+  tr.mark("upload");
   r = build_materials(c, props, mat_type);
   if (r) return fail(r);
+  tr.mark("materials");
   {
     std::lock_guard<std::mutex> lk(g_ctx_mu);
     g_ctxs.insert(c);
@@ -548,11 +622,60 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   return 0;
 }
 
+__global__ void k_offset_i32(int64_t m, const int32_t* __restrict__ src, int32_t add, int32_t* __restrict__ dst) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < m) dst[k] = src[k] + add;
+}
+__global__ void k_offset_i64(int64_t m, const int64_t* __restrict__ src, int64_t add, int64_t* __restrict__ dst) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < m) dst[k] = src[k] + add;
+}
+
+// Instances searched one at a time, each with its own bin grid (their node
+// ranges may overlap in space; no instance sees another's nodes), then their
+// lists merged into one block-diagonal CSR in the global numbering, with the
+// cell orders concatenated into the renumbering.
+static int search_instances(Ctx* c, DevCSR& csr, DevPool& out) {
+  const int K = (int)c->inst_off.size() - 1;
+  DevPool parts_pool(c->s);
+  std::vector<DevCSR> parts(K);
+  std::vector<int64_t> base(K + 1, 0);
+  int32_t gmax = 0;
+  for (int k = 0; k < K; ++k) {
+    const int32_t o = c->inst_off[k], nk = c->inst_off[k + 1] - o;
+    const double* dmax = c->inst_dmax.empty() ? c->p.dist_max : c->inst_dmax.data() + 3 * k;
+    int r = bin_search(c->s, nk, c->coo + 3 * (int64_t)o, c->win + 3 * (int64_t)o, c->sm_len + 6 * (int64_t)o,
+                       dmax, c->p.itype_int, c->p.shsup, c->status, parts[k], nullptr, parts_pool, nullptr,
+                       c->perm + o);
+    if (r) return r;
+    k_offset_i32<<<grid_for(nk, 256), 256, 0, c->s>>>(nk, c->perm + o, o, c->perm + o);
+    MEGA_CHECK_LAUNCH();
+    base[k + 1] = base[k] + parts[k].nnz;
+    gmax = std::max(gmax, parts[k].gmaxn);
+  }
+  const int32_t n = c->n;
+  csr.n = n;
+  csr.nnz = base[K];
+  csr.gmaxn = gmax;
+  MEGA_ALLOC(out, csr.rowptr, (int64_t)n + 1);
+  MEGA_ALLOC(out, csr.col, csr.nnz);
+  for (int k = 0; k < K; ++k) {
+    const int32_t o = c->inst_off[k], nk = c->inst_off[k + 1] - o;
+    // rows 0..nk of the part (its last offset doubles as the next part's first)
+    k_offset_i64<<<grid_for((int64_t)nk + 1, 256), 256, 0, c->s>>>((int64_t)nk + 1, parts[k].rowptr, base[k],
+                                                                    csr.rowptr + o);
+    k_offset_i32<<<grid_for(parts[k].nnz, 256), 256, 0, c->s>>>(parts[k].nnz, parts[k].col, o, csr.col + base[k]);
+    MEGA_CHECK_LAUNCH();
+  }
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  return 0;
+}
+
 // Gather every per-node array through map (dst[r] = src[map[r]]): perm moves
 // the original numbering to the bin-cell numbering, iperm moves it back.
 static int permute_nodes(Ctx* c, const int32_t* map) {
   const int32_t n = c->n;
-  DevPool tp;
+  DevPool tp(c->s);
   unsigned char* tmp = nullptr;
   MEGA_ALLOC(tp, tmp, (int64_t)n * 48);
   struct Arr { void* p; int w; int es; };
@@ -592,14 +715,17 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     c->searched = false;
     if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
   }
+  PhaseTrace tr(c->s, "search_and_shapes");
   // 1. search and shapes in the reference's numbering (what the caller may download)
-  DevPool tmp0;
+  DevPool tmp0(c->s);
   DevCSR csr0;
   MEGA_ALLOC(c->nbpool, c->perm, n);
   MEGA_ALLOC(c->nbpool, c->iperm, n);
-  int r = bin_search(c->s, n, c->coo, c->win, c->sm_len, c->p.dist_max, c->p.itype_int, c->p.shsup, c->status, csr0,
-                     nullptr, tmp0, nullptr, c->perm);
+  int r = (c->inst_off.size() > 2) ? search_instances(c, csr0, tmp0)
+                                   : bin_search(c->s, n, c->coo, c->win, c->sm_len, c->p.dist_max, c->p.itype_int,
+                                                c->p.shsup, c->status, csr0, nullptr, tmp0, nullptr, c->perm);
   if (r) return r;
+  tr.mark("bin_search");
   const int64_t m = csr0.nnz;
   double *shp0, *g0x, *g0y, *g0z;
   MEGA_ALLOC(tmp0, shp0, m);
@@ -608,6 +734,7 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   MEGA_ALLOC(tmp0, g0z, m);
   r = rk_shapes(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr0, shp0, g0x, g0y, g0z, c->status);
   if (r) return r;
+  tr.mark("rk_shapes");
   int st = 0;
   if (gn || gstart || gstack || shp || dshp) {
     std::vector<int64_t> rp(n + 1);
@@ -636,12 +763,13 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     }
     MEGA_TRY(cudaStreamSynchronize(c->s));
   }
+  tr.mark("downloads");
   // 2. renumber the nodes in bin-cell order (spatially compact rows and tiles)
   k_iperm<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->perm, c->iperm);
   MEGA_CHECK_LAUNCH();
   r = permute_nodes(c, c->perm);
   if (r) return r;
-  DevPool tmp1;
+  DevPool tmp1(c->s);
   int32_t* len1;
   MEGA_ALLOC(tmp1, len1, n);
   c->csr.n = n;
@@ -664,13 +792,16 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   MEGA_CHECK_LAUNCH();
   MEGA_TRY(cudaStreamSynchronize(c->s));
   tmp0.free_all();
+  tr.mark("renumber");
   // 3. transposed view, tiles, packed records
   r = configure_tiled_kernels();
   if (r) return r;
   r = build_transpose(c->s, c->csr, c->nbpool);
   if (r) return r;
+  tr.mark("transpose");
   r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->rt, c->nbpool, nullptr);
   if (r) return r;
+  tr.mark("row_tiles");
   int32_t cmax = 0;
   {
     // the longest column bounds a column tile's set from below
@@ -681,30 +812,33 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   }
   r = build_tiles(c->s, n, c->csr.colptr, c->csr.trow, m, cmax, c->ct, c->nbpool, nullptr);
   if (r) return r;
-  {
+  tr.mark("column_tiles");
+  if (c->prec_mask & 1) {
     double *a = nullptr, *b = nullptr;  // 4 doubles per entry
     MEGA_ALLOC(c->nbpool, a, 4 * m);
     MEGA_ALLOC(c->nbpool, b, 4 * m);
     c->pk64 = a;
     c->tpk64 = b;
+    if ((r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, true, c->pk64)) ||
+        (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, true, c->tpk64)))
+      return r;
+    MEGA_ALLOC(c->nbpool, c->sdphi, 3 * (int64_t)n);
+    k_rowsum3<double><<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, g1x, g1y, g1z, c->sdphi);
+    MEGA_CHECK_LAUNCH();
   }
-  {
+  if (c->prec_mask & 2) {
     float4 *a = nullptr, *b = nullptr;
     MEGA_ALLOC(c->nbpool, a, m);
     MEGA_ALLOC(c->nbpool, b, m);
     c->pk32 = a;
     c->tpk32 = b;
+    if ((r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, false, c->pk32)) ||
+        (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, false, c->tpk32)))
+      return r;
+    MEGA_ALLOC(c->nbpool, c->sdphi32, 3 * (int64_t)n);
+    k_rowsum_pk32<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, (const float4*)c->pk32, c->sdphi32);
+    MEGA_CHECK_LAUNCH();
   }
-  if ((r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, true, c->pk64)) ||
-      (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, true, c->tpk64)) ||
-      (r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, false, c->pk32)) ||
-      (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, false, c->tpk32)))
-    return r;
-  MEGA_ALLOC(c->nbpool, c->sdphi, 3 * (int64_t)n);
-  MEGA_ALLOC(c->nbpool, c->sdphi32, 3 * (int64_t)n);
-  k_rowsum3<double><<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, g1x, g1y, g1z, c->sdphi);
-  k_rowsum_pk32<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, (const float4*)c->pk32, c->sdphi32);
-  MEGA_CHECK_LAUNCH();
   if (c->has_body) {
     MEGA_ALLOC(c->nbpool, c->tshp, m);
     k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->csr.tpos, c->shp, c->tshp);
@@ -717,6 +851,7 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   c->csr.trow = nullptr;
   c->csr.tpos = nullptr;
   tmp1.free_all();
+  tr.mark("pack_and_release");
   c->searched = true;
   if (nnz) *nnz = m;
   if (gmaxn) *gmaxn = c->csr.gmaxn;
@@ -736,7 +871,7 @@ int mega_step_resident(int64_t h, int32_t nsteps, double dt, int32_t mode) {
 int mega_step_timed(int64_t h, int32_t nsteps, double dt, int32_t mode, float* ms) {
   Ctx* c = get_ctx(h);
   if (!c || !ms) return c ? MEGA_ERR_ARG : MEGA_ERR_HANDLE;
-  if (c->searched && (mode & 0xff) == MEGA_MODE_MIXED) { int r = ensure_mixed(c); if (r) return r; }
+  if (c->searched) { int r = ((mode & 0xff) == MEGA_MODE_MIXED) ? ensure_mixed(c) : ensure_fp64(c); if (r) return r; }
   if (c->searched && nsteps > 16) { int r = graph_for(c, dt, mode, 16); if (r) return r; }
   cudaEvent_t e0, e1;
   MEGA_TRY(cudaEventCreate(&e0));
@@ -758,7 +893,7 @@ int mega_kernel_times(int64_t h, int32_t reps, double dt, int32_t mode, float* o
   Ctx* c = get_ctx(h);
   if (!c || !out_ms || reps <= 0) return c ? MEGA_ERR_ARG : MEGA_ERR_HANDLE;
   if (!c->searched) return MEGA_ERR_STATE;
-  if ((mode & 0xff) == MEGA_MODE_MIXED) { int r = ensure_mixed(c); if (r) return r; }
+  { int r = ((mode & 0xff) == MEGA_MODE_MIXED) ? ensure_mixed(c) : ensure_fp64(c); if (r) return r; }
   if (!(mode & MEGA_FLAG_INTERP_EACH_STEP)) c->phy_valid = false;
   cudaEvent_t ev[4];
   for (auto& e : ev) MEGA_TRY(cudaEventCreate(&e));
@@ -791,7 +926,7 @@ static int download_nodes(Ctx* c, const void* src, int w, int es, void* dst) {
     MEGA_TRY(cudaStreamSynchronize(c->s));
     return 0;
   }
-  DevPool tp;
+  DevPool tp(c->s);
   unsigned char* tmp = nullptr;
   MEGA_ALLOC(tp, tmp, bytes);
   k_perm_gather<<<grid_for((int64_t)n * w, 256), 256, 0, c->s>>>(n, w, es, c->iperm, (const unsigned char*)src, tmp);
@@ -876,7 +1011,7 @@ int mega_upload(int64_t h, int32_t field, const double* src) {
     MEGA_TRY(cudaStreamSynchronize(c->s));
     return 0;
   }
-  DevPool tp;
+  DevPool tp(c->s);
   unsigned char* tmp = nullptr;
   MEGA_ALLOC(tp, tmp, bytes);
   MEGA_TRY(cudaMemcpyAsync(tmp, src, bytes, cudaMemcpyHostToDevice, c->s));
@@ -916,6 +1051,31 @@ int64_t mega_kernel_launches(int64_t h) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
   return c->launches;
+}
+
+int mega_set_instances(int64_t h, int32_t ninst, const int32_t* inst_nodes, const double* dist_max) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (ninst < 1 || !inst_nodes) return MEGA_ERR_ARG;
+  std::vector<int32_t> off(ninst + 1, 0);
+  for (int32_t k = 0; k < ninst; ++k) {
+    if (inst_nodes[k] <= 0) return MEGA_ERR_ARG;
+    off[k + 1] = off[k] + inst_nodes[k];
+  }
+  if (off[ninst] != c->n) return MEGA_ERR_ARG;
+  c->inst_off = off;
+  c->inst_dmax.clear();
+  if (dist_max) c->inst_dmax.assign(dist_max, dist_max + 3 * (size_t)ninst);
+  return 0;
+}
+
+int mega_set_precisions(int64_t h, int32_t mask) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (mask < 1 || mask > 3) return MEGA_ERR_ARG;
+  if (c->searched && (mask & ~c->prec_mask)) return MEGA_ERR_STATE;  // records not built
+  c->prec_mask = mask;
+  return 0;
 }
 
 static void drop_graph(Ctx* c) {
@@ -1172,7 +1332,8 @@ int mega_constitution(const mega_params* p, int32_t n, const double* stress_pred
       (r = upload(sg.s, dst, state, 20 * (size_t)n)) || (r = upload(sg.s, dm, mat_type, (size_t)n)))
     return r;
   MEGA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), sg.s));
-  k_constitution<<<grid_for(n, 128), 128, 0, sg.s>>>(n, dp, dm, dprop, dlt, p->newton_max_iter, p->newton_rtol, dst,
+  k_constitution<<<grid_for(n, 128), 128, 0, sg.s>>>(n, dp, dm, dprop, dlt, p->newton_max_iter, p->rate_solver,
+                                                     p->newton_rtol, dst,
                                                      dsig, dit, st);
   MEGA_CHECK_LAUNCH();
   unsigned hst = 0;
@@ -1290,7 +1451,7 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   a.strain_eq = deq; a.wvel = dwv; a.tmat = dT; a.bodyforce = dbf;
   a.grav[0] = p->gravity[0]; a.grav[1] = p->gravity[1]; a.grav[2] = p->gravity[2];
   a.has_body = has_body; a.inv3_exact = p->inv3_exact; a.finite_strain = p->finite_strain;
-  a.maxit = p->newton_max_iter; a.rtol = p->newton_rtol; a.dt = dlt; a.acc = acc; a.status = st;
+  a.maxit = p->newton_max_iter; a.rate_solver = p->rate_solver; a.rtol = p->newton_rtol; a.dt = dlt; a.acc = acc; a.status = st;
   r = launch_stress(s, false, a);
   if (r) return r;
   DevCSR* dcsr;

@@ -131,21 +131,28 @@ __device__ __forceinline__ T block_sum(T v, T* sm) {
 
 // State of one node between the trial part of the update (kinematics,
 // rotation, elastic predictor) and the rest (return mapping, write-back).
-template <typename T>
+// LEAN: the old stress / strain and the material entry are re-read by the
+// second part instead of held (the members stay unused and take no
+// registers), which keeps the state small across the learned kernel's
+// network evaluation.
+template <typename T, bool LEAN>
 struct Trial {
-  double spred[6], sold[6], eold[6];
+  double spred[6];
   T eps6[6], D[6], IF[3][3];
-  double det, vol;
+  double det;
+  int mi;  // material table index
+  double sold[6], eold[6];
   MatEntry me;
 };
 
 // FINT.F90:363-794: |det F|, INV3(F), L = G0 INV3(F), Hughes-Winget, rotation
 // of sigma and eps, eps += dstrain, elastic predictor.
-template <typename T>
-__device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Trial<T>& w) {
+template <typename T, bool LEAN>
+__device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Trial<T, LEAN>& w) {
   const double* fgi = a.fg + 18 * i;
-  w.me = a.mats[a.matidx[i]];
-  w.vol = a.vol[i];
+  w.mi = a.matidx[i];
+  if (!LEAN) w.me = a.mats[w.mi];
+  const MatEntry& me = LEAN ? a.mats[w.mi] : w.me;
   T G0[3][3], L[3][3], sig[6], dstr[6];
 #pragma unroll
   for (int k = 0; k < 3; ++k)
@@ -154,10 +161,10 @@ __device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Tri
   w.det = 1.0;
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    w.sold[k] = a.stress[6 * i + k];
-    w.eold[k] = a.strain[6 * i + k];
-    sig[k] = (T)w.sold[k];
-    w.eps6[k] = (T)w.eold[k];
+    const double so = a.stress[6 * i + k], eo = a.strain[6 * i + k];
+    if (!LEAN) { w.sold[k] = so; w.eold[k] = eo; }
+    sig[k] = (T)so;
+    w.eps6[k] = (T)eo;
     w.D[k] = T(0);
   }
   if (a.finite_strain) {
@@ -191,7 +198,7 @@ __device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Tri
 #pragma unroll
   for (int k = 0; k < 6; ++k) w.eps6[k] = w.eps6[k] + dstr[k];
   // elastic predictor with FORM_CMAT (FINT_FUNCTIONS.F90:252-288)
-  const T lam = (T)w.me.lam, mu = (T)w.me.mu, l2m = (T)w.me.l2m;
+  const T lam = (T)me.lam, mu = (T)me.mu, l2m = (T)me.l2m;
   w.spred[0] = (double)(sig[0] + (l2m * dstr[0] + lam * dstr[1] + lam * dstr[2]));
   w.spred[1] = (double)(sig[1] + (lam * dstr[0] + l2m * dstr[1] + lam * dstr[2]));
   w.spred[2] = (double)(sig[2] + (lam * dstr[0] + lam * dstr[1] + l2m * dstr[2]));
@@ -206,9 +213,10 @@ __device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Tri
 //   x1 = eps0^n                             hardening state
 //   x2 = ln(max(sqrt(2/3) f/(2 mu)/dt, epsdot0)/epsdot0) / 10   rate
 //   x3 = 1e3 sqrt(2/3) sy0 / (2 mu)          yield-strain scale
-// The target is y = dgamma / (f / (2 mu)).  Returns f (<= 0: elastic).
+// The target is y = dgamma / ub with ub = rate_upper_bound(f, eps0).
+// Returns f (<= 0: elastic) and ub.
 __device__ __forceinline__ double rate_features(const double spred[6], double eps0, const MatEntry& me, double dt,
-                                                float x[4], double& dgpp) {
+                                                float x[4], double& ub) {
   const double mu = me.E / (2.0 * (1.0 + me.nu));
   const double kk = spred[0] + spred[1] + spred[2];
   const double d0 = spred[0] - kk / 3.0, d1 = spred[1] - kk / 3.0, d2 = spred[2] - kk / 3.0;
@@ -218,7 +226,8 @@ __device__ __forceinline__ double rate_features(const double spred[6], double ep
   const double epn = (eps0 > 0.0) ? pow(eps0, me.C) : 0.0;
   const double sy0 = me.sig0 + me.B * epn;
   const double f = q - s23 * sy0;
-  dgpp = f / (2.0 * mu);
+  const double dgpp = f / (2.0 * mu);
+  ub = f > 0.0 ? rate_upper_bound(f, eps0, mu, me.B, me.C) : 0.0;
   x[0] = (float)log(fmax(f, 1e-30 * sy0) / (s23 * sy0));
   x[1] = (float)epn;
   x[2] = (float)(log(fmax(s23 * dgpp / dt, me.p8) / me.p8) / 10.0);
@@ -228,10 +237,12 @@ __device__ __forceinline__ double rate_features(const double spred[6], double ep
 
 // FINT.F90:797-870, 999-1116: return mapping (dg0 >= 0 starts the rate law's
 // Newton there), state write-back, strain_eq, internal work, wave speed, T_i.
-template <typename T, typename TS>
-__device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Trial<T>& w, double dg0, double& work,
+template <typename T, typename TS, bool LEAN>
+__device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Trial<T, LEAN>& w, double dg0, double& work,
                                               unsigned long long& nit, unsigned long long& npl, unsigned& st) {
-  const NodeMat m = to_nodemat(w.me);
+  const MatEntry& me = LEAN ? a.mats[w.mi] : w.me;
+  const NodeMat m = to_nodemat(me);
+  const double vol = a.vol[i];
   double snew[6];
   double ep = a.eps[i];
   const double ep0 = ep;
@@ -244,21 +255,20 @@ __device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Tr
     it = von_mises(w.spred, ep, m, a.maxit, snew, cap);
   } else if (m.type == MEGA_MAT_VM_RATE) {
     double dg = 0.0, ftr = 0.0;
-    const double g0 = (dg0 >= 0.0) ? dg0 : (a.mlp_guess ? (double)a.mlp_guess[i] : -1.0);
-    it = vm_rate(w.spred, ep, m, a.dt, a.rtol, a.maxit, g0, snew, cap, dg, ftr);
+    it = vm_rate(w.spred, ep, m, a.dt, a.rtol, a.maxit, a.rate_solver, dg0, snew, cap, dg, ftr);
     if (a.log_buf && it > 0) {  // sample (features, converged multiplier) for the surrogate
       const uint64_t sb = (uint64_t)__double_as_longlong(w.spred[0]);
       const uint32_t hsh = ((uint32_t)i * 2654435761u) ^ (uint32_t)(sb ^ (sb >> 29)) ^ a.log_seed;
       if (hsh % a.log_stride == 0) {
         float x[4];
-        double dgpp;
-        const double f = rate_features(w.spred, ep0, w.me, a.dt, x, dgpp);
-        if (f > 0.0) {
+        double ub;
+        const double f = rate_features(w.spred, ep0, me, a.dt, x, ub);
+        if (f > 0.0 && ub > 0.0) {
           const unsigned long long k = atomicAdd(a.log_count, 1ull);
           if ((int64_t)k < a.log_cap) {
             float* o = a.log_buf + 5 * k;
             o[0] = x[0]; o[1] = x[1]; o[2] = x[2]; o[3] = x[3];
-            o[4] = (float)(dg / dgpp);
+            o[4] = (float)(dg / ub);
           }
         }
       }
@@ -276,8 +286,8 @@ __device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Tr
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
     enew[k] = (double)w.eps6[k];
-    sinc[k] = snew[k] - w.sold[k];
-    einc[k] = enew[k] - w.eold[k];
+    sinc[k] = snew[k] - (LEAN ? a.stress[6 * i + k] : w.sold[k]);
+    einc[k] = enew[k] - (LEAN ? a.strain[6 * i + k] : w.eold[k]);
     a.stress[6 * i + k] = snew[k];
     a.strain[6 * i + k] = enew[k];
   }
@@ -287,17 +297,17 @@ __device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Tr
   a.strain_eq[i] = sqrt(eq * 2.0 / 3.0);
   if (a.finite_strain) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) work += 0.5 * (double)w.D[k] * (2.0 * snew[k] - sinc[k]) * w.vol * w.det;
+    for (int k = 0; k < 6; ++k) work += 0.5 * (double)w.D[k] * (2.0 * snew[k] - sinc[k]) * vol * w.det;
   } else {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) work += 0.5 * einc[k] * sinc[k] * w.vol * w.det;
+    for (int k = 0; k < 6; ++k) work += 0.5 * einc[k] * sinc[k] * vol * w.det;
   }
   double bulk = m.E / (3.0 * (1.0 - 2.0 * m.nu)), shear = m.E / (2.0 * (1.0 + m.nu));
   if (m.type > 1) estimate_moduli(sinc, einc, shear, bulk);
   const double pmod = bulk + 4.0 * shear / 3.0;
   a.wvel[i] = sqrt(fmax(pmod, shear) / m.rho);
   // T_i = V J sigma IF^T: f_J(k) = sum_m T(k,m) grad0 phi_iJ(m)
-  const T vj = (T)(w.vol * w.det);
+  const T vj = (T)(vol * w.det);
   T S[3][3];
   T sn[6];
 #pragma unroll
@@ -310,7 +320,7 @@ __device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Tr
     for (int mm = 0; mm < 3; ++mm)
       to[3 * k + mm] = (TS)(vj * (S[k][0] * w.IF[mm][0] + S[k][1] * w.IF[mm][1] + S[k][2] * w.IF[mm][2]));
   if (a.has_body) {
-    const double rvj = m.rho * w.vol * w.det;
+    const double rvj = m.rho * vol * w.det;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const double b = (a.bodyforce ? a.bodyforce[3 * i + k] : 0.0) + a.grav[k];
@@ -350,9 +360,9 @@ __global__ void __launch_bounds__(256, 2) k_stress(StressArgs a) {
   unsigned long long nit = 0, npl = 0;
   unsigned st = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
-    Trial<T> w;
+    Trial<T, false> w;
     stress_trial(a, i, w);
-    stress_finish<T, TS>(a, i, w, -1.0, work, nit, npl, st);
+    stress_finish<T, TS, false>(a, i, w, -1.0, work, nit, npl, st);
   }
   stress_reduce<T>(a, work, nit, npl, st, smd, smu);
 }
@@ -360,11 +370,12 @@ __global__ void __launch_bounds__(256, 2) k_stress(StressArgs a) {
 // The learned start: a warp of 32 nodes evaluates the surrogate together
 // (the 64x64 layer on the tensor cores, mlp_tc.cuh) and each plastic
 // rate-dependent node starts its Newton iteration from
-// dgamma0 = clamp(y, 0.02, 1) f_trial / (2 mu).  The loop is warp-uniform.
+// dgamma0 = clamp(y, 1e-3, 1) ub (ub = rate_upper_bound).  The loop is
+// warp-uniform.
 constexpr int kLearnBlock = 128;
 
 template <typename T, typename TS>
-__global__ void __launch_bounds__(kLearnBlock, 2) k_stress_learned(StressArgs a) {
+__global__ void __launch_bounds__(kLearnBlock, 4) k_stress_learned(StressArgs a) {
   __shared__ double smd[32];
   __shared__ unsigned long long smu[32];
   __shared__ __align__(16) MlpSmem net;
@@ -384,17 +395,19 @@ __global__ void __launch_bounds__(kLearnBlock, 2) k_stress_learned(StressArgs a)
        base += nwarps * 32) {
     const int64_t i = base + lane;
     const bool act = i < a.n;
-    Trial<T> w;
+    Trial<T, true> w;
     float x[4] = {0.f, 0.f, 0.f, 0.f};
-    double dgpp = 0.0, f = -1.0;
+    double ub = 0.0, f = -1.0;
     if (act) {
       stress_trial(a, i, w);
-      if (w.me.type == MEGA_MAT_VM_RATE) f = rate_features(w.spred, a.eps[i], w.me, a.dt, x, dgpp);
+      const MatEntry& me = a.mats[w.mi];
+      if (me.type == MEGA_MAT_VM_RATE) f = rate_features(w.spred, a.eps[i], me, a.dt, x, ub);
     }
-    const float y = warp_mlp(x, f > 0.0, net, hw, ow);
+    // warps without a plastic rate-dependent node skip the network
+    const float y = __any_sync(0xffffffffu, f > 0.0) ? warp_mlp(x, f > 0.0, net, hw, ow) : 0.f;
     if (act) {
-      const double dg0 = f > 0.0 ? (double)fminf(fmaxf(y, 0.02f), 1.0f) * dgpp : -1.0;
-      stress_finish<T, TS>(a, i, w, dg0, work, nit, npl, st);
+      const double dg0 = f > 0.0 ? (double)fminf(fmaxf(y, 1e-3f), 1.0f) * ub : -1.0;
+      stress_finish<T, TS, true>(a, i, w, dg0, work, nit, npl, st);
     }
   }
   stress_reduce<T>(a, work, nit, npl, st, smd, smu);

@@ -215,9 +215,36 @@ __device__ __forceinline__ int von_mises(const double spred[6], double& eps, con
 // sigma_y = A + B*ep^n*(1 + C*ln(max(epdot,epdot0)/epdot0)), epdot =
 // sqrt(2/3)*dg/dt.  Safeguarded Newton on dg in [0, q/(2mu)], converged at
 // |f| <= rtol*sqrt(2/3)*sigma_y.  dg0 < 0 selects the plain start f_tr/(2mu).
+// Upper bound of the rate-dependent plastic multiplier for a trial overstress
+// f0 > 0 at plastic strain eps0: the smaller of the perfectly plastic value
+// f0 / (2 mu) and the pure power-law value ((eps0^n + f0 / (sqrt(2/3) B))^(1/n)
+// - eps0) / sqrt(2/3); both bound the root because the rate factor is >= 1
+// and 2 mu dg >= 0.
+__device__ __forceinline__ double rate_upper_bound(double f0, double eps0, double mu, double B, double nexp) {
+  const double s23 = sqrt(2.0 / 3.0);
+  double hi = f0 / (2.0 * mu);
+  if (B > 0.0) {
+    const double epn0 = (eps0 > 0.0) ? pow(eps0, nexp) : 0.0;
+    const double pw = (pow(epn0 + f0 / (s23 * B), 1.0 / nexp) - eps0) / s23;
+    if (pw > 0.0 && pw < hi) hi = pw;
+  }
+  return hi;
+}
+
+// Power-law rate-dependent J2 (material 7, no reference counterpart):
+// sy = A + B eps^n (1 + C ln(epsdot / epsdot0)) for epsdot > epsdot0, with
+// epsdot = sqrt(2/3) dg / dt.  Radial return solved by Newton in y = ln(dg)
+// from the upper bound (f is concave in y, so the iterates decrease
+// monotonically onto the root from the right), with bracket and bisection
+// in y as the guard; converged when |f| <= rtol sqrt(2/3) sy or when an
+// update no longer changes dg beyond its rounding.  dg0 >= 0
+// starts there instead (clamped into the bracket).  solver = 1 is the
+// textbook form kept for comparison: Newton in dg from the perfectly plastic
+// estimate f_trial / (2 mu), bracket [0, q / (2 mu)], arithmetic bisection.
+// Returns the iterations.
 __device__ __forceinline__ int vm_rate(const double spred[6], double& eps, const NodeMat& m, double dt,
-                                       double rtol, int maxit, double dg0, double stress[6], bool& cap,
-                                       double& dg_out, double& f_tr) {
+                                       double rtol, int maxit, int solver, double dg0, double stress[6],
+                                       bool& cap, double& dg_out, double& f_tr) {
   const double mu = m.E / (2.0 * (1.0 + m.nu));
   const double A = m.sig0, Bh = m.B, nexp = m.C, C = m.p7, ed0 = m.p8;
   const double kk = spred[0] + spred[1] + spred[2];
@@ -233,26 +260,56 @@ __device__ __forceinline__ int vm_rate(const double spred[6], double& eps, const
   int it = 0;
   double dg = 0.0;
   if (f_tr > 0.0) {
-    double lo = 0.0, hi = tn / (2.0 * mu);
-    dg = (dg0 >= 0.0) ? dg0 : f_tr / (2.0 * mu);
-    if (!(dg > lo && dg < hi)) dg = 0.5 * (lo + hi);
+    const bool textbook = solver == 1;
+    double lo = 0.0, hi = textbook ? tn / (2.0 * mu) : rate_upper_bound(f_tr, eps0, mu, Bh, nexp);
+    dg = (dg0 >= 0.0) ? dg0 : (textbook ? f_tr / (2.0 * mu) : hi);
+    if (textbook ? !(dg > lo && dg < hi) : !(dg > lo && dg <= hi)) dg = textbook ? 0.5 * (lo + hi) : hi;
     bool conv = false;
-    for (int i = 1; i <= maxit; ++i) {
-      ++it;
-      const double ep = eps0 + s23 * dg;
-      const double ed = s23 * dg / dt;
-      double rate = 1.0, drate = 0.0;
-      if (ed > ed0) { rate = 1.0 + C * log(ed / ed0); drate = C / dg; }
-      const double epn = (ep > 0.0) ? pow(ep, nexp) : 0.0;
-      const double depn = (ep > 0.0) ? nexp * pow(ep, nexp - 1.0) * s23 : 0.0;
-      const double sy = A + Bh * epn * rate;
-      const double f = tn - 2.0 * mu * dg - s23 * sy;
-      if (fabs(f) <= rtol * s23 * sy) { conv = true; break; }
-      if (f > 0.0) lo = dg; else hi = dg;
-      const double df = -2.0 * mu - s23 * Bh * (depn * rate + epn * drate);
-      double nd = dg - f / df;
-      if (!(nd > lo && nd < hi) || !isfinite(nd)) nd = 0.5 * (lo + hi);
-      dg = nd;
+    if (textbook) {
+      for (int i = 1; i <= maxit; ++i) {
+        ++it;
+        const double ep = eps0 + s23 * dg;
+        const double ed = s23 * dg / dt;
+        double rate = 1.0, drate = 0.0;
+        if (ed > ed0) { rate = 1.0 + C * log(ed / ed0); drate = C / dg; }
+        const double epn = (ep > 0.0) ? pow(ep, nexp) : 0.0;
+        const double depn = (ep > 0.0) ? nexp * pow(ep, nexp - 1.0) * s23 : 0.0;
+        const double sy = A + Bh * epn * rate;
+        const double f = tn - 2.0 * mu * dg - s23 * sy;
+        if (fabs(f) <= rtol * s23 * sy) { conv = true; break; }
+        if (f > 0.0) lo = dg; else hi = dg;
+        const double df = -2.0 * mu - s23 * Bh * (depn * rate + epn * drate);
+        double nd = dg - f / df;
+        if (!(nd > lo && nd < hi) || !isfinite(nd)) nd = 0.5 * (lo + hi);
+        const bool stalled = fabs(nd - dg) <= 4.0e-16 * dg;  // below the rounding of dg
+        dg = nd;
+        if (stalled) { conv = true; break; }
+      }
+    } else {
+      // the iterate is y = ln(dg); ln(epsdot / epsdot0) = y - ythr, and
+      // eps^n = exp(n ln eps): three transcendentals per iteration
+      const double ythr = log(ed0 * dt / s23);
+      double y = log(dg), ylo = -INFINITY, yhi = log(hi);
+      for (int i = 1; i <= maxit; ++i) {
+        ++it;
+        const double ep = eps0 + s23 * dg;
+        const double epn = exp(nexp * log(ep));
+        const double depn = nexp * epn / ep * s23;
+        double rate = 1.0, drate = 0.0;
+        if (y > ythr) { rate = 1.0 + C * (y - ythr); drate = C / dg; }
+        const double sy = A + Bh * epn * rate;
+        const double f = tn - 2.0 * mu * dg - s23 * sy;
+        if (fabs(f) <= rtol * s23 * sy) { conv = true; break; }
+        if (f > 0.0) ylo = y; else yhi = y;
+        const double df = -2.0 * mu - s23 * Bh * (depn * rate + epn * drate);
+        double yn = y + fmax(fmin(-f / (df * dg), 50.0), -50.0);
+        if (!(yn > ylo && yn < yhi) || !isfinite(yn))
+          yn = isfinite(ylo) ? 0.5 * (ylo + yhi) : yhi - 0.69314718055994530942;  // bisect in y
+        const bool stalled = fabs(yn - y) <= 4.0e-16;  // below the rounding of dg
+        y = yn;
+        dg = exp(y);
+        if (stalled) { conv = true; break; }
+      }
     }
     if (!conv) cap = true;
     const double sc = dg * 2.0 * mu / tn;

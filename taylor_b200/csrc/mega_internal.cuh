@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <chrono>
 #include <vector>
 #include <cuda_runtime.h>
 #include "mega_device.cuh"
@@ -29,17 +30,46 @@ void record_error_text(const char* msg);
 
 #define MEGA_CHECK_LAUNCH() MEGA_TRY(cudaGetLastError())
 
-// Device allocations owned by one object; freed together.
+// Keep freed stream-ordered memory in the device's default pool for reuse
+// instead of returning it to the driver (once per device and process).
+void retain_pool_memory();
+// With MEGA_TRACE set: report allocations slower than 5 ms to stderr.
+bool trace_on();
+void trace_alloc(size_t bytes, double ms, bool ordered);
+
+// Device allocations owned by one object; freed together.  A pool bound to a
+// stream allocates and frees in that stream's order from the device's memory
+// pool (cudaMallocAsync / cudaFreeAsync): every user of its memory must run
+// on that stream.  An unbound pool uses cudaMalloc / cudaFree.
 struct DevPool {
   std::vector<void*> ptrs;
   int64_t bytes = 0;
+  cudaStream_t stream = nullptr;
+  bool ordered = false;
+  DevPool() = default;
+  explicit DevPool(cudaStream_t s) { bind(s); }
+  DevPool(const DevPool&) = delete;
+  DevPool& operator=(const DevPool&) = delete;
+  void bind(cudaStream_t s) {
+    stream = s;
+    ordered = true;
+    retain_pool_memory();
+  }
   template <typename T>
   int alloc(T** p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    const bool tr = trace_on();
+    const auto t0 = tr ? std::chrono::steady_clock::now() : std::chrono::steady_clock::time_point();
+    cudaError_t e = ordered ? cudaMallocAsync((void**)p, count * sizeof(T), stream)
+                            : cudaMalloc((void**)p, count * sizeof(T));
+    if (tr) {
+      if (ordered) cudaStreamSynchronize(stream);
+      trace_alloc(count * sizeof(T),
+                  std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(), ordered);
+    }
     if (e != cudaSuccess) {
-      record_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
+      record_cuda_error(e, ordered ? "cudaMallocAsync" : "cudaMalloc", __FILE__, __LINE__);
       *p = nullptr;
       return MEGA_ERR_NOMEM;
     }
@@ -47,12 +77,23 @@ struct DevPool {
     bytes += (int64_t)(count * sizeof(T));
     return 0;
   }
+  void drop(void* p) {
+    if (ordered) cudaFreeAsync(p, stream);
+    else cudaFree(p);
+  }
   void release(void* p) {
     for (size_t k = 0; k < ptrs.size(); ++k)
-      if (ptrs[k] == p) { cudaFree(p); ptrs.erase(ptrs.begin() + k); return; }
+      if (ptrs[k] == p) { drop(p); ptrs.erase(ptrs.begin() + k); return; }
+  }
+  // move every allocation of o into this pool (same binding required)
+  void adopt(DevPool& o) {
+    for (void* p : o.ptrs) ptrs.push_back(p);
+    bytes += o.bytes;
+    o.ptrs.clear();
+    o.bytes = 0;
   }
   void free_all() {
-    for (void* p : ptrs) cudaFree(p);
+    for (void* p : ptrs) drop(p);
     ptrs.clear();
     bytes = 0;
   }
@@ -153,10 +194,10 @@ struct StressArgs {
   int inv3_exact;
   int finite_strain;
   int maxit;
+  int rate_solver;           // material 7: 0 bounded Newton in ln(dgamma), 1 textbook
   double rtol;
   double dt;
   int32_t* iters;            // per-node Newton passes (or null)
-  const float* mlp_guess;    // per-node Newton start for the rate law (or null)
   const uint16_t* mlp_w2;    // surrogate network: W2 (64x64) as bf16 bits, or null
   const float* mlp_small;    // W1 (64x4), b1, b2, W3, b3 as fp32, or null
   float* log_buf;            // sample log: 5 floats (4 features, target) per sample, or null

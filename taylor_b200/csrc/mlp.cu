@@ -221,7 +221,7 @@ int mlp_pack(cudaStream_t s, const float* dtheta, uint16_t* w2, float* small) {
 int mlp_train_dev(cudaStream_t s, float* dth, int64_t ns, const float* X, int xs, const float* T, int ts,
                   int32_t epochs, int32_t batch, float lr, uint64_t seed, float* loss_host) {
   static_assert(H == kMlpH, "inference and training widths differ");
-  DevPool pool;
+  DevPool pool(s);
   float *dg, *dm, *dv, *dl;
   int64_t* order;
   MEGA_ALLOC(pool, dg, NP);

@@ -32,6 +32,14 @@ __device__ __forceinline__ void mma_16816_bf16(float c[4], const uint32_t a[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
+// hardware tanh (one SFU instruction, max error about 2^-11): the network
+// runs in bf16 anyway, and training uses the accurate tanhf
+__device__ __forceinline__ float tanh_sfu(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ uint32_t bf16_bits(float f) {
   const __nv_bfloat16 b = __float2bfloat16_rn(f);
   return (uint32_t) * reinterpret_cast<const uint16_t*>(&b);
@@ -63,9 +71,10 @@ __device__ __forceinline__ float warp_mlp(const float x[4], bool on, const MlpSm
   for (int o = 0; o < kMlpH; o += 2) {
     float h0 = 0.f, h1 = 0.f;
     if (on) {
-      h0 = tanhf(b1[o] + W1[4 * o] * x[0] + W1[4 * o + 1] * x[1] + W1[4 * o + 2] * x[2] + W1[4 * o + 3] * x[3]);
-      h1 = tanhf(b1[o + 1] + W1[4 * o + 4] * x[0] + W1[4 * o + 5] * x[1] + W1[4 * o + 6] * x[2] +
-                 W1[4 * o + 7] * x[3]);
+      h0 = tanh_sfu(b1[o] + W1[4 * o] * x[0] + W1[4 * o + 1] * x[1] + W1[4 * o + 2] * x[2] +
+                    W1[4 * o + 3] * x[3]);
+      h1 = tanh_sfu(b1[o + 1] + W1[4 * o + 4] * x[0] + W1[4 * o + 5] * x[1] + W1[4 * o + 6] * x[2] +
+                    W1[4 * o + 7] * x[3]);
     }
     *reinterpret_cast<uint32_t*>(row + o) = bf16_bits(h0) | (bf16_bits(h1) << 16);
   }
@@ -104,8 +113,8 @@ __device__ __forceinline__ float warp_mlp(const float x[4], bool on, const MlpSm
       float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
       for (int ks = 0; ks < 4; ++ks) mma_16816_bf16(c, af[mt][ks], bf[ks]);
-      rs[mt][0] += tanhf(c[0] + b2[c0]) * W3[c0] + tanhf(c[1] + b2[c0 + 1]) * W3[c0 + 1];
-      rs[mt][1] += tanhf(c[2] + b2[c0]) * W3[c0] + tanhf(c[3] + b2[c0 + 1]) * W3[c0 + 1];
+      rs[mt][0] += tanh_sfu(c[0] + b2[c0]) * W3[c0] + tanh_sfu(c[1] + b2[c0 + 1]) * W3[c0 + 1];
+      rs[mt][1] += tanh_sfu(c[2] + b2[c0]) * W3[c0] + tanh_sfu(c[3] + b2[c0 + 1]) * W3[c0 + 1];
     }
   }
   // the 4 lanes of a quad hold the 4 column pairs of the same rows

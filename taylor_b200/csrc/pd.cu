@@ -138,6 +138,7 @@ struct PdStressArgs {
   int linit;
   int inv3_exact;
   int maxit;
+  int rate_solver;
   double rtol;
   double dt;
   unsigned* status;
@@ -193,7 +194,7 @@ __global__ void k_pd_stress(PdStressArgs a) {
     von_mises(sp, ep, m, a.maxit, sn, cap);
   } else if (m.type == MEGA_MAT_VM_RATE) {
     double dg, ftr;
-    vm_rate(sp, ep, m, a.dt, a.rtol, a.maxit, -1.0, sn, cap, dg, ftr);
+    vm_rate(sp, ep, m, a.dt, a.rtol, a.maxit, a.rate_solver, -1.0, sn, cap, dg, ftr);
   } else {
     st |= MEGA_ST_BAD_MATERIAL;
     for (int k = 0; k < 6; ++k) sn[k] = sp[k];
@@ -269,8 +270,6 @@ struct PmbArgs {
   int32_t n;
   const int64_t* rowptr;
   const int32_t* col;
-  const float* xi;        // 3 per bond: X_j - X_i (float; static)
-  const float* l0;        // |xi| per bond
   uint32_t* broken;       // bit per bond
   const double* vol;
   const double* X;        // reference positions (double-precision bond geometry)
@@ -296,20 +295,22 @@ __global__ void __launch_bounds__(256) k_pmb_step(PmbArgs a) {
   const unsigned gm = 0xFu << (threadIdx.x & 28);
   if (i >= a.n) return;
   const double ui0 = a.u_in[3 * i], ui1 = a.u_in[3 * i + 1], ui2 = a.u_in[3 * i + 2];
+  const double Xi0 = a.X[3 * i], Xi1 = a.X[3 * i + 1], Xi2 = a.X[3 * i + 2];
   T f0 = T(0), f1 = T(0), f2 = T(0);
   unsigned nb = 0;
   const T c = (T)a.c, sc = (T)a.s_c;
+  // per bond only its column index (and broken bit) comes from HBM; the
+  // bond vector is rebuilt from the reference positions, which like u and
+  // vol are gathered per particle and stay in L2
   for (int64_t p = a.rowptr[i] + q; p < a.rowptr[i + 1]; p += kG) {
-    const float L0f = a.l0[p];
-    if (L0f == 0.f) continue;  // the particle itself
+    const int64_t j = a.col[p];
+    if (j == i) continue;  // the particle itself
     const uint32_t word = a.broken[p >> 5], bit = 1u << (p & 31);
     if (word & bit) continue;
-    const int64_t j = a.col[p];
     T s, e0, e1, e2, l;
     if (sizeof(T) == sizeof(double)) {
       // the oracle's arithmetic: xi from X, eta = xi + (u_j - u_i), s = (|eta| - |xi|)/|xi|
-      const double x0 = a.X[3 * j] - a.X[3 * i], x1 = a.X[3 * j + 1] - a.X[3 * i + 1],
-                   x2 = a.X[3 * j + 2] - a.X[3 * i + 2];
+      const double x0 = a.X[3 * j] - Xi0, x1 = a.X[3 * j + 1] - Xi1, x2 = a.X[3 * j + 2] - Xi2;
       e0 = (T)(x0 + (a.u_in[3 * j] - ui0));
       e1 = (T)(x1 + (a.u_in[3 * j + 1] - ui1));
       e2 = (T)(x2 + (a.u_in[3 * j + 2] - ui2));
@@ -318,8 +319,8 @@ __global__ void __launch_bounds__(256) k_pmb_step(PmbArgs a) {
       s = (l - L0) / L0;
     } else {
       const T d0 = (T)(a.u_in[3 * j] - ui0), d1 = (T)(a.u_in[3 * j + 1] - ui1), d2 = (T)(a.u_in[3 * j + 2] - ui2);
-      const T x0 = (T)a.xi[3 * p], x1 = (T)a.xi[3 * p + 1], x2 = (T)a.xi[3 * p + 2];
-      const T L0 = (T)L0f;
+      const T x0 = (T)(a.X[3 * j] - Xi0), x1 = (T)(a.X[3 * j + 1] - Xi1), x2 = (T)(a.X[3 * j + 2] - Xi2);
+      const T L0 = (T)sqrtf((float)(x0 * x0 + x1 * x1 + x2 * x2));
       // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|))
       e0 = x0 + d0; e1 = x1 + d1; e2 = x2 + d2;
       l = (T)sqrtf((float)(e0 * e0 + e1 * e1 + e2 * e2));
@@ -361,17 +362,33 @@ __global__ void __launch_bounds__(256) k_pmb_step(PmbArgs a) {
   if (q == 0 && nb && a.nbroken) atomicAdd(a.nbroken, (unsigned long long)nb);
 }
 
-__global__ void k_pmb_geometry(int32_t n, const double* __restrict__ X, const int64_t* __restrict__ rowptr,
-                               const int32_t* __restrict__ col, float* __restrict__ xi, float* __restrict__ l0) {
+// Pre-crack: break every bond whose reference segment X_i -> X_j crosses the
+// rectangle {p0 + s a + t b : 0 <= s, t <= 1} (strictly between its ends).
+__global__ void k_pmb_cut(int32_t n, const double* __restrict__ X, const int64_t* __restrict__ rowptr,
+                          const int32_t* __restrict__ col, double3 p0, double3 ea, double3 eb,
+                          uint32_t* __restrict__ broken, unsigned long long* __restrict__ ncut) {
   const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kG;
   const int q = threadIdx.x & (kG - 1);
   if (i >= n) return;
+  const double nx = ea.y * eb.z - ea.z * eb.y, ny = ea.z * eb.x - ea.x * eb.z, nz = ea.x * eb.y - ea.y * eb.x;
+  const double aa = ea.x * ea.x + ea.y * ea.y + ea.z * ea.z, bb = eb.x * eb.x + eb.y * eb.y + eb.z * eb.z;
+  const double xi0 = X[3 * i], xi1 = X[3 * i + 1], xi2 = X[3 * i + 2];
+  const double si = (xi0 - p0.x) * nx + (xi1 - p0.y) * ny + (xi2 - p0.z) * nz;
+  unsigned long long cnt = 0;
   for (int64_t p = rowptr[i] + q; p < rowptr[i + 1]; p += kG) {
     const int64_t j = col[p];
-    const double a0 = X[3 * j] - X[3 * i], a1 = X[3 * j + 1] - X[3 * i + 1], a2 = X[3 * j + 2] - X[3 * i + 2];
-    xi[3 * p] = (float)a0; xi[3 * p + 1] = (float)a1; xi[3 * p + 2] = (float)a2;
-    l0[p] = (j == i) ? 0.f : (float)sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+    const double d0 = X[3 * j] - xi0, d1 = X[3 * j + 1] - xi1, d2 = X[3 * j + 2] - xi2;
+    const double sj = si + d0 * nx + d1 * ny + d2 * nz;
+    if (!((si < 0.0 && sj > 0.0) || (si > 0.0 && sj < 0.0))) continue;
+    const double t = si / (si - sj);
+    const double c0 = xi0 + t * d0 - p0.x, c1 = xi1 + t * d1 - p0.y, c2 = xi2 + t * d2 - p0.z;
+    const double s = (c0 * ea.x + c1 * ea.y + c2 * ea.z) / aa, r = (c0 * eb.x + c1 * eb.y + c2 * eb.z) / bb;
+    if (s >= 0.0 && s <= 1.0 && r >= 0.0 && r <= 1.0) {
+      const uint32_t bit = 1u << (p & 31);
+      if (!(atomicOr(&broken[p >> 5], bit) & bit)) ++cnt;
+    }
   }
+  if (cnt) atomicAdd(ncut, cnt);
 }
 
 // predictor of the first step: u1 = u0 + dt v0 + dt^2/2 a0
@@ -407,7 +424,7 @@ int pd_step(cudaStream_t s, int32_t n, const double* X, const double* xc, const 
   PdStressArgs a{};
   a.n = n; a.fg = fg; a.ginvk = ginvk; a.matidx = matidx; a.mats = mats; a.stress = stress; a.strain = strain;
   a.eps = eps; a.wvel = wvel; a.amat = amat; a.linit = linit; a.inv3_exact = p.inv3_exact;
-  a.maxit = p.newton_max_iter; a.rtol = p.newton_rtol; a.dt = dt; a.status = status;
+  a.maxit = p.newton_max_iter; a.rate_solver = p.rate_solver; a.rtol = p.newton_rtol; a.dt = dt; a.status = status;
   k_pd_stress<<<(n + 127) / 128, 128, 0, s>>>(a);
   MEGA_CHECK_LAUNCH();
   k_pd_force<<<gridg(n), 256, 0, s>>>(n, X, vol, csr.colptr, csr.trow, csr.tpos, shp, amat, svec, fint);
@@ -422,7 +439,6 @@ struct PmbCtx {
   DevPool pool;
   DevCSR csr;
   double *X = nullptr, *vol = nullptr, *u[2] = {nullptr, nullptr}, *vel = nullptr, *acl = nullptr;
-  float *xi = nullptr, *l0 = nullptr;
   uint32_t* broken = nullptr;
   int8_t* fixed = nullptr;
   unsigned long long* nbroken = nullptr;
@@ -435,13 +451,17 @@ struct PmbCtx {
   double g_dt = 0;
   ~PmbCtx() {
     if (g) cudaGraphExecDestroy(g);
-    if (s) cudaStreamDestroy(s);
+    pool.free_all();  // stream-ordered frees before the stream goes
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
   }
 };
 
 static PmbArgs pmb_args(PmbCtx* c, double dt) {
   PmbArgs a{};
-  a.n = c->n; a.rowptr = c->csr.rowptr; a.col = c->csr.col; a.xi = c->xi; a.l0 = c->l0; a.broken = c->broken;
+  a.n = c->n; a.rowptr = c->csr.rowptr; a.col = c->csr.col; a.broken = c->broken;
   a.vol = c->vol; a.X = c->X; a.u_in = c->u[c->cur]; a.u_out = c->u[1 - c->cur]; a.vel = c->vel; a.acl = c->acl;
   a.fixed = c->fixed; a.c = c->c; a.s_c = c->s_c; a.inv_rho = 1.0 / c->rho; a.dt = dt; a.nbroken = c->nbroken;
   return a;
@@ -585,12 +605,13 @@ int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double*
   c->n = n; c->c = micromodulus; c->s_c = s_c; c->rho = rho;
   c->f64 = ((mode & 0xff) == MEGA_MODE_FP64);
   if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) return fail(MEGA_ERR_CUDA);
+  c->pool.bind(c->s);
   const int64_t n3 = 3 * (int64_t)n;
 #define PA(ptr, cnt) do { if (c->pool.alloc(&(ptr), (size_t)(cnt))) return fail(MEGA_ERR_NOMEM); } while (0)
   double *win = nullptr, *sml = nullptr;
   PA(c->X, n3); PA(c->vol, n); PA(c->u[0], n3); PA(c->u[1], n3); PA(c->vel, n3); PA(c->acl, n3);
   PA(c->fixed, n); PA(c->nbroken, 1); PA(c->status, 1);
-  DevPool tmp;
+  DevPool tmp(c->s);
   if (tmp.alloc(&win, n3) || tmp.alloc(&sml, 6 * (int64_t)n)) return fail(MEGA_ERR_NOMEM);
   std::vector<double> hw(n3, horizon);
   std::vector<int8_t> hf(n, 0);
@@ -612,9 +633,8 @@ int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double*
   int r = bin_search(c->s, n, c->X, win, sml, dmax, 0, 1, c->status, c->csr, nullptr, c->pool, nullptr);
   if (r) return fail(r);
   const int64_t m = c->csr.nnz;
-  PA(c->xi, 3 * m); PA(c->l0, m); PA(c->broken, (m + 31) / 32);
+  PA(c->broken, (m + 31) / 32);
 #undef PA
-  k_pmb_geometry<<<gridg(n), 256, 0, c->s>>>(n, c->X, c->csr.rowptr, c->csr.col, c->xi, c->l0);
   cudaMemsetAsync(c->broken, 0, sizeof(uint32_t) * ((m + 31) / 32), c->s);
   if (broken0) {
     std::vector<uint32_t> bits((m + 31) / 32, 0);
@@ -714,6 +734,26 @@ int mega_pmb_download(int64_t h, int32_t what, double* dst, int64_t* nbroken) {
     MEGA_TRY(cudaMemcpy(bits.data(), c->broken, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost));
     for (int64_t p = 0; p < m; ++p) dst[p] = (bits[p >> 5] >> (p & 31)) & 1u;
   } else return MEGA_ERR_ARG;
+  return 0;
+}
+
+int mega_pmb_cut(int64_t h, const double* corner, const double* edge_a, const double* edge_b, int64_t* ncut) {
+  PmbCtx* c = get_pmb(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (!corner || !edge_a || !edge_b) return MEGA_ERR_ARG;
+  DevPool tmp(c->s);
+  unsigned long long* d = nullptr;
+  MEGA_ALLOC(tmp, d, 1);
+  MEGA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->s));
+  k_pmb_cut<<<gridg(c->n), 256, 0, c->s>>>(c->n, c->X, c->csr.rowptr, c->csr.col,
+                                           make_double3(corner[0], corner[1], corner[2]),
+                                           make_double3(edge_a[0], edge_a[1], edge_a[2]),
+                                           make_double3(edge_b[0], edge_b[1], edge_b[2]), c->broken, d);
+  MEGA_CHECK_LAUNCH();
+  unsigned long long v = 0;
+  MEGA_TRY(cudaMemcpyAsync(&v, d, sizeof(v), cudaMemcpyDeviceToHost, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  if (ncut) *ncut = (int64_t)v;
   return 0;
 }
 

@@ -15,6 +15,7 @@
 // FMA contraction can change a comparison: the lists are bit-exact.
 #include <algorithm>
 #include <mutex>
+#include <climits>
 #include "mega_internal.cuh"
 
 namespace mega {
@@ -170,34 +171,56 @@ __global__ void __launch_bounds__(256) k_soft_search(
   for (int k = 0; k < 6; ++k) sl[k] = sm_len[6 * i + k];
   const int32_t m0 = cell[i];
   const int32_t is = m0 % nx + 1, js = (m0 / nx) % ny + 1, ks = m0 / (nx * ny) + 1;
-  const int32_t i0 = max(is - 1, 1), i1 = min(is + 1, nx);
-  const int32_t j0 = max(js - 1, 1), j1 = min(js + 1, ny);
-  const int32_t k0 = max(ks - 1, 1), k1 = min(ks + 1, nz);
+  // Lane k < 27 owns neighbour cell k in the reference's visiting order (IX
+  // outer, IY, IZ inner; cells outside the grid are empty).  The candidates
+  // of all 27 cells form one index range [0, total) walked 32 at a time, so
+  // the output keeps the reference order with every lane busy.
+  int64_t cbeg = 0;
+  int32_t clen = 0;
+  if (lane < 27) {
+    const int32_t ix = is - 1 + lane / 9, iy = js - 1 + (lane / 3) % 3, iz = ks - 1 + lane % 3;
+    if (ix >= 1 && ix <= nx && iy >= 1 && iy <= ny && iz >= 1 && iz <= nz) {
+      const int64_t m = (int64_t)(iz - 1) * nx * ny + (int64_t)(iy - 1) * nx + (ix - 1);
+      cbeg = cstart[m];
+      clen = (int32_t)(cstart[m + 1] - cbeg);
+    }
+  }
+  int32_t pre = clen;  // inclusive scan of the cell lengths
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t y = __shfl_up_sync(0xffffffffu, pre, o);
+    if (lane >= o) pre += y;
+  }
+  const int32_t total = __shfl_sync(0xffffffffu, pre, 31);
+  pre -= clen;  // exclusive
   const unsigned lt = (1u << lane) - 1u;
   int32_t count = 0;
-  int64_t ncand = 0;
-  int64_t base = FILL ? rowptr[i] : 0;
-  for (int32_t ix = i0; ix <= i1; ++ix)
-    for (int32_t iy = j0; iy <= j1; ++iy)
-      for (int32_t iz = k0; iz <= k1; ++iz) {
-        const int64_t m = (int64_t)(iz - 1) * nx * ny + (int64_t)(iy - 1) * nx + (ix - 1);
-        const int64_t p0 = cstart[m], p1 = cstart[m + 1];
-        ncand += p1 - p0;
-        for (int64_t q = p0; q < p1; q += 32) {
-          const int64_t p = q + lane;
-          bool add = false;
-          int32_t j = 0;
-          if (p < p1) {
-            j = sorted[p];
-            const double xj[3] = {coo[3 * (int64_t)j], coo[3 * (int64_t)j + 1], coo[3 * (int64_t)j + 2]};
-            const double wj[3] = {win[3 * (int64_t)j], win[3 * (int64_t)j + 1], win[3 * (int64_t)j + 2]};
-            add = accept(xi, xj, wj, sl, mmax, shsup);
-          }
-          const unsigned b = __ballot_sync(0xffffffffu, add);
-          if (FILL && add) col[base + count + __popc(b & lt)] = j;
-          count += __popc(b);
-        }
-      }
+  const int64_t ncand = total;
+  const int64_t base = FILL ? rowptr[i] : 0;
+  for (int32_t c0 = 0; c0 < total; c0 += 32) {
+    const int32_t c = c0 + lane;
+    bool add = false;
+    int32_t j = 0;
+    // owning cell: the last k with pre_k <= c (binary search over lanes 0..26)
+    int k = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const int t = k + step;
+      const int32_t pt = __shfl_sync(0xffffffffu, pre, t < 27 ? t : 26);
+      if (t < 27 && pt <= c) k = t;
+    }
+    const int64_t cb = __shfl_sync(0xffffffffu, cbeg, k);
+    const int32_t pk = __shfl_sync(0xffffffffu, pre, k);
+    if (c < total) {
+      j = sorted[cb + (c - pk)];
+      const double xj[3] = {coo[3 * (int64_t)j], coo[3 * (int64_t)j + 1], coo[3 * (int64_t)j + 2]};
+      const double wj[3] = {win[3 * (int64_t)j], win[3 * (int64_t)j + 1], win[3 * (int64_t)j + 2]};
+      add = accept(xi, xj, wj, sl, mmax, shsup);
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, add);
+    if (FILL && add) col[base + count + __popc(b & lt)] = j;
+    count += __popc(b);
+  }
   if (lane == 0) {
     if (!FILL) {
       gn[i] = count;
@@ -311,20 +334,77 @@ __global__ void k_col_scatter(int32_t n, const int64_t* __restrict__ rowptr, con
     trow[e] = (int32_t)i;
   }
 }
-// order each column by CSR position (equivalently by row, rows being
-// contiguous and ascending), so the CSC sums are deterministic
-__global__ void k_col_sort(int32_t n, const int64_t* __restrict__ colptr, int64_t* __restrict__ tpos,
-                           int32_t* __restrict__ trow) {
-  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// Order each column by CSR position (equivalently by row, rows being
+// contiguous and ascending), so the CSC sums are deterministic.  Warp per
+// column: up to kSortCap entries are sorted in registers by a bitonic network
+// (element e = k * 32 + lane, 4 per lane; cross-lane stages by shuffles, the
+// others between a lane's own registers); longer columns fall back to an
+// insertion sort by one lane.
+constexpr int kSortPer = 4;
+constexpr int kSortCap = 32 * kSortPer;
+
+__global__ void __launch_bounds__(256) k_col_sort(int32_t n, const int64_t* __restrict__ colptr,
+                                                  int64_t* __restrict__ tpos, int32_t* __restrict__ trow) {
+  const int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (j >= n) return;
   const int64_t s = colptr[j], e = colptr[j + 1];
-  for (int64_t a = s + 1; a < e; ++a) {
-    const int64_t v = tpos[a];
-    const int32_t r = trow[a];
-    int64_t b = a - 1;
-    while (b >= s && tpos[b] > v) { tpos[b + 1] = tpos[b]; trow[b + 1] = trow[b]; --b; }
-    tpos[b + 1] = v;
-    trow[b + 1] = r;
+  const int64_t len = e - s;
+  if (len <= 1) return;
+  if (len > kSortCap) {
+    if (lane == 0) {
+      for (int64_t a = s + 1; a < e; ++a) {
+        const int64_t v = tpos[a];
+        const int32_t r = trow[a];
+        int64_t b = a - 1;
+        while (b >= s && tpos[b] > v) { tpos[b + 1] = tpos[b]; trow[b + 1] = trow[b]; --b; }
+        tpos[b + 1] = v;
+        trow[b + 1] = r;
+      }
+    }
+    return;
+  }
+  long long key[kSortPer];
+  int32_t val[kSortPer];
+#pragma unroll
+  for (int k = 0; k < kSortPer; ++k) {
+    const int idx = k * 32 + lane;
+    key[k] = idx < len ? (long long)tpos[s + idx] : LLONG_MAX;
+    val[k] = idx < len ? trow[s + idx] : 0;
+  }
+#pragma unroll
+  for (int size = 2; size <= kSortCap; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {
+        const int ks = stride >> 5;
+#pragma unroll
+        for (int k = 0; k < kSortPer; ++k) {
+          if (k & ks) continue;
+          const int k2 = k | ks;
+          const bool up = ((k * 32 + lane) & size) == 0;
+          if ((key[k] > key[k2]) == up) {
+            const long long tk = key[k]; key[k] = key[k2]; key[k2] = tk;
+            const int32_t tv = val[k]; val[k] = val[k2]; val[k2] = tv;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < kSortPer; ++k) {
+          const long long ok = __shfl_xor_sync(0xffffffffu, key[k], stride);
+          const int32_t ov = __shfl_xor_sync(0xffffffffu, val[k], stride);
+          const bool up = ((k * 32 + lane) & size) == 0;
+          const bool lower = (lane & stride) == 0;
+          const bool take_min = (lower == up);
+          if (take_min ? (ok < key[k]) : (ok > key[k])) { key[k] = ok; val[k] = ov; }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kSortPer; ++k) {
+    const int idx = k * 32 + lane;
+    if (idx < len) { tpos[s + idx] = (int64_t)key[k]; trow[s + idx] = val[k]; }
   }
 }
 
@@ -352,7 +432,7 @@ int scan_counts(cudaStream_t s, const int32_t* cnt, int64_t* off, int64_t m, Dev
 int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, const double* sm_len,
                const double dist_max[3], int32_t itype_int, int32_t shsup, unsigned* status, DevCSR& csr,
                int32_t* ijk, DevPool& pool, BinGeom* geom_out, int32_t* cell_order) {
-  DevPool scratch;  // freed on return
+  DevPool scratch(s);  // freed on return
   csr.n = n;
   const int nbb = 148 * 2;
   double* part = nullptr;
@@ -421,7 +501,7 @@ int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, 
 }
 
 int build_transpose(cudaStream_t s, DevCSR& csr, DevPool& pool) {
-  DevPool scratch;
+  DevPool scratch(s);
   const int32_t n = csr.n;
   int32_t *ccnt = nullptr, *cfill = nullptr;
   MEGA_ALLOC(scratch, ccnt, n);
@@ -438,7 +518,7 @@ int build_transpose(cudaStream_t s, DevCSR& csr, DevPool& pool) {
   k_col_scatter<<<grid_for((int64_t)n * 32, 256), 256, 0, s>>>(n, csr.rowptr, csr.col, csr.colptr, cfill, csr.tpos,
                                                               csr.trow);
   MEGA_CHECK_LAUNCH();
-  k_col_sort<<<grid_for(n, 128), 128, 0, s>>>(n, csr.colptr, csr.tpos, csr.trow);
+  k_col_sort<<<grid_for((int64_t)n * 32, 256), 256, 0, s>>>(n, csr.colptr, csr.tpos, csr.trow);
   MEGA_CHECK_LAUNCH();
   MEGA_TRY(cudaStreamSynchronize(s));
   return 0;

@@ -159,7 +159,7 @@ __device__ __forceinline__ void load_entry64(const void* pk, int64_t p, double& 
 }
 
 template <typename A, bool F64, bool INTERP>
-__global__ void __launch_bounds__(256) k_defgrad_t(int32_t n, int32_t R, int32_t jmax,
+__global__ void __launch_bounds__(256, F64 ? 3 : 4) k_defgrad_t(int32_t n, int32_t R, int32_t jmax,
                                                    const int64_t* __restrict__ rowptr, const void* __restrict__ pk,
                                                    const int32_t* __restrict__ jset, const int32_t* __restrict__ jcnt,
                                                    const double* __restrict__ dsp, const double* __restrict__ dsp_tot,
@@ -173,13 +173,32 @@ __global__ void __launch_bounds__(256) k_defgrad_t(int32_t n, int32_t R, int32_t
   }
   const int64_t t = blockIdx.x;
   const int cnt = jcnt[t];
-  double* su = sm;             // 3 per local neighbour
-  double* sd = sm + 3 * cnt;
   const int32_t* js = jset + t * (int64_t)jmax;
+  // Staged neighbour displacements.  FP64: u_J and du_J as doubles.  Mixed:
+  // float offsets from the tile's first node r0 (u_J - u_r0, du_J - du_r0),
+  // half the shared-memory traffic; the differences u_J - u_i are formed
+  // between offsets, exact up to float rounding of the offsets.
+  double* su = sm;
+  double* sd = sm + 3 * cnt;
+  float4* sa = reinterpret_cast<float4*>(sm);
+  float2* sb = reinterpret_cast<float2*>(sa + cnt);
+  const int64_t r0 = t * R;
+  double ur0 = 0.0, ur1 = 0.0, ur2 = 0.0, dr0 = 0.0, dr1 = 0.0, dr2 = 0.0;
+  if (!F64) {
+    ur0 = dsp_tot[3 * r0]; ur1 = dsp_tot[3 * r0 + 1]; ur2 = dsp_tot[3 * r0 + 2];
+    dr0 = dsp[3 * r0]; dr1 = dsp[3 * r0 + 1]; dr2 = dsp[3 * r0 + 2];
+  }
   for (int l = threadIdx.x; l < cnt; l += blockDim.x) {
     const int64_t g = js[l];
-    su[3 * l] = dsp_tot[3 * g]; su[3 * l + 1] = dsp_tot[3 * g + 1]; su[3 * l + 2] = dsp_tot[3 * g + 2];
-    sd[3 * l] = dsp[3 * g]; sd[3 * l + 1] = dsp[3 * g + 1]; sd[3 * l + 2] = dsp[3 * g + 2];
+    const double a0 = dsp_tot[3 * g], a1 = dsp_tot[3 * g + 1], a2 = dsp_tot[3 * g + 2];
+    const double b0 = dsp[3 * g], b1 = dsp[3 * g + 1], b2 = dsp[3 * g + 2];
+    if (F64) {
+      su[3 * l] = a0; su[3 * l + 1] = a1; su[3 * l + 2] = a2;
+      sd[3 * l] = b0; sd[3 * l + 1] = b1; sd[3 * l + 2] = b2;
+    } else {
+      sa[l] = make_float4((float)(a0 - ur0), (float)(a1 - ur1), (float)(a2 - ur2), (float)(b0 - dr0));
+      sb[l] = make_float2((float)(b1 - dr1), (float)(b2 - dr2));
+    }
   }
   __syncthreads();
   const int64_t i = t * R + threadIdx.x / kG;
@@ -188,6 +207,8 @@ __global__ void __launch_bounds__(256) k_defgrad_t(int32_t n, int32_t R, int32_t
   if (threadIdx.x / kG >= R || i >= n) return;
   const double ui0 = dsp_tot[3 * i], ui1 = dsp_tot[3 * i + 1], ui2 = dsp_tot[3 * i + 2];
   const double di0 = dsp[3 * i], di1 = dsp[3 * i + 1], di2 = dsp[3 * i + 2];
+  const float fu0 = (float)(ui0 - ur0), fu1 = (float)(ui1 - ur1), fu2 = (float)(ui2 - ur2);
+  const float fd0 = (float)(di0 - dr0), fd1 = (float)(di1 - dr1), fd2 = (float)(di2 - dr2);
   A F[9], L[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) { F[k] = A(0); L[k] = A(0); }
@@ -195,9 +216,20 @@ __global__ void __launch_bounds__(256) k_defgrad_t(int32_t n, int32_t R, int32_t
   const int64_t pend = rowptr[i + 1];
   // One entry: F += (u_J - u_i) (x) g, L += (d_J - d_i) (x) g (+ phi d_J).
   auto body = [&](int64_t p, A g0, A g1, A g2, int l) {
-    const A u0 = (A)(su[3 * l] - ui0), u1 = (A)(su[3 * l + 1] - ui1), u2 = (A)(su[3 * l + 2] - ui2);
-    const double dj0 = sd[3 * l], dj1 = sd[3 * l + 1], dj2 = sd[3 * l + 2];
-    const A d0 = (A)(dj0 - di0), d1 = (A)(dj1 - di1), d2 = (A)(dj2 - di2);
+    A u0, u1, u2, d0, d1, d2;
+    double dj0, dj1, dj2;  // du_J itself, for the per-step interpolation
+    if (F64) {
+      u0 = (A)(su[3 * l] - ui0); u1 = (A)(su[3 * l + 1] - ui1); u2 = (A)(su[3 * l + 2] - ui2);
+      dj0 = sd[3 * l]; dj1 = sd[3 * l + 1]; dj2 = sd[3 * l + 2];
+      d0 = (A)(dj0 - di0); d1 = (A)(dj1 - di1); d2 = (A)(dj2 - di2);
+    } else {
+      const float4 va = sa[l];
+      const float2 vb = sb[l];
+      u0 = (A)(va.x - fu0); u1 = (A)(va.y - fu1); u2 = (A)(va.z - fu2);
+      d0 = (A)(va.w - fd0); d1 = (A)(vb.x - fd1); d2 = (A)(vb.y - fd2);
+      if (INTERP) { dj0 = dr0 + (double)va.w; dj1 = dr1 + (double)vb.x; dj2 = dr2 + (double)vb.y; }
+      else { dj0 = dj1 = dj2 = 0.0; }
+    }
     F[0] += u0 * g0; F[1] += u0 * g1; F[2] += u0 * g2;
     F[3] += u1 * g0; F[4] += u1 * g1; F[5] += u1 * g2;
     F[6] += u2 * g0; F[7] += u2 * g1; F[8] += u2 * g2;
@@ -289,9 +321,29 @@ __global__ void __launch_bounds__(256) k_force_t(TiledForceArgs a) {
   TS* sT = (TS*)smx;
   const int32_t* js = a.jset + t * (int64_t)a.jmax;
   const TS* tm = (const TS*)a.tmat;
-  for (int w = threadIdx.x; w < cnt * nv; w += blockDim.x) {
-    const int l = w / nv, k = w - l * nv;
-    sT[l * nv + k] = tm[12 * (int64_t)js[l] + k];
+  // thread per staged node: one index load, then its T row (12 values,
+  // 48 or 96 bytes, 16-byte aligned) as independent vector loads
+  for (int l = threadIdx.x; l < cnt; l += blockDim.x) {
+    const TS* src = tm + 12 * (int64_t)js[l];
+    TS v[12];
+    if (sizeof(TS) == 4) {
+      const float4* s4 = reinterpret_cast<const float4*>(src);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float4 x = __ldg(s4 + k);
+        v[4 * k] = (TS)x.x; v[4 * k + 1] = (TS)x.y; v[4 * k + 2] = (TS)x.z; v[4 * k + 3] = (TS)x.w;
+      }
+    } else {
+      const double2* s2 = reinterpret_cast<const double2*>(src);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double2 x = __ldg(s2 + k);
+        v[2 * k] = (TS)x.x; v[2 * k + 1] = (TS)x.y;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) sT[l * nv + k] = v[k];
+    if (nv == 12) { sT[l * nv + 9] = v[9]; sT[l * nv + 10] = v[10]; sT[l * nv + 11] = v[11]; }
   }
   __syncthreads();
   const int64_t J = t * a.R + threadIdx.x / kG;
@@ -427,7 +479,7 @@ int build_tiles(cudaStream_t s, int32_t n, const int64_t* ptr, const int32_t* id
   constexpr int HS = 2048;
   const int32_t jmax = HS / 2;
   if (gmaxn > jmax) return MEGA_ERR_UNSUPPORTED;
-  DevPool scratch;
+  DevPool scratch(s);
   int16_t* slot_tmp = nullptr;
   int32_t* ovf = nullptr;
   MEGA_ALLOC(scratch, slot_tmp, nnz);
@@ -437,6 +489,7 @@ int build_tiles(cudaStream_t s, int32_t n, const int64_t* ptr, const int32_t* id
     int32_t *jset = nullptr, *jcnt = nullptr;
     uint16_t* lidx = nullptr;
     DevPool trial;
+    if (pool.ordered) trial.bind(pool.stream);
     MEGA_ALLOC(trial, jset, ntiles * jmax);
     MEGA_ALLOC(trial, jcnt, ntiles);
     MEGA_ALLOC(trial, lidx, nnz);
@@ -452,9 +505,7 @@ int build_tiles(cudaStream_t s, int32_t n, const int64_t* ptr, const int32_t* id
     int32_t mx = 0;
     for (int32_t v : hc) mx = std::max(mx, v);
     // keep the trial buffers: move ownership into the persistent pool
-    for (void* p : trial.ptrs) pool.ptrs.push_back(p);
-    pool.bytes += trial.bytes;
-    trial.ptrs.clear();
+    pool.adopt(trial);
     ts.R = R;
     ts.ntiles = ntiles;
     ts.jmax = jmax;
@@ -497,7 +548,7 @@ int configure_tiled_kernels() {
 int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
                          const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
                          const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc) {
-  const size_t smem = sizeof(double) * 6 * (size_t)ts.maxcnt;
+  const size_t smem = (mixed ? 24 : 48) * (size_t)ts.maxcnt;
   const unsigned grid = (unsigned)ts.ntiles;
   const int block = ts.R * kG;
   if (mixed) {

@@ -196,6 +196,16 @@ class Mega:
         self.h = h.value
         self.nnz = 0
 
+    def set_instances(self, counts, dist_max=None):
+        """The nodes are len(counts) independent instances (searched apart,
+        instance k with bin-grid DIST_MAX dist_max[k] when given)."""
+        cnt = np.ascontiguousarray(counts, dtype=np.int32)
+        dm = None if dist_max is None else _f64(dist_max, (len(cnt), 3))
+        check(_lib.lib().mega_set_instances(self.h, len(cnt), ptr(cnt), ptr(dm)), "set_instances")
+
+    def set_precisions(self, fp64=True, mixed=True):
+        check(_lib.lib().mega_set_precisions(self.h, (1 if fp64 else 0) | (2 if mixed else 0)), "set_precisions")
+
     def search_and_shapes(self, download=False, allow_status=False):
         nnz = C.c_int64(0)
         gmaxn = C.c_int32(0)
@@ -234,11 +244,13 @@ class Mega:
                                            self.mode_bits(mode, interp_each_step, learned))
         return check(st, "step", allow_status)
 
-    def step_timed(self, nsteps, dt, mode="fp64", interp_each_step=False, learned=False):
+    def step_timed(self, nsteps, dt, mode="fp64", interp_each_step=False, learned=False, allow_status=False):
+        """Device milliseconds of nsteps steps; the status bits of the call are
+        kept in self.last_status (raised unless allow_status)."""
         ms = C.c_float(0.0)
         st = _lib.lib().mega_step_timed(self.h, int(nsteps), float(dt),
                                         self.mode_bits(mode, interp_each_step, learned), C.byref(ms))
-        check(st, "step_timed")
+        self.last_status = check(st, "step_timed", allow_status)
         return ms.value
 
     def kernel_times(self, reps, dt, mode="fp64", learned=False):
@@ -357,6 +369,13 @@ class Pmb:
         ms = C.c_float(0.0)
         check(_lib.lib().mega_pmb_step(self.h, int(nsteps), float(dt), C.byref(ms) if timed else None), "pmb_step")
         return ms.value
+
+    def cut(self, corner, edge_a, edge_b):
+        """Break the bonds crossing the rectangle corner + s a + t b (0..1)."""
+        k = C.c_int64(0)
+        check(_lib.lib().mega_pmb_cut(self.h, ptr(_f64(corner)), ptr(_f64(edge_a)), ptr(_f64(edge_b)),
+                                      C.byref(k)), "pmb_cut")
+        return k.value
 
     def download(self, what):
         m = self.nnz if what == 3 else 3 * self.n

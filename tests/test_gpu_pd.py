@@ -65,7 +65,8 @@ def _oracle_pmb(case, nb, broken, nsteps, dt):
 
 
 def _plate_and_lists():
-    c = cases.pd_plate(h=0.5e-3, nx=40, ny=40, nz=4, notch=6e-3, v_edge=20.0)
+    # notch end between lattice bond midpoints, so the crossing test has no ties
+    c = cases.pd_plate(h=0.5e-3, nx=40, ny=40, nz=4, notch=6.1e-3, v_edge=20.0)
     nb = O.bin_search(c["coo"], c["win"], c["sm_len"], c["dist_max"], 0, 1)
     got_nb = mega.bin_search(c["coo"], c["win"], c["sm_len"], c["dist_max"], 0, 1)
     np.testing.assert_array_equal(got_nb["gstack"], nb["gstack"])
@@ -80,6 +81,18 @@ def _pair_mismatch(nb, n, flags):
     cols = nb["gstack"] - 1
     key = {(int(i), int(j)): k for k, (i, j) in enumerate(zip(rows, cols))}
     return sum(1 for k, (i, j) in enumerate(zip(rows, cols)) if flags[k] != flags[key[(int(j), int(i))]])
+
+
+def test_pmb_device_cut_matches_host_notch():
+    c, nb, broken0, dt = _plate_and_lists()
+    p = mega.Pmb(c, None, mode="mixed")
+    k = p.cut(*cases.notch_rect(c))
+    flags, nbk = p.download(3)
+    np.testing.assert_array_equal(flags.astype(np.uint8), broken0)
+    assert k == int(broken0.sum())
+    # a second cut over the same rectangle breaks nothing new
+    assert p.cut(*cases.notch_rect(c)) == 0
+    p.close()
 
 
 def test_pmb_fp64_matches_oracle_exactly():
