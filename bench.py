@@ -15,6 +15,15 @@ from host buffers: model upload, step-0 search and shapes, K steps with the
 per-step scalars MAIN writes (energies, reaction force) read back to the
 host every step, and the end-state download, all inside the timed region.
 
+Further sections of the same line (each skippable by its flag):
+  accuracy      FP64 vs mixed end states after --full-steps steps
+  learned       the 2M-node rate-dependent bar: FP64, mixed, mixed with the
+                textbook Newton start, mixed with the learned start
+  peridynamics  the 2.56M-particle bond-based plate (--pmb-nx)
+  batch         --batch-bars bars of uneven size in one context vs one
+                context per bar
+  cpu_baseline  the C++ OpenMP restatement of the reference on the host
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: replicas only (one independent bar per rank), weak scaling.
 """

@@ -265,6 +265,13 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo,
  * Energies and reaction sums in mega_get_scalars are totals over all
  * instances. */
 int mega_set_instances(int64_t h, int32_t ninst, const int32_t* inst_nodes, const double* dist_max);
+/* Autotuner: time each launch variant of the two per-step gathers (lanes
+ * per row 4 or 8 x records in flight 4 or 2, in that order: variants 0..3)
+ * for the given precision on this context's lists, reps launches each,
+ * keep the fastest, and leave the state as it was.  choice (2) receives the
+ * deformation-gradient and force variants, times_ms (2 x 4, may be NULL) the
+ * mean launch times. */
+int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* choice, float* times_ms);
 /* Precisions the context will step: mask bit 0 FP64, bit 1 mixed (default
  * 3).  Call before mega_search_and_shapes; only the asked-for packed records
  * are built (the FP64 records are 32 B per list entry, the mixed 16 B).

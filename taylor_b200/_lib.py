@@ -77,6 +77,7 @@ SIGNATURES = {
     "mega_search_and_shapes": (I32, [I64, P, P, P, I64, P, P, P, P]),
     "mega_set_instances": (I32, [I64, I32, P, P]),
     "mega_set_precisions": (I32, [I64, I32]),
+    "mega_autotune": (I32, [I64, D, I32, I32, P, P]),
     "mega_step_resident": (I32, [I64, I32, D, I32]),
     "mega_step_timed": (I32, [I64, I32, D, I32, C.POINTER(F32)]),
     "mega_kernel_times": (I32, [I64, I32, D, I32, P]),

@@ -138,9 +138,10 @@ def batch_bars(nbars=256, seed=5, h_range=(0.15e-3, 0.6e-3), v0_range=(100.0, 30
 def param_kwargs(case, **over):
     """mega_params values for a case (Control.dat defaults: RK 1/3/0, QL 1
     0.001, DNI, Lagrangian finite strain, box support)."""
+    dmax = np.asarray(case["dist_max"], dtype=np.float64).reshape(-1, 3).max(axis=0)  # a batch: the largest
     kw = dict(rk_degree=1, rk_cont=3, rk_impl=0, itype_int=0, ql=1, lagrangian=1, finite_strain=1, shsup=0,
               peridynamics=0, inv3_exact=0, newton_max_iter=20, ql_coef=0.001, ql_len=float(case["ql_len"]),
-              gravity=(0.0, 0.0, 0.0), dist_max=tuple(float(v) for v in case["dist_max"]), newton_rtol=1e-10)
+              gravity=(0.0, 0.0, 0.0), dist_max=tuple(float(v) for v in dmax), newton_rtol=1e-10)
     kw.update(over)
     return kw
 

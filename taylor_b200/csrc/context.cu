@@ -191,6 +191,8 @@ struct Ctx {
   std::vector<int32_t> inst_off;  // ninst + 1 prefix offsets, empty = one instance
   std::vector<double> inst_dmax;  // 3 per instance: DIST_MAX of its bin grid
   int prec_mask = 3;              // bit 0: FP64 records built, bit 1: mixed records
+  int var_defgrad[2] = {0, 0};    // launch variant of the row gather, [FP64, mixed]
+  int var_force[2] = {0, 0};      // launch variant of the column gather
   // surrogate of the rate-dependent return mapping and its sample log
   DevPool mlppool;
   float* mlp_theta = nullptr;  // fp32 parameters (training copy)
@@ -298,13 +300,14 @@ static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) 
   const bool interp = (mode & MEGA_FLAG_INTERP_EACH_STEP) != 0;
   if (ev) MEGA_TRY(cudaEventRecord(ev[0], c->s));
   int r = launch_defgrad_tiled(c->s, mixed, interp, c->n, c->rt, c->csr.rowptr, mixed ? c->pk32 : c->pk64, c->dsp,
-                               c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc);
+                               c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc,
+                               c->var_defgrad[mixed]);
   if (r) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[1], c->s));
   r = launch_stress(c->s, mixed, stress_args(c, dt, mode));
   if (r) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[2], c->s));
-  r = launch_force_tiled(c->s, mixed, force_args(c, dt, mode, predict));
+  r = launch_force_tiled(c->s, mixed, force_args(c, dt, mode, predict), c->var_force[mixed]);
   if (r) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[3], c->s));
   c->launches += 3;
@@ -1051,6 +1054,85 @@ int64_t mega_kernel_launches(int64_t h) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
   return c->launches;
+}
+
+// Autotuner: time every launch variant of the two gathers on this context's
+// own lists (reps launches each, CUDA events), keep the fastest, and put the
+// state back as it was (the force kernel integrates when it runs).
+int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* choice, float* times_ms) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (!c->searched) return MEGA_ERR_STATE;
+  if (reps <= 0) return MEGA_ERR_ARG;
+  const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
+  { int r = mixed ? ensure_mixed(c) : ensure_fp64(c); if (r) return r; }
+  const int nvar = tiled_variants();
+  const size_t n = (size_t)c->n, n3 = 3 * n;
+  // snapshot of everything a step writes
+  struct Arr { void* p; size_t bytes; };
+  const size_t ts = mixed ? sizeof(float) : sizeof(double);
+  std::vector<Arr> arrs = {
+      {c->dsp, 8 * n3}, {c->dsp_tot, 8 * n3}, {c->dsp_tot_phy, 8 * n3}, {c->vel, 8 * n3}, {c->acl, 8 * n3},
+      {c->fint, 8 * n3}, {c->fext, 8 * n3}, {c->prforce, 8 * n3}, {c->stress, 48 * n}, {c->strain, 48 * n},
+      {c->eps, 8 * n}, {c->strain_eq, 8 * n}, {c->wvel, 8 * n}, {c->fg, 144 * n}, {c->tmat, 12 * ts * n},
+      {c->iters, 4 * n}, {c->acc, sizeof(StepAccum)}, {c->status, sizeof(unsigned)}};
+  DevPool snap(c->s);
+  std::vector<unsigned char*> copies;
+  for (const Arr& a : arrs) {
+    unsigned char* d = nullptr;
+    MEGA_ALLOC(snap, d, a.bytes);
+    MEGA_TRY(cudaMemcpyAsync(d, a.p, a.bytes, cudaMemcpyDeviceToDevice, c->s));
+    copies.push_back(d);
+  }
+  cudaEvent_t e0, e1;
+  MEGA_TRY(cudaEventCreate(&e0));
+  MEGA_TRY(cudaEventCreate(&e1));
+  std::vector<float> tdef(nvar, 0.f), tfor(nvar, 0.f);
+  int r = 0;
+  const StressArgs sa = stress_args(c, dt, mode & 0xff);
+  for (int v = 0; v < nvar && !r; ++v) {
+    const auto def = [&]() {
+      return launch_defgrad_tiled(c->s, mixed, false, c->n, c->rt, c->csr.rowptr, mixed ? c->pk32 : c->pk64, c->dsp,
+                                  c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc,
+                                  v);
+    };
+    r = def();  // warm-up
+    if (r) break;
+    cudaEventRecord(e0, c->s);
+    for (int k = 0; k < reps && !r; ++k) r = def();
+    cudaEventRecord(e1, c->s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&tdef[v], e0, e1);
+    if (r) break;
+    r = launch_stress(c->s, mixed, sa);
+    if (r) break;
+    const TiledForceArgs fa = force_args(c, dt, mode & 0xff, 0);
+    r = launch_force_tiled(c->s, mixed, fa, v);  // warm-up
+    cudaEventRecord(e0, c->s);
+    for (int k = 0; k < reps && !r; ++k) r = launch_force_tiled(c->s, mixed, fa, v);
+    cudaEventRecord(e1, c->s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&tfor[v], e0, e1);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (size_t k = 0; k < arrs.size(); ++k)
+    MEGA_TRY(cudaMemcpyAsync(arrs[k].p, copies[k], arrs[k].bytes, cudaMemcpyDeviceToDevice, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  if (r) return r;
+  int bd = 0, bf = 0;
+  for (int v = 1; v < nvar; ++v) {
+    if (tdef[v] < tdef[bd]) bd = v;
+    if (tfor[v] < tfor[bf]) bf = v;
+  }
+  c->var_defgrad[mixed] = bd;
+  c->var_force[mixed] = bf;
+  if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+  c->g_mode = -1;
+  if (choice) { choice[0] = bd; choice[1] = bf; }
+  if (times_ms)
+    for (int v = 0; v < nvar; ++v) { times_ms[v] = tdef[v] / reps; times_ms[nvar + v] = tfor[v] / reps; }
+  return read_status(c, true);
 }
 
 int mega_set_instances(int64_t h, int32_t ninst, const int32_t* inst_nodes, const double* dist_max) {

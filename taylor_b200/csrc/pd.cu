@@ -288,55 +288,81 @@ struct PmbArgs {
 // T = per-bond arithmetic: float (the mixed path: float bond geometry and
 // force, double accumulation of nothing but the integrator) or double (the
 // oracle's arithmetic, recomputed from X, for exact parity checks).
+constexpr int kGP = 8;  // lanes per particle of the bond loop
+constexpr int kUP = 4;  // bonds in flight per lane
+inline unsigned gridp(int64_t n) { return (unsigned)((n * kGP + 255) / 256); }
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_pmb_step(PmbArgs a) {
-  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kG;
-  const int q = threadIdx.x & (kG - 1);
-  const unsigned gm = 0xFu << (threadIdx.x & 28);
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kGP;
+  const int q = threadIdx.x & (kGP - 1);
+  const unsigned gm = 0xFFu << (threadIdx.x & 24);
   if (i >= a.n) return;
   const double ui0 = a.u_in[3 * i], ui1 = a.u_in[3 * i + 1], ui2 = a.u_in[3 * i + 2];
   const double Xi0 = a.X[3 * i], Xi1 = a.X[3 * i + 1], Xi2 = a.X[3 * i + 2];
   T f0 = T(0), f1 = T(0), f2 = T(0);
   unsigned nb = 0;
   const T c = (T)a.c, sc = (T)a.s_c;
+  const int64_t p1 = a.rowptr[i + 1];
   // per bond only its column index (and broken bit) comes from HBM; the
   // bond vector is rebuilt from the reference positions, which like u and
-  // vol are gathered per particle and stay in L2
-  for (int64_t p = a.rowptr[i] + q; p < a.rowptr[i + 1]; p += kG) {
-    const int64_t j = a.col[p];
-    if (j == i) continue;  // the particle itself
-    const uint32_t word = a.broken[p >> 5], bit = 1u << (p & 31);
-    if (word & bit) continue;
-    T s, e0, e1, e2, l;
-    if (sizeof(T) == sizeof(double)) {
-      // the oracle's arithmetic: xi from X, eta = xi + (u_j - u_i), s = (|eta| - |xi|)/|xi|
-      const double x0 = a.X[3 * j] - Xi0, x1 = a.X[3 * j + 1] - Xi1, x2 = a.X[3 * j + 2] - Xi2;
-      e0 = (T)(x0 + (a.u_in[3 * j] - ui0));
-      e1 = (T)(x1 + (a.u_in[3 * j + 1] - ui1));
-      e2 = (T)(x2 + (a.u_in[3 * j + 2] - ui2));
-      const T L0 = (T)sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-      l = (T)sqrt((double)(e0 * e0 + e1 * e1 + e2 * e2));
-      s = (l - L0) / L0;
-    } else {
-      const T d0 = (T)(a.u_in[3 * j] - ui0), d1 = (T)(a.u_in[3 * j + 1] - ui1), d2 = (T)(a.u_in[3 * j + 2] - ui2);
-      const T x0 = (T)(a.X[3 * j] - Xi0), x1 = (T)(a.X[3 * j + 1] - Xi1), x2 = (T)(a.X[3 * j + 2] - Xi2);
-      const T L0 = (T)sqrtf((float)(x0 * x0 + x1 * x1 + x2 * x2));
-      // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|))
-      e0 = x0 + d0; e1 = x1 + d1; e2 = x2 + d2;
-      l = (T)sqrtf((float)(e0 * e0 + e1 * e1 + e2 * e2));
-      const T num = T(2) * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
-      s = num / (L0 * (l + L0));
+  // vol are gathered per particle and stay in L2.  kUP bonds per lane are
+  // loaded before any is used.
+  for (int64_t pb = a.rowptr[i] + q; pb < p1; pb += kGP * kUP) {
+    int64_t jj[kUP];
+    double xj[kUP][3], uj[kUP][3], vj[kUP];
+    uint32_t wd[kUP];
+#pragma unroll
+    for (int u = 0; u < kUP; ++u) {
+      const int64_t p = pb + u * kGP;
+      jj[u] = p < p1 ? (int64_t)a.col[p] : i;
+      wd[u] = p < p1 ? a.broken[p >> 5] : 0u;
     }
-    if (s > sc) {
-      atomicOr(&a.broken[p >> 5], bit);
-      ++nb;
-      continue;
+#pragma unroll
+    for (int u = 0; u < kUP; ++u) {
+      const int64_t j = jj[u];
+      xj[u][0] = a.X[3 * j]; xj[u][1] = a.X[3 * j + 1]; xj[u][2] = a.X[3 * j + 2];
+      uj[u][0] = a.u_in[3 * j]; uj[u][1] = a.u_in[3 * j + 1]; uj[u][2] = a.u_in[3 * j + 2];
+      vj[u] = a.vol[j];
     }
-    const T w = c * s * (T)a.vol[j] / l;
-    f0 += w * e0; f1 += w * e1; f2 += w * e2;
+#pragma unroll
+    for (int u = 0; u < kUP; ++u) {
+      const int64_t p = pb + u * kGP;
+      const int64_t j = jj[u];
+      if (j == i) continue;  // the particle itself, or past the row
+      const uint32_t bit = 1u << (p & 31);
+      if (wd[u] & bit) continue;
+      T s, e0, e1, e2, l;
+      if (sizeof(T) == sizeof(double)) {
+        // the oracle's arithmetic: xi from X, eta = xi + (u_j - u_i), s = (|eta| - |xi|)/|xi|
+        const double x0 = xj[u][0] - Xi0, x1 = xj[u][1] - Xi1, x2 = xj[u][2] - Xi2;
+        e0 = (T)(x0 + (uj[u][0] - ui0));
+        e1 = (T)(x1 + (uj[u][1] - ui1));
+        e2 = (T)(x2 + (uj[u][2] - ui2));
+        const T L0 = (T)sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+        l = (T)sqrt((double)(e0 * e0 + e1 * e1 + e2 * e2));
+        s = (l - L0) / L0;
+      } else {
+        const T d0 = (T)(uj[u][0] - ui0), d1 = (T)(uj[u][1] - ui1), d2 = (T)(uj[u][2] - ui2);
+        const T x0 = (T)(xj[u][0] - Xi0), x1 = (T)(xj[u][1] - Xi1), x2 = (T)(xj[u][2] - Xi2);
+        const T L0 = (T)sqrtf((float)(x0 * x0 + x1 * x1 + x2 * x2));
+        // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|))
+        e0 = x0 + d0; e1 = x1 + d1; e2 = x2 + d2;
+        l = (T)sqrtf((float)(e0 * e0 + e1 * e1 + e2 * e2));
+        const T num = T(2) * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
+        s = num / (L0 * (l + L0));
+      }
+      if (s > sc) {
+        atomicOr(&a.broken[p >> 5], bit);
+        ++nb;
+        continue;
+      }
+      const T w = c * s * (T)vj[u] / l;
+      f0 += w * e0; f1 += w * e1; f2 += w * e2;
+    }
   }
 #pragma unroll
-  for (int o = 1; o < kG; o <<= 1) {
+  for (int o = 1; o < kGP; o <<= 1) {
     f0 += __shfl_xor_sync(gm, f0, o);
     f1 += __shfl_xor_sync(gm, f1, o);
     f2 += __shfl_xor_sync(gm, f2, o);
@@ -676,8 +702,8 @@ int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms) {
     MEGA_TRY(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < 2; ++k) {
       PmbArgs a = pmb_args(c, dt);
-      if (c->f64) k_pmb_step<double><<<gridg(c->n), 256, 0, c->s>>>(a);
-      else k_pmb_step<float><<<gridg(c->n), 256, 0, c->s>>>(a);
+      if (c->f64) k_pmb_step<double><<<gridp(c->n), 256, 0, c->s>>>(a);
+      else k_pmb_step<float><<<gridp(c->n), 256, 0, c->s>>>(a);
       c->cur = 1 - c->cur;
     }
     cudaError_t e = cudaStreamEndCapture(c->s, &gr);
@@ -693,8 +719,8 @@ int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms) {
   }
   for (; done < nsteps; ++done) {
     PmbArgs a = pmb_args(c, dt);
-    if (c->f64) k_pmb_step<double><<<gridg(c->n), 256, 0, c->s>>>(a);
-    else k_pmb_step<float><<<gridg(c->n), 256, 0, c->s>>>(a);
+    if (c->f64) k_pmb_step<double><<<gridp(c->n), 256, 0, c->s>>>(a);
+    else k_pmb_step<float><<<gridp(c->n), 256, 0, c->s>>>(a);
     MEGA_CHECK_LAUNCH();
     c->cur = 1 - c->cur;
   }

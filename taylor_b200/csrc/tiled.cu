@@ -19,8 +19,13 @@
 namespace mega {
 namespace {
 
-constexpr int kG = 4;  // lanes per row
-constexpr int kU = 4;  // records in flight per lane
+// Launch variants of the two gathers (picked per context by the autotuner):
+// KG lanes per row / column (4 or 8), KU packed records in flight per lane
+// (2 or 4).  A block serves one tile of R rows with R * KG threads.
+template <int KG>
+__device__ __forceinline__ unsigned group_mask() {
+  return ((1u << KG) - 1u) << (threadIdx.x & (32 - KG));
+}
 
 __device__ __forceinline__ unsigned hash_u32(unsigned x) {
   x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
@@ -158,8 +163,8 @@ __device__ __forceinline__ void load_entry64(const void* pk, int64_t p, double& 
   g0 = a.x; g1 = a.y; g2 = b.x; l = (int)__double_as_longlong(b.y);
 }
 
-template <typename A, bool F64, bool INTERP>
-__global__ void __launch_bounds__(256, F64 ? 3 : 4) k_defgrad_t(int32_t n, int32_t R, int32_t jmax,
+template <typename A, bool F64, bool INTERP, int KG, int KU>
+__global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int32_t n, int32_t R, int32_t jmax,
                                                    const int64_t* __restrict__ rowptr, const void* __restrict__ pk,
                                                    const int32_t* __restrict__ jset, const int32_t* __restrict__ jcnt,
                                                    const double* __restrict__ dsp, const double* __restrict__ dsp_tot,
@@ -201,10 +206,10 @@ __global__ void __launch_bounds__(256, F64 ? 3 : 4) k_defgrad_t(int32_t n, int32
     }
   }
   __syncthreads();
-  const int64_t i = t * R + threadIdx.x / kG;
-  const int q = threadIdx.x & (kG - 1);
-  const unsigned gmask = 0xFu << (threadIdx.x & 28);
-  if (threadIdx.x / kG >= R || i >= n) return;
+  const int64_t i = t * R + threadIdx.x / KG;
+  const int q = threadIdx.x & (KG - 1);
+  const unsigned gmask = group_mask<KG>();
+  if (threadIdx.x / KG >= R || i >= n) return;
   const double ui0 = dsp_tot[3 * i], ui1 = dsp_tot[3 * i + 1], ui2 = dsp_tot[3 * i + 2];
   const double di0 = dsp[3 * i], di1 = dsp[3 * i + 1], di2 = dsp[3 * i + 2];
   const float fu0 = (float)(ui0 - ur0), fu1 = (float)(ui1 - ur1), fu2 = (float)(ui2 - ur2);
@@ -241,31 +246,31 @@ __global__ void __launch_bounds__(256, F64 ? 3 : 4) k_defgrad_t(int32_t n, int32
       ph0 += s * dj0; ph1 += s * dj1; ph2 += s * dj2;
     }
   };
-  // kU records in flight per lane before any is used (the loop is bound by
+  // KU records in flight per lane before any is used (the loop is bound by
   // DRAM latency otherwise); each lane still sums its entries in list order.
   int64_t p = rowptr[i] + q;
   if (F64) {
-    for (; p + (kU - 1) * kG < pend; p += kU * kG) {
-      double2 ra[kU], rb[kU];
+    for (; p + (KU - 1) * KG < pend; p += KU * KG) {
+      double2 ra[KU], rb[KU];
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
-        ra[u] = __ldg((const double2*)pk + 2 * (p + u * kG));
-        rb[u] = __ldg((const double2*)pk + 2 * (p + u * kG) + 1);
+      for (int u = 0; u < KU; ++u) {
+        ra[u] = __ldg((const double2*)pk + 2 * (p + u * KG));
+        rb[u] = __ldg((const double2*)pk + 2 * (p + u * KG) + 1);
       }
 #pragma unroll
-      for (int u = 0; u < kU; ++u)
-        body(p + u * kG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y));
+      for (int u = 0; u < KU; ++u)
+        body(p + u * KG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y));
     }
   } else {
-    for (; p + (kU - 1) * kG < pend; p += kU * kG) {
-      float4 r[kU];
+    for (; p + (KU - 1) * KG < pend; p += KU * KG) {
+      float4 r[KU];
 #pragma unroll
-      for (int u = 0; u < kU; ++u) r[u] = __ldg((const float4*)pk + p + u * kG);
+      for (int u = 0; u < KU; ++u) r[u] = __ldg((const float4*)pk + p + u * KG);
 #pragma unroll
-      for (int u = 0; u < kU; ++u) body(p + u * kG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w));
+      for (int u = 0; u < KU; ++u) body(p + u * KG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w));
     }
   }
-  for (; p < pend; p += kG) {
+  for (; p < pend; p += KG) {
     if (F64) {
       double a0, a1, a2;
       int l;
@@ -279,7 +284,7 @@ __global__ void __launch_bounds__(256, F64 ? 3 : 4) k_defgrad_t(int32_t n, int32
     }
   }
 #pragma unroll
-  for (int o = 1; o < kG; o <<= 1) {
+  for (int o = 1; o < KG; o <<= 1) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
       F[k] += __shfl_xor_sync(gmask, F[k], o);
@@ -311,8 +316,8 @@ __global__ void __launch_bounds__(256, F64 ? 3 : 4) k_defgrad_t(int32_t n, int32
 }
 
 // TS = storage of T_i (float / double), A = accumulation, F64 = record width
-template <typename TS, typename A, bool F64>
-__global__ void __launch_bounds__(256) k_force_t(TiledForceArgs a) {
+template <typename TS, typename A, bool F64, int KG, int KU>
+__global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
   extern __shared__ double smx[];
   __shared__ double red[8 * 8];
   const int64_t t = blockIdx.x;
@@ -346,12 +351,12 @@ __global__ void __launch_bounds__(256) k_force_t(TiledForceArgs a) {
     if (nv == 12) { sT[l * nv + 9] = v[9]; sT[l * nv + 10] = v[10]; sT[l * nv + 11] = v[11]; }
   }
   __syncthreads();
-  const int64_t J = t * a.R + threadIdx.x / kG;
-  const int q = threadIdx.x & (kG - 1);
-  const unsigned gmask = 0xFu << (threadIdx.x & 28);
+  const int64_t J = t * a.R + threadIdx.x / KG;
+  const int q = threadIdx.x & (KG - 1);
+  const unsigned gmask = group_mask<KG>();
   double ke = 0.0, ee = 0.0, tf0 = 0.0, tf1 = 0.0, tf2 = 0.0, tf3 = 0.0, tf4 = 0.0, tf5 = 0.0;
   unsigned st = 0;
-  if (threadIdx.x / kG < a.R && J < a.n) {
+  if (threadIdx.x / KG < a.R && J < a.n) {
     A f0 = A(0), f1 = A(0), f2 = A(0);
     double e0 = 0.0, e1 = 0.0, e2 = 0.0;
     const int64_t c1 = a.colptr[J + 1];
@@ -367,27 +372,27 @@ __global__ void __launch_bounds__(256) k_force_t(TiledForceArgs a) {
     };
     int64_t e = a.colptr[J] + q;
     if (F64) {
-      for (; e + (kU - 1) * kG < c1; e += kU * kG) {
-        double2 ra[kU], rb[kU];
+      for (; e + (KU - 1) * KG < c1; e += KU * KG) {
+        double2 ra[KU], rb[KU];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          ra[u] = __ldg((const double2*)a.pk + 2 * (e + u * kG));
-          rb[u] = __ldg((const double2*)a.pk + 2 * (e + u * kG) + 1);
+        for (int u = 0; u < KU; ++u) {
+          ra[u] = __ldg((const double2*)a.pk + 2 * (e + u * KG));
+          rb[u] = __ldg((const double2*)a.pk + 2 * (e + u * KG) + 1);
         }
 #pragma unroll
-        for (int u = 0; u < kU; ++u)
-          body(e + u * kG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y));
+        for (int u = 0; u < KU; ++u)
+          body(e + u * KG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y));
       }
     } else {
-      for (; e + (kU - 1) * kG < c1; e += kU * kG) {
-        float4 r[kU];
+      for (; e + (KU - 1) * KG < c1; e += KU * KG) {
+        float4 r[KU];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) r[u] = __ldg((const float4*)a.pk + e + u * kG);
+        for (int u = 0; u < KU; ++u) r[u] = __ldg((const float4*)a.pk + e + u * KG);
 #pragma unroll
-        for (int u = 0; u < kU; ++u) body(e + u * kG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w));
+        for (int u = 0; u < KU; ++u) body(e + u * KG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w));
       }
     }
-    for (; e < c1; e += kG) {
+    for (; e < c1; e += KG) {
       if (F64) {
         double b0, b1, b2;
         int l;
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(256) k_force_t(TiledForceArgs a) {
       }
     }
 #pragma unroll
-    for (int o = 1; o < kG; o <<= 1) {
+    for (int o = 1; o < KG; o <<= 1) {
       f0 += __shfl_xor_sync(gmask, f0, o);
       f1 += __shfl_xor_sync(gmask, f1, o);
       f2 += __shfl_xor_sync(gmask, f2, o);
@@ -528,6 +533,27 @@ int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* 
   return 0;
 }
 
+// The launch variants, in the order the autotuner tries them:
+// (KG, KU) = (4, 4), (4, 2), (8, 4), (8, 2).
+constexpr int kVariants = 4;
+
+template <typename K>
+static int raise_smem(K k, int lim) {
+  MEGA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  return 0;
+}
+
+template <int KG, int KU>
+static int configure_variant(int lim) {
+  int r = 0;
+  if ((r = raise_smem(k_defgrad_t<float, false, true, KG, KU>, lim))) return r;
+  if ((r = raise_smem(k_defgrad_t<float, false, false, KG, KU>, lim))) return r;
+  if ((r = raise_smem(k_defgrad_t<double, true, true, KG, KU>, lim))) return r;
+  if ((r = raise_smem(k_defgrad_t<double, true, false, KG, KU>, lim))) return r;
+  if ((r = raise_smem(k_force_t<float, float, false, KG, KU>, lim))) return r;
+  return raise_smem(k_force_t<double, double, true, KG, KU>, lim);
+}
+
 // Raise the dynamic shared-memory limit of the tiled kernels once (outside
 // any stream capture): a tile stages at most 1024 neighbours, 96 KB for the
 // double-precision T_i of the force kernel.
@@ -535,46 +561,69 @@ int configure_tiled_kernels() {
   static bool done = false;
   if (done) return 0;
   const int lim = 12 * 8 * 1024 + 1024;
-  MEGA_TRY(cudaFuncSetAttribute(k_defgrad_t<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  MEGA_TRY(cudaFuncSetAttribute(k_defgrad_t<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  MEGA_TRY(cudaFuncSetAttribute(k_defgrad_t<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  MEGA_TRY(cudaFuncSetAttribute(k_defgrad_t<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  MEGA_TRY(cudaFuncSetAttribute(k_force_t<float, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  MEGA_TRY(cudaFuncSetAttribute(k_force_t<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  int r = 0;
+  if ((r = configure_variant<4, 4>(lim)) || (r = configure_variant<4, 2>(lim)) ||
+      (r = configure_variant<8, 4>(lim)) || (r = configure_variant<8, 2>(lim)))
+    return r;
   done = true;
   return 0;
 }
 
-int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
-                         const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
-                         const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc) {
+int tiled_variants() { return kVariants; }
+
+template <int KG, int KU>
+static void defgrad_variant(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
+                            const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
+                            const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg,
+                            StepAccum* acc) {
   const size_t smem = (mixed ? 24 : 48) * (size_t)ts.maxcnt;
   const unsigned grid = (unsigned)ts.ntiles;
-  const int block = ts.R * kG;
+  const int block = ts.R * KG;
   if (mixed) {
-    auto k = interp ? k_defgrad_t<float, false, true> : k_defgrad_t<float, false, false>;
+    auto k = interp ? k_defgrad_t<float, false, true, KG, KU> : k_defgrad_t<float, false, false, KG, KU>;
     k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
                                 dsp_tot_phy, fg, acc);
   } else {
-    auto k = interp ? k_defgrad_t<double, true, true> : k_defgrad_t<double, true, false>;
+    auto k = interp ? k_defgrad_t<double, true, true, KG, KU> : k_defgrad_t<double, true, false, KG, KU>;
     k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
                                 dsp_tot_phy, fg, acc);
+  }
+}
+
+int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
+                         const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
+                         const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc,
+                         int variant) {
+  switch (variant) {
+    case 1: defgrad_variant<4, 2>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
+      break;
+    case 2: defgrad_variant<8, 4>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
+      break;
+    case 3: defgrad_variant<8, 2>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
+      break;
+    default: defgrad_variant<4, 4>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg,
+                                   acc);
   }
   MEGA_CHECK_LAUNCH();
   return 0;
 }
 
-int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a) {
+template <int KG, int KU>
+static void force_variant(cudaStream_t s, bool mixed, const TiledForceArgs& a) {
   const int nv = a.has_body ? 12 : 9;
   const size_t smem = (mixed ? sizeof(float) : sizeof(double)) * nv * (size_t)a.maxcnt;
   const unsigned grid = (unsigned)a.ntiles;
-  const int block = a.R * kG;
-  if (mixed) {
-    auto k = k_force_t<float, float, false>;
-    k<<<grid, block, smem, s>>>(a);
-  } else {
-    auto k = k_force_t<double, double, true>;
-    k<<<grid, block, smem, s>>>(a);
+  const int block = a.R * KG;
+  if (mixed) k_force_t<float, float, false, KG, KU><<<grid, block, smem, s>>>(a);
+  else k_force_t<double, double, true, KG, KU><<<grid, block, smem, s>>>(a);
+}
+
+int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a, int variant) {
+  switch (variant) {
+    case 1: force_variant<4, 2>(s, mixed, a); break;
+    case 2: force_variant<8, 4>(s, mixed, a); break;
+    case 3: force_variant<8, 2>(s, mixed, a); break;
+    default: force_variant<4, 4>(s, mixed, a);
   }
   MEGA_CHECK_LAUNCH();
   return 0;

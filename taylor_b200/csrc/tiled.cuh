@@ -54,9 +54,12 @@ int build_tiles(cudaStream_t s, int32_t n, const int64_t* ptr, const int32_t* id
 int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* gx, const double* gy,
                  const double* gz, const int64_t* pos, bool f64, void* out);
 int configure_tiled_kernels();
+// launch variants of the two gathers (lanes per row x records in flight)
+int tiled_variants();
 int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
                          const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
-                         const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc);
-int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a);
+                         const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc,
+                         int variant = 0);
+int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a, int variant = 0);
 
 }  // namespace mega

@@ -203,6 +203,15 @@ class Mega:
         dm = None if dist_max is None else _f64(dist_max, (len(cnt), 3))
         check(_lib.lib().mega_set_instances(self.h, len(cnt), ptr(cnt), ptr(dm)), "set_instances")
 
+    def autotune(self, dt, mode="mixed", reps=5):
+        """Pick the fastest launch variant of each gather; returns the chosen
+        (defgrad, force) variants and the per-variant mean times (ms)."""
+        ch = np.zeros(2, np.int32)
+        t = np.zeros(8, np.float32)
+        check(_lib.lib().mega_autotune(self.h, float(dt), self.mode_bits(mode), int(reps), ptr(ch), ptr(t)),
+              "autotune")
+        return (int(ch[0]), int(ch[1])), t.reshape(2, 4)
+
     def set_precisions(self, fp64=True, mixed=True):
         check(_lib.lib().mega_set_precisions(self.h, (1 if fp64 else 0) | (2 if mixed else 0)), "set_precisions")
 

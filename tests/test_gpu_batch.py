@@ -72,3 +72,30 @@ def test_precision_mask_refuses_unbuilt_mode():
     with pytest.raises(_lib.MegaError):
         m.step(1, 3e-8, mode="fp64")
     m.close()
+
+
+def test_autotune_keeps_state_and_results():
+    bar = cases.taylor_bar(h=0.8e-3)
+    p = _lib.params(**cases.param_kwargs(bar))
+    dt = 3.0e-8
+    a = mega.Mega(bar, p)
+    b = mega.Mega(bar, p)
+    a.search_and_shapes()
+    b.search_and_shapes()
+    a.step(20, dt)
+    b.step(20, dt)
+    before = [a.download(f) for f in (_lib.F_DSP_TOT, _lib.F_VEL, _lib.F_STRESS, _lib.F_EPS)]
+    for mode in ("fp64", "mixed"):
+        choice, times = a.autotune(dt, mode=mode, reps=3)
+        assert all(0 <= c < 4 for c in choice)
+        assert np.all(times > 0)
+    after = [a.download(f) for f in (_lib.F_DSP_TOT, _lib.F_VEL, _lib.F_STRESS, _lib.F_EPS)]
+    for x, y in zip(before, after):
+        np.testing.assert_array_equal(x, y)
+    # another variant only regroups each row's partial sums
+    a.step(20, dt)
+    b.step(20, dt)
+    xa, xb = a.download(_lib.F_COO_CURRENT), b.download(_lib.F_COO_CURRENT)
+    assert np.abs(xa - xb).max() <= 1e-10 * np.abs(xb - bar["coo"]).max()
+    a.close()
+    b.close()
