@@ -266,7 +266,7 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo,
  * instances. */
 int mega_set_instances(int64_t h, int32_t ninst, const int32_t* inst_nodes, const double* dist_max);
 /* Autotuner: time each launch variant of the two per-step gathers (lanes
- * per row 4 or 8 x records in flight 4 or 2, in that order: variants 0..3)
+ * per row x records in flight: (4, 4), (4, 2), (4, 1), (8, 2), variants 0..3)
  * for the given precision on this context's lists, reps launches each,
  * keep the fastest, and leave the state as it was.  choice (2) receives the
  * deformation-gradient and force variants, times_ms (2 x 4, may be NULL) the

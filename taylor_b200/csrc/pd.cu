@@ -22,6 +22,7 @@
 #include <mutex>
 #include <set>
 #include "mega_internal.cuh"
+#include "tiled.cuh"
 
 namespace mega {
 namespace {
@@ -263,13 +264,21 @@ __global__ void k_pd_force(int32_t n, const double* __restrict__ X, const double
 }
 
 // ------------------------------------------------------------------ PMB
-// Bond-based force density and velocity-Verlet, one group of 4 lanes per
-// particle.  u_in is read, u_out written (double buffered: the kernel reads
-// every neighbour's displacement of this step while it advances its own).
+// Bond-based force density and velocity-Verlet.  The particles are
+// renumbered in bin-cell order at set-up, so a tile of R consecutive
+// particles has a compact neighbour set; a block per tile stages that set's
+// reference positions, displacements and volumes in shared memory and each
+// bond then reads only its 2-byte rank in the set (and its broken bit) from
+// HBM.  u_in is read, u_out written (double buffered: the kernel reads every
+// neighbour's displacement of this step while it advances its own).
 struct PmbArgs {
   int32_t n;
+  int32_t R;              // particles per tile
+  int32_t jmax;           // stride of jset
   const int64_t* rowptr;
-  const int32_t* col;
+  const int32_t* jset;    // per tile: the sorted neighbour set
+  const int32_t* jcnt;
+  const uint16_t* lidx;   // per bond: rank of its neighbour in the tile's set
   uint32_t* broken;       // bit per bond
   const double* vol;
   const double* X;        // reference positions (double-precision bond geometry)
@@ -286,78 +295,101 @@ struct PmbArgs {
 };
 
 // T = per-bond arithmetic: float (the mixed path: float bond geometry and
-// force, double accumulation of nothing but the integrator) or double (the
-// oracle's arithmetic, recomputed from X, for exact parity checks).
+// force from float offsets to the tile's first particle) or double (the
+// oracle's arithmetic, from X and u, for exact parity checks).
 constexpr int kGP = 8;  // lanes per particle of the bond loop
-constexpr int kUP = 4;  // bonds in flight per lane
-inline unsigned gridp(int64_t n) { return (unsigned)((n * kGP + 255) / 256); }
+constexpr int kUP = 4;  // bond ranks in flight per lane
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_pmb_step(PmbArgs a) {
-  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kGP;
+__global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
+  extern __shared__ double smp[];
+  const int64_t t = blockIdx.x;
+  const int cnt = a.jcnt[t];
+  const int32_t* js = a.jset + t * (int64_t)a.jmax;
+  const bool f64 = sizeof(T) == sizeof(double);
+  // staged set: FP64 8 doubles per particle (X, u, vol, pad); float: X as
+  // 3 doubles (the bond vector is rounded from the exact difference, as the
+  // FP64 path forms it) and one float4 (u - u_r0, vol)
+  double* sd = smp;
+  float4* sf = reinterpret_cast<float4*>(smp + ((3 * cnt + 1) & ~1));
+  const int64_t r0 = t * a.R;
+  const double ur0 = a.u_in[3 * r0], ur1 = a.u_in[3 * r0 + 1], ur2 = a.u_in[3 * r0 + 2];
+  for (int l = threadIdx.x; l < cnt; l += blockDim.x) {
+    const int64_t g = js[l];
+    const double x0 = a.X[3 * g], x1 = a.X[3 * g + 1], x2 = a.X[3 * g + 2];
+    const double u0 = a.u_in[3 * g], u1 = a.u_in[3 * g + 1], u2 = a.u_in[3 * g + 2];
+    const double v = a.vol[g];
+    if (f64) {
+      double2* d = reinterpret_cast<double2*>(sd + 8 * l);
+      d[0] = make_double2(x0, x1); d[1] = make_double2(x2, u0); d[2] = make_double2(u1, u2);
+      d[3] = make_double2(v, 0.0);
+    } else {
+      sd[3 * l] = x0; sd[3 * l + 1] = x1; sd[3 * l + 2] = x2;
+      sf[l] = make_float4((float)(u0 - ur0), (float)(u1 - ur1), (float)(u2 - ur2), (float)v);
+    }
+  }
+  __syncthreads();
+  const int64_t i = t * a.R + threadIdx.x / kGP;
   const int q = threadIdx.x & (kGP - 1);
   const unsigned gm = 0xFFu << (threadIdx.x & 24);
-  if (i >= a.n) return;
+  if (threadIdx.x / kGP >= a.R || i >= a.n) return;
   const double ui0 = a.u_in[3 * i], ui1 = a.u_in[3 * i + 1], ui2 = a.u_in[3 * i + 2];
   const double Xi0 = a.X[3 * i], Xi1 = a.X[3 * i + 1], Xi2 = a.X[3 * i + 2];
+  const float fu0 = (float)(ui0 - ur0), fu1 = (float)(ui1 - ur1), fu2 = (float)(ui2 - ur2);
   T f0 = T(0), f1 = T(0), f2 = T(0);
   unsigned nb = 0;
   const T c = (T)a.c, sc = (T)a.s_c;
   const int64_t p1 = a.rowptr[i + 1];
-  // per bond only its column index (and broken bit) comes from HBM; the
-  // bond vector is rebuilt from the reference positions, which like u and
-  // vol are gathered per particle and stay in L2.  kUP bonds per lane are
-  // loaded before any is used.
   for (int64_t pb = a.rowptr[i] + q; pb < p1; pb += kGP * kUP) {
-    int64_t jj[kUP];
-    double xj[kUP][3], uj[kUP][3], vj[kUP];
+    int lj[kUP];
     uint32_t wd[kUP];
 #pragma unroll
     for (int u = 0; u < kUP; ++u) {
       const int64_t p = pb + u * kGP;
-      jj[u] = p < p1 ? (int64_t)a.col[p] : i;
+      lj[u] = p < p1 ? (int)a.lidx[p] : -1;
       wd[u] = p < p1 ? a.broken[p >> 5] : 0u;
     }
 #pragma unroll
     for (int u = 0; u < kUP; ++u) {
-      const int64_t j = jj[u];
-      xj[u][0] = a.X[3 * j]; xj[u][1] = a.X[3 * j + 1]; xj[u][2] = a.X[3 * j + 2];
-      uj[u][0] = a.u_in[3 * j]; uj[u][1] = a.u_in[3 * j + 1]; uj[u][2] = a.u_in[3 * j + 2];
-      vj[u] = a.vol[j];
-    }
-#pragma unroll
-    for (int u = 0; u < kUP; ++u) {
       const int64_t p = pb + u * kGP;
-      const int64_t j = jj[u];
-      if (j == i) continue;  // the particle itself, or past the row
+      if (lj[u] < 0) continue;  // past the row
       const uint32_t bit = 1u << (p & 31);
       if (wd[u] & bit) continue;
-      T s, e0, e1, e2, l;
-      if (sizeof(T) == sizeof(double)) {
+      T s, e0, e1, e2, l, vj;
+      if (f64) {
         // the oracle's arithmetic: xi from X, eta = xi + (u_j - u_i), s = (|eta| - |xi|)/|xi|
-        const double x0 = xj[u][0] - Xi0, x1 = xj[u][1] - Xi1, x2 = xj[u][2] - Xi2;
-        e0 = (T)(x0 + (uj[u][0] - ui0));
-        e1 = (T)(x1 + (uj[u][1] - ui1));
-        e2 = (T)(x2 + (uj[u][2] - ui2));
-        const T L0 = (T)sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+        const double2* d = reinterpret_cast<const double2*>(sd + 8 * lj[u]);
+        const double2 q0 = d[0], q1 = d[1], q2 = d[2], q3 = d[3];
+        const double x0 = q0.x - Xi0, x1 = q0.y - Xi1, x2 = q1.x - Xi2;
+        const double L0d = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+        if (L0d == 0.0) continue;  // the particle itself
+        e0 = (T)(x0 + (q1.y - ui0));
+        e1 = (T)(x1 + (q2.x - ui1));
+        e2 = (T)(x2 + (q2.y - ui2));
+        const T L0 = (T)L0d;
         l = (T)sqrt((double)(e0 * e0 + e1 * e1 + e2 * e2));
         s = (l - L0) / L0;
+        vj = (T)q3.x;
       } else {
-        const T d0 = (T)(uj[u][0] - ui0), d1 = (T)(uj[u][1] - ui1), d2 = (T)(uj[u][2] - ui2);
-        const T x0 = (T)(xj[u][0] - Xi0), x1 = (T)(xj[u][1] - Xi1), x2 = (T)(xj[u][2] - Xi2);
+        const double* xq = sd + 3 * lj[u];
+        const float4 qb = sf[lj[u]];
+        const T x0 = (T)(xq[0] - Xi0), x1 = (T)(xq[1] - Xi1), x2 = (T)(xq[2] - Xi2);
         const T L0 = (T)sqrtf((float)(x0 * x0 + x1 * x1 + x2 * x2));
+        if (L0 == T(0)) continue;  // the particle itself
+        const T d0 = (T)(qb.x - fu0), d1 = (T)(qb.y - fu1), d2 = (T)(qb.z - fu2);
         // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|))
         e0 = x0 + d0; e1 = x1 + d1; e2 = x2 + d2;
         l = (T)sqrtf((float)(e0 * e0 + e1 * e1 + e2 * e2));
         const T num = T(2) * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
         s = num / (L0 * (l + L0));
+        vj = (T)qb.w;
       }
       if (s > sc) {
         atomicOr(&a.broken[p >> 5], bit);
         ++nb;
         continue;
       }
-      const T w = c * s * (T)vj[u] / l;
+      const T w = c * s * vj / l;
       f0 += w * e0; f1 += w * e1; f2 += w * e2;
     }
   }
@@ -386,6 +418,56 @@ __global__ void __launch_bounds__(256) k_pmb_step(PmbArgs a) {
     a.u_out[m] = u;
   }
   if (q == 0 && nb && a.nbroken) atomicAdd(a.nbroken, (unsigned long long)nb);
+}
+
+// ---- renumbering of the particles in bin-cell order
+__global__ void k_pmb_iperm(int32_t n, const int32_t* __restrict__ perm, int32_t* __restrict__ iperm) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r < n) iperm[perm[r]] = (int32_t)r;
+}
+// dst[r w + k] = src[perm[r] w + k] (to = true) or dst[perm[r] w + k] = src[r w + k]
+template <typename V>
+__global__ void k_pmb_perm(int32_t n, int w, const int32_t* __restrict__ perm, const V* __restrict__ src,
+                           V* __restrict__ dst, bool to) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n * w) return;
+  const int64_t r = e / w, k = e - r * w;
+  if (to) dst[e] = src[(int64_t)perm[r] * w + k];
+  else dst[(int64_t)perm[r] * w + k] = src[e];
+}
+__global__ void k_pmb_rowlen(int32_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ rowptr0,
+                             int32_t* __restrict__ len) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r < n) len[r] = (int32_t)(rowptr0[perm[r] + 1] - rowptr0[perm[r]]);
+}
+// warp per new row: the old row's entries in their order, columns renumbered
+__global__ void k_pmb_rows(int32_t n, const int32_t* __restrict__ perm, const int32_t* __restrict__ iperm,
+                           const int64_t* __restrict__ rowptr0, const int32_t* __restrict__ col0,
+                           const int64_t* __restrict__ rowptr1, int32_t* __restrict__ col1) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const int64_t a0 = rowptr0[perm[r]], len = rowptr0[perm[r] + 1] - a0, b0 = rowptr1[r];
+  for (int64_t k = lane; k < len; k += 32) col1[b0 + k] = iperm[col0[a0 + k]];
+}
+// per-bond flags between the two orders: new entry rowptr1[r] + k is old
+// entry rowptr0[perm[r]] + k.  to_new: old bytes -> new bits (OR); else new
+// bits -> old bytes.
+__global__ void k_pmb_flags(int32_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ rowptr0,
+                            const int64_t* __restrict__ rowptr1, uint32_t* __restrict__ bits,
+                            uint8_t* __restrict__ bytes, bool to_new) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const int64_t a0 = rowptr0[perm[r]], len = rowptr0[perm[r] + 1] - a0, b0 = rowptr1[r];
+  for (int64_t k = lane; k < len; k += 32) {
+    const int64_t p = b0 + k;
+    if (to_new) {
+      if (bytes[a0 + k]) atomicOr(&bits[p >> 5], 1u << (p & 31));
+    } else {
+      bytes[a0 + k] = (uint8_t)((bits[p >> 5] >> (p & 31)) & 1u);
+    }
+  }
 }
 
 // Pre-crack: break every bond whose reference segment X_i -> X_j crosses the
@@ -463,7 +545,10 @@ struct PmbCtx {
   int32_t n = 0;
   cudaStream_t s = nullptr;
   DevPool pool;
-  DevCSR csr;
+  DevCSR csr;          // in the bin-cell numbering
+  int32_t* perm = nullptr;      // new particle r = caller's particle perm[r]
+  int64_t* rowptr0 = nullptr;   // the caller's row offsets (bond flags map through them)
+  TileSet tiles;
   double *X = nullptr, *vol = nullptr, *u[2] = {nullptr, nullptr}, *vel = nullptr, *acl = nullptr;
   uint32_t* broken = nullptr;
   int8_t* fixed = nullptr;
@@ -487,10 +572,19 @@ struct PmbCtx {
 
 static PmbArgs pmb_args(PmbCtx* c, double dt) {
   PmbArgs a{};
-  a.n = c->n; a.rowptr = c->csr.rowptr; a.col = c->csr.col; a.broken = c->broken;
+  a.n = c->n; a.R = c->tiles.R; a.jmax = c->tiles.jmax; a.rowptr = c->csr.rowptr; a.jset = c->tiles.jset;
+  a.jcnt = c->tiles.jcnt; a.lidx = c->tiles.lidx; a.broken = c->broken;
   a.vol = c->vol; a.X = c->X; a.u_in = c->u[c->cur]; a.u_out = c->u[1 - c->cur]; a.vel = c->vel; a.acl = c->acl;
   a.fixed = c->fixed; a.c = c->c; a.s_c = c->s_c; a.inv_rho = 1.0 / c->rho; a.dt = dt; a.nbroken = c->nbroken;
   return a;
+}
+
+static void launch_pmb(PmbCtx* c, const PmbArgs& a) {
+  const unsigned grid = (unsigned)c->tiles.ntiles;
+  const int block = c->tiles.R * kGP;
+  const size_t smem = (c->f64 ? 64 : 40) * (size_t)c->tiles.maxcnt + 16;
+  if (c->f64) k_pmb_step<double><<<grid, block, smem, c->s>>>(a);
+  else k_pmb_step<float><<<grid, block, smem, c->s>>>(a);
 }
 
 }  // namespace mega
@@ -627,17 +721,22 @@ int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double*
                   int32_t mode, int64_t* handle, int64_t* nbonds) {
   if (n <= 0 || !coo || !vol || !vinit || !handle || !(horizon > 0) || !(rho > 0)) return MEGA_ERR_ARG;
   PmbCtx* c = new PmbCtx();
-  auto fail = [&](int code) { delete c; return code; };
+  DevPool tmp;  // set-up temporaries, freed (in stream order) before the stream goes
+  auto fail = [&](int code) {
+    tmp.free_all();
+    delete c;
+    return code;
+  };
   c->n = n; c->c = micromodulus; c->s_c = s_c; c->rho = rho;
   c->f64 = ((mode & 0xff) == MEGA_MODE_FP64);
   if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) return fail(MEGA_ERR_CUDA);
   c->pool.bind(c->s);
+  tmp.bind(c->s);
   const int64_t n3 = 3 * (int64_t)n;
 #define PA(ptr, cnt) do { if (c->pool.alloc(&(ptr), (size_t)(cnt))) return fail(MEGA_ERR_NOMEM); } while (0)
   double *win = nullptr, *sml = nullptr;
   PA(c->X, n3); PA(c->vol, n); PA(c->u[0], n3); PA(c->u[1], n3); PA(c->vel, n3); PA(c->acl, n3);
   PA(c->fixed, n); PA(c->nbroken, 1); PA(c->status, 1);
-  DevPool tmp(c->s);
   if (tmp.alloc(&win, n3) || tmp.alloc(&sml, 6 * (int64_t)n)) return fail(MEGA_ERR_NOMEM);
   std::vector<double> hw(n3, horizon);
   std::vector<int8_t> hf(n, 0);
@@ -655,18 +754,63 @@ int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double*
   cudaMemsetAsync(c->nbroken, 0, sizeof(unsigned long long), c->s);
   cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->s);
   const double dmax[3] = {0.0, 0.0, 0.0};
-  // spherical horizon: the ellipsoidal support test of SOFT_SEARCH (SHSUP)
-  int r = bin_search(c->s, n, c->X, win, sml, dmax, 0, 1, c->status, c->csr, nullptr, c->pool, nullptr);
+  // spherical horizon: the ellipsoidal support test of SOFT_SEARCH (SHSUP),
+  // in the caller's numbering, with the bin-cell order of the particles
+  DevCSR csr0;
+  PA(c->perm, n);
+  int r = bin_search(c->s, n, c->X, win, sml, dmax, 0, 1, c->status, csr0, nullptr, tmp, nullptr, c->perm);
   if (r) return fail(r);
-  const int64_t m = c->csr.nnz;
+  const int64_t m = csr0.nnz;
+  // renumber the particles in that order: rows keep their entries' order
+  int32_t *iperm = nullptr, *len = nullptr;
+  double* buf = nullptr;
+  int8_t* bf8 = nullptr;
+  if (tmp.alloc(&iperm, n) || tmp.alloc(&len, n) || tmp.alloc(&buf, n3) || tmp.alloc(&bf8, n))
+    return fail(MEGA_ERR_NOMEM);
+  const unsigned gn = (unsigned)((n + 255) / 256), g3 = (unsigned)((n3 + 255) / 256);
+  k_pmb_iperm<<<gn, 256, 0, c->s>>>(n, c->perm, iperm);
+  cudaMemcpyAsync(buf, c->X, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->s);
+  k_pmb_perm<double><<<g3, 256, 0, c->s>>>(n, 3, c->perm, buf, c->X, true);
+  cudaMemcpyAsync(buf, c->vel, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->s);
+  k_pmb_perm<double><<<g3, 256, 0, c->s>>>(n, 3, c->perm, buf, c->vel, true);
+  cudaMemcpyAsync(buf, c->vol, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->s);
+  k_pmb_perm<double><<<gn, 256, 0, c->s>>>(n, 1, c->perm, buf, c->vol, true);
+  cudaMemcpyAsync(bf8, c->fixed, n, cudaMemcpyDeviceToDevice, c->s);
+  k_pmb_perm<int8_t><<<gn, 256, 0, c->s>>>(n, 1, c->perm, bf8, c->fixed, true);
+  c->csr.n = n;
+  c->csr.nnz = m;
+  c->csr.gmaxn = csr0.gmaxn;
+  PA(c->rowptr0, (int64_t)n + 1);
+  cudaMemcpyAsync(c->rowptr0, csr0.rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToDevice, c->s);
+  PA(c->csr.rowptr, (int64_t)n + 1);
+  PA(c->csr.col, m);
+  k_pmb_rowlen<<<gn, 256, 0, c->s>>>(n, c->perm, csr0.rowptr, len);
+  if ((r = scan_counts(c->s, len, c->csr.rowptr, n, tmp))) return fail(r);
+  const unsigned gw = (unsigned)(((int64_t)n * 32 + 255) / 256);
+  k_pmb_rows<<<gw, 256, 0, c->s>>>(n, c->perm, iperm, csr0.rowptr, csr0.col, c->csr.rowptr, c->csr.col);
+  if (cudaGetLastError() != cudaSuccess) return fail(MEGA_ERR_CUDA);
+  // tiles of consecutive particles with their neighbour sets
+  if ((r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->tiles, c->pool, nullptr)))
+    return fail(r);
+  {
+    static bool smem_set = false;  // FP64 stages 64 bytes per particle, float 40: up to 64 KB
+    if (!smem_set) {
+      if (cudaFuncSetAttribute(k_pmb_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024 + 16) !=
+              cudaSuccess ||
+          cudaFuncSetAttribute(k_pmb_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 40 * 1024 + 16) !=
+              cudaSuccess)
+        return fail(MEGA_ERR_CUDA);
+      smem_set = true;
+    }
+  }
   PA(c->broken, (m + 31) / 32);
 #undef PA
   cudaMemsetAsync(c->broken, 0, sizeof(uint32_t) * ((m + 31) / 32), c->s);
-  if (broken0) {
-    std::vector<uint32_t> bits((m + 31) / 32, 0);
-    for (int64_t p = 0; p < m; ++p)
-      if (broken0[p]) bits[p >> 5] |= 1u << (p & 31);
-    cudaMemcpyAsync(c->broken, bits.data(), sizeof(uint32_t) * bits.size(), cudaMemcpyHostToDevice, c->s);
+  if (broken0) {  // the caller's order -> bits in the renumbered order
+    uint8_t* b0 = nullptr;
+    if (tmp.alloc(&b0, m)) return fail(MEGA_ERR_NOMEM);
+    cudaMemcpyAsync(b0, broken0, (size_t)m, cudaMemcpyHostToDevice, c->s);
+    k_pmb_flags<<<gw, 256, 0, c->s>>>(n, c->perm, c->rowptr0, c->csr.rowptr, c->broken, b0, true);
   }
   if (cudaStreamSynchronize(c->s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return fail(MEGA_ERR_CUDA);
   if (nbonds) *nbonds = m;
@@ -702,8 +846,7 @@ int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms) {
     MEGA_TRY(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < 2; ++k) {
       PmbArgs a = pmb_args(c, dt);
-      if (c->f64) k_pmb_step<double><<<gridp(c->n), 256, 0, c->s>>>(a);
-      else k_pmb_step<float><<<gridp(c->n), 256, 0, c->s>>>(a);
+      launch_pmb(c, a);
       c->cur = 1 - c->cur;
     }
     cudaError_t e = cudaStreamEndCapture(c->s, &gr);
@@ -719,8 +862,7 @@ int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms) {
   }
   for (; done < nsteps; ++done) {
     PmbArgs a = pmb_args(c, dt);
-    if (c->f64) k_pmb_step<double><<<gridp(c->n), 256, 0, c->s>>>(a);
-    else k_pmb_step<float><<<gridp(c->n), 256, 0, c->s>>>(a);
+    launch_pmb(c, a);
     MEGA_CHECK_LAUNCH();
     c->cur = 1 - c->cur;
   }
@@ -744,21 +886,34 @@ int mega_pmb_download(int64_t h, int32_t what, double* dst, int64_t* nbroken) {
   const int64_t n3 = 3 * (int64_t)c->n;
   if (nbroken) {
     unsigned long long v = 0;
-    MEGA_TRY(cudaMemcpy(&v, c->nbroken, sizeof(v), cudaMemcpyDeviceToHost));
+    MEGA_TRY(cudaMemcpyAsync(&v, c->nbroken, sizeof(v), cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
     *nbroken = (int64_t)v;
   }
   if (!dst) return 0;
   // after a step, u[cur] already holds the next step's predictor; the
   // displacement of the last completed step is the one it started from
   const double* ucur = c->steps > 0 ? c->u[1 - c->cur] : c->u[c->cur];
-  if (what == 0) MEGA_TRY(cudaMemcpy(dst, ucur, sizeof(double) * n3, cudaMemcpyDeviceToHost));
-  else if (what == 1) MEGA_TRY(cudaMemcpy(dst, c->vel, sizeof(double) * n3, cudaMemcpyDeviceToHost));
-  else if (what == 2) MEGA_TRY(cudaMemcpy(dst, c->acl, sizeof(double) * n3, cudaMemcpyDeviceToHost));
-  else if (what == 3) {
+  DevPool tp(c->s);
+  if (what >= 0 && what <= 2) {  // back to the caller's particle order
+    const double* src = what == 0 ? ucur : (what == 1 ? c->vel : c->acl);
+    double* d = nullptr;
+    MEGA_ALLOC(tp, d, n3);
+    k_pmb_perm<double><<<(unsigned)((n3 + 255) / 256), 256, 0, c->s>>>(c->n, 3, c->perm, src, d, false);
+    MEGA_CHECK_LAUNCH();
+    MEGA_TRY(cudaMemcpyAsync(dst, d, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+  } else if (what == 3) {  // the caller's list order
     const int64_t m = c->csr.nnz;
-    std::vector<uint32_t> bits((m + 31) / 32);
-    MEGA_TRY(cudaMemcpy(bits.data(), c->broken, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost));
-    for (int64_t p = 0; p < m; ++p) dst[p] = (bits[p >> 5] >> (p & 31)) & 1u;
+    uint8_t* d = nullptr;
+    MEGA_ALLOC(tp, d, m);
+    k_pmb_flags<<<(unsigned)(((int64_t)c->n * 32 + 255) / 256), 256, 0, c->s>>>(c->n, c->perm, c->rowptr0,
+                                                                              c->csr.rowptr, c->broken, d, false);
+    MEGA_CHECK_LAUNCH();
+    std::vector<uint8_t> hb(m);
+    MEGA_TRY(cudaMemcpyAsync(hb.data(), d, (size_t)m, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    for (int64_t p = 0; p < m; ++p) dst[p] = hb[p];
   } else return MEGA_ERR_ARG;
   return 0;
 }
