@@ -373,15 +373,21 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
       } else {
         const double* xq = sd + 3 * lj[u];
         const float4 qb = sf[lj[u]];
-        const T x0 = (T)(xq[0] - Xi0), x1 = (T)(xq[1] - Xi1), x2 = (T)(xq[2] - Xi2);
-        const T L0 = (T)sqrtf((float)(x0 * x0 + x1 * x1 + x2 * x2));
-        if (L0 == T(0)) continue;  // the particle itself
-        const T d0 = (T)(qb.x - fu0), d1 = (T)(qb.y - fu1), d2 = (T)(qb.z - fu2);
-        // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|))
-        e0 = x0 + d0; e1 = x1 + d1; e2 = x2 + d2;
-        l = (T)sqrtf((float)(e0 * e0 + e1 * e1 + e2 * e2));
-        const T num = T(2) * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
-        s = num / (L0 * (l + L0));
+        const float x0 = (float)(xq[0] - Xi0), x1 = (float)(xq[1] - Xi1), x2 = (float)(xq[2] - Xi2);
+        const float xx = x0 * x0 + x1 * x1 + x2 * x2;
+        if (xx == 0.f) continue;  // the particle itself
+        const float d0 = qb.x - fu0, d1 = qb.y - fu1, d2 = qb.z - fu2;
+        // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|)),
+        // lengths from the hardware reciprocal square root (about 2 ulp)
+        const float f_e0 = x0 + d0, f_e1 = x1 + d1, f_e2 = x2 + d2;
+        const float ee = f_e0 * f_e0 + f_e1 * f_e1 + f_e2 * f_e2;
+        const float rL0 = rsqrtf(xx), rl = rsqrtf(ee);
+        const float fL0 = xx * rL0, fl = ee * rl;
+        const float num = 2.f * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
+        s = (T)(num * rL0 * __frcp_rn(fl + fL0));
+        // eta / |eta| directly, so the force weight needs no division
+        e0 = (T)(f_e0 * rl); e1 = (T)(f_e1 * rl); e2 = (T)(f_e2 * rl);
+        l = T(1);
         vj = (T)qb.w;
       }
       if (s > sc) {
@@ -389,7 +395,7 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
         ++nb;
         continue;
       }
-      const T w = c * s * vj / l;
+      const T w = f64 ? c * s * vj / l : c * s * vj;  // the float path's eta is already unit
       f0 += w * e0; f1 += w * e1; f2 += w * e2;
     }
   }

@@ -188,6 +188,32 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
   float4* sa = reinterpret_cast<float4*>(sm);
   float2* sb = reinterpret_cast<float2*>(sa + cnt);
   const int64_t r0 = t * R;
+  const int64_t i = t * R + threadIdx.x / KG;
+  const int q = threadIdx.x & (KG - 1);
+  const unsigned gmask = group_mask<KG>();
+  const bool valid = threadIdx.x / KG < R && i < n;
+  // this lane's first KU packed records are requested before the staging,
+  // so their latency overlaps it
+  int64_t p = 0, pend = 0;
+  bool pre = false;
+  float4 pf[KU];
+  double2 pfa[KU], pfb[KU];
+  if (valid) {
+    p = rowptr[i] + q;
+    pend = rowptr[i + 1];
+    pre = p + (KU - 1) * KG < pend;
+    if (pre) {
+#pragma unroll
+      for (int u = 0; u < KU; ++u) {
+        if (F64) {
+          pfa[u] = __ldg((const double2*)pk + 2 * (p + u * KG));
+          pfb[u] = __ldg((const double2*)pk + 2 * (p + u * KG) + 1);
+        } else {
+          pf[u] = __ldg((const float4*)pk + p + u * KG);
+        }
+      }
+    }
+  }
   double ur0 = 0.0, ur1 = 0.0, ur2 = 0.0, dr0 = 0.0, dr1 = 0.0, dr2 = 0.0;
   if (!F64) {
     ur0 = dsp_tot[3 * r0]; ur1 = dsp_tot[3 * r0 + 1]; ur2 = dsp_tot[3 * r0 + 2];
@@ -206,10 +232,7 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
     }
   }
   __syncthreads();
-  const int64_t i = t * R + threadIdx.x / KG;
-  const int q = threadIdx.x & (KG - 1);
-  const unsigned gmask = group_mask<KG>();
-  if (threadIdx.x / KG >= R || i >= n) return;
+  if (!valid) return;
   const double ui0 = dsp_tot[3 * i], ui1 = dsp_tot[3 * i + 1], ui2 = dsp_tot[3 * i + 2];
   const double di0 = dsp[3 * i], di1 = dsp[3 * i + 1], di2 = dsp[3 * i + 2];
   const float fu0 = (float)(ui0 - ur0), fu1 = (float)(ui1 - ur1), fu2 = (float)(ui2 - ur2);
@@ -218,7 +241,6 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
 #pragma unroll
   for (int k = 0; k < 9; ++k) { F[k] = A(0); L[k] = A(0); }
   double ph0 = 0.0, ph1 = 0.0, ph2 = 0.0;
-  const int64_t pend = rowptr[i + 1];
   // One entry: F += (u_J - u_i) (x) g, L += (d_J - d_i) (x) g (+ phi d_J).
   auto body = [&](int64_t p, A g0, A g1, A g2, int l) {
     A u0, u1, u2, d0, d1, d2;
@@ -248,7 +270,16 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
   };
   // KU records in flight per lane before any is used (the loop is bound by
   // DRAM latency otherwise); each lane still sums its entries in list order.
-  int64_t p = rowptr[i] + q;
+  if (pre) {
+#pragma unroll
+    for (int u = 0; u < KU; ++u) {
+      if (F64)
+        body(p + u * KG, (A)pfa[u].x, (A)pfa[u].y, (A)pfb[u].x, (int)__double_as_longlong(pfb[u].y));
+      else
+        body(p + u * KG, (A)pf[u].x, (A)pf[u].y, (A)pf[u].z, __float_as_int(pf[u].w));
+    }
+    p += KU * KG;
+  }
   if (F64) {
     for (; p + (KU - 1) * KG < pend; p += KU * KG) {
       double2 ra[KU], rb[KU];
@@ -326,6 +357,32 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
   TS* sT = (TS*)smx;
   const int32_t* js = a.jset + t * (int64_t)a.jmax;
   const TS* tm = (const TS*)a.tmat;
+  const int64_t J = t * a.R + threadIdx.x / KG;
+  const int q = threadIdx.x & (KG - 1);
+  const unsigned gmask = group_mask<KG>();
+  const bool valid = threadIdx.x / KG < a.R && J < a.n;
+  // this lane's first KU packed records are requested before the staging,
+  // so their latency overlaps it
+  int64_t e = 0, c1 = 0;
+  bool pre = false;
+  float4 pf[KU];
+  double2 pfa[KU], pfb[KU];
+  if (valid) {
+    e = a.colptr[J] + q;
+    c1 = a.colptr[J + 1];
+    pre = e + (KU - 1) * KG < c1;
+    if (pre) {
+#pragma unroll
+      for (int u = 0; u < KU; ++u) {
+        if (F64) {
+          pfa[u] = __ldg((const double2*)a.pk + 2 * (e + u * KG));
+          pfb[u] = __ldg((const double2*)a.pk + 2 * (e + u * KG) + 1);
+        } else {
+          pf[u] = __ldg((const float4*)a.pk + e + u * KG);
+        }
+      }
+    }
+  }
   // thread per staged node: one index load, then its T row (12 values,
   // 48 or 96 bytes, 16-byte aligned) as independent vector loads
   for (int l = threadIdx.x; l < cnt; l += blockDim.x) {
@@ -351,15 +408,11 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
     if (nv == 12) { sT[l * nv + 9] = v[9]; sT[l * nv + 10] = v[10]; sT[l * nv + 11] = v[11]; }
   }
   __syncthreads();
-  const int64_t J = t * a.R + threadIdx.x / KG;
-  const int q = threadIdx.x & (KG - 1);
-  const unsigned gmask = group_mask<KG>();
   double ke = 0.0, ee = 0.0, tf0 = 0.0, tf1 = 0.0, tf2 = 0.0, tf3 = 0.0, tf4 = 0.0, tf5 = 0.0;
   unsigned st = 0;
-  if (threadIdx.x / KG < a.R && J < a.n) {
+  if (valid) {
     A f0 = A(0), f1 = A(0), f2 = A(0);
     double e0 = 0.0, e1 = 0.0, e2 = 0.0;
-    const int64_t c1 = a.colptr[J + 1];
     auto body = [&](int64_t e, A g0, A g1, A g2, int l) {
       const TS* T = sT + l * nv;
       f0 += (A)T[0] * g0 + (A)T[1] * g1 + (A)T[2] * g2;
@@ -370,7 +423,16 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
         e0 += s * (double)T[9]; e1 += s * (double)T[10]; e2 += s * (double)T[11];
       }
     };
-    int64_t e = a.colptr[J] + q;
+    if (pre) {
+#pragma unroll
+      for (int u = 0; u < KU; ++u) {
+        if (F64)
+          body(e + u * KG, (A)pfa[u].x, (A)pfa[u].y, (A)pfb[u].x, (int)__double_as_longlong(pfb[u].y));
+        else
+          body(e + u * KG, (A)pf[u].x, (A)pf[u].y, (A)pf[u].z, __float_as_int(pf[u].w));
+      }
+      e += KU * KG;
+    }
     if (F64) {
       for (; e + (KU - 1) * KG < c1; e += KU * KG) {
         double2 ra[KU], rb[KU];
@@ -534,7 +596,7 @@ int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* 
 }
 
 // The launch variants, in the order the autotuner tries them:
-// (KG, KU) = (4, 4), (4, 2), (8, 4), (8, 2).
+// (KG, KU) = (4, 4), (4, 2), (4, 1), (8, 2).
 constexpr int kVariants = 4;
 
 template <typename K>
@@ -563,7 +625,7 @@ int configure_tiled_kernels() {
   const int lim = 12 * 8 * 1024 + 1024;
   int r = 0;
   if ((r = configure_variant<4, 4>(lim)) || (r = configure_variant<4, 2>(lim)) ||
-      (r = configure_variant<8, 4>(lim)) || (r = configure_variant<8, 2>(lim)))
+      (r = configure_variant<4, 1>(lim)) || (r = configure_variant<8, 2>(lim)))
     return r;
   done = true;
   return 0;
@@ -597,7 +659,7 @@ int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, con
   switch (variant) {
     case 1: defgrad_variant<4, 2>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
       break;
-    case 2: defgrad_variant<8, 4>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
+    case 2: defgrad_variant<4, 1>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
       break;
     case 3: defgrad_variant<8, 2>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
       break;
@@ -621,7 +683,7 @@ static void force_variant(cudaStream_t s, bool mixed, const TiledForceArgs& a) {
 int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a, int variant) {
   switch (variant) {
     case 1: force_variant<4, 2>(s, mixed, a); break;
-    case 2: force_variant<8, 4>(s, mixed, a); break;
+    case 2: force_variant<4, 1>(s, mixed, a); break;
     case 3: force_variant<8, 2>(s, mixed, a); break;
     default: force_variant<4, 4>(s, mixed, a);
   }
