@@ -9,10 +9,12 @@
 // correction vectors b = e1 M^-1 and b_,x = -e1 M^-1 M_,x M^-1
 // (RK.f90:311-342), and finally phi_J = (b.H~)phi, grad phi_J =
 // (b_,x.H~ + b.H_,x)phi + (b.H~)phi_,x (RK.f90:346-405).
-// Lanes stride the neighbour list and accumulate the 4 symmetric 4x4
-// matrices; a butterfly reduction leaves the sums in every lane, each lane
-// inverts redundantly (no shared memory), then the lanes write their own
-// entries (coalesced SoA stores).
+// A group of kLPN lanes serves one node: the lanes stride the neighbour list
+// and accumulate the 4 symmetric 4x4 matrices, a butterfly reduction within
+// the group leaves the sums in every lane, each lane of the group inverts
+// redundantly (no shared memory), then the lanes write their own entries.
+// kLPN = 8 keeps the redundant per-node work to 8 copies while the ~60
+// neighbours still give every lane several entries.
 #include "mega_internal.cuh"
 
 namespace mega {
@@ -71,6 +73,8 @@ __device__ __forceinline__ int sidx(int j, int k) {
   return j == 0 ? k : (j == 1 ? 3 + k : (j == 2 ? 5 + k : 9));
 }
 
+constexpr int kLPN = 8;  // lanes per node
+
 __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __restrict__ coo,
                                                    const double* __restrict__ win,
                                                    const int32_t* __restrict__ ebc_nodes,
@@ -79,15 +83,16 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
                                                    double ql_len, int shsup, double* __restrict__ shp,
                                                    double* __restrict__ gx, double* __restrict__ gy,
                                                    double* __restrict__ gz, unsigned* __restrict__ status) {
-  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= n) return;
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kLPN;
+  const int lane = threadIdx.x & (kLPN - 1);
+  const unsigned gm = ((1u << kLPN) - 1u) << (threadIdx.x & (32 - kLPN));
+  if (i >= n) return;  // whole groups leave together
   const double xi[3] = {coo[3 * i], coo[3 * i + 1], coo[3 * i + 2]};
   const int64_t p0 = rowptr[i], p1 = rowptr[i + 1];
   double M[10], Mx[10], My[10], Mz[10], psum = 0.0;
 #pragma unroll
   for (int k = 0; k < 10; ++k) { M[k] = 0.0; Mx[k] = 0.0; My[k] = 0.0; Mz[k] = 0.0; }
-  for (int64_t p = p0 + lane; p < p1; p += 32) {
+  for (int64_t p = p0 + lane; p < p1; p += kLPN) {
     const int64_t j = col[p];
     const double xj[3] = {coo[3 * j], coo[3 * j + 1], coo[3 * j + 2]};
     const double aj[3] = {win[3 * j], win[3 * j + 1], win[3 * j + 2]};
@@ -108,14 +113,14 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
       }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    psum += __shfl_xor_sync(0xffffffffu, psum, o);
+  for (int o = kLPN / 2; o > 0; o >>= 1) {
+    psum += __shfl_xor_sync(gm, psum, o);
 #pragma unroll
     for (int k = 0; k < 10; ++k) {
-      M[k] += __shfl_xor_sync(0xffffffffu, M[k], o);
-      Mx[k] += __shfl_xor_sync(0xffffffffu, Mx[k], o);
-      My[k] += __shfl_xor_sync(0xffffffffu, My[k], o);
-      Mz[k] += __shfl_xor_sync(0xffffffffu, Mz[k], o);
+      M[k] += __shfl_xor_sync(gm, M[k], o);
+      Mx[k] += __shfl_xor_sync(gm, Mx[k], o);
+      My[k] += __shfl_xor_sync(gm, My[k], o);
+      Mz[k] += __shfl_xor_sync(gm, Mz[k], o);
     }
   }
   double Mf[4][4];
@@ -174,7 +179,7 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
 #pragma unroll
     for (int k = 0; k < 4; ++k) out[k] = t[0] * Mi[0][k] + t[1] * Mi[1][k] + t[2] * Mi[2][k] + t[3] * Mi[3][k];
   }
-  for (int64_t p = p0 + lane; p < p1; p += 32) {
+  for (int64_t p = p0 + lane; p < p1; p += kLPN) {
     const int64_t j = col[p];
     const double xj[3] = {coo[3 * j], coo[3 * j + 1], coo[3 * j + 2]};
     const double aj[3] = {win[3 * j], win[3 * j + 1], win[3 * j + 2]};
@@ -201,7 +206,7 @@ int rk_shapes(cudaStream_t s, const mega_params& p, int32_t n, const double* coo
               unsigned* status) {
   if (p.rk_degree != 1 || p.rk_cont != 3) return MEGA_ERR_UNSUPPORTED;
   const int block = 128;
-  const unsigned grid = (unsigned)(((int64_t)n * 32 + block - 1) / block);
+  const unsigned grid = (unsigned)(((int64_t)n * kLPN + block - 1) / block);
   k_rk_shapes<<<grid, block, 0, s>>>(n, coo, win, ebc_nodes, csr.rowptr, csr.col, p.ql, p.ql_coef, p.ql_len,
                                      p.shsup, shp, gx, gy, gz, status);
   MEGA_CHECK_LAUNCH();

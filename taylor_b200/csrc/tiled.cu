@@ -362,12 +362,12 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
   const unsigned gmask = group_mask<KG>();
   const bool valid = threadIdx.x / KG < a.R && J < a.n;
   // this lane's first KU packed records are requested before the staging,
-  // so their latency overlaps it
+  // so their latency overlaps it (FP64 records only)
   int64_t e = 0, c1 = 0;
   bool pre = false;
   float4 pf[KU];
   double2 pfa[KU], pfb[KU];
-  if (valid) {
+  if (F64 && valid) {  // measured: pays in FP64, costs occupancy in mixed
     e = a.colptr[J] + q;
     c1 = a.colptr[J + 1];
     pre = e + (KU - 1) * KG < c1;
@@ -408,6 +408,10 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
     if (nv == 12) { sT[l * nv + 9] = v[9]; sT[l * nv + 10] = v[10]; sT[l * nv + 11] = v[11]; }
   }
   __syncthreads();
+  if (!F64 && valid) {
+    e = a.colptr[J] + q;
+    c1 = a.colptr[J + 1];
+  }
   double ke = 0.0, ee = 0.0, tf0 = 0.0, tf1 = 0.0, tf2 = 0.0, tf3 = 0.0, tf4 = 0.0, tf5 = 0.0;
   unsigned st = 0;
   if (valid) {
