@@ -149,7 +149,20 @@ struct Trial {
 // of sigma and eps, eps += dstrain, elastic predictor.
 template <typename T, bool LEAN>
 __device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Trial<T, LEAN>& w) {
-  const double* fgi = a.fg + 18 * i;
+  // F, G0 (18 doubles), stress and strain (6 each) as 16-byte loads
+  double fgi[18], sv[6], ev[6];
+  {
+    const double2* f2 = reinterpret_cast<const double2*>(a.fg + 18 * i);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { const double2 v = f2[k]; fgi[2 * k] = v.x; fgi[2 * k + 1] = v.y; }
+    const double2* s2 = reinterpret_cast<const double2*>(a.stress + 6 * i);
+    const double2* e2 = reinterpret_cast<const double2*>(a.strain + 6 * i);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double2 v = s2[k], u = e2[k];
+      sv[2 * k] = v.x; sv[2 * k + 1] = v.y; ev[2 * k] = u.x; ev[2 * k + 1] = u.y;
+    }
+  }
   w.mi = a.matidx[i];
   if (!LEAN) w.me = a.mats[w.mi];
   const MatEntry& me = LEAN ? a.mats[w.mi] : w.me;
@@ -161,7 +174,7 @@ __device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Tri
   w.det = 1.0;
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    const double so = a.stress[6 * i + k], eo = a.strain[6 * i + k];
+    const double so = sv[k], eo = ev[k];
     if (!LEAN) { w.sold[k] = so; w.eold[k] = eo; }
     sig[k] = (T)so;
     w.eps6[k] = (T)eo;
@@ -288,8 +301,15 @@ __device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Tr
     enew[k] = (double)w.eps6[k];
     sinc[k] = snew[k] - (LEAN ? a.stress[6 * i + k] : w.sold[k]);
     einc[k] = enew[k] - (LEAN ? a.strain[6 * i + k] : w.eold[k]);
-    a.stress[6 * i + k] = snew[k];
-    a.strain[6 * i + k] = enew[k];
+  }
+  {
+    double2* s2 = reinterpret_cast<double2*>(a.stress + 6 * i);
+    double2* e2 = reinterpret_cast<double2*>(a.strain + 6 * i);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      s2[k] = make_double2(snew[2 * k], snew[2 * k + 1]);
+      e2[k] = make_double2(enew[2 * k], enew[2 * k + 1]);
+    }
   }
   a.eps[i] = ep;
   const double eq = enew[0] * enew[0] + enew[1] * enew[1] + enew[2] * enew[2] +
@@ -313,19 +333,31 @@ __device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Tr
 #pragma unroll
   for (int k = 0; k < 6; ++k) sn[k] = (T)snew[k];
   v2t(sn, S);
-  TS* to = (TS*)a.tmat + 12 * i;
+  TS tv[12];
 #pragma unroll
   for (int k = 0; k < 3; ++k)
 #pragma unroll
     for (int mm = 0; mm < 3; ++mm)
-      to[3 * k + mm] = (TS)(vj * (S[k][0] * w.IF[mm][0] + S[k][1] * w.IF[mm][1] + S[k][2] * w.IF[mm][2]));
+      tv[3 * k + mm] = (TS)(vj * (S[k][0] * w.IF[mm][0] + S[k][1] * w.IF[mm][1] + S[k][2] * w.IF[mm][2]));
+  tv[9] = tv[10] = tv[11] = TS(0);
   if (a.has_body) {
     const double rvj = m.rho * vol * w.det;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const double b = (a.bodyforce ? a.bodyforce[3 * i + k] : 0.0) + a.grav[k];
-      to[9 + k] = (TS)(b * rvj);
+      tv[9 + k] = (TS)(b * rvj);
     }
+  }
+  // the 12-value row (48 or 96 bytes, 16-byte aligned) as vector stores
+  if (sizeof(TS) == 4) {
+    float4* t4 = reinterpret_cast<float4*>((TS*)a.tmat + 12 * i);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      t4[k] = make_float4((float)tv[4 * k], (float)tv[4 * k + 1], (float)tv[4 * k + 2], (float)tv[4 * k + 3]);
+  } else {
+    double2* t2 = reinterpret_cast<double2*>((TS*)a.tmat + 12 * i);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) t2[k] = make_double2((double)tv[2 * k], (double)tv[2 * k + 1]);
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k)
