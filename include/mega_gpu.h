@@ -70,6 +70,8 @@ extern "C" {
 /* ---- material types handled by the fused force kernel ------------------- */
 #define MEGA_MAT_ELASTIC      1  /* CONSTITUTION.F90:48-52 */
 #define MEGA_MAT_VONMISES     2  /* CONSTITUTE_VONMISES.F90:21-158 */
+#define MEGA_MAT_DRUCKER_PRAGER 3 /* CONSTITUTE_DRUCKPRAG.F90:17-241 (shear yield, damage) */
+#define MEGA_MAT_VM_DAMAGE    6  /* CONSTITUTE_VONMISES_DAM.F90:21-196 (J2 + damage) */
 #define MEGA_MAT_VM_RATE      7  /* power-law rate-dependent J2 (no reference
                                     counterpart): sigma_y = A + B*ep^n *
                                     (1 + C*ln(max(epdot,epdot0)/epdot0));
@@ -91,7 +93,9 @@ enum mega_field {
   MEGA_F_WAVE_VEL    = 11,/* (N) GMAX_WVEL                                   */
   MEGA_F_DSP_TOT_PHY = 12,/* (3N) physical total displacement                */
   MEGA_F_PRFORCE     = 13,/* (3,N) reaction force on fixed DOFs              */
-  MEGA_F_NEWTON_IT   = 14 /* (N) Newton iterations of the last step (int32 stored as double) */
+  MEGA_F_NEWTON_IT   = 14,/* (N) Newton iterations of the last step (int32 stored as double) */
+  MEGA_F_STATE_AUX   = 15 /* (4,N) STATE(1,2,4,5) = EPS_SHEAR, EPS_VOL, DAM, DAM_SV of the damaged
+                             models (materials 3, 6); MEGA_ERR_STATE when no node has one */
 };
 
 /* Scalars reported by mega_scalars (energies are those MAIN.F90:524-555 writes). */

@@ -518,9 +518,131 @@ void estimate_moduli(const double sinc[6], const double einc[6], double& shear, 
   bulk = bt;
 }
 
-// CONSTITUTION.F90:46-85 dispatch.  status bits as in mega_gpu.h.
+// Damage shared by both damaged models (CONSTITUTE_VONMISES_DAM.F90:94-125,
+// CONSTITUTE_DRUCKPRAG.F90:84-113): eta = TENSOR_NORM(total strain) (the
+// stress norm, as written); between K_I and K_C the damage follows
+// K_C (eta - K_I) / (eta (K_C - K_I)), capped at DAM_MAX.
+static void damage_update(const double total_strain[6], double k_i, double k_c, double dam_max, double& dam,
+                          double& dam_sv) {
+  const double eta = tensor_norm(total_strain);
+  const double k_i_check = dam_sv + k_i;
+  if (eta < k_i_check) {
+  } else if (eta > k_i && eta < k_c) {
+    dam = k_c * (eta - k_i) / (eta * (k_c - k_i));
+    dam_sv = eta;
+    dam_sv = dam_sv - k_i;
+  }
+  if (dam > dam_max) dam = dam_max;
+}
+
+// effective predictor STRESS / (1 - DAM) + MATMUL(ELAS_MAT, INC_STRAIN)
+static void effective_predictor(const double stress[6], double dam, const double* props, const double inc[6],
+                                double eff[6]) {
+  double lam = props[27], mu = props[28], l2m = props[29];
+  double C[6][6] = {};
+  C[0][0] = C[1][1] = C[2][2] = l2m;
+  C[3][3] = C[4][4] = C[5][5] = mu;
+  C[0][1] = C[1][0] = C[0][2] = C[2][0] = C[2][1] = C[1][2] = lam;
+  for (int r = 0; r < 6; ++r) {
+    double v = 0.0;
+    for (int c = 0; c < 6; ++c) v += C[r][c] * inc[c];
+    eff[r] = stress[r] / (1.0 - dam) + v;
+  }
+}
+
+// VON_MISES_DAM (CONSTITUTE_VONMISES_DAM.F90:21-196): J2 with the power
+// hardening of VON_MISES in effective-stress space, isotropic damage.
+// stress: the rotated old stress in, the new stress out.
+int von_mises_dam(double stress[6], const double total_strain[6], const double inc[6], double state[20],
+                  const double* props, int maxit, bool* capped) {
+  const double poiss = props[0], young = props[1], sig0 = props[3], B = props[4], ce = props[5];
+  const double k_i = props[8], k_c = props[9], dam_max = props[10];
+  const double mu = shear_mod(young, poiss);
+  double eps = state[2], dam = state[3], dam_sv = state[4];
+  double eff[6], dev[6], sph[6];
+  effective_predictor(stress, dam, props, inc, eff);
+  dev_proj(eff, dev);
+  damage_update(total_strain, k_i, k_c, dam_max, dam, dam_sv);
+  sphr_proj(eff, sph);
+  const double tn = tensor_norm(dev);
+  const double s23 = std::sqrt(2.0 / 3.0);
+  const double sig23 = s23 * sig0;
+  double xk = sig23 * std::pow(1.0 + B * eps, ce);
+  double yld = tn - xk;
+  int it = 0;
+  if (yld > 0.0) {
+    double dg = 0.0;
+    const double epst = eps;
+    for (int i = 1; i <= maxit; ++i) {
+      ++it;
+      xk = sig23 * std::pow(1.0 + B * eps, ce);
+      yld = tn - xk - (2.0 * mu * dg);
+      if (std::fabs(yld) > sig23 * (double)1.0e-5f) {
+        const double xkp = B * ce * sig0 * std::pow(1.0 + B * eps, ce - 1.0);
+        const double dy = -2.0 * mu * (1.0 + xkp / 3.0 / mu);
+        dg = dg - yld / dy;
+        if (i == maxit && capped) *capped = true;
+      } else {
+        eps = epst + s23 * dg;
+        break;
+      }
+      eps = epst + s23 * dg;
+    }
+    for (int k = 0; k < 6; ++k) dev[k] = dev[k] - dg * 2.0 * mu * dev[k] / tn;
+  }
+  state[2] = eps;
+  state[3] = dam;
+  state[4] = dam_sv;
+  for (int k = 0; k < 6; ++k) stress[k] = (-sph[k] + dev[k]) * (1.0 - dam);
+  return it;
+}
+
+// DRUCK_PRAG (CONSTITUTE_DRUCKPRAG.F90:17-241): Drucker-Prager shear yield
+// with non-associated flow and isotropic damage in effective-stress space.
+// The tension branch is unreachable as written (its flag is never set) and
+// is not restated.  stress: the rotated old stress in, the new stress out.
+int druck_prag(double stress[6], const double total_strain[6], const double inc[6], double state[20],
+               const double* props) {
+  const double poiss = props[0], young = props[1];
+  const double q_phi = props[24], k_phi = props[25], q_psi = props[26];
+  const double k_i = props[8], k_c = props[9], dam_max = props[10];
+  double eps_shear = state[0], eps_vol = state[1], eps = state[2], dam = state[3], dam_sv = state[4];
+  double eff[6], dev[6];
+  effective_predictor(stress, dam, props, inc, eff);
+  damage_update(total_strain, k_i, k_c, dam_max, dam, dam_sv);
+  dev_proj(eff, dev);
+  const double tau_pre = tensor_norm(dev);
+  const double sph_pre = (eff[0] + eff[1] + eff[2]) / 3.0;
+  const double f_shear = tau_pre + q_phi * sph_pre - k_phi;
+  int plastic = 0;
+  if (f_shear < 0.0) {
+    for (int k = 0; k < 6; ++k) stress[k] = eff[k];
+  } else {
+    plastic = 1;
+    const double tau = k_phi - q_phi * sph_pre;
+    const double bulk = bulk_mod(young, poiss), shear = shear_mod(young, poiss);
+    const double gamma = f_shear / (2.0 * shear + bulk * q_phi * q_psi);
+    const double sph = sph_pre - bulk * q_psi * gamma;
+    for (int k = 0; k < 6; ++k) stress[k] = dev[k] * tau / tau_pre;
+    stress[0] += sph; stress[1] += sph; stress[2] += sph;
+    eps_shear = eps_shear + gamma * std::sqrt(2.0 / 3.0 + 2.0 / 9.0 * q_psi * q_psi);
+    eps = eps + eps_shear;
+  }
+  for (int k = 0; k < 6; ++k) stress[k] = stress[k] * (1.0 - dam);
+  state[0] = eps_shear;
+  state[1] = eps_vol;
+  state[2] = eps;
+  state[3] = dam;
+  state[4] = dam_sv;
+  return plastic;  // a closed-form return counts as one pass
+}
+
+// CONSTITUTION.F90:46-85 dispatch.  status bits as in mega_gpu.h.  The
+// damaged models (3, 6) also need the rotated old stress (in stress), the
+// total and the incremental strain; without them they are rejected.
 int constitution(const double spred[6], int mat, const double* props, double dlt, double state[20],
-                 double stress[6], int maxit, double rtol, int* status, int* iters_out, int solver = 0) {
+                 double stress[6], int maxit, double rtol, int* status, int* iters_out, int solver = 0,
+                 const double* total_strain = nullptr, const double* inc_strain = nullptr) {
   int it = 0;
   bool capped = false;
   switch (mat) {
@@ -532,6 +654,14 @@ int constitution(const double spred[6], int mat, const double* props, double dlt
       break;
     case MEGA_MAT_VM_RATE:
       it = vm_rate(stress, spred, state, props, dlt, rtol, maxit, solver, -1.0, &capped, nullptr);
+      break;
+    case MEGA_MAT_DRUCKER_PRAGER:
+      if (!total_strain || !inc_strain) { *status |= MEGA_ST_BAD_MATERIAL; break; }
+      it = druck_prag(stress, total_strain, inc_strain, state, props);
+      break;
+    case MEGA_MAT_VM_DAMAGE:
+      if (!total_strain || !inc_strain) { *status |= MEGA_ST_BAD_MATERIAL; break; }
+      it = von_mises_dam(stress, total_strain, inc_strain, state, props, maxit, &capped);
       break;
     default:
       *status |= MEGA_ST_BAD_MATERIAL;
@@ -719,6 +849,21 @@ int orc_constitution(int n, const double* spred, const int* mat, const double* p
   return status;
 }
 
+// The damaged models on their own: stress holds the rotated old stress on
+// entry and the new stress on return; tot = total strain after the step,
+// inc = the strain increment (the LSTRAIN and STRAIN of CONSTITUTION).
+int orc_damaged(int n, const int* mat, const double* props, const double* tot, const double* inc, double* state,
+                double* stress, int* iters, int maxit) {
+  int status = 0;
+  for (int i = 0; i < n; ++i) {
+    double spred[6];  // unused by the damaged models (they form their own predictor)
+    for (int k = 0; k < 6; ++k) spred[k] = stress[6 * (size_t)i + k];
+    constitution(spred, mat[i], props + 30 * (size_t)i, 0.0, state + 20 * (size_t)i, stress + 6 * (size_t)i,
+                 maxit, 0.0, &status, iters ? iters + i : nullptr, 0, tot + 6 * (size_t)i, inc + 6 * (size_t)i);
+  }
+  return status;
+}
+
 // Rate-dependent return mapping with an explicit Newton start (the learned
 // guess enters here).  dg0 < 0 selects the plain start.
 int orc_vm_rate(int n, const double* spred, const double* props, double dt, double rtol,
@@ -736,6 +881,83 @@ int orc_vm_rate(int n, const double* spred, const double* props, double dt, doub
   return status;
 }
 
+// ------------------------------------------------------------------ NSNI
+// Naturally stabilised nodal integration (ITYPE_INT = 2).  The reference's
+// NSNI is unfinished (its second derivatives are never formed on the live
+// path and its moments never assigned, FINT.F90:441-576, 707-753, 1120-1222),
+// so this restates the published method (Hillman & Chen 2016, IJNME 107:603)
+// in the form the reference lays out: smoothed second derivatives from the
+// shape-function gradients on the faces of each node's smoothing cell
+// (FINT.F90:446-535), the strain-gradient increments of D_HUGHES_WINGET
+// (HUGHES_WINGET.F90:84-165), stress gradients kept per node
+// (LOCAL_DX_STRESS, MAIN.F90:62, 206) and the force term
+// B_{,a}^T sigma_{,a} V J M_a (FINT.F90:1127-1208) with the second moments
+// M_a = (cell width_a)^2 / 12 of SECOND_MOMENT (PRE_MODEL_SECOND_MOMENT.F90).
+// Stress gradients evolve with the elastic moduli (the stabilisation acts on
+// the modes nodal integration misses, not on the material response).
+
+// Smoothed second derivatives of node i's shape functions (6 per neighbour,
+// order XX, YY, ZZ, XY, YZ, XZ as SHPDD_SM): RK1 gradients at the six face
+// points x +- SM_LEN (order +X, -X, +Y, -Y, +Z, -Z), differenced over the
+// cell width.  Returns false if a moment matrix was singular.
+static bool nsni_second_derivatives(const double x[3], const double sml[6], const double* gcoo,
+                                    const double* gwin, const int* nb, int ln, const int32_t* ebcs,
+                                    const mega_params* p, double* dd, std::vector<double>& work) {
+  std::vector<double> g(6 * 3 * (size_t)ln), sh(ln);
+  bool ok = true;
+  for (int f = 0; f < 6; ++f) {
+    double pt[3] = {x[0], x[1], x[2]};
+    const int a = f / 2;
+    pt[a] = (f % 2 == 0) ? x[a] + sml[f] : x[a] - sml[f];
+    ok = rk1(pt, gcoo, gwin, nb, ln, ebcs, p->ql != 0, p->ql_coef, p->ql_len, p->shsup != 0, sh.data(),
+             g.data() + 3 * (size_t)ln * f, work) && ok;
+  }
+  for (int j = 0; j < ln; ++j) {
+    double D[3][3];  // D[a][b]: difference along a of the b-derivative
+    for (int a = 0; a < 3; ++a) {
+      const double w = sml[2 * a] + sml[2 * a + 1];
+      for (int b = 0; b < 3; ++b)
+        D[a][b] = (g[3 * ((size_t)ln * (2 * a) + j) + b] - g[3 * ((size_t)ln * (2 * a + 1) + j) + b]) / w;
+    }
+    double* o = dd + 6 * (size_t)j;
+    o[0] = D[0][0];
+    o[1] = D[1][1];
+    o[2] = D[2][2];
+    o[3] = 0.5 * (D[0][1] + D[1][0]);
+    o[4] = 0.5 * (D[1][2] + D[2][1]);
+    o[5] = 0.5 * (D[0][2] + D[2][0]);
+  }
+  return ok;
+}
+
+// index of S_(m a) in the XX, YY, ZZ, XY, YZ, XZ order (XMAP/YMAP/ZMAP of
+// FINT.F90:714-726)
+static const int kDD[3][3] = {{0, 3, 5}, {3, 1, 4}, {5, 4, 2}};
+
+// D_HUGHES_WINGET (HUGHES_WINGET.F90:84-165): the derivative of the
+// objective strain increment along one direction, DG = DL A^-1 -
+// L A^-1 (DL / 2) A^-1 with A = I + L / 2; engineering shear.
+static void d_hughes_winget(const M3 L, const M3 DL, double de[6], bool exact) {
+  M3 A, Ai, DA, t, ida, t1, t2, E;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      A[i][j] = (i == j ? 1.0 : 0.0) + 0.5 * L[i][j];
+      DA[i][j] = 0.5 * DL[i][j];
+    }
+  inv3(A, Ai, exact);
+  M3 nAi;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) nAi[i][j] = -Ai[i][j];
+  mm3(nAi, DA, t);
+  mm3(t, Ai, ida);
+  mm3(DL, Ai, t1);
+  mm3(L, ida, t2);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) E[i][j] = 0.5 * ((t1[i][j] + t2[i][j]) + (t1[j][i] + t2[j][i]));
+  t2v(E, de);
+  de[3] = 2.0 * de[3]; de[4] = 2.0 * de[4]; de[5] = 2.0 * de[5];
+}
+
 // CONSTRUCT_FINT (FINT.F90:16-1336), Lagrangian DNI path.  When linit, the
 // shape functions are built (RK1) and stored; otherwise they are recalled.
 // nthreads > 1 keeps the per-thread FINT_TEMP/FEXT_TEMP buffers.
@@ -747,8 +969,11 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
                        const double* gdinc_tot, const int* gn, const int* gstart,
                        const int* gstack, double* shp_stack, double* dshp_stack, int linit,
                        double dlt, double* fint, double* fext, double* gmax_wvel,
-                       double* gstrain_eq, double* gint_work, int nthreads, int* newton_iters) {
+                       double* gstrain_eq, double* gint_work, int nthreads, int* newton_iters,
+                       const double* sm_len, double* ddshp, double* sgrad) {
   const bool exact = p->inv3_exact != 0;
+  const bool nsni = p->itype_int == 2;
+  if (nsni && (!sm_len || !ddshp || !sgrad)) return -2;
   int status = 0;
   int nt = std::max(1, nthreads);
   std::vector<double> fint_t((size_t)nt * 3 * n, 0.0), fext_t((size_t)nt * 3 * n, 0.0);
@@ -777,13 +1002,16 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
         if (!rk1(gcoo + 3 * (size_t)i, gcoo, gwin, nb.data(), ln, gebc_nodes, p->ql != 0, p->ql_coef,
                  p->ql_len, p->shsup != 0, shp_stack + s, dshp_stack + 3 * s, work))
           status |= MEGA_ST_SINGULAR_MOMENT;
+        if (nsni && !nsni_second_derivatives(gcoo + 3 * (size_t)i, sm_len + 6 * (size_t)i, gcoo, gwin, nb.data(),
+                                             ln, gebc_nodes, p, ddshp + 6 * s, work))
+          status |= MEGA_ST_SINGULAR_MOMENT;
       }
       for (int j = 0; j < ln; ++j) {                                  // FINT.F90:354-359
         shp0[j] = shp_stack[s + j];
         for (int c = 0; c < 3; ++c) shpd[3 * j + c] = dshp_stack[3 * (s + j) + c];
       }
       double det = 1.0;
-      M3 fm;
+      M3 fm, ifm_s = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}, L_s = {}, R_s = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
       if (p->finite_strain) {                                         // FINT.F90:361-391
         for (int k = 0; k < 3; ++k)
           for (int l = 0; l < 3; ++l) {
@@ -794,6 +1022,7 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
         det = det_abs(fm);
         M3 ifm;
         inv3(fm, ifm, exact);
+        std::memcpy(ifm_s, ifm, sizeof(M3));
         for (int j = 0; j < ln; ++j) {
           double t[3] = {shpd[3 * j], shpd[3 * j + 1], shpd[3 * j + 2]};
           double o[3] = {0, 0, 0};
@@ -818,6 +1047,8 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
         hughes_winget(L, R, strain, D, exact);
         rotate_tensor(R, lstress);
         rotate_tensor(R, lstrain);
+        std::memcpy(L_s, L, sizeof(M3));
+        std::memcpy(R_s, R, sizeof(M3));
       } else {                                                        // FINT.F90:772-783
         for (int k = 0; k < 6; ++k) strain[k] = 0.0;
         for (int j = 0; j < ln; ++j) {
@@ -845,7 +1076,7 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
       }
       int it = 0;
       constitution(spred, gmat[i], lprop, dlt, lstate, lstress, p->newton_max_iter, p->newton_rtol,
-                   &status, &it, p->rate_solver);
+                   &status, &it, p->rate_solver, lstrain, strain);
       if (newton_iters) newton_iters[i] = it;
       for (int k = 0; k < 20; ++k) gstate[20 * (size_t)i + k] = lstate[k];   // FINT.F90:809-811
       double sinc[6], einc[6];
@@ -883,6 +1114,65 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
           double fb = lbod ? shp0[j] * lbod[c] * dens : 0.0;
           ET[3 * jj + c] += (fb + fg) * vol * det;
         }
+      }
+      if (nsni) {
+        // the gradients along a of the incremental displacement gradient,
+        // (H_a)_km = sum_J S_(m a)(J) du_J,k (XLMAT/YLMAT/ZLMAT, FINT.F90:728-737)
+        const double* dd = ddshp + 6 * s;
+        double* sg = sgrad + 18 * (size_t)i;
+        M3 H[3];
+        for (int a = 0; a < 3; ++a)
+          for (int k = 0; k < 3; ++k)
+            for (int m = 0; m < 3; ++m) {
+              double v = 0.0;
+              for (int j = 0; j < ln; ++j) v += dd[6 * (size_t)j + kDD[m][a]] * gdinc[3 * (size_t)nb[j] + k];
+              H[a][k][m] = v;
+            }
+        const double* sml = sm_len + 6 * (size_t)i;
+        double fac[3], W[3][3][3];  // W[a] = M_a / V * V J sigma_a INV3(F)^T
+        for (int a = 0; a < 3; ++a) {
+          const double wd = sml[2 * a] + sml[2 * a + 1];
+          fac[a] = wd * wd / 12.0;
+          double de[6];
+          if (p->finite_strain) {
+            M3 La;
+            mm3(H[a], ifm_s, La);
+            d_hughes_winget(L_s, La, de, exact);
+            rotate_tensor(R_s, sg + 6 * a);
+          } else {
+            de[0] = H[a][0][0]; de[1] = H[a][1][1]; de[2] = H[a][2][2];
+            de[3] = H[a][2][1] + H[a][1][2]; de[4] = H[a][2][0] + H[a][0][2]; de[5] = H[a][1][0] + H[a][0][1];
+          }
+          double ds[6];
+          for (int r = 0; r < 6; ++r) {
+            double v = 0.0;
+            for (int c = 0; c < 6; ++c) v += C[r][c] * de[c];
+            ds[r] = v;
+          }
+          for (int k = 0; k < 6; ++k) sg[6 * a + k] += ds[k];
+          for (int k = 0; k < 6; ++k) work_t[tid] += 0.5 * fac[a] * de[k] * (2.0 * sg[6 * a + k] - ds[k]) * vol * det;
+          M3 Sa;
+          v2t(sg + 6 * a, Sa);
+          for (int k = 0; k < 3; ++k)
+            for (int m = 0; m < 3; ++m) {
+              double v = 0.0;
+              for (int q = 0; q < 3; ++q) v += Sa[k][q] * ifm_s[m][q];
+              W[a][k][m] = fac[a] * vol * det * v;
+            }
+        }
+        for (int j = 0; j < ln; ++j) {                                // FINT.F90:1127-1208
+          const double* d = dd + 6 * (size_t)j;
+          double f[3] = {0.0, 0.0, 0.0};
+          for (int a = 0; a < 3; ++a)
+            for (int k = 0; k < 3; ++k)
+              for (int m = 0; m < 3; ++m) f[k] += W[a][k][m] * d[kDD[m][a]];
+          const size_t jj = (size_t)nb[j];
+          FT[3 * jj + 0] += f[0];
+          FT[3 * jj + 1] += f[1];
+          FT[3 * jj + 2] += f[2];
+        }
+        for (int k = 0; k < 18; ++k)
+          if (!std::isfinite(sg[k])) status |= MEGA_ST_NONFINITE;
       }
       for (int k = 0; k < 6; ++k)
         if (!std::isfinite(lstress[k])) status |= MEGA_ST_NONFINITE;
@@ -1028,7 +1318,7 @@ int orc_construct_fint_pd(const mega_params* p, int n, const double* gcoo, const
         spred[r] = lstress[r] + v;
       }
       constitution(spred, gmat[i], lprop, dlt, lstate, lstress, p->newton_max_iter, p->newton_rtol,
-                   &status, nullptr, p->rate_solver);
+                   &status, nullptr, p->rate_solver, lstrain, strain);
       for (int k = 0; k < 20; ++k) gstate[20 * (size_t)i + k] = lstate[k];
       double sinc[6], einc[6];
       for (int k = 0; k < 6; ++k) {                                   // :505-518 (STRAIN_INC uses
@@ -1108,7 +1398,8 @@ int orc_step(const mega_params* p, int n, const double* coo, const double* win, 
              double* stress, double* strain, double* dsp, double* dsp_tot, double* dsp_tot_phy,
              double* vel, double* acl, double* fint, double* fext, double* prforce, double* coo_cur,
              double* wvel, double* strain_eq, double* en, double* total_force, double dlt,
-             int nthreads, int serial_interp, int* newton_iters) {
+             int nthreads, int serial_interp, int* newton_iters, const double* sm_len, double* ddshp,
+             double* sgrad) {
   size_t n3 = 3 * (size_t)n;
   for (size_t m = 0; m < n3; ++m) {                                  // predictor
     dsp[m] = dlt * vel[m] + dlt * dlt * 0.5 * acl[m];
@@ -1124,7 +1415,7 @@ int orc_step(const mega_params* p, int n, const double* coo, const double* win, 
   std::vector<double> fext_nmo(fext, fext + n3);
   int st = orc_construct_fint(p, n, coo, win, vol, props, mat, ebc_nodes, bodyforce, state, stress,
                               strain, dsp, dsp_tot, gn, gstart, gstack, shp, dshp, 0, dlt, fint,
-                              fext, wvel, strain_eq, &en[3], nthreads, newton_iters);
+                              fext, wvel, strain_eq, &en[3], nthreads, newton_iters, sm_len, ddshp, sgrad);
   std::vector<double> p21(n);
   for (int i = 0; i < n; ++i) p21[i] = props[30 * (size_t)i + 20];
   orc_corrector(n, ebc, p21.data(), mass, fint, fext, vel, acl, prforce, body_id, total_force, dlt);

@@ -22,13 +22,14 @@ _SIG = {
     "orc_rotate_tensor": (None, [I32, P, P]),
     "orc_constitution": (I32, [I32, P, P, P, D, P, P, P, I32, D, I32]),
     "orc_vm_rate": (I32, [I32, P, P, D, D, I32, P, P, P, P, P, I32]),
+    "orc_damaged": (I32, [I32, P, P, P, P, P, P, P, I32]),
     "orc_construct_fint": (I32, [P, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, I32, D, P, P, P, P,
-                                 P, I32, P]),
+                                 P, I32, P, P, P, P]),
     "orc_interp": (None, [I32, P, P, P, P, P, P, I32]),
     "orc_pd_shape": (I32, [I32, P, P, P, P, P, P, P, P, I32]),
     "orc_construct_fint_pd": (I32, [P, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, I32, D, P, P, I32]),
     "orc_corrector": (None, [I32, P, P, P, P, P, P, P, P, P, P, D]),
-    "orc_step": (I32, [P, I32] + [P] * 31 + [D, I32, I32, P]),
+    "orc_step": (I32, [P, I32] + [P] * 31 + [D, I32, I32, P, P, P, P]),
     "orc_pmb_force": (I64, [I32, P, P, P, P, P, P, D, D, P, P, I32]),
     "orc_mlp_nparams": (I64, [I32]),
     "orc_mlp_forward_backward": (D, [I32, P, I32, P, P, P, P]),
@@ -155,6 +156,18 @@ def constitution(spred, mat, props, dlt, state, maxit=20, rtol=1e-10, solver=0):
     return stress, state, it, st
 
 
+def damaged(stress_rot, tot, inc, mat, props, state, maxit=20):
+    """DRUCK_PRAG (3) / VON_MISES_DAM (6) from the rotated old stress, the
+    total strain and the strain increment: (stress, state, passes, status)."""
+    stress = f64(stress_rot).copy()
+    n = len(stress)
+    state = f64(state).copy()
+    it = np.zeros(n, np.int32)
+    st = lib().orc_damaged(n, _p(i32(mat)), _p(f64(props)), _p(f64(tot)), _p(f64(inc)), _p(state), _p(stress),
+                           _p(it), int(maxit))
+    return stress, state, it, st
+
+
 def vm_rate(spred, props, dt, state, dg0=None, rtol=1e-10, maxit=50, solver=0):
     spred = f64(spred)
     n = len(spred)
@@ -169,7 +182,10 @@ def vm_rate(spred, props, dt, state, dg0=None, rtol=1e-10, maxit=50, solver=0):
 
 
 def construct_fint(p, case, state, stress, strain, dinc, dinc_tot, nb, shp, dshp, linit, dlt, nthreads=1,
-                   gint_work=0.0):
+                   gint_work=0.0, ddshp=None, sgrad=None):
+    """CONSTRUCT_FINT; with p.itype_int == 2 (NSNI) ddshp (6 per list entry,
+    built when linit) and sgrad (18 per node, the stress gradients) are
+    updated in place too."""
     n = case["n"]
     fint = np.zeros(3 * n)
     fext = np.zeros(3 * n)
@@ -184,7 +200,7 @@ def construct_fint(p, case, state, stress, strain, dinc, dinc_tot, nb, shp, dshp
         _p(i32(case["mat_type"])), _p(en), _p(None if bf is None else f64(bf)), _p(state), _p(stress), _p(strain),
         _p(f64(dinc)), _p(f64(dinc_tot)), _p(i32(nb["gn"])), _p(i32(nb["gstart"])), _p(i32(nb["gstack"])), _p(shp),
         _p(dshp), int(bool(linit)), float(dlt), _p(fint), _p(fext), _p(wv), _p(seq), C.byref(gw), int(nthreads),
-        _p(it))
+        _p(it), _p(f64(case["sm_len"]) if ddshp is not None else None), _p(ddshp), _p(sgrad))
     return dict(fint=fint, fext=fext, gmax_wvel=wv, gstrain_eq=seq, gint_work=gw.value, iters=it, status=st)
 
 
@@ -221,9 +237,12 @@ class Run:
         self.iters = np.zeros(n, np.int32)
         self.time = 0.0
         self.steps = 0
+        # NSNI: smoothed second derivatives (6 per entry), stress gradients (18 per node)
+        self.ddshp = np.zeros(6 * nnz) if p.itype_int == 2 else None
+        self.sgrad = np.zeros((n, 18)) if p.itype_int == 2 else None
         # LINIT: shapes + a force call at zero displacement (MAIN.F90:320-334)
         r = construct_fint(p, case, self.state, self.stress, self.strain, self.dsp, self.dsp_tot, self.nb,
-                           self.shp, self.dshp, True, 0.0, nthreads)
+                           self.shp, self.dshp, True, 0.0, nthreads, ddshp=self.ddshp, sgrad=self.sgrad)
         self.init_status = r["status"]
         self.en[3] = r["gint_work"]
 
@@ -240,7 +259,8 @@ class Run:
                 _p(self.nb["gstack"]), _p(self.shp), _p(self.dshp), _p(self.state), _p(self.stress), _p(self.strain),
                 _p(self.dsp), _p(self.dsp_tot), _p(self.dsp_tot_phy), _p(self.vel), _p(self.acl), _p(self.fint),
                 _p(self.fext), _p(self.prforce), _p(self.coo_cur), _p(self.wvel), _p(self.strain_eq), _p(self.en),
-                _p(self.total_force), float(dt), int(self.nthreads), int(bool(self.serial_interp)), _p(self.iters))
+                _p(self.total_force), float(dt), int(self.nthreads), int(bool(self.serial_interp)), _p(self.iters),
+                _p(f64(c["sm_len"]) if self.ddshp is not None else None), _p(self.ddshp), _p(self.sgrad))
             self.time += dt
             self.steps += 1
         return st

@@ -30,6 +30,21 @@ def props_vector(mat_type, E, nu, rho, p4=0.0, p5=0.0, p6=0.0, p7=0.0, p8=0.0, d
     return p
 
 
+def with_damage(case, mat_type, k_i, k_c, dam_max, q_phi=0.0, k_phi=0.0, q_psi=0.0):
+    """The case with a damaged model on every node: material 6 (J2 with the
+    case's hardening, isotropic damage) or 3 (Drucker-Prager shear yield
+    with damage).  PROPS(9..11) = K_I, K_C, DAM_MAX (thresholds on the
+    total-strain norm), PROPS(25..27) = Q_PHI, K_PHI, Q_PSI."""
+    c = dict(case)
+    pr = np.array(case["props"], copy=True)
+    pr[:, 8], pr[:, 9], pr[:, 10] = k_i, k_c, dam_max
+    pr[:, 24], pr[:, 25], pr[:, 26] = q_phi, k_phi, q_psi
+    c["props"] = pr
+    c["mat_type"] = np.full(case["n"], mat_type, np.int32)
+    c["name"] = f"{case.get('name', 'case')}_mat{mat_type}"
+    return c
+
+
 def smoothing_lengths(vol, win_raw):
     """GET_SMOOTHING_LENGTHS (PRE_MODEL_SMOOTHING_LENGTHS.F90:49-99) with the
     raw windows: SM_LEN(6,N) and (XDIST_MAX, YDIST_MAX, ZDIST_MAX)."""

@@ -181,6 +181,7 @@ struct Ctx {
   double *eps = nullptr, *strain_eq = nullptr, *wvel = nullptr, *fg = nullptr, *scratch3 = nullptr;
   void* tmat = nullptr;
   int32_t* iters = nullptr;
+  double* aux = nullptr;  // 4 per node, STATE(1, 2, 4, 5), when a damaged model is present
   StepAccum* acc = nullptr;
   unsigned* status = nullptr;
   bool phy_valid = true;
@@ -273,7 +274,7 @@ static StressArgs stress_args(Ctx* c, double dt, int mode) {
   a.grav[0] = c->p.gravity[0]; a.grav[1] = c->p.gravity[1]; a.grav[2] = c->p.gravity[2];
   a.has_body = c->has_body; a.inv3_exact = c->p.inv3_exact; a.finite_strain = c->p.finite_strain;
   a.maxit = c->p.newton_max_iter; a.rate_solver = c->p.rate_solver; a.rtol = c->p.newton_rtol; a.dt = dt; a.iters = c->iters;
-  a.acc = c->acc; a.status = c->status;
+  a.aux = c->aux; a.acc = c->acc; a.status = c->status;
   if ((mode & MEGA_FLAG_LEARNED_GUESS) && c->mlp_on) { a.mlp_w2 = c->mlp_w2; a.mlp_small = c->mlp_small; }
   if (c->log_cap > 0) {
     a.log_buf = c->log_buf; a.log_count = c->log_count; a.log_cap = c->log_cap;
@@ -369,6 +370,7 @@ static int build_materials(Ctx* c, const double* props, const int32_t* mat_type)
   std::map<std::vector<double>, uint16_t> tab;
   std::vector<uint16_t> idx(c->n);
   std::vector<MatEntry> ents;
+  bool damaged = false;
   int64_t prev = -1;
   for (int32_t i = 0; i < c->n; ++i) {
     // fast path: same PROPS row and type as the previous node
@@ -384,11 +386,8 @@ static int build_materials(Ctx* c, const double* props, const int32_t* mat_type)
     auto it = tab.find(key);
     if (it == tab.end()) {
       if (ents.size() >= 65535) return MEGA_ERR_UNSUPPORTED;
-      MatEntry e{};
-      const double* pr = props + 30 * (size_t)i;
-      e.type = mat_type[i];
-      e.nu = pr[0]; e.E = pr[1]; e.rho = pr[2]; e.sig0 = pr[3]; e.B = pr[4]; e.C = pr[5];
-      e.p7 = pr[6]; e.p8 = pr[7]; e.damp = pr[20]; e.lam = pr[27]; e.mu = pr[28]; e.l2m = pr[29];
+      const MatEntry e = mat_entry(mat_type[i], props + 30 * (size_t)i);
+      damaged = damaged || damaged_type(e.type);
       uint16_t id = (uint16_t)ents.size();
       ents.push_back(e);
       it = tab.emplace(key, id).first;
@@ -397,6 +396,10 @@ static int build_materials(Ctx* c, const double* props, const int32_t* mat_type)
   }
   MEGA_ALLOC(c->pool, c->matidx, c->n);
   MEGA_ALLOC(c->pool, c->mats, ents.size());
+  if (damaged) {  // STATE(1, 2, 4, 5) start at zero (STATE_INIT.f90)
+    MEGA_ALLOC(c->pool, c->aux, 4 * (int64_t)c->n);
+    MEGA_TRY(cudaMemsetAsync(c->aux, 0, sizeof(double) * 4 * c->n, c->s));
+  }
   MEGA_TRY(cudaMemcpyAsync(c->matidx, idx.data(), sizeof(uint16_t) * c->n, cudaMemcpyHostToDevice, c->s));
   MEGA_TRY(cudaMemcpyAsync(c->mats, ents.data(), sizeof(MatEntry) * ents.size(), cudaMemcpyHostToDevice, c->s));
   MEGA_TRY(cudaStreamSynchronize(c->s));
@@ -687,7 +690,7 @@ static int permute_nodes(Ctx* c, const int32_t* map) {
       {c->vel, 3, 8}, {c->acl, 3, 8}, {c->fint, 3, 8}, {c->fext, 3, 8}, {c->prforce, 3, 8}, {c->bodyforce, 3, 8},
       {c->sm_len, 6, 8}, {c->stress, 6, 8}, {c->strain, 6, 8}, {c->vol, 1, 8}, {c->eps, 1, 8},
       {c->strain_eq, 1, 8}, {c->wvel, 1, 8}, {c->ebc, 3, 1}, {c->body_id, 1, 1}, {c->ebc_nodes, 1, 4},
-      {c->iters, 1, 4}, {c->matidx, 1, 2}};
+      {c->iters, 1, 4}, {c->matidx, 1, 2}, {c->aux, 4, 8}};
   for (const Arr& a : list) {
     if (!a.p) continue;
     k_perm_gather<<<grid_for((int64_t)n * a.w, 256), 256, 0, c->s>>>(n, a.w, a.es, map, (const unsigned char*)a.p,
@@ -959,6 +962,9 @@ int mega_download(int64_t h, int32_t field, double* dst) {
     case MEGA_F_STRAIN_EQ: src = c->strain_eq; w = 1; break;
     case MEGA_F_WAVE_VEL: src = c->wvel; w = 1; break;
     case MEGA_F_PRFORCE: src = c->prforce; w = 3; break;
+    case MEGA_F_STATE_AUX:
+      if (!c->aux) return MEGA_ERR_STATE;
+      src = c->aux; w = 4; break;
     case MEGA_F_NEWTON_IT: {
       std::vector<int32_t> it(n);
       int r = download_nodes(c, c->iters, 1, 4, it.data());
@@ -1006,6 +1012,9 @@ int mega_upload(int64_t h, int32_t field, const double* src) {
     case MEGA_F_STRESS: dst = c->stress; w = 6; break;
     case MEGA_F_STRAIN: dst = c->strain; w = 6; break;
     case MEGA_F_EPS: dst = c->eps; w = 1; break;
+    case MEGA_F_STATE_AUX:
+      if (!c->aux) return MEGA_ERR_STATE;
+      dst = c->aux; w = 4; break;
     default: return MEGA_ERR_ARG;
   }
   const size_t bytes = (size_t)n * w * sizeof(double);
@@ -1076,6 +1085,7 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
       {c->fint, 8 * n3}, {c->fext, 8 * n3}, {c->prforce, 8 * n3}, {c->stress, 48 * n}, {c->strain, 48 * n},
       {c->eps, 8 * n}, {c->strain_eq, 8 * n}, {c->wvel, 8 * n}, {c->fg, 144 * n}, {c->tmat, 12 * ts * n},
       {c->iters, 4 * n}, {c->acc, sizeof(StepAccum)}, {c->status, sizeof(unsigned)}};
+  if (c->aux) arrs.push_back({c->aux, 32 * n});
   DevPool snap(c->s);
   std::vector<unsigned char*> copies;
   for (const Arr& a : arrs) {
@@ -1477,16 +1487,15 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   std::map<std::vector<double>, uint16_t> tab;
   std::vector<uint16_t> hidx(n);
   std::vector<MatEntry> ents;
+  bool damaged = false;
   for (int32_t i = 0; i < n; ++i) {
     std::vector<double> key(gprop + 30 * (size_t)i, gprop + 30 * (size_t)i + 30);
     key.push_back(gmat_type[i]);
     auto it = tab.find(key);
     if (it == tab.end()) {
       if (ents.size() >= 65535) return MEGA_ERR_UNSUPPORTED;
-      const double* pr = gprop + 30 * (size_t)i;
-      MatEntry e{};
-      e.type = gmat_type[i]; e.nu = pr[0]; e.E = pr[1]; e.rho = pr[2]; e.sig0 = pr[3]; e.B = pr[4]; e.C = pr[5];
-      e.p7 = pr[6]; e.p8 = pr[7]; e.damp = pr[20]; e.lam = pr[27]; e.mu = pr[28]; e.l2m = pr[29];
+      const MatEntry e = mat_entry(gmat_type[i], gprop + 30 * (size_t)i);
+      damaged = damaged || damaged_type(e.type);
       it = tab.emplace(key, (uint16_t)ents.size()).first;
       ents.push_back(e);
     }
@@ -1494,8 +1503,19 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   }
   MatEntry* dmat;
   MEGA_ALLOC(pool, dmat, ents.size());
-  std::vector<double> hs(n), hsig(6 * (size_t)n), heps(6 * (size_t)n);
+  std::vector<double> hs(n), hsig(6 * (size_t)n), heps(6 * (size_t)n), hax;
   for (int32_t i = 0; i < n; ++i) hs[i] = gstate[20 * (size_t)i + 2];
+  double* dax = nullptr;  // GSTATE(1, 2, 4, 5) when a damaged model is present
+  if (damaged) {
+    MEGA_ALLOC(pool, dax, 4 * (int64_t)n);
+    hax.resize(4 * (size_t)n);
+    for (int32_t i = 0; i < n; ++i) {
+      const double* g = gstate + 20 * (size_t)i;
+      hax[4 * (size_t)i] = g[0]; hax[4 * (size_t)i + 1] = g[1]; hax[4 * (size_t)i + 2] = g[3];
+      hax[4 * (size_t)i + 3] = g[4];
+    }
+    if ((r = upload(s, dax, hax.data(), hax.size()))) return r;
+  }
   if ((r = upload(s, dc, gcoo, n3)) || (r = upload(s, dw, gwin, n3)) || (r = upload(s, dv, gvol, (size_t)n)) ||
       (r = upload(s, ddsp, gdinc, n3)) || (r = upload(s, dtot, gdinc_tot, n3)) ||
       (r = upload(s, dsig, gstress, 6 * (size_t)n)) || (r = upload(s, deps6, gstrain, 6 * (size_t)n)) ||
@@ -1530,7 +1550,7 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   if (r) return r;
   StressArgs a{};
   a.n = n; a.fg = dfg; a.matidx = midx; a.mats = dmat; a.vol = dv; a.stress = dsig; a.strain = deps6; a.eps = dep;
-  a.strain_eq = deq; a.wvel = dwv; a.tmat = dT; a.bodyforce = dbf;
+  a.strain_eq = deq; a.wvel = dwv; a.tmat = dT; a.bodyforce = dbf; a.aux = dax;
   a.grav[0] = p->gravity[0]; a.grav[1] = p->gravity[1]; a.grav[2] = p->gravity[2];
   a.has_body = has_body; a.inv3_exact = p->inv3_exact; a.finite_strain = p->finite_strain;
   a.maxit = p->newton_max_iter; a.rate_solver = p->rate_solver; a.rtol = p->newton_rtol; a.dt = dlt; a.acc = acc; a.status = st;
@@ -1551,6 +1571,7 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   MEGA_TRY(cudaMemcpyAsync(gstress, dsig, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(gstrain, deps6, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(hs.data(), dep, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  if (damaged) MEGA_TRY(cudaMemcpyAsync(hax.data(), dax, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(gmax_wvel, dwv, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(gstrain_eq, deq, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(&hacc, acc, sizeof(hacc), cudaMemcpyDeviceToHost, s));
@@ -1570,6 +1591,12 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   }
   MEGA_TRY(cudaStreamSynchronize(s));
   for (int32_t i = 0; i < n; ++i) gstate[20 * (size_t)i + 2] = hs[i];
+  if (damaged)
+    for (int32_t i = 0; i < n; ++i) {
+      double* g = gstate + 20 * (size_t)i;
+      g[0] = hax[4 * (size_t)i]; g[1] = hax[4 * (size_t)i + 1]; g[3] = hax[4 * (size_t)i + 2];
+      g[4] = hax[4 * (size_t)i + 3];
+    }
   *gint_work += slot_sum(hacc.int_work);
   return (int)hst;
 }

@@ -147,7 +147,9 @@ struct Trial {
 
 // FINT.F90:363-794: |det F|, INV3(F), L = G0 INV3(F), Hughes-Winget, rotation
 // of sigma and eps, eps += dstrain, elastic predictor.
-template <typename T, bool LEAN>
+// DAM: the context holds damaged models (materials 3, 6) and their state;
+// without it their branches compile out of the J2 path.
+template <typename T, bool LEAN, bool DAM>
 __device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Trial<T, LEAN>& w) {
   // F, G0 (18 doubles), stress and strain (6 each) as 16-byte loads
   double fgi[18], sv[6], ev[6];
@@ -210,6 +212,13 @@ __device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Tri
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k) w.eps6[k] = w.eps6[k] + dstr[k];
+  // the damaged models predict in effective space: STRESS / (1 - DAM)
+  // (CONSTITUTE_VONMISES_DAM.F90:83, CONSTITUTE_DRUCKPRAG.F90:79)
+  if (DAM && damaged_type(me.type)) {
+    const T keep = T(1) - (T)a.aux[4 * i + 2];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sig[k] = sig[k] / keep;
+  }
   // elastic predictor with FORM_CMAT (FINT_FUNCTIONS.F90:252-288)
   const T lam = (T)me.lam, mu = (T)me.mu, l2m = (T)me.l2m;
   w.spred[0] = (double)(sig[0] + (l2m * dstr[0] + lam * dstr[1] + lam * dstr[2]));
@@ -250,7 +259,7 @@ __device__ __forceinline__ double rate_features(const double spred[6], double ep
 
 // FINT.F90:797-870, 999-1116: return mapping (dg0 >= 0 starts the rate law's
 // Newton there), state write-back, strain_eq, internal work, wave speed, T_i.
-template <typename T, typename TS, bool LEAN>
+template <typename T, typename TS, bool LEAN, bool DAM>
 __device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Trial<T, LEAN>& w, double dg0, double& work,
                                               unsigned long long& nit, unsigned long long& npl, unsigned& st) {
   const MatEntry& me = LEAN ? a.mats[w.mi] : w.me;
@@ -286,6 +295,21 @@ __device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Tr
         }
       }
     }
+  } else if (DAM && damaged_type(m.type)) {
+    // CONSTITUTION.F90:60-64, 72-76: the total strain (already advanced by
+    // dstrain) and the four damage-state values ride along; spred is the
+    // effective predictor
+    double tot[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) tot[k] = (double)w.eps6[k];
+    double2* a2 = reinterpret_cast<double2*>(a.aux + 4 * i);
+    const double2 x0 = a2[0], x1 = a2[1];
+    double ax[4] = {x0.x, x0.y, x1.x, x1.y};
+    const DamageMat d{me.ki, me.kc, me.dmax, me.qphi, me.kphi, me.qpsi};
+    if (m.type == MEGA_MAT_VM_DAMAGE) it = von_mises_dam(w.spred, tot, ep, ax, m, d, a.maxit, snew, cap);
+    else it = drucker_prager(w.spred, tot, ep, ax, m, d, snew);
+    a2[0] = make_double2(ax[0], ax[1]);
+    a2[1] = make_double2(ax[2], ax[3]);
   } else {
     st |= MEGA_ST_BAD_MATERIAL;
 #pragma unroll
@@ -381,7 +405,7 @@ __device__ __forceinline__ void stress_reduce(const StressArgs& a, double work, 
 }
 
 // T = arithmetic of kinematics / rotation / predictor, TS = storage of T_i
-template <typename T, typename TS>
+template <typename T, typename TS, bool DAM>
 __global__ void __launch_bounds__(256, 2) k_stress(StressArgs a) {
   __shared__ double smd[32];
   __shared__ unsigned long long smu[32];
@@ -393,8 +417,8 @@ __global__ void __launch_bounds__(256, 2) k_stress(StressArgs a) {
   unsigned st = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
     Trial<T, false> w;
-    stress_trial(a, i, w);
-    stress_finish<T, TS, false>(a, i, w, -1.0, work, nit, npl, st);
+    stress_trial<T, false, DAM>(a, i, w);
+    stress_finish<T, TS, false, DAM>(a, i, w, -1.0, work, nit, npl, st);
   }
   stress_reduce<T>(a, work, nit, npl, st, smd, smu);
 }
@@ -406,7 +430,7 @@ __global__ void __launch_bounds__(256, 2) k_stress(StressArgs a) {
 // warp-uniform.
 constexpr int kLearnBlock = 128;
 
-template <typename T, typename TS>
+template <typename T, typename TS, bool DAM>
 __global__ void __launch_bounds__(kLearnBlock, 4) k_stress_learned(StressArgs a) {
   __shared__ double smd[32];
   __shared__ unsigned long long smu[32];
@@ -431,7 +455,7 @@ __global__ void __launch_bounds__(kLearnBlock, 4) k_stress_learned(StressArgs a)
     float x[4] = {0.f, 0.f, 0.f, 0.f};
     double ub = 0.0, f = -1.0;
     if (act) {
-      stress_trial(a, i, w);
+      stress_trial<T, true, DAM>(a, i, w);
       const MatEntry& me = a.mats[w.mi];
       if (me.type == MEGA_MAT_VM_RATE) f = rate_features(w.spred, a.eps[i], me, a.dt, x, ub);
     }
@@ -439,7 +463,7 @@ __global__ void __launch_bounds__(kLearnBlock, 4) k_stress_learned(StressArgs a)
     const float y = __any_sync(0xffffffffu, f > 0.0) ? warp_mlp(x, f > 0.0, net, hw, ow) : 0.f;
     if (act) {
       const double dg0 = f > 0.0 ? (double)fminf(fmaxf(y, 1e-3f), 1.0f) * ub : -1.0;
-      stress_finish<T, TS, true>(a, i, w, dg0, work, nit, npl, st);
+      stress_finish<T, TS, true, DAM>(a, i, w, dg0, work, nit, npl, st);
     }
   }
   stress_reduce<T>(a, work, nit, npl, st, smd, smu);
@@ -634,12 +658,22 @@ int launch_stress(cudaStream_t s, bool mixed, const StressArgs& a) {
   if (a.mlp_w2 && a.mlp_small) {  // learned start of the rate-dependent return mapping
     const int64_t lneed = grid_for(a.n, kLearnBlock);
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(lneed, (int64_t)device_sm_count() * 8));
-    if (mixed) k_stress_learned<float, float><<<grid, kLearnBlock, 0, s>>>(a);
-    else k_stress_learned<double, double><<<grid, kLearnBlock, 0, s>>>(a);
+    if (a.aux) {
+      if (mixed) k_stress_learned<float, float, true><<<grid, kLearnBlock, 0, s>>>(a);
+      else k_stress_learned<double, double, true><<<grid, kLearnBlock, 0, s>>>(a);
+    } else {
+      if (mixed) k_stress_learned<float, float, false><<<grid, kLearnBlock, 0, s>>>(a);
+      else k_stress_learned<double, double, false><<<grid, kLearnBlock, 0, s>>>(a);
+    }
   } else {
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)device_sm_count() * 8));
-    if (mixed) k_stress<float, float><<<grid, block, 0, s>>>(a);
-    else k_stress<double, double><<<grid, block, 0, s>>>(a);
+    if (a.aux) {
+      if (mixed) k_stress<float, float, true><<<grid, block, 0, s>>>(a);
+      else k_stress<double, double, true><<<grid, block, 0, s>>>(a);
+    } else {
+      if (mixed) k_stress<float, float, false><<<grid, block, 0, s>>>(a);
+      else k_stress<double, double, false><<<grid, block, 0, s>>>(a);
+    }
   }
   MEGA_CHECK_LAUNCH();
   return 0;

@@ -211,6 +211,83 @@ __device__ __forceinline__ int von_mises(const double spred[6], double& eps, con
   return it;
 }
 
+// The damaged models keep four more state values per node,
+// aux = {EPS_SHEAR, EPS_VOL, DAM, DAM_SV} = STATE(1, 2, 4, 5), and read
+// PROPS(9..11) and PROPS(25..27).
+struct DamageMat {
+  double ki, kc, dmax;      // K_I, K_C, DAM_MAX
+  double qphi, kphi, qpsi;  // Q_PHI, K_PHI, Q_PSI (Drucker-Prager)
+};
+
+// Damage of CONSTITUTE_VONMISES_DAM.F90:94-125 / CONSTITUTE_DRUCKPRAG.F90:
+// 84-113: eta = TENSOR_NORM(total strain) (the stress-norm weighting, as
+// written); once eta passes DAM_SV + K_I and while K_I < eta < K_C the
+// damage is K_C (eta - K_I) / (eta (K_C - K_I)) and DAM_SV = eta - K_I;
+// capped at DAM_MAX.
+__device__ __forceinline__ void damage_update(const double tot[6], const DamageMat& d, double& dam, double& dsv) {
+  const double eta = tensor_norm(tot);
+  if (eta < dsv + d.ki) {
+  } else if (eta > d.ki && eta < d.kc) {
+    dam = d.kc * (eta - d.ki) / (eta * (d.kc - d.ki));
+    dsv = eta - d.ki;
+  }
+  if (dam > d.dmax) dam = d.dmax;
+}
+
+// VON_MISES_DAM (CONSTITUTE_VONMISES_DAM.F90:21-196).  eff = the effective
+// predictor STRESS / (1 - DAM) + C dstrain (formed by the caller from the
+// rotated old stress); the radial return of VON_MISES in effective space
+// (the same Newton iteration and tolerance), then back to the real stress
+// with the new damage.
+__device__ __forceinline__ int von_mises_dam(const double eff[6], const double tot[6], double& eps, double aux[4],
+                                             const NodeMat& m, const DamageMat& d, int maxit, double stress[6],
+                                             bool& cap) {
+  damage_update(tot, d, aux[2], aux[3]);
+  const int it = von_mises(eff, eps, m, maxit, stress, cap);
+  const double keep = 1.0 - aux[2];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) stress[k] = stress[k] * keep;
+  return it;
+}
+
+// DRUCK_PRAG (CONSTITUTE_DRUCKPRAG.F90:17-241): shear yield
+// f = |dev| + Q_PHI p - K_PHI (p = tr/3 of the effective predictor), a
+// closed-form return with non-associated dilatancy Q_PSI, then the real
+// stress with the new damage.  The tension cut-off branch is unreachable as
+// written (its flag is never set) and is not restated.  Returns 1 on a
+// plastic return.
+__device__ __forceinline__ int drucker_prager(const double eff[6], const double tot[6], double& eps, double aux[4],
+                                              const NodeMat& m, const DamageMat& d, double stress[6]) {
+  damage_update(tot, d, aux[2], aux[3]);
+  const double kk = eff[0] + eff[1] + eff[2];
+  double dev[6];
+  dev[0] = eff[0] - kk / 3.0; dev[1] = eff[1] - kk / 3.0; dev[2] = eff[2] - kk / 3.0;
+  dev[3] = eff[3]; dev[4] = eff[4]; dev[5] = eff[5];
+  const double tau_pre = tensor_norm(dev);
+  const double sph_pre = kk / 3.0;
+  const double f = tau_pre + d.qphi * sph_pre - d.kphi;
+  int plastic = 0;
+  if (f < 0.0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) stress[k] = eff[k];
+  } else {
+    const double tau = d.kphi - d.qphi * sph_pre;
+    const double bulk = m.E / (3.0 * (1.0 - 2.0 * m.nu)), shear = m.E / (2.0 * (1.0 + m.nu));
+    const double gamma = f / (2.0 * shear + bulk * d.qphi * d.qpsi);
+    const double sph = sph_pre - bulk * d.qpsi * gamma;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) stress[k] = dev[k] * tau / tau_pre;
+    stress[0] += sph; stress[1] += sph; stress[2] += sph;
+    aux[0] = aux[0] + gamma * sqrt(2.0 / 3.0 + 2.0 / 9.0 * d.qpsi * d.qpsi);
+    eps = eps + aux[0];  // EPS accumulates the running EPS_SHEAR, as written
+    plastic = 1;
+  }
+  const double keep = 1.0 - aux[2];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) stress[k] = stress[k] * keep;
+  return plastic;
+}
+
 // Power-law rate-dependent J2 return mapping (no reference counterpart):
 // sigma_y = A + B*ep^n*(1 + C*ln(max(epdot,epdot0)/epdot0)), epdot =
 // sqrt(2/3)*dg/dt.  Safeguarded Newton on dg in [0, q/(2mu)], converged at

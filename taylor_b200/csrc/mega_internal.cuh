@@ -148,7 +148,19 @@ struct MatEntry {
   int32_t type;
   int32_t pad;
   double nu, E, rho, sig0, B, C, p7, p8, lam, mu, l2m, damp;
+  double ki, kc, dmax;      // PROPS(9..11): damage thresholds K_I, K_C and DAM_MAX
+  double qphi, kphi, qpsi;  // PROPS(25..27): Drucker-Prager Q_PHI, K_PHI, Q_PSI
 };
+inline MatEntry mat_entry(int32_t type, const double* pr) {
+  MatEntry e{};
+  e.type = type;
+  e.nu = pr[0]; e.E = pr[1]; e.rho = pr[2]; e.sig0 = pr[3]; e.B = pr[4]; e.C = pr[5];
+  e.p7 = pr[6]; e.p8 = pr[7]; e.damp = pr[20]; e.lam = pr[27]; e.mu = pr[28]; e.l2m = pr[29];
+  e.ki = pr[8]; e.kc = pr[9]; e.dmax = pr[10]; e.qphi = pr[24]; e.kphi = pr[25]; e.qpsi = pr[26];
+  return e;
+}
+// the models that carry STATE(1, 2, 4, 5) besides the plastic strain
+__host__ __device__ inline bool damaged_type(int32_t t) { return t == MEGA_MAT_DRUCKER_PRAGER || t == MEGA_MAT_VM_DAMAGE; }
 
 // Reductions the step kernels accumulate on the device.  Each quantity has
 // kSlots partial sums (a block adds into slot blockIdx % kSlots) so that
@@ -198,6 +210,7 @@ struct StressArgs {
   double rtol;
   double dt;
   int32_t* iters;            // per-node Newton passes (or null)
+  double* aux;               // 4 per node: STATE(1, 2, 4, 5) of the damaged models (or null)
   const uint16_t* mlp_w2;    // surrogate network: W2 (64x64) as bf16 bits, or null
   const float* mlp_small;    // W1 (64x4), b1, b2, W3, b3 as fp32, or null
   float* log_buf;            // sample log: 5 floats (4 features, target) per sample, or null

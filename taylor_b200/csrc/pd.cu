@@ -19,6 +19,7 @@
 //    evaluated from both ends with bitwise-identical arithmetic, so both
 //    copies break in the same step.  Float force arithmetic, double
 //    positions and velocity-Verlet integration.
+#include <cstring>
 #include <mutex>
 #include <set>
 #include "mega_internal.cuh"
@@ -136,6 +137,7 @@ struct PdStressArgs {
   double* eps;
   double* wvel;
   double* amat;  // 9 per node, row-major A_i = P_i K_i^-1
+  double* aux;   // 4 per node: STATE(1, 2, 4, 5) of the damaged models (or null)
   int linit;
   int inv3_exact;
   int maxit;
@@ -179,6 +181,10 @@ __global__ void k_pd_stress(PdStressArgs a) {
   NodeMat m;
   m.type = me.type; m.nu = me.nu; m.E = me.E; m.rho = me.rho; m.sig0 = me.sig0; m.B = me.B; m.C = me.C;
   m.lam = me.lam; m.mu = me.mu; m.l2m = me.l2m; m.p7 = me.p7; m.p8 = me.p8;
+  if (damaged_type(me.type)) {  // effective-space predictor of the damaged models
+    const double keep = 1.0 - a.aux[4 * i + 2];
+    for (int k = 0; k < 6; ++k) sig[k] = sig[k] / keep;
+  }
   double sp[6];
   sp[0] = sig[0] + (me.l2m * dstr[0] + me.lam * dstr[1] + me.lam * dstr[2]);
   sp[1] = sig[1] + (me.lam * dstr[0] + me.l2m * dstr[1] + me.lam * dstr[2]);
@@ -196,6 +202,11 @@ __global__ void k_pd_stress(PdStressArgs a) {
   } else if (m.type == MEGA_MAT_VM_RATE) {
     double dg, ftr;
     vm_rate(sp, ep, m, a.dt, a.rtol, a.maxit, a.rate_solver, -1.0, sn, cap, dg, ftr);
+  } else if (damaged_type(m.type)) {
+    double* ax = a.aux + 4 * i;
+    const DamageMat d{me.ki, me.kc, me.dmax, me.qphi, me.kphi, me.qpsi};
+    if (m.type == MEGA_MAT_VM_DAMAGE) von_mises_dam(sp, e6, ep, ax, m, d, a.maxit, sn, cap);
+    else drucker_prager(sp, e6, ep, ax, m, d, sn);
   } else {
     st |= MEGA_ST_BAD_MATERIAL;
     for (int k = 0; k < 6; ++k) sn[k] = sp[k];
@@ -531,13 +542,13 @@ int pd_svec(cudaStream_t s, int32_t n, const double* X, const double* vol, const
 }
 int pd_step(cudaStream_t s, int32_t n, const double* X, const double* xc, const double* du, const double* vol,
             const DevCSR& csr, const double* shp, const double* ginvk, const double* svec, const uint16_t* matidx,
-            const MatEntry* mats, double* stress, double* strain, double* eps, double* wvel, double* fg,
+            const MatEntry* mats, double* stress, double* strain, double* eps, double* aux, double* wvel, double* fg,
             double* amat, double* fint, int linit, const mega_params& p, double dt, unsigned* status) {
   k_pd_defgrad<<<gridg(n), 256, 0, s>>>(n, X, xc, du, vol, csr.rowptr, csr.col, shp, fg);
   MEGA_CHECK_LAUNCH();
   PdStressArgs a{};
   a.n = n; a.fg = fg; a.ginvk = ginvk; a.matidx = matidx; a.mats = mats; a.stress = stress; a.strain = strain;
-  a.eps = eps; a.wvel = wvel; a.amat = amat; a.linit = linit; a.inv3_exact = p.inv3_exact;
+  a.eps = eps; a.aux = aux; a.wvel = wvel; a.amat = amat; a.linit = linit; a.inv3_exact = p.inv3_exact;
   a.maxit = p.newton_max_iter; a.rate_solver = p.rate_solver; a.rtol = p.newton_rtol; a.dt = dt; a.status = status;
   k_pd_stress<<<(n + 127) / 128, 128, 0, s>>>(a);
   MEGA_CHECK_LAUNCH();
@@ -646,30 +657,37 @@ int mega_construct_fint_pd(const mega_params* p, int32_t n, const double* gcoo, 
   MEGA_ALLOC(pool, am, 9 * (int64_t)n); MEGA_ALLOC(pool, fi, n3); MEGA_ALLOC(pool, midx, n); MEGA_ALLOC(pool, st, 1);
   // material table
   std::vector<MatEntry> ents;
+  std::vector<const double*> rows;  // the PROPS row each entry was made from
   std::vector<uint16_t> idx(n);
+  bool damaged = false;
   for (int32_t i = 0; i < n; ++i) {
     const double* pr = gprop + 30 * (size_t)i;
     int found = -1;
-    for (size_t e = 0; e < ents.size() && found < 0; ++e) {
-      const MatEntry& q = ents[e];
-      if (q.type == gmat_type[i] && q.nu == pr[0] && q.E == pr[1] && q.rho == pr[2] && q.sig0 == pr[3] &&
-          q.B == pr[4] && q.C == pr[5] && q.p7 == pr[6] && q.p8 == pr[7] && q.lam == pr[27] && q.mu == pr[28] &&
-          q.l2m == pr[29])
-        found = (int)e;
-    }
+    for (size_t e = 0; e < ents.size() && found < 0; ++e)
+      if (ents[e].type == gmat_type[i] && std::memcmp(rows[e], pr, 30 * sizeof(double)) == 0) found = (int)e;
     if (found < 0) {
       if (ents.size() >= 1024) return MEGA_ERR_UNSUPPORTED;
-      MatEntry q{};
-      q.type = gmat_type[i]; q.nu = pr[0]; q.E = pr[1]; q.rho = pr[2]; q.sig0 = pr[3]; q.B = pr[4]; q.C = pr[5];
-      q.p7 = pr[6]; q.p8 = pr[7]; q.damp = pr[20]; q.lam = pr[27]; q.mu = pr[28]; q.l2m = pr[29];
       found = (int)ents.size();
-      ents.push_back(q);
+      ents.push_back(mat_entry(gmat_type[i], pr));
+      rows.push_back(pr);
+      damaged = damaged || damaged_type(gmat_type[i]);
     }
     idx[i] = (uint16_t)found;
   }
   MEGA_ALLOC(pool, dm, ents.size());
-  std::vector<double> hep(n);
+  std::vector<double> hep(n), hax;
   for (int32_t i = 0; i < n; ++i) hep[i] = gstate[20 * (size_t)i + 2];
+  double* aux = nullptr;  // GSTATE(1, 2, 4, 5) when a damaged model is present
+  if (damaged) {
+    MEGA_ALLOC(pool, aux, 4 * (int64_t)n);
+    hax.resize(4 * (size_t)n);
+    for (int32_t i = 0; i < n; ++i) {
+      const double* g = gstate + 20 * (size_t)i;
+      hax[4 * (size_t)i] = g[0]; hax[4 * (size_t)i + 1] = g[1]; hax[4 * (size_t)i + 2] = g[3];
+      hax[4 * (size_t)i + 3] = g[4];
+    }
+    MEGA_TRY(cudaMemcpyAsync(aux, hax.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
+  }
   MEGA_TRY(cudaMemcpyAsync(X, gcoo, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
   MEGA_TRY(cudaMemcpyAsync(xc, gcoo_current, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
   MEGA_TRY(cudaMemcpyAsync(w, gwin, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
@@ -693,13 +711,15 @@ int mega_construct_fint_pd(const mega_params* p, int32_t n, const double* gcoo, 
     r = pd_svec(s, n, X, v, csr, shp, sv);
     if (r) return r;
   }
-  r = pd_step(s, n, X, xc, du, v, csr, shp, ik, sv, midx, dm, sig, eps6, ep, wv, fg, am, fi, linit, *p, dlt, st);
+  r = pd_step(s, n, X, xc, du, v, csr, shp, ik, sv, midx, dm, sig, eps6, ep, aux, wv, fg, am, fi, linit, *p, dlt,
+              st);
   if (r) return r;
   unsigned hst = 0;
   MEGA_TRY(cudaMemcpyAsync(fint, fi, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(gstress, sig, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(gstrain, eps6, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(hep.data(), ep, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  if (damaged) MEGA_TRY(cudaMemcpyAsync(hax.data(), aux, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(gmax_wvel, wv, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(&hst, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   std::vector<double> hs(m);
@@ -711,6 +731,12 @@ int mega_construct_fint_pd(const mega_params* p, int32_t n, const double* gcoo, 
   if (linit)
     for (int64_t k = 0; k < m; ++k) gstack_shp[hpos[k]] = hs[k];
   for (int32_t i = 0; i < n; ++i) gstate[20 * (size_t)i + 2] = hep[i];
+  if (damaged)
+    for (int32_t i = 0; i < n; ++i) {
+      double* g = gstate + 20 * (size_t)i;
+      g[0] = hax[4 * (size_t)i]; g[1] = hax[4 * (size_t)i + 1]; g[3] = hax[4 * (size_t)i + 2];
+      g[4] = hax[4 * (size_t)i + 3];
+    }
   return (int)hst;
 }
 
