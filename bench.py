@@ -20,6 +20,8 @@ Further sections of the same line (each skippable by its flag):
   learned       the 2M-node rate-dependent bar: FP64, mixed, mixed with the
                 textbook Newton start, mixed with the learned start
   peridynamics  the 2.56M-particle bond-based plate (--pmb-nx)
+  nsni          the same bar with stabilised nodal integration: timing in
+                both precisions and --nsni-steps from impact
   batch         --batch-bars bars of uneven size in one context vs one
                 context per bar
   cpu_baseline  the C++ OpenMP restatement of the reference on the host
@@ -61,6 +63,8 @@ def parse():
     ap.add_argument("--pmb-nx", type=int, default=400,
                     help="in-plane particles per side of the bond-based peridynamics plate; 0 skips it")
     ap.add_argument("--pmb-steps", type=int, default=4000, help="steps of the peridynamics run")
+    ap.add_argument("--nsni-steps", type=int, default=2000,
+                    help="steps of the stabilised-nodal-integration runs of the same bar; 0 skips them")
     ap.add_argument("--batch-bars", type=int, default=256, help="bars of the batched run; 0 skips it")
     ap.add_argument("--batch-steps", type=int, default=64, help="timed steps of the batched and sequential runs")
     return ap.parse_args()
@@ -240,11 +244,16 @@ def run_ours(args, rank, world, dist):
     except Exception as ex:
         pmb = dict(error=str(ex))
     try:
+        nsni = nsni_run(case, dt, args) if args.nsni_steps > 0 else None
+    except Exception as ex:
+        nsni = dict(error=str(ex))
+    try:
         batch = batch_run(args) if args.batch_bars > 0 else None
     except Exception as ex:
         batch = dict(error=str(ex))
     out = dict(case=case, n=n, nnz=nnz, kmean=kmean, dt=dt, res=res, step0_s=step0_s, e2e_s=e2e_s, h2d=h2d,
-               d2h=d2h, peak=peak, peak_kind=peak_kind, scalars=s, dev_bytes=dev_bytes, accuracy=acc, learned=lrn, pmb=pmb, batch=batch,
+               d2h=d2h, peak=peak, peak_kind=peak_kind, scalars=s, dev_bytes=dev_bytes, accuracy=acc, learned=lrn, pmb=pmb,
+               nsni=nsni, batch=batch,
                tuned=tuned,
                e2e_parts=e2e_parts)
     return out
@@ -279,6 +288,42 @@ def accuracy(case, p, dt, steps):
     rel = {k: abs(mix[k] - ref[k]) / abs(ref[k]) for k in ref}
     return dict(steps=steps, fp64=ref, mixed=mix, mixed_rel_err=rel,
                 force_rel_l2_one_step=float(np.linalg.norm(f32 - f64) / np.linalg.norm(f64)))
+
+
+def nsni_run(case, dt, args):
+    """The same bar with stabilised nodal integration (ITYPE_INT = 2):
+    set-up time, device-timed steps in both precisions, then FP64 and mixed
+    runs from impact for --nsni-steps steps (the horizon direct nodal
+    integration does not reach on this lattice) with their end states."""
+    from taylor_b200 import _lib, cases, mega
+    p = _lib.params(**cases.param_kwargs(case, itype_int=2))
+    out = dict(steps=args.nsni_steps)
+    for mode in ("mixed", "fp64"):
+        t0 = time.perf_counter()
+        m = mega.Mega(case, p)
+        res = m.search_and_shapes()
+        setup_s = time.perf_counter() - t0
+        m.step(args.warmup, dt, mode=mode)
+        clk = Clocks()
+        clk.start()
+        ms = m.step_timed(args.steps, dt, mode=mode)
+        clocks = clk.stop()
+        st = m.step(args.nsni_steps - args.warmup - args.steps, dt, mode=mode, allow_status=True)
+        end = cases.bar_metrics(case, m.download(_lib.F_COO_CURRENT), m.download(_lib.F_EPS))
+        out[mode] = dict(setup_s=setup_s, nnz=int(res["nnz"]), ms_per_step=ms / args.steps,
+                         node_steps_per_s=case["n"] * args.steps / (ms / 1e3), clocks=clocks, status=int(st),
+                         end_state=end, device_bytes=m.device_bytes())
+        m.close()
+    if "end_state" in out.get("fp64", {}) and "end_state" in out.get("mixed", {}):
+        ref, mix = out["fp64"]["end_state"], out["mixed"]["end_state"]
+        out["mixed_rel_err"] = {k: abs(mix[k] - ref[k]) / abs(ref[k]) for k in ref}
+    # direct nodal integration over the same steps, for its status
+    d = mega.Mega(case, _lib.params(**cases.param_kwargs(case)))
+    d.search_and_shapes()
+    out["dni_fp64_status"] = int(d.step(args.nsni_steps, dt, mode="fp64", allow_status=True))
+    out["dni_fp64_end_state"] = cases.bar_metrics(case, d.download(_lib.F_COO_CURRENT), d.download(_lib.F_EPS))
+    d.close()
+    return out
 
 
 RATE_LAW = (90e6, 292e6, 0.31, 0.025, 1.0)  # A, B, n, C, epsdot0 of the power-law rate-dependent hardening
@@ -543,7 +588,7 @@ def main():
                  parts=r["e2e_parts"]),
         gpu_launches=mix["launches"], clocks=mix["clocks"], clocks_fp64=f64["clocks"],
         newton_iters_last_step=r["scalars"]["newton_iters"], plastic_nodes_last_step=r["scalars"]["plastic_nodes"],
-        accuracy=r["accuracy"], learned=r["learned"], peridynamics=r["pmb"], batch=r["batch"])
+        accuracy=r["accuracy"], learned=r["learned"], peridynamics=r["pmb"], nsni=r["nsni"], batch=r["batch"])
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -94,8 +94,10 @@ enum mega_field {
   MEGA_F_DSP_TOT_PHY = 12,/* (3N) physical total displacement                */
   MEGA_F_PRFORCE     = 13,/* (3,N) reaction force on fixed DOFs              */
   MEGA_F_NEWTON_IT   = 14,/* (N) Newton iterations of the last step (int32 stored as double) */
-  MEGA_F_STATE_AUX   = 15 /* (4,N) STATE(1,2,4,5) = EPS_SHEAR, EPS_VOL, DAM, DAM_SV of the damaged
+  MEGA_F_STATE_AUX   = 15,/* (4,N) STATE(1,2,4,5) = EPS_SHEAR, EPS_VOL, DAM, DAM_SV of the damaged
                              models (materials 3, 6); MEGA_ERR_STATE when no node has one */
+  MEGA_F_NSNI_SGRAD  = 16 /* (18,N) NSNI stress gradients d sigma/dx, d sigma/dy, d sigma/dz
+                             (Voigt each; the reference's LOCAL_DX/DY/DZ_STRESS), ITYPE_INT = 2 */
 };
 
 /* Scalars reported by mega_scalars (energies are those MAIN.F90:524-555 writes). */
@@ -118,7 +120,7 @@ typedef struct mega_params {
   int32_t rk_degree;       /* RK_DEGREE; only 1 (linear basis) is live        */
   int32_t rk_cont;         /* RK_CONT; 3 = cubic B-spline (KERNEL.F90:57-71)   */
   int32_t rk_impl;         /* RK_IMPL; read, no effect on the live path        */
-  int32_t itype_int;       /* ITYPE_INT; 0 = direct nodal integration         */
+  int32_t itype_int;       /* ITYPE_INT; 0 = direct nodal integration, 2 = NSNI (resident contexts) */
   int32_t ql;              /* QL (logical): quasi-linear moment regularisation */
   int32_t lagrangian;      /* LLAGRANGIAN (logical); only 1 is on this path    */
   int32_t finite_strain;   /* LFINITE_STRAIN (logical)                         */

@@ -518,6 +518,18 @@ void estimate_moduli(const double sinc[6], const double einc[6], double& shear, 
   bulk = bt;
 }
 
+// ESTIMATE_MODULI with NSNI_FLAG = .TRUE. (no clamp to half the elastic
+// moduli), then capped at the elastic moduli.
+void estimate_moduli_nsni(const double sinc[6], const double einc[6], double& shear, double& bulk) {
+  double sd[6], ss[6], ed[6], es[6];
+  dev_proj(sinc, sd); sphr_proj(sinc, ss);
+  dev_proj(einc, ed); sphr_proj(einc, es);
+  double nsd = tensor_norm(sd), nss = tensor_norm(ss);
+  double ned = tensor_norm_strain(ed), nes = tensor_norm_strain(es);
+  if (ned > 1.0e-8 && nsd > 1.0e-8) shear = std::min(nsd / ned / 2.0, shear);
+  if (nes > 1.0e-8 && nss > 1.0e-8) bulk = std::min(nss / nes / 3.0, bulk);
+}
+
 // Damage shared by both damaged models (CONSTITUTE_VONMISES_DAM.F90:94-125,
 // CONSTITUTE_DRUCKPRAG.F90:84-113): eta = TENSOR_NORM(total strain) (the
 // stress norm, as written); between K_I and K_C the damage follows
@@ -893,8 +905,10 @@ int orc_vm_rate(int n, const double* spred, const double* props, double dt, doub
 // (LOCAL_DX_STRESS, MAIN.F90:62, 206) and the force term
 // B_{,a}^T sigma_{,a} V J M_a (FINT.F90:1127-1208) with the second moments
 // M_a = (cell width_a)^2 / 12 of SECOND_MOMENT (PRE_MODEL_SECOND_MOMENT.F90).
-// Stress gradients evolve with the elastic moduli (the stabilisation acts on
-// the modes nodal integration misses, not on the material response).
+// Stress gradients evolve with an isotropic tangent probed from this step's
+// stress and strain increments: ESTIMATE_MODULI with NSNI_FLAG set
+// (ESTIMATE_MODULI.F90:16-86, the lower clamp off), kept at most elastic so
+// the stable step of the elastic moduli still holds.
 
 // Smoothed second derivatives of node i's shape functions (6 per neighbour,
 // order XX, YY, ZZ, XY, YZ, XZ as SHPDD_SM): RK1 gradients at the six face
@@ -1063,6 +1077,8 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
         }
       }
       for (int k = 0; k < 6; ++k) lstrain[k] = lstrain[k] + strain[k];   // FINT.F90:789
+      double srot[6];  // the rotated old stress (NSNI probes the material's increment from it)
+      std::memcpy(srot, lstress, sizeof(srot));
       double lam = lprop[27], mu = lprop[28], l2m = lprop[29];            // FORM_CMAT :252-288
       double C[6][6] = {};
       C[0][0] = C[1][1] = C[2][2] = l2m;
@@ -1129,6 +1145,19 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
               H[a][k][m] = v;
             }
         const double* sml = sm_len + 6 * (size_t)i;
+        double gs = shear_mod(lprop[1], lprop[0]), ks = bulk_mod(lprop[1], lprop[0]);
+        {
+          double dso[6];
+          for (int k = 0; k < 6; ++k) dso[k] = lstress[k] - srot[k];
+          estimate_moduli_nsni(dso, strain, gs, ks);
+        }
+        double Cs[6][6] = {};
+        {
+          const double lam_s = ks - 2.0 * gs / 3.0, l2m_s = ks + 4.0 * gs / 3.0;
+          Cs[0][0] = Cs[1][1] = Cs[2][2] = l2m_s;
+          Cs[3][3] = Cs[4][4] = Cs[5][5] = gs;
+          Cs[0][1] = Cs[1][0] = Cs[0][2] = Cs[2][0] = Cs[2][1] = Cs[1][2] = lam_s;
+        }
         double fac[3], W[3][3][3];  // W[a] = M_a / V * V J sigma_a INV3(F)^T
         for (int a = 0; a < 3; ++a) {
           const double wd = sml[2 * a] + sml[2 * a + 1];
@@ -1146,7 +1175,7 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
           double ds[6];
           for (int r = 0; r < 6; ++r) {
             double v = 0.0;
-            for (int c = 0; c < 6; ++c) v += C[r][c] * de[c];
+            for (int c = 0; c < 6; ++c) v += Cs[r][c] * de[c];
             ds[r] = v;
           }
           for (int k = 0; k < 6; ++k) sg[6 * a + k] += ds[k];

@@ -32,7 +32,7 @@ FLAG_LEARNED_GUESS = 0x200
 MAT_ELASTIC, MAT_VONMISES, MAT_DRUCKER_PRAGER, MAT_VM_DAMAGE, MAT_VM_RATE = 1, 2, 3, 6, 7
 
 F_COO_CURRENT, F_DSP, F_DSP_TOT, F_VEL, F_ACL, F_FINT, F_FEXT, F_STRESS, F_STRAIN, F_EPS = range(10)
-F_STRAIN_EQ, F_WAVE_VEL, F_DSP_TOT_PHY, F_PRFORCE, F_NEWTON_IT, F_STATE_AUX = range(10, 16)
+F_STRAIN_EQ, F_WAVE_VEL, F_DSP_TOT_PHY, F_PRFORCE, F_NEWTON_IT, F_STATE_AUX, F_NSNI_SGRAD = range(10, 17)
 
 
 class MegaParams(C.Structure):

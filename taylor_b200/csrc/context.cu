@@ -182,6 +182,11 @@ struct Ctx {
   void* tmat = nullptr;
   int32_t* iters = nullptr;
   double* aux = nullptr;  // 4 per node, STATE(1, 2, 4, 5), when a damaged model is present
+  // NSNI (ITYPE_INT = 2): second derivatives per entry in CSR and CSC order,
+  // stress gradients (18 per node) and per-step scratch
+  bool nsni = false;
+  NsniS nsr{}, nsc{};
+  double *sgrad = nullptr, *hq = nullptr, *nsw = nullptr, *fstab = nullptr, *stress_prev = nullptr;
   StepAccum* acc = nullptr;
   unsigned* status = nullptr;
   bool phy_valid = true;
@@ -292,26 +297,42 @@ static TiledForceArgs force_args(Ctx* c, double dt, int mode, int predict) {
   f.tshp = c->tshp; f.tmat = c->tmat; f.has_body = c->has_body; f.predict = predict;
   f.ebc = c->ebc; f.mass = c->mass; f.matidx = c->matidx; f.mats = c->mats; f.body_id = c->body_id;
   f.fint = c->fint; f.fext = c->fext; f.vel = c->vel; f.acl = c->acl; f.dsp = c->dsp; f.dsp_tot = c->dsp_tot;
-  f.prforce = c->prforce; f.dt = dt; f.acc = c->acc; f.status = c->status;
+  f.prforce = c->prforce; f.fadd = c->nsni ? c->fstab : nullptr; f.dt = dt; f.acc = c->acc; f.status = c->status;
   return f;
 }
+
+static NsniStepArgs nsni_args(Ctx* c) {
+  NsniStepArgs a{};
+  a.n = c->n; a.fg = c->fg; a.stress_old = c->stress_prev; a.stress_new = c->stress; a.sml = c->sm_len;
+  a.vol = c->vol; a.matidx = c->matidx; a.mats = c->mats; a.hq = c->hq; a.sgrad = c->sgrad; a.w = c->nsw;
+  a.fstab = c->fstab; a.finite_strain = c->p.finite_strain; a.inv3_exact = c->p.inv3_exact; a.acc = c->acc;
+  a.status = c->status;
+  return a;
+}
+
+// kernels one step launches
+static int kernels_per_step(const Ctx* c) { return c->nsni ? 6 : 3; }
 
 static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) {
   const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
   const bool interp = (mode & MEGA_FLAG_INTERP_EACH_STEP) != 0;
   if (ev) MEGA_TRY(cudaEventRecord(ev[0], c->s));
+  if (c->nsni)
+    MEGA_TRY(cudaMemcpyAsync(c->stress_prev, c->stress, sizeof(double) * 6 * c->n, cudaMemcpyDeviceToDevice, c->s));
   int r = launch_defgrad_tiled(c->s, mixed, interp, c->n, c->rt, c->csr.rowptr, mixed ? c->pk32 : c->pk64, c->dsp,
                                c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc,
                                c->var_defgrad[mixed]);
   if (r) return r;
+  if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->dsp, 0))) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[1], c->s));
   r = launch_stress(c->s, mixed, stress_args(c, dt, mode));
   if (r) return r;
+  if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->dsp, 1))) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[2], c->s));
   r = launch_force_tiled(c->s, mixed, force_args(c, dt, mode, predict), c->var_force[mixed]);
   if (r) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[3], c->s));
-  c->launches += 3;
+  c->launches += kernels_per_step(c);
   return 0;
 }
 
@@ -352,7 +373,7 @@ static int run_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
     if (r) return r;
     while (rem >= len) {
       MEGA_TRY(cudaGraphLaunch(c->gexec, c->s));
-      c->launches += 3 * len;
+      c->launches += kernels_per_step(c) * len;
       rem -= len;
     }
   }
@@ -547,6 +568,7 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   if (!p || n <= 0 || !coo || !win || !vol || !mass || !ebc || !vinit || !props || !mat_type || !sm_len || !handle)
     return MEGA_ERR_ARG;
   if (p->lagrangian != 1 || p->peridynamics != 0) return MEGA_ERR_UNSUPPORTED;
+  if (p->itype_int != 0 && p->itype_int != 2) return MEGA_ERR_UNSUPPORTED;  // DNI or NSNI
   for (int64_t m = 0; m < 3 * (int64_t)n; ++m)
     if (ebc[m] != 0 && ebc[m] != 1) return MEGA_ERR_UNSUPPORTED;  // prescribed-velocity fixity (code 2)
   Ctx* c = new Ctx();
@@ -568,6 +590,13 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   CA(c->fint, n3); CA(c->fext, n3); CA(c->prforce, n3); CA(c->scratch3, n3);
   CA(c->stress, 6 * (int64_t)n); CA(c->strain, 6 * (int64_t)n); CA(c->eps, n); CA(c->strain_eq, n);
   CA(c->wvel, n); CA(c->fg, 18 * (int64_t)n); CA(c->iters, n); CA(c->acc, 1); CA(c->status, 1);
+  c->nsni = p->itype_int == 2;
+  if (c->nsni) {
+    CA(c->sgrad, 18 * (int64_t)n); CA(c->hq, 18 * (int64_t)n); CA(c->nsw, 18 * (int64_t)n);
+    CA(c->fstab, n3); CA(c->stress_prev, 6 * (int64_t)n);
+    cudaMemsetAsync(c->sgrad, 0, sizeof(double) * 18 * n, c->s);
+    cudaMemsetAsync(c->fstab, 0, sizeof(double) * n3, c->s);
+  }
   {
     double* t = nullptr;
     CA(t, 12 * (int64_t)n);
@@ -681,16 +710,19 @@ static int search_instances(Ctx* c, DevCSR& csr, DevPool& out) {
 // the original numbering to the bin-cell numbering, iperm moves it back.
 static int permute_nodes(Ctx* c, const int32_t* map) {
   const int32_t n = c->n;
-  DevPool tp(c->s);
-  unsigned char* tmp = nullptr;
-  MEGA_ALLOC(tp, tmp, (int64_t)n * 48);
   struct Arr { void* p; int w; int es; };
   const Arr list[] = {
       {c->coo, 3, 8}, {c->win, 3, 8}, {c->mass, 3, 8}, {c->dsp, 3, 8}, {c->dsp_tot, 3, 8}, {c->dsp_tot_phy, 3, 8},
       {c->vel, 3, 8}, {c->acl, 3, 8}, {c->fint, 3, 8}, {c->fext, 3, 8}, {c->prforce, 3, 8}, {c->bodyforce, 3, 8},
       {c->sm_len, 6, 8}, {c->stress, 6, 8}, {c->strain, 6, 8}, {c->vol, 1, 8}, {c->eps, 1, 8},
       {c->strain_eq, 1, 8}, {c->wvel, 1, 8}, {c->ebc, 3, 1}, {c->body_id, 1, 1}, {c->ebc_nodes, 1, 4},
-      {c->iters, 1, 4}, {c->matidx, 1, 2}, {c->aux, 4, 8}};
+      {c->iters, 1, 4}, {c->matidx, 1, 2}, {c->aux, 4, 8}, {c->sgrad, 18, 8}};
+  int64_t row_bytes = 0;  // the widest per-node row
+  for (const Arr& a : list)
+    if (a.p) row_bytes = std::max<int64_t>(row_bytes, (int64_t)a.w * a.es);
+  DevPool tp(c->s);
+  unsigned char* tmp = nullptr;
+  MEGA_ALLOC(tp, tmp, (int64_t)n * row_bytes);
   for (const Arr& a : list) {
     if (!a.p) continue;
     k_perm_gather<<<grid_for((int64_t)n * a.w, 256), 256, 0, c->s>>>(n, a.w, a.es, map, (const unsigned char*)a.p,
@@ -741,6 +773,25 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   r = rk_shapes(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr0, shp0, g0x, g0y, g0z, c->status);
   if (r) return r;
   tr.mark("rk_shapes");
+  NsniS s0{};
+  if (c->nsni) {  // smoothed second derivatives, one axis (two faces) at a time
+    for (int k = 0; k < 6; ++k) MEGA_ALLOC(tmp0, s0.v[k], m);
+    DevPool faces(c->s);
+    double* g[6];
+    for (int k = 0; k < 6; ++k) MEGA_ALLOC(faces, g[k], m);
+    for (int ax = 0; ax < 3; ++ax) {
+      if ((r = rk_grad_at_face(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr0, c->sm_len, 2 * ax, g[0], g[1],
+                               g[2], c->status)) ||
+          (r = rk_grad_at_face(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr0, c->sm_len, 2 * ax + 1, g[3],
+                               g[4], g[5], c->status)))
+        return r;
+      const double* gp[3] = {g[0], g[1], g[2]};
+      const double* gm[3] = {g[3], g[4], g[5]};
+      if ((r = nsni_combine(c->s, n, ax, csr0.rowptr, c->sm_len, gp, gm, s0))) return r;
+    }
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    tr.mark("nsni_second_derivatives");
+  }
   int st = 0;
   if (gn || gstart || gstack || shp || dshp) {
     std::vector<int64_t> rp(n + 1);
@@ -796,6 +847,17 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
                                                                     g0x, g0y, g0z, c->csr.rowptr, c->csr.col, c->shp,
                                                                     g1x, g1y, g1z);
   MEGA_CHECK_LAUNCH();
+  if (c->nsni) {
+    for (int k = 0; k < 6; ++k) {
+      MEGA_ALLOC(c->nbpool, c->nsr.v[k], m);
+      MEGA_ALLOC(c->nbpool, c->nsc.v[k], m);
+    }
+    for (int k = 0; k < 6; k += 2)  // (the column indices are rewritten with the same values)
+      k_permute_rows<<<grid_for((int64_t)n * 32, 256), 256, 0, c->s>>>(
+          n, c->perm, c->iperm, csr0.rowptr, csr0.col, s0.v[k], s0.v[k + 1], s0.v[k], s0.v[k + 1], c->csr.rowptr,
+          c->csr.col, c->nsr.v[k], c->nsr.v[k + 1], c->nsr.v[k], c->nsr.v[k + 1]);
+    MEGA_CHECK_LAUNCH();
+  }
   MEGA_TRY(cudaStreamSynchronize(c->s));
   tmp0.free_all();
   tr.mark("renumber");
@@ -804,6 +866,11 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   if (r) return r;
   r = build_transpose(c->s, c->csr, c->nbpool);
   if (r) return r;
+  if (c->nsni) {
+    for (int k = 0; k < 6; ++k)
+      k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->csr.tpos, c->nsr.v[k], c->nsc.v[k]);
+    MEGA_CHECK_LAUNCH();
+  }
   tr.mark("transpose");
   r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->rt, c->nbpool, nullptr);
   if (r) return r;
@@ -851,10 +918,13 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     MEGA_CHECK_LAUNCH();
   }
   MEGA_TRY(cudaStreamSynchronize(c->s));
-  // the per-step kernels read neither the transposed row ids nor the positions
-  c->nbpool.release(c->csr.trow);
+  // the per-step kernels read neither the transposed row ids (but NSNI's
+  // column gather) nor the positions
+  if (!c->nsni) {
+    c->nbpool.release(c->csr.trow);
+    c->csr.trow = nullptr;
+  }
   c->nbpool.release(c->csr.tpos);
-  c->csr.trow = nullptr;
   c->csr.tpos = nullptr;
   tmp1.free_all();
   tr.mark("pack_and_release");
@@ -965,6 +1035,9 @@ int mega_download(int64_t h, int32_t field, double* dst) {
     case MEGA_F_STATE_AUX:
       if (!c->aux) return MEGA_ERR_STATE;
       src = c->aux; w = 4; break;
+    case MEGA_F_NSNI_SGRAD:
+      if (!c->sgrad) return MEGA_ERR_STATE;
+      src = c->sgrad; w = 18; break;
     case MEGA_F_NEWTON_IT: {
       std::vector<int32_t> it(n);
       int r = download_nodes(c, c->iters, 1, 4, it.data());
@@ -1015,6 +1088,9 @@ int mega_upload(int64_t h, int32_t field, const double* src) {
     case MEGA_F_STATE_AUX:
       if (!c->aux) return MEGA_ERR_STATE;
       dst = c->aux; w = 4; break;
+    case MEGA_F_NSNI_SGRAD:
+      if (!c->sgrad) return MEGA_ERR_STATE;
+      dst = c->sgrad; w = 18; break;
     default: return MEGA_ERR_ARG;
   }
   const size_t bytes = (size_t)n * w * sizeof(double);
@@ -1086,6 +1162,7 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
       {c->eps, 8 * n}, {c->strain_eq, 8 * n}, {c->wvel, 8 * n}, {c->fg, 144 * n}, {c->tmat, 12 * ts * n},
       {c->iters, 4 * n}, {c->acc, sizeof(StepAccum)}, {c->status, sizeof(unsigned)}};
   if (c->aux) arrs.push_back({c->aux, 32 * n});
+  if (c->sgrad) arrs.push_back({c->sgrad, 144 * n});
   DevPool snap(c->s);
   std::vector<unsigned char*> copies;
   for (const Arr& a : arrs) {
@@ -1448,7 +1525,9 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
       !gdinc || !gdinc_tot || !gn || !gstart || !gstack || !gstack_shp || !gstack_dshp || !fint || !fext ||
       !gmax_wvel || !gstrain_eq || !gint_work)
     return MEGA_ERR_ARG;
-  if (p->lagrangian != 1) return MEGA_ERR_UNSUPPORTED;
+  // NSNI keeps second derivatives and stress gradients this argument list
+  // has no room for: resident contexts only
+  if (p->lagrangian != 1 || p->itype_int == 2) return MEGA_ERR_UNSUPPORTED;
   StreamGuard sg;
   int r = make_stream(&sg.s);
   if (r) return r;

@@ -143,6 +143,10 @@ int rk_shapes(cudaStream_t s, const mega_params& p, int32_t n, const double* coo
               const int32_t* ebc_nodes, const DevCSR& csr, double* shp, double* gx, double* gy, double* gz,
               unsigned* status);
 
+int rk_grad_at_face(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
+                    const int32_t* ebc_nodes, const DevCSR& csr, const double* sml, int face, double* gx, double* gy,
+                    double* gz, unsigned* status);
+
 // Per-material constants, deduplicated from PROPS(30,N) at init.
 struct MatEntry {
   int32_t type;
@@ -226,6 +230,35 @@ int launch_defgrad(cudaStream_t s, bool mixed, bool interp, int32_t n, const Dev
                    const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg,
                    StepAccum* acc);
 int launch_stress(cudaStream_t s, bool mixed, const StressArgs& a);
+
+// ---------------- NSNI (nsni.cu)
+struct NsniS {
+  double* v[6];  // smoothed second derivatives per list entry: XX, YY, ZZ, XY, YZ, XZ
+};
+struct NsniStepArgs {
+  int32_t n;
+  const double* fg;          // F, G0 of this step
+  const double* stress_old;  // the stress before this step's update
+  const double* stress_new;
+  const double* sml;         // SM_LEN (6, n)
+  const double* vol;
+  const uint16_t* matidx;
+  const MatEntry* mats;
+  double* hq;                // 18 per node: sum_J S_q du_J,k
+  double* sgrad;             // 18 per node: sigma_,x, sigma_,y, sigma_,z (Voigt)
+  double* w;                 // 18 per node: force weights on the six S components
+  double* fstab;             // 3 per node: the stabilisation force
+  int finite_strain;
+  int inv3_exact;
+  StepAccum* acc;
+  unsigned* status;
+};
+int nsni_combine(cudaStream_t s, int32_t n, int axis, const int64_t* rowptr, const double* sml, const double* gp[3],
+                 const double* gm[3], const NsniS& out);
+// stage 0: the row gather of H (after the displacement increment is known);
+// stage 1: stress gradients, weights and the column gather of the force
+int nsni_step(cudaStream_t s, const NsniStepArgs& a, const DevCSR& csr, const NsniS& rows, const NsniS& cols,
+              const double* du, int stage);
 
 // surrogate network of the rate-dependent return mapping (mlp.cu)
 int mlp_nparams();

@@ -306,10 +306,16 @@ struct PmbArgs {
 };
 
 // T = per-bond arithmetic: float (the mixed path: float bond geometry and
-// force from float offsets to the tile's first particle) or double (the
-// oracle's arithmetic, from X and u, for exact parity checks).
+// force, the bond vector rounded from the double difference of X and the
+// displacements from float offsets to the tile's first particle) or double
+// (the oracle's arithmetic, from X and u, for exact parity checks).
+//
+// FP64 rows are padded to multiples of 4 bonds (pads point at the particle
+// itself and start broken), so a lane reads the ranks of 4 consecutive bonds
+// as one 8-byte load and their 4 broken bits from one 32-bit word; the float
+// path, bound by its shared-memory gathers rather than by these loads, keeps
+// unpadded rows and one bond per load.
 constexpr int kGP = 8;  // lanes per particle of the bond loop
-constexpr int kUP = 4;  // bond ranks in flight per lane
 
 template <typename T>
 __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
@@ -320,7 +326,9 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
   const bool f64 = sizeof(T) == sizeof(double);
   // staged set: FP64 8 doubles per particle (X, u, vol, pad); float: X as
   // 3 doubles (the bond vector is rounded from the exact difference, as the
-  // FP64 path forms it) and one float4 (u - u_r0, vol)
+  // FP64 path forms it: float offsets of X put 1e-6 of the bond length into
+  // the stretch and move the break of near-critical bonds) and one float4
+  // (u - u_r0, vol)
   double* sd = smp;
   float4* sf = reinterpret_cast<float4*>(smp + ((3 * cnt + 1) & ~1));
   const int64_t r0 = t * a.R;
@@ -350,65 +358,78 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
   T f0 = T(0), f1 = T(0), f2 = T(0);
   unsigned nb = 0;
   const T c = (T)a.c, sc = (T)a.s_c;
+  constexpr int GB = sizeof(T) == sizeof(double) ? 4 : 1;  // bonds per load group
+  constexpr int NQ = GB == 4 ? 2 : 4;                          // groups in flight per lane
   const int64_t p1 = a.rowptr[i + 1];
-  for (int64_t pb = a.rowptr[i] + q; pb < p1; pb += kGP * kUP) {
-    int lj[kUP];
-    uint32_t wd[kUP];
+  for (int64_t pb = a.rowptr[i] + GB * q; pb < p1; pb += GB * kGP * NQ) {
+    uint32_t lw[NQ][2];
+    uint32_t wd[NQ];
 #pragma unroll
-    for (int u = 0; u < kUP; ++u) {
-      const int64_t p = pb + u * kGP;
-      lj[u] = p < p1 ? (int)a.lidx[p] : -1;
-      wd[u] = p < p1 ? a.broken[p >> 5] : 0u;
-    }
-#pragma unroll
-    for (int u = 0; u < kUP; ++u) {
-      const int64_t p = pb + u * kGP;
-      if (lj[u] < 0) continue;  // past the row
-      const uint32_t bit = 1u << (p & 31);
-      if (wd[u] & bit) continue;
-      T s, e0, e1, e2, l, vj;
-      if (f64) {
-        // the oracle's arithmetic: xi from X, eta = xi + (u_j - u_i), s = (|eta| - |xi|)/|xi|
-        const double2* d = reinterpret_cast<const double2*>(sd + 8 * lj[u]);
-        const double2 q0 = d[0], q1 = d[1], q2 = d[2], q3 = d[3];
-        const double x0 = q0.x - Xi0, x1 = q0.y - Xi1, x2 = q1.x - Xi2;
-        const double L0d = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-        if (L0d == 0.0) continue;  // the particle itself
-        e0 = (T)(x0 + (q1.y - ui0));
-        e1 = (T)(x1 + (q2.x - ui1));
-        e2 = (T)(x2 + (q2.y - ui2));
-        const T L0 = (T)L0d;
-        l = (T)sqrt((double)(e0 * e0 + e1 * e1 + e2 * e2));
-        s = (l - L0) / L0;
-        vj = (T)q3.x;
+    for (int g = 0; g < NQ; ++g) {
+      const int64_t p = pb + GB * kGP * g;
+      lw[g][0] = lw[g][1] = 0u;
+      if (p < p1) {
+        if (GB == 4) {
+          const uint2 v = *reinterpret_cast<const uint2*>(a.lidx + p);
+          lw[g][0] = v.x; lw[g][1] = v.y;
+        } else {
+          lw[g][0] = a.lidx[p];
+        }
+        wd[g] = a.broken[p >> 5] >> (p & 31);
       } else {
-        const double* xq = sd + 3 * lj[u];
-        const float4 qb = sf[lj[u]];
-        const float x0 = (float)(xq[0] - Xi0), x1 = (float)(xq[1] - Xi1), x2 = (float)(xq[2] - Xi2);
-        const float xx = x0 * x0 + x1 * x1 + x2 * x2;
-        if (xx == 0.f) continue;  // the particle itself
-        const float d0 = qb.x - fu0, d1 = qb.y - fu1, d2 = qb.z - fu2;
-        // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|)),
-        // lengths from the hardware reciprocal square root (about 2 ulp)
-        const float f_e0 = x0 + d0, f_e1 = x1 + d1, f_e2 = x2 + d2;
-        const float ee = f_e0 * f_e0 + f_e1 * f_e1 + f_e2 * f_e2;
-        const float rL0 = rsqrtf(xx), rl = rsqrtf(ee);
-        const float fL0 = xx * rL0, fl = ee * rl;
-        const float num = 2.f * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
-        s = (T)(num * rL0 * __frcp_rn(fl + fL0));
-        // eta / |eta| directly, so the force weight needs no division
-        e0 = (T)(f_e0 * rl); e1 = (T)(f_e1 * rl); e2 = (T)(f_e2 * rl);
-        l = T(1);
-        vj = (T)qb.w;
+        wd[g] = 0xFu;  // past the row: skipped
       }
-      if (s > sc) {
-        atomicOr(&a.broken[p >> 5], bit);
-        ++nb;
-        continue;
-      }
-      const T w = f64 ? c * s * vj / l : c * s * vj;  // the float path's eta is already unit
-      f0 += w * e0; f1 += w * e1; f2 += w * e2;
     }
+#pragma unroll
+    for (int g = 0; g < NQ; ++g)
+#pragma unroll
+      for (int u = 0; u < GB; ++u) {
+        if ((wd[g] >> u) & 1u) continue;  // broken (or a pad)
+        const int64_t p = pb + GB * kGP * g + u;
+        const int lj = (int)((lw[g][u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+        T s, e0, e1, e2, l, vj;
+        if (f64) {
+          // the oracle's arithmetic: xi from X, eta = xi + (u_j - u_i), s = (|eta| - |xi|)/|xi|
+          const double2* d = reinterpret_cast<const double2*>(sd + 8 * lj);
+          const double2 q0 = d[0], q1 = d[1], q2 = d[2], q3 = d[3];
+          const double x0 = q0.x - Xi0, x1 = q0.y - Xi1, x2 = q1.x - Xi2;
+          const double L0d = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+          if (L0d == 0.0) continue;  // the particle itself
+          e0 = (T)(x0 + (q1.y - ui0));
+          e1 = (T)(x1 + (q2.x - ui1));
+          e2 = (T)(x2 + (q2.y - ui2));
+          const T L0 = (T)L0d;
+          l = (T)sqrt((double)(e0 * e0 + e1 * e1 + e2 * e2));
+          s = (l - L0) / L0;
+          vj = (T)q3.x;
+        } else {
+          const double* xq = sd + 3 * lj;
+          const float4 ua = sf[lj];
+          const float x0 = (float)(xq[0] - Xi0), x1 = (float)(xq[1] - Xi1), x2 = (float)(xq[2] - Xi2);
+          const float xx = x0 * x0 + x1 * x1 + x2 * x2;
+          if (xx == 0.f) continue;  // the particle itself
+          const float d0 = ua.x - fu0, d1 = ua.y - fu1, d2 = ua.z - fu2;
+          // stretch without cancellation: (|xi+d|^2 - |xi|^2) / (|xi| (|xi+d| + |xi|)),
+          // lengths from the hardware reciprocal square root (about 2 ulp)
+          const float f_e0 = x0 + d0, f_e1 = x1 + d1, f_e2 = x2 + d2;
+          const float ee = f_e0 * f_e0 + f_e1 * f_e1 + f_e2 * f_e2;
+          const float rL0 = rsqrtf(xx), rl = rsqrtf(ee);
+          const float fL0 = xx * rL0, fl = ee * rl;
+          const float num = 2.f * (x0 * d0 + x1 * d1 + x2 * d2) + (d0 * d0 + d1 * d1 + d2 * d2);
+          s = (T)(num * rL0 * __frcp_rn(fl + fL0));
+          // eta / |eta| directly, so the force weight needs no division
+          e0 = (T)(f_e0 * rl); e1 = (T)(f_e1 * rl); e2 = (T)(f_e2 * rl);
+          l = T(1);
+          vj = (T)ua.w;
+        }
+        if (s > sc) {
+          atomicOr(&a.broken[p >> 5], 1u << (p & 31));
+          ++nb;
+          continue;
+        }
+        const T w = f64 ? c * s * vj / l : c * s * vj;  // the float path's eta is already unit
+        f0 += w * e0; f1 += w * e1; f2 += w * e2;
+      }
   }
 #pragma unroll
   for (int o = 1; o < kGP; o <<= 1) {
@@ -452,10 +473,11 @@ __global__ void k_pmb_perm(int32_t n, int w, const int32_t* __restrict__ perm, c
   if (to) dst[e] = src[(int64_t)perm[r] * w + k];
   else dst[(int64_t)perm[r] * w + k] = src[e];
 }
+// row lengths in the new order, rounded up to whole groups of pad bonds
 __global__ void k_pmb_rowlen(int32_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ rowptr0,
-                             int32_t* __restrict__ len) {
+                             int32_t pad, int32_t* __restrict__ len) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (r < n) len[r] = (int32_t)(rowptr0[perm[r] + 1] - rowptr0[perm[r]]);
+  if (r < n) len[r] = ((int32_t)(rowptr0[perm[r] + 1] - rowptr0[perm[r]]) + pad - 1) / pad * pad;
 }
 // warp per new row: the old row's entries in their order, columns renumbered
 __global__ void k_pmb_rows(int32_t n, const int32_t* __restrict__ perm, const int32_t* __restrict__ iperm,
@@ -465,7 +487,16 @@ __global__ void k_pmb_rows(int32_t n, const int32_t* __restrict__ perm, const in
   const int lane = threadIdx.x & 31;
   if (r >= n) return;
   const int64_t a0 = rowptr0[perm[r]], len = rowptr0[perm[r] + 1] - a0, b0 = rowptr1[r];
-  for (int64_t k = lane; k < len; k += 32) col1[b0 + k] = iperm[col0[a0 + k]];
+  const int64_t lp = rowptr1[r + 1] - b0;
+  for (int64_t k = lane; k < lp; k += 32) col1[b0 + k] = k < len ? iperm[col0[a0 + k]] : (int32_t)r;  // pads: self
+}
+// the pads of each padded row start broken
+__global__ void k_pmb_padbits(int32_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ rowptr0,
+                              const int64_t* __restrict__ rowptr1, uint32_t* __restrict__ bits) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t len = rowptr0[perm[r] + 1] - rowptr0[perm[r]];
+  for (int64_t p = rowptr1[r] + len; p < rowptr1[r + 1]; ++p) atomicOr(&bits[p >> 5], 1u << (p & 31));
 }
 // per-bond flags between the two orders: new entry rowptr1[r] + k is old
 // entry rowptr0[perm[r]] + k.  to_new: old bytes -> new bits (OR); else new
@@ -562,7 +593,8 @@ struct PmbCtx {
   int32_t n = 0;
   cudaStream_t s = nullptr;
   DevPool pool;
-  DevCSR csr;          // in the bin-cell numbering
+  DevCSR csr;          // in the bin-cell numbering (FP64: rows padded to groups of 4 bonds)
+  int64_t nreal = 0;   // bonds without the pads
   int32_t* perm = nullptr;      // new particle r = caller's particle perm[r]
   int64_t* rowptr0 = nullptr;   // the caller's row offsets (bond flags map through them)
   TileSet tiles;
@@ -810,19 +842,25 @@ int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double*
   cudaMemcpyAsync(bf8, c->fixed, n, cudaMemcpyDeviceToDevice, c->s);
   k_pmb_perm<int8_t><<<gn, 256, 0, c->s>>>(n, 1, c->perm, bf8, c->fixed, true);
   c->csr.n = n;
-  c->csr.nnz = m;
-  c->csr.gmaxn = csr0.gmaxn;
+  const int32_t pad = c->f64 ? 4 : 1;  // FP64 rows in groups of 4 bonds
+  c->csr.gmaxn = (csr0.gmaxn + pad - 1) / pad * pad;
+  c->nreal = m;
   PA(c->rowptr0, (int64_t)n + 1);
   cudaMemcpyAsync(c->rowptr0, csr0.rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToDevice, c->s);
   PA(c->csr.rowptr, (int64_t)n + 1);
-  PA(c->csr.col, m);
-  k_pmb_rowlen<<<gn, 256, 0, c->s>>>(n, c->perm, csr0.rowptr, len);
+  k_pmb_rowlen<<<gn, 256, 0, c->s>>>(n, c->perm, csr0.rowptr, pad, len);
   if ((r = scan_counts(c->s, len, c->csr.rowptr, n, tmp))) return fail(r);
+  int64_t mp = 0;  // entries with the rows padded
+  if (cudaMemcpyAsync(&mp, c->csr.rowptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->s) != cudaSuccess ||
+      cudaStreamSynchronize(c->s) != cudaSuccess)
+    return fail(MEGA_ERR_CUDA);
+  c->csr.nnz = mp;
+  PA(c->csr.col, mp);
   const unsigned gw = (unsigned)(((int64_t)n * 32 + 255) / 256);
   k_pmb_rows<<<gw, 256, 0, c->s>>>(n, c->perm, iperm, csr0.rowptr, csr0.col, c->csr.rowptr, c->csr.col);
   if (cudaGetLastError() != cudaSuccess) return fail(MEGA_ERR_CUDA);
   // tiles of consecutive particles with their neighbour sets
-  if ((r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->tiles, c->pool, nullptr)))
+  if ((r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, mp, c->csr.gmaxn, c->tiles, c->pool, nullptr)))
     return fail(r);
   {
     static bool smem_set = false;  // FP64 stages 64 bytes per particle, float 40: up to 64 KB
@@ -835,9 +873,10 @@ int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double*
       smem_set = true;
     }
   }
-  PA(c->broken, (m + 31) / 32);
+  PA(c->broken, (mp + 31) / 32);
 #undef PA
-  cudaMemsetAsync(c->broken, 0, sizeof(uint32_t) * ((m + 31) / 32), c->s);
+  cudaMemsetAsync(c->broken, 0, sizeof(uint32_t) * ((mp + 31) / 32), c->s);
+  k_pmb_padbits<<<gn, 256, 0, c->s>>>(n, c->perm, c->rowptr0, c->csr.rowptr, c->broken);
   if (broken0) {  // the caller's order -> bits in the renumbered order
     uint8_t* b0 = nullptr;
     if (tmp.alloc(&b0, m)) return fail(MEGA_ERR_NOMEM);
@@ -936,7 +975,7 @@ int mega_pmb_download(int64_t h, int32_t what, double* dst, int64_t* nbroken) {
     MEGA_TRY(cudaMemcpyAsync(dst, d, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->s));
     MEGA_TRY(cudaStreamSynchronize(c->s));
   } else if (what == 3) {  // the caller's list order
-    const int64_t m = c->csr.nnz;
+    const int64_t m = c->nreal;
     uint8_t* d = nullptr;
     MEGA_ALLOC(tp, d, m);
     k_pmb_flags<<<(unsigned)(((int64_t)c->n * 32 + 255) / 256), 256, 0, c->s>>>(c->n, c->perm, c->rowptr0,

@@ -80,14 +80,19 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
                                                    const int32_t* __restrict__ ebc_nodes,
                                                    const int64_t* __restrict__ rowptr,
                                                    const int32_t* __restrict__ col, int ql, double ql_coef,
-                                                   double ql_len, int shsup, double* __restrict__ shp,
+                                                   double ql_len, int shsup, const double* __restrict__ sml,
+                                                   int face, double* __restrict__ shp,
                                                    double* __restrict__ gx, double* __restrict__ gy,
                                                    double* __restrict__ gz, unsigned* __restrict__ status) {
   const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kLPN;
   const int lane = threadIdx.x & (kLPN - 1);
   const unsigned gm = ((1u << kLPN) - 1u) << (threadIdx.x & (32 - kLPN));
   if (i >= n) return;  // whole groups leave together
-  const double xi[3] = {coo[3 * i], coo[3 * i + 1], coo[3 * i + 2]};
+  double xi[3] = {coo[3 * i], coo[3 * i + 1], coo[3 * i + 2]};
+  if (face >= 0) {  // a face point of the smoothing cell, x +- SM_LEN (+X, -X, +Y, -Y, +Z, -Z)
+    const int ax = face >> 1;
+    xi[ax] = (face & 1) ? xi[ax] - sml[6 * i + face] : xi[ax] + sml[6 * i + face];
+  }
   const int64_t p0 = rowptr[i], p1 = rowptr[i + 1];
   double M[10], Mx[10], My[10], Mz[10], psum = 0.0;
 #pragma unroll
@@ -192,7 +197,7 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
     const double CX = BX[0] * H[0] + BX[1] * H[1] + BX[2] * H[2] + BX[3] * H[3] + B[1];
     const double CY = BY[0] * H[0] + BY[1] * H[1] + BY[2] * H[2] + BY[3] * H[3] + B[2];
     const double CZ = BZ[0] * H[0] + BZ[1] * H[1] + BZ[2] * H[2] + BZ[3] * H[3] + B[3];
-    shp[p] = C * e.phi;
+    if (shp) shp[p] = C * e.phi;
     gx[p] = CX * e.phi + C * e.px;
     gy[p] = CY * e.phi + C * e.py;
     gz[p] = CZ * e.phi + C * e.pz;
@@ -208,7 +213,19 @@ int rk_shapes(cudaStream_t s, const mega_params& p, int32_t n, const double* coo
   const int block = 128;
   const unsigned grid = (unsigned)(((int64_t)n * kLPN + block - 1) / block);
   k_rk_shapes<<<grid, block, 0, s>>>(n, coo, win, ebc_nodes, csr.rowptr, csr.col, p.ql, p.ql_coef, p.ql_len,
-                                     p.shsup, shp, gx, gy, gz, status);
+                                     p.shsup, nullptr, -1, shp, gx, gy, gz, status);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int rk_grad_at_face(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
+                    const int32_t* ebc_nodes, const DevCSR& csr, const double* sml, int face, double* gx, double* gy,
+                    double* gz, unsigned* status) {
+  if (p.rk_degree != 1 || p.rk_cont != 3) return MEGA_ERR_UNSUPPORTED;
+  const int block = 128;
+  const unsigned grid = (unsigned)(((int64_t)n * kLPN + block - 1) / block);
+  k_rk_shapes<<<grid, block, 0, s>>>(n, coo, win, ebc_nodes, csr.rowptr, csr.col, p.ql, p.ql_coef, p.ql_len,
+                                     p.shsup, sml, face, nullptr, gx, gy, gz, status);
   MEGA_CHECK_LAUNCH();
   return 0;
 }

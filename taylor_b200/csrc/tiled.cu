@@ -484,7 +484,8 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
     }
     if (q < 3) {
       const int64_t m = 3 * J + q;
-      const double fi = (double)(q == 0 ? f0 : (q == 1 ? f1 : f2));
+      double fi = (double)(q == 0 ? f0 : (q == 1 ? f1 : f2));
+      if (a.fadd) fi += a.fadd[m];
       double fe = (q == 0 ? e0 : (q == 1 ? e1 : e2));
       if (!isfinite(fi)) st |= MEGA_ST_NONFINITE;
       const double mass = a.mass[m];

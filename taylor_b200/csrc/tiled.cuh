@@ -41,6 +41,7 @@ struct TiledForceArgs {
   double* dsp;
   double* dsp_tot;
   double* prforce;
+  const double* fadd;     // 3 per node added to the internal force (NSNI), or null
   double dt;
   StepAccum* acc;
   unsigned* status;

@@ -296,7 +296,7 @@ class Mega:
                                               ptr(loss)), "train_surrogate")
         return th, loss
 
-    _SIZES = {0: 3, 1: 3, 2: 3, 3: 3, 4: 3, 5: 3, 6: 3, 7: 6, 8: 6, 9: 1, 10: 1, 11: 1, 12: 3, 13: 3, 14: 1, 15: 4}
+    _SIZES = {0: 3, 1: 3, 2: 3, 3: 3, 4: 3, 5: 3, 6: 3, 7: 6, 8: 6, 9: 1, 10: 1, 11: 1, 12: 3, 13: 3, 14: 1, 15: 4, 16: 18}
 
     def download(self, field):
         k = self._SIZES[field]

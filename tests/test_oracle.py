@@ -284,3 +284,79 @@ def test_pmb_forces_are_pairwise_balanced():
     u2[0::3] += 1e-2 * c["coo"][:, 0]
     f2, nbk2 = O.pmb_force(c, nb, u2, broken)
     assert nbk2 > 0 and nbk2 % 2 == 0
+
+
+# ---------------------------------------------------------------- NSNI
+def _nsni_run(h=0.8e-3, **kw):
+    c = cases.taylor_bar(h=h, **kw)
+    p = cases.param_kwargs(c, itype_int=2, ql=0)
+    return c, O.Run(c, O.params(**p), nthreads=4)
+
+
+def test_nsni_second_derivatives_reproduce_quadratics():
+    """The smoothed second derivatives (gradient differences over each
+    node's smoothing cell) annihilate constants and linear fields and return
+    the curvature of quadratic fields at interior nodes."""
+    c, r = _nsni_run(h=0.5e-3)
+    nb, dd = r.nb, r.ddshp.reshape(-1, 6)
+    rows = np.repeat(np.arange(c["n"]), nb["gn"])
+    cols = nb["gstack"] - 1
+    x = c["coo"]
+
+    def apply(f):
+        out = np.zeros((c["n"], 6))
+        np.add.at(out, rows, dd * f[cols][:, None])
+        return out
+
+    rad = np.hypot(x[:, 0], x[:, 1])
+    inner = (rad < c["R"] - 2.5 * c["h"]) & (x[:, 2] > 2.5 * c["h"]) & (x[:, 2] < c["L"] - 2.5 * c["h"])
+    assert inner.sum() > 100
+    assert np.abs(apply(np.ones(c["n"]))[inner]).max() < 1e-6 / c["h"] ** 2
+    assert np.abs(apply(x[:, 0] - x[:, 0].mean())[inner]).max() < 1e-6 / c["h"]
+    q = apply((x[:, 0] - 1e-3) ** 2)[inner]   # d2/dx2 = 2, the rest 0
+    assert abs(np.median(q[:, 0]) - 2.0) < 0.02 and np.percentile(np.abs(q[:, 0] - 2.0), 99) < 0.15
+    assert np.percentile(np.abs(q[:, 1:]), 99) < 0.15
+    q = apply(x[:, 0] * x[:, 1])[inner]       # XY entry (order XX YY ZZ XY YZ XZ) = 1
+    assert abs(np.median(q[:, 3]) - 1.0) < 0.02
+
+
+def test_nsni_adds_nothing_for_a_linear_field():
+    """A linear displacement increment has no strain gradient: the stress
+    gradients stay zero and NSNI's force equals DNI's on the same lists."""
+    c, r = _nsni_run()
+    n = c["n"]
+    rng = np.random.default_rng(4)
+    A = rng.normal(scale=1e-4, size=(3, 3))
+    du = (c["coo"] @ A.T).ravel()
+    p2 = O.params(**cases.param_kwargs(c, itype_int=2, ql=0))
+    p0 = O.params(**cases.param_kwargs(c, itype_int=0, ql=0))
+    sg = np.zeros((n, 18))
+    res = []
+    for p, kw in ((p2, dict(ddshp=r.ddshp, sgrad=sg)), (p0, {})):
+        st, s6, e6 = np.zeros((n, 20)), np.zeros((n, 6)), np.zeros((n, 6))
+        res.append(O.construct_fint(p, c, st, s6, e6, du, du, r.nb, r.shp, r.dshp, False, 1e-8, **kw))
+    rad = np.hypot(c["coo"][:, 0], c["coo"][:, 1])
+    inner = (rad < c["R"] - 2.5 * c["h"]) & (c["coo"][:, 2] > 2.5 * c["h"]) & (c["coo"][:, 2] < c["L"] - 2.5 * c["h"])
+    assert np.abs(sg[inner]).max() <= 1e-6 * np.abs(sg).max() + 1.0   # interior: no gradient
+    f2, f0 = res[0]["fint"], res[1]["fint"]
+    assert np.linalg.norm(f2 - f0) <= 1e-3 * np.linalg.norm(f0)
+
+
+def test_nsni_damps_the_spurious_velocity_spikes_of_dni():
+    """On the jittered 0.8 mm bar DNI's low-energy modes throw nodes faster
+    than the impact speed; with NSNI the peak speed stays near it."""
+    peaks = {}
+    for itype in (0, 2):
+        c = cases.taylor_bar(h=0.8e-3)
+        p = O.params(**cases.param_kwargs(c, itype_int=itype, ql=0))
+        r = O.Run(c, p, nthreads=4)
+        nb = O.bin_search(c["coo"], c["win"], c["sm_len"], c["dist_max"])
+        dt = cases.stable_dt(c, nb["gn"], nb["gstart"], nb["gstack"])
+        peak = 0.0
+        for _ in range(20):
+            assert r.step(20, dt) == 0
+            peak = max(peak, np.abs(r.vel).max())
+        assert np.all(np.isfinite(r.coo_cur))
+        peaks[itype] = peak / c["v0"]
+    assert peaks[0] > 1.4, peaks
+    assert peaks[2] < 1.25, peaks
