@@ -10,6 +10,7 @@
 #include <map>
 #include <mutex>
 #include <set>
+#include <thread>
 #include <vector>
 #include "mega_internal.cuh"
 #include "tiled.cuh"
@@ -103,6 +104,11 @@ __global__ void k_iperm(int32_t n, const int32_t* __restrict__ perm, int32_t* __
   if (r < n) iperm[perm[r]] = (int32_t)r;
 }
 // dst[r*w + k] = src[perm[r]*w + k]  (gather = old -> new), element size es bytes
+__global__ void k_add_kernel(int64_t m, const double* __restrict__ a, const double* __restrict__ b,
+                             double* __restrict__ out) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < m) out[k] = a[k] + b[k];
+}
 __global__ void k_perm_gather(int32_t n, int w, int es, const int32_t* __restrict__ perm,
                               const unsigned char* __restrict__ src, unsigned char* __restrict__ dst) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -149,6 +155,51 @@ __global__ void k_rowsum_pk32(int32_t n, const int64_t* __restrict__ rowptr, con
 
 inline unsigned grid_for(int64_t work, int block) { return (unsigned)((work + block - 1) / block); }
 
+// fn(lo, hi) over [0, n) in contiguous chunks on the host's cores (the
+// per-node set-up scans of a million-node model)
+template <typename F>
+void host_parallel(int64_t n, F fn) {
+  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(16, (int64_t)std::thread::hardware_concurrency()),
+                                                             n / 65536));
+  if (nt == 1) { fn((int64_t)0, n); return; }
+  std::vector<std::thread> th;
+  for (int64_t t = 0; t < nt; ++t) th.emplace_back(fn, n * t / nt, n * (t + 1) / nt);
+  for (auto& x : th) x.join();
+}
+
+// Deduplication of PROPS(30,N) and the material type into a table of
+// entries and a per-node index.  Rows equal to their predecessor (the usual
+// case: materials come in blocks) reuse its entry; that comparison runs in
+// parallel, the table lookups of the remaining rows serially.
+static int material_table(int32_t n, const double* props, const int32_t* mat_type, size_t cap,
+                          std::vector<MatEntry>& ents, std::vector<uint16_t>& idx, bool& damaged) {
+  std::vector<uint8_t> same(n, 0);
+  host_parallel(n, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = std::max<int64_t>(lo, 1); i < hi; ++i)
+      same[i] = mat_type[i] == mat_type[i - 1] &&
+                std::memcmp(props + 30 * (size_t)i, props + 30 * (size_t)(i - 1), 30 * sizeof(double)) == 0;
+  });
+  std::map<std::vector<double>, uint16_t> tab;
+  idx.assign(n, 0);
+  ents.clear();
+  damaged = false;
+  for (int32_t i = 0; i < n; ++i) {
+    if (same[i]) { idx[i] = idx[i - 1]; continue; }
+    std::vector<double> key(props + 30 * (size_t)i, props + 30 * (size_t)i + 30);
+    key.push_back((double)mat_type[i]);
+    auto it = tab.find(key);
+    if (it == tab.end()) {
+      if (ents.size() >= cap) return MEGA_ERR_UNSUPPORTED;
+      const MatEntry e = mat_entry(mat_type[i], props + 30 * (size_t)i);
+      damaged = damaged || damaged_type(e.type);
+      it = tab.emplace(key, (uint16_t)ents.size()).first;
+      ents.push_back(e);
+    }
+    idx[i] = it->second;
+  }
+  return 0;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- context
@@ -186,6 +237,7 @@ struct Ctx {
   // stress gradients (18 per node) and per-step scratch
   bool nsni = false;
   NsniS nsr{}, nsc{};
+  NsniSF nsr32{}, nsc32{};  // float copies for the mixed steps
   double *sgrad = nullptr, *hq = nullptr, *nsw = nullptr, *fstab = nullptr, *stress_prev = nullptr;
   StepAccum* acc = nullptr;
   unsigned* status = nullptr;
@@ -323,11 +375,13 @@ static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) 
                                c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc,
                                c->var_defgrad[mixed]);
   if (r) return r;
-  if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->dsp, 0))) return r;
+  if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->nsr32, c->nsc32, mixed, c->dsp, 0)))
+    return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[1], c->s));
   r = launch_stress(c->s, mixed, stress_args(c, dt, mode));
   if (r) return r;
-  if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->dsp, 1))) return r;
+  if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->nsr32, c->nsc32, mixed, c->dsp, 1)))
+    return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[2], c->s));
   r = launch_force_tiled(c->s, mixed, force_args(c, dt, mode, predict), c->var_force[mixed]);
   if (r) return r;
@@ -386,35 +440,9 @@ static int run_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
   return 0;
 }
 
-// Host-side deduplication of PROPS(30,N) into a small table.
-static int build_materials(Ctx* c, const double* props, const int32_t* mat_type) {
-  std::map<std::vector<double>, uint16_t> tab;
-  std::vector<uint16_t> idx(c->n);
-  std::vector<MatEntry> ents;
-  bool damaged = false;
-  int64_t prev = -1;
-  for (int32_t i = 0; i < c->n; ++i) {
-    // fast path: same PROPS row and type as the previous node
-    if (prev >= 0 && mat_type[i] == mat_type[prev] &&
-        std::memcmp(props + 30 * (size_t)i, props + 30 * (size_t)prev, 30 * sizeof(double)) == 0) {
-      idx[i] = idx[prev];
-      prev = i;
-      continue;
-    }
-    prev = i;
-    std::vector<double> key(props + 30 * (size_t)i, props + 30 * (size_t)i + 30);
-    key.push_back((double)mat_type[i]);
-    auto it = tab.find(key);
-    if (it == tab.end()) {
-      if (ents.size() >= 65535) return MEGA_ERR_UNSUPPORTED;
-      const MatEntry e = mat_entry(mat_type[i], props + 30 * (size_t)i);
-      damaged = damaged || damaged_type(e.type);
-      uint16_t id = (uint16_t)ents.size();
-      ents.push_back(e);
-      it = tab.emplace(key, id).first;
-    }
-    idx[i] = it->second;
-  }
+// The deduplicated PROPS(30,N) table and per-node index onto the device.
+static int install_materials(Ctx* c, const std::vector<MatEntry>& ents, const std::vector<uint16_t>& idx,
+                             bool damaged) {
   MEGA_ALLOC(c->pool, c->matidx, c->n);
   MEGA_ALLOC(c->pool, c->mats, ents.size());
   if (damaged) {  // STATE(1, 2, 4, 5) start at zero (STATE_INIT.f90)
@@ -584,7 +612,8 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   c->mlppool.bind(c->s);
   PhaseTrace tr(c->s, "gpu_init");
 #define CA(ptr, cnt) do { if (c->pool.alloc(&(ptr), (size_t)(cnt))) return fail(MEGA_ERR_NOMEM); } while (0)
-  CA(c->coo, n3); CA(c->win, n3); CA(c->vol, n); CA(c->mass, n3); CA(c->sm_len, 6 * (int64_t)n);
+  CA(c->coo, n3); CA(c->win, n3); CA(c->vol, n); CA(c->mass, n3);
+  if (p->itype_int != 0) CA(c->sm_len, 6 * (int64_t)n);  // DNI never reads the smoothing cells
   CA(c->ebc, n3); CA(c->body_id, n); CA(c->ebc_nodes, n);
   CA(c->dsp, n3); CA(c->dsp_tot, n3); CA(c->dsp_tot_phy, n3); CA(c->vel, n3); CA(c->acl, n3);
   CA(c->fint, n3); CA(c->fext, n3); CA(c->prforce, n3); CA(c->scratch3, n3);
@@ -612,23 +641,35 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   }
 #undef CA
   tr.mark("allocate");
+  // the material table is built on another host thread while this one
+  // converts the fixity and copies the node arrays (pageable copies hold
+  // the calling thread)
+  std::vector<uint16_t> midx;
+  std::vector<MatEntry> ments;
+  bool mdamaged = false;
+  int mres = 0;
+  std::thread mt([&] { mres = material_table(n, props, mat_type, 65535, ments, midx, mdamaged); });
   std::vector<int8_t> hebc(n3), hbody(n);
   std::vector<int32_t> hen(n, 0);
   std::vector<double> v0(n3);
-  for (int32_t i = 0; i < n; ++i) {
-    hbody[i] = (int8_t)(body_id ? body_id[i] : 1);
-    for (int j = 0; j < 3; ++j) {
-      const int64_t m = 3 * (int64_t)i + j;
-      hebc[m] = (int8_t)ebc[m];
-      if (ebc[m] == 1) { v0[m] = 0.0; hen[i] = 1; }  // STATE_INIT.f90:97-105
-      else v0[m] = vinit[m];
+  host_parallel(n, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi; ++i) {
+      hbody[i] = (int8_t)(body_id ? body_id[i] : 1);
+      for (int j = 0; j < 3; ++j) {
+        const int64_t m = 3 * i + j;
+        hebc[m] = (int8_t)ebc[m];
+        if (ebc[m] == 1) { v0[m] = 0.0; hen[i] = 1; }  // STATE_INIT.f90:97-105
+        else v0[m] = vinit[m];
+      }
     }
-  }
-  if (upload(c->s, c->coo, coo, n3) || upload(c->s, c->win, win, n3) || upload(c->s, c->vol, vol, n) ||
-      upload(c->s, c->mass, mass, n3) || upload(c->s, c->sm_len, sm_len, 6 * (size_t)n) ||
+  });
+  const bool up_fail =
+      upload(c->s, c->coo, coo, n3) || upload(c->s, c->win, win, n3) || upload(c->s, c->vol, vol, n) ||
+      upload(c->s, c->mass, mass, n3) || (c->sm_len && upload(c->s, c->sm_len, sm_len, 6 * (size_t)n)) ||
       upload(c->s, c->ebc, hebc.data(), n3) || upload(c->s, c->body_id, hbody.data(), n) ||
-      upload(c->s, c->ebc_nodes, hen.data(), n) || upload(c->s, c->vel, v0.data(), n3))
-    return fail(MEGA_ERR_CUDA);
+      upload(c->s, c->ebc_nodes, hen.data(), n) || upload(c->s, c->vel, v0.data(), n3);
+  mt.join();
+  if (up_fail) return fail(MEGA_ERR_CUDA);
   cudaMemsetAsync(c->dsp, 0, sizeof(double) * n3, c->s);
   cudaMemsetAsync(c->dsp_tot, 0, sizeof(double) * n3, c->s);
   cudaMemsetAsync(c->dsp_tot_phy, 0, sizeof(double) * n3, c->s);
@@ -646,7 +687,7 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   cudaMemsetAsync(c->tmat, 0, sizeof(double) * 12 * n, c->s);
   if (cudaStreamSynchronize(c->s) != cudaSuccess) return fail(MEGA_ERR_CUDA);
   tr.mark("upload");
-  r = build_materials(c, props, mat_type);
+  r = mres ? mres : install_materials(c, ments, midx, mdamaged);
   if (r) return fail(r);
   tr.mark("materials");
   {
@@ -679,7 +720,8 @@ static int search_instances(Ctx* c, DevCSR& csr, DevPool& out) {
   for (int k = 0; k < K; ++k) {
     const int32_t o = c->inst_off[k], nk = c->inst_off[k + 1] - o;
     const double* dmax = c->inst_dmax.empty() ? c->p.dist_max : c->inst_dmax.data() + 3 * k;
-    int r = bin_search(c->s, nk, c->coo + 3 * (int64_t)o, c->win + 3 * (int64_t)o, c->sm_len + 6 * (int64_t)o,
+    int r = bin_search(c->s, nk, c->coo + 3 * (int64_t)o, c->win + 3 * (int64_t)o,
+                       c->sm_len ? c->sm_len + 6 * (int64_t)o : nullptr,
                        dmax, c->p.itype_int, c->p.shsup, c->status, parts[k], nullptr, parts_pool, nullptr,
                        c->perm + o);
     if (r) return r;
@@ -870,6 +912,13 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     for (int k = 0; k < 6; ++k)
       k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->csr.tpos, c->nsr.v[k], c->nsc.v[k]);
     MEGA_CHECK_LAUNCH();
+    if (c->prec_mask & 2) {
+      for (int k = 0; k < 6; ++k) {
+        MEGA_ALLOC(c->nbpool, c->nsr32.v[k], m);
+        MEGA_ALLOC(c->nbpool, c->nsc32.v[k], m);
+      }
+      if ((r = nsni_to_float(c->s, m, c->nsr, c->nsr32)) || (r = nsni_to_float(c->s, m, c->nsc, c->nsc32))) return r;
+    }
   }
   tr.mark("transpose");
   r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->rt, c->nbpool, nullptr);
@@ -1054,15 +1103,15 @@ int mega_download(int64_t h, int32_t field, double* dst) {
         if (r) return r;
         phy = c->scratch3;
       }
-      int r = download_nodes(c, phy, 3, 8, dst);
-      if (r) return r;
-      if (field == MEGA_F_COO_CURRENT) {
-        std::vector<double> x(n3);
-        r = download_nodes(c, c->coo, 3, 8, x.data());
-        if (r) return r;
-        for (int64_t k = 0; k < n3; ++k) dst[k] = x[k] + dst[k];  // MAIN.F90:382-386
+      if (field == MEGA_F_COO_CURRENT) {  // x = X + the physical displacement (MAIN.F90:382-386), one copy out
+        DevPool tp(c->s);
+        double* x = nullptr;
+        MEGA_ALLOC(tp, x, n3);
+        k_add_kernel<<<grid_for(n3, 256), 256, 0, c->s>>>(n3, c->coo, phy, x);
+        MEGA_CHECK_LAUNCH();
+        return download_nodes(c, x, 3, 8, dst);
       }
-      return 0;
+      return download_nodes(c, phy, 3, 8, dst);
     }
     default: return MEGA_ERR_ARG;
   }
@@ -1563,23 +1612,10 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   }
   if (gebc_nodes) { MEGA_ALLOC(pool, den, n); if ((r = upload(s, den, gebc_nodes, (size_t)n))) return r; }
   // material table (per call)
-  std::map<std::vector<double>, uint16_t> tab;
-  std::vector<uint16_t> hidx(n);
+  std::vector<uint16_t> hidx;
   std::vector<MatEntry> ents;
   bool damaged = false;
-  for (int32_t i = 0; i < n; ++i) {
-    std::vector<double> key(gprop + 30 * (size_t)i, gprop + 30 * (size_t)i + 30);
-    key.push_back(gmat_type[i]);
-    auto it = tab.find(key);
-    if (it == tab.end()) {
-      if (ents.size() >= 65535) return MEGA_ERR_UNSUPPORTED;
-      const MatEntry e = mat_entry(gmat_type[i], gprop + 30 * (size_t)i);
-      damaged = damaged || damaged_type(e.type);
-      it = tab.emplace(key, (uint16_t)ents.size()).first;
-      ents.push_back(e);
-    }
-    hidx[i] = it->second;
-  }
+  if ((r = material_table(n, gprop, gmat_type, 65535, ents, hidx, damaged))) return r;
   MatEntry* dmat;
   MEGA_ALLOC(pool, dmat, ents.size());
   std::vector<double> hs(n), hsig(6 * (size_t)n), heps(6 * (size_t)n), hax;

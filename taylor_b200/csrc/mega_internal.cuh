@@ -232,9 +232,15 @@ int launch_defgrad(cudaStream_t s, bool mixed, bool interp, int32_t n, const Dev
 int launch_stress(cudaStream_t s, bool mixed, const StressArgs& a);
 
 // ---------------- NSNI (nsni.cu)
-struct NsniS {
-  double* v[6];  // smoothed second derivatives per list entry: XX, YY, ZZ, XY, YZ, XZ
+// smoothed second derivatives per list entry, one array per component:
+// XX, YY, ZZ, XY, YZ, XZ (double for the set-up and FP64 steps, float for
+// the mixed steps)
+template <typename V>
+struct NsniArr {
+  V* v[6];
 };
+using NsniS = NsniArr<double>;
+using NsniSF = NsniArr<float>;
 struct NsniStepArgs {
   int32_t n;
   const double* fg;          // F, G0 of this step
@@ -246,7 +252,7 @@ struct NsniStepArgs {
   const MatEntry* mats;
   double* hq;                // 18 per node: sum_J S_q du_J,k
   double* sgrad;             // 18 per node: sigma_,x, sigma_,y, sigma_,z (Voigt)
-  double* w;                 // 18 per node: force weights on the six S components
+  void* w;                   // 18 per node: force weights on the six S components (double, or float when mixed)
   double* fstab;             // 3 per node: the stabilisation force
   int finite_strain;
   int inv3_exact;
@@ -256,9 +262,11 @@ struct NsniStepArgs {
 int nsni_combine(cudaStream_t s, int32_t n, int axis, const int64_t* rowptr, const double* sml, const double* gp[3],
                  const double* gm[3], const NsniS& out);
 // stage 0: the row gather of H (after the displacement increment is known);
-// stage 1: stress gradients, weights and the column gather of the force
+// stage 1: stress gradients, weights and the column gather of the force.
+// mixed: float second derivatives (rows32 / cols32) and float weights.
 int nsni_step(cudaStream_t s, const NsniStepArgs& a, const DevCSR& csr, const NsniS& rows, const NsniS& cols,
-              const double* du, int stage);
+              const NsniSF& rows32, const NsniSF& cols32, bool mixed, const double* du, int stage);
+int nsni_to_float(cudaStream_t s, int64_t m, const NsniS& src, const NsniSF& dst);
 
 // surrogate network of the rate-dependent return mapping (mlp.cu)
 int mlp_nparams();

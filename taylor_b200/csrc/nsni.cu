@@ -1,5 +1,5 @@
 // nsni.cu -- naturally stabilised nodal integration (ITYPE_INT = 2) on the
-// resident path, FP64 in both precision modes.
+// resident path.
 //
 // The reference lays NSNI out but never finishes it (FINT.F90:441-576,
 // 707-753, 1120-1222 are commented out or read arrays nothing fills), so
@@ -9,7 +9,9 @@
 //            at the six faces x +- SM_LEN of the node's smoothing cell,
 //            differenced over the cell width (FINT.F90:446-535), order
 //            XX, YY, ZZ, XY, YZ, XZ (SHPDD_SM);
-//   per step k_nsni_h      (row gather) the gradients of the incremental
+//   per step (double arithmetic; S and the force weights stored as float in
+//            mixed mode)
+//            k_nsni_h      (row gather) the gradients of the incremental
 //            displacement gradient, H_a(k,m) = sum_J S_(m a)(J) du_J,k
 //            (XLMAT/YLMAT/ZLMAT, FINT.F90:728-737);
 //            k_nsni_stress (node) the strain-gradient increments of
@@ -67,9 +69,10 @@ __global__ void k_nsni_combine(int32_t n, int a, const int64_t* __restrict__ row
   }
 }
 
-// hq[18 i + 6 k + q] = sum_J S_q(J) du_J,k
+// hq[18 i + 6 k + q] = sum_J S_q(J) du_J,k (S double or float, sums in double)
+template <typename SV>
 __global__ void __launch_bounds__(256) k_nsni_h(int32_t n, const int64_t* __restrict__ rowptr,
-                                                const int32_t* __restrict__ col, NsniS s,
+                                                const int32_t* __restrict__ col, NsniArr<SV> s,
                                                 const double* __restrict__ du, double* __restrict__ hq) {
   const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kNL;
   const int q = threadIdx.x & (kNL - 1);
@@ -83,7 +86,7 @@ __global__ void __launch_bounds__(256) k_nsni_h(int32_t n, const int64_t* __rest
     const double u0 = du[3 * j], u1 = du[3 * j + 1], u2 = du[3 * j + 2];
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
-      const double sv = s.v[c][p];
+      const double sv = (double)s.v[c][p];
       h[c] += sv * u0;
       h[6 + c] += sv * u1;
       h[12 + c] += sv * u2;
@@ -142,6 +145,7 @@ __device__ __forceinline__ void estimate_moduli_nsni(const double sinc[6], const
   if (nes > 1.0e-8 && nss > 1.0e-8) bulk = fmin(nss / nes / 3.0, bulk);
 }
 
+template <typename WV>
 __global__ void __launch_bounds__(128) k_nsni_stress(NsniStepArgs a) {
   __shared__ double red[4];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -231,15 +235,15 @@ __global__ void __launch_bounds__(128) k_nsni_stress(NsniStepArgs a) {
           Wm[ax][k][m] = fac * vol * det * (S[k][0] * IF[m][0] + S[k][1] * IF[m][1] + S[k][2] * IF[m][2]);
     }
     // the weights folded onto the six symmetric second derivatives
-    double* w = a.w + 18 * i;
+    WV* w = reinterpret_cast<WV*>(a.w) + 18 * i;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      w[6 * k + 0] = Wm[0][k][0];
-      w[6 * k + 1] = Wm[1][k][1];
-      w[6 * k + 2] = Wm[2][k][2];
-      w[6 * k + 3] = Wm[1][k][0] + Wm[0][k][1];  // XY
-      w[6 * k + 4] = Wm[2][k][1] + Wm[1][k][2];  // YZ
-      w[6 * k + 5] = Wm[2][k][0] + Wm[0][k][2];  // XZ
+      w[6 * k + 0] = (WV)Wm[0][k][0];
+      w[6 * k + 1] = (WV)Wm[1][k][1];
+      w[6 * k + 2] = (WV)Wm[2][k][2];
+      w[6 * k + 3] = (WV)(Wm[1][k][0] + Wm[0][k][1]);  // XY
+      w[6 * k + 4] = (WV)(Wm[2][k][1] + Wm[1][k][2]);  // YZ
+      w[6 * k + 5] = (WV)(Wm[2][k][0] + Wm[0][k][2]);  // XZ
     }
     if (st) atomicOr(a.status, st);
   }
@@ -253,20 +257,22 @@ __global__ void __launch_bounds__(128) k_nsni_stress(NsniStepArgs a) {
   }
 }
 
-// fstab[3 J + k] = sum over the rows i holding J of sum_q W_i(k, q) S_q(i, J)
+// fstab[3 J + k] = sum over the rows i holding J of sum_q W_i(k, q) S_q(i, J);
+// V = the arithmetic and storage type of S and W (double or float)
+template <typename V>
 __global__ void __launch_bounds__(256) k_nsni_force(int32_t n, const int64_t* __restrict__ colptr,
-                                                    const int32_t* __restrict__ trow, NsniS st,
-                                                    const double* __restrict__ w, double* __restrict__ fstab) {
+                                                    const int32_t* __restrict__ trow, NsniArr<V> st,
+                                                    const V* __restrict__ w, double* __restrict__ fstab) {
   const int64_t J = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kNL;
   const int q = threadIdx.x & (kNL - 1);
   const unsigned gm = 0xFFu << (threadIdx.x & 24);
   if (J >= n) return;
-  double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+  V f0 = V(0), f1 = V(0), f2 = V(0);
   for (int64_t e = colptr[J] + q; e < colptr[J + 1]; e += kNL) {
-    const double* wi = w + 18 * (int64_t)trow[e];
+    const V* wi = w + 18 * (int64_t)trow[e];
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
-      const double sv = st.v[c][e];
+      const V sv = st.v[c][e];
       f0 += wi[c] * sv;
       f1 += wi[6 + c] * sv;
       f2 += wi[12 + c] * sv;
@@ -279,10 +285,17 @@ __global__ void __launch_bounds__(256) k_nsni_force(int32_t n, const int64_t* __
     f2 += __shfl_xor_sync(gm, f2, o);
   }
   if (q == 0) {
-    fstab[3 * J] = f0;
-    fstab[3 * J + 1] = f1;
-    fstab[3 * J + 2] = f2;
+    fstab[3 * J] = (double)f0;
+    fstab[3 * J + 1] = (double)f1;
+    fstab[3 * J + 2] = (double)f2;
   }
+}
+
+__global__ void k_nsni_narrow(int64_t m, NsniS src, NsniSF dst) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= m) return;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) dst.v[c][e] = (float)src.v[c][e];
 }
 
 }  // namespace
@@ -296,15 +309,27 @@ int nsni_combine(cudaStream_t s, int32_t n, int axis, const int64_t* rowptr, con
 }
 
 int nsni_step(cudaStream_t s, const NsniStepArgs& a, const DevCSR& csr, const NsniS& rows, const NsniS& cols,
-              const double* du, int stage) {
+              const NsniSF& rows32, const NsniSF& cols32, bool mixed, const double* du, int stage) {
   const unsigned gg = (unsigned)(((int64_t)a.n * kNL + 255) / 256);
+  const unsigned gn = (unsigned)((a.n + 127) / 128);
   if (stage == 0) {
-    k_nsni_h<<<gg, 256, 0, s>>>(a.n, csr.rowptr, csr.col, rows, du, a.hq);
-  } else {
-    k_nsni_stress<<<(unsigned)((a.n + 127) / 128), 128, 0, s>>>(a);
+    if (mixed) k_nsni_h<float><<<gg, 256, 0, s>>>(a.n, csr.rowptr, csr.col, rows32, du, a.hq);
+    else k_nsni_h<double><<<gg, 256, 0, s>>>(a.n, csr.rowptr, csr.col, rows, du, a.hq);
+  } else if (mixed) {
+    k_nsni_stress<float><<<gn, 128, 0, s>>>(a);
     MEGA_CHECK_LAUNCH();
-    k_nsni_force<<<gg, 256, 0, s>>>(a.n, csr.colptr, csr.trow, cols, a.w, a.fstab);
+    k_nsni_force<float><<<gg, 256, 0, s>>>(a.n, csr.colptr, csr.trow, cols32, (const float*)a.w, a.fstab);
+  } else {
+    k_nsni_stress<double><<<gn, 128, 0, s>>>(a);
+    MEGA_CHECK_LAUNCH();
+    k_nsni_force<double><<<gg, 256, 0, s>>>(a.n, csr.colptr, csr.trow, cols, (const double*)a.w, a.fstab);
   }
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int nsni_to_float(cudaStream_t s, int64_t m, const NsniS& src, const NsniSF& dst) {
+  k_nsni_narrow<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(m, src, dst);
   MEGA_CHECK_LAUNCH();
   return 0;
 }

@@ -166,9 +166,9 @@ __global__ void __launch_bounds__(256) k_soft_search(
   const int lane = threadIdx.x & 31;
   if (i >= n) return;  // whole warp leaves together
   const double xi[3] = {coo[3 * i], coo[3 * i + 1], coo[3 * i + 2]};
-  double sl[6];
+  double sl[6];  // smoothing cells: read only by the seven-point test (mmax = 7)
 #pragma unroll
-  for (int k = 0; k < 6; ++k) sl[k] = sm_len[6 * i + k];
+  for (int k = 0; k < 6; ++k) sl[k] = mmax > 1 ? sm_len[6 * i + k] : 0.0;
   const int32_t m0 = cell[i];
   const int32_t is = m0 % nx + 1, js = (m0 / nx) % ny + 1, ks = m0 / (nx * ny) + 1;
   // Lane k < 27 owns neighbour cell k in the reference's visiting order (IX
