@@ -140,6 +140,17 @@ __global__ void k_permute_rows(int32_t n, const int32_t* __restrict__ perm, cons
     w0[b0 + k] = v0[a0 + k]; w1[b0 + k] = v1[a0 + k]; w2[b0 + k] = v2[a0 + k]; w3[b0 + k] = v3[a0 + k];
   }
 }
+// the lists in the new numbering without values: rows in the new order, each
+// keeping its entries' order, columns renumbered
+__global__ void k_renumber_cols(int32_t n, const int32_t* __restrict__ perm, const int32_t* __restrict__ iperm,
+                                const int64_t* __restrict__ rowptr0, const int32_t* __restrict__ col0,
+                                const int64_t* __restrict__ rowptr1, int32_t* __restrict__ col1) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const int64_t a0 = rowptr0[perm[r]], len = rowptr0[perm[r] + 1] - a0, b0 = rowptr1[r];
+  for (int64_t k = lane; k < len; k += 32) col1[b0 + k] = iperm[col0[a0 + k]];
+}
 // row sums of the float-rounded packed gradients (the mixed path's sum_J g)
 __global__ void k_rowsum_pk32(int32_t n, const int64_t* __restrict__ rowptr, const float4* __restrict__ pk,
                               double* __restrict__ out) {
@@ -165,6 +176,78 @@ void host_parallel(int64_t n, F fn) {
   std::vector<std::thread> th;
   for (int64_t t = 0; t < nt; ++t) th.emplace_back(fn, n * t / nt, n * (t + 1) / nt);
   for (auto& x : th) x.join();
+}
+
+// Bulk host <-> device copies go through one pinned buffer kept for the
+// process: the host's cores copy the caller's (pageable) arrays into it and
+// each array moves with one DMA, instead of the driver staging pageable
+// memory on the calling thread.  One user at a time; a failed pinned
+// allocation falls back to plain pageable copies.
+struct PinnedStage {
+  std::mutex mu;
+  unsigned char* p = nullptr;
+  size_t cap = 0;
+};
+PinnedStage g_stage;
+
+void host_copy(void* dst, const void* src, size_t bytes) {
+  const int64_t chunks = (int64_t)((bytes + (1 << 20) - 1) >> 20);  // 1 MiB pieces
+  host_parallel(chunks, [&](int64_t lo, int64_t hi) {
+    for (int64_t k = lo; k < hi; ++k) {
+      const size_t a = (size_t)k << 20, b = std::min(bytes, (size_t)(k + 1) << 20);
+      std::memcpy((unsigned char*)dst + a, (const unsigned char*)src + a, b - a);
+    }
+  });
+}
+
+struct HostToDevice { void* dst; const void* src; size_t bytes; };
+
+// the copies in order on stream s, complete on return
+int upload_staged(cudaStream_t s, const std::vector<HostToDevice>& items) {
+  size_t total = 0;
+  for (const auto& it : items) total += (it.bytes + 255) & ~(size_t)255;
+  std::lock_guard<std::mutex> lk(g_stage.mu);
+  if (g_stage.cap < total) {
+    if (g_stage.p) cudaFreeHost(g_stage.p);
+    g_stage.p = nullptr;
+    g_stage.cap = 0;
+    if (cudaHostAlloc((void**)&g_stage.p, total, cudaHostAllocDefault) == cudaSuccess) g_stage.cap = total;
+    else { g_stage.p = nullptr; cudaGetLastError(); }
+  }
+  if (!g_stage.p) {
+    for (const auto& it : items) MEGA_TRY(cudaMemcpyAsync(it.dst, it.src, it.bytes, cudaMemcpyHostToDevice, s));
+    MEGA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  }
+  size_t off = 0;
+  for (const auto& it : items) {  // copy in, then DMA while the next array is copied in
+    host_copy(g_stage.p + off, it.src, it.bytes);
+    MEGA_TRY(cudaMemcpyAsync(it.dst, g_stage.p + off, it.bytes, cudaMemcpyHostToDevice, s));
+    off += (it.bytes + 255) & ~(size_t)255;
+  }
+  MEGA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// device -> host through the pinned buffer (stream s ordered, complete on return)
+int download_staged(cudaStream_t s, void* dst, const void* src, size_t bytes) {
+  std::lock_guard<std::mutex> lk(g_stage.mu);
+  if (g_stage.cap < bytes) {
+    if (g_stage.p) cudaFreeHost(g_stage.p);
+    g_stage.p = nullptr;
+    g_stage.cap = 0;
+    if (cudaHostAlloc((void**)&g_stage.p, bytes, cudaHostAllocDefault) == cudaSuccess) g_stage.cap = bytes;
+    else { g_stage.p = nullptr; cudaGetLastError(); }
+  }
+  if (!g_stage.p) {
+    MEGA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    MEGA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  }
+  MEGA_TRY(cudaMemcpyAsync(g_stage.p, src, bytes, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaStreamSynchronize(s));
+  host_copy(dst, g_stage.p, bytes);
+  return 0;
 }
 
 // Deduplication of PROPS(30,N) and the material type into a table of
@@ -663,11 +746,14 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
       }
     }
   });
-  const bool up_fail =
-      upload(c->s, c->coo, coo, n3) || upload(c->s, c->win, win, n3) || upload(c->s, c->vol, vol, n) ||
-      upload(c->s, c->mass, mass, n3) || (c->sm_len && upload(c->s, c->sm_len, sm_len, 6 * (size_t)n)) ||
-      upload(c->s, c->ebc, hebc.data(), n3) || upload(c->s, c->body_id, hbody.data(), n) ||
-      upload(c->s, c->ebc_nodes, hen.data(), n) || upload(c->s, c->vel, v0.data(), n3);
+  std::vector<HostToDevice> items = {
+      {c->coo, coo, 8 * (size_t)n3}, {c->win, win, 8 * (size_t)n3}, {c->vol, vol, 8 * (size_t)n},
+      {c->mass, mass, 8 * (size_t)n3}, {c->ebc, hebc.data(), (size_t)n3}, {c->body_id, hbody.data(), (size_t)n},
+      {c->ebc_nodes, hen.data(), 4 * (size_t)n}, {c->vel, v0.data(), 8 * (size_t)n3}};
+  if (c->sm_len) items.push_back({c->sm_len, sm_len, 48 * (size_t)n});
+  tr.mark("fixity");
+  const bool up_fail = upload_staged(c->s, items) != 0;
+  tr.mark("copies");
   mt.join();
   if (up_fail) return fail(MEGA_ERR_CUDA);
   cudaMemsetAsync(c->dsp, 0, sizeof(double) * n3, c->s);
@@ -807,35 +893,46 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   if (r) return r;
   tr.mark("bin_search");
   const int64_t m = csr0.nnz;
-  double *shp0, *g0x, *g0y, *g0z;
-  MEGA_ALLOC(tmp0, shp0, m);
-  MEGA_ALLOC(tmp0, g0x, m);
-  MEGA_ALLOC(tmp0, g0y, m);
-  MEGA_ALLOC(tmp0, g0z, m);
-  r = rk_shapes(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr0, shp0, g0x, g0y, g0z, c->status);
-  if (r) return r;
-  tr.mark("rk_shapes");
-  NsniS s0{};
-  if (c->nsni) {  // smoothed second derivatives, one axis (two faces) at a time
-    for (int k = 0; k < 6; ++k) MEGA_ALLOC(tmp0, s0.v[k], m);
+  // NSNI's smoothed second derivatives on the lists `csr` of the current
+  // node order, one axis (two faces) at a time
+  auto second_derivatives = [&](const DevCSR& csr, const NsniS& out) -> int {
     DevPool faces(c->s);
     double* g[6];
     for (int k = 0; k < 6; ++k) MEGA_ALLOC(faces, g[k], m);
     for (int ax = 0; ax < 3; ++ax) {
-      if ((r = rk_grad_at_face(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr0, c->sm_len, 2 * ax, g[0], g[1],
+      int q;
+      if ((q = rk_grad_at_face(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr, c->sm_len, 2 * ax, g[0], g[1],
                                g[2], c->status)) ||
-          (r = rk_grad_at_face(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr0, c->sm_len, 2 * ax + 1, g[3],
-                               g[4], g[5], c->status)))
-        return r;
+          (q = rk_grad_at_face(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr, c->sm_len, 2 * ax + 1, g[3], g[4],
+                               g[5], c->status)))
+        return q;
       const double* gp[3] = {g[0], g[1], g[2]};
       const double* gm[3] = {g[3], g[4], g[5]};
-      if ((r = nsni_combine(c->s, n, ax, csr0.rowptr, c->sm_len, gp, gm, s0))) return r;
+      if ((q = nsni_combine(c->s, n, ax, csr.rowptr, c->sm_len, gp, gm, out))) return q;
     }
     MEGA_TRY(cudaStreamSynchronize(c->s));
-    tr.mark("nsni_second_derivatives");
-  }
+    return 0;
+  };
+  // The shapes are computed in the caller's numbering only when the caller
+  // asks for the lists; otherwise directly on the renumbered lists (each row
+  // keeps its entries' order, so the values are the same to the bit).
+  const bool want = gn || gstart || gstack || shp || dshp;
+  double *shp0 = nullptr, *g0x = nullptr, *g0y = nullptr, *g0z = nullptr;
+  NsniS s0{};
   int st = 0;
-  if (gn || gstart || gstack || shp || dshp) {
+  if (want) {
+    MEGA_ALLOC(tmp0, shp0, m);
+    MEGA_ALLOC(tmp0, g0x, m);
+    MEGA_ALLOC(tmp0, g0y, m);
+    MEGA_ALLOC(tmp0, g0z, m);
+    r = rk_shapes(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, csr0, shp0, g0x, g0y, g0z, c->status);
+    if (r) return r;
+    tr.mark("rk_shapes");
+    if (c->nsni) {
+      for (int k = 0; k < 6; ++k) MEGA_ALLOC(tmp0, s0.v[k], m);
+      if ((r = second_derivatives(csr0, s0))) return r;
+      tr.mark("nsni_second_derivatives");
+    }
     std::vector<int64_t> rp(n + 1);
     MEGA_TRY(cudaMemcpyAsync(rp.data(), csr0.rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, c->s));
     MEGA_TRY(cudaStreamSynchronize(c->s));
@@ -861,8 +958,8 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
       for (int64_t k = 0; k < m; ++k) { dshp[3 * k] = a[k]; dshp[3 * k + 1] = b[k]; dshp[3 * k + 2] = d[k]; }
     }
     MEGA_TRY(cudaStreamSynchronize(c->s));
+    tr.mark("downloads");
   }
-  tr.mark("downloads");
   // 2. renumber the nodes in bin-cell order (spatially compact rows and tiles)
   k_iperm<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->perm, c->iperm);
   MEGA_CHECK_LAUNCH();
@@ -885,20 +982,34 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   MEGA_CHECK_LAUNCH();
   r = scan_counts(c->s, len1, c->csr.rowptr, n, tmp1);
   if (r) return r;
-  k_permute_rows<<<grid_for((int64_t)n * 32, 256), 256, 0, c->s>>>(n, c->perm, c->iperm, csr0.rowptr, csr0.col, shp0,
-                                                                    g0x, g0y, g0z, c->csr.rowptr, c->csr.col, c->shp,
-                                                                    g1x, g1y, g1z);
-  MEGA_CHECK_LAUNCH();
-  if (c->nsni) {
+  if (c->nsni)
     for (int k = 0; k < 6; ++k) {
       MEGA_ALLOC(c->nbpool, c->nsr.v[k], m);
       MEGA_ALLOC(c->nbpool, c->nsc.v[k], m);
     }
-    for (int k = 0; k < 6; k += 2)  // (the column indices are rewritten with the same values)
-      k_permute_rows<<<grid_for((int64_t)n * 32, 256), 256, 0, c->s>>>(
-          n, c->perm, c->iperm, csr0.rowptr, csr0.col, s0.v[k], s0.v[k + 1], s0.v[k], s0.v[k + 1], c->csr.rowptr,
-          c->csr.col, c->nsr.v[k], c->nsr.v[k + 1], c->nsr.v[k], c->nsr.v[k + 1]);
+  if (want) {
+    k_permute_rows<<<grid_for((int64_t)n * 32, 256), 256, 0, c->s>>>(n, c->perm, c->iperm, csr0.rowptr, csr0.col,
+                                                                      shp0, g0x, g0y, g0z, c->csr.rowptr, c->csr.col,
+                                                                      c->shp, g1x, g1y, g1z);
     MEGA_CHECK_LAUNCH();
+    if (c->nsni) {
+      for (int k = 0; k < 6; k += 2)  // (the column indices are rewritten with the same values)
+        k_permute_rows<<<grid_for((int64_t)n * 32, 256), 256, 0, c->s>>>(
+            n, c->perm, c->iperm, csr0.rowptr, csr0.col, s0.v[k], s0.v[k + 1], s0.v[k], s0.v[k + 1], c->csr.rowptr,
+            c->csr.col, c->nsr.v[k], c->nsr.v[k + 1], c->nsr.v[k], c->nsr.v[k + 1]);
+      MEGA_CHECK_LAUNCH();
+    }
+  } else {
+    k_renumber_cols<<<grid_for((int64_t)n * 32, 256), 256, 0, c->s>>>(n, c->perm, c->iperm, csr0.rowptr, csr0.col,
+                                                                       c->csr.rowptr, c->csr.col);
+    MEGA_CHECK_LAUNCH();
+    r = rk_shapes(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, c->csr, c->shp, g1x, g1y, g1z, c->status);
+    if (r) return r;
+    tr.mark("rk_shapes");
+    if (c->nsni) {
+      if ((r = second_derivatives(c->csr, c->nsr))) return r;
+      tr.mark("nsni_second_derivatives");
+    }
   }
   MEGA_TRY(cudaStreamSynchronize(c->s));
   tmp0.free_all();
@@ -1056,9 +1167,7 @@ static int download_nodes(Ctx* c, const void* src, int w, int es, void* dst) {
   MEGA_ALLOC(tp, tmp, bytes);
   k_perm_gather<<<grid_for((int64_t)n * w, 256), 256, 0, c->s>>>(n, w, es, c->iperm, (const unsigned char*)src, tmp);
   MEGA_CHECK_LAUNCH();
-  MEGA_TRY(cudaMemcpyAsync(dst, tmp, bytes, cudaMemcpyDeviceToHost, c->s));
-  MEGA_TRY(cudaStreamSynchronize(c->s));
-  return 0;
+  return download_staged(c->s, dst, tmp, bytes);
 }
 
 int mega_download(int64_t h, int32_t field, double* dst) {

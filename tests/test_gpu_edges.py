@@ -111,3 +111,22 @@ def test_list_buffer_too_small_is_reported():
     assert st > 0 and st & _lib.ST_STACK_OVERFLOW
     assert nnz.value > 10 and gn.sum() == nnz.value
     m.close()
+
+
+@pytest.mark.parametrize("itype", [0, 2])
+def test_shapes_on_renumbered_lists_equal_the_downloaded_path(itype):
+    """Without a list download the shapes (and NSNI's second derivatives) are
+    computed directly on the renumbered lists; the steps that follow are the
+    same to the bit as after the path that builds them in the caller's
+    numbering first."""
+    c = cases.taylor_bar(h=0.8e-3)
+    p = _lib.params(**cases.param_kwargs(c, itype_int=itype))
+    a, b = mega.Mega(c, p), mega.Mega(c, p)
+    a.search_and_shapes(download=True)
+    b.search_and_shapes(download=False)
+    a.step(30, 3e-8)
+    b.step(30, 3e-8)
+    for f in (_lib.F_COO_CURRENT, _lib.F_STRESS, _lib.F_EPS):
+        np.testing.assert_array_equal(a.download(f), b.download(f))
+    a.close()
+    b.close()
