@@ -122,7 +122,7 @@ typedef struct mega_params {
   int32_t rk_impl;         /* RK_IMPL; read, no effect on the live path        */
   int32_t itype_int;       /* ITYPE_INT; 0 = direct nodal integration, 2 = NSNI (resident contexts) */
   int32_t ql;              /* QL (logical): quasi-linear moment regularisation */
-  int32_t lagrangian;      /* LLAGRANGIAN (logical); only 1 is on this path    */
+  int32_t lagrangian;      /* LLAGRANGIAN (logical); 0 = semi-Lagrangian (resident, DNI, FP64) */
   int32_t finite_strain;   /* LFINITE_STRAIN (logical)                         */
   int32_t shsup;           /* SHSUP (logical): 1 = ellipsoidal support         */
   int32_t peridynamics;    /* PERIDYNAMICS (logical)                          */

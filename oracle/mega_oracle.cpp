@@ -695,7 +695,8 @@ extern "C" {
 int orc_bin_search(int n, const double* coo, const double* win, const double* sm_len,
                    const double* dist_max, int itype_int, int shsup, int* gn, int* gstart,
                    int* gstack, int64_t cap, int64_t* nnz_out, int* gmaxn, int* ijk,
-                   double* geom_out /* xmin,ymin,zmin,xbin,ybin,zbin,nx,ny,nz */) {
+                   double* geom_out /* xmin,ymin,zmin,xbin,ybin,zbin,nx,ny,nz */,
+                   const double* geom_in /* the same, kept from LINIT (semi-Lagrangian re-search) or null */) {
   if (n <= 0) return 0;
   double xbin = 0, ybin = 0, zbin = 0;
   double xmax = coo[0], ymax = coo[1], zmax = coo[2];
@@ -721,6 +722,11 @@ int orc_bin_search(int n, const double* coo, const double* win, const double* sm
   int nx = (int)std::ceil((xmax - xmin) / xbin);                      // :235-241
   int ny = (int)std::ceil((ymax - ymin) / ybin);
   int nz = (int)std::ceil((zmax - zmin) / zbin);
+  if (geom_in) {  // the bins of HANDELER.F90:181-250 are laid out at LINIT only
+    xmin = geom_in[0]; ymin = geom_in[1]; zmin = geom_in[2];
+    xbin = geom_in[3]; ybin = geom_in[4]; zbin = geom_in[5];
+    nx = (int)geom_in[6]; ny = (int)geom_in[7]; nz = (int)geom_in[8];
+  }
   if (geom_out) {
     geom_out[0] = xmin; geom_out[1] = ymin; geom_out[2] = zmin;
     geom_out[3] = xbin; geom_out[4] = ybin; geom_out[5] = zbin;
@@ -984,10 +990,16 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
                        const int* gstack, double* shp_stack, double* dshp_stack, int linit,
                        double dlt, double* fint, double* fext, double* gmax_wvel,
                        double* gstrain_eq, double* gint_work, int nthreads, int* newton_iters,
-                       const double* sm_len, double* ddshp, double* sgrad) {
+                       const double* sm_len, double* ddshp, double* sgrad, const double* gcoo_current) {
   const bool exact = p->inv3_exact != 0;
   const bool nsni = p->itype_int == 2;
+  // semi-Lagrangian (LLAGRANGIAN = .FALSE.): RK1 on the current coordinates
+  // every call (FINT.F90:410-436), gradients used as they are (no push-
+  // forward), DET left at its initial 1 (FINT.F90:230: only the Lagrangian
+  // branches set it)
+  const bool semi = p->lagrangian == 0;
   if (nsni && (!sm_len || !ddshp || !sgrad)) return -2;
+  if (semi && (!gcoo_current || nsni)) return -2;
   int status = 0;
   int nt = std::max(1, nthreads);
   std::vector<double> fint_t((size_t)nt * 3 * n, 0.0), fext_t((size_t)nt * 3 * n, 0.0);
@@ -1012,8 +1024,9 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
       for (int k = 0; k < 20; ++k) lstate[k] = gstate[20 * (size_t)i + k];
       shpd.resize(3 * (size_t)ln);
       shp0.resize(ln);
-      if (linit) {                                                    // FINT.F90:400-408, 580-587
-        if (!rk1(gcoo + 3 * (size_t)i, gcoo, gwin, nb.data(), ln, gebc_nodes, p->ql != 0, p->ql_coef,
+      if (linit || semi) {                                            // FINT.F90:400-436, 580-587
+        const double* xs = semi ? gcoo_current : gcoo;
+        if (!rk1(xs + 3 * (size_t)i, xs, gwin, nb.data(), ln, gebc_nodes, p->ql != 0, p->ql_coef,
                  p->ql_len, p->shsup != 0, shp_stack + s, dshp_stack + 3 * s, work))
           status |= MEGA_ST_SINGULAR_MOMENT;
         if (nsni && !nsni_second_derivatives(gcoo + 3 * (size_t)i, sm_len + 6 * (size_t)i, gcoo, gwin, nb.data(),
@@ -1026,7 +1039,7 @@ int orc_construct_fint(const mega_params* p, int n, const double* gcoo, const do
       }
       double det = 1.0;
       M3 fm, ifm_s = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}, L_s = {}, R_s = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-      if (p->finite_strain) {                                         // FINT.F90:361-391
+      if (p->finite_strain && !semi) {                                // FINT.F90:361-391
         for (int k = 0; k < 3; ++k)
           for (int l = 0; l < 3; ++l) {
             double v = (k == l) ? 1.0 : 0.0;
@@ -1444,7 +1457,8 @@ int orc_step(const mega_params* p, int n, const double* coo, const double* win, 
   std::vector<double> fext_nmo(fext, fext + n3);
   int st = orc_construct_fint(p, n, coo, win, vol, props, mat, ebc_nodes, bodyforce, state, stress,
                               strain, dsp, dsp_tot, gn, gstart, gstack, shp, dshp, 0, dlt, fint,
-                              fext, wvel, strain_eq, &en[3], nthreads, newton_iters, sm_len, ddshp, sgrad);
+                              fext, wvel, strain_eq, &en[3], nthreads, newton_iters, sm_len, ddshp, sgrad,
+                              nullptr);
   std::vector<double> p21(n);
   for (int i = 0; i < n; ++i) p21[i] = props[30 * (size_t)i + 20];
   orc_corrector(n, ebc, p21.data(), mass, fint, fext, vel, acl, prforce, body_id, total_force, dlt);

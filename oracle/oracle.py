@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "liboracle.so")
 P, I32, I64, D = C.c_void_p, C.c_int32, C.c_int64, C.c_double
 
 _SIG = {
-    "orc_bin_search": (I32, [I32, P, P, P, P, I32, I32, P, P, P, I64, P, P, P, P]),
+    "orc_bin_search": (I32, [I32, P, P, P, P, I32, I32, P, P, P, I64, P, P, P, P, P]),
     "orc_rk_shapes": (I32, [P, I32, P, P, P, P, P, P, P, P, I32]),
     "orc_hughes_winget": (None, [I32, P, P, P, P, I32]),
     "orc_rotate_tensor": (None, [I32, P, P]),
@@ -24,7 +24,7 @@ _SIG = {
     "orc_vm_rate": (I32, [I32, P, P, D, D, I32, P, P, P, P, P, I32]),
     "orc_damaged": (I32, [I32, P, P, P, P, P, P, P, I32]),
     "orc_construct_fint": (I32, [P, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, I32, D, P, P, P, P,
-                                 P, I32, P, P, P, P]),
+                                 P, I32, P, P, P, P, P]),
     "orc_interp": (None, [I32, P, P, P, P, P, P, I32]),
     "orc_pd_shape": (I32, [I32, P, P, P, P, P, P, P, P, I32]),
     "orc_construct_fint_pd": (I32, [P, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, I32, D, P, P, I32]),
@@ -70,7 +70,9 @@ def i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
 
-def bin_search(coo, win, sm_len, dist_max, itype_int=0, shsup=False):
+def bin_search(coo, win, sm_len, dist_max, itype_int=0, shsup=False, geom_in=None):
+    """BIN_SEARCH; geom_in (9 values, as returned in "geom") reuses the bins
+    laid out at LINIT, as the semi-Lagrangian re-search does."""
     coo, win, sm_len, dist_max = f64(coo), f64(win), f64(sm_len), f64(dist_max)
     n = len(coo)
     gn = np.zeros(n, np.int32)
@@ -84,7 +86,7 @@ def bin_search(coo, win, sm_len, dist_max, itype_int=0, shsup=False):
         gstack = np.zeros(cap, np.int32)
         st = lib().orc_bin_search(n, _p(coo), _p(win), _p(sm_len), _p(dist_max), int(itype_int), int(bool(shsup)),
                                   _p(gn), _p(gstart), _p(gstack), cap, C.byref(nnz), C.byref(gmaxn), _p(ijk),
-                                  _p(geom))
+                                  _p(geom), _p(None if geom_in is None else f64(geom_in)))
         if not (st & 0x40):
             break
         cap = int(nnz.value)
@@ -182,10 +184,11 @@ def vm_rate(spred, props, dt, state, dg0=None, rtol=1e-10, maxit=50, solver=0):
 
 
 def construct_fint(p, case, state, stress, strain, dinc, dinc_tot, nb, shp, dshp, linit, dlt, nthreads=1,
-                   gint_work=0.0, ddshp=None, sgrad=None):
+                   gint_work=0.0, ddshp=None, sgrad=None, coo_current=None):
     """CONSTRUCT_FINT; with p.itype_int == 2 (NSNI) ddshp (6 per list entry,
     built when linit) and sgrad (18 per node, the stress gradients) are
-    updated in place too."""
+    updated in place too; p.lagrangian == 0 (semi-Lagrangian) builds the
+    shapes on coo_current every call."""
     n = case["n"]
     fint = np.zeros(3 * n)
     fext = np.zeros(3 * n)
@@ -200,7 +203,8 @@ def construct_fint(p, case, state, stress, strain, dinc, dinc_tot, nb, shp, dshp
         _p(i32(case["mat_type"])), _p(en), _p(None if bf is None else f64(bf)), _p(state), _p(stress), _p(strain),
         _p(f64(dinc)), _p(f64(dinc_tot)), _p(i32(nb["gn"])), _p(i32(nb["gstart"])), _p(i32(nb["gstack"])), _p(shp),
         _p(dshp), int(bool(linit)), float(dlt), _p(fint), _p(fext), _p(wv), _p(seq), C.byref(gw), int(nthreads),
-        _p(it), _p(f64(case["sm_len"]) if ddshp is not None else None), _p(ddshp), _p(sgrad))
+        _p(it), _p(f64(case["sm_len"]) if ddshp is not None else None), _p(ddshp), _p(sgrad),
+        _p(None if coo_current is None else f64(coo_current)))
     return dict(fint=fint, fext=fext, gmax_wvel=wv, gstrain_eq=seq, gint_work=gw.value, iters=it, status=st)
 
 
@@ -213,7 +217,9 @@ class Run:
         self.n = n = case["n"]
         self.nthreads = nthreads
         self.serial_interp = serial_interp
+        self.semi = p.lagrangian == 0
         self.nb = bin_search(case["coo"], case["win"], case["sm_len"], case["dist_max"], p.itype_int, p.shsup)
+        self.geom = self.nb["geom"].copy()  # the LINIT bins (kept by the semi-Lagrangian re-search)
         nnz = self.nb["nnz"]
         self.shp = np.zeros(nnz)
         self.dshp = np.zeros(3 * nnz)
@@ -242,13 +248,55 @@ class Run:
         self.sgrad = np.zeros((n, 18)) if p.itype_int == 2 else None
         # LINIT: shapes + a force call at zero displacement (MAIN.F90:320-334)
         r = construct_fint(p, case, self.state, self.stress, self.strain, self.dsp, self.dsp_tot, self.nb,
-                           self.shp, self.dshp, True, 0.0, nthreads, ddshp=self.ddshp, sgrad=self.sgrad)
+                           self.shp, self.dshp, True, 0.0, nthreads, ddshp=self.ddshp, sgrad=self.sgrad,
+                           coo_current=self.coo_cur if self.semi else None)
         self.init_status = r["status"]
         self.en[3] = r["gint_work"]
+
+    def _semi_step(self, dt):
+        """MAIN.F90:348-488 with LLAGRANGIAN = .FALSE.: predictor, DO_INTERP
+        with the last lists and shapes, the current coordinates, a re-search
+        on them in the LINIT bins (HANDELER.F90:145, 252-273), CONSTRUCT_FINT
+        with shapes on the current coordinates, corrector, energies."""
+        c, n, p = self.case, self.n, self.p
+        dsp = dt * self.vel + dt * dt * 0.5 * self.acl                 # MAIN.F90:353-355
+        self.dsp[:] = dsp
+        self.dsp_tot += dsp
+        self.vel += dt * 0.5 * self.acl
+        dphy = np.zeros(3 * n)
+        nb = self.nb
+        lib().orc_interp(n, _p(nb["gn"]), _p(nb["gstart"]), _p(nb["gstack"]), _p(self.shp), _p(self.dsp), _p(dphy), 1)
+        self.dsp_tot_phy += dphy                                         # MAIN.F90:377-386
+        self.coo_cur[:] = f64(c["coo"]).reshape(-1) + self.dsp_tot_phy
+        self.nb = bin_search(self.coo_cur.reshape(-1, 3), c["win"], c["sm_len"], c["dist_max"], p.itype_int,
+                             p.shsup, geom_in=self.geom)
+        self.shp = np.zeros(self.nb["nnz"])
+        self.dshp = np.zeros(3 * self.nb["nnz"])
+        fext_nmo = self.fext.copy()
+        r = construct_fint(p, c, self.state, self.stress, self.strain, self.dsp, self.dsp_tot, self.nb, self.shp,
+                           self.dshp, False, dt, self.nthreads, gint_work=self.en[3], coo_current=self.coo_cur)
+        self.en[3] = r["gint_work"]
+        self.fint[:], self.fext[:] = r["fint"], r["fext"]
+        self.wvel[:], self.strain_eq[:], self.iters[:] = r["gmax_wvel"], r["gstrain_eq"], r["iters"]
+        p21 = np.ascontiguousarray(f64(c["props"])[:, 20])
+        lib().orc_corrector(n, _p(i32(c["ebc"])), _p(p21), _p(f64(c["mass"])), _p(self.fint), _p(self.fext),
+                            _p(self.vel), _p(self.acl), _p(self.prforce), _p(i32(c["body_id"])),
+                            _p(self.total_force), float(dt))
+        mass = f64(c["mass"]).reshape(-1)
+        self.en[0] = self.en[3]
+        self.en[1] = float(np.sum(0.5 * mass * self.vel * self.vel))
+        self.en[2] = self.en[2] + float(np.sum(0.5 * (self.fext + fext_nmo) * self.dsp))
+        return r["status"] | (self.nb["status"] & ~0x40)
 
     def step(self, nsteps, dt):
         c = self.case
         st = 0
+        if self.semi:
+            for _ in range(nsteps):
+                st |= self._semi_step(dt)
+                self.time += dt
+                self.steps += 1
+            return st
         en_ebc = i32(np.any(c["ebc"] == 1, axis=1))
         bf = c.get("bodyforce")
         for _ in range(nsteps):

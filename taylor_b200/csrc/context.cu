@@ -321,6 +321,16 @@ struct Ctx {
   bool nsni = false;
   NsniS nsr{}, nsc{};
   NsniSF nsr32{}, nsc32{};  // float copies for the mixed steps
+  // semi-Lagrangian (LLAGRANGIAN = .FALSE.): lists and shapes rebuilt on the
+  // current coordinates every step, in the caller's numbering, FP64
+  bool semi = false;
+  BinGeom sgeom{};           // the LINIT bins
+  DevPool sempool;           // this step's lists and shapes
+  DevCSR scsr;
+  DevCSR* dscsr = nullptr;   // device copy of scsr (read by the force kernel)
+  double *sshp = nullptr, *sgx = nullptr, *sgy = nullptr, *sgz = nullptr, *ssd = nullptr;
+  double *stgx = nullptr, *stgy = nullptr, *stgz = nullptr, *stshp = nullptr;
+  double *coo_cur = nullptr, *zero3 = nullptr;
   double *sgrad = nullptr, *hq = nullptr, *nsw = nullptr, *fstab = nullptr, *stress_prev = nullptr;
   StepAccum* acc = nullptr;
   unsigned* status = nullptr;
@@ -352,6 +362,7 @@ struct Ctx {
   ~Ctx() {
     if (gexec) cudaGraphExecDestroy(gexec);
     // stream-ordered frees first, then the stream
+    sempool.free_all();
     mlppool.free_all();
     mixpool.free_all();
     nbpool.free_all();
@@ -492,9 +503,12 @@ static int graph_for(Ctx* c, double dt, int mode, int len) {
   return 0;
 }
 
+static int semi_steps(Ctx* c, int32_t nsteps, double dt, int mode);
+
 static int run_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
   if (!c->searched) return MEGA_ERR_STATE;
   if (nsteps <= 0) return 0;
+  if (c->semi) return semi_steps(c, nsteps, dt, mode);
   const int prec = mode & 0xff;
   if (prec != MEGA_MODE_FP64 && prec != MEGA_MODE_MIXED) return MEGA_ERR_ARG;
   if ((mode & MEGA_FLAG_LEARNED_GUESS) && !c->mlp_on) return MEGA_ERR_STATE;
@@ -619,6 +633,139 @@ struct StreamGuard {
   ~StreamGuard() { if (s) cudaStreamDestroy(s); }
 };
 
+// ---- semi-Lagrangian steps
+__global__ void k_iota(int32_t n, int32_t* __restrict__ a) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) a[i] = (int32_t)i;
+}
+
+// Lists and shapes on the coordinates x (the LINIT bins are laid out when
+// linit, reused afterwards), their transposed gradients and row sums.
+static int semi_build(Ctx* c, const double* x, bool linit) {
+  const int32_t n = c->n;
+  c->sempool.free_all();
+  c->scsr = DevCSR();
+  int r = bin_search(c->s, n, x, c->win, c->sm_len, c->p.dist_max, 0, c->p.shsup, c->status, c->scsr, nullptr,
+                     c->sempool, linit ? &c->sgeom : nullptr, nullptr, linit ? nullptr : &c->sgeom);
+  if (r) return r;
+  const int64_t m = c->scsr.nnz;
+  MEGA_ALLOC(c->sempool, c->sshp, m);
+  MEGA_ALLOC(c->sempool, c->sgx, m);
+  MEGA_ALLOC(c->sempool, c->sgy, m);
+  MEGA_ALLOC(c->sempool, c->sgz, m);
+  if ((r = rk_shapes(c->s, c->p, n, x, c->win, c->ebc_nodes, c->scsr, c->sshp, c->sgx, c->sgy, c->sgz, c->status)))
+    return r;
+  if ((r = build_transpose(c->s, c->scsr, c->sempool))) return r;
+  MEGA_ALLOC(c->sempool, c->stgx, m);
+  MEGA_ALLOC(c->sempool, c->stgy, m);
+  MEGA_ALLOC(c->sempool, c->stgz, m);
+  k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->scsr.tpos, c->sgx, c->stgx);
+  k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->scsr.tpos, c->sgy, c->stgy);
+  k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->scsr.tpos, c->sgz, c->stgz);
+  c->stshp = nullptr;
+  if (c->has_body) {
+    MEGA_ALLOC(c->sempool, c->stshp, m);
+    k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->scsr.tpos, c->sshp, c->stshp);
+  }
+  MEGA_ALLOC(c->sempool, c->ssd, 3 * (int64_t)n);
+  k_rowsum3<double><<<grid_for(n, 256), 256, 0, c->s>>>(n, c->scsr.rowptr, c->sgx, c->sgy, c->sgz, c->ssd);
+  MEGA_CHECK_LAUNCH();
+  MEGA_ALLOC(c->sempool, c->dscsr, 1);
+  MEGA_TRY(cudaMemcpyAsync(c->dscsr, &c->scsr, sizeof(DevCSR), cudaMemcpyHostToDevice, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));  // (the host copy of scsr goes with this scope's changes)
+  return 0;
+}
+
+// LINIT of the semi-Lagrangian context: lists and shapes on the initial
+// coordinates, the caller's numbering kept (identity permutation).
+static int semi_search(Ctx* c, int32_t* gn, int32_t* gstart, int32_t* gstack, int64_t dim_nn_list, double* shp,
+                       double* dshp, int64_t* nnz, int32_t* gmaxn) {
+  const int32_t n = c->n;
+  if (!c->perm) {
+    MEGA_ALLOC(c->nbpool, c->perm, n);
+    MEGA_ALLOC(c->nbpool, c->iperm, n);
+    k_iota<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->perm);
+    k_iota<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->iperm);
+    MEGA_CHECK_LAUNCH();
+  }
+  MEGA_TRY(cudaMemcpyAsync(c->coo_cur, c->coo, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, c->s));
+  int r = semi_build(c, c->coo_cur, true);
+  if (r) return r;
+  const int64_t m = c->scsr.nnz;
+  int st = 0;
+  if (gn || gstart) {
+    std::vector<int64_t> rp(n + 1);
+    MEGA_TRY(cudaMemcpyAsync(rp.data(), c->scsr.rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    for (int32_t i = 0; i < n; ++i) {
+      if (gn) gn[i] = (int32_t)(rp[i + 1] - rp[i]);
+      if (gstart) gstart[i] = (int32_t)(rp[i] + 1);
+    }
+  }
+  if (gstack) {
+    if (m > dim_nn_list) st |= MEGA_ST_STACK_OVERFLOW;
+    else {
+      MEGA_TRY(cudaMemcpyAsync(gstack, c->scsr.col, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, c->s));
+      MEGA_TRY(cudaStreamSynchronize(c->s));
+      for (int64_t k = 0; k < m; ++k) gstack[k] += 1;
+    }
+  }
+  if (shp) MEGA_TRY(cudaMemcpyAsync(shp, c->sshp, sizeof(double) * m, cudaMemcpyDeviceToHost, c->s));
+  if (dshp) {
+    std::vector<double> a(m), b(m), d(m);
+    MEGA_TRY(cudaMemcpyAsync(a.data(), c->sgx, sizeof(double) * m, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaMemcpyAsync(b.data(), c->sgy, sizeof(double) * m, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaMemcpyAsync(d.data(), c->sgz, sizeof(double) * m, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    for (int64_t k = 0; k < m; ++k) { dshp[3 * k] = a[k]; dshp[3 * k + 1] = b[k]; dshp[3 * k + 2] = d[k]; }
+  }
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  c->searched = true;
+  c->phy_valid = true;
+  if (nnz) *nnz = m;
+  if (gmaxn) *gmaxn = c->scsr.gmaxn;
+  int ds = read_status(c, true);
+  if (ds < 0) return ds;
+  return st | ds;
+}
+
+// MAIN.F90:348-488 with LLAGRANGIAN = .FALSE. (HANDELER.F90:145, FINT.F90:
+// 410-436): predictor; the physical increment from the last lists and
+// shapes; the current coordinates; a re-search on them in the LINIT bins
+// and shapes on them; the force with those gradients as they are (F = I:
+// no push-forward, J = 1 as the reference's DET stays 1 on this path);
+// corrector.  FP64.
+static int semi_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
+  if ((mode & 0xff) != MEGA_MODE_FP64 || (mode & MEGA_FLAG_INTERP_EACH_STEP)) return MEGA_ERR_UNSUPPORTED;
+  if ((mode & MEGA_FLAG_LEARNED_GUESS) && !c->mlp_on) return MEGA_ERR_STATE;
+  const int32_t n = c->n;
+  const int64_t n3 = 3 * (int64_t)n;
+  for (int32_t k = 0; k < nsteps; ++k) {
+    int r = launch_predict(c->s, n3, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
+    if (r) return r;
+    if ((r = launch_interp(c->s, n, c->scsr, c->sshp, c->dsp, c->dsp_tot_phy, c->dsp_tot_phy))) return r;
+    k_add_kernel<<<grid_for(n3, 256), 256, 0, c->s>>>(n3, c->coo, c->dsp_tot_phy, c->coo_cur);
+    MEGA_CHECK_LAUNCH();
+    if ((r = semi_build(c, c->coo_cur, false))) return r;
+    if ((r = launch_defgrad(c->s, false, false, n, c->scsr, c->sgx, c->sgy, c->sgz, c->dsp, c->zero3, c->ssd,
+                            c->sshp, nullptr, c->fg, c->acc)))
+      return r;
+    if ((r = launch_stress(c->s, false, stress_args(c, dt, mode)))) return r;
+    ForceArgs f{};
+    f.n = n; f.csr = c->dscsr; f.tgx = c->stgx; f.tgy = c->stgy; f.tgz = c->stgz; f.tshp = c->stshp;
+    f.tmat = c->tmat; f.has_body = c->has_body; f.integrate = 1; f.predict = 0;
+    f.ebc = c->ebc; f.mass = c->mass; f.matidx = c->matidx; f.mats = c->mats; f.body_id = c->body_id;
+    f.fint = c->fint; f.fext = c->fext; f.vel = c->vel; f.acl = c->acl; f.dsp = c->dsp; f.dsp_tot = c->dsp_tot;
+    f.prforce = c->prforce; f.dt = dt; f.acc = c->acc; f.status = c->status;
+    if ((r = launch_force(c->s, false, f))) return r;
+    c->launches += 6;
+    c->time = c->time + dt;
+    c->steps += 1;
+  }
+  c->phy_valid = true;
+  return 0;
+}
+
 }  // namespace mega
 
 using namespace mega;
@@ -678,8 +825,9 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
                   const double* sm_len, int64_t* handle) {
   if (!p || n <= 0 || !coo || !win || !vol || !mass || !ebc || !vinit || !props || !mat_type || !sm_len || !handle)
     return MEGA_ERR_ARG;
-  if (p->lagrangian != 1 || p->peridynamics != 0) return MEGA_ERR_UNSUPPORTED;
+  if ((p->lagrangian != 1 && p->lagrangian != 0) || p->peridynamics != 0) return MEGA_ERR_UNSUPPORTED;
   if (p->itype_int != 0 && p->itype_int != 2) return MEGA_ERR_UNSUPPORTED;  // DNI or NSNI
+  if (p->lagrangian == 0 && p->itype_int != 0) return MEGA_ERR_UNSUPPORTED;  // semi-Lagrangian: DNI
   for (int64_t m = 0; m < 3 * (int64_t)n; ++m)
     if (ebc[m] != 0 && ebc[m] != 1) return MEGA_ERR_UNSUPPORTED;  // prescribed-velocity fixity (code 2)
   Ctx* c = new Ctx();
@@ -702,6 +850,12 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   CA(c->fint, n3); CA(c->fext, n3); CA(c->prforce, n3); CA(c->scratch3, n3);
   CA(c->stress, 6 * (int64_t)n); CA(c->strain, 6 * (int64_t)n); CA(c->eps, n); CA(c->strain_eq, n);
   CA(c->wvel, n); CA(c->fg, 18 * (int64_t)n); CA(c->iters, n); CA(c->acc, 1); CA(c->status, 1);
+  c->semi = p->lagrangian == 0;
+  if (c->semi) {
+    c->sempool.bind(c->s);
+    CA(c->coo_cur, n3); CA(c->zero3, n3);
+    cudaMemsetAsync(c->zero3, 0, sizeof(double) * n3, c->s);
+  }
   c->nsni = p->itype_int == 2;
   if (c->nsni) {
     CA(c->sgrad, 18 * (int64_t)n); CA(c->hq, 18 * (int64_t)n); CA(c->nsw, 18 * (int64_t)n);
@@ -867,6 +1021,7 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
   const int32_t n = c->n;
+  if (c->semi) return semi_search(c, gn, gstart, gstack, dim_nn_list, shp, dshp, nnz, gmaxn);
   if (c->searched) {  // back to the original numbering, then search afresh
     int r = permute_nodes(c, c->iperm);
     if (r) return r;
@@ -1108,7 +1263,7 @@ int mega_step_timed(int64_t h, int32_t nsteps, double dt, int32_t mode, float* m
   Ctx* c = get_ctx(h);
   if (!c || !ms) return c ? MEGA_ERR_ARG : MEGA_ERR_HANDLE;
   if (c->searched) { int r = ((mode & 0xff) == MEGA_MODE_MIXED) ? ensure_mixed(c) : ensure_fp64(c); if (r) return r; }
-  if (c->searched && nsteps > 16) { int r = graph_for(c, dt, mode, 16); if (r) return r; }
+  if (c->searched && !c->semi && nsteps > 16) { int r = graph_for(c, dt, mode, 16); if (r) return r; }
   cudaEvent_t e0, e1;
   MEGA_TRY(cudaEventCreate(&e0));
   MEGA_TRY(cudaEventCreate(&e1));
@@ -1128,6 +1283,7 @@ int mega_step_timed(int64_t h, int32_t nsteps, double dt, int32_t mode, float* m
 int mega_kernel_times(int64_t h, int32_t reps, double dt, int32_t mode, float* out_ms) {
   Ctx* c = get_ctx(h);
   if (!c || !out_ms || reps <= 0) return c ? MEGA_ERR_ARG : MEGA_ERR_HANDLE;
+  if (c->semi) return MEGA_ERR_UNSUPPORTED;  // the tiled gathers and instances are Lagrangian only
   if (!c->searched) return MEGA_ERR_STATE;
   { int r = ((mode & 0xff) == MEGA_MODE_MIXED) ? ensure_mixed(c) : ensure_fp64(c); if (r) return r; }
   if (!(mode & MEGA_FLAG_INTERP_EACH_STEP)) c->phy_valid = false;
@@ -1305,6 +1461,7 @@ int64_t mega_kernel_launches(int64_t h) {
 int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* choice, float* times_ms) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
+  if (c->semi) return MEGA_ERR_UNSUPPORTED;  // the tiled gathers and instances are Lagrangian only
   if (!c->searched) return MEGA_ERR_STATE;
   if (reps <= 0) return MEGA_ERR_ARG;
   const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
@@ -1341,8 +1498,10 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
                                   c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc,
                                   v);
     };
-    r = def();  // warm-up
+    r = def();  // warm-up (twice: the first launch of a variant may also load its code)
+    if (!r) r = def();
     if (r) break;
+    MEGA_TRY(cudaStreamSynchronize(c->s));
     cudaEventRecord(e0, c->s);
     for (int k = 0; k < reps && !r; ++k) r = def();
     cudaEventRecord(e1, c->s);
@@ -1353,6 +1512,9 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
     if (r) break;
     const TiledForceArgs fa = force_args(c, dt, mode & 0xff, 0);
     r = launch_force_tiled(c->s, mixed, fa, v);  // warm-up
+    if (!r) r = launch_force_tiled(c->s, mixed, fa, v);
+    if (r) break;
+    MEGA_TRY(cudaStreamSynchronize(c->s));
     cudaEventRecord(e0, c->s);
     for (int k = 0; k < reps && !r; ++k) r = launch_force_tiled(c->s, mixed, fa, v);
     cudaEventRecord(e1, c->s);
@@ -1383,6 +1545,7 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
 int mega_set_instances(int64_t h, int32_t ninst, const int32_t* inst_nodes, const double* dist_max) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
+  if (c->semi) return MEGA_ERR_UNSUPPORTED;  // the tiled gathers and instances are Lagrangian only
   if (ninst < 1 || !inst_nodes) return MEGA_ERR_ARG;
   std::vector<int32_t> off(ninst + 1, 0);
   for (int32_t k = 0; k < ninst; ++k) {

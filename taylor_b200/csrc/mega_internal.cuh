@@ -134,7 +134,8 @@ int scan_counts(cudaStream_t s, const int32_t* cnt, int64_t* off, int64_t m, Dev
 // ijk (3,n) 1-based may be null.  status is a device word (OR-ed).
 int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, const double* sm_len,
                const double dist_max[3], int32_t itype_int, int32_t shsup, unsigned* status,
-               DevCSR& csr, int32_t* ijk, DevPool& pool, BinGeom* geom_out, int32_t* cell_order = nullptr);
+               DevCSR& csr, int32_t* ijk, DevPool& pool, BinGeom* geom_out, int32_t* cell_order = nullptr,
+               const BinGeom* fixed = nullptr);  // fixed: reuse these bins instead of laying them out
 // Build the CSC view of csr.
 int build_transpose(cudaStream_t s, DevCSR& csr, DevPool& pool);
 

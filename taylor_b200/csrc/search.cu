@@ -431,7 +431,7 @@ int scan_counts(cudaStream_t s, const int32_t* cnt, int64_t* off, int64_t m, Dev
 
 int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, const double* sm_len,
                const double dist_max[3], int32_t itype_int, int32_t shsup, unsigned* status, DevCSR& csr,
-               int32_t* ijk, DevPool& pool, BinGeom* geom_out, int32_t* cell_order) {
+               int32_t* ijk, DevPool& pool, BinGeom* geom_out, int32_t* cell_order, const BinGeom* fixed) {
   DevPool scratch(s);  // freed on return
   csr.n = n;
   const int nbb = 148 * 2;
@@ -441,16 +441,21 @@ int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, 
   MEGA_ALLOC(scratch, part, 9 * nbb);
   MEGA_ALLOC(scratch, geom, 6);
   MEGA_ALLOC(scratch, dims, 3);
-  k_bbox_partial<<<nbb, 256, 0, s>>>(n, coo, win, dist_max[0], dist_max[1], dist_max[2], part);
-  MEGA_CHECK_LAUNCH();
-  k_bbox_final<<<1, 1, 0, s>>>(nbb, part, geom, dims);
-  MEGA_CHECK_LAUNCH();
   BinGeom bg;
-  MEGA_TRY(cudaMemcpyAsync(bg.g, geom, sizeof(double) * 6, cudaMemcpyDeviceToHost, s));
-  int32_t hd[3];
-  MEGA_TRY(cudaMemcpyAsync(hd, dims, sizeof(hd), cudaMemcpyDeviceToHost, s));
-  MEGA_TRY(cudaStreamSynchronize(s));
-  bg.nx = hd[0]; bg.ny = hd[1]; bg.nz = hd[2];
+  if (fixed) {  // the semi-Lagrangian re-search keeps the LINIT bins (HANDELER.F90:181-250 run at LINIT only)
+    bg = *fixed;
+    MEGA_TRY(cudaMemcpyAsync(geom, bg.g, sizeof(double) * 6, cudaMemcpyHostToDevice, s));
+  } else {
+    k_bbox_partial<<<nbb, 256, 0, s>>>(n, coo, win, dist_max[0], dist_max[1], dist_max[2], part);
+    MEGA_CHECK_LAUNCH();
+    k_bbox_final<<<1, 1, 0, s>>>(nbb, part, geom, dims);
+    MEGA_CHECK_LAUNCH();
+    MEGA_TRY(cudaMemcpyAsync(bg.g, geom, sizeof(double) * 6, cudaMemcpyDeviceToHost, s));
+    int32_t hd[3];
+    MEGA_TRY(cudaMemcpyAsync(hd, dims, sizeof(hd), cudaMemcpyDeviceToHost, s));
+    MEGA_TRY(cudaStreamSynchronize(s));
+    bg.nx = hd[0]; bg.ny = hd[1]; bg.nz = hd[2];
+  }
   if (geom_out) *geom_out = bg;
   const int64_t nbins = (int64_t)bg.nx * bg.ny * bg.nz;
   if (bg.nx <= 0 || bg.ny <= 0 || bg.nz <= 0 || nbins > INT32_MAX) return MEGA_ERR_UNSUPPORTED;

@@ -360,3 +360,22 @@ def test_nsni_damps_the_spurious_velocity_spikes_of_dni():
         peaks[itype] = peak / c["v0"]
     assert peaks[0] > 1.4, peaks
     assert peaks[2] < 1.25, peaks
+
+
+# ------------------------------------------------------- semi-Lagrangian
+def test_semi_lagrangian_research_in_linit_bins():
+    """The re-search in the bins laid out at LINIT returns the LINIT lists on
+    the LINIT coordinates, and the first semi-Lagrangian steps stay close to
+    the Lagrangian ones (their shapes differ only by the small deformation)."""
+    c = cases.taylor_bar(h=0.8e-3)
+    nb = O.bin_search(c["coo"], c["win"], c["sm_len"], c["dist_max"])
+    again = O.bin_search(c["coo"], c["win"], c["sm_len"], c["dist_max"], geom_in=nb["geom"])
+    np.testing.assert_array_equal(again["gstack"], nb["gstack"])
+    runs = {}
+    for lag in (1, 0):
+        r = O.Run(c, O.params(**cases.param_kwargs(c, lagrangian=lag)), nthreads=4)
+        dt = cases.stable_dt(c, nb["gn"], nb["gstart"], nb["gstack"])
+        assert r.step(5, dt) == 0
+        runs[lag] = r.coo_cur.reshape(-1, 3) - c["coo"]
+    assert np.abs(runs[0] - runs[1]).max() <= 2e-2 * np.abs(runs[1]).max()
+    assert np.abs(runs[0] - runs[1]).max() > 0.0
