@@ -24,6 +24,7 @@ Further sections of the same line (each skippable by its flag):
   peridynamics  the 2.56M-particle bond-based plate (--pmb-nx)
   nsni          the same bar with stabilised nodal integration: timing in
                 both precisions and --nsni-steps from impact
+  pre_model     device mesh pre-processing of a --pre-nodes^3 hexahedral box
   batch         --batch-bars bars of uneven size in one context vs one
                 context per bar
   cpu_baseline  the C++ OpenMP restatement of the reference on the host
@@ -67,6 +68,8 @@ def parse():
     ap.add_argument("--pmb-steps", type=int, default=4000, help="steps of the peridynamics run")
     ap.add_argument("--nsni-steps", type=int, default=2000,
                     help="steps of the stabilised-nodal-integration runs of the same bar; 0 skips them")
+    ap.add_argument("--pre-nodes", type=int, default=100,
+                    help="nodes per side of the hexahedral mesh of the pre-processing run; 0 skips it")
     ap.add_argument("--batch-bars", type=int, default=256, help="bars of the batched run; 0 skips it")
     ap.add_argument("--batch-steps", type=int, default=64, help="timed steps of the batched and sequential runs")
     return ap.parse_args()
@@ -257,12 +260,16 @@ def run_ours(args, rank, world, dist):
     except Exception as ex:
         nsni = dict(error=str(ex))
     try:
+        pre = pre_model_run(args) if args.pre_nodes > 0 else None
+    except Exception as ex:
+        pre = dict(error=str(ex))
+    try:
         batch = batch_run(args) if args.batch_bars > 0 else None
     except Exception as ex:
         batch = dict(error=str(ex))
     out = dict(case=case, n=n, nnz=nnz, kmean=kmean, dt=dt, res=res, step0_s=step0_s, e2e_s=e2e_s, h2d=h2d,
                d2h=d2h, peak=peak, peak_kind=peak_kind, scalars=s, dev_bytes=dev_bytes, accuracy=acc, learned=lrn, pmb=pmb,
-               nsni=nsni, batch=batch,
+               nsni=nsni, pre_model=pre, batch=batch,
                tuned=tuned,
                e2e_parts=e2e_parts)
     return out
@@ -333,6 +340,28 @@ def nsni_run(case, dt, args):
     out["dni_fp64_end_state"] = cases.bar_metrics(case, d.download(_lib.F_COO_CURRENT), d.download(_lib.F_EPS))
     d.close()
     return out
+
+
+def pre_model_run(args):
+    """Mesh pre-processing (windows, volumes, smoothing cells) of a jittered
+    hexahedral box through the C ABI from host arrays, against the oracle's
+    vectorised CPU restatement of the same loops."""
+    from taylor_b200 import cases, mega
+    sys.path.insert(0, ROOT)
+    from oracle import premodel as P
+    k = args.pre_nodes
+    coo, elems = cases.hex_box(k, k, k, 0.1e-3, jitter=0.05, seed=3)
+    mega.pre_model_hex(coo, elems, norm_win=2.0)  # warm-up (same sizes)
+    t0 = time.perf_counter()
+    got = mega.pre_model_hex(coo, elems, norm_win=2.0)
+    gpu_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    w, v = P.hex_windows_and_volumes(coo, elems)
+    P.smoothing_lengths(v, w)
+    cpu_s = time.perf_counter() - t0
+    same = bool(np.array_equal(got["win_raw"], w) and np.array_equal(got["vol"], v))
+    return dict(workload=f"hex box {k}^3 nodes, h=0.1mm, 5% jitter", nodes=len(coo), elements=len(elems),
+                gpu_s_with_copies=gpu_s, cpu_numpy_s=cpu_s, windows_and_volumes_bit_exact=same)
 
 
 RATE_LAW = (90e6, 292e6, 0.31, 0.025, 1.0)  # A, B, n, C, epsdot0 of the power-law rate-dependent hardening
@@ -598,7 +627,8 @@ def main():
                  parts=r["e2e_parts"]),
         gpu_launches=mix["launches"], clocks=mix["clocks"], clocks_fp64=f64["clocks"],
         newton_iters_last_step=r["scalars"]["newton_iters"], plastic_nodes_last_step=r["scalars"]["plastic_nodes"],
-        accuracy=r["accuracy"], learned=r["learned"], peridynamics=r["pmb"], nsni=r["nsni"], batch=r["batch"])
+        accuracy=r["accuracy"], learned=r["learned"], peridynamics=r["pmb"], nsni=r["nsni"],
+        pre_model=r["pre_model"], batch=r["batch"])
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

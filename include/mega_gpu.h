@@ -45,6 +45,8 @@ extern "C" {
                                           caller's DIM_NN_LIST */
 #define MEGA_ST_SINGULAR_SHAPE  0x0080 /* PD shape tensor K not invertible
                                           (INVERSE.F90:41-45) */
+#define MEGA_ST_BAD_MESH        0x0100 /* element connectivity names a node
+                                          outside 1..N */
 
 /* ---- API errors (negative return codes) --------------------------------- */
 #define MEGA_ERR_CUDA     (-1)
@@ -233,6 +235,21 @@ int mega_construct_fint(const mega_params* p, int32_t n,
  * Lagrangian path.  At linit != 0 the influence functions and K^-1 are built
  * (UDFM_SHAPE_TENSOR, RK.f90:579-726) into gstack_shp and ginvk (3,3,n).
  * gcoo_current (3,n) are the current coordinates. */
+/* Mesh pre-processing of PRE_MODEL.F90:248-268 and PRE_CONTROL.F90:803-871
+ * for hexahedral meshes, on the device: conn = IDELM(8,NELEM), 1-based.
+ * Out: win_raw (3,N) = ADIAL (GET_ADIAL, PRE_MODEL_ADIAL.F90:64-153), vol (N)
+ * (GET_VOLUMES / GET_VOL2, PRE_MODEL_VOLUMES.F90:70-117), sm_len (6,N),
+ * mom (3,N) = X/Y/Z_MOM and dist_max (3) (GET_SMOOTHING_LENGTHS,
+ * PRE_MODEL_SMOOTHING_LENGTHS.F90:49-99), win (3,N) = ADIAL * norm_win
+ * (PRE_CONTROL.F90:870-872; norm_win (N) may be NULL for 1) and the smallest
+ * raw window (the automatic QL_LEN before QL_LEN_REDUCE_AUTO,
+ * PRE_CONTROL.F90:803-815).  win, mom and min_raw_window may be NULL.
+ * Windows and volumes are bit-exact with the reference's element-order
+ * loops. */
+int mega_pre_model_hex(int32_t n, const double* coo, int32_t nelem, const int32_t* conn, const double* norm_win,
+                       double* win_raw, double* win, double* vol, double* sm_len, double* mom, double* dist_max,
+                       double* min_raw_window);
+
 int mega_construct_fint_pd(const mega_params* p, int32_t n,
                            const double* gcoo, const double* gcoo_current,
                            const double* gwin, const double* gvol,

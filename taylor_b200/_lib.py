@@ -22,6 +22,7 @@ ST_NONFINITE = 0x0010
 ST_BAD_MATERIAL = 0x0020
 ST_STACK_OVERFLOW = 0x0040
 ST_SINGULAR_SHAPE = 0x0080
+ST_BAD_MESH = 0x0100
 ERR_CUDA, ERR_ARG, ERR_HANDLE, ERR_STATE, ERR_NOMEM, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6
 
 MODE_FP64 = 0
@@ -99,6 +100,7 @@ SIGNATURES = {
     "mega_log_rate_samples": (I32, [I64, I64, I32, C.c_uint32]),
     "mega_rate_samples": (I32, [I64, P, I64, C.POINTER(I64)]),
     "mega_train_surrogate": (I32, [I64, P, I32, I32, F32, C.c_uint64, P]),
+    "mega_pre_model_hex": (I32, [I32, P, I32, P, P, P, P, P, P, P, P, P]),
     "mega_status_string": (C.c_char_p, [I32]),
     "mega_gpu_finalize": (I32, [I64]),
 }

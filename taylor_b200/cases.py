@@ -45,6 +45,25 @@ def with_damage(case, mat_type, k_i, k_c, dam_max, q_phi=0.0, k_phi=0.0, q_psi=0
     return c
 
 
+def hex_box(nx, ny, nz, h, jitter=0.0, seed=1):
+    """A structured hexahedral mesh of nx*ny*nz nodes at spacing h, each
+    coordinate jittered by a seeded uniform +-jitter*h; hexes in the
+    LS-DYNA node order (bottom face counter-clockwise, then the top face),
+    0-based node ids, (nx-1)(ny-1)(nz-1) elements."""
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    coo = np.stack([i.ravel() * h, j.ravel() * h, k.ravel() * h], axis=1).astype(np.float64)
+    if jitter:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        coo += rng.uniform(-jitter * h, jitter * h, size=coo.shape)
+    nid = lambda a, b, c: a + nx * (b + ny * c)
+    ek, ej, ei = np.meshgrid(np.arange(nz - 1), np.arange(ny - 1), np.arange(nx - 1), indexing="ij")
+    ei, ej, ek = ei.ravel(), ej.ravel(), ek.ravel()
+    elems = np.stack([nid(ei, ej, ek), nid(ei + 1, ej, ek), nid(ei + 1, ej + 1, ek), nid(ei, ej + 1, ek),
+                      nid(ei, ej, ek + 1), nid(ei + 1, ej, ek + 1), nid(ei + 1, ej + 1, ek + 1),
+                      nid(ei, ej + 1, ek + 1)], axis=1).astype(np.int32)
+    return coo, elems
+
+
 def smoothing_lengths(vol, win_raw):
     """GET_SMOOTHING_LENGTHS (PRE_MODEL_SMOOTHING_LENGTHS.F90:49-99) with the
     raw windows: SM_LEN(6,N) and (XDIST_MAX, YDIST_MAX, ZDIST_MAX)."""

@@ -810,7 +810,8 @@ const char* mega_status_string(int32_t st) {
       {MEGA_ST_NONFINITE, "non-finite force or stress"},
       {MEGA_ST_BAD_MATERIAL, "INVALID MATERIAL TYPE IN SUBROUTINE CONSTITUTION"},
       {MEGA_ST_STACK_OVERFLOW, "neighbour stack larger than DIM_NN_LIST"},
-      {MEGA_ST_SINGULAR_SHAPE, "PROBLEM INVERTING MATRIX"}};
+      {MEGA_ST_SINGULAR_SHAPE, "PROBLEM INVERTING MATRIX"},
+      {MEGA_ST_BAD_MESH, "element connectivity names a node outside the model"}};
   for (auto& t : tab)
     if (st & t.bit) {
       if (buf[0]) strncat(buf, "; ", sizeof(buf) - strlen(buf) - 1);

@@ -126,6 +126,27 @@ def construct_fint(params, coo, win, vol, props, mat_type, ebc_nodes, state, str
                 gint_work=gw.value, shp=shp, dshp=dshp, status=st)
 
 
+def pre_model_hex(coo, elems, norm_win=None, allow_status=False):
+    """Mesh pre-processing on the device (PRE_MODEL.F90:248-268, PRE_CONTROL.F90:
+    803-871) for a hexahedral mesh: elems (E, 8) 0-based node ids.  Returns
+    win_raw, win (scaled by norm_win, per node or scalar), vol, sm_len, mom
+    (X/Y/Z_MOM), dist_max and the smallest raw window."""
+    coo = _f64(coo)
+    n = len(coo)
+    conn = np.ascontiguousarray(np.asarray(elems, np.int64) + 1, dtype=np.int32)
+    nw = None
+    if norm_win is not None:
+        nw = _f64(np.broadcast_to(np.asarray(norm_win, np.float64), (n,)))
+    win_raw, win, mom = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+    vol, sm_len, dmax = np.zeros(n), np.zeros((n, 6)), np.zeros(3)
+    wmin = C.c_double(0.0)
+    st = _lib.lib().mega_pre_model_hex(n, ptr(coo), len(conn), ptr(conn), ptr(nw), ptr(win_raw), ptr(win), ptr(vol),
+                                       ptr(sm_len), ptr(mom), ptr(dmax), C.byref(wmin))
+    check(st, "pre_model_hex", allow_status)
+    return dict(win_raw=win_raw, win=win, vol=vol, sm_len=sm_len, mom=mom, dist_max=dmax, min_raw_window=wmin.value,
+                status=st)
+
+
 MLP_HIDDEN = 64
 
 

@@ -98,7 +98,7 @@ def main(ref=None):
     coo, elems, sets = read_k(os.path.join(ref, "Taylor_bar.k"))
     win_raw, vol = windows_and_volumes(coo, elems)
     out = os.path.join(HERE, "case_a.npz")
-    np.savez_compressed(out, coo=coo, win_raw=win_raw, vol=vol, bar=sets[1], wall=sets[2],
+    np.savez_compressed(out, coo=coo, win_raw=win_raw, vol=vol, elems=elems, bar=sets[1], wall=sets[2],
                         norm_win=2.75, v0=373.0, dt=0.78363e-07, time_end=5.5e-05, ql_coef=0.001,
                         props=np.array([0.3, 78.2e9, 2700.0, 0.29e9, 125.0, 0.1]), mat_type=2)
     print("wrote", out, "nodes", len(coo), "elements", len(elems), "wall", len(sets[2]))

@@ -6,6 +6,8 @@ conditions of the RK shape functions (TEST.F90:1-300) and objectivity under
 a rigid rotation (TEST.F90:305-326).  These tests run them against the
 oracle, plus properties of the return mapping, the force assembly and the
 neighbour search that hold by construction in the reference."""
+import os
+
 import numpy as np
 import pytest
 
@@ -379,3 +381,23 @@ def test_semi_lagrangian_research_in_linit_bins():
         runs[lag] = r.coo_cur.reshape(-1, 3) - c["coo"]
     assert np.abs(runs[0] - runs[1]).max() <= 2e-2 * np.abs(runs[1]).max()
     assert np.abs(runs[0] - runs[1]).max() > 0.0
+
+
+# ------------------------------------------------------- pre-processing
+def test_premodel_oracle_reproduces_case_a_and_a_regular_grid():
+    from oracle import premodel as P
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "case_a.npz"))
+    w, v = P.hex_windows_and_volumes(d["coo"], d["elems"])
+    np.testing.assert_array_equal(w, d["win_raw"])
+    np.testing.assert_array_equal(v, d["vol"])
+    h = 0.5e-3
+    coo, elems = cases.hex_box(6, 5, 4, h)
+    w, v = P.hex_windows_and_volumes(coo, elems)
+    assert abs(v.sum() - 5 * 4 * 3 * h ** 3) <= 1e-12 * v.sum()          # the hexes tile the box
+    inner = ((coo[:, 0] > 0.1 * h) & (coo[:, 0] < 4.9 * h) & (coo[:, 1] > 0.1 * h) & (coo[:, 1] < 3.9 * h)
+             & (coo[:, 2] > 0.1 * h) & (coo[:, 2] < 2.9 * h))
+    np.testing.assert_allclose(v[inner], h ** 3, rtol=1e-12)
+    np.testing.assert_allclose(w, h, rtol=1e-12)
+    sm, mom, dmax = P.smoothing_lengths(v, w)
+    np.testing.assert_allclose(sm[inner], h / 2, rtol=1e-12)            # the cell of a lattice node
+    np.testing.assert_allclose(mom[inner], h * h / 12, rtol=1e-12)
