@@ -327,6 +327,11 @@ int mega_kernel_times(int64_t h, int32_t reps, double dt, int32_t mode,
 
 /* Copy a field (enum mega_field) to host memory (sizes in the enum). */
 int mega_download(int64_t h, int32_t field, double* dst);
+/* Several fields at an output step in one device-to-host copy: the fields
+ * (MEGA_F_* codes) one after another in dst, each in its mega_download
+ * layout and the caller's node order (the arrays VTK_OUTPUT.F90 writes at
+ * MAIN's output steps, gathered without one round trip per field). */
+int mega_snapshot(int64_t h, int32_t nfields, const int32_t* fields, double* dst);
 /* Replace a field from host memory (DSP_TOT, VEL, ACL, STRESS, STRAIN, EPS). */
 int mega_upload(int64_t h, int32_t field, const double* src);
 int mega_get_scalars(int64_t h, mega_scalars_t* out);

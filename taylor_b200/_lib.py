@@ -84,6 +84,7 @@ SIGNATURES = {
     "mega_kernel_times": (I32, [I64, I32, D, I32, P]),
     "mega_download": (I32, [I64, I32, P]),
     "mega_upload": (I32, [I64, I32, P]),
+    "mega_snapshot": (I32, [I64, I32, P, P]),
     "mega_get_scalars": (I32, [I64, C.POINTER(MegaScalars)]),
     "mega_device_bytes": (I64, [I64]),
     "mega_kernel_launches": (I64, [I64]),

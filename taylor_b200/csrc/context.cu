@@ -104,6 +104,10 @@ __global__ void k_iperm(int32_t n, const int32_t* __restrict__ perm, int32_t* __
   if (r < n) iperm[perm[r]] = (int32_t)r;
 }
 // dst[r*w + k] = src[perm[r]*w + k]  (gather = old -> new), element size es bytes
+__global__ void k_i32_to_f64(int64_t m, const int32_t* __restrict__ a, double* __restrict__ out) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < m) out[k] = (double)a[k];
+}
 __global__ void k_add_kernel(int64_t m, const double* __restrict__ a, const double* __restrict__ b,
                              double* __restrict__ out) {
   const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1382,6 +1386,84 @@ int mega_download(int64_t h, int32_t field, double* dst) {
     default: return MEGA_ERR_ARG;
   }
   return download_nodes(c, src, w, 8, dst);
+}
+
+// Several fields in one copy to the host (the output step of MAIN: the
+// VTK writer's arrays), each in the caller's node order, one after another.
+int mega_snapshot(int64_t h, int32_t nfields, const int32_t* fields, double* dst) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (nfields <= 0 || !fields || !dst) return MEGA_ERR_ARG;
+  const int64_t n = c->n, n3 = 3 * n;
+  std::vector<int> width(nfields);
+  int64_t total = 0;
+  for (int32_t f = 0; f < nfields; ++f) {
+    int w = 0;
+    switch (fields[f]) {
+      case MEGA_F_DSP: case MEGA_F_DSP_TOT: case MEGA_F_VEL: case MEGA_F_ACL: case MEGA_F_FINT: case MEGA_F_FEXT:
+      case MEGA_F_PRFORCE: case MEGA_F_COO_CURRENT: case MEGA_F_DSP_TOT_PHY: w = 3; break;
+      case MEGA_F_STRESS: case MEGA_F_STRAIN: w = 6; break;
+      case MEGA_F_EPS: case MEGA_F_STRAIN_EQ: case MEGA_F_WAVE_VEL: case MEGA_F_NEWTON_IT: w = 1; break;
+      case MEGA_F_STATE_AUX: if (!c->aux) return MEGA_ERR_STATE; w = 4; break;
+      case MEGA_F_NSNI_SGRAD: if (!c->sgrad) return MEGA_ERR_STATE; w = 18; break;
+      default: return MEGA_ERR_ARG;
+    }
+    width[f] = w;
+    total += n * w;
+  }
+  DevPool tp(c->s);
+  double *out = nullptr, *tmp = nullptr;
+  MEGA_ALLOC(tp, out, total);
+  MEGA_ALLOC(tp, tmp, n3);
+  int64_t off = 0;
+  for (int32_t f = 0; f < nfields; ++f) {
+    const int w = width[f];
+    const double* src = nullptr;
+    switch (fields[f]) {
+      case MEGA_F_DSP: src = c->dsp; break;
+      case MEGA_F_DSP_TOT: src = c->dsp_tot; break;
+      case MEGA_F_VEL: src = c->vel; break;
+      case MEGA_F_ACL: src = c->acl; break;
+      case MEGA_F_FINT: src = c->fint; break;
+      case MEGA_F_FEXT: src = c->fext; break;
+      case MEGA_F_PRFORCE: src = c->prforce; break;
+      case MEGA_F_STRESS: src = c->stress; break;
+      case MEGA_F_STRAIN: src = c->strain; break;
+      case MEGA_F_EPS: src = c->eps; break;
+      case MEGA_F_STRAIN_EQ: src = c->strain_eq; break;
+      case MEGA_F_WAVE_VEL: src = c->wvel; break;
+      case MEGA_F_STATE_AUX: src = c->aux; break;
+      case MEGA_F_NSNI_SGRAD: src = c->sgrad; break;
+      case MEGA_F_NEWTON_IT:
+        k_i32_to_f64<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->iters, tmp);
+        MEGA_CHECK_LAUNCH();
+        src = tmp;
+        break;
+      default: {  // the physical displacement, or the current coordinates
+        const double* phy = c->dsp_tot_phy;
+        if (!c->phy_valid) {
+          if (!c->searched) return MEGA_ERR_STATE;
+          int r = launch_interp(c->s, c->n, c->csr, c->shp, c->dsp_tot, nullptr, tmp);
+          if (r) return r;
+          phy = tmp;
+        }
+        if (fields[f] == MEGA_F_COO_CURRENT) {
+          k_add_kernel<<<grid_for(n3, 256), 256, 0, c->s>>>(n3, c->coo, phy, tmp);
+          MEGA_CHECK_LAUNCH();
+          phy = tmp;
+        }
+        src = phy;
+      }
+    }
+    if (c->searched)
+      k_perm_gather<<<grid_for(n * w, 256), 256, 0, c->s>>>((int32_t)n, w, 8, c->iperm, (const unsigned char*)src,
+                                                             (unsigned char*)(out + off));
+    else
+      MEGA_TRY(cudaMemcpyAsync(out + off, src, sizeof(double) * n * w, cudaMemcpyDeviceToDevice, c->s));
+    MEGA_CHECK_LAUNCH();
+    off += n * w;
+  }
+  return download_staged(c->s, dst, out, sizeof(double) * (size_t)total);
 }
 
 int mega_upload(int64_t h, int32_t field, const double* src) {

@@ -325,6 +325,19 @@ class Mega:
         check(_lib.lib().mega_download(self.h, int(field), ptr(out)), "download")
         return out.reshape(self.n, k) if k > 1 else out
 
+    def snapshot(self, fields):
+        """Several fields in one device-to-host copy: {field code: array}."""
+        codes = np.ascontiguousarray([int(f) for f in fields], dtype=np.int32)
+        sizes = [self._SIZES[int(f)] for f in codes]
+        out = np.zeros(self.n * sum(sizes))
+        check(_lib.lib().mega_snapshot(self.h, len(codes), ptr(codes), ptr(out)), "snapshot")
+        res, off = {}, 0
+        for f, k in zip(codes, sizes):
+            a = out[off:off + self.n * k]
+            res[int(f)] = a.reshape(self.n, k).copy() if k > 1 else a.copy()
+            off += self.n * k
+        return res
+
     def upload(self, field, arr):
         check(_lib.lib().mega_upload(self.h, int(field), ptr(_f64(arr).ravel())), "upload")
 

@@ -130,3 +130,23 @@ def test_shapes_on_renumbered_lists_equal_the_downloaded_path(itype):
         np.testing.assert_array_equal(a.download(f), b.download(f))
     a.close()
     b.close()
+
+
+def test_snapshot_equals_single_downloads(tmp_path):
+    """One device-to-host copy of several fields equals their single
+    downloads, and the output step writes them as VTK."""
+    from taylor_b200 import vtk
+    c = cases.taylor_bar(h=1.0e-3)
+    m = mega.Mega(c, _lib.params(**cases.param_kwargs(c)))
+    m.search_and_shapes()
+    m.step(20, 3e-8)
+    fields = (_lib.F_COO_CURRENT, _lib.F_STRESS, _lib.F_EPS, _lib.F_NEWTON_IT, _lib.F_VEL, _lib.F_DSP_TOT_PHY)
+    snap = m.snapshot(fields)
+    for f in fields:
+        np.testing.assert_array_equal(snap[int(f)], m.download(f))
+    p = tmp_path / "MEGAOUT_0001.vtk"
+    vtk.write_output_step(m, p)
+    lines = p.read_text().splitlines()
+    assert lines[4].split() == ["POINTS", str(c["n"]), "double"]
+    assert sum(1 for l in lines if l.startswith("SCALARS")) == 3 + 3 + 6 + 1
+    m.close()
