@@ -218,6 +218,7 @@ def run_ours(args, rank, world, dist):
     def job(steps):
         t0 = time.perf_counter()
         e = mega.Mega(case, p)
+        e.set_precisions(fp64=False, mixed=True)   # the job steps in mixed precision only
         t1 = time.perf_counter()
         e.search_and_shapes()
         t2 = time.perf_counter()

@@ -2,11 +2,15 @@
 // MAIN.F90:304-658 time loop on the device, captured in CUDA graphs) and the
 // copy-in/copy-out drop-ins for the reference's subroutines.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <set>
@@ -170,16 +174,78 @@ __global__ void k_rowsum_pk32(int32_t n, const int64_t* __restrict__ rowptr, con
 
 inline unsigned grid_for(int64_t work, int block) { return (unsigned)((work + block - 1) / block); }
 
+// Worker threads for the host-side set-up loops, started once per process
+// (up to 15 besides the caller) and kept: starting threads for every loop
+// cost more than the copies they split.  Tasks from concurrent callers share
+// one queue; a caller waiting for its own tasks runs queued ones meanwhile,
+// so a call completes even with every worker busy elsewhere.
+class HostPool {
+ public:
+  static HostPool& get() {
+    static HostPool* p = new HostPool();  // never destroyed: the workers block in wait() at exit
+    return *p;
+  }
+  int workers() const { return nw_; }
+  void submit(std::function<void()> f) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      q_.push_back(std::move(f));
+    }
+    cv_.notify_one();
+  }
+  bool run_one() {
+    std::function<void()> f;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (q_.empty()) return false;
+      f = std::move(q_.front());
+      q_.pop_front();
+    }
+    f();
+    return true;
+  }
+
+ private:
+  HostPool() {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    nw_ = (int)std::min(15u, hw - 1);
+    for (int k = 0; k < nw_; ++k) std::thread([this] { loop(); }).detach();
+  }
+  void loop() {
+    for (;;) {
+      std::function<void()> f;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [this] { return !q_.empty(); });
+        f = std::move(q_.front());
+        q_.pop_front();
+      }
+      f();
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<std::function<void()>> q_;
+  int nw_ = 0;
+};
+
 // fn(lo, hi) over [0, n) in contiguous chunks on the host's cores (the
-// per-node set-up scans of a million-node model)
+// per-node set-up scans of a million-node model), at least `grain` items
+// per chunk; the caller runs the first chunk
 template <typename F>
-void host_parallel(int64_t n, F fn) {
-  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(16, (int64_t)std::thread::hardware_concurrency()),
-                                                             n / 65536));
+void host_parallel(int64_t n, F fn, int64_t grain = 65536) {
+  HostPool& pool = HostPool::get();
+  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(pool.workers() + 1, n / grain));
   if (nt == 1) { fn((int64_t)0, n); return; }
-  std::vector<std::thread> th;
-  for (int64_t t = 0; t < nt; ++t) th.emplace_back(fn, n * t / nt, n * (t + 1) / nt);
-  for (auto& x : th) x.join();
+  std::atomic<int64_t> left(nt - 1);
+  for (int64_t t = 1; t < nt; ++t)
+    pool.submit([&fn, &left, n, nt, t] {
+      fn(n * t / nt, n * (t + 1) / nt);
+      left.fetch_sub(1, std::memory_order_release);
+    });
+  fn((int64_t)0, n / nt);
+  while (left.load(std::memory_order_acquire) > 0)
+    if (!pool.run_one()) std::this_thread::yield();
 }
 
 // Bulk host <-> device copies go through one pinned buffer kept for the
@@ -201,10 +267,17 @@ void host_copy(void* dst, const void* src, size_t bytes) {
       const size_t a = (size_t)k << 20, b = std::min(bytes, (size_t)(k + 1) << 20);
       std::memcpy((unsigned char*)dst + a, (const unsigned char*)src + a, b - a);
     }
-  });
+  }, 2);
 }
 
-struct HostToDevice { void* dst; const void* src; size_t bytes; };
+// one array to upload: copied from src, or written by fill(staging) when
+// the host array is formed on the way (fill writes `bytes` bytes)
+struct HostToDevice {
+  void* dst;
+  const void* src;
+  size_t bytes;
+  std::function<void(void*)> fill = nullptr;
+};
 
 // the copies in order on stream s, complete on return
 int upload_staged(cudaStream_t s, const std::vector<HostToDevice>& items) {
@@ -219,13 +292,22 @@ int upload_staged(cudaStream_t s, const std::vector<HostToDevice>& items) {
     else { g_stage.p = nullptr; cudaGetLastError(); }
   }
   if (!g_stage.p) {
-    for (const auto& it : items) MEGA_TRY(cudaMemcpyAsync(it.dst, it.src, it.bytes, cudaMemcpyHostToDevice, s));
+    for (const auto& it : items) {
+      if (it.fill) {
+        std::vector<unsigned char> tmp(it.bytes);
+        it.fill(tmp.data());
+        MEGA_TRY(cudaMemcpy(it.dst, tmp.data(), it.bytes, cudaMemcpyHostToDevice));
+      } else {
+        MEGA_TRY(cudaMemcpyAsync(it.dst, it.src, it.bytes, cudaMemcpyHostToDevice, s));
+      }
+    }
     MEGA_TRY(cudaStreamSynchronize(s));
     return 0;
   }
   size_t off = 0;
   for (const auto& it : items) {  // copy in, then DMA while the next array is copied in
-    host_copy(g_stage.p + off, it.src, it.bytes);
+    if (it.fill) it.fill(g_stage.p + off);
+    else host_copy(g_stage.p + off, it.src, it.bytes);
     MEGA_TRY(cudaMemcpyAsync(it.dst, g_stage.p + off, it.bytes, cudaMemcpyHostToDevice, s));
     off += (it.bytes + 255) & ~(size_t)255;
   }
@@ -891,24 +973,36 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   bool mdamaged = false;
   int mres = 0;
   std::thread mt([&] { mres = material_table(n, props, mat_type, 65535, ments, midx, mdamaged); });
-  std::vector<int8_t> hebc(n3), hbody(n);
-  std::vector<int32_t> hen(n, 0);
-  std::vector<double> v0(n3);
-  host_parallel(n, [&](int64_t lo, int64_t hi) {
-    for (int64_t i = lo; i < hi; ++i) {
-      hbody[i] = (int8_t)(body_id ? body_id[i] : 1);
-      for (int j = 0; j < 3; ++j) {
-        const int64_t m = 3 * i + j;
-        hebc[m] = (int8_t)ebc[m];
-        if (ebc[m] == 1) { v0[m] = 0.0; hen[i] = 1; }  // STATE_INIT.f90:97-105
-        else v0[m] = vinit[m];
-      }
-    }
-  });
+  // fixity codes, body ids, EBC node flags and the initial velocity
+  // (zero on fixed components, STATE_INIT.f90:97-105) are formed straight
+  // into the staging buffer
+  auto fill_ebc = [&](void* d) {
+    int8_t* o = (int8_t*)d;
+    host_parallel(n3, [&](int64_t lo, int64_t hi) { for (int64_t m = lo; m < hi; ++m) o[m] = (int8_t)ebc[m]; });
+  };
+  auto fill_body = [&](void* d) {
+    int8_t* o = (int8_t*)d;
+    host_parallel(n, [&](int64_t lo, int64_t hi) {
+      for (int64_t i = lo; i < hi; ++i) o[i] = (int8_t)(body_id ? body_id[i] : 1);
+    });
+  };
+  auto fill_en = [&](void* d) {
+    int32_t* o = (int32_t*)d;
+    host_parallel(n, [&](int64_t lo, int64_t hi) {
+      for (int64_t i = lo; i < hi; ++i) o[i] = (ebc[3 * i] == 1 || ebc[3 * i + 1] == 1 || ebc[3 * i + 2] == 1);
+    });
+  };
+  auto fill_vel = [&](void* d) {
+    double* o = (double*)d;
+    host_parallel(n3, [&](int64_t lo, int64_t hi) {
+      for (int64_t m = lo; m < hi; ++m) o[m] = ebc[m] == 1 ? 0.0 : vinit[m];
+    });
+  };
   std::vector<HostToDevice> items = {
       {c->coo, coo, 8 * (size_t)n3}, {c->win, win, 8 * (size_t)n3}, {c->vol, vol, 8 * (size_t)n},
-      {c->mass, mass, 8 * (size_t)n3}, {c->ebc, hebc.data(), (size_t)n3}, {c->body_id, hbody.data(), (size_t)n},
-      {c->ebc_nodes, hen.data(), 4 * (size_t)n}, {c->vel, v0.data(), 8 * (size_t)n3}};
+      {c->mass, mass, 8 * (size_t)n3}, {c->ebc, nullptr, (size_t)n3, fill_ebc},
+      {c->body_id, nullptr, (size_t)n, fill_body}, {c->ebc_nodes, nullptr, 4 * (size_t)n, fill_en},
+      {c->vel, nullptr, 8 * (size_t)n3, fill_vel}};
   if (c->sm_len) items.push_back({c->sm_len, sm_len, 48 * (size_t)n});
   tr.mark("fixity");
   const bool up_fail = upload_staged(c->s, items) != 0;
@@ -1195,15 +1289,8 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->rt, c->nbpool, nullptr);
   if (r) return r;
   tr.mark("row_tiles");
-  int32_t cmax = 0;
-  {
-    // the longest column bounds a column tile's set from below
-    std::vector<int64_t> cp(n + 1);
-    MEGA_TRY(cudaMemcpyAsync(cp.data(), c->csr.colptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, c->s));
-    MEGA_TRY(cudaStreamSynchronize(c->s));
-    for (int32_t i = 0; i < n; ++i) cmax = std::max<int32_t>(cmax, (int32_t)(cp[i + 1] - cp[i]));
-  }
-  r = build_tiles(c->s, n, c->csr.colptr, c->csr.trow, m, cmax, c->ct, c->nbpool, nullptr);
+  // the longest column bounds a column tile's set from below
+  r = build_tiles(c->s, n, c->csr.colptr, c->csr.trow, m, c->csr.gmaxc, c->ct, c->nbpool, nullptr);
   if (r) return r;
   tr.mark("column_tiles");
   if (c->prec_mask & 1) {

@@ -114,6 +114,7 @@ struct DevCSR {
   int32_t n = 0;
   int64_t nnz = 0;
   int32_t gmaxn = 0;
+  int32_t gmaxc = 0;          // longest column (set with the transposed view)
   int64_t* rowptr = nullptr;  // n + 1
   int32_t* col = nullptr;     // nnz
   int64_t* colptr = nullptr;  // n + 1

@@ -111,10 +111,9 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
         const int q = sidx(a, b);
         const double hh = e.H[a] * e.H[b];
         M[q] += hh * e.phi;
-        // (Hd H^T + H Hd^T) phi with Hd = unit vector of the axis
-        Mx[q] += hh * e.px + ((a == 1 ? e.H[b] : 0.0) + (b == 1 ? e.H[a] : 0.0)) * e.phi;
-        My[q] += hh * e.py + ((a == 2 ? e.H[b] : 0.0) + (b == 2 ? e.H[a] : 0.0)) * e.phi;
-        Mz[q] += hh * e.pz + ((a == 3 ? e.H[b] : 0.0) + (b == 3 ? e.H[a] : 0.0)) * e.phi;
+        Mx[q] += hh * e.px;
+        My[q] += hh * e.py;
+        Mz[q] += hh * e.pz;
       }
   }
 #pragma unroll
@@ -128,6 +127,18 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
       Mz[k] += __shfl_xor_sync(gm, Mz[k], o);
     }
   }
+  // the basis-derivative part of M_,d: sum (H_,d H^T + H H_,d^T) phi with
+  // H_,d the unit vector e_d adds to entry (a, b) delta(a,d) sum H_b phi +
+  // delta(b,d) sum H_a phi, the first moments M(0, b) and M(0, a) (H_0 = 1)
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = a; b < 4; ++b) {
+      const int q = sidx(a, b);
+      Mx[q] += (a == 1 ? M[sidx(0, b)] : 0.0) + (b == 1 ? M[sidx(0, a)] : 0.0);
+      My[q] += (a == 2 ? M[sidx(0, b)] : 0.0) + (b == 2 ? M[sidx(0, a)] : 0.0);
+      Mz[q] += (a == 3 ? M[sidx(0, b)] : 0.0) + (b == 3 ? M[sidx(0, a)] : 0.0);
+    }
   double Mf[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)

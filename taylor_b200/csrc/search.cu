@@ -10,7 +10,9 @@
 //   4. warp-per-node candidate filter over the 27 cells in BIN_INODE order
 //      (IX outer, IZ inner, BIN_SEARCH.F90:105-127), ballot + popc compaction
 //      so the output rows keep the reference's order exactly;
-//   5. count pass -> scan -> fill pass.
+//   5. one filter pass into per-node candidate slots, scan, compaction
+//      (or, where the slots do not fit in memory and in the allocation-free
+//      entry point, a count pass -> scan -> fill pass).
 // Every floating-point operation of the test uses __d*_rn intrinsics, so no
 // FMA contraction can change a comparison: the lists are bit-exact.
 #include <algorithm>
@@ -63,13 +65,22 @@ __global__ void k_bbox_partial(int32_t n, const double* __restrict__ coo, const 
   }
 }
 
-// HANDELER.F90:221-243 in one thread, with the same IEEE operations.
+// HANDELER.F90:221-243, with the same IEEE operations: one warp reduces the
+// block partials (max is exact in any order), lane 0 forms the geometry.
 __global__ void k_bbox_final(int nb, const double* __restrict__ part, double* __restrict__ geom,
                              int32_t* __restrict__ dims) {
+  const int lane = threadIdx.x & 31;
   double v[9];
-  for (int k = 0; k < 9; ++k) v[k] = part[k];
-  for (int b = 1; b < nb; ++b)
+#pragma unroll
+  for (int k = 0; k < 9; ++k) v[k] = (k < 3) ? 0.0 : -INFINITY;
+  for (int b = lane; b < nb; b += 32)
+#pragma unroll
     for (int k = 0; k < 9; ++k) v[k] = fmax(v[k], part[9 * b + k]);
+#pragma unroll
+  for (int k = 0; k < 9; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] = fmax(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+  if (lane != 0) return;
   const double xbin = v[0], ybin = v[1], zbin = v[2];
   const double xmin = __dsub_rn(-v[6], __dmul_rn(xbin, 10.0));
   const double ymin = __dsub_rn(-v[7], __dmul_rn(ybin, 10.0));
@@ -129,6 +140,14 @@ __global__ void k_cell_sort(int64_t nbins, const int64_t* __restrict__ cstart, i
   }
 }
 
+// dx / w < 1 with the quotient rounded to nearest, decided without the
+// division for w > 0: the largest double below w divided by w is at most
+// 1 - 2^-53, which is a double, so the rounded quotient of any dx < w stays
+// below 1, and dx >= w gives a quotient of at least 1.  (NaN dx fails both.)
+__device__ __forceinline__ bool quotient_below_one(double dx, double w) {
+  return w > 0.0 ? dx < w : __ddiv_rn(dx, w) < 1.0;
+}
+
 // SOFT_SEARCH acceptance test (BIN_SEARCH.F90:235-293), exact arithmetic.
 __device__ __forceinline__ bool accept(const double xi[3], const double xj[3], const double wj[3],
                                        const double sl[6], int mmax, int shsup) {
@@ -148,33 +167,36 @@ __device__ __forceinline__ bool accept(const double xi[3], const double xj[3], c
       const double s = __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c));
       if (__dsqrt_rn(s) < 1.0) return true;
     } else {
-      if (__ddiv_rn(dx, wj[0]) < 1.0 && __ddiv_rn(dy, wj[1]) < 1.0 && __ddiv_rn(dz, wj[2]) < 1.0) return true;
+      if (quotient_below_one(dx, wj[0]) && quotient_below_one(dy, wj[1]) && quotient_below_one(dz, wj[2]))
+        return true;
     }
   }
   return false;
 }
 
-// ---- 4/5. warp per node; FILL = false counts, FILL = true writes the row.
-template <bool FILL>
-__global__ void __launch_bounds__(256) k_soft_search(
-    int32_t n, const double* __restrict__ coo, const double* __restrict__ win, const double* __restrict__ sm_len,
-    const int32_t* __restrict__ cell, int32_t nx, int32_t ny, int32_t nz, const int64_t* __restrict__ cstart,
-    const int32_t* __restrict__ sorted, int mmax, int shsup, int32_t* __restrict__ gn,
-    const int64_t* __restrict__ rowptr, int32_t* __restrict__ col, int32_t* __restrict__ gmaxn,
-    unsigned* __restrict__ status) {
-  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= n) return;  // whole warp leaves together
+// ---- 4/5. warp-per-node filter of node i's candidates.  Lane k < 27 owns
+// neighbour cell k in the reference's visiting order (IX outer, IY, IZ
+// inner; cells outside the grid are empty).  The candidates of all 27 cells
+// form one index range [0, total) walked 32 at a time, so the output keeps
+// the reference order with every lane busy.  SORTED: candidate coordinates
+// and windows come from the cell-sorted copies xs / ws (contiguous within a
+// cell, independent of the index load); otherwise from coo / win by index.
+// WRITE: accepted indices go to out[0 .. count).  Returns the count; the
+// candidate total in *total_out (lane values agree).
+template <bool WRITE, bool SORTED, int MMAX = 0>
+__device__ __forceinline__ int32_t filter_row(int64_t i, int lane, const double* __restrict__ coo,
+                                              const double* __restrict__ win, const double* __restrict__ xs,
+                                              const double* __restrict__ ws, const double* __restrict__ sm_len,
+                                              const int32_t* __restrict__ cell, int32_t nx, int32_t ny, int32_t nz,
+                                              const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted,
+                                              int mmax, int shsup, int32_t* __restrict__ out, int32_t* total_out) {
+  if (MMAX) mmax = MMAX;  // the seven-point test count fixed at compile time
   const double xi[3] = {coo[3 * i], coo[3 * i + 1], coo[3 * i + 2]};
   double sl[6];  // smoothing cells: read only by the seven-point test (mmax = 7)
 #pragma unroll
   for (int k = 0; k < 6; ++k) sl[k] = mmax > 1 ? sm_len[6 * i + k] : 0.0;
   const int32_t m0 = cell[i];
   const int32_t is = m0 % nx + 1, js = (m0 / nx) % ny + 1, ks = m0 / (nx * ny) + 1;
-  // Lane k < 27 owns neighbour cell k in the reference's visiting order (IX
-  // outer, IY, IZ inner; cells outside the grid are empty).  The candidates
-  // of all 27 cells form one index range [0, total) walked 32 at a time, so
-  // the output keeps the reference order with every lane busy.
   int64_t cbeg = 0;
   int32_t clen = 0;
   if (lane < 27) {
@@ -195,8 +217,6 @@ __global__ void __launch_bounds__(256) k_soft_search(
   pre -= clen;  // exclusive
   const unsigned lt = (1u << lane) - 1u;
   int32_t count = 0;
-  const int64_t ncand = total;
-  const int64_t base = FILL ? rowptr[i] : 0;
   for (int32_t c0 = 0; c0 < total; c0 += 32) {
     const int32_t c = c0 + lane;
     bool add = false;
@@ -212,22 +232,107 @@ __global__ void __launch_bounds__(256) k_soft_search(
     const int64_t cb = __shfl_sync(0xffffffffu, cbeg, k);
     const int32_t pk = __shfl_sync(0xffffffffu, pre, k);
     if (c < total) {
-      j = sorted[cb + (c - pk)];
-      const double xj[3] = {coo[3 * (int64_t)j], coo[3 * (int64_t)j + 1], coo[3 * (int64_t)j + 2]};
-      const double wj[3] = {win[3 * (int64_t)j], win[3 * (int64_t)j + 1], win[3 * (int64_t)j + 2]};
+      const int64_t q = cb + (c - pk);
+      j = sorted[q];
+      const int64_t src = SORTED ? q : (int64_t)j;
+      const double* xp = SORTED ? xs : coo;
+      const double* wp = SORTED ? ws : win;
+      const double xj[3] = {xp[3 * src], xp[3 * src + 1], xp[3 * src + 2]};
+      const double wj[3] = {wp[3 * src], wp[3 * src + 1], wp[3 * src + 2]};
       add = accept(xi, xj, wj, sl, mmax, shsup);
     }
     const unsigned b = __ballot_sync(0xffffffffu, add);
-    if (FILL && add) col[base + count + __popc(b & lt)] = j;
+    if (WRITE && add) out[count + __popc(b & lt)] = j;
     count += __popc(b);
   }
-  if (lane == 0) {
-    if (!FILL) {
-      gn[i] = count;
-      atomic_max_int(gmaxn, count);
-      if (ncand > kMaxCandidates) atomicOr(status, (unsigned)MEGA_ST_CAND_OVERFLOW);
-    }
+  *total_out = total;
+  return count;
+}
+
+// FILL = false counts, FILL = true writes the row (two-pass form)
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_soft_search(
+    int32_t n, const double* __restrict__ coo, const double* __restrict__ win, const double* __restrict__ sm_len,
+    const int32_t* __restrict__ cell, int32_t nx, int32_t ny, int32_t nz, const int64_t* __restrict__ cstart,
+    const int32_t* __restrict__ sorted, int mmax, int shsup, int32_t* __restrict__ gn,
+    const int64_t* __restrict__ rowptr, int32_t* __restrict__ col, int32_t* __restrict__ gmaxn,
+    unsigned* __restrict__ status) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;  // whole warp leaves together
+  int32_t total = 0;
+  const int32_t count = filter_row<FILL, false>(i, lane, coo, win, nullptr, nullptr, sm_len, cell, nx, ny, nz, cstart,
+                                                sorted, mmax, shsup, FILL ? col + rowptr[i] : nullptr, &total);
+  if (lane == 0 && !FILL) {
+    gn[i] = count;
+    atomic_max_int(gmaxn, count);
+    if (total > kMaxCandidates) atomicOr(status, (unsigned)MEGA_ST_CAND_OVERFLOW);
   }
+}
+
+// coordinates and windows in cell-sorted order
+__global__ void k_sorted_coords(int32_t n, const int32_t* __restrict__ sorted, const double* __restrict__ coo,
+                                const double* __restrict__ win, double* __restrict__ xs, double* __restrict__ ws) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int64_t j = sorted[q];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    xs[3 * q + k] = coo[3 * j + k];
+    ws[3 * q + k] = win[3 * j + k];
+  }
+}
+
+// candidates of each node: the node counts of its 27 cells
+__global__ void k_cand_count(int32_t n, const int32_t* __restrict__ cell, int32_t nx, int32_t ny, int32_t nz,
+                             const int64_t* __restrict__ cstart, int32_t* __restrict__ cand,
+                             unsigned* __restrict__ status) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t m0 = cell[i];
+  const int32_t is = m0 % nx + 1, js = (m0 / nx) % ny + 1, ks = m0 / (nx * ny) + 1;
+  int64_t t = 0;
+  for (int32_t ix = is - 1; ix <= is + 1; ++ix)
+    for (int32_t iy = js - 1; iy <= js + 1; ++iy)
+      for (int32_t iz = ks - 1; iz <= ks + 1; ++iz)
+        if (ix >= 1 && ix <= nx && iy >= 1 && iy <= ny && iz >= 1 && iz <= nz) {
+          const int64_t m = (int64_t)(iz - 1) * nx * ny + (int64_t)(iy - 1) * nx + (ix - 1);
+          t += cstart[m + 1] - cstart[m];
+        }
+  cand[i] = (int32_t)t;
+  if (t > kMaxCandidates) atomicOr(status, (unsigned)MEGA_ST_CAND_OVERFLOW);
+}
+
+// one filter pass: node i's accepted indices into its candidate slots
+// buf[coff[i] ..), its count into gn[i]; MMAX = 1 (DNI) or 7
+template <int MMAX>
+__global__ void __launch_bounds__(256, MMAX == 1 ? 4 : 3) k_search_once(
+    int32_t n, const double* __restrict__ coo, const double* __restrict__ win, const double* __restrict__ xs,
+    const double* __restrict__ ws, const double* __restrict__ sm_len, const int32_t* __restrict__ cell, int32_t nx,
+    int32_t ny, int32_t nz, const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted, int mmax,
+    int shsup, const int64_t* __restrict__ coff, int32_t* __restrict__ buf, int32_t* __restrict__ gn,
+    int32_t* __restrict__ gmaxn) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  int32_t total = 0;
+  const int32_t count = filter_row<true, true, MMAX>(i, lane, coo, win, xs, ws, sm_len, cell, nx, ny, nz, cstart,
+                                                     sorted, mmax, shsup, buf + coff[i], &total);
+  if (lane == 0) {
+    gn[i] = count;
+    atomic_max_int(gmaxn, count);
+  }
+}
+
+// warp per row: the accepted indices from the candidate slots into the CSR
+__global__ void __launch_bounds__(256) k_compact_rows(int32_t n, const int64_t* __restrict__ coff,
+                                                      const int32_t* __restrict__ buf,
+                                                      const int64_t* __restrict__ rowptr, int32_t* __restrict__ col) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const int64_t a = coff[i], d = rowptr[i], len = rowptr[i + 1] - d;
+  for (int64_t k = lane; k < len; k += 32) col[d + k] = buf[a + k];
 }
 
 // ---- scan helpers
@@ -321,77 +426,58 @@ __global__ void k_col_count(int64_t nnz, const int32_t* __restrict__ col, int32_
   const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p < nnz) atomicAdd(&ccnt[col[p]], 1);
 }
+
+// the largest of n counts into *mx (zeroed by the caller)
+__global__ void k_max_count(int32_t n, const int32_t* __restrict__ cnt, int32_t* __restrict__ mx) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int32_t v = i < n ? cnt[i] : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v > 0) atomicMax(mx, v);
+}
+// Entry (i, j) of the lists into column j at an arbitrary free slot: its row
+// i and its offset inside row i (the order is restored by k_col_sort).
 __global__ void k_col_scatter(int32_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
                               const int64_t* __restrict__ colptr, int32_t* __restrict__ cfill,
-                              int64_t* __restrict__ tpos, int32_t* __restrict__ trow) {
+                              int32_t* __restrict__ toff, int32_t* __restrict__ trow) {
   const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (i >= n) return;
-  for (int64_t p = rowptr[i] + lane; p < rowptr[i + 1]; p += 32) {
+  const int64_t r0 = rowptr[i];
+  for (int64_t p = r0 + lane; p < rowptr[i + 1]; p += 32) {
     const int32_t j = col[p];
     const int64_t e = colptr[j] + atomicAdd(&cfill[j], 1);
-    tpos[e] = p;
+    toff[e] = (int32_t)(p - r0);
     trow[e] = (int32_t)i;
   }
 }
-// Order each column by CSR position (equivalently by row, rows being
-// contiguous and ascending), so the CSC sums are deterministic.  Warp per
-// column: up to kSortCap entries are sorted in registers by a bitonic network
-// (element e = k * 32 + lane, 4 per lane; cross-lane stages by shuffles, the
-// others between a lane's own registers); longer columns fall back to an
-// insertion sort by one lane.
-constexpr int kSortPer = 4;
-constexpr int kSortCap = 32 * kSortPer;
 
-__global__ void __launch_bounds__(256) k_col_sort(int32_t n, const int64_t* __restrict__ colptr,
-                                                  int64_t* __restrict__ tpos, int32_t* __restrict__ trow) {
-  const int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (j >= n) return;
-  const int64_t s = colptr[j], e = colptr[j + 1];
-  const int64_t len = e - s;
-  if (len <= 1) return;
-  if (len > kSortCap) {
-    if (lane == 0) {
-      for (int64_t a = s + 1; a < e; ++a) {
-        const int64_t v = tpos[a];
-        const int32_t r = trow[a];
-        int64_t b = a - 1;
-        while (b >= s && tpos[b] > v) { tpos[b + 1] = tpos[b]; trow[b + 1] = trow[b]; --b; }
-        tpos[b + 1] = v;
-        trow[b + 1] = r;
-      }
-    }
-    return;
-  }
-  long long key[kSortPer];
-  int32_t val[kSortPer];
+// Bitonic sort of 32 * PER (row, offset) pairs by row across one warp:
+// element e = k * 32 + lane; stages of stride >= 32 compare a lane's own
+// registers, the others exchange by shuffles.  Rows are distinct within a
+// column, so the order is total.
+template <int PER>
+__device__ __forceinline__ void warp_bitonic(int32_t (&key)[PER], int32_t (&val)[PER], int lane) {
 #pragma unroll
-  for (int k = 0; k < kSortPer; ++k) {
-    const int idx = k * 32 + lane;
-    key[k] = idx < len ? (long long)tpos[s + idx] : LLONG_MAX;
-    val[k] = idx < len ? trow[s + idx] : 0;
-  }
-#pragma unroll
-  for (int size = 2; size <= kSortCap; size <<= 1) {
+  for (int size = 2; size <= 32 * PER; size <<= 1) {
 #pragma unroll
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
       if (stride >= 32) {
         const int ks = stride >> 5;
 #pragma unroll
-        for (int k = 0; k < kSortPer; ++k) {
+        for (int k = 0; k < PER; ++k) {
           if (k & ks) continue;
           const int k2 = k | ks;
           const bool up = ((k * 32 + lane) & size) == 0;
           if ((key[k] > key[k2]) == up) {
-            const long long tk = key[k]; key[k] = key[k2]; key[k2] = tk;
+            const int32_t tk = key[k]; key[k] = key[k2]; key[k2] = tk;
             const int32_t tv = val[k]; val[k] = val[k2]; val[k2] = tv;
           }
         }
       } else {
 #pragma unroll
-        for (int k = 0; k < kSortPer; ++k) {
-          const long long ok = __shfl_xor_sync(0xffffffffu, key[k], stride);
+        for (int k = 0; k < PER; ++k) {
+          const int32_t ok = __shfl_xor_sync(0xffffffffu, key[k], stride);
           const int32_t ov = __shfl_xor_sync(0xffffffffu, val[k], stride);
           const bool up = ((k * 32 + lane) & size) == 0;
           const bool lower = (lane & stride) == 0;
@@ -401,10 +487,57 @@ __global__ void __launch_bounds__(256) k_col_sort(int32_t n, const int64_t* __re
       }
     }
   }
+}
+
+template <int PER>
+__device__ __forceinline__ void sort_column(int64_t s, int64_t len, int lane, const int64_t* __restrict__ rowptr,
+                                            const int32_t* __restrict__ toff, int64_t* __restrict__ tpos,
+                                            int32_t* __restrict__ trow) {
+  int32_t key[PER], val[PER];
 #pragma unroll
-  for (int k = 0; k < kSortPer; ++k) {
+  for (int k = 0; k < PER; ++k) {
     const int idx = k * 32 + lane;
-    if (idx < len) { tpos[s + idx] = (int64_t)key[k]; trow[s + idx] = val[k]; }
+    key[k] = idx < len ? trow[s + idx] : INT_MAX;
+    val[k] = idx < len ? toff[s + idx] : 0;
+  }
+  warp_bitonic<PER>(key, val, lane);
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int idx = k * 32 + lane;
+    if (idx < len) {
+      trow[s + idx] = key[k];
+      tpos[s + idx] = rowptr[key[k]] + val[k];
+    }
+  }
+}
+
+// Order each column by row (equivalently by CSR position, rows being
+// contiguous and ascending), so the CSC sums are deterministic, and form
+// the CSR position of every entry.  Warp per column: up to 256 entries
+// sorted in registers by a network sized to the column; longer columns by
+// one lane's insertion sort.
+__global__ void __launch_bounds__(256) k_col_sort(int32_t n, const int64_t* __restrict__ colptr,
+                                                  const int64_t* __restrict__ rowptr,
+                                                  const int32_t* __restrict__ toff, int64_t* __restrict__ tpos,
+                                                  int32_t* __restrict__ trow) {
+  const int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= n) return;
+  const int64_t s = colptr[j], e = colptr[j + 1];
+  const int64_t len = e - s;
+  if (len <= 32) sort_column<1>(s, len, lane, rowptr, toff, tpos, trow);
+  else if (len <= 64) sort_column<2>(s, len, lane, rowptr, toff, tpos, trow);
+  else if (len <= 128) sort_column<4>(s, len, lane, rowptr, toff, tpos, trow);
+  else if (len <= 256) sort_column<8>(s, len, lane, rowptr, toff, tpos, trow);
+  else if (lane == 0) {
+    for (int64_t a = s; a < e; ++a) {
+      const int32_t r = trow[a];
+      const int64_t v = rowptr[r] + toff[a];
+      int64_t b = a - 1;
+      while (b >= s && trow[b] > r) { tpos[b + 1] = tpos[b]; trow[b + 1] = trow[b]; --b; }
+      tpos[b + 1] = v;
+      trow[b + 1] = r;
+    }
   }
 }
 
@@ -448,7 +581,7 @@ int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, 
   } else {
     k_bbox_partial<<<nbb, 256, 0, s>>>(n, coo, win, dist_max[0], dist_max[1], dist_max[2], part);
     MEGA_CHECK_LAUNCH();
-    k_bbox_final<<<1, 1, 0, s>>>(nbb, part, geom, dims);
+    k_bbox_final<<<1, 32, 0, s>>>(nbb, part, geom, dims);
     MEGA_CHECK_LAUNCH();
     MEGA_TRY(cudaMemcpyAsync(bg.g, geom, sizeof(double) * 6, cudaMemcpyDeviceToHost, s));
     int32_t hd[3];
@@ -487,8 +620,38 @@ int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, 
   MEGA_TRY(cudaMemsetAsync(gmaxn, 0, sizeof(int32_t), s));
   MEGA_ALLOC(pool, csr.rowptr, (int64_t)n + 1);
   const unsigned gw = grid_for((int64_t)n * 32, 256);
-  k_soft_search<false><<<gw, 256, 0, s>>>(n, coo, win, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax,
-                                          shsup, gn, nullptr, nullptr, gmaxn, status);
+  // One filter pass into per-node candidate slots (4 bytes per candidate,
+  // about 27 cells x 8 nodes per node), then a compaction; the two-pass form
+  // where the slots do not fit.
+  int32_t* cand = nullptr;
+  int64_t* coff = nullptr;
+  MEGA_ALLOC(scratch, cand, n);
+  MEGA_ALLOC(scratch, coff, (int64_t)n + 1);
+  k_cand_count<<<grid_for(n, 256), 256, 0, s>>>(n, cell, bg.nx, bg.ny, bg.nz, cstart, cand, status);
+  MEGA_CHECK_LAUNCH();
+  r = scan_counts(s, cand, coff, n, scratch);
+  if (r) return r;
+  int64_t ctot = 0;
+  MEGA_TRY(cudaMemcpyAsync(&ctot, coff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaStreamSynchronize(s));
+  int32_t* buf = nullptr;
+  double *xs = nullptr, *ws = nullptr;
+  size_t fr = 0, tot = 0;
+  const bool once = cudaMemGetInfo(&fr, &tot) == cudaSuccess &&
+                    (size_t)ctot * sizeof(int32_t) + 48 * (size_t)n + ((size_t)1 << 30) < fr;
+  if (once) {
+    MEGA_ALLOC(scratch, buf, ctot);
+    MEGA_ALLOC(scratch, xs, 3 * (int64_t)n);
+    MEGA_ALLOC(scratch, ws, 3 * (int64_t)n);
+    k_sorted_coords<<<grid_for(n, 256), 256, 0, s>>>(n, sorted, coo, win, xs, ws);
+    MEGA_CHECK_LAUNCH();
+    auto k = mmax == 1 ? k_search_once<1> : k_search_once<7>;
+    k<<<gw, 256, 0, s>>>(n, coo, win, xs, ws, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax, shsup, coff, buf,
+                         gn, gmaxn);
+  } else {
+    k_soft_search<false><<<gw, 256, 0, s>>>(n, coo, win, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax,
+                                            shsup, gn, nullptr, nullptr, gmaxn, status);
+  }
   MEGA_CHECK_LAUNCH();
   r = scan_counts(s, gn, csr.rowptr, n, scratch);
   if (r) return r;
@@ -498,8 +661,11 @@ int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, 
   MEGA_TRY(cudaStreamSynchronize(s));
   csr.nnz = nnz;
   MEGA_ALLOC(pool, csr.col, nnz);
-  k_soft_search<true><<<gw, 256, 0, s>>>(n, coo, win, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax,
-                                         shsup, gn, csr.rowptr, csr.col, gmaxn, status);
+  if (once)
+    k_compact_rows<<<gw, 256, 0, s>>>(n, coff, buf, csr.rowptr, csr.col);
+  else
+    k_soft_search<true><<<gw, 256, 0, s>>>(n, coo, win, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax,
+                                           shsup, gn, csr.rowptr, csr.col, gmaxn, status);
   MEGA_CHECK_LAUNCH();
   MEGA_TRY(cudaStreamSynchronize(s));
   return 0;
@@ -509,22 +675,30 @@ int build_transpose(cudaStream_t s, DevCSR& csr, DevPool& pool) {
   DevPool scratch(s);
   const int32_t n = csr.n;
   int32_t *ccnt = nullptr, *cfill = nullptr;
+  int32_t* cmax = nullptr;
   MEGA_ALLOC(scratch, ccnt, n);
   MEGA_ALLOC(scratch, cfill, n);
+  MEGA_ALLOC(scratch, cmax, 1);
   MEGA_ALLOC(pool, csr.colptr, (int64_t)n + 1);
   MEGA_ALLOC(pool, csr.trow, csr.nnz);
   MEGA_ALLOC(pool, csr.tpos, csr.nnz);
   MEGA_TRY(cudaMemsetAsync(ccnt, 0, sizeof(int32_t) * n, s));
   MEGA_TRY(cudaMemsetAsync(cfill, 0, sizeof(int32_t) * n, s));
+  MEGA_TRY(cudaMemsetAsync(cmax, 0, sizeof(int32_t), s));
   k_col_count<<<grid_for(csr.nnz, 256), 256, 0, s>>>(csr.nnz, csr.col, ccnt);
+  MEGA_CHECK_LAUNCH();
+  k_max_count<<<grid_for(n, 256), 256, 0, s>>>(n, ccnt, cmax);
   MEGA_CHECK_LAUNCH();
   int r = scan_counts(s, ccnt, csr.colptr, n, scratch);
   if (r) return r;
-  k_col_scatter<<<grid_for((int64_t)n * 32, 256), 256, 0, s>>>(n, csr.rowptr, csr.col, csr.colptr, cfill, csr.tpos,
+  int32_t* toff = nullptr;
+  MEGA_ALLOC(scratch, toff, csr.nnz);
+  k_col_scatter<<<grid_for((int64_t)n * 32, 256), 256, 0, s>>>(n, csr.rowptr, csr.col, csr.colptr, cfill, toff,
                                                               csr.trow);
   MEGA_CHECK_LAUNCH();
-  k_col_sort<<<grid_for((int64_t)n * 32, 256), 256, 0, s>>>(n, csr.colptr, csr.tpos, csr.trow);
+  k_col_sort<<<grid_for((int64_t)n * 32, 256), 256, 0, s>>>(n, csr.colptr, csr.rowptr, toff, csr.tpos, csr.trow);
   MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaMemcpyAsync(&csr.gmaxc, cmax, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaStreamSynchronize(s));
   return 0;
 }
@@ -670,7 +844,7 @@ extern "C" int mega_bin_search_noalloc(int32_t n, const double* d_coo, const dou
   const int64_t head = cv.used;
   k_bbox_partial<<<nbb, 256, 0, s>>>(n, d_coo, d_win, dist_max[0], dist_max[1], dist_max[2], part);
   MEGA_CHECK_LAUNCH();
-  k_bbox_final<<<1, 1, 0, s>>>(nbb, part, geom, dims);
+  k_bbox_final<<<1, 32, 0, s>>>(nbb, part, geom, dims);
   MEGA_CHECK_LAUNCH();
   int32_t hd[3];
   MEGA_TRY(cudaMemcpyAsync(hd, dims, sizeof(hd), cudaMemcpyDeviceToHost, s));
