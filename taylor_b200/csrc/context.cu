@@ -304,12 +304,34 @@ int upload_staged(cudaStream_t s, const std::vector<HostToDevice>& items) {
     MEGA_TRY(cudaStreamSynchronize(s));
     return 0;
   }
+  // Pieces of at most 4 MiB (a filled array is one piece), each copied into
+  // its place in the stage by a pool thread and sent as soon as it is there,
+  // so the DMA runs while the host is still copying the rest.
+  struct Piece { const HostToDevice* it; size_t at, bytes; unsigned char* stage; };
+  constexpr size_t kPiece = (size_t)4 << 20;
+  std::vector<Piece> pieces;
   size_t off = 0;
-  for (const auto& it : items) {  // copy in, then DMA while the next array is copied in
-    if (it.fill) it.fill(g_stage.p + off);
-    else host_copy(g_stage.p + off, it.src, it.bytes);
-    MEGA_TRY(cudaMemcpyAsync(it.dst, g_stage.p + off, it.bytes, cudaMemcpyHostToDevice, s));
+  for (const auto& it : items) {
+    if (it.fill) pieces.push_back({&it, 0, it.bytes, g_stage.p + off});
+    else
+      for (size_t a = 0; a < it.bytes; a += kPiece)
+        pieces.push_back({&it, a, std::min(kPiece, it.bytes - a), g_stage.p + off + a});
     off += (it.bytes + 255) & ~(size_t)255;
+  }
+  std::atomic<int> err(0);
+  host_parallel((int64_t)pieces.size(), [&](int64_t lo, int64_t hi) {
+    for (int64_t k = lo; k < hi; ++k) {
+      const Piece& pc = pieces[k];
+      if (pc.it->fill) pc.it->fill(pc.stage);
+      else std::memcpy(pc.stage, (const unsigned char*)pc.it->src + pc.at, pc.bytes);
+      const cudaError_t e = cudaMemcpyAsync((unsigned char*)pc.it->dst + pc.at, pc.stage, pc.bytes,
+                                            cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) err.store((int)e);
+    }
+  }, 1);
+  if (err.load()) {
+    record_cuda_error((cudaError_t)err.load(), "cudaMemcpyAsync", __FILE__, __LINE__);
+    return MEGA_ERR_CUDA;
   }
   MEGA_TRY(cudaStreamSynchronize(s));
   return 0;
@@ -712,6 +734,118 @@ void retain_pool_memory() {
     cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
   }
   done.insert(dev);
+}
+
+namespace {
+struct CachedBlock {
+  void* p;
+  size_t bytes;
+  int dev;
+  cudaEvent_t ev;  // recorded after the block's last use
+};
+std::mutex g_blk_mu;
+std::multimap<size_t, CachedBlock> g_blk;  // by block size
+size_t g_blk_total = 0;
+
+// 512-byte granularity below 1 MiB, 2 MiB above (a re-search whose list
+// grew by a few entries still finds its old block)
+size_t block_round(size_t b) {
+  if (b < ((size_t)1 << 20)) return (b + 511) & ~(size_t)511;
+  const size_t g = (size_t)2 << 20;
+  return (b + g - 1) / g * g;
+}
+
+// hand every cached block of device dev back to the memory pool
+void flush_blocks(int dev, cudaStream_t s) {
+  std::vector<CachedBlock> out;
+  {
+    std::lock_guard<std::mutex> lk(g_blk_mu);
+    for (auto it = g_blk.begin(); it != g_blk.end();) {
+      if (it->second.dev == dev) {
+        out.push_back(it->second);
+        g_blk_total -= it->second.bytes;
+        it = g_blk.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+  for (auto& b : out) {
+    cudaStreamWaitEvent(s, b.ev, 0);
+    cudaEventDestroy(b.ev);
+    cudaFreeAsync(b.p, s);
+  }
+}
+}  // namespace
+
+int cached_alloc(void** p, size_t bytes, cudaStream_t s, size_t* got) {
+  const size_t want = block_round(bytes);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::unique_lock<std::mutex> lk(g_blk_mu);
+    for (auto it = g_blk.lower_bound(want); it != g_blk.end() && it->first <= want + want / 4; ++it) {
+      if (it->second.dev != dev) continue;
+      const CachedBlock b = it->second;
+      g_blk.erase(it);
+      g_blk_total -= b.bytes;
+      lk.unlock();
+      cudaStreamWaitEvent(s, b.ev, 0);
+      cudaEventDestroy(b.ev);
+      *p = b.p;
+      *got = b.bytes;
+      return 0;
+    }
+  }
+  cudaError_t e = cudaMallocAsync(p, want, s);
+  if (e != cudaSuccess) {  // give the cache back to the pool and try once more
+    cudaGetLastError();
+    flush_blocks(dev, s);
+    e = cudaMallocAsync(p, want, s);
+  }
+  if (e != cudaSuccess) {
+    record_cuda_error(e, "cudaMallocAsync", __FILE__, __LINE__);
+    *p = nullptr;
+    return MEGA_ERR_NOMEM;
+  }
+  *got = want;
+  return 0;
+}
+
+void cached_free(void* p, size_t block_bytes, cudaStream_t s) {
+  if (!p) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaEvent_t ev = nullptr;
+  if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess || cudaEventRecord(ev, s) != cudaSuccess) {
+    cudaGetLastError();
+    if (ev) cudaEventDestroy(ev);
+    cudaFreeAsync(p, s);
+    return;
+  }
+  // at most a quarter of the device's memory waits in the cache
+  size_t fr = 0, tot = 0;
+  static size_t cap = 0;
+  if (!cap && cudaMemGetInfo(&fr, &tot) == cudaSuccess) cap = tot / 4;
+  std::vector<CachedBlock> evict;
+  {
+    std::lock_guard<std::mutex> lk(g_blk_mu);
+    g_blk.emplace(block_bytes, CachedBlock{p, block_bytes, dev, ev});
+    g_blk_total += block_bytes;
+    // the largest blocks of this device go first
+    for (auto it = g_blk.end(); cap && g_blk_total > cap && it != g_blk.begin();) {
+      --it;
+      if (it->second.dev != dev) continue;
+      evict.push_back(it->second);
+      g_blk_total -= it->second.bytes;
+      it = g_blk.erase(it);
+    }
+  }
+  for (auto& b : evict) {
+    cudaStreamWaitEvent(s, b.ev, 0);
+    cudaEventDestroy(b.ev);
+    cudaFreeAsync(b.p, s);
+  }
 }
 
 struct StreamGuard {

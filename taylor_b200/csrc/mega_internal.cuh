@@ -37,12 +37,22 @@ void retain_pool_memory();
 bool trace_on();
 void trace_alloc(size_t bytes, double ms, bool ordered);
 
+// Stream-ordered device blocks kept for reuse by the process: a freed block
+// waits in a cache (with an event marking the end of its last use) and a
+// later request of about its size, on any stream, takes it after waiting on
+// that event.  Set-up passes that run again with the same sizes (a new
+// context on the same model, a re-search) then reach no driver allocation,
+// whose cost grows with the pool's fragmentation.  *got = the block's size.
+int cached_alloc(void** p, size_t bytes, cudaStream_t s, size_t* got);
+void cached_free(void* p, size_t block_bytes, cudaStream_t s);
+
 // Device allocations owned by one object; freed together.  A pool bound to a
-// stream allocates and frees in that stream's order from the device's memory
-// pool (cudaMallocAsync / cudaFreeAsync): every user of its memory must run
-// on that stream.  An unbound pool uses cudaMalloc / cudaFree.
+// stream allocates and frees in that stream's order (through the block cache
+// over cudaMallocAsync / cudaFreeAsync): every user of its memory must run on
+// that stream.  An unbound pool uses cudaMalloc / cudaFree.
 struct DevPool {
   std::vector<void*> ptrs;
+  std::vector<size_t> blocks;  // block size of each pointer (bound pools)
   int64_t bytes = 0;
   cudaStream_t stream = nullptr;
   bool ordered = false;
@@ -61,8 +71,13 @@ struct DevPool {
     if (count == 0) count = 1;
     const bool tr = trace_on();
     const auto t0 = tr ? std::chrono::steady_clock::now() : std::chrono::steady_clock::time_point();
-    cudaError_t e = ordered ? cudaMallocAsync((void**)p, count * sizeof(T), stream)
-                            : cudaMalloc((void**)p, count * sizeof(T));
+    size_t blk = count * sizeof(T);
+    cudaError_t e = cudaSuccess;
+    if (ordered) {
+      if (cached_alloc((void**)p, count * sizeof(T), stream, &blk)) e = cudaErrorMemoryAllocation;
+    } else {
+      e = cudaMalloc((void**)p, count * sizeof(T));
+    }
     if (tr) {
       if (ordered) cudaStreamSynchronize(stream);
       trace_alloc(count * sizeof(T),
@@ -74,27 +89,38 @@ struct DevPool {
       return MEGA_ERR_NOMEM;
     }
     ptrs.push_back((void*)*p);
+    blocks.push_back(blk);
     bytes += (int64_t)(count * sizeof(T));
     return 0;
   }
-  void drop(void* p) {
-    if (ordered) cudaFreeAsync(p, stream);
+  void drop(void* p, size_t blk) {
+    if (ordered) cached_free(p, blk, stream);
     else cudaFree(p);
   }
   void release(void* p) {
     for (size_t k = 0; k < ptrs.size(); ++k)
-      if (ptrs[k] == p) { drop(p); ptrs.erase(ptrs.begin() + k); return; }
+      if (ptrs[k] == p) {
+        drop(p, blocks[k]);
+        ptrs.erase(ptrs.begin() + k);
+        blocks.erase(blocks.begin() + k);
+        return;
+      }
   }
   // move every allocation of o into this pool (same binding required)
   void adopt(DevPool& o) {
-    for (void* p : o.ptrs) ptrs.push_back(p);
+    for (size_t k = 0; k < o.ptrs.size(); ++k) {
+      ptrs.push_back(o.ptrs[k]);
+      blocks.push_back(o.blocks[k]);
+    }
     bytes += o.bytes;
     o.ptrs.clear();
+    o.blocks.clear();
     o.bytes = 0;
   }
   void free_all() {
-    for (void* p : ptrs) drop(p);
+    for (size_t k = 0; k < ptrs.size(); ++k) drop(ptrs[k], blocks[k]);
     ptrs.clear();
+    blocks.clear();
     bytes = 0;
   }
   ~DevPool() { free_all(); }

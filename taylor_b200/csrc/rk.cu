@@ -9,12 +9,19 @@
 // correction vectors b = e1 M^-1 and b_,x = -e1 M^-1 M_,x M^-1
 // (RK.f90:311-342), and finally phi_J = (b.H~)phi, grad phi_J =
 // (b_,x.H~ + b.H_,x)phi + (b.H~)phi_,x (RK.f90:346-405).
-// A group of kLPN lanes serves one node: the lanes stride the neighbour list
-// and accumulate the 4 symmetric 4x4 matrices, a butterfly reduction within
-// the group leaves the sums in every lane, each lane of the group inverts
-// redundantly (no shared memory), then the lanes write their own entries.
-// kLPN = 8 keeps the redundant per-node work to 8 copies while the ~60
-// neighbours still give every lane several entries.
+// Three kernels, so that none carries the registers of the others (one
+// kernel holding the 41 sums, the inverse and the correction vectors at once
+// ran at 12 resident warps per SM):
+//   k_rk_moments  a group of kLPN lanes per node strides the neighbour list
+//                 and accumulates psum and the 4 symmetric 4x4 matrices M,
+//                 M_,x, M_,y, M_,z (41 sums), reduced by a butterfly in the
+//                 group and stored per node;
+//   k_rk_solve    thread per node: the basis-derivative part of M_,d, the
+//                 QL term, the inverse and the correction vectors (16 values
+//                 per node);
+//   k_rk_values   a group per node again: phi_J and grad phi_J per entry.
+// kLPN = 8 lanes per node: the ~60 neighbours still give every lane several
+// entries.
 #include "mega_internal.cuh"
 
 namespace mega {
@@ -74,25 +81,32 @@ __device__ __forceinline__ int sidx(int j, int k) {
 }
 
 constexpr int kLPN = 8;  // lanes per node
+constexpr int kMom = 41;  // psum, M, M_,x, M_,y, M_,z (10 packed values each)
 
-__global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __restrict__ coo,
-                                                   const double* __restrict__ win,
-                                                   const int32_t* __restrict__ ebc_nodes,
-                                                   const int64_t* __restrict__ rowptr,
-                                                   const int32_t* __restrict__ col, int ql, double ql_coef,
-                                                   double ql_len, int shsup, const double* __restrict__ sml,
-                                                   int face, double* __restrict__ shp,
-                                                   double* __restrict__ gx, double* __restrict__ gy,
-                                                   double* __restrict__ gz, unsigned* __restrict__ status) {
+// the node's position, or a face point of its smoothing cell, x +- SM_LEN
+// (face 0..5: +X, -X, +Y, -Y, +Z, -Z)
+__device__ __forceinline__ void node_point(int64_t i, const double* __restrict__ coo,
+                                           const double* __restrict__ sml, int face, double xi[3]) {
+  xi[0] = coo[3 * i]; xi[1] = coo[3 * i + 1]; xi[2] = coo[3 * i + 2];
+  if (face >= 0) {
+    const int ax = face >> 1;
+    xi[ax] = (face & 1) ? xi[ax] - sml[6 * i + face] : xi[ax] + sml[6 * i + face];
+  }
+}
+
+__global__ void __launch_bounds__(128) k_rk_moments(int32_t n, const double* __restrict__ coo,
+                                                    const double* __restrict__ win,
+                                                    const int32_t* __restrict__ ebc_nodes,
+                                                    const int64_t* __restrict__ rowptr,
+                                                    const int32_t* __restrict__ col, int shsup,
+                                                    const double* __restrict__ sml, int face,
+                                                    double* __restrict__ mom) {
   const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kLPN;
   const int lane = threadIdx.x & (kLPN - 1);
   const unsigned gm = ((1u << kLPN) - 1u) << (threadIdx.x & (32 - kLPN));
   if (i >= n) return;  // whole groups leave together
-  double xi[3] = {coo[3 * i], coo[3 * i + 1], coo[3 * i + 2]};
-  if (face >= 0) {  // a face point of the smoothing cell, x +- SM_LEN (+X, -X, +Y, -Y, +Z, -Z)
-    const int ax = face >> 1;
-    xi[ax] = (face & 1) ? xi[ax] - sml[6 * i + face] : xi[ax] + sml[6 * i + face];
-  }
+  double xi[3];
+  node_point(i, coo, sml, face, xi);
   const int64_t p0 = rowptr[i], p1 = rowptr[i + 1];
   double M[10], Mx[10], My[10], Mz[10], psum = 0.0;
 #pragma unroll
@@ -127,6 +141,27 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
       Mz[k] += __shfl_xor_sync(gm, Mz[k], o);
     }
   }
+  // every lane holds the sums; lane l stores values l, l + kLPN, ...
+  double* o = mom + kMom * i;
+#pragma unroll
+  for (int v = 0; v < kMom; ++v) {
+    if ((v & (kLPN - 1)) != lane) continue;
+    o[v] = v == 0 ? psum : (v <= 10 ? M[v - 1] : (v <= 20 ? Mx[v - 11] : (v <= 30 ? My[v - 21] : Mz[v - 31])));
+  }
+}
+
+// thread per node: bv[16 i ..] = b, b_,x, b_,y, b_,z
+__global__ void __launch_bounds__(128) k_rk_solve(int32_t n, const double* __restrict__ coo, int ql, double ql_coef,
+                                                  double ql_len, const double* __restrict__ sml, int face,
+                                                  const double* __restrict__ mom, double* __restrict__ bv,
+                                                  unsigned* __restrict__ status) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* m = mom + kMom * i;
+  const double psum = m[0];
+  double M[10], Mx[10], My[10], Mz[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) { M[k] = m[1 + k]; Mx[k] = m[11 + k]; My[k] = m[21 + k]; Mz[k] = m[31 + k]; }
   // the basis-derivative part of M_,d: sum (H_,d H^T + H H_,d^T) phi with
   // H_,d the unit vector e_d adds to entry (a, b) delta(a,d) sum H_b phi +
   // delta(b,d) sum H_a phi, the first moments M(0, b) and M(0, a) (H_0 = 1)
@@ -144,13 +179,14 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) Mf[a][b] = M[sidx(a, b)];
-  double Hs[4] = {0.0, 0.0, 0.0, 0.0};
   if (ql) {
     // RK.f90:253-301: the six points X +- QL_LEN e_d, differences evaluated
     // in floating point as the reference does
+    double xi[3];
+    node_point(i, coo, sml, face, xi);
     double d[6][3];
 #pragma unroll
-    for (int m = 0; m < 6; ++m) { d[m][0] = 0.0; d[m][1] = 0.0; d[m][2] = 0.0; }
+    for (int k = 0; k < 6; ++k) { d[k][0] = 0.0; d[k][1] = 0.0; d[k][2] = 0.0; }
     d[0][0] = xi[0] - (xi[0] + ql_len); d[1][0] = xi[0] - (xi[0] - ql_len);
     d[2][1] = xi[1] - (xi[1] + ql_len); d[3][1] = xi[1] - (xi[1] - ql_len);
     d[4][2] = xi[2] - (xi[2] + ql_len); d[5][2] = xi[2] - (xi[2] - ql_len);
@@ -160,13 +196,12 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
 #pragma unroll
       for (int b = 0; b < 4; ++b) Ms[a][b] = 0.0;
 #pragma unroll
-    for (int m = 0; m < 6; ++m) {
-      const double H[4] = {1.0, d[m][0], d[m][1], d[m][2]};
+    for (int k = 0; k < 6; ++k) {
+      const double H[4] = {1.0, d[k][0], d[k][1], d[k][2]};
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) Ms[a][b] += H[a] * H[b];
-      Hs[0] += 1.0; Hs[1] += d[m][0]; Hs[2] += d[m][1]; Hs[3] += d[m][2];
     }
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -175,26 +210,57 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
   }
   double Mi[4][4];
   const double det = m44inv(Mf, Mi);
-  if (lane == 0 && (!isfinite(det) || det == 0.0)) atomicOr(status, (unsigned)MEGA_ST_SINGULAR_MOMENT);
-  double B[4], BX[4], BY[4], BZ[4];
+  if (!isfinite(det) || det == 0.0) atomicOr(status, (unsigned)MEGA_ST_SINGULAR_MOMENT);
+  double B[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) B[k] = Mi[0][k];
+  double* o = bv + 16 * i;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) o[k] = B[k];
   // b_,d = -(b M_,d) M^-1
-  double t[4];
 #pragma unroll
   for (int dd = 0; dd < 3; ++dd) {
     const double* Md = dd == 0 ? Mx : (dd == 1 ? My : Mz);
+    double t[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      double s = 0.0;
+      double sacc = 0.0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) s += B[q] * Md[sidx(q, k)];
-      t[k] = -s;
+      for (int q = 0; q < 4; ++q) sacc += B[q] * Md[sidx(q, k)];
+      t[k] = -sacc;
     }
-    double* out = dd == 0 ? BX : (dd == 1 ? BY : BZ);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) out[k] = t[0] * Mi[0][k] + t[1] * Mi[1][k] + t[2] * Mi[2][k] + t[3] * Mi[3][k];
+    for (int k = 0; k < 4; ++k)
+      o[4 + 4 * dd + k] = t[0] * Mi[0][k] + t[1] * Mi[1][k] + t[2] * Mi[2][k] + t[3] * Mi[3][k];
   }
+}
+
+__global__ void __launch_bounds__(128) k_rk_values(int32_t n, const double* __restrict__ coo,
+                                                   const double* __restrict__ win,
+                                                   const int32_t* __restrict__ ebc_nodes,
+                                                   const int64_t* __restrict__ rowptr,
+                                                   const int32_t* __restrict__ col, int ql, double ql_coef,
+                                                   double ql_len, int shsup, const double* __restrict__ sml,
+                                                   int face, const double* __restrict__ bv,
+                                                   double* __restrict__ shp, double* __restrict__ gx,
+                                                   double* __restrict__ gy, double* __restrict__ gz) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kLPN;
+  const int lane = threadIdx.x & (kLPN - 1);
+  if (i >= n) return;
+  double xi[3];
+  node_point(i, coo, sml, face, xi);
+  double Hs[4] = {0.0, 0.0, 0.0, 0.0};
+  if (ql) {  // the QL shift of the basis, RK.f90:357-377
+    Hs[0] = 6.0;
+    Hs[1] = (xi[0] - (xi[0] + ql_len)) + (xi[0] - (xi[0] - ql_len));
+    Hs[2] = (xi[1] - (xi[1] + ql_len)) + (xi[1] - (xi[1] - ql_len));
+    Hs[3] = (xi[2] - (xi[2] + ql_len)) + (xi[2] - (xi[2] - ql_len));
+  }
+  const double* b = bv + 16 * i;
+  double B[4], BX[4], BY[4], BZ[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) { B[k] = b[k]; BX[k] = b[4 + k]; BY[k] = b[8 + k]; BZ[k] = b[12 + k]; }
+  const int64_t p0 = rowptr[i], p1 = rowptr[i + 1];
   for (int64_t p = p0 + lane; p < p1; p += kLPN) {
     const int64_t j = col[p];
     const double xj[3] = {coo[3 * j], coo[3 * j + 1], coo[3 * j + 2]};
@@ -215,30 +281,40 @@ __global__ void __launch_bounds__(128) k_rk_shapes(int32_t n, const double* __re
   }
 }
 
+// the three kernels in order on stream s, with their per-node scratch
+int rk_run(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
+           const int32_t* ebc_nodes, const DevCSR& csr, const double* sml, int face, double* shp, double* gx,
+           double* gy, double* gz, unsigned* status) {
+  if (p.rk_degree != 1 || p.rk_cont != 3) return MEGA_ERR_UNSUPPORTED;
+  DevPool scratch(s);
+  double *mom = nullptr, *bv = nullptr;
+  MEGA_ALLOC(scratch, mom, (int64_t)kMom * n);
+  MEGA_ALLOC(scratch, bv, 16 * (int64_t)n);
+  const int block = 128;
+  const unsigned gg = (unsigned)(((int64_t)n * kLPN + block - 1) / block);
+  const unsigned gn = (unsigned)((n + block - 1) / block);
+  k_rk_moments<<<gg, block, 0, s>>>(n, coo, win, ebc_nodes, csr.rowptr, csr.col, p.shsup, sml, face, mom);
+  MEGA_CHECK_LAUNCH();
+  k_rk_solve<<<gn, block, 0, s>>>(n, coo, p.ql, p.ql_coef, p.ql_len, sml, face, mom, bv, status);
+  MEGA_CHECK_LAUNCH();
+  k_rk_values<<<gg, block, 0, s>>>(n, coo, win, ebc_nodes, csr.rowptr, csr.col, p.ql, p.ql_coef, p.ql_len, p.shsup,
+                                   sml, face, bv, shp, gx, gy, gz);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
 }  // namespace
 
 int rk_shapes(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
               const int32_t* ebc_nodes, const DevCSR& csr, double* shp, double* gx, double* gy, double* gz,
               unsigned* status) {
-  if (p.rk_degree != 1 || p.rk_cont != 3) return MEGA_ERR_UNSUPPORTED;
-  const int block = 128;
-  const unsigned grid = (unsigned)(((int64_t)n * kLPN + block - 1) / block);
-  k_rk_shapes<<<grid, block, 0, s>>>(n, coo, win, ebc_nodes, csr.rowptr, csr.col, p.ql, p.ql_coef, p.ql_len,
-                                     p.shsup, nullptr, -1, shp, gx, gy, gz, status);
-  MEGA_CHECK_LAUNCH();
-  return 0;
+  return rk_run(s, p, n, coo, win, ebc_nodes, csr, nullptr, -1, shp, gx, gy, gz, status);
 }
 
 int rk_grad_at_face(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
                     const int32_t* ebc_nodes, const DevCSR& csr, const double* sml, int face, double* gx, double* gy,
                     double* gz, unsigned* status) {
-  if (p.rk_degree != 1 || p.rk_cont != 3) return MEGA_ERR_UNSUPPORTED;
-  const int block = 128;
-  const unsigned grid = (unsigned)(((int64_t)n * kLPN + block - 1) / block);
-  k_rk_shapes<<<grid, block, 0, s>>>(n, coo, win, ebc_nodes, csr.rowptr, csr.col, p.ql, p.ql_coef, p.ql_len,
-                                     p.shsup, sml, face, nullptr, gx, gy, gz, status);
-  MEGA_CHECK_LAUNCH();
-  return 0;
+  return rk_run(s, p, n, coo, win, ebc_nodes, csr, sml, face, nullptr, gx, gy, gz, status);
 }
 
 }  // namespace mega
