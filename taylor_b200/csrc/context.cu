@@ -249,8 +249,9 @@ void host_parallel(int64_t n, F fn, int64_t grain = 65536) {
 }
 
 // Bulk host <-> device copies go through one pinned buffer kept for the
-// process: the host's cores copy the caller's (pageable) arrays into it and
-// each array moves with one DMA, instead of the driver staging pageable
+// process: the host's cores copy the caller's (pageable) arrays into it in
+// 4 MiB pieces and each piece moves with its own DMA as soon as it is there
+// (downloads the other way round), instead of the driver staging pageable
 // memory on the calling thread.  One user at a time; a failed pinned
 // allocation falls back to plain pageable copies.
 struct PinnedStage {
@@ -259,16 +260,6 @@ struct PinnedStage {
   size_t cap = 0;
 };
 PinnedStage g_stage;
-
-void host_copy(void* dst, const void* src, size_t bytes) {
-  const int64_t chunks = (int64_t)((bytes + (1 << 20) - 1) >> 20);  // 1 MiB pieces
-  host_parallel(chunks, [&](int64_t lo, int64_t hi) {
-    for (int64_t k = lo; k < hi; ++k) {
-      const size_t a = (size_t)k << 20, b = std::min(bytes, (size_t)(k + 1) << 20);
-      std::memcpy((unsigned char*)dst + a, (const unsigned char*)src + a, b - a);
-    }
-  }, 2);
-}
 
 // one array to upload: copied from src, or written by fill(staging) when
 // the host array is formed on the way (fill writes `bytes` bytes)
@@ -352,10 +343,36 @@ int download_staged(cudaStream_t s, void* dst, const void* src, size_t bytes) {
     MEGA_TRY(cudaStreamSynchronize(s));
     return 0;
   }
-  MEGA_TRY(cudaMemcpyAsync(g_stage.p, src, bytes, cudaMemcpyDeviceToHost, s));
-  MEGA_TRY(cudaStreamSynchronize(s));
-  host_copy(dst, g_stage.p, bytes);
-  return 0;
+  // 4 MiB pieces, each copied out by a pool thread as soon as its DMA is done
+  constexpr size_t kPiece = (size_t)4 << 20;
+  const int64_t np = (int64_t)((bytes + kPiece - 1) / kPiece);
+  std::vector<cudaEvent_t> ev(np, nullptr);
+  int r = 0;
+  for (int64_t k = 0; k < np && !r; ++k) {
+    const size_t a = (size_t)k * kPiece, len = std::min(kPiece, bytes - a);
+    if (cudaMemcpyAsync(g_stage.p + a, (const unsigned char*)src + a, len, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(ev[k], s) != cudaSuccess)
+      r = MEGA_ERR_CUDA;
+  }
+  std::atomic<int> bad(0);
+  if (!r)
+    host_parallel(np, [&](int64_t lo, int64_t hi) {
+      for (int64_t k = lo; k < hi; ++k) {
+        const size_t a = (size_t)k * kPiece, len = std::min(kPiece, bytes - a);
+        if (cudaEventSynchronize(ev[k]) != cudaSuccess) { bad.store(1); continue; }
+        std::memcpy((unsigned char*)dst + a, g_stage.p + a, len);
+      }
+    }, 1);
+  if (r || bad.load()) {
+    cudaStreamSynchronize(s);  // no DMA may still write the stage
+    record_cuda_error(cudaGetLastError(), "download_staged", __FILE__, __LINE__);
+    r = MEGA_ERR_CUDA;
+  }
+  for (auto e : ev)
+    if (e) cudaEventDestroy(e);
+  return r;
 }
 
 // Deduplication of PROPS(30,N) and the material type into a table of
@@ -1362,10 +1379,15 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   MEGA_ALLOC(c->nbpool, c->csr.rowptr, (int64_t)n + 1);
   MEGA_ALLOC(c->nbpool, c->csr.col, m);
   MEGA_ALLOC(c->nbpool, c->shp, m);
-  double *g1x, *g1y, *g1z;
-  MEGA_ALLOC(tmp1, g1x, m);
-  MEGA_ALLOC(tmp1, g1y, m);
-  MEGA_ALLOC(tmp1, g1z, m);
+  // Mixed precision alone (DNI, shapes not asked for): the shape kernel
+  // writes the packed row records itself, so no double gradients are kept.
+  const bool packed = !want && c->prec_mask == 2 && !c->nsni;
+  double *g1x = nullptr, *g1y = nullptr, *g1z = nullptr;
+  if (!packed) {
+    MEGA_ALLOC(tmp1, g1x, m);
+    MEGA_ALLOC(tmp1, g1y, m);
+    MEGA_ALLOC(tmp1, g1z, m);
+  }
   k_newrow_len<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->perm, csr0.rowptr, len1);
   MEGA_CHECK_LAUNCH();
   r = scan_counts(c->s, len1, c->csr.rowptr, n, tmp1);
@@ -1391,7 +1413,17 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     k_renumber_cols<<<grid_for((int64_t)n * 32, 256), 256, 0, c->s>>>(n, c->perm, c->iperm, csr0.rowptr, csr0.col,
                                                                        c->csr.rowptr, c->csr.col);
     MEGA_CHECK_LAUNCH();
-    r = rk_shapes(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, c->csr, c->shp, g1x, g1y, g1z, c->status);
+    if (packed) {  // the row tiles first: the records carry the tile ranks
+      if ((r = configure_tiled_kernels())) return r;
+      r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->rt, c->nbpool, nullptr);
+      if (r) return r;
+      float4* a = nullptr;
+      MEGA_ALLOC(c->nbpool, a, m);
+      c->pk32 = a;
+      r = rk_shapes_packed(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, c->csr, c->rt.lidx, c->shp, a, c->status);
+    } else {
+      r = rk_shapes(c->s, c->p, n, c->coo, c->win, c->ebc_nodes, c->csr, c->shp, g1x, g1y, g1z, c->status);
+    }
     if (r) return r;
     tr.mark("rk_shapes");
     if (c->nsni) {
@@ -1420,8 +1452,10 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     }
   }
   tr.mark("transpose");
-  r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->rt, c->nbpool, nullptr);
-  if (r) return r;
+  if (!packed) {
+    r = build_tiles(c->s, n, c->csr.rowptr, c->csr.col, m, c->csr.gmaxn, c->rt, c->nbpool, nullptr);
+    if (r) return r;
+  }
   tr.mark("row_tiles");
   // the longest column bounds a column tile's set from below
   r = build_tiles(c->s, n, c->csr.colptr, c->csr.trow, m, c->csr.gmaxc, c->ct, c->nbpool, nullptr);
@@ -1441,14 +1475,19 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     MEGA_CHECK_LAUNCH();
   }
   if (c->prec_mask & 2) {
-    float4 *a = nullptr, *b = nullptr;
-    MEGA_ALLOC(c->nbpool, a, m);
+    float4* b = nullptr;
     MEGA_ALLOC(c->nbpool, b, m);
-    c->pk32 = a;
     c->tpk32 = b;
-    if ((r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, false, c->pk32)) ||
-        (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, false, c->tpk32)))
-      return r;
+    if (packed) {
+      if ((r = pack_transposed32(c->s, m, c->ct.lidx, (const float4*)c->pk32, c->csr.tpos, b))) return r;
+    } else {
+      float4* a = nullptr;
+      MEGA_ALLOC(c->nbpool, a, m);
+      c->pk32 = a;
+      if ((r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, false, c->pk32)) ||
+          (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, false, c->tpk32)))
+        return r;
+    }
     MEGA_ALLOC(c->nbpool, c->sdphi32, 3 * (int64_t)n);
     k_rowsum_pk32<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, (const float4*)c->pk32, c->sdphi32);
     MEGA_CHECK_LAUNCH();

@@ -171,6 +171,12 @@ int rk_shapes(cudaStream_t s, const mega_params& p, int32_t n, const double* coo
               const int32_t* ebc_nodes, const DevCSR& csr, double* shp, double* gx, double* gy, double* gz,
               unsigned* status);
 
+// the same shapes with the gradients written straight as mixed-precision
+// records (float gradient + lidx[p]) into pk; shp as doubles
+int rk_shapes_packed(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
+                     const int32_t* ebc_nodes, const DevCSR& csr, const uint16_t* lidx, double* shp, float4* pk,
+                     unsigned* status);
+
 int rk_grad_at_face(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
                     const int32_t* ebc_nodes, const DevCSR& csr, const double* sml, int face, double* gx, double* gy,
                     double* gz, unsigned* status);

@@ -243,7 +243,8 @@ __global__ void __launch_bounds__(128) k_rk_values(int32_t n, const double* __re
                                                    double ql_len, int shsup, const double* __restrict__ sml,
                                                    int face, const double* __restrict__ bv,
                                                    double* __restrict__ shp, double* __restrict__ gx,
-                                                   double* __restrict__ gy, double* __restrict__ gz) {
+                                                   double* __restrict__ gy, double* __restrict__ gz,
+                                                   float4* __restrict__ pk, const uint16_t* __restrict__ lidx) {
   const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kLPN;
   const int lane = threadIdx.x & (kLPN - 1);
   if (i >= n) return;
@@ -275,16 +276,21 @@ __global__ void __launch_bounds__(128) k_rk_values(int32_t n, const double* __re
     const double CY = BY[0] * H[0] + BY[1] * H[1] + BY[2] * H[2] + BY[3] * H[3] + B[2];
     const double CZ = BZ[0] * H[0] + BZ[1] * H[1] + BZ[2] * H[2] + BZ[3] * H[3] + B[3];
     if (shp) shp[p] = C * e.phi;
-    gx[p] = CX * e.phi + C * e.px;
-    gy[p] = CY * e.phi + C * e.py;
-    gz[p] = CZ * e.phi + C * e.pz;
+    const double vx = CX * e.phi + C * e.px, vy = CY * e.phi + C * e.py, vz = CZ * e.phi + C * e.pz;
+    if (pk) {  // the mixed-precision record (gradient in float, tile rank) instead of the doubles
+      pk[p] = make_float4((float)vx, (float)vy, (float)vz, __int_as_float((int)lidx[p]));
+    } else {
+      gx[p] = vx;
+      gy[p] = vy;
+      gz[p] = vz;
+    }
   }
 }
 
 // the three kernels in order on stream s, with their per-node scratch
 int rk_run(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
            const int32_t* ebc_nodes, const DevCSR& csr, const double* sml, int face, double* shp, double* gx,
-           double* gy, double* gz, unsigned* status) {
+           double* gy, double* gz, float4* pk, const uint16_t* lidx, unsigned* status) {
   if (p.rk_degree != 1 || p.rk_cont != 3) return MEGA_ERR_UNSUPPORTED;
   DevPool scratch(s);
   double *mom = nullptr, *bv = nullptr;
@@ -298,7 +304,7 @@ int rk_run(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, c
   k_rk_solve<<<gn, block, 0, s>>>(n, coo, p.ql, p.ql_coef, p.ql_len, sml, face, mom, bv, status);
   MEGA_CHECK_LAUNCH();
   k_rk_values<<<gg, block, 0, s>>>(n, coo, win, ebc_nodes, csr.rowptr, csr.col, p.ql, p.ql_coef, p.ql_len, p.shsup,
-                                   sml, face, bv, shp, gx, gy, gz);
+                                   sml, face, bv, shp, gx, gy, gz, pk, lidx);
   MEGA_CHECK_LAUNCH();
   return 0;
 }
@@ -308,13 +314,19 @@ int rk_run(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, c
 int rk_shapes(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
               const int32_t* ebc_nodes, const DevCSR& csr, double* shp, double* gx, double* gy, double* gz,
               unsigned* status) {
-  return rk_run(s, p, n, coo, win, ebc_nodes, csr, nullptr, -1, shp, gx, gy, gz, status);
+  return rk_run(s, p, n, coo, win, ebc_nodes, csr, nullptr, -1, shp, gx, gy, gz, nullptr, nullptr, status);
+}
+
+int rk_shapes_packed(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
+                     const int32_t* ebc_nodes, const DevCSR& csr, const uint16_t* lidx, double* shp, float4* pk,
+                     unsigned* status) {
+  return rk_run(s, p, n, coo, win, ebc_nodes, csr, nullptr, -1, shp, nullptr, nullptr, nullptr, pk, lidx, status);
 }
 
 int rk_grad_at_face(cudaStream_t s, const mega_params& p, int32_t n, const double* coo, const double* win,
                     const int32_t* ebc_nodes, const DevCSR& csr, const double* sml, int face, double* gx, double* gy,
                     double* gz, unsigned* status) {
-  return rk_run(s, p, n, coo, win, ebc_nodes, csr, sml, face, nullptr, gx, gy, gz, status);
+  return rk_run(s, p, n, coo, win, ebc_nodes, csr, sml, face, nullptr, gx, gy, gz, nullptr, nullptr, status);
 }
 
 }  // namespace mega

@@ -180,13 +180,14 @@ __device__ __forceinline__ bool accept(const double xi[3], const double xj[3], c
 // form one index range [0, total) walked 32 at a time, so the output keeps
 // the reference order with every lane busy.  SORTED: candidate coordinates
 // and windows come from the cell-sorted copies xs / ws (contiguous within a
-// cell, independent of the index load); otherwise from coo / win by index.
+// cell; one 48-byte record x, w per node, read as three 16-byte loads, with
+// no dependence on the index load); otherwise from coo / win by index.
 // WRITE: accepted indices go to out[0 .. count).  Returns the count; the
 // candidate total in *total_out (lane values agree).
 template <bool WRITE, bool SORTED, int MMAX = 0>
 __device__ __forceinline__ int32_t filter_row(int64_t i, int lane, const double* __restrict__ coo,
-                                              const double* __restrict__ win, const double* __restrict__ xs,
-                                              const double* __restrict__ ws, const double* __restrict__ sm_len,
+                                              const double* __restrict__ win, const double* __restrict__ xw,
+                                              const double* __restrict__ sm_len,
                                               const int32_t* __restrict__ cell, int32_t nx, int32_t ny, int32_t nz,
                                               const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted,
                                               int mmax, int shsup, int32_t* __restrict__ out, int32_t* total_out) {
@@ -233,13 +234,19 @@ __device__ __forceinline__ int32_t filter_row(int64_t i, int lane, const double*
     const int32_t pk = __shfl_sync(0xffffffffu, pre, k);
     if (c < total) {
       const int64_t q = cb + (c - pk);
-      j = sorted[q];
-      const int64_t src = SORTED ? q : (int64_t)j;
-      const double* xp = SORTED ? xs : coo;
-      const double* wp = SORTED ? ws : win;
-      const double xj[3] = {xp[3 * src], xp[3 * src + 1], xp[3 * src + 2]};
-      const double wj[3] = {wp[3 * src], wp[3 * src + 1], wp[3 * src + 2]};
-      add = accept(xi, xj, wj, sl, mmax, shsup);
+      if (SORTED) {
+        if (WRITE) j = sorted[q];  // requested with the record, not after the test
+        const double2* r = reinterpret_cast<const double2*>(xw + 6 * q);
+        const double2 r0 = r[0], r1 = r[1], r2 = r[2];
+        const double xj[3] = {r0.x, r0.y, r1.x};
+        const double wj[3] = {r1.y, r2.x, r2.y};
+        add = accept(xi, xj, wj, sl, mmax, shsup);
+      } else {
+        j = sorted[q];
+        const double xj[3] = {coo[3 * (int64_t)j], coo[3 * (int64_t)j + 1], coo[3 * (int64_t)j + 2]};
+        const double wj[3] = {win[3 * (int64_t)j], win[3 * (int64_t)j + 1], win[3 * (int64_t)j + 2]};
+        add = accept(xi, xj, wj, sl, mmax, shsup);
+      }
     }
     const unsigned b = __ballot_sync(0xffffffffu, add);
     if (WRITE && add) out[count + __popc(b & lt)] = j;
@@ -261,8 +268,8 @@ __global__ void __launch_bounds__(256) k_soft_search(
   const int lane = threadIdx.x & 31;
   if (i >= n) return;  // whole warp leaves together
   int32_t total = 0;
-  const int32_t count = filter_row<FILL, false>(i, lane, coo, win, nullptr, nullptr, sm_len, cell, nx, ny, nz, cstart,
-                                                sorted, mmax, shsup, FILL ? col + rowptr[i] : nullptr, &total);
+  const int32_t count = filter_row<FILL, false>(i, lane, coo, win, nullptr, sm_len, cell, nx, ny, nz, cstart, sorted,
+                                                mmax, shsup, FILL ? col + rowptr[i] : nullptr, &total);
   if (lane == 0 && !FILL) {
     gn[i] = count;
     atomic_max_int(gmaxn, count);
@@ -270,16 +277,16 @@ __global__ void __launch_bounds__(256) k_soft_search(
   }
 }
 
-// coordinates and windows in cell-sorted order
+// coordinates and windows in cell-sorted order, (x, w) per node
 __global__ void k_sorted_coords(int32_t n, const int32_t* __restrict__ sorted, const double* __restrict__ coo,
-                                const double* __restrict__ win, double* __restrict__ xs, double* __restrict__ ws) {
+                                const double* __restrict__ win, double* __restrict__ xw) {
   const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= n) return;
   const int64_t j = sorted[q];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    xs[3 * q + k] = coo[3 * j + k];
-    ws[3 * q + k] = win[3 * j + k];
+    xw[6 * q + k] = coo[3 * j + k];
+    xw[6 * q + 3 + k] = win[3 * j + k];
   }
 }
 
@@ -307,8 +314,8 @@ __global__ void k_cand_count(int32_t n, const int32_t* __restrict__ cell, int32_
 // buf[coff[i] ..), its count into gn[i]; MMAX = 1 (DNI) or 7
 template <int MMAX>
 __global__ void __launch_bounds__(256, MMAX == 1 ? 4 : 3) k_search_once(
-    int32_t n, const double* __restrict__ coo, const double* __restrict__ win, const double* __restrict__ xs,
-    const double* __restrict__ ws, const double* __restrict__ sm_len, const int32_t* __restrict__ cell, int32_t nx,
+    int32_t n, const double* __restrict__ coo, const double* __restrict__ win, const double* __restrict__ xw,
+    const double* __restrict__ sm_len, const int32_t* __restrict__ cell, int32_t nx,
     int32_t ny, int32_t nz, const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted, int mmax,
     int shsup, const int64_t* __restrict__ coff, int32_t* __restrict__ buf, int32_t* __restrict__ gn,
     int32_t* __restrict__ gmaxn) {
@@ -316,8 +323,8 @@ __global__ void __launch_bounds__(256, MMAX == 1 ? 4 : 3) k_search_once(
   const int lane = threadIdx.x & 31;
   if (i >= n) return;
   int32_t total = 0;
-  const int32_t count = filter_row<true, true, MMAX>(i, lane, coo, win, xs, ws, sm_len, cell, nx, ny, nz, cstart,
-                                                     sorted, mmax, shsup, buf + coff[i], &total);
+  const int32_t count = filter_row<true, true, MMAX>(i, lane, coo, win, xw, sm_len, cell, nx, ny, nz, cstart, sorted,
+                                                     mmax, shsup, buf + coff[i], &total);
   if (lane == 0) {
     gn[i] = count;
     atomic_max_int(gmaxn, count);
@@ -635,19 +642,18 @@ int bin_search(cudaStream_t s, int32_t n, const double* coo, const double* win, 
   MEGA_TRY(cudaMemcpyAsync(&ctot, coff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaStreamSynchronize(s));
   int32_t* buf = nullptr;
-  double *xs = nullptr, *ws = nullptr;
+  double* xw = nullptr;
   size_t fr = 0, tot = 0;
   const bool once = cudaMemGetInfo(&fr, &tot) == cudaSuccess &&
                     (size_t)ctot * sizeof(int32_t) + 48 * (size_t)n + ((size_t)1 << 30) < fr;
   if (once) {
     MEGA_ALLOC(scratch, buf, ctot);
-    MEGA_ALLOC(scratch, xs, 3 * (int64_t)n);
-    MEGA_ALLOC(scratch, ws, 3 * (int64_t)n);
-    k_sorted_coords<<<grid_for(n, 256), 256, 0, s>>>(n, sorted, coo, win, xs, ws);
+    MEGA_ALLOC(scratch, xw, 6 * (int64_t)n);
+    k_sorted_coords<<<grid_for(n, 256), 256, 0, s>>>(n, sorted, coo, win, xw);
     MEGA_CHECK_LAUNCH();
     auto k = mmax == 1 ? k_search_once<1> : k_search_once<7>;
-    k<<<gw, 256, 0, s>>>(n, coo, win, xs, ws, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax, shsup, coff, buf,
-                         gn, gmaxn);
+    k<<<gw, 256, 0, s>>>(n, coo, win, xw, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax, shsup, coff, buf, gn,
+                         gmaxn);
   } else {
     k_soft_search<false><<<gw, 256, 0, s>>>(n, coo, win, sm_len, cell, bg.nx, bg.ny, bg.nz, cstart, sorted, mmax,
                                             shsup, gn, nullptr, nullptr, gmaxn, status);

@@ -139,6 +139,14 @@ __global__ void k_pack_f32(int64_t m, const uint16_t* __restrict__ lidx, const d
   out[e] = make_float4((float)gx[p], (float)gy[p], (float)gz[p], __int_as_float((int)lidx[e]));
 }
 
+__global__ void k_pack_t32(int64_t m, const uint16_t* __restrict__ lidx, const float4* __restrict__ in,
+                           const int64_t* __restrict__ pos, float4* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= m) return;
+  const float4 v = in[pos[e]];
+  out[e] = make_float4(v.x, v.y, v.z, __int_as_float((int)lidx[e]));
+}
+
 __global__ void k_pack_f64(int64_t m, const uint16_t* __restrict__ lidx, const double* __restrict__ gx,
                            const double* __restrict__ gy, const double* __restrict__ gz,
                            const int64_t* __restrict__ pos, double2* __restrict__ out) {
@@ -589,6 +597,14 @@ int build_tiles(cudaStream_t s, int32_t n, const int64_t* ptr, const int32_t* id
     return 0;
   }
   return MEGA_ERR_UNSUPPORTED;
+}
+
+int pack_transposed32(cudaStream_t s, int64_t m, const uint16_t* lidx, const float4* in, const int64_t* pos,
+                      float4* out) {
+  if (m <= 0) return 0;
+  k_pack_t32<<<grid_for(m, 256), 256, 0, s>>>(m, lidx, in, pos, out);
+  MEGA_CHECK_LAUNCH();
+  return 0;
 }
 
 int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* gx, const double* gy,

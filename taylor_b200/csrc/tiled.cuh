@@ -54,6 +54,10 @@ int build_tiles(cudaStream_t s, int32_t n, const int64_t* ptr, const int32_t* id
 // out[e] = (g[pos[e]], lidx[e]) as float4 (f64 = false) or 2 x double2
 int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* gx, const double* gy,
                  const double* gz, const int64_t* pos, bool f64, void* out);
+// out[e] = (in[pos[e]] gradient, lidx[e]): mixed records of the transposed
+// view from those of the rows
+int pack_transposed32(cudaStream_t s, int64_t m, const uint16_t* lidx, const float4* in, const int64_t* pos,
+                      float4* out);
 int configure_tiled_kernels();
 // launch variants of the two gathers (lanes per row x records in flight)
 int tiled_variants();

@@ -132,6 +132,26 @@ def test_shapes_on_renumbered_lists_equal_the_downloaded_path(itype):
     b.close()
 
 
+def test_mixed_only_context_steps_like_the_two_precision_one():
+    """A context asked for mixed records alone writes them straight from the
+    shape kernel (no double gradients kept); its mixed steps are the same to
+    the bit as those of a context that built both precisions."""
+    c = cases.taylor_bar(h=0.8e-3, seed=2)
+    p = _lib.params(**cases.param_kwargs(c))
+    a, b = mega.Mega(c, p), mega.Mega(c, p)
+    b.set_precisions(fp64=False, mixed=True)
+    a.search_and_shapes()
+    b.search_and_shapes()
+    a.step(30, 3e-8, mode="mixed")
+    b.step(30, 3e-8, mode="mixed")
+    for f in (_lib.F_COO_CURRENT, _lib.F_STRESS, _lib.F_EPS, _lib.F_VEL):
+        np.testing.assert_array_equal(a.download(f), b.download(f))
+    with pytest.raises(_lib.MegaError):  # FP64 records were not built
+        b.step(1, 3e-8, mode="fp64")
+    a.close()
+    b.close()
+
+
 def test_snapshot_equals_single_downloads(tmp_path):
     """One device-to-host copy of several fields equals their single
     downloads, and the output step writes them as VTK."""
