@@ -32,6 +32,11 @@ namespace {
 
 constexpr int kNL = 8;  // lanes per node of the two gathers
 
+// node stride of the force weights W: 18 doubles (144 B, nine 16-byte
+// loads) or 18 floats padded to 20 (80 B, five 16-byte loads)
+template <typename V>
+constexpr int w_stride() { return sizeof(V) == 4 ? 20 : 18; }
+
 // index of S_(m a) in the XX, YY, ZZ, XY, YZ, XZ order
 __device__ __forceinline__ int dd_index(int m, int a) {
   if (m == a) return m;
@@ -235,7 +240,7 @@ __global__ void __launch_bounds__(128) k_nsni_stress(NsniStepArgs a) {
           Wm[ax][k][m] = fac * vol * det * (S[k][0] * IF[m][0] + S[k][1] * IF[m][1] + S[k][2] * IF[m][2]);
     }
     // the weights folded onto the six symmetric second derivatives
-    WV* w = reinterpret_cast<WV*>(a.w) + 18 * i;
+    WV* w = reinterpret_cast<WV*>(a.w) + w_stride<WV>() * i;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       w[6 * k + 0] = (WV)Wm[0][k][0];
@@ -269,7 +274,23 @@ __global__ void __launch_bounds__(256) k_nsni_force(int32_t n, const int64_t* __
   if (J >= n) return;
   V f0 = V(0), f1 = V(0), f2 = V(0);
   for (int64_t e = colptr[J] + q; e < colptr[J + 1]; e += kNL) {
-    const V* wi = w + 18 * (int64_t)trow[e];
+    // the row's 18 weights as 16-byte loads
+    V wi[w_stride<V>()];
+    if constexpr (sizeof(V) == 4) {
+      const float4* src = reinterpret_cast<const float4*>(w + 20 * (int64_t)trow[e]);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const float4 x = src[k];
+        wi[4 * k] = x.x; wi[4 * k + 1] = x.y; wi[4 * k + 2] = x.z; wi[4 * k + 3] = x.w;
+      }
+    } else {
+      const double2* src = reinterpret_cast<const double2*>(w + 18 * (int64_t)trow[e]);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const double2 x = src[k];
+        wi[2 * k] = x.x; wi[2 * k + 1] = x.y;
+      }
+    }
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
       const V sv = st.v[c][e];
