@@ -86,9 +86,9 @@ __global__ void __launch_bounds__(256) k_nsni_h(int32_t n, const int64_t* __rest
   double h[18];
 #pragma unroll
   for (int k = 0; k < 18; ++k) h[k] = 0.0;
-  for (int64_t p = rowptr[i] + q; p < rowptr[i + 1]; p += kNL) {
-    const int64_t j = col[p];
-    const double u0 = du[3 * j], u1 = du[3 * j + 1], u2 = du[3 * j + 2];
+  // two entries per pass (p, p + kNL): both gathers are in flight before
+  // either is summed; each lane still sums its entries in list order
+  auto add = [&](int64_t p, double u0, double u1, double u2) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
       const double sv = (double)s.v[c][p];
@@ -96,6 +96,19 @@ __global__ void __launch_bounds__(256) k_nsni_h(int32_t n, const int64_t* __rest
       h[6 + c] += sv * u1;
       h[12 + c] += sv * u2;
     }
+  };
+  int64_t p = rowptr[i] + q;
+  const int64_t pe = rowptr[i + 1];
+  for (; p + kNL < pe; p += 2 * kNL) {
+    const int64_t j0 = col[p], j1 = col[p + kNL];
+    const double a0 = du[3 * j0], a1 = du[3 * j0 + 1], a2 = du[3 * j0 + 2];
+    const double b0 = du[3 * j1], b1 = du[3 * j1 + 1], b2 = du[3 * j1 + 2];
+    add(p, a0, a1, a2);
+    add(p + kNL, b0, b1, b2);
+  }
+  if (p < pe) {
+    const int64_t j = col[p];
+    add(p, du[3 * j], du[3 * j + 1], du[3 * j + 2]);
   }
 #pragma unroll
   for (int o = 1; o < kNL; o <<= 1)
@@ -273,9 +286,8 @@ __global__ void __launch_bounds__(256) k_nsni_force(int32_t n, const int64_t* __
   const unsigned gm = 0xFFu << (threadIdx.x & 24);
   if (J >= n) return;
   V f0 = V(0), f1 = V(0), f2 = V(0);
-  for (int64_t e = colptr[J] + q; e < colptr[J + 1]; e += kNL) {
-    // the row's 18 weights as 16-byte loads
-    V wi[w_stride<V>()];
+  // the row's 18 weights as 16-byte loads
+  auto load_w = [&](int64_t e, V* wi) {
     if constexpr (sizeof(V) == 4) {
       const float4* src = reinterpret_cast<const float4*>(w + 20 * (int64_t)trow[e]);
 #pragma unroll
@@ -291,6 +303,8 @@ __global__ void __launch_bounds__(256) k_nsni_force(int32_t n, const int64_t* __
         wi[2 * k] = x.x; wi[2 * k + 1] = x.y;
       }
     }
+  };
+  auto add = [&](int64_t e, const V* wi) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
       const V sv = st.v[c][e];
@@ -298,6 +312,21 @@ __global__ void __launch_bounds__(256) k_nsni_force(int32_t n, const int64_t* __
       f1 += wi[6 + c] * sv;
       f2 += wi[12 + c] * sv;
     }
+  };
+  // two entries per pass, both rows requested before either is summed
+  int64_t e = colptr[J] + q;
+  const int64_t ee = colptr[J + 1];
+  for (; e + kNL < ee; e += 2 * kNL) {
+    V wa[w_stride<V>()], wb[w_stride<V>()];
+    load_w(e, wa);
+    load_w(e + kNL, wb);
+    add(e, wa);
+    add(e + kNL, wb);
+  }
+  if (e < ee) {
+    V wa[w_stride<V>()];
+    load_w(e, wa);
+    add(e, wa);
   }
 #pragma unroll
   for (int o = 1; o < kNL; o <<= 1) {
