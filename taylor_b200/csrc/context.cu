@@ -764,11 +764,15 @@ std::mutex g_blk_mu;
 std::multimap<size_t, CachedBlock> g_blk;  // by block size
 size_t g_blk_total = 0;
 
-// 512-byte granularity below 1 MiB, 2 MiB above (a re-search whose list
-// grew by a few entries still finds its old block)
+// Size classes: 512 bytes below 1 MiB; above, an eighth of the size's
+// power of two (at least 2 MiB), so a list that grew by some entries since
+// the last search (semi-Lagrangian re-search under compression) still finds
+// the block of the last one
 size_t block_round(size_t b) {
   if (b < ((size_t)1 << 20)) return (b + 511) & ~(size_t)511;
-  const size_t g = (size_t)2 << 20;
+  size_t top = (size_t)1 << 20;
+  while (top * 2 <= b) top *= 2;
+  const size_t g = std::max(top >> 3, (size_t)2 << 20);
   return (b + g - 1) / g * g;
 }
 
@@ -812,6 +816,28 @@ int cached_alloc(void** p, size_t bytes, cudaStream_t s, size_t* got) {
       *p = b.p;
       *got = b.bytes;
       return 0;
+    }
+  }
+  if (want >= ((size_t)64 << 20)) {
+    // a large miss: blocks of this device between half the request and the
+    // request are the predecessors of a grown array; hand them back first
+    std::vector<CachedBlock> stale;
+    {
+      std::lock_guard<std::mutex> lk(g_blk_mu);
+      for (auto it = g_blk.lower_bound(want / 2); it != g_blk.end() && it->first < want;) {
+        if (it->second.dev == dev) {
+          stale.push_back(it->second);
+          g_blk_total -= it->second.bytes;
+          it = g_blk.erase(it);
+        } else {
+          ++it;
+        }
+      }
+    }
+    for (auto& b : stale) {
+      cudaStreamWaitEvent(s, b.ev, 0);
+      cudaEventDestroy(b.ev);
+      cudaFreeAsync(b.p, s);
     }
   }
   cudaError_t e = cudaMallocAsync(p, want, s);
