@@ -805,10 +805,18 @@ int cached_alloc(void** p, size_t bytes, cudaStream_t s, size_t* got) {
   cudaGetDevice(&dev);
   {
     std::unique_lock<std::mutex> lk(g_blk_mu);
-    for (auto it = g_blk.lower_bound(want); it != g_blk.end() && it->first <= want + want / 4; ++it) {
-      if (it->second.dev != dev) continue;
-      const CachedBlock b = it->second;
-      g_blk.erase(it);
+    // the same size class first (a repeated set-up finds all its blocks so
+    // and takes none that another of its requests will ask for); failing
+    // that, the smallest block up to a quarter larger (an array that grew)
+    auto pick = g_blk.end();
+    for (auto it = g_blk.lower_bound(want); it != g_blk.end() && it->first == want; ++it)
+      if (it->second.dev == dev) { pick = it; break; }
+    if (pick == g_blk.end())
+      for (auto it = g_blk.upper_bound(want); it != g_blk.end() && it->first <= want + want / 4; ++it)
+        if (it->second.dev == dev) { pick = it; break; }
+    if (pick != g_blk.end()) {
+      const CachedBlock b = pick->second;
+      g_blk.erase(pick);
       g_blk_total -= b.bytes;
       lk.unlock();
       cudaStreamWaitEvent(s, b.ev, 0);

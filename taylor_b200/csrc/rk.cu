@@ -20,8 +20,8 @@
 //                 QL term, the inverse and the correction vectors (16 values
 //                 per node);
 //   k_rk_values   a group per node again: phi_J and grad phi_J per entry.
-// kLPN = 8 lanes per node: the ~60 neighbours still give every lane several
-// entries.
+// kLPN = 4 lanes per node: the ~60 neighbours give every lane ~15 entries,
+// and the butterfly over the 41 sums takes two rounds.
 #include "mega_internal.cuh"
 
 namespace mega {
@@ -80,7 +80,7 @@ __device__ __forceinline__ int sidx(int j, int k) {
   return j == 0 ? k : (j == 1 ? 3 + k : (j == 2 ? 5 + k : 9));
 }
 
-constexpr int kLPN = 8;  // lanes per node
+constexpr int kLPN = 4;  // lanes per node
 constexpr int kMom = 41;  // psum, M, M_,x, M_,y, M_,z (10 packed values each)
 
 // the node's position, or a face point of its smoothing cell, x +- SM_LEN
