@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--h", type=float, default=0.1e-3, help="lattice spacing (m)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=0, help="CPU baseline sample steps (0 = auto)")
+    ap.add_argument("--cpu-steps", type=int, default=0, help="timed steps of the CPU baseline (0 = --steps)")
     ap.add_argument("--modes", default="fp64,mixed", help="order in which the precision modes run")
     ap.add_argument("--full-steps", type=int, default=600,
                     help="steps of the accuracy runs (FP64 vs mixed end states); 0 skips them")
@@ -156,6 +156,23 @@ def measured_peak():
         return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def cpu_model():
+    """The host CPU's model name (from /proc/cpuinfo), for the CPU baselines."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def workload_name(h, n):
+    """The workload string both arms report for the same bar."""
+    return f"taylor_bar_1M h={h*1e3:.3g}mm n={n} direct nodal integration"
 
 
 def kernel_bytes(n, nnz, mixed):
@@ -535,13 +552,16 @@ def _held_count(m):
     return k.value
 
 
-def cpu_baseline(case, steps, nthreads):
+def cpu_baseline(case, steps, nthreads, warmup=1):
+    """The oracle (C++ OpenMP restatement of MEGA with the reference's
+    per-thread FINT_TEMP buffers) on the host cores: step 0, `warmup`
+    untimed steps, then `steps` timed steps of the same bar."""
     from oracle import oracle as O
     from taylor_b200 import cases
     p = O.params(**cases.param_kwargs(case))
     r = O.Run(case, p, nthreads=nthreads)
     dt = cases.stable_dt(case, r.nb["gn"], r.nb["gstart"], r.nb["gstack"])
-    r.step(1, dt)
+    r.step(max(1, warmup), dt)
     t0 = time.perf_counter()
     r.step(steps, dt)
     el = time.perf_counter() - t0
@@ -557,18 +577,18 @@ def main():
         from taylor_b200 import cases
         case = cases.taylor_bar(h=args.h, seed=1)
         nthreads = os.cpu_count() or 1
-        steps = args.cpu_steps or max(1, min(args.steps, 10))
-        for _ in range(0):
-            pass
-        val, el = cpu_baseline(case, steps, nthreads)
-        line = dict(metric=METRIC, value=val, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+        steps = args.steps
+        val, el = cpu_baseline(case, steps, nthreads, warmup=args.warmup)
+        sample = (f"{steps} timed explicit steps of the {case['n']}-node bar after step 0 and {args.warmup} "
+                  f"untimed ones, C++ OpenMP restatement of MEGA with per-thread FINT_TEMP buffers on "
+                  f"{nthreads} threads of {cpu_model()} (the Fortran reference cannot be compiled here)")
+        line = dict(metric=METRIC, value=val, unit=UNIT, n_gpus=args.gpus, steps=steps, warmup=args.warmup,
                     ms_per_step=1e3 * el / steps, higher_is_better=True, scaling="weak", vs_baseline=None,
-                    dtype="f64", data="synthetic", impl="reference",
-                    config=dict(workload=f"taylor_bar_1M h={args.h*1e3:.3g}mm n={case['n']}", nodes=case["n"],
-                                sample=f"{steps} explicit steps after step 0 (reference arm: C++ OpenMP "
-                                       f"restatement of MEGA, the Fortran reference cannot be compiled here)"),
-                    cpu_baseline=dict(value=val, unit=UNIT, cores=nthreads, kind="port",
-                                      sample=f"{steps} steps of the {case['n']}-node bar"),
+                    dtype="f64", data="synthetic (seeded jittered lattice of the 0.1 mm copper bar)",
+                    impl="reference",
+                    config=dict(workload=workload_name(args.h, case["n"]), nodes=case["n"], sample=sample),
+                    cpu_baseline=dict(value=val, unit=UNIT, cores=nthreads, kind="port", cpu=cpu_model(),
+                                      sample=sample),
                     e2e=dict(value=val, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
         print(json.dumps(line))
         return
@@ -607,17 +627,18 @@ def main():
     cpu = None
     if not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
-        steps = args.cpu_steps or 5
+        steps = args.cpu_steps or args.steps
         val, el = cpu_baseline(r["case"], steps, nthreads)
-        cpu = dict(value=val, unit=UNIT, cores=nthreads, kind="port",
-                   sample=f"{steps} explicit steps of the same {n}-node bar after step 0, C++ OpenMP restatement "
-                          f"of MEGA with per-thread FINT_TEMP buffers (the Fortran reference cannot be compiled here)")
+        cpu = dict(value=val, unit=UNIT, cores=nthreads, kind="port", cpu=cpu_model(), seconds=el,
+                   sample=f"{steps} timed explicit steps of the same {n}-node bar after step 0 and one untimed "
+                          f"step, C++ OpenMP restatement of MEGA with per-thread FINT_TEMP buffers on {nthreads} "
+                          f"threads of {cpu_model()} (the Fortran reference cannot be compiled here)")
     e2e_val = world * n * K / r["e2e_s"]
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=K, warmup=args.warmup,
         ms_per_step=mix["ms"] / K, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32+f64",
         data="synthetic (seeded jittered lattice of the 0.1 mm copper bar, random-free material data)",
-        config=dict(workload=f"taylor_bar_1M h={args.h*1e3:.3g}mm", nodes=n, nnz=nnz, mean_neighbours=nnz / n,
+        config=dict(workload=workload_name(args.h, n), nodes=n, nnz=nnz, mean_neighbours=nnz / n,
                     dt=r["dt"], parallelism=f"replicas{world}", l2="inputs larger than L2 (no flush needed)",
                     step0_search_shapes_s=r["step0_s"], device_bytes=r["dev_bytes"], autotuned=r["tuned"]),
         fp64_value=fp64_value, fp64_ms_per_step=f64["ms"] / K, mixed_over_fp64=value / fp64_value,

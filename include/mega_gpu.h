@@ -47,6 +47,9 @@ extern "C" {
                                           (INVERSE.F90:41-45) */
 #define MEGA_ST_BAD_MESH        0x0100 /* element connectivity names a node
                                           outside 1..N */
+#define MEGA_ST_WAIT_TIMEOUT    0x0200 /* a kernel gave up waiting for its own
+                                          asynchronous copies (bounded wait);
+                                          its outputs of that step are void */
 
 /* ---- API errors (negative return codes) --------------------------------- */
 #define MEGA_ERR_CUDA     (-1)
@@ -170,9 +173,10 @@ int mega_bin_search(int32_t n, const double* coo, const double* win,
  * out d_gn (n), d_gstart (n), d_gstack (dim_nn_list) 1-based, d_ijk (3,n)
  * or NULL -- and every temporary lives in one fixed 48 MiB __device__ array
  * compiled into the library, held by every GPU that loads it until exit.
- * Problems that do not fit (about 12 bytes per bin plus 20 per node, e.g.
- * 1.04 M nodes in 0.32 M bins fit) are rejected with MEGA_ERR_UNSUPPORTED
- * and a message.  dist_max, *gmaxn and *nnz are host memory; stream is a
+ * Problems that do not fit (about 16 bytes per bin plus 20 per node, e.g.
+ * 1.04 M nodes in 0.32 M bins fit), or whose lists hold more than
+ * INT32_MAX entries (GSTART is 32-bit), are rejected with
+ * MEGA_ERR_UNSUPPORTED and a message.  dist_max, *gmaxn and *nnz are host memory; stream is a
  * cudaStream_t (NULL = default stream); the call returns after the work on
  * that stream finished.  The first call on a device looks the array up
  * (cudaGetSymbolAddress), so make it before any stream capture.  Calls share
@@ -268,9 +272,11 @@ int mega_construct_fint_pd(const mega_params* p, int32_t n,
 
 /* Upload the model and create a context.  Arrays as in MAIN.F90:146-221:
  *   coo (3,n), win (3,n) normalised windows, vol (n), mass (3n), ebc (3,n)
- *   fixity codes (0 free, 1 fixed), vinit (3,n), props (30,n), mat_type (n),
+ *   fixity codes (0 free, 1 fixed, 2 prescribed velocity: see
+ *   mega_set_fixity2), vinit (3,n), props (30,n), mat_type (n),
  *   body_id (n), bodyforce (3,n) (may be NULL), sm_len (6,n).
- * Velocity starts at vinit except on fixed DOFs (STATE_INIT.f90:97-105). */
+ * Velocity starts at vinit except on fixed DOFs (STATE_INIT.f90:97-105);
+ * only code-1 nodes take the singular kernel (LOCAL_EBC_NODES). */
 int mega_gpu_init(const mega_params* p, int32_t n, const double* coo,
                   const double* win, const double* vol, const double* mass,
                   const int32_t* ebc, const double* vinit, const double* props,
@@ -288,13 +294,33 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo,
  * Energies and reaction sums in mega_get_scalars are totals over all
  * instances. */
 int mega_set_instances(int64_t h, int32_t ninst, const int32_t* inst_nodes, const double* dist_max);
-/* Autotuner: time each launch variant of the two per-step gathers (lanes
- * per row x records in flight: (4, 4), (4, 2), (4, 1), (8, 2), variants 0..3)
- * for the given precision on this context's lists, reps launches each,
- * keep the fastest, and leave the state as it was.  choice (2) receives the
- * deformation-gradient and force variants, times_ms (2 x 4, may be NULL) the
- * mean launch times. */
+/* Autotuner: time each launch variant of the two per-step gathers for the
+ * given precision on this context's lists, reps launches each, keep the
+ * fastest, and leave the state as it was.  Variants 0..3 hold the packed
+ * records in registers (lanes per row x records in flight: (4, 4), (4, 2),
+ * (4, 1), (8, 2)); 4 and 5 have the copy engine stream each tile's records
+ * into shared memory (4 or 8 lanes per row), where the tiles fit.  choice
+ * (2) receives the deformation-gradient and force variants, times_ms
+ * (2 x MEGA_TUNE_VARIANTS, may be NULL) the mean launch times, -1 for a
+ * variant that does not fit. */
+#define MEGA_TUNE_VARIANTS 6
+/* Pin the launch variants of the two gathers for one precision (after
+ * mega_search_and_shapes), e.g. to repeat a run bit for bit: variants with
+ * the same lanes per row (0, 1, 2, 4 and 3, 5) sum in the same order and
+ * give identical results.  MEGA_ERR_UNSUPPORTED when a streamed variant
+ * does not fit the context's tiles. */
+int mega_set_variants(int64_t h, int32_t mode, int32_t defgrad_variant, int32_t force_variant);
 int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* choice, float* times_ms);
+/* The windows of fixity code 2 (MODEL.F90:61-62, read by READ.F90:185-266):
+ * ftime = FIXITY2_TIME (steps,2) and fdisp = FIXITY2_NONZERO_EBC (steps,3),
+ * column-major.  In every step the corrector gives each code-2 DOF in
+ * direction j the velocity fdisp(k,j) / (ftime(k,2) - ftime(k,1)) of the
+ * first window k with ftime(k,1) < TIME < ftime(k,2), TIME the step's start
+ * time, or 0 outside every window, with zero acceleration and the reaction
+ * -FINT (MAIN.F90:447-470).  Without a call there is no window and the
+ * prescribed velocity is 0.  MEGA_ERR_ARG when a window ends
+ * before it starts (READ.F90:265), MEGA_ERR_STATE when no DOF has code 2. */
+int mega_set_fixity2(int64_t h, int32_t steps, const double* ftime, const double* fdisp);
 /* Precisions the context will step: mask bit 0 FP64, bit 1 mixed (default
  * 3).  Call before mega_search_and_shapes; only the asked-for packed records
  * are built (the FP64 records are 32 B per list entry, the mixed 16 B).
@@ -418,6 +444,18 @@ int mega_pmb_finalize(int64_t h);
 
 const char* mega_status_string(int32_t status);
 int mega_gpu_finalize(int64_t h);
+
+/* No counterpart in the reference (device memory of this library).  Set-up
+ * temporaries and finalised contexts leave their device blocks in a
+ * process-wide cache (at most a quarter of each device's memory) and in the
+ * device's default memory pool, whose release threshold the library raises
+ * to its maximum, so a repeated set-up allocates nothing from the driver.
+ * This call hands every cached block to the pool, puts back each device's
+ * previous release threshold and trims the pool to what live contexts hold,
+ * for a host program whose own allocator needs the memory.  Contexts stay
+ * valid; a later set-up caches again.  Call it with no library call in
+ * flight on another thread. */
+int mega_release_cached_memory(void);
 
 #ifdef __cplusplus
 }

@@ -1403,16 +1403,40 @@ int orc_construct_fint_pd(const mega_params* p, int n, const double* gcoo, const
   return status;
 }
 
-// Central-difference update of MAIN.F90:432-488 for fixity codes 0/1.
+// Prescribed velocity of the fixity-2 DOFs at TIME (MAIN.F90:448-462): the
+// first window k with FIXITY2_TIME(k,1) < TIME < FIXITY2_TIME(k,2) gives
+// FIXITY2_NONZERO_EBC(k,j) / (FIXITY2_TIME(k,2) - FIXITY2_TIME(k,1)) for
+// direction j; outside every window the velocity is zero.  ftime is
+// (steps,2) and fdisp (steps,3), column-major as MODEL.F90:62 holds them.
+void orc_fixity2_velocity(int steps, const double* ftime, const double* fdisp, double time, double* vel2) {
+  int step_num = 0;
+  for (int k = 1; k <= steps; ++k)
+    if (ftime[k - 1] < time && time < ftime[steps + k - 1]) { step_num = k; break; }
+  for (int j = 0; j < 3; ++j) {
+    if (1 <= step_num && step_num <= steps)
+      vel2[j] = fdisp[(size_t)j * steps + step_num - 1] / (ftime[steps + step_num - 1] - ftime[step_num - 1]);
+    else
+      vel2[j] = 0.0;
+  }
+}
+
+// Central-difference update of MAIN.F90:432-488 for fixity codes 0, 1 and 2
+// (vel2 = the prescribed velocities of this step's TIME, from
+// orc_fixity2_velocity; may be null when no DOF has code 2).
 // total_force (3,2) accumulates as TOTAL_FORCE does.
 void orc_corrector(int n, const int* ebc, const double* prop21, const double* mass, const double* fint,
                    double* fext, double* vel, double* acl, double* prforce, const int* body_id,
-                   double* total_force, double dlt) {
+                   double* total_force, double dlt, const double* vel2) {
   for (int i = 0; i < n; ++i)
     for (int j = 0; j < 3; ++j) {
       size_t m = 3 * (size_t)i + j;
       if (ebc[m] == 1) {
         vel[m] = 0.0;
+        acl[m] = 0.0;
+        prforce[m] = -fint[m];
+        fext[m] = -fint[m];
+      } else if (ebc[m] == 2) {                                       // MAIN.F90:447-470
+        vel[m] = vel2 ? vel2[j] : 0.0;
         acl[m] = 0.0;
         prforce[m] = -fint[m];
         fext[m] = -fint[m];
@@ -1441,7 +1465,7 @@ int orc_step(const mega_params* p, int n, const double* coo, const double* win, 
              double* vel, double* acl, double* fint, double* fext, double* prforce, double* coo_cur,
              double* wvel, double* strain_eq, double* en, double* total_force, double dlt,
              int nthreads, int serial_interp, int* newton_iters, const double* sm_len, double* ddshp,
-             double* sgrad) {
+             double* sgrad, const double* vel2) {
   size_t n3 = 3 * (size_t)n;
   for (size_t m = 0; m < n3; ++m) {                                  // predictor
     dsp[m] = dlt * vel[m] + dlt * dlt * 0.5 * acl[m];
@@ -1461,7 +1485,7 @@ int orc_step(const mega_params* p, int n, const double* coo, const double* win, 
                               nullptr);
   std::vector<double> p21(n);
   for (int i = 0; i < n; ++i) p21[i] = props[30 * (size_t)i + 20];
-  orc_corrector(n, ebc, p21.data(), mass, fint, fext, vel, acl, prforce, body_id, total_force, dlt);
+  orc_corrector(n, ebc, p21.data(), mass, fint, fext, vel, acl, prforce, body_id, total_force, dlt, vel2);
   double ke = 0.0, ee = en[2];
   for (size_t m = 0; m < n3; ++m) {
     ke += 0.5 * mass[m] * vel[m] * vel[m];

@@ -28,8 +28,9 @@ _SIG = {
     "orc_interp": (None, [I32, P, P, P, P, P, P, I32]),
     "orc_pd_shape": (I32, [I32, P, P, P, P, P, P, P, P, I32]),
     "orc_construct_fint_pd": (I32, [P, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, I32, D, P, P, I32]),
-    "orc_corrector": (None, [I32, P, P, P, P, P, P, P, P, P, P, D]),
-    "orc_step": (I32, [P, I32] + [P] * 31 + [D, I32, I32, P, P, P, P]),
+    "orc_fixity2_velocity": (None, [I32, P, P, D, P]),
+    "orc_corrector": (None, [I32, P, P, P, P, P, P, P, P, P, P, D, P]),
+    "orc_step": (I32, [P, I32] + [P] * 31 + [D, I32, I32, P, P, P, P, P]),
     "orc_pmb_force": (I64, [I32, P, P, P, P, P, P, D, D, P, P, I32]),
     "orc_mlp_nparams": (I64, [I32]),
     "orc_mlp_forward_backward": (D, [I32, P, I32, P, P, P, P]),
@@ -252,6 +253,21 @@ class Run:
                            coo_current=self.coo_cur if self.semi else None)
         self.init_status = r["status"]
         self.en[3] = r["gint_work"]
+        self.fixity2 = None  # (FIXITY2_TIME (steps,2), FIXITY2_NONZERO_EBC (steps,3)) of fixity code 2
+
+    def set_fixity2(self, times, disp):
+        """The prescribed-displacement windows of fixity code 2 (MODEL.F90:61-62)."""
+        t = np.asfortranarray(np.asarray(times, np.float64).reshape(-1, 2))
+        d = np.asfortranarray(np.asarray(disp, np.float64).reshape(-1, 3))
+        self.fixity2 = (len(t), t.ravel(order="F").copy(), d.ravel(order="F").copy())
+
+    def _vel2(self):
+        """Prescribed velocities of this step's TIME (MAIN.F90:448-462)."""
+        v = np.zeros(3)
+        if self.fixity2 is not None:
+            k, t, d = self.fixity2
+            lib().orc_fixity2_velocity(k, _p(t), _p(d), float(self.time), _p(v))
+        return v
 
     def _semi_step(self, dt):
         """MAIN.F90:348-488 with LLAGRANGIAN = .FALSE.: predictor, DO_INTERP
@@ -281,7 +297,7 @@ class Run:
         p21 = np.ascontiguousarray(f64(c["props"])[:, 20])
         lib().orc_corrector(n, _p(i32(c["ebc"])), _p(p21), _p(f64(c["mass"])), _p(self.fint), _p(self.fext),
                             _p(self.vel), _p(self.acl), _p(self.prforce), _p(i32(c["body_id"])),
-                            _p(self.total_force), float(dt))
+                            _p(self.total_force), float(dt), _p(self._vel2()))
         mass = f64(c["mass"]).reshape(-1)
         self.en[0] = self.en[3]
         self.en[1] = float(np.sum(0.5 * mass * self.vel * self.vel))
@@ -308,7 +324,8 @@ class Run:
                 _p(self.dsp), _p(self.dsp_tot), _p(self.dsp_tot_phy), _p(self.vel), _p(self.acl), _p(self.fint),
                 _p(self.fext), _p(self.prforce), _p(self.coo_cur), _p(self.wvel), _p(self.strain_eq), _p(self.en),
                 _p(self.total_force), float(dt), int(self.nthreads), int(bool(self.serial_interp)), _p(self.iters),
-                _p(f64(c["sm_len"]) if self.ddshp is not None else None), _p(self.ddshp), _p(self.sgrad))
+                _p(f64(c["sm_len"]) if self.ddshp is not None else None), _p(self.ddshp), _p(self.sgrad),
+                _p(self._vel2()))
             self.time += dt
             self.steps += 1
         return st

@@ -23,12 +23,14 @@ ST_BAD_MATERIAL = 0x0020
 ST_STACK_OVERFLOW = 0x0040
 ST_SINGULAR_SHAPE = 0x0080
 ST_BAD_MESH = 0x0100
+ST_WAIT_TIMEOUT = 0x0200
 ERR_CUDA, ERR_ARG, ERR_HANDLE, ERR_STATE, ERR_NOMEM, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6
 
 MODE_FP64 = 0
 MODE_MIXED = 1
 FLAG_INTERP_EACH_STEP = 0x100
 FLAG_LEARNED_GUESS = 0x200
+TUNE_VARIANTS = 6  # MEGA_TUNE_VARIANTS: launch variants of each per-step gather
 
 MAT_ELASTIC, MAT_VONMISES, MAT_DRUCKER_PRAGER, MAT_VM_DAMAGE, MAT_VM_RATE = 1, 2, 3, 6, 7
 
@@ -78,6 +80,9 @@ SIGNATURES = {
     "mega_search_and_shapes": (I32, [I64, P, P, P, I64, P, P, P, P]),
     "mega_set_instances": (I32, [I64, I32, P, P]),
     "mega_set_precisions": (I32, [I64, I32]),
+    "mega_set_fixity2": (I32, [I64, I32, P, P]),
+    "mega_release_cached_memory": (I32, []),
+    "mega_set_variants": (I32, [I64, I32, I32, I32]),
     "mega_autotune": (I32, [I64, D, I32, I32, P, P]),
     "mega_step_resident": (I32, [I64, I32, D, I32]),
     "mega_step_timed": (I32, [I64, I32, D, I32, C.POINTER(F32)]),

@@ -1,17 +1,21 @@
 """Build recipe for libmega_gpu.so (sm_100a) -- compiled in-tree so the
-shared library travels with the source tree."""
+shared library travels with the source tree.  Each .cu file compiles to an
+object under _build/ in parallel (a file is recompiled when it, or any
+header, is newer than its object), then the objects link into the library."""
 import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libmega_gpu.so")
+OBJ = os.path.join(os.path.dirname(HERE), "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "-ccbin", "/usr/bin/g++",
     "--expt-relaxed-constexpr",
 ]
@@ -26,6 +30,15 @@ def headers():
         os.path.join(HERE, "..", "include", "mega_gpu.h")]
 
 
+def _obj(src):
+    return os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
+
+
+def _stale(src, newest_header):
+    o = _obj(src)
+    return not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(src), newest_header)
+
+
 def up_to_date():
     if not os.path.exists(LIB):
         return False
@@ -36,7 +49,21 @@ def up_to_date():
 def build(force=False, verbose=False, extra=()):
     if not force and up_to_date():
         return LIB
-    cmd = [NVCC] + FLAGS + list(extra) + ["-o", LIB] + sources()
+    os.makedirs(OBJ, exist_ok=True)
+    newest = max(os.path.getmtime(h) for h in headers())
+    todo = [s for s in sources() if force or extra or _stale(s, newest)]
+
+    def compile_one(src):
+        cmd = [NVCC] + FLAGS + list(extra) + ["-c", "-o", _obj(src), src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(compile_one, s) for s in todo]:
+            f.result()
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-ccbin", "/usr/bin/g++", "-o", LIB] + [
+        _obj(s) for s in sources()]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -460,6 +460,13 @@ struct Ctx {
   StepAccum* acc = nullptr;
   unsigned* status = nullptr;
   bool phy_valid = true;
+  // fixity code 2 (prescribed velocity, MAIN.F90:447-470): the windows of
+  // FIXITY2_TIME / FIXITY2_NONZERO_EBC on the device (time (steps,2) then
+  // displacement (steps,3), column-major), the device copy of TIME and the
+  // three velocities of the current step
+  bool has_ebc2 = false;
+  int32_t f2_steps = 0;
+  double *f2 = nullptr, *dtime = nullptr, *vel2 = nullptr;
   double time = 0.0;
   int64_t steps = 0;
   int64_t launches = 0;
@@ -474,6 +481,8 @@ struct Ctx {
   float* mlp_theta = nullptr;  // fp32 parameters (training copy)
   uint16_t* mlp_w2 = nullptr;  // bf16 W2 for the tensor cores
   float* mlp_small = nullptr;
+  int32_t* mlp_queue = nullptr;    // plastic rate-dependent nodes of a learned step (n)
+  unsigned* mlp_qcount = nullptr;
   bool mlp_on = false;
   float* log_buf = nullptr;
   unsigned long long* log_count = nullptr;
@@ -551,7 +560,9 @@ static StressArgs stress_args(Ctx* c, double dt, int mode) {
   a.has_body = c->has_body; a.inv3_exact = c->p.inv3_exact; a.finite_strain = c->p.finite_strain;
   a.maxit = c->p.newton_max_iter; a.rate_solver = c->p.rate_solver; a.rtol = c->p.newton_rtol; a.dt = dt; a.iters = c->iters;
   a.aux = c->aux; a.acc = c->acc; a.status = c->status;
-  if ((mode & MEGA_FLAG_LEARNED_GUESS) && c->mlp_on) { a.mlp_w2 = c->mlp_w2; a.mlp_small = c->mlp_small; }
+  if ((mode & MEGA_FLAG_LEARNED_GUESS) && c->mlp_on) {
+    a.mlp_w2 = c->mlp_w2; a.mlp_small = c->mlp_small; a.queue = c->mlp_queue; a.qcount = c->mlp_qcount;
+  }
   if (c->log_cap > 0) {
     a.log_buf = c->log_buf; a.log_count = c->log_count; a.log_cap = c->log_cap;
     a.log_stride = c->log_stride; a.log_seed = c->log_seed;
@@ -563,13 +574,45 @@ static TiledForceArgs force_args(Ctx* c, double dt, int mode, int predict) {
   const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
   TiledForceArgs f{};
   f.n = c->n; f.R = c->ct.R; f.ntiles = c->ct.ntiles; f.jmax = c->ct.jmax; f.maxcnt = c->ct.maxcnt;
+  f.recmax = c->ct.recmax;
   f.jset = c->ct.jset; f.jcnt = c->ct.jcnt; f.colptr = c->csr.colptr;
   f.pk = mixed ? c->tpk32 : c->tpk64;
   f.tshp = c->tshp; f.tmat = c->tmat; f.has_body = c->has_body; f.predict = predict;
   f.ebc = c->ebc; f.mass = c->mass; f.matidx = c->matidx; f.mats = c->mats; f.body_id = c->body_id;
   f.fint = c->fint; f.fext = c->fext; f.vel = c->vel; f.acl = c->acl; f.dsp = c->dsp; f.dsp_tot = c->dsp_tot;
   f.prforce = c->prforce; f.fadd = c->nsni ? c->fstab : nullptr; f.dt = dt; f.acc = c->acc; f.status = c->status;
+  f.vel2 = c->vel2;
   return f;
+}
+
+// The prescribed velocities of the fixity-2 DOFs at the step's TIME
+// (MAIN.F90:448-462: the first window with FIXITY2_TIME(k,1) < TIME <
+// FIXITY2_TIME(k,2), FIXITY2_NONZERO_EBC(k,j) over its length, else zero),
+// then TIME = TIME + DLT (MAIN.F90:644).  One thread; launched once per step
+// between the stress and force kernels of contexts with code-2 DOFs.
+__global__ void k_fixity2(int32_t steps, const double* __restrict__ f2, double* time, double* vel2, double dt) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double t = *time;
+  int32_t k = 0;
+  for (int32_t i = 1; i <= steps; ++i)
+    if (f2[i - 1] < t && t < f2[steps + i - 1]) { k = i; break; }
+  for (int j = 0; j < 3; ++j)
+    vel2[j] = k ? f2[(int64_t)(2 + j) * steps + k - 1] / (f2[steps + k - 1] - f2[k - 1]) : 0.0;
+  *time = t + dt;
+}
+
+static int launch_fixity2(Ctx* c, double dt) {
+  if (!c->has_ebc2) return 0;
+  k_fixity2<<<1, 32, 0, c->s>>>(c->f2_steps, c->f2, c->dtime, c->vel2, dt);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+// The device's TIME from the host's before a run of steps (the device copy
+// advances with the steps; timing and tuning calls step it too).
+static int sync_time(Ctx* c) {
+  if (c->has_ebc2) MEGA_TRY(cudaMemcpyAsync(c->dtime, &c->time, sizeof(double), cudaMemcpyHostToDevice, c->s));
+  return 0;
 }
 
 static NsniStepArgs nsni_args(Ctx* c) {
@@ -581,8 +624,10 @@ static NsniStepArgs nsni_args(Ctx* c) {
   return a;
 }
 
-// kernels one step launches
-static int kernels_per_step(const Ctx* c) { return c->nsni ? 6 : 3; }
+// kernels one step launches (the learned start splits the stress kernel in two)
+static int kernels_per_step(const Ctx* c, int mode = 0) {
+  return (c->nsni ? 6 : 3) + (c->has_ebc2 ? 1 : 0) + (((mode & MEGA_FLAG_LEARNED_GUESS) && c->mlp_on) ? 1 : 0);
+}
 
 static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) {
   const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
@@ -592,7 +637,7 @@ static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) 
     MEGA_TRY(cudaMemcpyAsync(c->stress_prev, c->stress, sizeof(double) * 6 * c->n, cudaMemcpyDeviceToDevice, c->s));
   int r = launch_defgrad_tiled(c->s, mixed, interp, c->n, c->rt, c->csr.rowptr, mixed ? c->pk32 : c->pk64, c->dsp,
                                c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc,
-                               c->var_defgrad[mixed]);
+                               c->status, c->var_defgrad[mixed]);
   if (r) return r;
   if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->nsr32, c->nsc32, mixed, c->dsp, 0)))
     return r;
@@ -601,11 +646,12 @@ static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) 
   if (r) return r;
   if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->nsr32, c->nsc32, mixed, c->dsp, 1)))
     return r;
+  if ((r = launch_fixity2(c, dt))) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[2], c->s));
   r = launch_force_tiled(c->s, mixed, force_args(c, dt, mode, predict), c->var_force[mixed]);
   if (r) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[3], c->s));
-  c->launches += kernels_per_step(c);
+  c->launches += kernels_per_step(c, mode);
   return 0;
 }
 
@@ -639,7 +685,9 @@ static int run_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
   if ((mode & MEGA_FLAG_LEARNED_GUESS) && !c->mlp_on) return MEGA_ERR_STATE;
   { int r = (prec == MEGA_MODE_MIXED) ? ensure_mixed(c) : ensure_fp64(c); if (r) return r; }
   if (!(mode & MEGA_FLAG_INTERP_EACH_STEP)) c->phy_valid = false;
-  int r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
+  int r = sync_time(c);
+  if (r) return r;
+  r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
   if (r) return r;
   c->launches += 1;
   int32_t rem = nsteps - 1;
@@ -649,7 +697,7 @@ static int run_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
     if (r) return r;
     while (rem >= len) {
       MEGA_TRY(cudaGraphLaunch(c->gexec, c->s));
-      c->launches += kernels_per_step(c) * len;
+      c->launches += kernels_per_step(c, mode) * len;
       rem -= len;
     }
   }
@@ -726,7 +774,10 @@ static int make_stream(cudaStream_t* s) {
 // Contexts and their set-up temporaries allocate from the device's default
 // memory pool; with the release threshold at its maximum, memory a context
 // or a temporary frees stays in the pool and the next allocation reuses it
-// without a driver round trip (it returns to the driver at process exit).
+// without a driver round trip.  The pool's previous threshold is kept per
+// device; mega_release_cached_memory puts it back, hands the block cache
+// below to the pool and trims the pool, so a host program with its own
+// allocator gets the memory back without ending the process.
 bool trace_on() {
   static const bool on = std::getenv("MEGA_TRACE") != nullptr;
   return on;
@@ -738,19 +789,27 @@ void trace_alloc(size_t bytes, double ms, bool ordered) {
                  bytes / 1048576.0, ms);
 }
 
+static std::mutex g_pool_mu;
+static std::map<int, uint64_t> g_prev_threshold;  // device -> release threshold before the library set it
+
 void retain_pool_memory() {
-  static std::mutex mu;
-  static std::set<int> done;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return;
-  std::lock_guard<std::mutex> lk(mu);
-  if (done.count(dev)) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (g_prev_threshold.count(dev)) return;
   cudaMemPool_t mp;
-  if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
-    uint64_t thr = UINT64_MAX;
-    cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
+  if (cudaDeviceGetDefaultMemPool(&mp, dev) != cudaSuccess) { cudaGetLastError(); return; }
+  uint64_t prev = 0;
+  if (cudaMemPoolGetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &prev) != cudaSuccess) {
+    cudaGetLastError();
+    return;
   }
-  done.insert(dev);
+  uint64_t thr = UINT64_MAX;
+  if (cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  g_prev_threshold[dev] = prev;
 }
 
 namespace {
@@ -763,6 +822,8 @@ struct CachedBlock {
 std::mutex g_blk_mu;
 std::multimap<size_t, CachedBlock> g_blk;  // by block size
 size_t g_blk_total = 0;
+std::map<int, size_t> g_blk_dev_total;     // bytes cached per device
+std::map<int, size_t> g_blk_cap;           // per device: a quarter of its memory
 
 // Size classes: 512 bytes below 1 MiB; above, an eighth of the size's
 // power of two (at least 2 MiB), so a list that grew by some entries since
@@ -785,6 +846,7 @@ void flush_blocks(int dev, cudaStream_t s) {
       if (it->second.dev == dev) {
         out.push_back(it->second);
         g_blk_total -= it->second.bytes;
+        g_blk_dev_total[dev] -= it->second.bytes;
         it = g_blk.erase(it);
       } else {
         ++it;
@@ -818,6 +880,7 @@ int cached_alloc(void** p, size_t bytes, cudaStream_t s, size_t* got) {
       const CachedBlock b = pick->second;
       g_blk.erase(pick);
       g_blk_total -= b.bytes;
+      g_blk_dev_total[dev] -= b.bytes;
       lk.unlock();
       cudaStreamWaitEvent(s, b.ev, 0);
       cudaEventDestroy(b.ev);
@@ -836,6 +899,7 @@ int cached_alloc(void** p, size_t bytes, cudaStream_t s, size_t* got) {
         if (it->second.dev == dev) {
           stale.push_back(it->second);
           g_blk_total -= it->second.bytes;
+          g_blk_dev_total[dev] -= it->second.bytes;
           it = g_blk.erase(it);
         } else {
           ++it;
@@ -874,20 +938,27 @@ void cached_free(void* p, size_t block_bytes, cudaStream_t s) {
     cudaFreeAsync(p, s);
     return;
   }
-  // at most a quarter of the device's memory waits in the cache
-  size_t fr = 0, tot = 0;
-  static size_t cap = 0;
-  if (!cap && cudaMemGetInfo(&fr, &tot) == cudaSuccess) cap = tot / 4;
+  // at most a quarter of this device's memory waits in the cache
   std::vector<CachedBlock> evict;
   {
     std::lock_guard<std::mutex> lk(g_blk_mu);
+    auto ci = g_blk_cap.find(dev);
+    if (ci == g_blk_cap.end()) {
+      size_t fr = 0, tot = 0;
+      if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); tot = 0; }
+      ci = g_blk_cap.emplace(dev, tot / 4).first;
+    }
+    const size_t cap = ci->second;
     g_blk.emplace(block_bytes, CachedBlock{p, block_bytes, dev, ev});
+    size_t& held = g_blk_dev_total[dev];
+    held += block_bytes;
     g_blk_total += block_bytes;
     // the largest blocks of this device go first
-    for (auto it = g_blk.end(); cap && g_blk_total > cap && it != g_blk.begin();) {
+    for (auto it = g_blk.end(); cap && held > cap && it != g_blk.begin();) {
       --it;
       if (it->second.dev != dev) continue;
       evict.push_back(it->second);
+      held -= it->second.bytes;
       g_blk_total -= it->second.bytes;
       it = g_blk.erase(it);
     }
@@ -1011,6 +1082,7 @@ static int semi_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
   if ((mode & MEGA_FLAG_LEARNED_GUESS) && !c->mlp_on) return MEGA_ERR_STATE;
   const int32_t n = c->n;
   const int64_t n3 = 3 * (int64_t)n;
+  if (int r = sync_time(c)) return r;
   for (int32_t k = 0; k < nsteps; ++k) {
     int r = launch_predict(c->s, n3, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
     if (r) return r;
@@ -1022,14 +1094,15 @@ static int semi_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
                             c->sshp, nullptr, c->fg, c->acc)))
       return r;
     if ((r = launch_stress(c->s, false, stress_args(c, dt, mode)))) return r;
+    if ((r = launch_fixity2(c, dt))) return r;
     ForceArgs f{};
     f.n = n; f.csr = c->dscsr; f.tgx = c->stgx; f.tgy = c->stgy; f.tgz = c->stgz; f.tshp = c->stshp;
     f.tmat = c->tmat; f.has_body = c->has_body; f.integrate = 1; f.predict = 0;
     f.ebc = c->ebc; f.mass = c->mass; f.matidx = c->matidx; f.mats = c->mats; f.body_id = c->body_id;
     f.fint = c->fint; f.fext = c->fext; f.vel = c->vel; f.acl = c->acl; f.dsp = c->dsp; f.dsp_tot = c->dsp_tot;
-    f.prforce = c->prforce; f.dt = dt; f.acc = c->acc; f.status = c->status;
+    f.prforce = c->prforce; f.dt = dt; f.acc = c->acc; f.status = c->status; f.vel2 = c->vel2;
     if ((r = launch_force(c->s, false, f))) return r;
-    c->launches += 6;
+    c->launches += 6 + (c->has_ebc2 ? 1 : 0);
     c->time = c->time + dt;
     c->steps += 1;
   }
@@ -1082,7 +1155,8 @@ const char* mega_status_string(int32_t st) {
       {MEGA_ST_BAD_MATERIAL, "INVALID MATERIAL TYPE IN SUBROUTINE CONSTITUTION"},
       {MEGA_ST_STACK_OVERFLOW, "neighbour stack larger than DIM_NN_LIST"},
       {MEGA_ST_SINGULAR_SHAPE, "PROBLEM INVERTING MATRIX"},
-      {MEGA_ST_BAD_MESH, "element connectivity names a node outside the model"}};
+      {MEGA_ST_BAD_MESH, "element connectivity names a node outside the model"},
+      {MEGA_ST_WAIT_TIMEOUT, "a kernel timed out waiting for its asynchronous copies"}};
   for (auto& t : tab)
     if (st & t.bit) {
       if (buf[0]) strncat(buf, "; ", sizeof(buf) - strlen(buf) - 1);
@@ -1100,9 +1174,13 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   if ((p->lagrangian != 1 && p->lagrangian != 0) || p->peridynamics != 0) return MEGA_ERR_UNSUPPORTED;
   if (p->itype_int != 0 && p->itype_int != 2) return MEGA_ERR_UNSUPPORTED;  // DNI or NSNI
   if (p->lagrangian == 0 && p->itype_int != 0) return MEGA_ERR_UNSUPPORTED;  // semi-Lagrangian: DNI
-  for (int64_t m = 0; m < 3 * (int64_t)n; ++m)
-    if (ebc[m] != 0 && ebc[m] != 1) return MEGA_ERR_UNSUPPORTED;  // prescribed-velocity fixity (code 2)
+  bool has_ebc2 = false;
+  for (int64_t m = 0; m < 3 * (int64_t)n; ++m) {
+    if (ebc[m] < 0 || ebc[m] > 2) return MEGA_ERR_ARG;  // fixity codes 0 free, 1 fixed, 2 prescribed velocity
+    has_ebc2 = has_ebc2 || ebc[m] == 2;
+  }
   Ctx* c = new Ctx();
+  c->has_ebc2 = has_ebc2;
   c->p = *p;
   c->n = n;
   int r = make_stream(&c->s);
@@ -1122,6 +1200,10 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo, const doub
   CA(c->fint, n3); CA(c->fext, n3); CA(c->prforce, n3); CA(c->scratch3, n3);
   CA(c->stress, 6 * (int64_t)n); CA(c->strain, 6 * (int64_t)n); CA(c->eps, n); CA(c->strain_eq, n);
   CA(c->wvel, n); CA(c->fg, 18 * (int64_t)n); CA(c->iters, n); CA(c->acc, 1); CA(c->status, 1);
+  if (has_ebc2) {  // no windows until mega_set_fixity2: the prescribed velocity is zero (MAIN.F90:458-462)
+    CA(c->dtime, 1); CA(c->vel2, 3);
+    cudaMemsetAsync(c->vel2, 0, sizeof(double) * 3, c->s);
+  }
   c->semi = p->lagrangian == 0;
   if (c->semi) {
     c->sempool.bind(c->s);
@@ -1586,6 +1668,7 @@ int mega_kernel_times(int64_t h, int32_t reps, double dt, int32_t mode, float* o
   if (!c->searched) return MEGA_ERR_STATE;
   { int r = ((mode & 0xff) == MEGA_MODE_MIXED) ? ensure_mixed(c) : ensure_fp64(c); if (r) return r; }
   if (!(mode & MEGA_FLAG_INTERP_EACH_STEP)) c->phy_valid = false;
+  if (int r = sync_time(c)) return r;
   cudaEvent_t ev[4];
   for (auto& e : ev) MEGA_TRY(cudaEventCreate(&e));
   double acc[3] = {0, 0, 0};
@@ -1867,15 +1950,21 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
   MEGA_TRY(cudaEventCreate(&e0));
   MEGA_TRY(cudaEventCreate(&e1));
   std::vector<float> tdef(nvar, 0.f), tfor(nvar, 0.f);
+  std::vector<bool> fits(nvar, true);
   int r = 0;
   const StressArgs sa = stress_args(c, dt, mode & 0xff);
   for (int v = 0; v < nvar && !r; ++v) {
     const auto def = [&]() {
       return launch_defgrad_tiled(c->s, mixed, false, c->n, c->rt, c->csr.rowptr, mixed ? c->pk32 : c->pk64, c->dsp,
                                   c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc,
-                                  v);
+                                  c->status, v);
     };
     r = def();  // warm-up (twice: the first launch of a variant may also load its code)
+    if (r == MEGA_ERR_UNSUPPORTED) {  // a streamed variant whose tiles do not fit shared memory
+      fits[v] = false;
+      r = 0;
+      continue;
+    }
     if (!r) r = def();
     if (r) break;
     MEGA_TRY(cudaStreamSynchronize(c->s));
@@ -1889,6 +1978,11 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
     if (r) break;
     const TiledForceArgs fa = force_args(c, dt, mode & 0xff, 0);
     r = launch_force_tiled(c->s, mixed, fa, v);  // warm-up
+    if (r == MEGA_ERR_UNSUPPORTED) {
+      fits[v] = false;
+      r = 0;
+      continue;
+    }
     if (!r) r = launch_force_tiled(c->s, mixed, fa, v);
     if (r) break;
     MEGA_TRY(cudaStreamSynchronize(c->s));
@@ -1906,6 +2000,7 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
   if (r) return r;
   int bd = 0, bf = 0;
   for (int v = 1; v < nvar; ++v) {
+    if (!fits[v]) { tdef[v] = tfor[v] = -1.f; continue; }  // reported as -1: not launchable on these tiles
     if (tdef[v] < tdef[bd]) bd = v;
     if (tfor[v] < tfor[bf]) bf = v;
   }
@@ -1915,7 +2010,10 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
   c->g_mode = -1;
   if (choice) { choice[0] = bd; choice[1] = bf; }
   if (times_ms)
-    for (int v = 0; v < nvar; ++v) { times_ms[v] = tdef[v] / reps; times_ms[nvar + v] = tfor[v] / reps; }
+    for (int v = 0; v < nvar; ++v) {
+      times_ms[v] = fits[v] ? tdef[v] / reps : -1.f;
+      times_ms[nvar + v] = fits[v] ? tfor[v] / reps : -1.f;
+    }
   return read_status(c, true);
 }
 
@@ -1950,6 +2048,44 @@ static void drop_graph(Ctx* c) {
   c->g_mode = -1;
 }
 
+int mega_set_variants(int64_t h, int32_t mode, int32_t defgrad_variant, int32_t force_variant) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (!c->searched) return MEGA_ERR_STATE;
+  const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
+  if ((mode & 0xff) != MEGA_MODE_FP64 && !mixed) return MEGA_ERR_ARG;
+  if (defgrad_variant < 0 || defgrad_variant >= tiled_variants() || force_variant < 0 ||
+      force_variant >= tiled_variants())
+    return MEGA_ERR_ARG;
+  if (!tiled_variant_fits(c->rt, mixed, defgrad_variant, false, c->has_body) ||
+      !tiled_variant_fits(c->ct, mixed, force_variant, true, c->has_body))
+    return MEGA_ERR_UNSUPPORTED;
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  drop_graph(c);
+  c->var_defgrad[mixed] = defgrad_variant;
+  c->var_force[mixed] = force_variant;
+  return 0;
+}
+
+int mega_set_fixity2(int64_t h, int32_t steps, const double* ftime, const double* fdisp) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (steps < 0 || (steps > 0 && (!ftime || !fdisp))) return MEGA_ERR_ARG;
+  for (int32_t k = 0; k < steps; ++k)  // READ.F90:265: a window may not end before it starts
+    if (!(ftime[k] <= ftime[steps + k])) return MEGA_ERR_ARG;
+  if (!c->has_ebc2) return MEGA_ERR_STATE;  // no DOF has fixity code 2
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  drop_graph(c);  // the captured window kernel names the old table
+  if (steps > c->f2_steps || !c->f2) MEGA_ALLOC(c->pool, c->f2, 5 * (int64_t)std::max(steps, 1));
+  std::vector<double> t(5 * (size_t)steps);
+  std::memcpy(t.data(), ftime, sizeof(double) * 2 * steps);
+  std::memcpy(t.data() + 2 * (size_t)steps, fdisp, sizeof(double) * 3 * steps);
+  if (steps) MEGA_TRY(cudaMemcpyAsync(c->f2, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, c->s));
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  c->f2_steps = steps;
+  return 0;
+}
+
 int mega_set_surrogate(int64_t h, int32_t hidden, const float* theta) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
@@ -1962,6 +2098,8 @@ int mega_set_surrogate(int64_t h, int32_t hidden, const float* theta) {
     MEGA_ALLOC(c->mlppool, c->mlp_theta, np);
     MEGA_ALLOC(c->mlppool, c->mlp_w2, 64 * 64);
     MEGA_ALLOC(c->mlppool, c->mlp_small, 4 * 64 + 3 * 64 + 1);
+    MEGA_ALLOC(c->mlppool, c->mlp_queue, c->n);
+    MEGA_ALLOC(c->mlppool, c->mlp_qcount, 1);
   }
   MEGA_TRY(cudaMemcpyAsync(c->mlp_theta, theta, sizeof(float) * np, cudaMemcpyHostToDevice, c->s));
   int r = mlp_pack(c->s, c->mlp_theta, c->mlp_w2, c->mlp_small);
@@ -2025,6 +2163,8 @@ int mega_train_surrogate(int64_t h, float* theta, int32_t epochs, int32_t batch,
     MEGA_ALLOC(c->mlppool, c->mlp_theta, np);
     MEGA_ALLOC(c->mlppool, c->mlp_w2, 64 * 64);
     MEGA_ALLOC(c->mlppool, c->mlp_small, 4 * 64 + 3 * 64 + 1);
+    MEGA_ALLOC(c->mlppool, c->mlp_queue, c->n);
+    MEGA_ALLOC(c->mlppool, c->mlp_qcount, 1);
   }
   drop_graph(c);
   MEGA_TRY(cudaMemcpyAsync(c->mlp_theta, theta, sizeof(float) * np, cudaMemcpyHostToDevice, c->s));
@@ -2037,6 +2177,44 @@ int mega_train_surrogate(int64_t h, float* theta, int32_t epochs, int32_t batch,
   MEGA_TRY(cudaStreamSynchronize(c->s));
   c->mlp_on = true;
   return 0;
+}
+
+int mega_release_cached_memory(void) {
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) { cudaGetLastError(); return MEGA_ERR_CUDA; }
+  std::map<int, uint64_t> prev;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    prev.swap(g_prev_threshold);
+  }
+  std::set<int> devs;
+  for (const auto& kv : prev) devs.insert(kv.first);
+  {
+    std::lock_guard<std::mutex> lk(g_blk_mu);
+    for (const auto& kv : g_blk) devs.insert(kv.second.dev);
+  }
+  int rc = 0;
+  for (int dev : devs) {
+    cudaStream_t s = nullptr;
+    if (cudaSetDevice(dev) != cudaSuccess || make_stream(&s)) { cudaGetLastError(); rc = MEGA_ERR_CUDA; continue; }
+    flush_blocks(dev, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) rc = MEGA_ERR_CUDA;
+    cudaStreamDestroy(s);
+    cudaMemPool_t mp;
+    if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
+      const auto it = prev.find(dev);
+      if (it != prev.end()) {
+        uint64_t thr = it->second;
+        if (cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr) != cudaSuccess) rc = MEGA_ERR_CUDA;
+      }
+      if (cudaMemPoolTrimTo(mp, 0) != cudaSuccess) rc = MEGA_ERR_CUDA;
+    } else {
+      rc = MEGA_ERR_CUDA;
+    }
+    cudaGetLastError();
+  }
+  cudaSetDevice(cur);
+  return rc;
 }
 
 int mega_gpu_finalize(int64_t h) {

@@ -404,8 +404,22 @@ __device__ __forceinline__ void stress_reduce(const StressArgs& a, double work, 
   if (st) atomicOr(a.status, st);
 }
 
-// T = arithmetic of kinematics / rotation / predictor, TS = storage of T_i
-template <typename T, typename TS, bool DAM>
+// Overstress f = q - sqrt(2/3) (A + B eps0^n) of a rate-dependent trial
+// state (q its deviatoric norm): f > 0 takes a plastic return.
+__device__ __forceinline__ double rate_overstress(const double spred[6], double eps0, const MatEntry& me) {
+  const double kk = spred[0] + spred[1] + spred[2];
+  const double d0 = spred[0] - kk / 3.0, d1 = spred[1] - kk / 3.0, d2 = spred[2] - kk / 3.0;
+  const double q = sqrt(d0 * d0 + d1 * d1 + d2 * d2 + 2.0 * (spred[3] * spred[3] + spred[4] * spred[4] +
+                                                             spred[5] * spred[5]));
+  const double epn = (eps0 > 0.0) ? pow(eps0, me.C) : 0.0;
+  return q - sqrt(2.0 / 3.0) * (me.sig0 + me.B * epn);
+}
+
+// T = arithmetic of kinematics / rotation / predictor, TS = storage of T_i.
+// QUEUE (the learned start): plastic rate-dependent nodes are not finished
+// here but listed in a.queue (one atomic per warp) for k_stress_queue, so
+// the network and its Newton polish run on full warps of plastic nodes only.
+template <typename T, typename TS, bool DAM, bool QUEUE>
 __global__ void __launch_bounds__(256, 2) k_stress(StressArgs a) {
   __shared__ double smd[32];
   __shared__ unsigned long long smu[32];
@@ -418,49 +432,65 @@ __global__ void __launch_bounds__(256, 2) k_stress(StressArgs a) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
     Trial<T, false> w;
     stress_trial<T, false, DAM>(a, i, w);
+    if (QUEUE) {
+      const bool push = w.me.type == MEGA_MAT_VM_RATE && rate_overstress(w.spred, a.eps[i], w.me) > 0.0;
+      const unsigned act = __activemask();
+      const unsigned bal = __ballot_sync(act, push);
+      if (bal) {
+        const int lane = threadIdx.x & 31, lead = __ffs(bal) - 1;
+        unsigned base = 0;
+        if (lane == lead) base = atomicAdd(a.qcount, (unsigned)__popc(bal));
+        base = __shfl_sync(act, base, lead);
+        if (push) a.queue[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)i;
+      }
+      if (push) continue;
+    }
     stress_finish<T, TS, false, DAM>(a, i, w, -1.0, work, nit, npl, st);
   }
   stress_reduce<T>(a, work, nit, npl, st, smd, smu);
 }
 
-// The learned start: a warp of 32 nodes evaluates the surrogate together
-// (the 64x64 layer on the tensor cores, mlp_tc.cuh) and each plastic
-// rate-dependent node starts its Newton iteration from
-// dgamma0 = clamp(y, 1e-3, 1) ub (ub = rate_upper_bound).  The loop is
-// warp-uniform.
+// The learned start: warps of 32 plastic rate-dependent nodes evaluate the
+// surrogate together (the 64x64 layer on the tensor cores, mlp_tc.cuh) and
+// each node starts its Newton iteration from dgamma0 = clamp(y, 1e-3, 1) ub
+// (ub = rate_upper_bound).
 constexpr int kLearnBlock = 128;
 
+// The queued plastic rate-dependent nodes of k_stress<..., QUEUE>: warps of
+// 32 queued nodes recompute their trial states (the stored state is still
+// the old one), evaluate the surrogate together and start Newton from it.
 template <typename T, typename TS, bool DAM>
-__global__ void __launch_bounds__(kLearnBlock, 4) k_stress_learned(StressArgs a) {
+__global__ void __launch_bounds__(kLearnBlock, 4) k_stress_queue(StressArgs a) {
   __shared__ double smd[32];
   __shared__ unsigned long long smu[32];
   __shared__ __align__(16) MlpSmem net;
   __shared__ __align__(16) uint16_t sH1[kLearnBlock * kMlpLd];
   __shared__ float sOut[kLearnBlock];
-  if (blockIdx.x == 0 && threadIdx.x < kSlots) a.acc->ke[threadIdx.x] = 0.0;
-  mlp_load(net, a.mlp_w2, a.mlp_small);
-  __syncthreads();
+  const int64_t count = *a.qcount;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  uint16_t* hw = sH1 + (wid * 32) * kMlpLd;
-  float* ow = sOut + wid * 32;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t first = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
   double work = 0.0;
   unsigned long long nit = 0, npl = 0;
   unsigned st = 0;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < a.n;
-       base += nwarps * 32) {
-    const int64_t i = base + lane;
-    const bool act = i < a.n;
+  if (first < count) {  // a block with queued nodes loads the network
+    mlp_load(net, a.mlp_w2, a.mlp_small);
+  }
+  __syncthreads();
+  uint16_t* hw = sH1 + (wid * 32) * kMlpLd;
+  float* ow = sOut + wid * 32;
+  for (int64_t base = first; base < count; base += nwarps * 32) {
+    const int64_t k = base + lane;
+    const bool act = k < count;
+    const int64_t i = act ? a.queue[k] : 0;
     Trial<T, true> w;
     float x[4] = {0.f, 0.f, 0.f, 0.f};
     double ub = 0.0, f = -1.0;
     if (act) {
       stress_trial<T, true, DAM>(a, i, w);
-      const MatEntry& me = a.mats[w.mi];
-      if (me.type == MEGA_MAT_VM_RATE) f = rate_features(w.spred, a.eps[i], me, a.dt, x, ub);
+      f = rate_features(w.spred, a.eps[i], a.mats[w.mi], a.dt, x, ub);
     }
-    // warps without a plastic rate-dependent node skip the network
-    const float y = __any_sync(0xffffffffu, f > 0.0) ? warp_mlp(x, f > 0.0, net, hw, ow) : 0.f;
+    const float y = warp_mlp(x, act && f > 0.0, net, hw, ow);
     if (act) {
       const double dg0 = f > 0.0 ? (double)fminf(fmaxf(y, 1e-3f), 1.0f) * ub : -1.0;
       stress_finish<T, TS, true, DAM>(a, i, w, dg0, work, nit, npl, st);
@@ -524,8 +554,9 @@ __global__ void __launch_bounds__(256) k_force(ForceArgs a) {
         const double mass = a.mass[m];
         const double fe_old = a.fext[m];
         double v = a.vel[m], acc, pr;
-        if (a.ebc[m] == 1) {  // MAIN.F90:438-445
-          v = 0.0;
+        const int code = a.ebc[m];
+        if (code == 1 || code == 2) {  // MAIN.F90:438-445 (fixed), 447-470 (prescribed velocity)
+          v = code == 1 ? 0.0 : a.vel2[q];
           acc = 0.0;
           pr = -fi;
           fe = -fi;
@@ -655,24 +686,33 @@ int launch_defgrad(cudaStream_t s, bool mixed, bool interp, int32_t n, const Dev
 int launch_stress(cudaStream_t s, bool mixed, const StressArgs& a) {
   const int block = 256;
   const int64_t need = grid_for(a.n, block);
-  if (a.mlp_w2 && a.mlp_small) {  // learned start of the rate-dependent return mapping
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)device_sm_count() * 8));
+  if (a.mlp_w2 && a.mlp_small && a.queue && a.qcount) {
+    // learned start: elastic nodes finish in the first kernel, plastic
+    // rate-dependent ones are queued for the network kernel
     const int64_t lneed = grid_for(a.n, kLearnBlock);
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(lneed, (int64_t)device_sm_count() * 8));
+    const unsigned lgrid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(lneed, (int64_t)device_sm_count() * 8));
+    MEGA_TRY(cudaMemsetAsync(a.qcount, 0, sizeof(unsigned), s));
     if (a.aux) {
-      if (mixed) k_stress_learned<float, float, true><<<grid, kLearnBlock, 0, s>>>(a);
-      else k_stress_learned<double, double, true><<<grid, kLearnBlock, 0, s>>>(a);
+      if (mixed) k_stress<float, float, true, true><<<grid, block, 0, s>>>(a);
+      else k_stress<double, double, true, true><<<grid, block, 0, s>>>(a);
+      MEGA_CHECK_LAUNCH();
+      if (mixed) k_stress_queue<float, float, true><<<lgrid, kLearnBlock, 0, s>>>(a);
+      else k_stress_queue<double, double, true><<<lgrid, kLearnBlock, 0, s>>>(a);
     } else {
-      if (mixed) k_stress_learned<float, float, false><<<grid, kLearnBlock, 0, s>>>(a);
-      else k_stress_learned<double, double, false><<<grid, kLearnBlock, 0, s>>>(a);
+      if (mixed) k_stress<float, float, false, true><<<grid, block, 0, s>>>(a);
+      else k_stress<double, double, false, true><<<grid, block, 0, s>>>(a);
+      MEGA_CHECK_LAUNCH();
+      if (mixed) k_stress_queue<float, float, false><<<lgrid, kLearnBlock, 0, s>>>(a);
+      else k_stress_queue<double, double, false><<<lgrid, kLearnBlock, 0, s>>>(a);
     }
   } else {
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)device_sm_count() * 8));
     if (a.aux) {
-      if (mixed) k_stress<float, float, true><<<grid, block, 0, s>>>(a);
-      else k_stress<double, double, true><<<grid, block, 0, s>>>(a);
+      if (mixed) k_stress<float, float, true, false><<<grid, block, 0, s>>>(a);
+      else k_stress<double, double, true, false><<<grid, block, 0, s>>>(a);
     } else {
-      if (mixed) k_stress<float, float, false><<<grid, block, 0, s>>>(a);
-      else k_stress<double, double, false><<<grid, block, 0, s>>>(a);
+      if (mixed) k_stress<float, float, false, false><<<grid, block, 0, s>>>(a);
+      else k_stress<double, double, false, false><<<grid, block, 0, s>>>(a);
     }
   }
   MEGA_CHECK_LAUNCH();

@@ -182,17 +182,20 @@ __device__ __forceinline__ int von_mises(const double spred[6], double& eps, con
   const double s23 = sqrt(2.0 / 3.0);
   const double sig23 = s23 * m.sig0;
   const double tol = sig23 * (double)1.0e-5f;  // single-precision literal 1.0E-05
-  double xk = sig23 * pow(1.0 + m.B * eps, m.C);
+  // (1 + B eps)^C and its derivative factor (1 + B eps)^(C - 1); linear
+  // hardening (C = 1) needs neither power: x^1 = x and x^0 = 1 exactly
+  const bool lin = m.C == 1.0;
+  double xk = sig23 * (lin ? 1.0 + m.B * eps : pow(1.0 + m.B * eps, m.C));
   int it = 0;
   if (tn - xk > 0.0) {
     double dg = 0.0;
     const double epst = eps;
     for (int i = 1; i <= maxit; ++i) {
       ++it;
-      xk = sig23 * pow(1.0 + m.B * eps, m.C);
+      xk = sig23 * (lin ? 1.0 + m.B * eps : pow(1.0 + m.B * eps, m.C));
       const double y = tn - xk - (2.0 * mu * dg);
       if (fabs(y) > tol) {
-        const double xkp = m.B * m.C * m.sig0 * pow(1.0 + m.B * eps, m.C - 1.0);
+        const double xkp = m.B * m.C * m.sig0 * (lin ? 1.0 : pow(1.0 + m.B * eps, m.C - 1.0));
         const double dy = -2.0 * mu * (1.0 + xkp / 3.0 / mu);
         dg = dg - y / dy;
         if (i == maxit) cap = true;

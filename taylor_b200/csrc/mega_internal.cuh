@@ -251,6 +251,8 @@ struct StressArgs {
   double* aux;               // 4 per node: STATE(1, 2, 4, 5) of the damaged models (or null)
   const uint16_t* mlp_w2;    // surrogate network: W2 (64x64) as bf16 bits, or null
   const float* mlp_small;    // W1 (64x4), b1, b2, W3, b3 as fp32, or null
+  int32_t* queue;            // learned start: plastic rate-dependent nodes of this step (n), or null
+  unsigned* qcount;          // their count (zeroed before the step's stress kernels)
   float* log_buf;            // sample log: 5 floats (4 features, target) per sample, or null
   unsigned long long* log_count;
   int64_t log_cap;
@@ -319,6 +321,7 @@ struct ForceArgs {
   int integrate;        // 0: only fint / fext (CONSTRUCT_FINT drop-in)
   int predict;          // fuse the next step's predictor
   const int8_t* ebc;
+  const double* vel2;   // prescribed velocities of fixity code 2 for this step (3), or null
   const double* mass;
   const uint16_t* matidx;
   const MatEntry* mats;

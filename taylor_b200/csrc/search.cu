@@ -897,6 +897,13 @@ extern "C" int mega_bin_search_noalloc(int32_t n, const double* d_coo, const dou
   MEGA_TRY(cudaMemcpyAsync(&hst, status, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaStreamSynchronize(s));
   *nnz = total;
+  if (total > (int64_t)INT32_MAX) {  // GSTART is a default INTEGER (int32): 1-based starts would wrap
+    char msg[256];
+    snprintf(msg, sizeof(msg),
+             "mega_bin_search_noalloc: %lld list entries exceed the 32-bit GSTART range", (long long)total);
+    record_error_text(msg);
+    return MEGA_ERR_UNSUPPORTED;
+  }
   k_noalloc_fortran<<<grid_for(n, 256), 256, 0, s>>>(n, rowptr, d_gn, d_gstart);
   MEGA_CHECK_LAUNCH();
   if (total > dim_nn_list) {  // the caller's GSTACK is too small: lists not written
@@ -908,6 +915,8 @@ extern "C" int mega_bin_search_noalloc(int32_t n, const double* d_coo, const dou
   MEGA_CHECK_LAUNCH();
   k_noalloc_plus_one<<<grid_for(total, 256), 256, 0, s>>>(total, d_gstack);
   MEGA_CHECK_LAUNCH();
+  // the fill pass ORs into the same status word: report both passes
+  MEGA_TRY(cudaMemcpyAsync(&hst, status, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaStreamSynchronize(s));
   return (int)hst;
 }

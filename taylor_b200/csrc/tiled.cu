@@ -15,6 +15,7 @@
 // deterministic, and identical in exact arithmetic to force.cu's.
 #include "mega_internal.cuh"
 #include "tiled.cuh"
+#include "bulk.cuh"
 
 namespace mega {
 namespace {
@@ -128,6 +129,15 @@ __global__ void __launch_bounds__(256) k_build_tiles(int32_t n, int32_t R, const
   if (tid == 0) jcnt[t] = total;
   __syncthreads();
   for (int64_t p = p0 + tid; p < p1; p += blockDim.x) lidx[p] = (uint16_t)rank[slot_tmp[p]];
+}
+
+// list entries of each tile of R consecutive rows
+__global__ void k_tile_entries(int32_t n, int32_t R, int64_t ntiles, const int64_t* __restrict__ ptr,
+                               int32_t* __restrict__ ent) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  const int64_t r0 = t * R, r1 = min((int64_t)n, r0 + R);
+  ent[t] = (int32_t)(ptr[r1] - ptr[r0]);
 }
 
 __global__ void k_pack_f32(int64_t m, const uint16_t* __restrict__ lidx, const double* __restrict__ gx,
@@ -354,6 +364,75 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
   }
 }
 
+// One DOF m = 3 J + q after its column sum fi (and body-force sum fe):
+// fixity, acceleration and corrector (MAIN.F90:432-488), the energy and
+// reaction sums, and the next step's predictor (MAIN.F90:353-355).
+__device__ __forceinline__ void correct_dof(const TiledForceArgs& a, int64_t J, int q, double fi, double fe,
+                                            double& ke, double& ee, double* tf, unsigned& st) {
+  const int64_t m = 3 * J + q;
+  if (a.fadd) fi += a.fadd[m];
+  if (!isfinite(fi)) st |= MEGA_ST_NONFINITE;
+  const double mass = a.mass[m];
+  const double fe_old = a.fext[m];
+  double v = a.vel[m], acc, pr;
+  const int code = a.ebc[m];
+  if (code == 1 || code == 2) {  // MAIN.F90:438-445 (fixed), 447-470 (prescribed velocity)
+    v = code == 1 ? 0.0 : a.vel2[q];
+    acc = 0.0;
+    pr = -fi;
+    fe = -fi;
+  } else {  // MAIN.F90:472-481
+    const double mpdc = a.mats[a.matidx[J]].damp * mass;
+    acc = (fe - fi - mpdc * v) / (mass + 0.5 * a.dt * mpdc);
+    v = v + 0.5 * a.dt * acc;
+    pr = 0.0;
+  }
+  ee += 0.5 * (fe + fe_old) * a.dsp[m];
+  ke += 0.5 * mass * v * v;
+  const int b = a.body_id ? a.body_id[J] : 1;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)  // constant indices: the sums stay in registers
+    if (q == k) {
+      if (b == 1) tf[k] += pr;
+      else if (b == 2) tf[3 + k] += pr;
+    }
+  a.fint[m] = fi;
+  a.fext[m] = fe;
+  a.acl[m] = acc;
+  a.prforce[m] = pr;
+  if (a.predict) {  // MAIN.F90:353-355 of the next step
+    const double d = a.dt * v + a.dt * a.dt * 0.5 * acc;
+    a.dsp[m] = d;
+    a.dsp_tot[m] = a.dsp_tot[m] + d;
+    v = v + a.dt * 0.5 * acc;
+  }
+  a.vel[m] = v;
+}
+
+// One block reduction of the eight step sums, then one atomic per sum into
+// this block's slot.  Every thread of the block takes part.
+__device__ __forceinline__ void step_sums(const TiledForceArgs& a, double ke, double ee, const double* tf,
+                                          double* red) {
+  double v[8] = {ke, ee, tf[0], tf[1], tf[2], tf[3], tf[4], tf[5]};
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) red[wid * 8 + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double tsum = 0.0;
+    for (int w = 0; w < nw; ++w) tsum += red[w * 8 + threadIdx.x];
+    const int sl = blockIdx.x % kSlots;
+    double* dst = threadIdx.x == 0 ? &a.acc->ke[sl] : (threadIdx.x == 1 ? &a.acc->ee[sl] : &a.acc->tf[threadIdx.x - 2][sl]);
+    if (tsum != 0.0) atomicAdd(dst, tsum);
+  }
+}
+
 // TS = storage of T_i (float / double), A = accumulation, F64 = record width
 template <typename TS, typename A, bool F64, int KG, int KU>
 __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
@@ -420,7 +499,7 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
     e = a.colptr[J] + q;
     c1 = a.colptr[J + 1];
   }
-  double ke = 0.0, ee = 0.0, tf0 = 0.0, tf1 = 0.0, tf2 = 0.0, tf3 = 0.0, tf4 = 0.0, tf5 = 0.0;
+  double ke = 0.0, ee = 0.0, tf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   unsigned st = 0;
   if (valid) {
     A f0 = A(0), f1 = A(0), f2 = A(0);
@@ -490,64 +569,293 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
         e2 += __shfl_xor_sync(gmask, e2, o);
       }
     }
-    if (q < 3) {
-      const int64_t m = 3 * J + q;
-      double fi = (double)(q == 0 ? f0 : (q == 1 ? f1 : f2));
-      if (a.fadd) fi += a.fadd[m];
-      double fe = (q == 0 ? e0 : (q == 1 ? e1 : e2));
-      if (!isfinite(fi)) st |= MEGA_ST_NONFINITE;
-      const double mass = a.mass[m];
-      const double fe_old = a.fext[m];
-      double v = a.vel[m], acc, pr;
-      if (a.ebc[m] == 1) {  // MAIN.F90:438-445
-        v = 0.0;
-        acc = 0.0;
-        pr = -fi;
-        fe = -fi;
-      } else {  // MAIN.F90:472-481
-        const double mpdc = a.mats[a.matidx[J]].damp * mass;
-        acc = (fe - fi - mpdc * v) / (mass + 0.5 * a.dt * mpdc);
-        v = v + 0.5 * a.dt * acc;
-        pr = 0.0;
-      }
-      ee += 0.5 * (fe + fe_old) * a.dsp[m];
-      ke += 0.5 * mass * v * v;
-      const int b = a.body_id ? a.body_id[J] : 1;
-      if (b == 1) { if (q == 0) tf0 += pr; else if (q == 1) tf1 += pr; else tf2 += pr; }
-      else if (b == 2) { if (q == 0) tf3 += pr; else if (q == 1) tf4 += pr; else tf5 += pr; }
-      a.fint[m] = fi;
-      a.fext[m] = fe;
-      a.acl[m] = acc;
-      a.prforce[m] = pr;
-      if (a.predict) {  // MAIN.F90:353-355 of the next step
-        const double d = a.dt * v + a.dt * a.dt * 0.5 * acc;
-        a.dsp[m] = d;
-        a.dsp_tot[m] = a.dsp_tot[m] + d;
-        v = v + a.dt * 0.5 * acc;
-      }
-      a.vel[m] = v;
+    if (q < 3) correct_dof(a, J, q, (double)(q == 0 ? f0 : (q == 1 ? f1 : f2)), q == 0 ? e0 : (q == 1 ? e1 : e2), ke, ee, tf, st);
+  }
+  step_sums(a, ke, ee, tf, red);
+  if (st) atomicOr(a.status, st);
+}
+
+// ---- record streams through the copy engine ------------------------------
+// The variants below ask the copy engine (cp.async.bulk) for the tile's
+// whole record range, in kChunks chunks with an mbarrier each, before the
+// block stages its neighbour data: the records stream into shared memory
+// while the threads gather, and the entry loop then reads them from shared
+// memory.  Sources are this GPU's record arrays (no peer memory, no
+// multicast).  Every wait is bounded; a wait that gives up raises
+// MEGA_ST_WAIT_TIMEOUT and the lane skips its sums.
+constexpr int kChunks = 4;
+constexpr int kPollLimit = 1 << 16;
+
+// Thread 0: the barriers, then the copies of entries [0, ne) of the tile
+// (src points at its first record, RB bytes each) into rec.
+template <int RB>
+__device__ __forceinline__ void issue_records(uint64_t* bar, unsigned char* rec, const unsigned char* src,
+                                              int64_t ne) {
+  if (threadIdx.x != 0) return;
+#pragma unroll
+  for (int c = 0; c < kChunks; ++c) mbar_init(&bar[c], 1);
+  mbar_fence_init();
+#pragma unroll
+  for (int c = 0; c < kChunks; ++c) {
+    const int64_t lo = c * ne / kChunks, hi = (c + 1) * ne / kChunks;
+    const uint32_t bytes = (uint32_t)((hi - lo) * RB);
+    mbar_arrive_expect(&bar[c], bytes);
+    for (uint32_t off = 0; off < bytes; off += 32768u)
+      bulk_load(rec + lo * RB + off, src + lo * RB + off, min(32768u, bytes - off), &bar[c]);
+  }
+}
+
+// Wait for the chunks holding entries [a, b) of the tile.
+__device__ __forceinline__ bool wait_records(uint64_t* bar, int64_t ne, int64_t a, int64_t b) {
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < kChunks; ++c) {
+    const int64_t lo = c * ne / kChunks, hi = (c + 1) * ne / kChunks;
+    if (ok && lo < b && hi > a) ok = mbar_wait_bounded(&bar[c], 0, kPollLimit);
+  }
+  return ok;
+}
+
+// Thread 0 before the block retires: no copy of the block is left in flight.
+__device__ __forceinline__ void drain_records(uint64_t* bar) {
+  if (threadIdx.x != 0) return;
+#pragma unroll
+  for (int c = 0; c < kChunks; ++c) mbar_wait_bounded(&bar[c], 0, kPollLimit);
+}
+
+template <typename A, bool F64, bool INTERP, int KG>
+__global__ void __launch_bounds__(64 * KG) k_defgrad_b(int32_t n, int32_t R, int32_t jmax, int32_t recmax,
+                                                       const int64_t* __restrict__ rowptr, const void* __restrict__ pk,
+                                                       const int32_t* __restrict__ jset, const int32_t* __restrict__ jcnt,
+                                                       const double* __restrict__ dsp, const double* __restrict__ dsp_tot,
+                                                       const double* __restrict__ sdphi, const double* __restrict__ shp,
+                                                       double* __restrict__ dsp_tot_phy, double* __restrict__ fg,
+                                                       StepAccum* __restrict__ acc, unsigned* __restrict__ status) {
+  constexpr int RB = F64 ? 32 : 16;
+  extern __shared__ __align__(128) unsigned char smb[];
+  __shared__ uint64_t bar[kChunks];
+  if (acc && blockIdx.x == 0 && threadIdx.x < kSlots) {
+    acc->newton_iters[threadIdx.x] = 0ull;
+    acc->plastic[threadIdx.x] = 0ull;
+  }
+  const int64_t t = blockIdx.x;
+  const int64_t r0 = t * R, r1 = min((int64_t)n, r0 + R);
+  const int64_t e0 = rowptr[r0], ne = rowptr[r1] - e0;
+  issue_records<RB>(bar, smb, (const unsigned char*)pk + e0 * RB, ne);
+  const int cnt = jcnt[t];
+  const int32_t* js = jset + t * (int64_t)jmax;
+  unsigned char* stg = smb + (size_t)recmax * RB;
+  double* su = reinterpret_cast<double*>(stg);
+  double* sd = su + 3 * cnt;
+  float4* sa = reinterpret_cast<float4*>(stg);
+  float2* sb = reinterpret_cast<float2*>(sa + cnt);
+  const int64_t i = r0 + threadIdx.x / KG;
+  const int q = threadIdx.x & (KG - 1);
+  const unsigned gmask = group_mask<KG>();
+  const bool valid = threadIdx.x / KG < R && i < n;
+  double ur0 = 0.0, ur1 = 0.0, ur2 = 0.0, dr0 = 0.0, dr1 = 0.0, dr2 = 0.0;
+  if (!F64) {
+    ur0 = dsp_tot[3 * r0]; ur1 = dsp_tot[3 * r0 + 1]; ur2 = dsp_tot[3 * r0 + 2];
+    dr0 = dsp[3 * r0]; dr1 = dsp[3 * r0 + 1]; dr2 = dsp[3 * r0 + 2];
+  }
+  for (int l = threadIdx.x; l < cnt; l += blockDim.x) {
+    const int64_t g = js[l];
+    const double a0 = dsp_tot[3 * g], a1 = dsp_tot[3 * g + 1], a2 = dsp_tot[3 * g + 2];
+    const double b0 = dsp[3 * g], b1 = dsp[3 * g + 1], b2 = dsp[3 * g + 2];
+    if (F64) {
+      su[3 * l] = a0; su[3 * l + 1] = a1; su[3 * l + 2] = a2;
+      sd[3 * l] = b0; sd[3 * l + 1] = b1; sd[3 * l + 2] = b2;
+    } else {
+      sa[l] = make_float4((float)(a0 - ur0), (float)(a1 - ur1), (float)(a2 - ur2), (float)(b0 - dr0));
+      sb[l] = make_float2((float)(b1 - dr1), (float)(b2 - dr2));
     }
   }
-  // one block reduction of the eight sums, then one atomic per sum into this block's slot
-  double v[8] = {ke, ee, tf0, tf1, tf2, tf3, tf4, tf5};
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < 8; ++k) red[wid * 8 + k] = v[k];
   __syncthreads();
-  if (threadIdx.x < 8) {
-    const int nw = (blockDim.x + 31) >> 5;
-    double tsum = 0.0;
-    for (int w = 0; w < nw; ++w) tsum += red[w * 8 + threadIdx.x];
-    const int sl = blockIdx.x % kSlots;
-    double* dst = threadIdx.x == 0 ? &a.acc->ke[sl] : (threadIdx.x == 1 ? &a.acc->ee[sl] : &a.acc->tf[threadIdx.x - 2][sl]);
-    if (tsum != 0.0) atomicAdd(dst, tsum);
+  if (!valid) {
+    drain_records(bar);
+    return;
   }
+  const int64_t pa = rowptr[i] - e0, pb = rowptr[i + 1] - e0;
+  const bool ok = __all_sync(gmask, wait_records(bar, ne, pa, pb));
+  const double ui0 = dsp_tot[3 * i], ui1 = dsp_tot[3 * i + 1], ui2 = dsp_tot[3 * i + 2];
+  const double di0 = dsp[3 * i], di1 = dsp[3 * i + 1], di2 = dsp[3 * i + 2];
+  const float fu0 = (float)(ui0 - ur0), fu1 = (float)(ui1 - ur1), fu2 = (float)(ui2 - ur2);
+  const float fd0 = (float)(di0 - dr0), fd1 = (float)(di1 - dr1), fd2 = (float)(di2 - dr2);
+  A F[9], L[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) { F[k] = A(0); L[k] = A(0); }
+  double ph0 = 0.0, ph1 = 0.0, ph2 = 0.0;
+  if (ok) {
+    const float4* rec32 = reinterpret_cast<const float4*>(smb);
+    const double2* rec64 = reinterpret_cast<const double2*>(smb);
+#pragma unroll 4
+    for (int64_t p = pa + q; p < pb; p += KG) {
+      A g0, g1, g2;
+      int l;
+      if (F64) {
+        const double2 ra = rec64[2 * p], rb = rec64[2 * p + 1];
+        g0 = (A)ra.x; g1 = (A)ra.y; g2 = (A)rb.x; l = (int)__double_as_longlong(rb.y);
+      } else {
+        const float4 r = rec32[p];
+        g0 = (A)r.x; g1 = (A)r.y; g2 = (A)r.z; l = __float_as_int(r.w);
+      }
+      A u0, u1, u2, d0, d1, d2;
+      double dj0, dj1, dj2;
+      if (F64) {
+        u0 = (A)(su[3 * l] - ui0); u1 = (A)(su[3 * l + 1] - ui1); u2 = (A)(su[3 * l + 2] - ui2);
+        dj0 = sd[3 * l]; dj1 = sd[3 * l + 1]; dj2 = sd[3 * l + 2];
+        d0 = (A)(dj0 - di0); d1 = (A)(dj1 - di1); d2 = (A)(dj2 - di2);
+      } else {
+        const float4 va = sa[l];
+        const float2 vb = sb[l];
+        u0 = (A)(va.x - fu0); u1 = (A)(va.y - fu1); u2 = (A)(va.z - fu2);
+        d0 = (A)(va.w - fd0); d1 = (A)(vb.x - fd1); d2 = (A)(vb.y - fd2);
+        if (INTERP) { dj0 = dr0 + (double)va.w; dj1 = dr1 + (double)vb.x; dj2 = dr2 + (double)vb.y; }
+        else { dj0 = dj1 = dj2 = 0.0; }
+      }
+      F[0] += u0 * g0; F[1] += u0 * g1; F[2] += u0 * g2;
+      F[3] += u1 * g0; F[4] += u1 * g1; F[5] += u1 * g2;
+      F[6] += u2 * g0; F[7] += u2 * g1; F[8] += u2 * g2;
+      L[0] += d0 * g0; L[1] += d0 * g1; L[2] += d0 * g2;
+      L[3] += d1 * g0; L[4] += d1 * g1; L[5] += d1 * g2;
+      L[6] += d2 * g0; L[7] += d2 * g1; L[8] += d2 * g2;
+      if (INTERP) {
+        const double s = shp[e0 + p];
+        ph0 += s * dj0; ph1 += s * dj1; ph2 += s * dj2;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < KG; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      F[k] += __shfl_xor_sync(gmask, F[k], o);
+      L[k] += __shfl_xor_sync(gmask, L[k], o);
+    }
+    if (INTERP) {
+      ph0 += __shfl_xor_sync(gmask, ph0, o);
+      ph1 += __shfl_xor_sync(gmask, ph1, o);
+      ph2 += __shfl_xor_sync(gmask, ph2, o);
+    }
+  }
+  if (q == 0) {
+    if (!ok) {
+      atomicOr(status, (unsigned)MEGA_ST_WAIT_TIMEOUT);
+    } else {
+      const double ui[3] = {ui0, ui1, ui2}, di[3] = {di0, di1, di2};
+      const double sd3[3] = {sdphi[3 * i], sdphi[3 * i + 1], sdphi[3 * i + 2]};
+      double* o = fg + 18 * i;
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+          o[3 * k + l] = (k == l ? 1.0 : 0.0) + ((double)F[3 * k + l] + ui[k] * sd3[l]);
+          o[9 + 3 * k + l] = (double)L[3 * k + l] + di[k] * sd3[l];
+        }
+      if (INTERP) {
+        dsp_tot_phy[3 * i] += ph0;
+        dsp_tot_phy[3 * i + 1] += ph1;
+        dsp_tot_phy[3 * i + 2] += ph2;
+      }
+    }
+  }
+  drain_records(bar);
+}
+
+template <typename TS, typename A, bool F64, int KG>
+__global__ void __launch_bounds__(64 * KG) k_force_b(TiledForceArgs a) {
+  constexpr int RB = F64 ? 32 : 16;
+  extern __shared__ __align__(128) unsigned char smb[];
+  __shared__ uint64_t bar[kChunks];
+  __shared__ double red[8 * 8];
+  const int64_t t = blockIdx.x;
+  const int64_t c0 = t * a.R, c1 = min((int64_t)a.n, c0 + a.R);
+  const int64_t e0 = a.colptr[c0], ne = a.colptr[c1] - e0;
+  issue_records<RB>(bar, smb, (const unsigned char*)a.pk + e0 * RB, ne);
+  const int cnt = a.jcnt[t];
+  const int nv = a.has_body ? 12 : 9;
+  TS* sT = reinterpret_cast<TS*>(smb + (size_t)a.recmax * RB);
+  const int32_t* js = a.jset + t * (int64_t)a.jmax;
+  const TS* tm = (const TS*)a.tmat;
+  const int64_t J = c0 + threadIdx.x / KG;
+  const int q = threadIdx.x & (KG - 1);
+  const unsigned gmask = group_mask<KG>();
+  const bool valid = threadIdx.x / KG < a.R && J < a.n;
+  for (int l = threadIdx.x; l < cnt; l += blockDim.x) {
+    const TS* src = tm + 12 * (int64_t)js[l];
+    TS v[12];
+    if (sizeof(TS) == 4) {
+      const float4* s4 = reinterpret_cast<const float4*>(src);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float4 x = __ldg(s4 + k);
+        v[4 * k] = (TS)x.x; v[4 * k + 1] = (TS)x.y; v[4 * k + 2] = (TS)x.z; v[4 * k + 3] = (TS)x.w;
+      }
+    } else {
+      const double2* s2 = reinterpret_cast<const double2*>(src);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double2 x = __ldg(s2 + k);
+        v[2 * k] = (TS)x.x; v[2 * k + 1] = (TS)x.y;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) sT[l * nv + k] = v[k];
+    if (nv == 12) { sT[l * nv + 9] = v[9]; sT[l * nv + 10] = v[10]; sT[l * nv + 11] = v[11]; }
+  }
+  __syncthreads();
+  double ke = 0.0, ee = 0.0, tf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  unsigned st = 0;
+  if (valid) {
+    const int64_t pa = a.colptr[J] - e0, pb = a.colptr[J + 1] - e0;
+    const bool ok = __all_sync(gmask, wait_records(bar, ne, pa, pb));
+    A f0 = A(0), f1 = A(0), f2 = A(0);
+    double b0 = 0.0, b1 = 0.0, b2 = 0.0;
+    if (ok) {
+      const float4* rec32 = reinterpret_cast<const float4*>(smb);
+      const double2* rec64 = reinterpret_cast<const double2*>(smb);
+#pragma unroll 4
+      for (int64_t p = pa + q; p < pb; p += KG) {
+        A g0, g1, g2;
+        int l;
+        if (F64) {
+          const double2 ra = rec64[2 * p], rb = rec64[2 * p + 1];
+          g0 = (A)ra.x; g1 = (A)ra.y; g2 = (A)rb.x; l = (int)__double_as_longlong(rb.y);
+        } else {
+          const float4 r = rec32[p];
+          g0 = (A)r.x; g1 = (A)r.y; g2 = (A)r.z; l = __float_as_int(r.w);
+        }
+        const TS* T = sT + l * nv;
+        f0 += (A)T[0] * g0 + (A)T[1] * g1 + (A)T[2] * g2;
+        f1 += (A)T[3] * g0 + (A)T[4] * g1 + (A)T[5] * g2;
+        f2 += (A)T[6] * g0 + (A)T[7] * g1 + (A)T[8] * g2;
+        if (a.has_body) {
+          const double s = a.tshp[e0 + p];
+          b0 += s * (double)T[9]; b1 += s * (double)T[10]; b2 += s * (double)T[11];
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < KG; o <<= 1) {
+      f0 += __shfl_xor_sync(gmask, f0, o);
+      f1 += __shfl_xor_sync(gmask, f1, o);
+      f2 += __shfl_xor_sync(gmask, f2, o);
+      if (a.has_body) {
+        b0 += __shfl_xor_sync(gmask, b0, o);
+        b1 += __shfl_xor_sync(gmask, b1, o);
+        b2 += __shfl_xor_sync(gmask, b2, o);
+      }
+    }
+    if (!ok) {
+      if (q == 0) st |= MEGA_ST_WAIT_TIMEOUT;
+    } else if (q < 3) {
+      correct_dof(a, J, q, (double)(q == 0 ? f0 : (q == 1 ? f1 : f2)), q == 0 ? b0 : (q == 1 ? b1 : b2), ke, ee, tf,
+                  st);
+    }
+  }
+  step_sums(a, ke, ee, tf, red);
   if (st) atomicOr(a.status, st);
+  drain_records(bar);
 }
 
 inline unsigned grid_for(int64_t work, int block) { return (unsigned)((work + block - 1) / block); }
@@ -584,12 +892,23 @@ int build_tiles(cudaStream_t s, int32_t n, const int64_t* ptr, const int32_t* id
     if (hovf) continue;  // too many distinct neighbours: halve the tile
     int32_t mx = 0;
     for (int32_t v : hc) mx = std::max(mx, v);
+    // the longest record range of any tile (sizes the streamed variants)
+    int32_t* ent = nullptr;
+    MEGA_ALLOC(scratch, ent, ntiles);
+    k_tile_entries<<<grid_for(ntiles, 256), 256, 0, s>>>(n, R, ntiles, ptr, ent);
+    MEGA_CHECK_LAUNCH();
+    std::vector<int32_t> he(ntiles);
+    MEGA_TRY(cudaMemcpyAsync(he.data(), ent, sizeof(int32_t) * ntiles, cudaMemcpyDeviceToHost, s));
+    MEGA_TRY(cudaStreamSynchronize(s));
+    int32_t emax = 0;
+    for (int32_t v : he) emax = std::max(emax, v);
     // keep the trial buffers: move ownership into the persistent pool
     pool.adopt(trial);
     ts.R = R;
     ts.ntiles = ntiles;
     ts.jmax = jmax;
     ts.maxcnt = mx;
+    ts.recmax = emax;
     ts.jset = jset;
     ts.jcnt = jcnt;
     ts.lidx = lidx;
@@ -617,8 +936,10 @@ int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* 
 }
 
 // The launch variants, in the order the autotuner tries them:
-// (KG, KU) = (4, 4), (4, 2), (4, 1), (8, 2).
-constexpr int kVariants = 4;
+// (KG, KU) = (4, 4), (4, 2), (4, 1), (8, 2) with register-held record
+// streams, then KG = 4, 8 with the records streamed into shared memory.
+constexpr int kVariants = kTiledVariants;
+constexpr int kBulkSmemMax = 227 * 1024;  // dynamic shared memory of one block on sm_100
 
 template <typename K>
 static int raise_smem(K k, int lim) {
@@ -637,22 +958,63 @@ static int configure_variant(int lim) {
   return raise_smem(k_force_t<double, double, true, KG, KU>, lim);
 }
 
+template <int KG>
+static int configure_bulk(int lim) {
+  int r = 0;
+  if ((r = raise_smem(k_defgrad_b<float, false, true, KG>, lim))) return r;
+  if ((r = raise_smem(k_defgrad_b<float, false, false, KG>, lim))) return r;
+  if ((r = raise_smem(k_defgrad_b<double, true, true, KG>, lim))) return r;
+  if ((r = raise_smem(k_defgrad_b<double, true, false, KG>, lim))) return r;
+  if ((r = raise_smem(k_force_b<float, float, false, KG>, lim))) return r;
+  return raise_smem(k_force_b<double, double, true, KG>, lim);
+}
+
 // Raise the dynamic shared-memory limit of the tiled kernels once (outside
 // any stream capture): a tile stages at most 1024 neighbours, 96 KB for the
-// double-precision T_i of the force kernel.
+// double-precision T_i of the force kernel; the streamed variants add the
+// tile's records.
 int configure_tiled_kernels() {
   static bool done = false;
   if (done) return 0;
   const int lim = 12 * 8 * 1024 + 1024;
   int r = 0;
   if ((r = configure_variant<4, 4>(lim)) || (r = configure_variant<4, 2>(lim)) ||
-      (r = configure_variant<4, 1>(lim)) || (r = configure_variant<8, 2>(lim)))
+      (r = configure_variant<4, 1>(lim)) || (r = configure_variant<8, 2>(lim)) ||
+      (r = configure_bulk<4>(kBulkSmemMax)) || (r = configure_bulk<8>(kBulkSmemMax)))
     return r;
   done = true;
   return 0;
 }
 
 int tiled_variants() { return kVariants; }
+
+bool tiled_variant_fits(const TileSet& ts, bool mixed, int variant, bool force, bool has_body) {
+  if (variant < 0 || variant >= kVariants) return false;
+  if (variant < 4) return true;
+  const size_t stage = force ? (mixed ? sizeof(float) : sizeof(double)) * (has_body ? 12 : 9) : (mixed ? 24 : 48);
+  return (size_t)ts.recmax * (mixed ? 16 : 32) + stage * (size_t)ts.maxcnt <= (size_t)kBulkSmemMax;
+}
+
+template <int KG>
+static int defgrad_bulk(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
+                        const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
+                        const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc,
+                        unsigned* status) {
+  const size_t smem = (size_t)ts.recmax * (mixed ? 16 : 32) + (mixed ? 24 : 48) * (size_t)ts.maxcnt;
+  if (smem > (size_t)kBulkSmemMax) return MEGA_ERR_UNSUPPORTED;
+  const unsigned grid = (unsigned)ts.ntiles;
+  const int block = ts.R * KG;
+  if (mixed) {
+    auto k = interp ? k_defgrad_b<float, false, true, KG> : k_defgrad_b<float, false, false, KG>;
+    k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, ts.recmax, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
+                                dsp_tot_phy, fg, acc, status);
+  } else {
+    auto k = interp ? k_defgrad_b<double, true, true, KG> : k_defgrad_b<double, true, false, KG>;
+    k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, ts.recmax, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
+                                dsp_tot_phy, fg, acc, status);
+  }
+  return 0;
+}
 
 template <int KG, int KU>
 static void defgrad_variant(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
@@ -676,8 +1038,15 @@ static void defgrad_variant(cudaStream_t s, bool mixed, bool interp, int32_t n, 
 int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
                          const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
                          const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc,
-                         int variant) {
+                         unsigned* status, int variant) {
+  int r = 0;
   switch (variant) {
+    case 4: r = defgrad_bulk<4>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc,
+                                status);
+      break;
+    case 5: r = defgrad_bulk<8>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc,
+                                status);
+      break;
     case 1: defgrad_variant<4, 2>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
       break;
     case 2: defgrad_variant<4, 1>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
@@ -687,7 +1056,21 @@ int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, con
     default: defgrad_variant<4, 4>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg,
                                    acc);
   }
+  if (r) return r;
   MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+template <int KG>
+static int force_bulk(cudaStream_t s, bool mixed, const TiledForceArgs& a) {
+  const int nv = a.has_body ? 12 : 9;
+  const size_t smem = (size_t)a.recmax * (mixed ? 16 : 32) + (mixed ? sizeof(float) : sizeof(double)) * nv *
+                      (size_t)a.maxcnt;
+  if (smem > (size_t)kBulkSmemMax) return MEGA_ERR_UNSUPPORTED;
+  const unsigned grid = (unsigned)a.ntiles;
+  const int block = a.R * KG;
+  if (mixed) k_force_b<float, float, false, KG><<<grid, block, smem, s>>>(a);
+  else k_force_b<double, double, true, KG><<<grid, block, smem, s>>>(a);
   return 0;
 }
 
@@ -702,12 +1085,16 @@ static void force_variant(cudaStream_t s, bool mixed, const TiledForceArgs& a) {
 }
 
 int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a, int variant) {
+  int r = 0;
   switch (variant) {
     case 1: force_variant<4, 2>(s, mixed, a); break;
     case 2: force_variant<4, 1>(s, mixed, a); break;
     case 3: force_variant<8, 2>(s, mixed, a); break;
+    case 4: r = force_bulk<4>(s, mixed, a); break;
+    case 5: r = force_bulk<8>(s, mixed, a); break;
     default: force_variant<4, 4>(s, mixed, a);
   }
+  if (r) return r;
   MEGA_CHECK_LAUNCH();
   return 0;
 }

@@ -10,6 +10,7 @@ struct TileSet {
   int64_t ntiles = 0;
   int32_t jmax = 0;        // stride of jset per tile
   int32_t maxcnt = 0;      // largest neighbour set of any tile
+  int32_t recmax = 0;      // most list entries of any tile (its packed-record range)
   int32_t* jset = nullptr; // [ntiles][jmax] sorted node ids
   int32_t* jcnt = nullptr; // [ntiles]
   uint16_t* lidx = nullptr;  // per entry: rank of its neighbour in the tile's set
@@ -21,6 +22,7 @@ struct TiledForceArgs {
   int64_t ntiles;
   int32_t jmax;
   int32_t maxcnt;
+  int32_t recmax;
   const int32_t* jset;
   const int32_t* jcnt;
   const int64_t* colptr;
@@ -42,6 +44,7 @@ struct TiledForceArgs {
   double* dsp_tot;
   double* prforce;
   const double* fadd;     // 3 per node added to the internal force (NSNI), or null
+  const double* vel2;     // prescribed velocities of fixity code 2 for this step (3), or null
   double dt;
   StepAccum* acc;
   unsigned* status;
@@ -59,12 +62,18 @@ int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* 
 int pack_transposed32(cudaStream_t s, int64_t m, const uint16_t* lidx, const float4* in, const int64_t* pos,
                       float4* out);
 int configure_tiled_kernels();
-// launch variants of the two gathers (lanes per row x records in flight)
+// launch variants of the two gathers: lanes per row x records in flight
+// (register streams, variants 0-3), and lanes per row with the tile's
+// records streamed into shared memory by the copy engine (variants 4, 5)
+constexpr int kTiledVariants = 6;
 int tiled_variants();
+// whether a variant's shared memory fits the row (defgrad) or column (force) tiles
+bool tiled_variant_fits(const TileSet& ts, bool mixed, int variant, bool force, bool has_body);
+// MEGA_ERR_UNSUPPORTED when the variant's shared memory does not fit the tiles
 int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
                          const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
                          const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc,
-                         int variant = 0);
+                         unsigned* status, int variant = 0);
 int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a, int variant = 0);
 
 }  // namespace mega

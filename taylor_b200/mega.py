@@ -228,10 +228,23 @@ class Mega:
         """Pick the fastest launch variant of each gather; returns the chosen
         (defgrad, force) variants and the per-variant mean times (ms)."""
         ch = np.zeros(2, np.int32)
-        t = np.zeros(8, np.float32)
+        t = np.zeros(2 * _lib.TUNE_VARIANTS, np.float32)
         check(_lib.lib().mega_autotune(self.h, float(dt), self.mode_bits(mode), int(reps), ptr(ch), ptr(t)),
               "autotune")
-        return (int(ch[0]), int(ch[1])), t.reshape(2, 4)
+        return (int(ch[0]), int(ch[1])), t.reshape(2, _lib.TUNE_VARIANTS)
+
+    def set_fixity2(self, times, disp):
+        """Windows of fixity code 2 (FIXITY2_TIME (steps,2), FIXITY2_NONZERO_EBC
+        (steps,3)): a code-2 DOF moves at disp[k, j] / (t2 - t1) inside window k."""
+        t = np.asarray(times, np.float64).reshape(-1, 2)
+        d = np.asarray(disp, np.float64).reshape(-1, 3)
+        tf = np.ascontiguousarray(t.ravel(order="F"))
+        df = np.ascontiguousarray(d.ravel(order="F"))
+        check(_lib.lib().mega_set_fixity2(self.h, len(t), ptr(tf), ptr(df)), "set_fixity2")
+
+    def set_variants(self, defgrad, force, mode="mixed"):
+        """Pin the gathers' launch variants for one precision."""
+        check(_lib.lib().mega_set_variants(self.h, self.mode_bits(mode), int(defgrad), int(force)), "set_variants")
 
     def set_precisions(self, fp64=True, mixed=True):
         check(_lib.lib().mega_set_precisions(self.h, (1 if fp64 else 0) | (2 if mixed else 0)), "set_precisions")

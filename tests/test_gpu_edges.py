@@ -170,3 +170,27 @@ def test_snapshot_equals_single_downloads(tmp_path):
     assert lines[4].split() == ["POINTS", str(c["n"]), "double"]
     assert sum(1 for l in lines if l.startswith("SCALARS")) == 3 + 3 + 6 + 1
     m.close()
+
+
+def test_release_cached_memory():
+    """Finalised contexts leave their blocks cached in the library and the
+    device pool; mega_release_cached_memory returns them to the driver (a
+    host program with its own allocator sees the memory free again) and the
+    library keeps working afterwards."""
+    import torch
+    c = cases.taylor_bar(h=0.4e-3)
+    free0 = torch.cuda.mem_get_info()[0]
+    m = mega.Mega(c, _lib.params(**cases.param_kwargs(c)))
+    m.search_and_shapes()
+    held = m.device_bytes()
+    m.close()
+    assert held > 0
+    free_cached = torch.cuda.mem_get_info()[0]
+    assert _lib.lib().mega_release_cached_memory() == 0
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 >= free_cached
+    assert free1 >= free0 - (64 << 20)  # back to within the driver's own granularity
+    again = mega.Mega(c, _lib.params(**cases.param_kwargs(c)))
+    again.search_and_shapes()
+    again.step(5, 3.9e-8)
+    again.close()
