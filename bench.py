@@ -459,8 +459,10 @@ def learned_runs(args, rank):
 
 def pmb_run(args):
     """Bond-based PMB plate (400 x 400 x 16 particles at 0.25 mm, horizon
-    3.015 h, pre-notch cut on the device): the mixed run (float bond force,
-    double positions) steps the whole job, the FP64 run a tenth of it."""
+    3.015 h, pre-notch cut on the device, the notch-side edge halves driven
+    apart at a sustained +-5 m/s): the mixed run (float bond force, double
+    positions) steps the whole job, the FP64 run a tenth of it; broken bonds
+    and the crack tip (from the particles' local damage) are reported."""
     from taylor_b200 import cases, mega
     nz = max(4, args.pmb_nx // 25)
     case = cases.pd_plate(nx=args.pmb_nx, ny=args.pmb_nx, nz=nz, notch=20e-3 * args.pmb_nx / 400)
@@ -470,7 +472,7 @@ def pmb_run(args):
     peak, _ = measured_peak()
     for mode, steps in (("mixed", args.pmb_steps), ("fp64", max(10, args.pmb_steps // 10))):
         t0 = time.perf_counter()
-        p = mega.Pmb(case, None, mode=mode)
+        p = mega.Pmb(case, None, fixed=case["fixed"], mode=mode)
         init_s = time.perf_counter() - t0
         ncut = p.cut(*cases.notch_rect(case))
         p.step(3, dt)
@@ -478,7 +480,8 @@ def pmb_run(args):
         clk.start()
         ms = p.step(steps, dt, timed=True)
         clocks = clk.stop()
-        _, nbroken = p.download(3)
+        dmg, nbroken = p.download(4)
+        tip = cases.crack_tip(case, dmg)
         bonds = p.nnz
         # per step: bond column index and broken bit; per particle u in/out,
         # velocity and acceleration read+write, X, volume, fixity
@@ -486,6 +489,8 @@ def pmb_run(args):
         gbs = algo / (ms / steps / 1e3) / 1e9
         out[mode] = dict(steps=steps, ms_per_step=ms / steps, particle_steps_per_s=n * steps / (ms / 1e3),
                          bonds=bonds, notch_bonds=ncut, broken_bond_entries=nbroken, init_s=init_s,
+                         crack_tip_x_m=tip, crack_growth_m=None if tip is None else tip - case["notch"],
+                         damaged_particles=int(np.count_nonzero(dmg > 0.35)),
                          roofline=dict(bound="hbm", achieved=gbs, peak=peak, unit="GB/s", frac=gbs / peak,
                                        algorithmic_bytes_per_step=algo),
                          clocks=clocks)

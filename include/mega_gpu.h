@@ -142,6 +142,10 @@ typedef struct mega_params {
   double  gravity[3];      /* IGRAVITY                                        */
   double  dist_max[3];     /* GXDIST_MAX, GYDIST_MAX, GZDIST_MAX              */
   double  newton_rtol;     /* rate-dependent law: relative residual tolerance */
+  int32_t auto_ts;         /* AUTO_TS (logical): construct_fint_pd_gpu returns the
+                              step of its CFL rule in DLT_FINT (FINT_PD.F90:690-754) */
+  int32_t reserved;
+  double  dlt_fac;         /* DLT_FAC, the factor of that step                 */
 } mega_params;
 
 /* Fill p with the reference's defaults for the Taylor-bar deck
@@ -214,8 +218,9 @@ int mega_constitution(const mega_params* p, int32_t n,
                       const double* props, double dlt, double* state,
                       double* stress, int32_t* iters);
 
-/* CONSTRUCT_FINT (FINT.F90:16-25) with the reference's argument meaning,
- * Lagrangian DNI path.  When linit != 0 the shape functions are computed
+/* CONSTRUCT_FINT (FINT.F90:16-25) with the reference's argument meaning in a
+ * shorter list (the arrays the Lagrangian DNI path reads), scalars by value;
+ * construct_fint_gpu below takes the full list.  When linit != 0 the shape functions are computed
  * (RK1) and written to gstack_shp / gstack_dshp; otherwise they are read.
  * In/out arrays follow FINT.F90: gstress, gstrain (6,n), gstate (20,n).
  * Outputs: fint, fext (3n), gmax_wvel (n), gstrain_eq (n), *gint_work
@@ -234,6 +239,53 @@ int mega_construct_fint(const mega_params* p, int32_t n,
                         double* fint, double* fext,
                         double* gmax_wvel, double* gstrain_eq,
                         double* gint_work);
+
+/* ---- the two force subroutines with the reference's own argument lists --
+ * construct_fint_gpu and construct_fint_pd_gpu take CONSTRUCT_FINT's
+ * (FINT.F90:16-25) and CONSTRUCT_FINT_PD's (FINT_PD.F90:16-25) arguments in
+ * their order, every one by reference as gfortran passes them (INTEGER
+ * int32_t*, LOGICAL LINIT int32_t*, DOUBLE PRECISION double*, arrays
+ * column-major), so HANDELER's calls (HANDELER.F90:285-306) bind them
+ * unchanged through BIND(C).  The CONTROL module values the reference
+ * reads as globals (RK_*, QL*, ITYPE_INT, LLAGRANGIAN, LFINITE_STRAIN,
+ * SHSUP, IGRAVITY, AUTO_TS, DLT_FAC, ...) come from one earlier
+ * mega_fint_control call.  Paths: Lagrangian DNI and NSNI (ITYPE_INT = 2:
+ * GSM_LEN in, GSTACK_DDSHP written at LINIT and read after, LOCAL_DX/DY/
+ * DZ_STRESS in/out) and semi-Lagrangian DNI (LLAGRANGIAN = .FALSE.: RK1 on
+ * GCOO_CUURENT in every call, GSTACK_SHP/DSHP written).  Accepted and not
+ * read, as on the reference's live path: GSM_AREA, GSM_VOL, GNSNI_FAC,
+ * GGHOST, G_H_STRESS, G_S_STRESS, GMAXN, GINVK (CONSTRUCT_FINT),
+ * MODEL_BODY_ID, G_X/Y/Z_MOM (the NSNI weights come from GSM_LEN);
+ * CONSTRUCT_FINT leaves DLT_FINT and GCHAR_DIST untouched (their block is
+ * commented out, FINT.F90:1250-1330), CONSTRUCT_FINT_PD sets them when
+ * AUTO_TS. */
+int mega_fint_control(const mega_params* p);
+int construct_fint_gpu(const double* gwin, const double* gvol, const int32_t* gnump, const double* gcoo,
+                       const double* gcoo_cuurent, const double* gsm_len, const double* gsm_area,
+                       const double* gsm_vol, const double* gnsni_fac, const int32_t* gghost, const double* gprop,
+                       double* gstate, double* gstress, double* gstrain, double* g_h_stress, double* g_s_stress,
+                       const double* gdinc, const double* gdinc_tot, const int32_t* gmat_type,
+                       const int32_t* gebc_nodes, const int32_t* gn, const int32_t* gstart,
+                       const int32_t* dim_nn_list, const int32_t* gstack, double* gstack_shp, double* gstack_dshp,
+                       double* gstack_ddshp, const int32_t* gmaxn, double* ginvk, const int32_t* linit, double* fint,
+                       double* fext, double* dlt_fint, double* gchar_dist, double* gmax_wvel,
+                       double* local_dx_stress, double* local_dy_stress, double* local_dz_stress,
+                       const double* g_x_mom, const double* g_y_mom, const double* g_z_mom,
+                       const double* model_bodyforce, double* gint_work, const int32_t* model_body_id,
+                       double* gstrain_eq, const double* dlt);
+int construct_fint_pd_gpu(const double* gwin, const double* gvol, const int32_t* gnump, const double* gcoo,
+                          const double* gcoo_cuurent, const double* gsm_len, const double* gsm_area,
+                          const double* gsm_vol, const double* gnsni_fac, const int32_t* gghost, const double* gprop,
+                          double* gstate, double* gstress, double* gstrain, double* g_h_stress, double* g_s_stress,
+                          const double* gdinc, const double* gdinc_tot, const int32_t* gmat_type,
+                          const int32_t* gebc_nodes, const int32_t* gn, const int32_t* gstart,
+                          const int32_t* dim_nn_list, const int32_t* gstack, double* gstack_shp,
+                          double* gstack_dshp, double* gstack_ddshp, const int32_t* gmaxn, double* ginvk,
+                          const int32_t* linit, double* fint, double* dlt_fint, double* gchar_dist,
+                          double* gmax_wvel, double* local_dx_stress, double* local_dy_stress,
+                          double* local_dz_stress, const double* g_x_mom, const double* g_y_mom,
+                          const double* g_z_mom, const double* model_bodyforce, double* gint_work,
+                          const double* dlt);
 
 /* CONSTRUCT_FINT_PD (FINT_PD.F90:16-759), correspondence peridynamics,
  * Lagrangian path.  At linit != 0 the influence functions and K^-1 are built
@@ -433,8 +485,10 @@ int mega_pmb_init(int32_t n, const double* coo, const double* vol, const double*
 /* nsteps of velocity-Verlet (float force, double positions); *ms device time
  * of the call when ms is not NULL. */
 int mega_pmb_step(int64_t h, int32_t nsteps, double dt, float* ms);
-/* what: 0 displacement (3,n), 1 velocity, 2 acceleration, 3 broken flags (nnz);
- * *nbroken = bond copies broken so far (each bond breaks at both ends). */
+/* what: 0 displacement (3,n), 1 velocity, 2 acceleration, 3 broken flags (nnz),
+ * 4 local damage (n): the fraction of each particle's bonds (self excluded)
+ * that are broken; *nbroken = bond copies broken so far (each bond breaks at
+ * both ends). */
 int mega_pmb_download(int64_t h, int32_t what, double* dst, int64_t* nbroken);
 /* Pre-crack on the device: break every bond whose reference segment crosses
  * the rectangle corner + s edge_a + t edge_b (0 <= s, t <= 1), each a

@@ -104,6 +104,7 @@ class Params(C.Structure):
         ("inv3_exact", C.c_int32), ("newton_max_iter", C.c_int32), ("rate_solver", C.c_int32),
         ("ql_coef", C.c_double), ("ql_len", C.c_double), ("gravity", C.c_double * 3),
         ("dist_max", C.c_double * 3), ("newton_rtol", C.c_double),
+        ("auto_ts", C.c_int32), ("reserved", C.c_int32), ("dlt_fac", C.c_double),
     ]
 
 

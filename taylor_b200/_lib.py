@@ -46,6 +46,7 @@ class MegaParams(C.Structure):
         ("inv3_exact", C.c_int32), ("newton_max_iter", C.c_int32), ("rate_solver", C.c_int32),
         ("ql_coef", C.c_double), ("ql_len", C.c_double), ("gravity", C.c_double * 3),
         ("dist_max", C.c_double * 3), ("newton_rtol", C.c_double),
+        ("auto_ts", C.c_int32), ("reserved", C.c_int32), ("dlt_fac", C.c_double),
     ]
 
 
@@ -83,6 +84,9 @@ SIGNATURES = {
     "mega_set_fixity2": (I32, [I64, I32, P, P]),
     "mega_release_cached_memory": (I32, []),
     "mega_set_variants": (I32, [I64, I32, I32, I32]),
+    "mega_fint_control": (I32, [PP]),
+    "construct_fint_gpu": (I32, [P] * 46),
+    "construct_fint_pd_gpu": (I32, [P] * 43),
     "mega_autotune": (I32, [I64, D, I32, I32, P, P]),
     "mega_step_resident": (I32, [I64, I32, D, I32]),
     "mega_step_timed": (I32, [I64, I32, D, I32, C.POINTER(F32)]),

@@ -216,7 +216,8 @@ def pd_plate(h=0.25e-3, nx=400, ny=400, nz=16, horizon=3.015, E=72e9, rho=2440.0
     micromodulus c = 18 K / (pi delta^4) with K = E / (3 (1 - 2 nu)), nu =
     1/4 (bond-based restriction).  A pre-notch of length `notch` at mid-edge
     (plane y = mid, x < notch) starts with the bonds that cross it broken;
-    the two halves of the edge x = 0 move apart at +-v_edge in y."""
+    the two halves of the edge x = 0 (three particle columns, `fixed`) are
+    driven apart at a sustained +-v_edge in y."""
     xs = (np.arange(nx) + 0.5) * h
     ys = (np.arange(ny) + 0.5) * h
     zs = (np.arange(nz) + 0.5) * h
@@ -237,7 +238,19 @@ def pd_plate(h=0.25e-3, nx=400, ny=400, nz=16, horizon=3.015, E=72e9, rho=2440.0
     vel[edge & (coo[:, 1] < ymid), 1] = -v_edge
     return dict(name=f"pmb_plate_{nx}x{ny}x{nz}", n=n, coo=coo, win=np.full((n, 3), delta), vol=vol, rho=rho,
                 c=c, s_c=s_c, delta=delta, h=h, notch=notch, ymid=ymid, vinit=vel, sm_len=np.zeros((n, 6)),
-                dist_max=np.zeros(3))
+                dist_max=np.zeros(3), fixed=edge.astype(np.int32))
+
+
+def crack_tip(case, damage, threshold=0.35):
+    """Crack tip of a plate from the local damage of its particles: the
+    largest x among particles within two horizons of the notch plane whose
+    damage exceeds `threshold` (None when none does)."""
+    coo = case["coo"]
+    near = np.abs(coo[:, 1] - case["ymid"]) < 2.0 * case["delta"]
+    hit = near & (np.asarray(damage) > threshold)
+    if not np.any(hit):
+        return None
+    return float(coo[hit, 0].max())
 
 
 def notch_broken(case, gn, gstart, gstack):

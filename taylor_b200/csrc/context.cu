@@ -1132,6 +1132,8 @@ void mega_params_default(mega_params* p) {
   p->ql_coef = 0.001;
   p->ql_len = 0.0;
   p->newton_rtol = 1e-10;
+  p->auto_ts = 0;
+  p->dlt_fac = 1.0;
 }
 
 const char* mega_status_string(int32_t st) {
@@ -2390,20 +2392,34 @@ int mega_constitution(const mega_params* p, int32_t n, const double* stress_pred
   return (int)hst;
 }
 
-int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, const double* gwin, const double* gvol,
-                        const double* gprop, const int32_t* gmat_type, const int32_t* gebc_nodes,
-                        const double* bodyforce, double* gstate, double* gstress, double* gstrain,
-                        const double* gdinc, const double* gdinc_tot, const int32_t* gn, const int32_t* gstart,
-                        const int32_t* gstack, int64_t nnz, double* gstack_shp, double* gstack_dshp,
-                        int32_t linit, double dlt, double* fint, double* fext, double* gmax_wvel,
-                        double* gstrain_eq, double* gint_work) {
-  if (!p || n <= 0 || !gcoo || !gwin || !gvol || !gprop || !gmat_type || !gstate || !gstress || !gstrain ||
-      !gdinc || !gdinc_tot || !gn || !gstart || !gstack || !gstack_shp || !gstack_dshp || !fint || !fext ||
-      !gmax_wvel || !gstrain_eq || !gint_work)
+// The inputs and outputs of one CONSTRUCT_FINT call (FINT.F90:16-25); the
+// pointers after `gint_work` may be null unless the path needs them.
+struct FintIO {
+  int32_t n;
+  const double *gcoo, *gwin, *gvol, *gprop, *bodyforce;
+  const int32_t *gmat_type, *gebc_nodes, *gn, *gstart, *gstack;
+  int64_t nnz;
+  double *gstate, *gstress, *gstrain;
+  const double *gdinc, *gdinc_tot;
+  double *gstack_shp, *gstack_dshp;
+  int32_t linit;
+  double dlt;
+  double *fint, *fext, *gmax_wvel, *gstrain_eq, *gint_work;
+  const double* gcoo_current;   // semi-Lagrangian: shapes on the current coordinates
+  const double* gsm_len;        // NSNI: smoothing cells (6, n)
+  double* gstack_ddshp;         // NSNI: smoothed second derivatives (6, nnz)
+  double *dx_stress, *dy_stress, *dz_stress;  // NSNI: LOCAL_DX/DY/DZ_STRESS (6, n) in/out
+};
+
+static int construct_fint_impl(const mega_params* p, const FintIO& io) {
+  const int32_t n = io.n;
+  const bool semi = p->lagrangian == 0, nsni = p->itype_int == 2;
+  if (p->itype_int != 0 && p->itype_int != 2) return MEGA_ERR_UNSUPPORTED;
+  if (semi && nsni) return MEGA_ERR_UNSUPPORTED;  // the semi-Lagrangian path is DNI (as the resident one)
+  if (semi && !io.gcoo_current) return MEGA_ERR_ARG;
+  if (nsni && (!io.gsm_len || !io.gstack_ddshp || !io.dx_stress || !io.dy_stress || !io.dz_stress))
     return MEGA_ERR_ARG;
-  // NSNI keeps second derivatives and stress gradients this argument list
-  // has no room for: resident contexts only
-  if (p->lagrangian != 1 || p->itype_int == 2) return MEGA_ERR_UNSUPPORTED;
+  const bool shapes_here = io.linit || semi;  // RK1 in this call (FINT.F90:387-436)
   StreamGuard sg;
   int r = make_stream(&sg.s);
   if (r) return r;
@@ -2411,13 +2427,13 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   DevPool pool;
   DevCSR csr;
   std::vector<int64_t> hpos;
-  r = csr_from_host(s, n, gn, gstart, gstack, nnz, pool, csr, hpos);
+  r = csr_from_host(s, n, io.gn, io.gstart, io.gstack, io.nnz, pool, csr, hpos);
   if (r) return r;
   r = build_transpose(s, csr, pool);
   if (r) return r;
   const int64_t n3 = 3 * (int64_t)n, m = csr.nnz;
   double *dc, *dw, *dv, *dsh, *dgx, *dgy, *dgz, *tgx, *tgy, *tgz, *tsh = nullptr, *sd, *ddsp, *dtot, *dsig, *deps6,
-         *dep, *deq, *dwv, *dfg, *dT, *dfi, *dfe, *dbf = nullptr;
+         *dep, *deq, *dwv, *dfg, *dT, *dfi, *dfe, *dbf = nullptr, *dcur = nullptr, *dsml = nullptr;
   int32_t* den = nullptr;
   uint16_t* midx;
   StepAccum* acc;
@@ -2431,54 +2447,102 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   MEGA_ALLOC(pool, dT, 12 * (int64_t)n); MEGA_ALLOC(pool, dfi, n3); MEGA_ALLOC(pool, dfe, n3);
   MEGA_ALLOC(pool, midx, n); MEGA_ALLOC(pool, acc, 1); MEGA_ALLOC(pool, st, 1);
   bool has_body = p->gravity[0] != 0.0 || p->gravity[1] != 0.0 || p->gravity[2] != 0.0;
-  if (bodyforce)
-    for (int64_t k = 0; k < n3 && !has_body; ++k) has_body = bodyforce[k] != 0.0;
+  if (io.bodyforce)
+    for (int64_t k = 0; k < n3 && !has_body; ++k) has_body = io.bodyforce[k] != 0.0;
   if (has_body) {
     MEGA_ALLOC(pool, tsh, m);
-    if (bodyforce) { MEGA_ALLOC(pool, dbf, n3); if ((r = upload(s, dbf, bodyforce, n3))) return r; }
+    if (io.bodyforce) { MEGA_ALLOC(pool, dbf, n3); if ((r = upload(s, dbf, io.bodyforce, n3))) return r; }
   }
-  if (gebc_nodes) { MEGA_ALLOC(pool, den, n); if ((r = upload(s, den, gebc_nodes, (size_t)n))) return r; }
+  if (io.gebc_nodes) { MEGA_ALLOC(pool, den, n); if ((r = upload(s, den, io.gebc_nodes, (size_t)n))) return r; }
+  if (semi) { MEGA_ALLOC(pool, dcur, n3); if ((r = upload(s, dcur, io.gcoo_current, n3))) return r; }
+  if (nsni) { MEGA_ALLOC(pool, dsml, 6 * (int64_t)n); if ((r = upload(s, dsml, io.gsm_len, 6 * (size_t)n))) return r; }
   // material table (per call)
   std::vector<uint16_t> hidx;
   std::vector<MatEntry> ents;
   bool damaged = false;
-  if ((r = material_table(n, gprop, gmat_type, 65535, ents, hidx, damaged))) return r;
+  if ((r = material_table(n, io.gprop, io.gmat_type, 65535, ents, hidx, damaged))) return r;
   MatEntry* dmat;
   MEGA_ALLOC(pool, dmat, ents.size());
-  std::vector<double> hs(n), hsig(6 * (size_t)n), heps(6 * (size_t)n), hax;
-  for (int32_t i = 0; i < n; ++i) hs[i] = gstate[20 * (size_t)i + 2];
+  std::vector<double> hs(n), hax;
+  for (int32_t i = 0; i < n; ++i) hs[i] = io.gstate[20 * (size_t)i + 2];
   double* dax = nullptr;  // GSTATE(1, 2, 4, 5) when a damaged model is present
   if (damaged) {
     MEGA_ALLOC(pool, dax, 4 * (int64_t)n);
     hax.resize(4 * (size_t)n);
     for (int32_t i = 0; i < n; ++i) {
-      const double* g = gstate + 20 * (size_t)i;
+      const double* g = io.gstate + 20 * (size_t)i;
       hax[4 * (size_t)i] = g[0]; hax[4 * (size_t)i + 1] = g[1]; hax[4 * (size_t)i + 2] = g[3];
       hax[4 * (size_t)i + 3] = g[4];
     }
     if ((r = upload(s, dax, hax.data(), hax.size()))) return r;
   }
-  if ((r = upload(s, dc, gcoo, n3)) || (r = upload(s, dw, gwin, n3)) || (r = upload(s, dv, gvol, (size_t)n)) ||
-      (r = upload(s, ddsp, gdinc, n3)) || (r = upload(s, dtot, gdinc_tot, n3)) ||
-      (r = upload(s, dsig, gstress, 6 * (size_t)n)) || (r = upload(s, deps6, gstrain, 6 * (size_t)n)) ||
-      (r = upload(s, dep, hs.data(), (size_t)n)) || (r = upload(s, midx, hidx.data(), (size_t)n)) ||
-      (r = upload(s, dmat, ents.data(), ents.size())))
+  if ((r = upload(s, dc, io.gcoo, n3)) || (r = upload(s, dw, io.gwin, n3)) || (r = upload(s, dv, io.gvol, (size_t)n)) ||
+      (r = upload(s, ddsp, io.gdinc, n3)) || (r = upload(s, dsig, io.gstress, 6 * (size_t)n)) ||
+      (r = upload(s, deps6, io.gstrain, 6 * (size_t)n)) || (r = upload(s, dep, hs.data(), (size_t)n)) ||
+      (r = upload(s, midx, hidx.data(), (size_t)n)) || (r = upload(s, dmat, ents.data(), ents.size())))
     return r;
+  // the total displacement pushes the gradients forward; on the
+  // semi-Lagrangian path they are current already (F = I, FINT.F90:410-436)
+  if (semi) MEGA_TRY(cudaMemsetAsync(dtot, 0, sizeof(double) * n3, s));
+  else if ((r = upload(s, dtot, io.gdinc_tot, n3))) return r;
   MEGA_TRY(cudaMemsetAsync(acc, 0, sizeof(StepAccum), s));
   MEGA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
-  if (linit) {
-    r = rk_shapes(s, *p, n, dc, dw, den, csr, dsh, dgx, dgy, dgz, st);
+  if (shapes_here) {
+    r = rk_shapes(s, *p, n, semi ? dcur : dc, dw, den, csr, dsh, dgx, dgy, dgz, st);
     if (r) return r;
   } else {
     std::vector<double> a(m), b(m), d(m), e(m);
     for (int64_t k = 0; k < m; ++k) {
       const int64_t q = hpos[k];
-      a[k] = gstack_shp[q];
-      b[k] = gstack_dshp[3 * q]; d[k] = gstack_dshp[3 * q + 1]; e[k] = gstack_dshp[3 * q + 2];
+      a[k] = io.gstack_shp[q];
+      b[k] = io.gstack_dshp[3 * q]; d[k] = io.gstack_dshp[3 * q + 1]; e[k] = io.gstack_dshp[3 * q + 2];
     }
     if ((r = upload(s, dsh, a.data(), m)) || (r = upload(s, dgx, b.data(), m)) || (r = upload(s, dgy, d.data(), m)) ||
         (r = upload(s, dgz, e.data(), m)))
       return r;
+    MEGA_TRY(cudaStreamSynchronize(s));
+  }
+  // NSNI: second derivatives (computed at LINIT, read otherwise) in CSR and
+  // CSC order, stress gradients, per-call scratch
+  NsniS nsr{}, nsc{};
+  NsniSF none{};
+  double *sgrad = nullptr, *hq = nullptr, *nsw = nullptr, *fstab = nullptr, *sprev = nullptr;
+  if (nsni) {
+    for (int k = 0; k < 6; ++k) { MEGA_ALLOC(pool, nsr.v[k], m); MEGA_ALLOC(pool, nsc.v[k], m); }
+    MEGA_ALLOC(pool, sgrad, 18 * (int64_t)n); MEGA_ALLOC(pool, hq, 18 * (int64_t)n);
+    MEGA_ALLOC(pool, nsw, 18 * (int64_t)n); MEGA_ALLOC(pool, fstab, n3); MEGA_ALLOC(pool, sprev, 6 * (int64_t)n);
+    if (io.linit) {
+      DevPool faces(s);
+      double* g[6];
+      for (int k = 0; k < 6; ++k) MEGA_ALLOC(faces, g[k], m);
+      for (int ax = 0; ax < 3; ++ax) {
+        if ((r = rk_grad_at_face(s, *p, n, dc, dw, den, csr, dsml, 2 * ax, g[0], g[1], g[2], st)) ||
+            (r = rk_grad_at_face(s, *p, n, dc, dw, den, csr, dsml, 2 * ax + 1, g[3], g[4], g[5], st)))
+          return r;
+        const double* gp[3] = {g[0], g[1], g[2]};
+        const double* gm[3] = {g[3], g[4], g[5]};
+        if ((r = nsni_combine(s, n, ax, csr.rowptr, dsml, gp, gm, nsr))) return r;
+      }
+      MEGA_TRY(cudaStreamSynchronize(s));
+    } else {
+      std::vector<double> v(m);
+      for (int k = 0; k < 6; ++k) {
+        for (int64_t e = 0; e < m; ++e) v[e] = io.gstack_ddshp[6 * hpos[e] + k];
+        if ((r = upload(s, nsr.v[k], v.data(), m))) return r;
+        MEGA_TRY(cudaStreamSynchronize(s));
+      }
+    }
+    for (int k = 0; k < 6; ++k) k_gather_pos<<<grid_for(m, 256), 256, 0, s>>>(m, csr.tpos, nsr.v[k], nsc.v[k]);
+    MEGA_CHECK_LAUNCH();
+    std::vector<double> hg(18 * (size_t)n);
+    for (int32_t i = 0; i < n; ++i)
+      for (int k = 0; k < 6; ++k) {
+        hg[18 * (size_t)i + k] = io.dx_stress[6 * (size_t)i + k];
+        hg[18 * (size_t)i + 6 + k] = io.dy_stress[6 * (size_t)i + k];
+        hg[18 * (size_t)i + 12 + k] = io.dz_stress[6 * (size_t)i + k];
+      }
+    if ((r = upload(s, sgrad, hg.data(), hg.size()))) return r;
+    MEGA_TRY(cudaMemcpyAsync(sprev, dsig, sizeof(double) * 6 * n, cudaMemcpyDeviceToDevice, s));
     MEGA_TRY(cudaStreamSynchronize(s));
   }
   const unsigned g = grid_for(m, 256);
@@ -2495,9 +2559,18 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   a.strain_eq = deq; a.wvel = dwv; a.tmat = dT; a.bodyforce = dbf; a.aux = dax;
   a.grav[0] = p->gravity[0]; a.grav[1] = p->gravity[1]; a.grav[2] = p->gravity[2];
   a.has_body = has_body; a.inv3_exact = p->inv3_exact; a.finite_strain = p->finite_strain;
-  a.maxit = p->newton_max_iter; a.rate_solver = p->rate_solver; a.rtol = p->newton_rtol; a.dt = dlt; a.acc = acc; a.status = st;
+  a.maxit = p->newton_max_iter; a.rate_solver = p->rate_solver; a.rtol = p->newton_rtol; a.dt = io.dlt; a.acc = acc;
+  a.status = st;
+  NsniStepArgs na{};
+  if (nsni) {
+    na.n = n; na.fg = dfg; na.stress_old = sprev; na.stress_new = dsig; na.sml = dsml; na.vol = dv; na.matidx = midx;
+    na.mats = dmat; na.hq = hq; na.sgrad = sgrad; na.w = nsw; na.fstab = fstab; na.finite_strain = p->finite_strain;
+    na.inv3_exact = p->inv3_exact; na.acc = acc; na.status = st;
+    if ((r = nsni_step(s, na, csr, nsr, nsc, none, none, false, ddsp, 0))) return r;
+  }
   r = launch_stress(s, false, a);
   if (r) return r;
+  if (nsni && (r = nsni_step(s, na, csr, nsr, nsc, none, none, false, ddsp, 1))) return r;
   DevCSR* dcsr;
   MEGA_ALLOC(pool, dcsr, 1);
   if ((r = upload(s, dcsr, &csr, 1))) return r;
@@ -2506,19 +2579,23 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
   f.integrate = 0; f.predict = 0; f.fint = dfi; f.fext = dfe; f.acc = acc; f.status = st;
   r = launch_force(s, false, f);
   if (r) return r;
+  if (nsni) {  // the stabilisation force joins the internal force (FINT.F90:1127-1208)
+    k_add_kernel<<<grid_for(n3, 256), 256, 0, s>>>(n3, dfi, fstab, dfi);
+    MEGA_CHECK_LAUNCH();
+  }
   StepAccum hacc;
   unsigned hst = 0;
-  MEGA_TRY(cudaMemcpyAsync(fint, dfi, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
-  MEGA_TRY(cudaMemcpyAsync(fext, dfe, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
-  MEGA_TRY(cudaMemcpyAsync(gstress, dsig, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
-  MEGA_TRY(cudaMemcpyAsync(gstrain, deps6, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(io.fint, dfi, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(io.fext, dfe, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(io.gstress, dsig, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(io.gstrain, deps6, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(hs.data(), dep, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   if (damaged) MEGA_TRY(cudaMemcpyAsync(hax.data(), dax, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
-  MEGA_TRY(cudaMemcpyAsync(gmax_wvel, dwv, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-  MEGA_TRY(cudaMemcpyAsync(gstrain_eq, deq, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(io.gmax_wvel, dwv, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  MEGA_TRY(cudaMemcpyAsync(io.gstrain_eq, deq, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(&hacc, acc, sizeof(hacc), cudaMemcpyDeviceToHost, s));
   MEGA_TRY(cudaMemcpyAsync(&hst, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-  if (linit) {
+  if (shapes_here) {  // GSTACK_SHP / GSTACK_DSHP written where RK1 ran (FINT.F90:427-434, 580-587)
     std::vector<double> a2(m), b(m), d(m), e(m);
     MEGA_TRY(cudaMemcpyAsync(a2.data(), dsh, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
     MEGA_TRY(cudaMemcpyAsync(b.data(), dgx, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
@@ -2527,20 +2604,125 @@ int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, con
     MEGA_TRY(cudaStreamSynchronize(s));
     for (int64_t k = 0; k < m; ++k) {
       const int64_t q = hpos[k];
-      gstack_shp[q] = a2[k];
-      gstack_dshp[3 * q] = b[k]; gstack_dshp[3 * q + 1] = d[k]; gstack_dshp[3 * q + 2] = e[k];
+      io.gstack_shp[q] = a2[k];
+      io.gstack_dshp[3 * q] = b[k]; io.gstack_dshp[3 * q + 1] = d[k]; io.gstack_dshp[3 * q + 2] = e[k];
     }
   }
+  if (nsni) {
+    std::vector<double> hg(18 * (size_t)n);
+    MEGA_TRY(cudaMemcpyAsync(hg.data(), sgrad, sizeof(double) * hg.size(), cudaMemcpyDeviceToHost, s));
+    std::vector<std::vector<double>> dd;
+    if (io.linit) {
+      dd.assign(6, std::vector<double>(m));
+      for (int k = 0; k < 6; ++k)
+        MEGA_TRY(cudaMemcpyAsync(dd[k].data(), nsr.v[k], sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    }
+    MEGA_TRY(cudaStreamSynchronize(s));
+    for (int32_t i = 0; i < n; ++i)
+      for (int k = 0; k < 6; ++k) {
+        io.dx_stress[6 * (size_t)i + k] = hg[18 * (size_t)i + k];
+        io.dy_stress[6 * (size_t)i + k] = hg[18 * (size_t)i + 6 + k];
+        io.dz_stress[6 * (size_t)i + k] = hg[18 * (size_t)i + 12 + k];
+      }
+    if (io.linit)
+      for (int64_t e = 0; e < m; ++e)
+        for (int k = 0; k < 6; ++k) io.gstack_ddshp[6 * hpos[e] + k] = dd[k][e];
+  }
   MEGA_TRY(cudaStreamSynchronize(s));
-  for (int32_t i = 0; i < n; ++i) gstate[20 * (size_t)i + 2] = hs[i];
+  for (int32_t i = 0; i < n; ++i) io.gstate[20 * (size_t)i + 2] = hs[i];
   if (damaged)
     for (int32_t i = 0; i < n; ++i) {
-      double* g = gstate + 20 * (size_t)i;
-      g[0] = hax[4 * (size_t)i]; g[1] = hax[4 * (size_t)i + 1]; g[3] = hax[4 * (size_t)i + 2];
-      g[4] = hax[4 * (size_t)i + 3];
+      double* gs = io.gstate + 20 * (size_t)i;
+      gs[0] = hax[4 * (size_t)i]; gs[1] = hax[4 * (size_t)i + 1]; gs[3] = hax[4 * (size_t)i + 2];
+      gs[4] = hax[4 * (size_t)i + 3];
     }
-  *gint_work += slot_sum(hacc.int_work);
+  *io.gint_work += slot_sum(hacc.int_work);
   return (int)hst;
+}
+
+int mega_construct_fint(const mega_params* p, int32_t n, const double* gcoo, const double* gwin, const double* gvol,
+                        const double* gprop, const int32_t* gmat_type, const int32_t* gebc_nodes,
+                        const double* bodyforce, double* gstate, double* gstress, double* gstrain,
+                        const double* gdinc, const double* gdinc_tot, const int32_t* gn, const int32_t* gstart,
+                        const int32_t* gstack, int64_t nnz, double* gstack_shp, double* gstack_dshp,
+                        int32_t linit, double dlt, double* fint, double* fext, double* gmax_wvel,
+                        double* gstrain_eq, double* gint_work) {
+  if (!p || n <= 0 || !gcoo || !gwin || !gvol || !gprop || !gmat_type || !gstate || !gstress || !gstrain ||
+      !gdinc || !gdinc_tot || !gn || !gstart || !gstack || !gstack_shp || !gstack_dshp || !fint || !fext ||
+      !gmax_wvel || !gstrain_eq || !gint_work)
+    return MEGA_ERR_ARG;
+  // this short list has no room for the NSNI arrays or the current
+  // coordinates: construct_fint_gpu takes the full list
+  if (p->lagrangian != 1 || p->itype_int == 2) return MEGA_ERR_UNSUPPORTED;
+  FintIO io{};
+  io.n = n; io.gcoo = gcoo; io.gwin = gwin; io.gvol = gvol; io.gprop = gprop; io.bodyforce = bodyforce;
+  io.gmat_type = gmat_type; io.gebc_nodes = gebc_nodes; io.gn = gn; io.gstart = gstart; io.gstack = gstack;
+  io.nnz = nnz; io.gstate = gstate; io.gstress = gstress; io.gstrain = gstrain; io.gdinc = gdinc;
+  io.gdinc_tot = gdinc_tot; io.gstack_shp = gstack_shp; io.gstack_dshp = gstack_dshp; io.linit = linit; io.dlt = dlt;
+  io.fint = fint; io.fext = fext; io.gmax_wvel = gmax_wvel; io.gstrain_eq = gstrain_eq; io.gint_work = gint_work;
+  return construct_fint_impl(p, io);
+}
+
+static std::mutex g_control_mu;
+static mega_params g_control{};
+static bool g_control_set = false;
+
+int mega_fint_control(const mega_params* p) {
+  if (!p) return MEGA_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_control_mu);
+  g_control = *p;
+  g_control_set = true;
+  return 0;
+}
+
+}  // extern "C"
+
+namespace mega {
+int fint_control_get(mega_params* out) {
+  std::lock_guard<std::mutex> lk(g_control_mu);
+  if (!g_control_set) return MEGA_ERR_STATE;
+  *out = g_control;
+  return 0;
+}
+}  // namespace mega
+
+extern "C" {
+
+int construct_fint_gpu(const double* gwin, const double* gvol, const int32_t* gnump, const double* gcoo,
+                       const double* gcoo_cuurent, const double* gsm_len, const double* gsm_area,
+                       const double* gsm_vol, const double* gnsni_fac, const int32_t* gghost, const double* gprop,
+                       double* gstate, double* gstress, double* gstrain, double* g_h_stress, double* g_s_stress,
+                       const double* gdinc, const double* gdinc_tot, const int32_t* gmat_type,
+                       const int32_t* gebc_nodes, const int32_t* gn, const int32_t* gstart,
+                       const int32_t* dim_nn_list, const int32_t* gstack, double* gstack_shp, double* gstack_dshp,
+                       double* gstack_ddshp, const int32_t* gmaxn, double* ginvk, const int32_t* linit, double* fint,
+                       double* fext, double* dlt_fint, double* gchar_dist, double* gmax_wvel,
+                       double* local_dx_stress, double* local_dy_stress, double* local_dz_stress,
+                       const double* g_x_mom, const double* g_y_mom, const double* g_z_mom,
+                       const double* model_bodyforce, double* gint_work, const int32_t* model_body_id,
+                       double* gstrain_eq, const double* dlt) {
+  (void)gsm_area; (void)gsm_vol; (void)gnsni_fac; (void)gghost; (void)g_h_stress; (void)g_s_stress;
+  (void)gmaxn; (void)ginvk; (void)dlt_fint; (void)gchar_dist; (void)g_x_mom; (void)g_y_mom; (void)g_z_mom;
+  (void)model_body_id;
+  mega_params p;
+  {
+    std::lock_guard<std::mutex> lk(g_control_mu);
+    if (!g_control_set) return MEGA_ERR_STATE;  // mega_fint_control first
+    p = g_control;
+  }
+  if (!gnump || !dim_nn_list || !linit || !dlt || *gnump <= 0 || !gcoo || !gwin || !gvol || !gprop || !gmat_type ||
+      !gstate || !gstress || !gstrain || !gdinc || !gdinc_tot || !gn || !gstart || !gstack || !gstack_shp ||
+      !gstack_dshp || !fint || !fext || !gmax_wvel || !gstrain_eq || !gint_work)
+    return MEGA_ERR_ARG;
+  FintIO io{};
+  io.n = *gnump; io.gcoo = gcoo; io.gwin = gwin; io.gvol = gvol; io.gprop = gprop; io.bodyforce = model_bodyforce;
+  io.gmat_type = gmat_type; io.gebc_nodes = gebc_nodes; io.gn = gn; io.gstart = gstart; io.gstack = gstack;
+  io.nnz = *dim_nn_list; io.gstate = gstate; io.gstress = gstress; io.gstrain = gstrain; io.gdinc = gdinc;
+  io.gdinc_tot = gdinc_tot; io.gstack_shp = gstack_shp; io.gstack_dshp = gstack_dshp; io.linit = *linit;
+  io.dlt = *dlt; io.fint = fint; io.fext = fext; io.gmax_wvel = gmax_wvel; io.gstrain_eq = gstrain_eq;
+  io.gint_work = gint_work; io.gcoo_current = gcoo_cuurent; io.gsm_len = gsm_len; io.gstack_ddshp = gstack_ddshp;
+  io.dx_stress = local_dx_stress; io.dy_stress = local_dy_stress; io.dz_stress = local_dz_stress;
+  return construct_fint_impl(&p, io);
 }
 
 }  // extern "C"

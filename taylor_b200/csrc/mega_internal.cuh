@@ -16,6 +16,9 @@ constexpr int kMaxBinCount = 1000;     // MAX_NEIGH, HANDELER.F90:245
 constexpr int kMaxCandidates = 10000;  // INODE(10000), BIN_SEARCH.F90:80
 
 void record_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+// the CONTROL values construct_fint_gpu / construct_fint_pd_gpu read (set
+// once by mega_fint_control); MEGA_ERR_STATE before that call
+int fint_control_get(mega_params* out);
 const char* last_error_text();
 void record_error_text(const char* msg);
 

@@ -518,6 +518,26 @@ __global__ void k_pmb_flags(int32_t n, const int32_t* __restrict__ perm, const i
   }
 }
 
+// Local damage of each particle (Silling & Askari 2005): the fraction of its
+// bonds that are broken (the self entry excluded), written in the caller's
+// particle order.
+__global__ void k_pmb_damage(int32_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ rowptr0,
+                             const int64_t* __restrict__ rowptr1, const uint32_t* __restrict__ bits,
+                             double* __restrict__ out) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const int64_t len = rowptr0[perm[r] + 1] - rowptr0[perm[r]], b0 = rowptr1[r];
+  int nb = 0;
+  for (int64_t k = lane; k < len; k += 32) {
+    const int64_t p = b0 + k;
+    nb += (bits[p >> 5] >> (p & 31)) & 1u;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nb += __shfl_xor_sync(0xffffffffu, nb, o);
+  if (lane == 0) out[perm[r]] = len > 1 ? (double)nb / (double)(len - 1) : 0.0;
+}
+
 // Pre-crack: break every bond whose reference segment X_i -> X_j crosses the
 // rectangle {p0 + s a + t b : 0 <= s, t <= 1} (strictly between its ends).
 __global__ void k_pmb_cut(int32_t n, const double* __restrict__ X, const int64_t* __restrict__ rowptr,
@@ -772,6 +792,54 @@ int mega_construct_fint_pd(const mega_params* p, int32_t n, const double* gcoo, 
   return (int)hst;
 }
 
+int construct_fint_pd_gpu(const double* gwin, const double* gvol, const int32_t* gnump, const double* gcoo,
+                          const double* gcoo_cuurent, const double* gsm_len, const double* gsm_area,
+                          const double* gsm_vol, const double* gnsni_fac, const int32_t* gghost, const double* gprop,
+                          double* gstate, double* gstress, double* gstrain, double* g_h_stress, double* g_s_stress,
+                          const double* gdinc, const double* gdinc_tot, const int32_t* gmat_type,
+                          const int32_t* gebc_nodes, const int32_t* gn, const int32_t* gstart,
+                          const int32_t* dim_nn_list, const int32_t* gstack, double* gstack_shp,
+                          double* gstack_dshp, double* gstack_ddshp, const int32_t* gmaxn, double* ginvk,
+                          const int32_t* linit, double* fint, double* dlt_fint, double* gchar_dist,
+                          double* gmax_wvel, double* local_dx_stress, double* local_dy_stress,
+                          double* local_dz_stress, const double* g_x_mom, const double* g_y_mom,
+                          const double* g_z_mom, const double* model_bodyforce, double* gint_work,
+                          const double* dlt) {
+  (void)gsm_len; (void)gsm_area; (void)gsm_vol; (void)gnsni_fac; (void)gghost; (void)g_h_stress; (void)g_s_stress;
+  (void)gdinc_tot; (void)gebc_nodes; (void)gstack_dshp; (void)gstack_ddshp; (void)gmaxn; (void)local_dx_stress;
+  (void)local_dy_stress; (void)local_dz_stress; (void)g_x_mom; (void)g_y_mom; (void)g_z_mom; (void)model_bodyforce;
+  mega_params p;
+  if (int r = fint_control_get(&p)) return r;
+  if (!gnump || !dim_nn_list || !linit || !dlt || *gnump <= 0 || !gcoo_cuurent) return MEGA_ERR_ARG;
+  const int32_t n = *gnump;
+  const int st = mega_construct_fint_pd(&p, n, gcoo, gcoo_cuurent, gwin, gvol, gprop, gmat_type, gstate, gstress,
+                                        gstrain, gdinc, gn, gstart, gstack, *dim_nn_list, gstack_shp, ginvk, *linit,
+                                        *dlt, fint, gmax_wvel, gint_work);
+  if (st < 0 || !p.auto_ts) return st;
+  // AUTO_TS (FINT_PD.F90:690-754): each node's nearest neighbour in the
+  // current configuration over its wave speed, the smallest, times DLT_FAC
+  if (!gchar_dist || !dlt_fint) return MEGA_ERR_ARG;
+  double dmin = 0.0;
+  for (int32_t i = 0; i < n; ++i) {
+    const double xi = gcoo_cuurent[3 * (size_t)i], yi = gcoo_cuurent[3 * (size_t)i + 1],
+                 zi = gcoo_cuurent[3 * (size_t)i + 2];
+    bool first = true;
+    for (int32_t k = 0; k < gn[i]; ++k) {
+      const int32_t jj = gstack[gstart[i] - 1 + k] - 1;
+      if (jj == i) continue;
+      const double dx = gcoo_cuurent[3 * (size_t)jj] - xi, dy = gcoo_cuurent[3 * (size_t)jj + 1] - yi,
+                   dz = gcoo_cuurent[3 * (size_t)jj + 2] - zi;
+      const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+      gchar_dist[i] = first ? d : std::min(gchar_dist[i], d);
+      first = false;
+    }
+    const double t = gchar_dist[i] / gmax_wvel[i];
+    dmin = (i == 0) ? t : std::min(t, dmin);
+  }
+  *dlt_fint = dmin * p.dlt_fac;
+  return st;
+}
+
 static std::mutex g_pmb_mu;
 static std::set<PmbCtx*> g_pmbs;
 static PmbCtx* get_pmb(int64_t h) {
@@ -985,6 +1053,14 @@ int mega_pmb_download(int64_t h, int32_t what, double* dst, int64_t* nbroken) {
     MEGA_TRY(cudaMemcpyAsync(hb.data(), d, (size_t)m, cudaMemcpyDeviceToHost, c->s));
     MEGA_TRY(cudaStreamSynchronize(c->s));
     for (int64_t p = 0; p < m; ++p) dst[p] = hb[p];
+  } else if (what == 4) {  // local damage per particle
+    double* d = nullptr;
+    MEGA_ALLOC(tp, d, c->n);
+    k_pmb_damage<<<(unsigned)(((int64_t)c->n * 32 + 255) / 256), 256, 0, c->s>>>(c->n, c->perm, c->rowptr0,
+                                                                               c->csr.rowptr, c->broken, d);
+    MEGA_CHECK_LAUNCH();
+    MEGA_TRY(cudaMemcpyAsync(dst, d, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->s));
+    MEGA_TRY(cudaStreamSynchronize(c->s));
   } else return MEGA_ERR_ARG;
   return 0;
 }

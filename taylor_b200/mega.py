@@ -126,6 +126,84 @@ def construct_fint(params, coo, win, vol, props, mat_type, ebc_nodes, state, str
                 gint_work=gw.value, shp=shp, dshp=dshp, status=st)
 
 
+def _ref(v, ct):
+    """A by-reference scalar, as gfortran passes every argument."""
+    return C.byref(ct(v))
+
+
+def construct_fint_full(params, coo, win, vol, props, mat_type, ebc_nodes, state, stress, strain, dinc, dinc_tot,
+                        gn, gstart, gstack, shp, dshp, linit, dlt, coo_current=None, sm_len=None, ddshp=None,
+                        sgrad=None, bodyforce=None, body_id=None, gint_work=0.0, allow_status=False):
+    """CONSTRUCT_FINT through construct_fint_gpu: the reference's own 46
+    arguments (FINT.F90:16-25) in order, all by reference.  ddshp (nnz, 6)
+    and sgrad (n, 18: the x, y and z stress gradients) for NSNI; returns the
+    outputs as construct_fint does, plus ddshp and sgrad."""
+    n = len(coo)
+    check(_lib.lib().mega_fint_control(C.byref(params)), "mega_fint_control")
+    state, stress, strain = _f64(state).copy(), _f64(stress).copy(), _f64(strain).copy()
+    shp, dshp = _f64(shp).copy(), _f64(dshp).copy()
+    nnz = len(gstack)
+    dd = np.zeros((nnz, 6)) if ddshp is None else _f64(ddshp).copy()
+    sg = np.zeros((n, 18)) if sgrad is None else _f64(sgrad).copy()
+    dx, dy, dz = (np.ascontiguousarray(sg[:, 6 * k:6 * k + 6]) for k in range(3))
+    cur = _f64(coo if coo_current is None else coo_current)
+    sml = _f64(np.zeros((n, 6)) if sm_len is None else sm_len)
+    fint, fext = np.zeros(3 * n), np.zeros(3 * n)
+    wv, seq, cdist = np.zeros(n), np.zeros(n), np.zeros(n)
+    h_s, s_s = np.zeros((n, 6)), np.zeros((n, 6))
+    z3n, zn = np.zeros((n, 3)), np.zeros(n)
+    ginvk = np.zeros((n, 3, 3))
+    gw = C.c_double(gint_work)
+    dlt_fint = C.c_double(-1.0)
+    en = _i32(np.zeros(n) if ebc_nodes is None else ebc_nodes)
+    bid = _i32(np.ones(n) if body_id is None else body_id)
+    bf = _f64(np.zeros((n, 3)) if bodyforce is None else bodyforce)
+    st = _lib.lib().construct_fint_gpu(
+        ptr(_f64(win)), ptr(_f64(vol)), _ref(n, C.c_int32), ptr(_f64(coo)), ptr(cur),
+        ptr(sml), ptr(z3n), ptr(zn), ptr(z3n),
+        ptr(_i32(np.zeros(n))), ptr(_f64(props)), ptr(state), ptr(stress),
+        ptr(strain), ptr(h_s), ptr(s_s), ptr(_f64(dinc)), ptr(_f64(dinc_tot)), ptr(_i32(mat_type)),
+        ptr(en),
+        ptr(_i32(gn)), ptr(_i32(gstart)), _ref(nnz, C.c_int32),
+        ptr(_i32(gstack)), ptr(shp), ptr(dshp), ptr(dd), _ref(int(np.max(gn)), C.c_int32), ptr(ginvk),
+        _ref(int(bool(linit)), C.c_int32),
+        ptr(fint), ptr(fext), C.byref(dlt_fint), ptr(cdist), ptr(wv),
+        ptr(dx), ptr(dy), ptr(dz),
+        ptr(zn), ptr(zn), ptr(zn), ptr(bf), C.byref(gw), ptr(bid), ptr(seq), _ref(float(dlt), C.c_double))
+    check(st, "construct_fint_gpu", allow_status)
+    return dict(fint=fint, fext=fext, stress=stress, strain=strain, state=state, gmax_wvel=wv, gstrain_eq=seq,
+                gint_work=gw.value, shp=shp, dshp=dshp, ddshp=dd, sgrad=np.concatenate([dx, dy, dz], axis=1),
+                dlt_fint=dlt_fint.value, status=st)
+
+
+def construct_fint_pd_full(params, coo, coo_current, win, vol, props, mat_type, state, stress, strain, dinc, gn,
+                           gstart, gstack, shp, ginvk, linit, dlt, allow_status=False):
+    """CONSTRUCT_FINT_PD through construct_fint_pd_gpu (FINT_PD.F90:16-25, 43
+    arguments by reference); ginvk (n,3,3) row-major here.  Returns fint,
+    stress, strain, state, gmax_wvel, shp, ginvk, gchar_dist and dlt_fint."""
+    n = len(coo)
+    check(_lib.lib().mega_fint_control(C.byref(params)), "mega_fint_control")
+    state, stress, strain = _f64(state).copy(), _f64(stress).copy(), _f64(strain).copy()
+    shp = _f64(shp).copy()
+    ik = np.ascontiguousarray(np.transpose(_f64(ginvk), (0, 2, 1)))
+    nnz = len(gstack)
+    fint, wv, cdist = np.zeros(3 * n), np.zeros(n), np.zeros(n)
+    z6, z3n, zn = np.zeros((n, 6)), np.zeros((n, 3)), np.zeros(n)
+    gw = C.c_double(0.0)
+    dlt_fint = C.c_double(-1.0)
+    st = _lib.lib().construct_fint_pd_gpu(
+        ptr(_f64(win)), ptr(_f64(vol)), _ref(n, C.c_int32), ptr(_f64(coo)), ptr(_f64(coo_current)),
+        ptr(z6), ptr(z3n), ptr(zn), ptr(z3n), ptr(_i32(np.zeros(n))), ptr(_f64(props)), ptr(state), ptr(stress),
+        ptr(strain), ptr(z6.copy()), ptr(z6.copy()), ptr(_f64(dinc)), ptr(_f64(np.zeros(3 * n))), ptr(_i32(mat_type)),
+        ptr(_i32(np.zeros(n))), ptr(_i32(gn)), ptr(_i32(gstart)), _ref(nnz, C.c_int32), ptr(_i32(gstack)), ptr(shp),
+        ptr(np.zeros((nnz, 3))), ptr(np.zeros((nnz, 6))), _ref(int(np.max(gn)), C.c_int32), ptr(ik),
+        _ref(int(bool(linit)), C.c_int32), ptr(fint), C.byref(dlt_fint), ptr(cdist), ptr(wv), ptr(z6.copy()),
+        ptr(z6.copy()), ptr(z6.copy()), ptr(zn), ptr(zn), ptr(zn), ptr(z3n), C.byref(gw), _ref(float(dlt), C.c_double))
+    check(st, "construct_fint_pd_gpu", allow_status)
+    return dict(fint=fint, stress=stress, strain=strain, state=state, gmax_wvel=wv, shp=shp,
+                ginvk=np.transpose(ik, (0, 2, 1)).copy(), gchar_dist=cdist, dlt_fint=dlt_fint.value, status=st)
+
+
 def pre_model_hex(coo, elems, norm_win=None, allow_status=False):
     """Mesh pre-processing on the device (PRE_MODEL.F90:248-268, PRE_CONTROL.F90:
     803-871) for a hexahedral mesh: elems (E, 8) 0-based node ids.  Returns
@@ -434,7 +512,7 @@ class Pmb:
         return k.value
 
     def download(self, what):
-        m = self.nnz if what == 3 else 3 * self.n
+        m = self.nnz if what == 3 else (self.n if what == 4 else 3 * self.n)
         out = np.zeros(m)
         nbk = C.c_int64(0)
         check(_lib.lib().mega_pmb_download(self.h, int(what), ptr(out), C.byref(nbk)), "pmb_download")

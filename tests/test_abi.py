@@ -85,3 +85,21 @@ def test_mirror_raises_on_error_codes():
     with pytest.raises(_lib.MegaError):
         _lib.check(_lib.ST_NEWTON_CAP, "x")
     assert _lib.check(_lib.ST_NEWTON_CAP, "x", allow_status=True) == _lib.ST_NEWTON_CAP
+
+
+def _build_fortran_abi_check(tmp_path):
+    """gcc-compiles tests/fortran_abi_check.c (the force subroutines called
+    with Fortran's by-reference conventions) against include/mega_gpu.h and
+    links it with the library."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib_dir = os.path.join(root, "taylor_b200")
+    exe = str(tmp_path / "fortran_abi_check")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-O1", "-o", exe,
+                    os.path.join(root, "tests", "fortran_abi_check.c"), "-L" + lib_dir, "-lmega_gpu",
+                    "-Wl,-rpath," + lib_dir, "-lm"], check=True)
+    return exe
+
+
+def test_fortran_abi_check_compiles(tmp_path):
+    assert os.path.exists(_build_fortran_abi_check(tmp_path))
