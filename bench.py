@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--pre-nodes", type=int, default=100,
                     help="nodes per side of the hexahedral mesh of the pre-processing run; 0 skips it")
     ap.add_argument("--batch-bars", type=int, default=256, help="bars of the batched run; 0 skips it")
-    ap.add_argument("--batch-steps", type=int, default=64, help="timed steps of the batched and sequential runs")
+    ap.add_argument("--batch-steps", type=int, default=1500, help="timed steps of the batched and sequential runs")
     return ap.parse_args()
 
 
@@ -501,33 +501,37 @@ def pmb_run(args):
 def batch_run(args):
     """Many bars of uneven size (spacing uniform in 0.15-0.6 mm, v0 in
     100-300 m/s, sigma_y in 200-600 MPa, H = 100 MPa, one seed) stepped as
-    one context, every step one CUDA-graph replay over all bars, against the
-    same bars stepped one context after another.  Mixed precision; every
-    bar takes the smallest bar's stable step (0.5 x 0.9 h_min / c, 0.9 h the
-    closest two nodes of the +-5 % jittered lattice can be)."""
+    one context, every step one CUDA-graph replay over all bars, each bar
+    with its own stable step (mega_set_instance_dt), against the same bars
+    stepped one context after another.  Mixed precision, --batch-steps steps
+    of every bar timed.  Then the same bars with the power-law
+    rate-dependent law (A = sigma_y) log return-mapping samples on the batch
+    path and train the surrogate on them on the device."""
     from taylor_b200 import _lib, cases, mega
     b = cases.batch_bars(args.batch_bars)
     n = b["n"]
     p = _lib.params(**cases.param_kwargs(b, dist_max=tuple(float(v) for v in b["dist_max"].max(axis=0)),
                                          ql_len=b["ql_len"]))
-    pr = b["props"][0]
-    E, nu, rho = pr[1], pr[0], pr[2]
-    K, G = E / (3.0 * (1.0 - 2.0 * nu)), E / (2.0 * (1.0 + nu))
-    dt = 0.5 * 0.9 * b["h"] / np.sqrt((K + 4.0 * G / 3.0) / rho)
+    dts = b["dt"]
     K_steps = args.batch_steps
     t0 = time.perf_counter()
     m = mega.Mega(b, p)
     m.set_instances(b["counts"], b["dist_max"])
     m.set_precisions(fp64=False, mixed=True)
     m.search_and_shapes()
+    m.set_instance_dt(dts)
     init_s = time.perf_counter() - t0
-    m.step(3, dt, mode="mixed")
+    m.step(3, float(dts.min()), mode="mixed")
     clk = Clocks()
     clk.start()
-    ms = m.step_timed(K_steps, dt, mode="mixed")
+    ms = m.step_timed(K_steps, float(dts.min()), mode="mixed", allow_status=True)
     clocks = clk.stop()
+    status = int(m.last_status)
+    eps = m.download(_lib.F_EPS)
     dev_bytes = m.device_bytes()
     m.close()
+    off = np.concatenate([[0], np.cumsum(b["counts"])])
+    finite_bars = int(sum(np.all(np.isfinite(eps[off[k]:off[k + 1]])) for k in range(len(b["bars"]))))
     seq_ms = 0.0
     t0 = time.perf_counter()
     for k, bar in enumerate(b["bars"]):
@@ -536,17 +540,40 @@ def batch_run(args):
         s = mega.Mega(bar, pk)
         s.set_precisions(fp64=False, mixed=True)
         s.search_and_shapes()
-        s.step(3, dt, mode="mixed")
-        seq_ms += s.step_timed(K_steps, dt, mode="mixed")
+        s.step(3, float(dts[k]), mode="mixed")
+        seq_ms += s.step_timed(K_steps, float(dts[k]), mode="mixed", allow_status=True)
         s.close()
     seq_wall = time.perf_counter() - t0
+    # the rate-dependent batch generates the surrogate's training data
+    rb = cases.batch_bars(args.batch_bars, rate_law=RATE_LAW[1:])
+    pr = _lib.params(**cases.param_kwargs(rb, dist_max=tuple(float(v) for v in rb["dist_max"].max(axis=0)),
+                                          ql_len=rb["ql_len"], newton_max_iter=60, newton_rtol=1e-10))
+    q = mega.Mega(rb, pr)
+    q.set_instances(rb["counts"], rb["dist_max"])
+    q.set_precisions(fp64=False, mixed=True)
+    q.search_and_shapes()
+    q.set_instance_dt(rb["dt"])
+    q.log_rate_samples(cap=10_000_000, stride=4, seed=11)
+    log_steps = max(1, K_steps // 5)
+    t1 = time.perf_counter()
+    rst = q.step(log_steps, float(rb["dt"].min()), mode="mixed", allow_status=True)
+    log_s = time.perf_counter() - t1
+    held = _held_count(q)
+    t1 = time.perf_counter()
+    _, loss = q.train_surrogate(mega.mlp_init(5), epochs=6, batch=8192, lr=2e-3, seed=9)
+    train_s = time.perf_counter() - t1
+    q.close()
     return dict(workload=f"{args.batch_bars} Taylor bars, h in 0.15-0.6 mm", bars=args.batch_bars, nodes=n,
-                nodes_min=int(b["counts"].min()), nodes_max=int(b["counts"].max()), dt=dt, steps=K_steps,
+                nodes_min=int(b["counts"].min()), nodes_max=int(b["counts"].max()),
+                dt_min=float(dts.min()), dt_max=float(dts.max()), steps=K_steps, per_instance_dt=True,
                 batched=dict(ms_per_step=ms / K_steps, node_steps_per_s=n * K_steps / (ms / 1e3), init_s=init_s,
-                             device_bytes=dev_bytes, clocks=clocks),
+                             device_bytes=dev_bytes, clocks=clocks, status=status, bars_finite=finite_bars),
                 sequential=dict(ms_per_step=seq_ms / K_steps, node_steps_per_s=n * K_steps / (seq_ms / 1e3),
                                 wall_s_with_init=seq_wall),
-                batched_over_sequential=seq_ms / ms)
+                batched_over_sequential=seq_ms / ms,
+                surrogate_data=dict(law="power-law rate-dependent, A = sigma_y of each bar", steps=log_steps,
+                                    samples=int(held), log_s=log_s, status=int(rst), train_s=train_s,
+                                    loss_first_epoch=float(loss[0]), loss_last_epoch=float(loss[-1])))
 
 
 def _held_count(m):

@@ -346,6 +346,13 @@ int mega_gpu_init(const mega_params* p, int32_t n, const double* coo,
  * Energies and reaction sums in mega_get_scalars are totals over all
  * instances. */
 int mega_set_instances(int64_t h, int32_t ninst, const int32_t* inst_nodes, const double* dist_max);
+/* Give each instance of a mega_set_instances context its own explicit step
+ * (after mega_search_and_shapes): dt_inst (ninst) > 0.  The steps of
+ * mega_step_resident then advance instance k by dt_inst[k] each (its own
+ * stable step instead of the smallest instance's); the call's dt is still
+ * what TIME advances by and what the fixity-2 windows see.  NULL goes back to
+ * one dt for all.  MEGA_ERR_STATE for a context without instances. */
+int mega_set_instance_dt(int64_t h, const double* dt_inst);
 /* Autotuner: time each launch variant of the two per-step gathers for the
  * given precision on this context's lists, reps launches each, keep the
  * fastest, and leave the state as it was.  Variants 0..3 hold the packed

@@ -84,6 +84,7 @@ SIGNATURES = {
     "mega_set_fixity2": (I32, [I64, I32, P, P]),
     "mega_release_cached_memory": (I32, []),
     "mega_set_variants": (I32, [I64, I32, I32, I32]),
+    "mega_set_instance_dt": (I32, [I64, P]),
     "mega_fint_control": (I32, [PP]),
     "construct_fint_gpu": (I32, [P] * 46),
     "construct_fint_pd_gpu": (I32, [P] * 43),

@@ -145,18 +145,21 @@ def bar_metrics(case, coo_cur, eps):
 
 
 def batch_bars(nbars=256, seed=5, h_range=(0.15e-3, 0.6e-3), v0_range=(100.0, 300.0), sy_range=(200e6, 600e6),
-               H=100e6, **bar):
+               H=100e6, rate_law=None, **bar):
     """Many Taylor bars of uneven size stepped as one batch: instance k has
     lattice spacing h_k, impact speed v0_k and yield stress sy_k drawn
-    uniformly from the ranges (one seed), linear hardening H.  The bars keep
-    their own coordinates (they overlap in space; each is searched alone).
-    Returns the concatenated case with `counts`, per-instance `dist_max`
-    (nbars, 3), `params` (h, v0, sy) and the instances themselves."""
+    uniformly from the ranges (one seed), linear hardening H -- or, with
+    rate_law = (B, n, C, epsdot0), the power-law rate-dependent law with
+    A = sy_k.  The bars keep their own coordinates (they overlap in space;
+    each is searched alone).  Returns the concatenated case with `counts`,
+    per-instance `dist_max` (nbars, 3), stable steps `dt` (nbars), `params`
+    (h, v0, sy) and the instances themselves."""
     rng = np.random.Generator(np.random.PCG64(seed))
     hs = rng.uniform(*h_range, nbars)
     v0s = rng.uniform(*v0_range, nbars)
     sys_ = rng.uniform(*sy_range, nbars)
-    bars = [taylor_bar(h=float(hs[k]), v0=float(v0s[k]), sy=float(sys_[k]), H=H, seed=seed * 1000 + k, **bar)
+    bars = [taylor_bar(h=float(hs[k]), v0=float(v0s[k]), sy=float(sys_[k]), H=H, seed=seed * 1000 + k,
+                       rate_law=None if rate_law is None else (float(sys_[k]),) + tuple(rate_law), **bar)
             for k in range(nbars)]
     keys = ("coo", "win", "win_raw", "vol", "mass", "ebc", "vinit", "props", "mat_type", "body_id", "sm_len", "wall",
             "layer")
@@ -165,8 +168,18 @@ def batch_bars(nbars=256, seed=5, h_range=(0.15e-3, 0.6e-3), v0_range=(100.0, 30
                counts=np.array([b["n"] for b in bars], np.int32),
                dist_max=np.stack([b["dist_max"] for b in bars]),
                ql_len=float(min(b["ql_len"] for b in bars)), params=np.stack([hs, v0s, sys_], axis=1), bars=bars,
-               h=float(hs.min()))
+               h=float(hs.min()), dt=np.array([lattice_dt(b) for b in bars]))
     return out
+
+
+def lattice_dt(bar, cfl=0.5):
+    """A stable step of a jittered lattice bar without its neighbour lists:
+    cfl x (0.9 h, the closest two nodes of a +-5 % jitter can be) over the
+    dilatational wave speed."""
+    p = bar["props"][0]
+    E, nu, rho = p[1], p[0], p[2]
+    K, G = E / (3.0 * (1.0 - 2.0 * nu)), E / (2.0 * (1.0 + nu))
+    return float(cfl * 0.9 * bar["h"] / np.sqrt((K + 4.0 * G / 3.0) / rho))
 
 
 def param_kwargs(case, **over):

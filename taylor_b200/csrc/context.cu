@@ -473,6 +473,7 @@ struct Ctx {
   // independent instances sharing the context (node ranges searched apart)
   std::vector<int32_t> inst_off;  // ninst + 1 prefix offsets, empty = one instance
   std::vector<double> inst_dmax;  // 3 per instance: DIST_MAX of its bin grid
+  double* ndt = nullptr;          // per-node step (renumbered order) when the instances step apart
   int prec_mask = 3;              // bit 0: FP64 records built, bit 1: mixed records
   int var_defgrad[2] = {0, 0};    // launch variant of the row gather, [FP64, mixed]
   int var_force[2] = {0, 0};      // launch variant of the column gather
@@ -559,7 +560,7 @@ static StressArgs stress_args(Ctx* c, double dt, int mode) {
   a.grav[0] = c->p.gravity[0]; a.grav[1] = c->p.gravity[1]; a.grav[2] = c->p.gravity[2];
   a.has_body = c->has_body; a.inv3_exact = c->p.inv3_exact; a.finite_strain = c->p.finite_strain;
   a.maxit = c->p.newton_max_iter; a.rate_solver = c->p.rate_solver; a.rtol = c->p.newton_rtol; a.dt = dt; a.iters = c->iters;
-  a.aux = c->aux; a.acc = c->acc; a.status = c->status;
+  a.aux = c->aux; a.acc = c->acc; a.status = c->status; a.ndt = c->ndt;
   if ((mode & MEGA_FLAG_LEARNED_GUESS) && c->mlp_on) {
     a.mlp_w2 = c->mlp_w2; a.mlp_small = c->mlp_small; a.queue = c->mlp_queue; a.qcount = c->mlp_qcount;
   }
@@ -582,6 +583,7 @@ static TiledForceArgs force_args(Ctx* c, double dt, int mode, int predict) {
   f.fint = c->fint; f.fext = c->fext; f.vel = c->vel; f.acl = c->acl; f.dsp = c->dsp; f.dsp_tot = c->dsp_tot;
   f.prforce = c->prforce; f.fadd = c->nsni ? c->fstab : nullptr; f.dt = dt; f.acc = c->acc; f.status = c->status;
   f.vel2 = c->vel2;
+  f.ndt = c->ndt;
   return f;
 }
 
@@ -687,7 +689,7 @@ static int run_steps(Ctx* c, int32_t nsteps, double dt, int mode) {
   if (!(mode & MEGA_FLAG_INTERP_EACH_STEP)) c->phy_valid = false;
   int r = sync_time(c);
   if (r) return r;
-  r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
+  r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt, c->ndt);
   if (r) return r;
   c->launches += 1;
   int32_t rem = nsteps - 1;
@@ -1674,7 +1676,7 @@ int mega_kernel_times(int64_t h, int32_t reps, double dt, int32_t mode, float* o
   cudaEvent_t ev[4];
   for (auto& e : ev) MEGA_TRY(cudaEventCreate(&e));
   double acc[3] = {0, 0, 0};
-  int r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt);
+  int r = launch_predict(c->s, 3 * (int64_t)c->n, c->dsp, c->dsp_tot, c->vel, c->acl, dt, c->ndt);
   for (int32_t k = 0; k < reps && !r; ++k) {
     r = step_once(c, dt, mode, k < reps - 1 ? 1 : 0, ev);
     if (r) break;
@@ -2048,6 +2050,37 @@ int mega_set_precisions(int64_t h, int32_t mask) {
 static void drop_graph(Ctx* c) {
   if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
   c->g_mode = -1;
+}
+
+__global__ void k_gather_inst_dt(int32_t n, const int32_t* __restrict__ perm, const double* __restrict__ src,
+                                 double* __restrict__ dst) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r < n) dst[r] = src[perm[r]];
+}
+
+int mega_set_instance_dt(int64_t h, const double* dt_inst) {
+  Ctx* c = get_ctx(h);
+  if (!c) return MEGA_ERR_HANDLE;
+  if (!c->searched || c->semi) return MEGA_ERR_STATE;
+  if (c->inst_off.size() < 2) return MEGA_ERR_STATE;  // not declared as instances
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  drop_graph(c);
+  if (!dt_inst) { c->ndt = nullptr; return 0; }      // back to the call's dt for every node
+  const size_t ninst = c->inst_off.size() - 1;
+  std::vector<double> hd(c->n);
+  for (size_t k = 0; k < ninst; ++k) {
+    if (!(dt_inst[k] > 0.0)) return MEGA_ERR_ARG;
+    for (int32_t i = c->inst_off[k]; i < c->inst_off[k + 1]; ++i) hd[i] = dt_inst[k];
+  }
+  if (!c->ndt) MEGA_ALLOC(c->pool, c->ndt, c->n);
+  DevPool tp(c->s);
+  double* tmp = nullptr;
+  MEGA_ALLOC(tp, tmp, c->n);
+  MEGA_TRY(cudaMemcpyAsync(tmp, hd.data(), sizeof(double) * c->n, cudaMemcpyHostToDevice, c->s));
+  k_gather_inst_dt<<<grid_for(c->n, 256), 256, 0, c->s>>>(c->n, c->perm, tmp, c->ndt);
+  MEGA_CHECK_LAUNCH();
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  return 0;
 }
 
 int mega_set_variants(int64_t h, int32_t mode, int32_t defgrad_variant, int32_t force_variant) {

@@ -277,14 +277,15 @@ __device__ __forceinline__ void stress_finish(const StressArgs& a, int64_t i, Tr
     it = von_mises(w.spred, ep, m, a.maxit, snew, cap);
   } else if (m.type == MEGA_MAT_VM_RATE) {
     double dg = 0.0, ftr = 0.0;
-    it = vm_rate(w.spred, ep, m, a.dt, a.rtol, a.maxit, a.rate_solver, dg0, snew, cap, dg, ftr);
+    const double dt = a.ndt ? a.ndt[i] : a.dt;
+    it = vm_rate(w.spred, ep, m, dt, a.rtol, a.maxit, a.rate_solver, dg0, snew, cap, dg, ftr);
     if (a.log_buf && it > 0) {  // sample (features, converged multiplier) for the surrogate
       const uint64_t sb = (uint64_t)__double_as_longlong(w.spred[0]);
       const uint32_t hsh = ((uint32_t)i * 2654435761u) ^ (uint32_t)(sb ^ (sb >> 29)) ^ a.log_seed;
       if (hsh % a.log_stride == 0) {
         float x[4];
         double ub;
-        const double f = rate_features(w.spred, ep0, me, a.dt, x, ub);
+        const double f = rate_features(w.spred, ep0, me, dt, x, ub);
         if (f > 0.0 && ub > 0.0) {
           const unsigned long long k = atomicAdd(a.log_count, 1ull);
           if ((int64_t)k < a.log_cap) {
@@ -488,7 +489,7 @@ __global__ void __launch_bounds__(kLearnBlock, 4) k_stress_queue(StressArgs a) {
     double ub = 0.0, f = -1.0;
     if (act) {
       stress_trial<T, true, DAM>(a, i, w);
-      f = rate_features(w.spred, a.eps[i], a.mats[w.mi], a.dt, x, ub);
+      f = rate_features(w.spred, a.eps[i], a.mats[w.mi], a.ndt ? a.ndt[i] : a.dt, x, ub);
     }
     const float y = warp_mlp(x, act && f > 0.0, net, hw, ow);
     if (act) {
@@ -605,9 +606,11 @@ __global__ void __launch_bounds__(256) k_force(ForceArgs a) {
 }
 
 __global__ void k_predict(int64_t n3, double* __restrict__ dsp, double* __restrict__ dsp_tot,
-                          double* __restrict__ vel, const double* __restrict__ acl, double dt) {
+                          double* __restrict__ vel, const double* __restrict__ acl, double dt,
+                          const double* __restrict__ ndt) {
   const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (m >= n3) return;
+  if (ndt) dt = ndt[m / 3];
   const double v = vel[m], a = acl[m];
   const double d = dt * v + dt * dt * 0.5 * a;
   dsp[m] = d;
@@ -730,9 +733,9 @@ int launch_force(cudaStream_t s, bool mixed, const ForceArgs& a) {
 }
 
 int launch_predict(cudaStream_t s, int64_t n3, double* dsp, double* dsp_tot, double* vel, const double* acl,
-                   double dt) {
+                   double dt, const double* ndt) {
   if (n3 <= 0) return 0;
-  k_predict<<<grid_for(n3, 256), 256, 0, s>>>(n3, dsp, dsp_tot, vel, acl, dt);
+  k_predict<<<grid_for(n3, 256), 256, 0, s>>>(n3, dsp, dsp_tot, vel, acl, dt, ndt);
   MEGA_CHECK_LAUNCH();
   return 0;
 }

@@ -254,6 +254,7 @@ struct StressArgs {
   double* aux;               // 4 per node: STATE(1, 2, 4, 5) of the damaged models (or null)
   const uint16_t* mlp_w2;    // surrogate network: W2 (64x64) as bf16 bits, or null
   const float* mlp_small;    // W1 (64x4), b1, b2, W3, b3 as fp32, or null
+  const double* ndt;         // per-node step of independent instances, or null (dt for all)
   int32_t* queue;            // learned start: plastic rate-dependent nodes of this step (n), or null
   unsigned* qcount;          // their count (zeroed before the step's stress kernels)
   float* log_buf;            // sample log: 5 floats (4 features, target) per sample, or null
@@ -342,7 +343,7 @@ struct ForceArgs {
 };
 int launch_force(cudaStream_t s, bool mixed, const ForceArgs& a);
 int launch_predict(cudaStream_t s, int64_t n3, double* dsp, double* dsp_tot, double* vel, const double* acl,
-                   double dt);
+                   double dt, const double* ndt = nullptr);
 // out[3i+k] = base[3i+k] + sum_J shp_iJ * val[3J+k]
 int launch_interp(cudaStream_t s, int32_t n, const DevCSR& csr, const double* shp, const double* val,
                   const double* base, double* out);

@@ -370,6 +370,7 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
 __device__ __forceinline__ void correct_dof(const TiledForceArgs& a, int64_t J, int q, double fi, double fe,
                                             double& ke, double& ee, double* tf, unsigned& st) {
   const int64_t m = 3 * J + q;
+  const double dt = a.ndt ? a.ndt[J] : a.dt;
   if (a.fadd) fi += a.fadd[m];
   if (!isfinite(fi)) st |= MEGA_ST_NONFINITE;
   const double mass = a.mass[m];
@@ -383,8 +384,8 @@ __device__ __forceinline__ void correct_dof(const TiledForceArgs& a, int64_t J, 
     fe = -fi;
   } else {  // MAIN.F90:472-481
     const double mpdc = a.mats[a.matidx[J]].damp * mass;
-    acc = (fe - fi - mpdc * v) / (mass + 0.5 * a.dt * mpdc);
-    v = v + 0.5 * a.dt * acc;
+    acc = (fe - fi - mpdc * v) / (mass + 0.5 * dt * mpdc);
+    v = v + 0.5 * dt * acc;
     pr = 0.0;
   }
   ee += 0.5 * (fe + fe_old) * a.dsp[m];
@@ -401,10 +402,10 @@ __device__ __forceinline__ void correct_dof(const TiledForceArgs& a, int64_t J, 
   a.acl[m] = acc;
   a.prforce[m] = pr;
   if (a.predict) {  // MAIN.F90:353-355 of the next step
-    const double d = a.dt * v + a.dt * a.dt * 0.5 * acc;
+    const double d = dt * v + dt * dt * 0.5 * acc;
     a.dsp[m] = d;
     a.dsp_tot[m] = a.dsp_tot[m] + d;
-    v = v + a.dt * 0.5 * acc;
+    v = v + dt * 0.5 * acc;
   }
   a.vel[m] = v;
 }

@@ -45,6 +45,7 @@ struct TiledForceArgs {
   double* prforce;
   const double* fadd;     // 3 per node added to the internal force (NSNI), or null
   const double* vel2;     // prescribed velocities of fixity code 2 for this step (3), or null
+  const double* ndt;      // per-node step of independent instances, or null (dt for all)
   double dt;
   StepAccum* acc;
   unsigned* status;

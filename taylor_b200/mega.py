@@ -320,6 +320,11 @@ class Mega:
         df = np.ascontiguousarray(d.ravel(order="F"))
         check(_lib.lib().mega_set_fixity2(self.h, len(t), ptr(tf), ptr(df)), "set_fixity2")
 
+    def set_instance_dt(self, dt_inst):
+        """Each instance steps by its own dt (None: one dt for all)."""
+        d = None if dt_inst is None else _f64(dt_inst)
+        check(_lib.lib().mega_set_instance_dt(self.h, ptr(d)), "set_instance_dt")
+
     def set_variants(self, defgrad, force, mode="mixed"):
         """Pin the gathers' launch variants for one precision."""
         check(_lib.lib().mega_set_variants(self.h, self.mode_bits(mode), int(defgrad), int(force)), "set_variants")

@@ -99,3 +99,31 @@ def test_autotune_keeps_state_and_results():
     assert np.abs(xa - xb).max() <= 1e-10 * np.abs(xb - bar["coo"]).max()
     a.close()
     b.close()
+
+
+def test_instances_with_their_own_steps():
+    """mega_set_instance_dt: each bar advances by its own stable step, and
+    equals its own context stepped with that step (FP64, bit for bit)."""
+    b = _batch()
+    dts = [2.0e-8, 3.0e-8, 2.5e-8][:len(b["bars"])]
+    m = mega.Mega(b, _params(b, b["dist_max"].max(axis=0)))
+    m.set_instances(b["counts"], b["dist_max"])
+    m.search_and_shapes()
+    m.set_instance_dt(dts)
+    m.step(40, 1.0e-8, mode="fp64")
+    xb = m.download(_lib.F_COO_CURRENT)
+    m.close()
+    off = np.concatenate([[0], np.cumsum(b["counts"])])
+    for k, bar in enumerate(b["bars"]):
+        s = mega.Mega(bar, _params(b, b["dist_max"][k]))
+        s.search_and_shapes()
+        s.step(40, dts[k], mode="fp64")
+        np.testing.assert_array_equal(xb[off[k]:off[k + 1]], s.download(_lib.F_COO_CURRENT))
+        s.close()
+    with pytest.raises(_lib.MegaError):
+        single = mega.Mega(b["bars"][0], _params(b, b["dist_max"][0]))
+        single.search_and_shapes()
+        try:
+            single.set_instance_dt([1e-8])   # no instances declared
+        finally:
+            single.close()
