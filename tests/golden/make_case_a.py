@@ -11,7 +11,7 @@ the arrays the hot path consumes:
                                                              PRE_MODEL_VOL2.F90:36-52
   the deck values the hot path uses (window 2.75, QL, props, v0, fixity, dt)
                                                              Control.dat, READ.F90:354-511
-Usage: python tests/golden/make_case_a.py [reference_dir]
+Usage: python tests/golden/make_case_a.py <reference_dir>   (the directory holding Taylor_bar.k)
 """
 import os
 import sys
@@ -93,8 +93,7 @@ def windows_and_volumes(coo, elems):
     return adial, vol
 
 
-def main(ref=None):
-    ref = ref or "/root/reference"
+def main(ref):
     coo, elems, sets = read_k(os.path.join(ref, "Taylor_bar.k"))
     win_raw, vol = windows_and_volumes(coo, elems)
     out = os.path.join(HERE, "case_a.npz")
@@ -105,4 +104,6 @@ def main(ref=None):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else None)
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_case_a.py <reference_dir>")
+    main(sys.argv[1])
