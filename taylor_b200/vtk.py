@@ -1,9 +1,16 @@
-"""Output steps as legacy ASCII VTK files in the layout VTK_OUTPUT.F90
-writes (MEGAOUT_####.vtk): the header (VTK_OUTPUT_HEADER), the current
-coordinates as POINTS (3E13.5), one vertex cell per node (and the hexes when
-a mesh is given), POINT_DATA with one SCALARS block per component (E20.5),
-as VTK_WRITE_DBL / VTK_WRITE_DBL_THREE lay them out.  The arrays come from
-one device-to-host copy (Mega.snapshot); this module only formats them.
+"""Output steps as legacy ASCII VTK files in the layouts MEGA writes
+(MEGAOUT_####.vtk): the header (VTK_OUTPUT_HEADER), the current coordinates
+as POINTS, one vertex cell per node (and the elements when a mesh is given),
+POINT_DATA with one SCALARS block per component.  Two number formats, as the
+reference has two writers:
+  write_vtk               VTK_OUTPUT.F90: points in 3E13.5, scalars in E20.5
+                          (five significant digits);
+  write_vtk_list_directed VTK_OUTPUT_UNFORMATTED.F90 (UNF_OUTPUT_STEP_VTK):
+                          every number in list-directed free format
+                          (WRITE(unit,*)), 17 significant digits for doubles,
+                          so the file keeps every double exactly.
+The arrays come from one device-to-host copy (Mega.snapshot); this module
+only formats them.
 """
 import numpy as np
 
@@ -22,6 +29,32 @@ def fortran_e(x, w, d):
     e = int(t[t.index("e") + 1:]) + 1             # 0.mmmmm x 10^e
     ex = f"E{'+' if e >= 0 else '-'}{abs(e):02d}" if abs(e) < 100 else f"{'+' if e >= 0 else '-'}{abs(e):03d}"
     return (("-" if x < 0 else "") + "0." + mant + ex).rjust(w)
+
+
+def fortran_list_real(x):
+    """One DOUBLE PRECISION item of gfortran list-directed output: a blank,
+    then the value in G25.17E3 editing -- F20.(17-k) followed by five blanks
+    when 0.1 <= |x| < 1e17 after rounding to 17 digits (k digits before the
+    point; zero counts as k = 1), else 1PE25.16E3."""
+    if not np.isfinite(x):
+        return " " + ("NaN" if np.isnan(x) else ("-Infinity" if x < 0 else "Infinity")).rjust(25)
+    d = 17
+    sign = "-" if np.signbit(x) else ""
+    if x == 0.0:
+        return " " + (sign + "0." + "0" * (d - 1)).rjust(20) + " " * 5
+    t = f"{abs(x):.{d - 1}e}"                     # d significant digits: m.mmm...e+XX
+    e10 = int(t[t.index("e") + 1:])
+    if -1 <= e10 < d:                             # F editing, d - k decimals
+        k = e10 + 1
+        return " " + (sign + f"{abs(x):.{d - k}f}").rjust(20) + " " * 5
+    mant = t[:t.index("e")]
+    ex = f"E{'+' if e10 >= 0 else '-'}{abs(e10):03d}"
+    return " " + (sign + mant + ex).rjust(25)
+
+
+def fortran_list_int(v):
+    """One default INTEGER item of gfortran list-directed output: width 12."""
+    return f"{int(v):12d}"
 
 
 def _scalars(lines, name, values):
@@ -70,6 +103,38 @@ def write_vtk(path, coo_current, data, elements=None):
     lines.append("POINT_DATA " + str(n).rjust(10))
     for name, values in data:
         _scalars(lines, name, np.asarray(values, np.float64).reshape(-1))
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def write_vtk_list_directed(path, coo_current, data, elements=None):
+    """The layout of UNF_OUTPUT_STEP_VTK (VTK_OUTPUT_UNFORMATTED.F90): as
+    write_vtk, with every number written list-directed (fortran_list_real,
+    fortran_list_int) -- points three per record, cells as (count, ids...),
+    cell types and scalar values one per record."""
+    x = np.asarray(coo_current, np.float64).reshape(-1, 3)
+    n = len(x)
+    ne = 0 if elements is None else len(elements)
+    lines = ["# vtk DataFile Version 2.0", "(MEGA VTK FILE)".rjust(30), "ASCII", "DATASET UNSTRUCTURED_GRID",
+             "POINTS " + str(n).rjust(10) + "double".rjust(10)]
+    lines.extend(fortran_list_real(a) + fortran_list_real(b) + fortran_list_real(c) for a, b, c in x)
+    lines.append("  ")
+    lines.append("CELLS " + str(n + ne).rjust(10) + str(2 * n + 9 * ne).rjust(20))
+    lines.extend(fortran_list_int(1) + fortran_list_int(i) for i in range(n))
+    if ne:
+        lines.extend(fortran_list_int(8) + "".join(fortran_list_int(v) for v in el) for el in np.asarray(elements))
+    lines.append("  ")
+    lines.append("CELL_TYPES" + str(n + ne).rjust(8))
+    lines.extend([fortran_list_int(1)] * n)
+    lines.extend([fortran_list_int(12)] * ne)
+    lines.append("  ")
+    lines.append("  ")
+    lines.append("POINT_DATA " + str(n).rjust(10))
+    for name, values in data:
+        lines.append("  ")
+        lines.append("SCALARS " + name.rjust(30) + "double 1".rjust(10))
+        lines.append("LOOKUP_TABLE default")
+        lines.extend(fortran_list_real(v) for v in np.asarray(values, np.float64).reshape(-1))
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
 
