@@ -305,6 +305,17 @@ int construct_fint_pd_gpu(const double* gwin, const double* gvol, const int32_t*
 int mega_pre_model_hex(int32_t n, const double* coo, int32_t nelem, const int32_t* conn, const double* norm_win,
                        double* win_raw, double* win, double* vol, double* sm_len, double* mom, double* dist_max,
                        double* min_raw_window);
+/* As mega_pre_model_hex for meshes of hexahedral and tetrahedral blocks:
+ * eltype (nelem) 2 = hexahedron, 1 = tetrahedron (the reference's block
+ * type, PRE_MODEL.F90:233-240: a block whose last element repeats its
+ * seventh node as its eighth; kfile.read_k applies that rule), NULL = all
+ * hexahedra.  A tetrahedron counts its first four nodes: its window is
+ * their largest per-axis extent (PRE_MODEL_ADIAL.F90:112-150) and each gets
+ * 1/4 of its volume (GET_VOL1, PRE_MODEL_VOL1.f90:37-45,
+ * PRE_MODEL_VOLUMES.F90:99-115). */
+int mega_pre_model(int32_t n, const double* coo, int32_t nelem, const int32_t* conn, const int32_t* eltype,
+                   const double* norm_win, double* win_raw, double* win, double* vol, double* sm_len, double* mom,
+                   double* dist_max, double* min_raw_window);
 
 int mega_construct_fint_pd(const mega_params* p, int32_t n,
                            const double* gcoo, const double* gcoo_current,

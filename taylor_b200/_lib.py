@@ -112,6 +112,7 @@ SIGNATURES = {
     "mega_rate_samples": (I32, [I64, P, I64, C.POINTER(I64)]),
     "mega_train_surrogate": (I32, [I64, P, I32, I32, F32, C.c_uint64, P]),
     "mega_pre_model_hex": (I32, [I32, P, I32, P, P, P, P, P, P, P, P, P]),
+    "mega_pre_model": (I32, [I32, P, I32, P, P, P, P, P, P, P, P, P, P]),
     "mega_status_string": (C.c_char_p, [I32]),
     "mega_gpu_finalize": (I32, [I64]),
 }

@@ -1,11 +1,16 @@
 // premodel.cu -- the mesh pre-processing of PRE_MODEL.F90:248-268 and
-// PRE_CONTROL.F90:803-871 on the device, for hexahedral meshes:
+// PRE_CONTROL.F90:803-871 on the device, for meshes of hexahedral and
+// tetrahedral blocks (a tetrahedron is an 8-node connectivity whose last
+// nodes repeat, PRE_MODEL.F90:233-240):
 //   raw nodal windows  ADIAL = the largest per-axis extent of the hexes
 //                      holding the node (GET_ADIAL, PRE_MODEL_ADIAL.F90:64-153)
 //   nodal volumes      the sum of 1/8 of every such hex's volume, the hex
 //                      split into three tetrahedral wedges about the 1-7
 //                      diagonal (GET_VOLUMES / GET_VOL2, PRE_MODEL_VOLUMES.F90:
-//                      70-117, PRE_MODEL_VOL2.F90:36-52)
+//                      70-117, PRE_MODEL_VOL2.F90:36-52), and 1/4 of every
+//                      tetrahedron's volume (GET_VOL1, PRE_MODEL_VOL1.f90:
+//                      37-45); a tetrahedron's window is the extent of its
+//                      first four nodes (PRE_MODEL_ADIAL.F90:112-150)
 //   smoothing cells    SM_LEN, second moments, DIST_MAX
 //                      (GET_SMOOTHING_LENGTHS, PRE_MODEL_SMOOTHING_LENGTHS.F90:
 //                      49-99)
@@ -14,9 +19,8 @@
 //                      window (the automatic QL_LEN before its reduction,
 //                      PRE_CONTROL.F90:803-815).
 // The element-to-node sums run over a node-to-element list sorted by element,
-// so each node adds its hexes' volumes in the reference's element order
-// (bit for bit; the hex volume uses no fused multiply-adds).  Tetrahedral
-// blocks (GET_VOL1) are not built.
+// so each node adds its elements' volumes in the reference's element order
+// (bit for bit; the element volumes use no fused multiply-adds).
 #include "mega_internal.cuh"
 
 namespace mega {
@@ -33,13 +37,21 @@ __device__ __forceinline__ double det_cols(const double c0[3], const double c1[3
   return fabs(__dadd_rn(__dadd_rn(__dmul_rn(c0[0], t1), __dmul_rn(c1[0], t2)), __dmul_rn(c2[0], t3)));
 }
 
-// per hex: the per-axis extents and the volume
-__global__ void k_hex_elem(int32_t n, int32_t ne, const double* __restrict__ coo, const int32_t* __restrict__ conn,
-                           double* __restrict__ ext, double* __restrict__ dvol, unsigned* __restrict__ status) {
+// nodes an element of type t (1 tetrahedron, 2 hexahedron) contributes to
+__device__ __forceinline__ int elem_nodes(const int8_t* eltype, int64_t e) {
+  return (eltype && eltype[e] == 1) ? 4 : 8;
+}
+
+// per element: the per-axis extents and its share of volume per node
+// (0.125 DVOL for a hex, 0.25 DVOL for a tetrahedron)
+__global__ void k_elem(int32_t n, int32_t ne, const double* __restrict__ coo, const int32_t* __restrict__ conn,
+                       const int8_t* __restrict__ eltype, double* __restrict__ ext, double* __restrict__ dvol,
+                       unsigned* __restrict__ status) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= ne) return;
+  const int nk = elem_nodes(eltype, e);
   double x[8][3];
-  for (int k = 0; k < 8; ++k) {
+  for (int k = 0; k < nk; ++k) {
     const int32_t id = conn[8 * e + k] - 1;  // IDELM is 1-based
     if (id < 0 || id >= n) {
       atomicOr(status, (unsigned)MEGA_ST_BAD_MESH);
@@ -49,11 +61,21 @@ __global__ void k_hex_elem(int32_t n, int32_t ne, const double* __restrict__ coo
     }
     x[k][0] = coo[3 * (int64_t)id]; x[k][1] = coo[3 * (int64_t)id + 1]; x[k][2] = coo[3 * (int64_t)id + 2];
   }
-  // max over node pairs of |x_K - x_J| is the range of the eight values
+  // max over node pairs of |x_K - x_J| is the range of the nk values
   for (int a = 0; a < 3; ++a) {
     double lo = x[0][a], hi = x[0][a];
-    for (int k = 1; k < 8; ++k) { lo = fmin(lo, x[k][a]); hi = fmax(hi, x[k][a]); }
+    for (int k = 1; k < nk; ++k) { lo = fmin(lo, x[k][a]); hi = fmax(hi, x[k][a]); }
     ext[3 * e + a] = __dsub_rn(hi, lo);
+  }
+  if (nk == 4) {  // GET_VOL1: rows X4-X3, X1-X3, X2-X3 of A, DVOL = |det A| / 6
+    double c[3][3];  // c[col][row]
+    for (int a = 0; a < 3; ++a) {
+      c[a][0] = __dsub_rn(x[3][a], x[2][a]);
+      c[a][1] = __dsub_rn(x[0][a], x[2][a]);
+      c[a][2] = __dsub_rn(x[1][a], x[2][a]);
+    }
+    dvol[e] = __dmul_rn(0.25, __ddiv_rn(det_cols(c[0], c[1], c[2]), 6.0));
+    return;
   }
   // GET_VOL2: columns (X7-X1, X2-X1, X3-X6), (X7-X1, X5-X1, X6-X8), (X7-X1, X4-X1, X8-X3)
   double d71[3], d21[3], d36[3], d51[3], d68[3], d41[3], d83[3];
@@ -67,20 +89,23 @@ __global__ void k_hex_elem(int32_t n, int32_t ne, const double* __restrict__ coo
     d83[a] = __dsub_rn(x[7][a], x[2][a]);
   }
   const double ad = det_cols(d71, d21, d36), bd = det_cols(d71, d51, d68), cd = det_cols(d71, d41, d83);
-  dvol[e] = __ddiv_rn(__dadd_rn(__dadd_rn(ad, bd), cd), 6.0);
+  dvol[e] = __dmul_rn(0.125, __ddiv_rn(__dadd_rn(__dadd_rn(ad, bd), cd), 6.0));
 }
 
-__global__ void k_adj_count(int32_t n, int32_t ne, const int32_t* __restrict__ conn, int32_t* __restrict__ cnt) {
+__global__ void k_adj_count(int32_t n, int32_t ne, const int32_t* __restrict__ conn, const int8_t* __restrict__ eltype,
+                            int32_t* __restrict__ cnt) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= 8 * (int64_t)ne) return;
+  if ((t & 7) >= elem_nodes(eltype, t >> 3)) return;
   const int32_t id = conn[t] - 1;
   if (id >= 0 && id < n) atomicAdd(&cnt[id], 1);
 }
 
-__global__ void k_adj_fill(int32_t n, int32_t ne, const int32_t* __restrict__ conn, const int64_t* __restrict__ off,
-                           int32_t* __restrict__ fill, int32_t* __restrict__ list) {
+__global__ void k_adj_fill(int32_t n, int32_t ne, const int32_t* __restrict__ conn, const int8_t* __restrict__ eltype,
+                           const int64_t* __restrict__ off, int32_t* __restrict__ fill, int32_t* __restrict__ list) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= 8 * (int64_t)ne) return;
+  if ((t & 7) >= elem_nodes(eltype, t >> 3)) return;
   const int32_t id = conn[t] - 1;
   if (id < 0 || id >= n) return;
   list[off[id] + atomicAdd(&fill[id], 1)] = (int32_t)(t >> 3);
@@ -132,7 +157,7 @@ __global__ void __launch_bounds__(256) k_node_pre(PreArgs a) {
       if (a.ext[3 * e] > w0) w0 = a.ext[3 * e];
       if (a.ext[3 * e + 1] > w1) w1 = a.ext[3 * e + 1];
       if (a.ext[3 * e + 2] > w2) w2 = a.ext[3 * e + 2];
-      v = __dadd_rn(v, __dmul_rn(0.125, a.dvol[e]));
+      v = __dadd_rn(v, a.dvol[e]);  // the element's share, 0.125 or 0.25 DVOL
     }
     a.win_raw[3 * i] = w0; a.win_raw[3 * i + 1] = w1; a.win_raw[3 * i + 2] = w2;
     a.vol[i] = v;
@@ -176,7 +201,22 @@ extern "C" {
 int mega_pre_model_hex(int32_t n, const double* coo, int32_t nelem, const int32_t* conn, const double* norm_win,
                        double* win_raw, double* win, double* vol, double* sm_len, double* mom, double* dist_max,
                        double* min_raw_window) {
+  return mega_pre_model(n, coo, nelem, conn, nullptr, norm_win, win_raw, win, vol, sm_len, mom, dist_max,
+                        min_raw_window);
+}
+
+int mega_pre_model(int32_t n, const double* coo, int32_t nelem, const int32_t* conn, const int32_t* eltype,
+                   const double* norm_win, double* win_raw, double* win, double* vol, double* sm_len, double* mom,
+                   double* dist_max, double* min_raw_window) {
   if (n <= 0 || nelem <= 0 || !coo || !conn || !win_raw || !vol || !sm_len || !dist_max) return MEGA_ERR_ARG;
+  std::vector<int8_t> het;
+  if (eltype) {
+    het.resize(nelem);
+    for (int32_t e = 0; e < nelem; ++e) {
+      if (eltype[e] != 1 && eltype[e] != 2) return MEGA_ERR_ARG;  // 1 tetrahedron, 2 hexahedron
+      het[e] = (int8_t)eltype[e];
+    }
+  }
   cudaStream_t s;
   MEGA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   struct SG { cudaStream_t s; ~SG() { cudaStreamSynchronize(s); cudaStreamDestroy(s); } } sg{s};
@@ -184,6 +224,7 @@ int mega_pre_model_hex(int32_t n, const double* coo, int32_t nelem, const int32_
   const int64_t n3 = 3 * (int64_t)n;
   double *dc, *dext, *dvol, *dnw = nullptr, *dwr, *dw = nullptr, *dv, *dsl, *dmom = nullptr, *dred;
   int32_t *dconn, *cnt, *fill, *list;
+  int8_t* det = nullptr;
   int64_t* off;
   unsigned* st;
   MEGA_ALLOC(pool, dc, n3);
@@ -201,6 +242,10 @@ int mega_pre_model_hex(int32_t n, const double* coo, int32_t nelem, const int32_
   MEGA_ALLOC(pool, st, 1);
   if (win) MEGA_ALLOC(pool, dw, n3);
   if (mom) MEGA_ALLOC(pool, dmom, n3);
+  if (eltype) {
+    MEGA_ALLOC(pool, det, nelem);
+    MEGA_TRY(cudaMemcpyAsync(det, het.data(), (size_t)nelem, cudaMemcpyHostToDevice, s));
+  }
   if (norm_win) {
     MEGA_ALLOC(pool, dnw, n);
     MEGA_TRY(cudaMemcpyAsync(dnw, norm_win, sizeof(double) * n, cudaMemcpyHostToDevice, s));
@@ -212,12 +257,12 @@ int mega_pre_model_hex(int32_t n, const double* coo, int32_t nelem, const int32_
   MEGA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
   const double red0[4] = {0.0, 0.0, 0.0, 1.0e300};
   MEGA_TRY(cudaMemcpyAsync(dred, red0, sizeof(red0), cudaMemcpyHostToDevice, s));
-  k_hex_elem<<<grid_of(nelem, 256), 256, 0, s>>>(n, nelem, dc, dconn, dext, dvol, st);
-  k_adj_count<<<grid_of(8 * (int64_t)nelem, 256), 256, 0, s>>>(n, nelem, dconn, cnt);
+  k_elem<<<grid_of(nelem, 256), 256, 0, s>>>(n, nelem, dc, dconn, det, dext, dvol, st);
+  k_adj_count<<<grid_of(8 * (int64_t)nelem, 256), 256, 0, s>>>(n, nelem, dconn, det, cnt);
   MEGA_CHECK_LAUNCH();
   int r = scan_counts(s, cnt, off, n, pool);
   if (r) return r;
-  k_adj_fill<<<grid_of(8 * (int64_t)nelem, 256), 256, 0, s>>>(n, nelem, dconn, off, fill, list);
+  k_adj_fill<<<grid_of(8 * (int64_t)nelem, 256), 256, 0, s>>>(n, nelem, dconn, det, off, fill, list);
   k_adj_sort<<<grid_of(n, 256), 256, 0, s>>>(n, off, list);
   MEGA_CHECK_LAUNCH();
   PreArgs a{};

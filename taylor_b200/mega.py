@@ -209,6 +209,12 @@ def pre_model_hex(coo, elems, norm_win=None, allow_status=False):
     803-871) for a hexahedral mesh: elems (E, 8) 0-based node ids.  Returns
     win_raw, win (scaled by norm_win, per node or scalar), vol, sm_len, mom
     (X/Y/Z_MOM), dist_max and the smallest raw window."""
+    return pre_model(coo, elems, None, norm_win, allow_status)
+
+
+def pre_model(coo, elems, eltype=None, norm_win=None, allow_status=False):
+    """As pre_model_hex for hexahedral (eltype 2) and tetrahedral (eltype 1)
+    elements, elems (E, 8) 0-based -- the arrays kfile.read_k returns."""
     coo = _f64(coo)
     n = len(coo)
     conn = np.ascontiguousarray(np.asarray(elems, np.int64) + 1, dtype=np.int32)
@@ -218,9 +224,10 @@ def pre_model_hex(coo, elems, norm_win=None, allow_status=False):
     win_raw, win, mom = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
     vol, sm_len, dmax = np.zeros(n), np.zeros((n, 6)), np.zeros(3)
     wmin = C.c_double(0.0)
-    st = _lib.lib().mega_pre_model_hex(n, ptr(coo), len(conn), ptr(conn), ptr(nw), ptr(win_raw), ptr(win), ptr(vol),
-                                       ptr(sm_len), ptr(mom), ptr(dmax), C.byref(wmin))
-    check(st, "pre_model_hex", allow_status)
+    et = None if eltype is None else _i32(eltype)
+    st = _lib.lib().mega_pre_model(n, ptr(coo), len(conn), ptr(conn), ptr(et), ptr(nw), ptr(win_raw), ptr(win),
+                                   ptr(vol), ptr(sm_len), ptr(mom), ptr(dmax), C.byref(wmin))
+    check(st, "pre_model", allow_status)
     return dict(win_raw=win_raw, win=win, vol=vol, sm_len=sm_len, mom=mom, dist_max=dmax, min_raw_window=wmin.value,
                 status=st)
 

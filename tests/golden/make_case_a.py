@@ -6,6 +6,7 @@ script runs where the reference tree is mounted (it is not needed, and not
 run, on a GPU box) and restates the pre-processing that turns the mesh into
 the arrays the hot path consumes:
   *NODE / *ELEMENT_SOLID / *SET_NODE_LIST fixed-width reads  PRE_MODEL.F90:149-231
+                                                             (taylor_b200/kfile.py)
   raw nodal windows = max element extent per axis            PRE_MODEL_ADIAL.F90:64-153
   nodal volumes = 1/8 of each adjacent hex (GET_VOL2)         PRE_MODEL_VOLUMES.F90:70-117,
                                                              PRE_MODEL_VOL2.F90:36-52
@@ -18,55 +19,10 @@ import sys
 
 import numpy as np
 
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", ".."))
+from taylor_b200 import kfile  # noqa: E402  the product's reader of the deck
+
 HERE = os.path.dirname(os.path.abspath(__file__))
-
-
-def read_k(path):
-    lines = open(path).read().splitlines()
-    nodes, elems, sets = {}, [], {}
-    i = 0
-    while i < len(lines):
-        t = lines[i].strip()
-        if t == "*NODE":
-            i += 2  # comment line follows the card (PRE_MODEL.F90:156)
-            while i < len(lines) and not lines[i].startswith("*"):
-                ln = lines[i]
-                if ln.startswith("$") or not ln.strip():
-                    i += 1
-                    continue
-                nid = int(ln[0:8])
-                nodes[nid] = (float(ln[8:24]), float(ln[24:40]), float(ln[40:56]))
-                i += 1
-            continue
-        if t == "*ELEMENT_SOLID":
-            i += 1
-            while i < len(lines) and not lines[i].startswith("*"):
-                ln = lines[i]
-                if ln.strip() and not ln.startswith("$"):
-                    elems.append([int(ln[8 * k:8 * k + 8]) for k in range(2, 10)])
-                i += 1
-            continue
-        if t == "*SET_NODE_LIST":
-            sid = int(lines[i + 1].split()[0])
-            i += 2
-            ids = []
-            while i < len(lines) and not lines[i].startswith("*"):
-                ln = lines[i]
-                for k in range(8):
-                    f = ln[10 * k:10 * k + 10].strip()
-                    if f:
-                        v = int(f)
-                        if v != 0:
-                            ids.append(v)
-                i += 1
-            sets[sid] = np.array(ids, np.int32)
-            continue
-        i += 1
-    n = max(nodes)
-    coo = np.zeros((n, 3))
-    for k, v in nodes.items():
-        coo[k - 1] = v
-    return coo, np.array(elems, np.int32) - 1, sets
 
 
 def det_abs(a):
@@ -94,7 +50,8 @@ def windows_and_volumes(coo, elems):
 
 
 def main(ref):
-    coo, elems, sets = read_k(os.path.join(ref, "Taylor_bar.k"))
+    deck = kfile.read_k(os.path.join(ref, "Taylor_bar.k"))
+    coo, elems, sets = deck["coo"], deck["elems"], deck["sets"]
     win_raw, vol = windows_and_volumes(coo, elems)
     out = os.path.join(HERE, "case_a.npz")
     np.savez_compressed(out, coo=coo, win_raw=win_raw, vol=vol, elems=elems, bar=sets[1], wall=sets[2],
