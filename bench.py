@@ -75,15 +75,19 @@ def parse():
     return ap.parse_args()
 
 
-def dist_setup(n):
+def dist_setup(n, backend="nccl"):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE): the
+    process group carries only the barriers and the max-over-ranks timing
+    (replicas: every rank steps its own bar, no data-path collective)."""
     rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
     if world > 1:
         import datetime
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         return rank, world, dist
     return rank, world, None
 
@@ -92,7 +96,8 @@ def max_over_ranks(v, dist):
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -602,9 +607,8 @@ def cpu_baseline(case, steps, nthreads, warmup=1):
 
 def main():
     args = parse()
-    rank, world, dist = dist_setup(args.gpus)
     if args.impl == "reference":
-        if rank != 0:
+        if int(os.environ.get("RANK", 0)) != 0:  # rank 0 alone times the host cores; no process group
             return
         from taylor_b200 import cases
         case = cases.taylor_bar(h=args.h, seed=1)
@@ -625,6 +629,7 @@ def main():
         print(json.dumps(line))
         return
 
+    rank, world, dist = dist_setup(args.gpus)
     r = run_ours(args, rank, world, dist)
     if rank != 0:
         if dist is not None:
