@@ -191,6 +191,23 @@ def kernel_bytes(n, nnz, mixed):
     return dict(defgrad=defgrad, stress=stress, force=force)     # mass, fint, fext rw, vel rw, acl, dsp rw, tot rw, pr
 
 
+def nsni_step_bytes(n, nnz, mixed):
+    """Algorithmic bytes of one NSNI step (every array touched once): the
+    DNI kernels on the seven-point lists (kernel_bytes), the six second
+    derivatives S of every entry in both NSNI gathers with their row / column
+    index (4 + 6 s bytes each, s = 4 mixed or 8), the increment gathered by
+    k_nsni_h (24 per node), H (18 doubles written, read), the stress
+    gradients (18 doubles read and written), the force weights (18 floats /
+    doubles written, read), the stress before the step (6 doubles copied and
+    read) and the stabilisation force (3 doubles written, read)."""
+    kb = kernel_bytes(n, nnz, mixed)
+    s = 4 if mixed else 8
+    w = 80 if mixed else 144
+    per_entry = 2 * (4 + 6 * s)
+    per_node = 24 + 2 * 144 + 2 * 144 + 2 * w + 3 * 48 + 2 * 24
+    return kb["defgrad"] + kb["stress"] + kb["force"] + nnz * per_entry + n * per_node
+
+
 def survey_step_bytes(k, mixed):
     """Whole-step algorithmic bytes per node-step: 36k + 600 (FP64), 20k + 484 (mixed)."""
     return (20 * k + 484) if mixed else (36 * k + 600)
@@ -349,9 +366,15 @@ def nsni_run(case, dt, args):
         clocks = clk.stop()
         st = m.step(args.nsni_steps - args.warmup - args.steps, dt, mode=mode, allow_status=True)
         end = cases.bar_metrics(case, m.download(_lib.F_COO_CURRENT), m.download(_lib.F_EPS))
+        peak, _ = measured_peak()
+        sb = nsni_step_bytes(case["n"], int(res["nnz"]), mode == "mixed")
+        gbs = sb / (ms / args.steps / 1e3) / 1e9
         out[mode] = dict(setup_s=setup_s, nnz=int(res["nnz"]), ms_per_step=ms / args.steps,
                          node_steps_per_s=case["n"] * args.steps / (ms / 1e3), clocks=clocks, status=int(st),
-                         end_state=end, device_bytes=m.device_bytes())
+                         end_state=end, device_bytes=m.device_bytes(),
+                         roofline=dict(bound="hbm", scope="whole NSNI step", achieved=gbs, peak=peak, unit="GB/s",
+                                       frac=gbs / peak, algorithmic_bytes_per_step=sb,
+                                       hbm_floor_ms=sb / (peak * 1e9) * 1e3))
         m.close()
     if "end_state" in out.get("fp64", {}) and "end_state" in out.get("mixed", {}):
         ref, mix = out["fp64"]["end_state"], out["mixed"]["end_state"]
