@@ -185,8 +185,9 @@ def kernel_bytes(n, nnz, mixed):
     touched once; neighbour data counted once per owning node)."""
     g = 12 if mixed else 24          # three gradient components per CSR entry
     t = 36 if mixed else 72          # T_i (3x3) per node
-    defgrad = nnz * (4 + g) + n * (8 + 48 + 24 + 144)           # col + grad; rowptr, u and du, sum grad, F/G0 out
-    stress = n * (144 + 192 + 16 + 8 + 8 + 8 + 2 + t)           # F/G0, sigma+eps rw, eps_p rw, eq, wvel, vol, mat, T
+    fg = 72 if mixed else 144        # F (less its identity in mixed) and G0 per node
+    defgrad = nnz * (4 + g) + n * (8 + 48 + 24 + fg)            # col + grad; rowptr, u and du, sum grad, F/G0 out
+    stress = n * (fg + 192 + 16 + 8 + 8 + 8 + 2 + t)            # F/G0, sigma+eps rw, eps_p rw, eq, wvel, vol, mat, T
     force = nnz * (4 + g) + n * (8 + t + 3 + 24 + 24 + 48 + 48 + 24 + 48 + 48 + 24)  # trow + grad^T; T, fixity,
     return dict(defgrad=defgrad, stress=stress, force=force)     # mass, fint, fext rw, vel rw, acl, dsp rw, tot rw, pr
 

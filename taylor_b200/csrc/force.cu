@@ -153,10 +153,8 @@ template <typename T, bool LEAN, bool DAM>
 __device__ __forceinline__ void stress_trial(const StressArgs& a, int64_t i, Trial<T, LEAN>& w) {
   // F, G0 (18 doubles), stress and strain (6 each) as 16-byte loads
   double fgi[18], sv[6], ev[6];
+  load_fg(a.fg, i, sizeof(T) == 4, fgi);  // float F - I and G0 in mixed precision
   {
-    const double2* f2 = reinterpret_cast<const double2*>(a.fg + 18 * i);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) { const double2 v = f2[k]; fgi[2 * k] = v.x; fgi[2 * k + 1] = v.y; }
     const double2* s2 = reinterpret_cast<const double2*>(a.stress + 6 * i);
     const double2* e2 = reinterpret_cast<const double2*>(a.strain + 6 * i);
 #pragma unroll

@@ -159,6 +159,48 @@ __device__ __forceinline__ T tensor_norm_strain(const T v[6]) {
   return dsqrt<T>(v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + (v[3] * v[3] + v[4] * v[4] + v[5] * v[5]));
 }
 
+// The per-node deformation gradient F and increment gradient G0 between the
+// row gather and the stress update.  FP64: 18 doubles, F with its identity.
+// Mixed precision: 18 floats holding F - I and G0 (half the bytes; the
+// identity is added back in double when read, so F keeps its FP64 unit part
+// and the float carries only the displacement gradient, itself a float sum).
+// h[0..8] = F - I, h[9..17] = G0, row-major.
+__device__ __forceinline__ void store_fg(double* fg, int64_t i, bool mixed, const double h[18]) {
+  if (mixed) {
+    float2* o = reinterpret_cast<float2*>(reinterpret_cast<float*>(fg) + 18 * i);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o[k] = make_float2((float)h[2 * k], (float)h[2 * k + 1]);
+  } else {
+    double* o = fg + 18 * i;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o[k] = ((k % 4) == 0 ? 1.0 : 0.0) + h[k];
+#pragma unroll
+    for (int k = 9; k < 18; ++k) o[k] = h[k];
+  }
+}
+// F (with its identity) in f[0..8], G0 in f[9..17]
+__device__ __forceinline__ void load_fg(const double* fg, int64_t i, bool mixed, double f[18]) {
+  if (mixed) {
+    const float2* g = reinterpret_cast<const float2*>(reinterpret_cast<const float*>(fg) + 18 * i);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float2 v = g[k];
+      f[2 * k] = (double)v.x;
+      f[2 * k + 1] = (double)v.y;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k += 4) f[k] = 1.0 + f[k];
+  } else {
+    const double2* g = reinterpret_cast<const double2*>(fg + 18 * i);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const double2 v = g[k];
+      f[2 * k] = v.x;
+      f[2 * k + 1] = v.y;
+    }
+  }
+}
+
 // Per-node material constants the force kernel needs (from PROPS(30,N)).
 struct NodeMat {
   int32_t type;

@@ -169,7 +169,8 @@ __global__ void __launch_bounds__(128) k_nsni_stress(NsniStepArgs a) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double work = 0.0;
   if (i < a.n) {
-    const double* g = a.fg + 18 * i;
+    double g[18];
+    load_fg(a.fg, i, sizeof(WV) == 4, g);  // the mixed step stores F - I and G0 as floats
     double F[3][3], G0[3][3], IF[3][3], L[3][3], R[3][3], dstr[6], D[6];
 #pragma unroll
     for (int k = 0; k < 3; ++k)

@@ -348,14 +348,15 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
   if (q == 0) {
     const double ui[3] = {ui0, ui1, ui2}, di[3] = {di0, di1, di2};
     const double sd3[3] = {sdphi[3 * i], sdphi[3 * i + 1], sdphi[3 * i + 2]};
-    double* o = fg + 18 * i;
+    double h[18];
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int l = 0; l < 3; ++l) {
-        o[3 * k + l] = (k == l ? 1.0 : 0.0) + ((double)F[3 * k + l] + ui[k] * sd3[l]);
-        o[9 + 3 * k + l] = (double)L[3 * k + l] + di[k] * sd3[l];
+        h[3 * k + l] = (double)F[3 * k + l] + ui[k] * sd3[l];
+        h[9 + 3 * k + l] = (double)L[3 * k + l] + di[k] * sd3[l];
       }
+    store_fg(fg, i, !F64, h);
     if (INTERP) {
       dsp_tot_phy[3 * i] += ph0;
       dsp_tot_phy[3 * i + 1] += ph1;
@@ -745,14 +746,15 @@ __global__ void __launch_bounds__(64 * KG) k_defgrad_b(int32_t n, int32_t R, int
     } else {
       const double ui[3] = {ui0, ui1, ui2}, di[3] = {di0, di1, di2};
       const double sd3[3] = {sdphi[3 * i], sdphi[3 * i + 1], sdphi[3 * i + 2]};
-      double* o = fg + 18 * i;
+      double h[18];
 #pragma unroll
       for (int k = 0; k < 3; ++k)
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
-          o[3 * k + l] = (k == l ? 1.0 : 0.0) + ((double)F[3 * k + l] + ui[k] * sd3[l]);
-          o[9 + 3 * k + l] = (double)L[3 * k + l] + di[k] * sd3[l];
+          h[3 * k + l] = (double)F[3 * k + l] + ui[k] * sd3[l];
+          h[9 + 3 * k + l] = (double)L[3 * k + l] + di[k] * sd3[l];
         }
+      store_fg(fg, i, !F64, h);
       if (INTERP) {
         dsp_tot_phy[3 * i] += ph0;
         dsp_tot_phy[3 * i + 1] += ph1;
