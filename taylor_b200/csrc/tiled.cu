@@ -942,7 +942,9 @@ int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* 
 // (KG, KU) = (4, 4), (4, 2), (4, 1), (8, 2) with register-held record
 // streams, then KG = 4, 8 with the records streamed into shared memory.
 constexpr int kVariants = kTiledVariants;
-constexpr int kBulkSmemMax = 227 * 1024;  // dynamic shared memory of one block on sm_100
+// dynamic shared memory a streamed-variant block may ask for: sm_100's 227 KB
+// per block less room for the kernels' static shared memory (under 1 KB)
+constexpr int kBulkSmemMax = 227 * 1024 - 1024;
 
 template <typename K>
 static int raise_smem(K k, int lim) {
@@ -961,15 +963,30 @@ static int configure_variant(int lim) {
   return raise_smem(k_force_t<double, double, true, KG, KU>, lim);
 }
 
+static int g_bulk_lim = kBulkSmemMax;  // what the device grants, set by configure_tiled_kernels
+
+template <typename K>
+static int raise_smem_upto(K k, int lim) {
+  cudaFuncAttributes fa{};
+  MEGA_TRY(cudaFuncGetAttributes(&fa, k));
+  const int room = lim - (int)fa.sharedSizeBytes;
+  g_bulk_lim = std::min(g_bulk_lim, room);
+  return raise_smem(k, room);
+}
+
 template <int KG>
 static int configure_bulk(int lim) {
+  int dev = 0, optin = 0;
+  MEGA_TRY(cudaGetDevice(&dev));
+  MEGA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  lim = std::min(lim + 1024, optin);  // the kernels' static shared memory comes off this
   int r = 0;
-  if ((r = raise_smem(k_defgrad_b<float, false, true, KG>, lim))) return r;
-  if ((r = raise_smem(k_defgrad_b<float, false, false, KG>, lim))) return r;
-  if ((r = raise_smem(k_defgrad_b<double, true, true, KG>, lim))) return r;
-  if ((r = raise_smem(k_defgrad_b<double, true, false, KG>, lim))) return r;
-  if ((r = raise_smem(k_force_b<float, float, false, KG>, lim))) return r;
-  return raise_smem(k_force_b<double, double, true, KG>, lim);
+  if ((r = raise_smem_upto(k_defgrad_b<float, false, true, KG>, lim))) return r;
+  if ((r = raise_smem_upto(k_defgrad_b<float, false, false, KG>, lim))) return r;
+  if ((r = raise_smem_upto(k_defgrad_b<double, true, true, KG>, lim))) return r;
+  if ((r = raise_smem_upto(k_defgrad_b<double, true, false, KG>, lim))) return r;
+  if ((r = raise_smem_upto(k_force_b<float, float, false, KG>, lim))) return r;
+  return raise_smem_upto(k_force_b<double, double, true, KG>, lim);
 }
 
 // Raise the dynamic shared-memory limit of the tiled kernels once (outside
@@ -995,7 +1012,7 @@ bool tiled_variant_fits(const TileSet& ts, bool mixed, int variant, bool force, 
   if (variant < 0 || variant >= kVariants) return false;
   if (variant < 4) return true;
   const size_t stage = force ? (mixed ? sizeof(float) : sizeof(double)) * (has_body ? 12 : 9) : (mixed ? 24 : 48);
-  return (size_t)ts.recmax * (mixed ? 16 : 32) + stage * (size_t)ts.maxcnt <= (size_t)kBulkSmemMax;
+  return (size_t)ts.recmax * (mixed ? 16 : 32) + stage * (size_t)ts.maxcnt <= (size_t)g_bulk_lim;
 }
 
 template <int KG>
@@ -1004,7 +1021,7 @@ static int defgrad_bulk(cudaStream_t s, bool mixed, bool interp, int32_t n, cons
                         const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc,
                         unsigned* status) {
   const size_t smem = (size_t)ts.recmax * (mixed ? 16 : 32) + (mixed ? 24 : 48) * (size_t)ts.maxcnt;
-  if (smem > (size_t)kBulkSmemMax) return MEGA_ERR_UNSUPPORTED;
+  if (smem > (size_t)g_bulk_lim) return MEGA_ERR_UNSUPPORTED;
   const unsigned grid = (unsigned)ts.ntiles;
   const int block = ts.R * KG;
   if (mixed) {
@@ -1069,7 +1086,7 @@ static int force_bulk(cudaStream_t s, bool mixed, const TiledForceArgs& a) {
   const int nv = a.has_body ? 12 : 9;
   const size_t smem = (size_t)a.recmax * (mixed ? 16 : 32) + (mixed ? sizeof(float) : sizeof(double)) * nv *
                       (size_t)a.maxcnt;
-  if (smem > (size_t)kBulkSmemMax) return MEGA_ERR_UNSUPPORTED;
+  if (smem > (size_t)g_bulk_lim) return MEGA_ERR_UNSUPPORTED;
   const unsigned grid = (unsigned)a.ntiles;
   const int block = a.R * KG;
   if (mixed) k_force_b<float, float, false, KG><<<grid, block, smem, s>>>(a);
