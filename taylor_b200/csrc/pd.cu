@@ -327,8 +327,10 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
   // staged set: FP64 8 doubles per particle (X, u, vol, pad); float: X as
   // 3 doubles (the bond vector is rounded from the exact difference, as the
   // FP64 path forms it: float offsets of X put 1e-6 of the bond length into
-  // the stretch and move the break of near-critical bonds) and one float4
-  // (u - u_r0, vol)
+  // the stretch and move the break of near-critical bonds), one array per
+  // axis so that the eight lanes of a particle, reading neighbours of
+  // consecutive rank, read consecutive words (fewer bank conflicts than
+  // 24-byte records), and one float4 (u - u_r0, vol)
   double* sd = smp;
   float4* sf = reinterpret_cast<float4*>(smp + ((3 * cnt + 1) & ~1));
   const int64_t r0 = t * a.R;
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
       d[0] = make_double2(x0, x1); d[1] = make_double2(x2, u0); d[2] = make_double2(u1, u2);
       d[3] = make_double2(v, 0.0);
     } else {
-      sd[3 * l] = x0; sd[3 * l + 1] = x1; sd[3 * l + 2] = x2;
+      sd[l] = x0; sd[cnt + l] = x1; sd[2 * cnt + l] = x2;
       sf[l] = make_float4((float)(u0 - ur0), (float)(u1 - ur1), (float)(u2 - ur2), (float)v);
     }
   }
@@ -403,9 +405,8 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
           s = (l - L0) / L0;
           vj = (T)q3.x;
         } else {
-          const double* xq = sd + 3 * lj;
           const float4 ua = sf[lj];
-          const float x0 = (float)(xq[0] - Xi0), x1 = (float)(xq[1] - Xi1), x2 = (float)(xq[2] - Xi2);
+          const float x0 = (float)(sd[lj] - Xi0), x1 = (float)(sd[cnt + lj] - Xi1), x2 = (float)(sd[2 * cnt + lj] - Xi2);
           const float xx = x0 * x0 + x1 * x1 + x2 * x2;
           if (xx == 0.f) continue;  // the particle itself
           const float d0 = ua.x - fu0, d1 = ua.y - fu1, d2 = ua.z - fu2;
