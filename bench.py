@@ -351,7 +351,10 @@ def nsni_run(case, dt, args):
     """The same bar with stabilised nodal integration (ITYPE_INT = 2):
     set-up time, device-timed steps in both precisions, then FP64 and mixed
     runs from impact for --nsni-steps steps (the horizon direct nodal
-    integration does not reach on this lattice) with their end states."""
+    integration does not reach on this lattice) with their end states, and a
+    second FP64 run whose initial velocity differs by one part in 1e12: how
+    far the end-state measures move under a perturbation at the FP64 noise
+    level (their conditioning), the yardstick for the mixed run's error."""
     from taylor_b200 import _lib, cases, mega
     p = _lib.params(**cases.param_kwargs(case, itype_int=2))
     out = dict(steps=args.nsni_steps)
@@ -380,6 +383,14 @@ def nsni_run(case, dt, args):
     if "end_state" in out.get("fp64", {}) and "end_state" in out.get("mixed", {}):
         ref, mix = out["fp64"]["end_state"], out["mixed"]["end_state"]
         out["mixed_rel_err"] = {k: abs(mix[k] - ref[k]) / abs(ref[k]) for k in ref}
+        cp = dict(case)
+        cp["vinit"] = np.asarray(case["vinit"]) * (1.0 + 1.0e-12)
+        q = mega.Mega(cp, p)
+        q.search_and_shapes()
+        q.step(args.nsni_steps, dt, mode="fp64", allow_status=True)
+        pert = cases.bar_metrics(case, q.download(_lib.F_COO_CURRENT), q.download(_lib.F_EPS))
+        q.close()
+        out["fp64_perturbed_1e-12_rel_change"] = {k: abs(pert[k] - ref[k]) / abs(ref[k]) for k in ref}
     # direct nodal integration over the same steps, for its status
     d = mega.Mega(case, _lib.params(**cases.param_kwargs(case)))
     d.search_and_shapes()

@@ -135,13 +135,18 @@ def taylor_bar(h=0.4e-3, R=3.2e-3, L=32.4e-3, jitter=0.05, seed=1, v0=227.0, E=1
 
 def bar_metrics(case, coo_cur, eps):
     """End-state measures of a Taylor test: bar length (z extent), mushroom
-    radius (largest radius of the wall layer) and peak equivalent plastic
-    strain."""
+    radius (largest radius of the wall layer), peak equivalent plastic
+    strain (the largest nodal value) and two aggregate measures of the same
+    field that one node's history cannot move: its 99.9th percentile over the
+    nodes and its mean over the wall layer."""
     x = np.asarray(coo_cur).reshape(-1, 3)
     w = case["wall"]
+    e = np.asarray(eps)
     return dict(length=float(x[:, 2].max() - x[:, 2].min()),
                 radius=float(np.sqrt(x[w, 0] ** 2 + x[w, 1] ** 2).max()),
-                peak_eps=float(np.max(eps)))
+                peak_eps=float(np.max(e)),
+                eps_p999=float(np.percentile(e, 99.9)),
+                eps_wall_mean=float(np.mean(e[w])))
 
 
 def batch_bars(nbars=256, seed=5, h_range=(0.15e-3, 0.6e-3), v0_range=(100.0, 300.0), sy_range=(200e6, 600e6),

@@ -30,7 +30,8 @@ def test_streamed_variants_are_bit_identical(bar16k, mode, pair):
     b, sb = _run(bar16k, mode, pair[1])
     for f in FIELDS:
         np.testing.assert_array_equal(a[f], b[f])
-    assert sa["kin_energy"] == sb["kin_energy"]
+    # the energy is a sum of per-block atomics, whose order the scheduler picks
+    assert abs(sa["kin_energy"] - sb["kin_energy"]) <= 1e-13 * abs(sa["kin_energy"])
 
 
 def test_repeat_run_is_bit_identical(bar16k):
