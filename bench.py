@@ -163,6 +163,11 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def rel_err(x, ref):
+    """|x - ref| / |ref| per measure (the absolute difference where ref is 0)."""
+    return {k: abs(x[k] - ref[k]) / abs(ref[k]) if ref[k] != 0 else abs(x[k] - ref[k]) for k in ref}
+
+
 def cpu_model():
     """The host CPU's model name (from /proc/cpuinfo), for the CPU baselines."""
     try:
@@ -342,7 +347,7 @@ def accuracy(case, p, dt, steps):
     q.step(steps, dt, mode="mixed")
     mix = cases.bar_metrics(case, q.download(_lib.F_COO_CURRENT), q.download(_lib.F_EPS))
     q.close()
-    rel = {k: abs(mix[k] - ref[k]) / abs(ref[k]) for k in ref}
+    rel = rel_err(mix, ref)
     return dict(steps=steps, fp64=ref, mixed=mix, mixed_rel_err=rel,
                 force_rel_l2_one_step=float(np.linalg.norm(f32 - f64) / np.linalg.norm(f64)))
 
@@ -382,7 +387,7 @@ def nsni_run(case, dt, args):
         m.close()
     if "end_state" in out.get("fp64", {}) and "end_state" in out.get("mixed", {}):
         ref, mix = out["fp64"]["end_state"], out["mixed"]["end_state"]
-        out["mixed_rel_err"] = {k: abs(mix[k] - ref[k]) / abs(ref[k]) for k in ref}
+        out["mixed_rel_err"] = rel_err(mix, ref)
         cp = dict(case)
         cp["vinit"] = np.asarray(case["vinit"]) * (1.0 + 1.0e-12)
         q = mega.Mega(cp, p)
@@ -390,7 +395,7 @@ def nsni_run(case, dt, args):
         q.step(args.nsni_steps, dt, mode="fp64", allow_status=True)
         pert = cases.bar_metrics(case, q.download(_lib.F_COO_CURRENT), q.download(_lib.F_EPS))
         q.close()
-        out["fp64_perturbed_1e-12_rel_change"] = {k: abs(pert[k] - ref[k]) / abs(ref[k]) for k in ref}
+        out["fp64_perturbed_1e-12_rel_change"] = rel_err(pert, ref)
     # direct nodal integration over the same steps, for its status
     d = mega.Mega(case, _lib.params(**cases.param_kwargs(case)))
     d.search_and_shapes()
@@ -486,7 +491,7 @@ def learned_runs(args, rank):
     ref = runs["fp64"]["end_state"]
     for name in ("mixed", "mixed_textbook_newton", "mixed_learned"):
         e = runs[name]["end_state"]
-        runs[name]["rel_err_vs_fp64"] = {k: abs(e[k] - ref[k]) / abs(ref[k]) for k in ref}
+        runs[name]["rel_err_vs_fp64"] = rel_err(e, ref)
     return dict(workload=f"rate-dependent taylor_bar h={args.rate_h*1e3:.3g}mm", nodes=n, dt=dt, steps=total,
                 timed_steps=rest, rate_law=dict(A=RATE_LAW[0], B=RATE_LAW[1], n=RATE_LAW[2], C=RATE_LAW[3],
                                                 epsdot0=RATE_LAW[4]), newton_rtol=1e-10, runs=runs,

@@ -439,7 +439,7 @@ __device__ __forceinline__ void step_sums(const TiledForceArgs& a, double ke, do
 template <typename TS, typename A, bool F64, int KG, int KU>
 __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
   extern __shared__ double smx[];
-  __shared__ double red[8 * 8];
+  __shared__ double red[16 * 8];  // eight sums per warp, up to 16 warps (KG = 8)
   const int64_t t = blockIdx.x;
   const int cnt = a.jcnt[t];
   const int nv = a.has_body ? 12 : 9;
@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(64 * KG) k_force_b(TiledForceArgs a) {
   constexpr int RB = F64 ? 32 : 16;
   extern __shared__ __align__(128) unsigned char smb[];
   __shared__ uint64_t bar[kChunks];
-  __shared__ double red[8 * 8];
+  __shared__ double red[16 * 8];  // eight sums per warp, up to 16 warps (KG = 8)
   const int64_t t = blockIdx.x;
   const int64_t c0 = t * a.R, c1 = min((int64_t)a.n, c0 + a.R);
   const int64_t e0 = a.colptr[c0], ne = a.colptr[c1] - e0;

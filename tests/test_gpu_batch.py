@@ -87,8 +87,8 @@ def test_autotune_keeps_state_and_results():
     before = [a.download(f) for f in (_lib.F_DSP_TOT, _lib.F_VEL, _lib.F_STRESS, _lib.F_EPS)]
     for mode in ("fp64", "mixed"):
         choice, times = a.autotune(dt, mode=mode, reps=3)
-        assert all(0 <= c < 4 for c in choice)
-        assert np.all(times > 0)
+        assert all(0 <= c < _lib.TUNE_VARIANTS for c in choice)
+        assert np.all((times > 0) | (times == -1.0))  # -1: a streamed variant the tiles do not fit
     after = [a.download(f) for f in (_lib.F_DSP_TOT, _lib.F_VEL, _lib.F_STRESS, _lib.F_EPS)]
     for x, y in zip(before, after):
         np.testing.assert_array_equal(x, y)
