@@ -432,7 +432,8 @@ struct Ctx {
   int32_t* perm = nullptr;   // new node r = original node perm[r]
   int32_t* iperm = nullptr;  // original node i = new node iperm[i]
   TileSet rt, ct;            // row tiles (deformation gradient), column tiles (force)
-  double *shp = nullptr, *sdphi = nullptr, *sdphi32 = nullptr, *tshp = nullptr;
+  double *shp = nullptr, *sdphi = nullptr, *sdphi32 = nullptr, *tshp = nullptr, *tshp32 = nullptr;
+  double* shp32 = nullptr;   // shp in the order of the float row records (pk32)
   void *pk64 = nullptr, *tpk64 = nullptr, *pk32 = nullptr, *tpk32 = nullptr;
   // state
   double *dsp = nullptr, *dsp_tot = nullptr, *dsp_tot_phy = nullptr, *vel = nullptr, *acl = nullptr;
@@ -578,7 +579,7 @@ static TiledForceArgs force_args(Ctx* c, double dt, int mode, int predict) {
   f.recmax = c->ct.recmax;
   f.jset = c->ct.jset; f.jcnt = c->ct.jcnt; f.colptr = c->csr.colptr;
   f.pk = mixed ? c->tpk32 : c->tpk64;
-  f.tshp = c->tshp; f.tmat = c->tmat; f.has_body = c->has_body; f.predict = predict;
+  f.tshp = mixed ? c->tshp32 : c->tshp; f.tmat = c->tmat; f.has_body = c->has_body; f.predict = predict;
   f.ebc = c->ebc; f.mass = c->mass; f.matidx = c->matidx; f.mats = c->mats; f.body_id = c->body_id;
   f.fint = c->fint; f.fext = c->fext; f.vel = c->vel; f.acl = c->acl; f.dsp = c->dsp; f.dsp_tot = c->dsp_tot;
   f.prforce = c->prforce; f.fadd = c->nsni ? c->fstab : nullptr; f.dt = dt; f.acc = c->acc; f.status = c->status;
@@ -638,7 +639,8 @@ static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) 
   if (c->nsni)
     MEGA_TRY(cudaMemcpyAsync(c->stress_prev, c->stress, sizeof(double) * 6 * c->n, cudaMemcpyDeviceToDevice, c->s));
   int r = launch_defgrad_tiled(c->s, mixed, interp, c->n, c->rt, c->csr.rowptr, mixed ? c->pk32 : c->pk64, c->dsp,
-                               c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc,
+                               c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, mixed ? c->shp32 : c->shp, c->dsp_tot_phy,
+                               c->fg, c->acc,
                                c->status, c->var_defgrad[mixed]);
   if (r) return r;
   if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->nsr32, c->nsc32, mixed, c->dsp, 0)))
@@ -1401,7 +1403,7 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     c->rt = TileSet();
     c->ct = TileSet();
     c->perm = c->iperm = nullptr;
-    c->shp = c->sdphi = c->sdphi32 = c->tshp = nullptr;
+    c->shp = c->sdphi = c->sdphi32 = c->tshp = c->tshp32 = c->shp32 = nullptr;
     c->pk64 = c->tpk64 = c->pk32 = c->tpk32 = nullptr;
     c->searched = false;
     if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
@@ -1594,27 +1596,60 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     k_rowsum3<double><<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, g1x, g1y, g1z, c->sdphi);
     MEGA_CHECK_LAUNCH();
   }
+  // The float column records take their own entry order, chosen for the
+  // force gather's shared-memory banks (bank_order); the double records keep
+  // the column order of the list (ascending rows), the oracle's scatter order.
+  int64_t* tpos32 = nullptr;
   if (c->prec_mask & 2) {
+    uint16_t* lidx32 = nullptr;
+    MEGA_ALLOC(tmp1, lidx32, m);
+    MEGA_ALLOC(tmp1, tpos32, m);
+    MEGA_TRY(cudaMemcpyAsync(lidx32, c->ct.lidx, sizeof(uint16_t) * m, cudaMemcpyDeviceToDevice, c->s));
+    MEGA_TRY(cudaMemcpyAsync(tpos32, c->csr.tpos, sizeof(int64_t) * m, cudaMemcpyDeviceToDevice, c->s));
+    if ((r = bank_order(c->s, n, c->ct, c->csr.colptr, lidx32, tpos32, false))) return r;
     float4* b = nullptr;
     MEGA_ALLOC(c->nbpool, b, m);
     c->tpk32 = b;
     if (packed) {
-      if ((r = pack_transposed32(c->s, m, c->ct.lidx, (const float4*)c->pk32, c->csr.tpos, b))) return r;
+      if ((r = pack_transposed32(c->s, m, lidx32, (const float4*)c->pk32, tpos32, b))) return r;
     } else {
       float4* a = nullptr;
       MEGA_ALLOC(c->nbpool, a, m);
       c->pk32 = a;
       if ((r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, false, c->pk32)) ||
-          (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, false, c->tpk32)))
+          (r = pack_entries(c->s, m, lidx32, g1x, g1y, g1z, tpos32, false, c->tpk32)))
         return r;
     }
     MEGA_ALLOC(c->nbpool, c->sdphi32, 3 * (int64_t)n);
     k_rowsum_pk32<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, (const float4*)c->pk32, c->sdphi32);
     MEGA_CHECK_LAUNCH();
+    // the float row records take their own entry order too, chosen for the
+    // deformation-gradient gather's banks (after every copy made from them in
+    // list order above); shp32 follows them for the per-step interpolation
+    uint16_t* rl = nullptr;
+    int64_t* rpos = nullptr;
+    float4* rec = nullptr;
+    MEGA_ALLOC(tmp1, rl, m);
+    MEGA_ALLOC(tmp1, rpos, m);
+    MEGA_TRY(cudaMemcpyAsync(rl, c->rt.lidx, sizeof(uint16_t) * m, cudaMemcpyDeviceToDevice, c->s));
+    if ((r = iota64(c->s, m, rpos)) || (r = bank_order(c->s, n, c->rt, c->csr.rowptr, rl, rpos, false))) return r;
+    MEGA_ALLOC(c->nbpool, rec, m);
+    if ((r = gather_records32(c->s, m, rpos, (const float4*)c->pk32, rec))) return r;
+    MEGA_ALLOC(c->nbpool, c->shp32, m);
+    k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, rpos, c->shp, c->shp32);
+    MEGA_CHECK_LAUNCH();
+    MEGA_TRY(cudaStreamSynchronize(c->s));
+    c->nbpool.release(c->pk32);
+    c->pk32 = rec;
   }
-  if (c->has_body) {
+  if (c->has_body && (c->prec_mask & 1)) {
     MEGA_ALLOC(c->nbpool, c->tshp, m);
     k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->csr.tpos, c->shp, c->tshp);
+    MEGA_CHECK_LAUNCH();
+  }
+  if (c->has_body && (c->prec_mask & 2)) {
+    MEGA_ALLOC(c->nbpool, c->tshp32, m);
+    k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, tpos32, c->shp, c->tshp32);
     MEGA_CHECK_LAUNCH();
   }
   MEGA_TRY(cudaStreamSynchronize(c->s));

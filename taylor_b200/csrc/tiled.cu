@@ -167,6 +167,68 @@ __global__ void k_pack_f64(int64_t m, const uint16_t* __restrict__ lidx, const d
   out[2 * e + 1] = make_double2(gz[p], __longlong_as_double((long long)lidx[e]));
 }
 
+// Entry order for conflict-free reads of the staged neighbour data.  In the
+// gathers the KG lanes of a row (column) take its entries KG at a time, and
+// the 32 lanes of a warp read the staged values of their current entries in
+// one instruction: lanes whose tile ranks l differ but agree modulo NC (the
+// bank period of the staged layout) are served one after another, lanes with
+// the same l by one broadcast.  This reorders the entries within each row so
+// that, at every step, the lanes of each group of GL lanes hold, per class
+// l mod NC, one rank only wherever the row's remaining entries allow (greedy,
+// lanes in order, each taking its first entry whose class is free or holds
+// the same rank); a row keeps all its entries, only their order changes.
+// pos, when given, is permuted with lidx.  One warp per warp of the gather's
+// blocks, four warps per block.
+template <int KG, int NC, int GL>
+__global__ void __launch_bounds__(128) k_bank_order(int32_t n, int32_t R, int64_t nwarps,
+                                                    const int64_t* __restrict__ ptr, uint16_t* lidx, int64_t* pos) {
+  __shared__ int held_s[4][32];
+  const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (w >= nwarps) return;  // whole warps leave together
+  const int lane = threadIdx.x & 31;
+  int* held = held_s[threadIdx.x >> 5] + (lane / GL) * NC;  // this lane's group: the rank held per class
+  const int wpt = R * KG / 32;  // warps per tile
+  const int64_t c = (w / wpt) * R + (w % wpt) * (32 / KG) + lane / KG;
+  const int q = lane & (KG - 1);
+  int64_t b = 0, e = 0;
+  if (c < n) { b = ptr[c]; e = ptr[c + 1]; }
+  int steps = (int)((e - b + KG - 1) / KG);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) steps = max(steps, __shfl_xor_sync(0xffffffffu, steps, o));
+  for (int s = 0; s < steps; ++s) {
+    const int64_t slot = b + (int64_t)s * KG + q;
+    held_s[threadIdx.x >> 5][lane] = -1;
+    __syncwarp();
+    for (int turn = 0; turn < 32; ++turn) {
+      if (lane == turn && slot < e) {
+        int64_t pick = slot;
+        for (int64_t k = slot; k < e; ++k) {
+          const int l = lidx[k], h = held[l & (NC - 1)];
+          if (h < 0 || h == l) { pick = k; break; }
+        }
+        if (pick != slot) {
+          const uint16_t x = lidx[pick]; lidx[pick] = lidx[slot]; lidx[slot] = x;
+          if (pos) { const int64_t y = pos[pick]; pos[pick] = pos[slot]; pos[slot] = y; }
+        }
+        const int l = lidx[slot];
+        if (held[l & (NC - 1)] < 0) held[l & (NC - 1)] = l;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void k_gather_rec32(int64_t m, const int64_t* __restrict__ pos, const float4* __restrict__ in,
+                               float4* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e < m) out[e] = in[pos[e]];
+}
+
+__global__ void k_iota64(int64_t m, int64_t* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e < m) out[e] = e;
+}
+
 template <bool F64>
 __device__ __forceinline__ void load_entry(const void* pk, int64_t p, float& g0, float& g1, float& g2, int& l);
 template <>
@@ -199,12 +261,13 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
   const int32_t* js = jset + t * (int64_t)jmax;
   // Staged neighbour displacements.  FP64: u_J and du_J as doubles.  Mixed:
   // float offsets from the tile's first node r0 (u_J - u_r0, du_J - du_r0),
-  // half the shared-memory traffic; the differences u_J - u_i are formed
-  // between offsets, exact up to float rounding of the offsets.
+  // half the shared-memory traffic, one array per component (value k of
+  // rank l at sf[k * cnt + l]: lanes with distinct l mod 32 read distinct
+  // banks); the differences u_J - u_i are formed between offsets, exact up
+  // to float rounding of the offsets.
   double* su = sm;
   double* sd = sm + 3 * cnt;
-  float4* sa = reinterpret_cast<float4*>(sm);
-  float2* sb = reinterpret_cast<float2*>(sa + cnt);
+  float* sf = reinterpret_cast<float*>(sm);
   const int64_t r0 = t * R;
   const int64_t i = t * R + threadIdx.x / KG;
   const int q = threadIdx.x & (KG - 1);
@@ -245,8 +308,8 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
       su[3 * l] = a0; su[3 * l + 1] = a1; su[3 * l + 2] = a2;
       sd[3 * l] = b0; sd[3 * l + 1] = b1; sd[3 * l + 2] = b2;
     } else {
-      sa[l] = make_float4((float)(a0 - ur0), (float)(a1 - ur1), (float)(a2 - ur2), (float)(b0 - dr0));
-      sb[l] = make_float2((float)(b1 - dr1), (float)(b2 - dr2));
+      sf[l] = (float)(a0 - ur0); sf[cnt + l] = (float)(a1 - ur1); sf[2 * cnt + l] = (float)(a2 - ur2);
+      sf[3 * cnt + l] = (float)(b0 - dr0); sf[4 * cnt + l] = (float)(b1 - dr1); sf[5 * cnt + l] = (float)(b2 - dr2);
     }
   }
   __syncthreads();
@@ -268,11 +331,11 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
       dj0 = sd[3 * l]; dj1 = sd[3 * l + 1]; dj2 = sd[3 * l + 2];
       d0 = (A)(dj0 - di0); d1 = (A)(dj1 - di1); d2 = (A)(dj2 - di2);
     } else {
-      const float4 va = sa[l];
-      const float2 vb = sb[l];
-      u0 = (A)(va.x - fu0); u1 = (A)(va.y - fu1); u2 = (A)(va.z - fu2);
-      d0 = (A)(va.w - fd0); d1 = (A)(vb.x - fd1); d2 = (A)(vb.y - fd2);
-      if (INTERP) { dj0 = dr0 + (double)va.w; dj1 = dr1 + (double)vb.x; dj2 = dr2 + (double)vb.y; }
+      const float* v = sf + l;
+      const float v3 = v[3 * cnt], v4 = v[4 * cnt], v5 = v[5 * cnt];
+      u0 = (A)(v[0] - fu0); u1 = (A)(v[cnt] - fu1); u2 = (A)(v[2 * cnt] - fu2);
+      d0 = (A)(v3 - fd0); d1 = (A)(v4 - fd1); d2 = (A)(v5 - fd2);
+      if (INTERP) { dj0 = dr0 + (double)v3; dj1 = dr1 + (double)v4; dj2 = dr2 + (double)v5; }
       else { dj0 = dj1 = dj2 = 0.0; }
     }
     F[0] += u0 * g0; F[1] += u0 * g1; F[2] += u0 * g2;
@@ -493,8 +556,8 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
       }
     }
 #pragma unroll
-    for (int k = 0; k < 9; ++k) sT[l * nv + k] = v[k];
-    if (nv == 12) { sT[l * nv + 9] = v[9]; sT[l * nv + 10] = v[10]; sT[l * nv + 11] = v[11]; }
+    for (int k = 0; k < 9; ++k) sT[k * cnt + l] = v[k];
+    if (nv == 12) { sT[9 * cnt + l] = v[9]; sT[10 * cnt + l] = v[10]; sT[11 * cnt + l] = v[11]; }
   }
   __syncthreads();
   if (!F64 && valid) {
@@ -507,13 +570,13 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
     A f0 = A(0), f1 = A(0), f2 = A(0);
     double e0 = 0.0, e1 = 0.0, e2 = 0.0;
     auto body = [&](int64_t e, A g0, A g1, A g2, int l) {
-      const TS* T = sT + l * nv;
-      f0 += (A)T[0] * g0 + (A)T[1] * g1 + (A)T[2] * g2;
-      f1 += (A)T[3] * g0 + (A)T[4] * g1 + (A)T[5] * g2;
-      f2 += (A)T[6] * g0 + (A)T[7] * g1 + (A)T[8] * g2;
+      const TS* T = sT + l;  // component k of T_l at T[k * cnt]
+      f0 += (A)T[0] * g0 + (A)T[cnt] * g1 + (A)T[2 * cnt] * g2;
+      f1 += (A)T[3 * cnt] * g0 + (A)T[4 * cnt] * g1 + (A)T[5 * cnt] * g2;
+      f2 += (A)T[6 * cnt] * g0 + (A)T[7 * cnt] * g1 + (A)T[8 * cnt] * g2;
       if (a.has_body) {
         const double s = a.tshp[e];
-        e0 += s * (double)T[9]; e1 += s * (double)T[10]; e2 += s * (double)T[11];
+        e0 += s * (double)T[9 * cnt]; e1 += s * (double)T[10 * cnt]; e2 += s * (double)T[11 * cnt];
       }
     };
     if (pre) {
@@ -649,8 +712,7 @@ __global__ void __launch_bounds__(64 * KG) k_defgrad_b(int32_t n, int32_t R, int
   unsigned char* stg = smb + (size_t)recmax * RB;
   double* su = reinterpret_cast<double*>(stg);
   double* sd = su + 3 * cnt;
-  float4* sa = reinterpret_cast<float4*>(stg);
-  float2* sb = reinterpret_cast<float2*>(sa + cnt);
+  float* sf = reinterpret_cast<float*>(stg);  // mixed: value k of rank l at sf[k * cnt + l]
   const int64_t i = r0 + threadIdx.x / KG;
   const int q = threadIdx.x & (KG - 1);
   const unsigned gmask = group_mask<KG>();
@@ -668,8 +730,8 @@ __global__ void __launch_bounds__(64 * KG) k_defgrad_b(int32_t n, int32_t R, int
       su[3 * l] = a0; su[3 * l + 1] = a1; su[3 * l + 2] = a2;
       sd[3 * l] = b0; sd[3 * l + 1] = b1; sd[3 * l + 2] = b2;
     } else {
-      sa[l] = make_float4((float)(a0 - ur0), (float)(a1 - ur1), (float)(a2 - ur2), (float)(b0 - dr0));
-      sb[l] = make_float2((float)(b1 - dr1), (float)(b2 - dr2));
+      sf[l] = (float)(a0 - ur0); sf[cnt + l] = (float)(a1 - ur1); sf[2 * cnt + l] = (float)(a2 - ur2);
+      sf[3 * cnt + l] = (float)(b0 - dr0); sf[4 * cnt + l] = (float)(b1 - dr1); sf[5 * cnt + l] = (float)(b2 - dr2);
     }
   }
   __syncthreads();
@@ -708,11 +770,11 @@ __global__ void __launch_bounds__(64 * KG) k_defgrad_b(int32_t n, int32_t R, int
         dj0 = sd[3 * l]; dj1 = sd[3 * l + 1]; dj2 = sd[3 * l + 2];
         d0 = (A)(dj0 - di0); d1 = (A)(dj1 - di1); d2 = (A)(dj2 - di2);
       } else {
-        const float4 va = sa[l];
-        const float2 vb = sb[l];
-        u0 = (A)(va.x - fu0); u1 = (A)(va.y - fu1); u2 = (A)(va.z - fu2);
-        d0 = (A)(va.w - fd0); d1 = (A)(vb.x - fd1); d2 = (A)(vb.y - fd2);
-        if (INTERP) { dj0 = dr0 + (double)va.w; dj1 = dr1 + (double)vb.x; dj2 = dr2 + (double)vb.y; }
+        const float* v = sf + l;
+        const float v3 = v[3 * cnt], v4 = v[4 * cnt], v5 = v[5 * cnt];
+        u0 = (A)(v[0] - fu0); u1 = (A)(v[cnt] - fu1); u2 = (A)(v[2 * cnt] - fu2);
+        d0 = (A)(v3 - fd0); d1 = (A)(v4 - fd1); d2 = (A)(v5 - fd2);
+        if (INTERP) { dj0 = dr0 + (double)v3; dj1 = dr1 + (double)v4; dj2 = dr2 + (double)v5; }
         else { dj0 = dj1 = dj2 = 0.0; }
       }
       F[0] += u0 * g0; F[1] += u0 * g1; F[2] += u0 * g2;
@@ -803,8 +865,8 @@ __global__ void __launch_bounds__(64 * KG) k_force_b(TiledForceArgs a) {
       }
     }
 #pragma unroll
-    for (int k = 0; k < 9; ++k) sT[l * nv + k] = v[k];
-    if (nv == 12) { sT[l * nv + 9] = v[9]; sT[l * nv + 10] = v[10]; sT[l * nv + 11] = v[11]; }
+    for (int k = 0; k < 9; ++k) sT[k * cnt + l] = v[k];
+    if (nv == 12) { sT[9 * cnt + l] = v[9]; sT[10 * cnt + l] = v[10]; sT[11 * cnt + l] = v[11]; }
   }
   __syncthreads();
   double ke = 0.0, ee = 0.0, tf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -828,13 +890,13 @@ __global__ void __launch_bounds__(64 * KG) k_force_b(TiledForceArgs a) {
           const float4 r = rec32[p];
           g0 = (A)r.x; g1 = (A)r.y; g2 = (A)r.z; l = __float_as_int(r.w);
         }
-        const TS* T = sT + l * nv;
-        f0 += (A)T[0] * g0 + (A)T[1] * g1 + (A)T[2] * g2;
-        f1 += (A)T[3] * g0 + (A)T[4] * g1 + (A)T[5] * g2;
-        f2 += (A)T[6] * g0 + (A)T[7] * g1 + (A)T[8] * g2;
+        const TS* T = sT + l;  // component k of T_l at T[k * cnt]
+        f0 += (A)T[0] * g0 + (A)T[cnt] * g1 + (A)T[2 * cnt] * g2;
+        f1 += (A)T[3 * cnt] * g0 + (A)T[4 * cnt] * g1 + (A)T[5 * cnt] * g2;
+        f2 += (A)T[6 * cnt] * g0 + (A)T[7 * cnt] * g1 + (A)T[8 * cnt] * g2;
         if (a.has_body) {
           const double s = a.tshp[e0 + p];
-          b0 += s * (double)T[9]; b1 += s * (double)T[10]; b2 += s * (double)T[11];
+          b0 += s * (double)T[9 * cnt]; b1 += s * (double)T[10 * cnt]; b2 += s * (double)T[11 * cnt];
         }
       }
     }
@@ -934,6 +996,32 @@ int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* 
   if (m <= 0) return 0;
   if (f64) k_pack_f64<<<grid_for(m, 256), 256, 0, s>>>(m, lidx, gx, gy, gz, pos, (double2*)out);
   else k_pack_f32<<<grid_for(m, 256), 256, 0, s>>>(m, lidx, gx, gy, gz, pos, (float4*)out);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int bank_order(cudaStream_t s, int32_t n, const TileSet& ts, const int64_t* ptr, uint16_t* lidx, int64_t* pos,
+               bool f64) {
+  if (n <= 0) return 0;
+  constexpr int KG = 4;  // the lanes per row (column) of the gathers' first variant
+  const int64_t nwarps = ts.ntiles * (int64_t)(ts.R * KG / 32);
+  const unsigned grid = (unsigned)((nwarps * 32 + 127) / 128);
+  if (f64) k_bank_order<KG, 16, 16><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos);  // double words
+  else k_bank_order<KG, 32, 32><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int iota64(cudaStream_t s, int64_t m, int64_t* out) {
+  if (m <= 0) return 0;
+  k_iota64<<<grid_for(m, 256), 256, 0, s>>>(m, out);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int gather_records32(cudaStream_t s, int64_t m, const int64_t* pos, const float4* in, float4* out) {
+  if (m <= 0) return 0;
+  k_gather_rec32<<<grid_for(m, 256), 256, 0, s>>>(m, pos, in, out);
   MEGA_CHECK_LAUNCH();
   return 0;
 }
