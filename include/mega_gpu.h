@@ -366,17 +366,18 @@ int mega_set_instances(int64_t h, int32_t ninst, const int32_t* inst_nodes, cons
 int mega_set_instance_dt(int64_t h, const double* dt_inst);
 /* Autotuner: time each launch variant of the two per-step gathers for the
  * given precision on this context's lists, reps launches each, keep the
- * fastest, and leave the state as it was.  Variants 0..3 hold the packed
- * records in registers (lanes per row x records in flight: (4, 4), (4, 2),
- * (4, 1), (8, 2)); 4 and 5 have the copy engine stream each tile's records
- * into shared memory (4 or 8 lanes per row), where the tiles fit.  choice
+ * fastest, and leave the state as it was.  Variants 0..3, 6 and 7 hold the
+ * packed records in registers (lanes per row x records in flight: (4, 4),
+ * (4, 2), (4, 1), (8, 2), (16, 1), (16, 2)); 4 and 5 have the copy engine
+ * stream each tile's records into shared memory (4 or 8 lanes per row),
+ * where the tiles fit (not with NSNI in mixed precision).  choice
  * (2) receives the deformation-gradient and force variants, times_ms
  * (2 x MEGA_TUNE_VARIANTS, may be NULL) the mean launch times, -1 for a
  * variant that does not fit. */
-#define MEGA_TUNE_VARIANTS 6
+#define MEGA_TUNE_VARIANTS 8
 /* Pin the launch variants of the two gathers for one precision (after
  * mega_search_and_shapes), e.g. to repeat a run bit for bit: variants with
- * the same lanes per row (0, 1, 2, 4 and 3, 5) sum in the same order and
+ * the same lanes per row (0, 1, 2, 4; 3, 5; 6, 7) sum in the same order and
  * give identical results.  MEGA_ERR_UNSUPPORTED when a streamed variant
  * does not fit the context's tiles. */
 int mega_set_variants(int64_t h, int32_t mode, int32_t defgrad_variant, int32_t force_variant);

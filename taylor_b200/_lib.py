@@ -30,7 +30,7 @@ MODE_FP64 = 0
 MODE_MIXED = 1
 FLAG_INTERP_EACH_STEP = 0x100
 FLAG_LEARNED_GUESS = 0x200
-TUNE_VARIANTS = 6  # MEGA_TUNE_VARIANTS: launch variants of each per-step gather
+TUNE_VARIANTS = 8  # MEGA_TUNE_VARIANTS: launch variants of each per-step gather
 
 MAT_ELASTIC, MAT_VONMISES, MAT_DRUCKER_PRAGER, MAT_VM_DAMAGE, MAT_VM_RATE = 1, 2, 3, 6, 7
 

@@ -446,7 +446,10 @@ struct Ctx {
   // stress gradients (18 per node) and per-step scratch
   bool nsni = false;
   NsniS nsr{}, nsc{};
-  NsniSF nsr32{}, nsc32{};  // float copies for the mixed steps
+  // mixed NSNI: S as six floats per record in the float row / column record
+  // orders, and its row sums (the tiled gathers carry the NSNI terms)
+  float *ns_srow = nullptr, *ns_scol = nullptr;
+  double* ns_ssum = nullptr;
   // semi-Lagrangian (LLAGRANGIAN = .FALSE.): lists and shapes rebuilt on the
   // current coordinates every step, in the caller's numbering, FP64
   bool semi = false;
@@ -582,7 +585,10 @@ static TiledForceArgs force_args(Ctx* c, double dt, int mode, int predict) {
   f.tshp = mixed ? c->tshp32 : c->tshp; f.tmat = c->tmat; f.has_body = c->has_body; f.predict = predict;
   f.ebc = c->ebc; f.mass = c->mass; f.matidx = c->matidx; f.mats = c->mats; f.body_id = c->body_id;
   f.fint = c->fint; f.fext = c->fext; f.vel = c->vel; f.acl = c->acl; f.dsp = c->dsp; f.dsp_tot = c->dsp_tot;
-  f.prforce = c->prforce; f.fadd = c->nsni ? c->fstab : nullptr; f.dt = dt; f.acc = c->acc; f.status = c->status;
+  f.prforce = c->prforce; f.fadd = (c->nsni && !mixed) ? c->fstab : nullptr; f.dt = dt; f.acc = c->acc;
+  f.status = c->status;
+  f.ns_scol = (c->nsni && mixed) ? c->ns_scol : nullptr;
+  f.ns_w = (c->nsni && mixed) ? (const float*)c->nsw : nullptr;
   f.vel2 = c->vel2;
   f.ndt = c->ndt;
   return f;
@@ -618,6 +624,15 @@ static int sync_time(Ctx* c) {
   return 0;
 }
 
+// the NSNI terms of the mixed tiled row gather (null: none)
+static const NsniTiles* nsni_tiles(Ctx* c, bool mixed, NsniTiles& buf) {
+  if (!c->nsni || !mixed) return nullptr;
+  buf.srow = c->ns_srow;
+  buf.ssum = c->ns_ssum;
+  buf.hq = c->hq;
+  return &buf;
+}
+
 static NsniStepArgs nsni_args(Ctx* c) {
   NsniStepArgs a{};
   a.n = c->n; a.fg = c->fg; a.stress_old = c->stress_prev; a.stress_new = c->stress; a.sml = c->sm_len;
@@ -627,9 +642,12 @@ static NsniStepArgs nsni_args(Ctx* c) {
   return a;
 }
 
-// kernels one step launches (the learned start splits the stress kernel in two)
+// kernels one step launches (the learned start splits the stress kernel in
+// two; NSNI adds the stress-gradient kernel, and in FP64 its two gathers)
 static int kernels_per_step(const Ctx* c, int mode = 0) {
-  return (c->nsni ? 6 : 3) + (c->has_ebc2 ? 1 : 0) + (((mode & MEGA_FLAG_LEARNED_GUESS) && c->mlp_on) ? 1 : 0);
+  const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
+  return (c->nsni ? (mixed ? 4 : 6) : 3) + (c->has_ebc2 ? 1 : 0) +
+         (((mode & MEGA_FLAG_LEARNED_GUESS) && c->mlp_on) ? 1 : 0);
 }
 
 static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) {
@@ -638,18 +656,18 @@ static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) 
   if (ev) MEGA_TRY(cudaEventRecord(ev[0], c->s));
   if (c->nsni)
     MEGA_TRY(cudaMemcpyAsync(c->stress_prev, c->stress, sizeof(double) * 6 * c->n, cudaMemcpyDeviceToDevice, c->s));
-  int r = launch_defgrad_tiled(c->s, mixed, interp, c->n, c->rt, c->csr.rowptr, mixed ? c->pk32 : c->pk64, c->dsp,
-                               c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, mixed ? c->shp32 : c->shp, c->dsp_tot_phy,
-                               c->fg, c->acc,
-                               c->status, c->var_defgrad[mixed]);
+  NsniTiles nt;
+  int r = launch_defgrad_tiled(c->s, mixed, interp, c->n, c->rt, nsni_tiles(c, mixed, nt), c->csr.rowptr,
+                               mixed ? c->pk32 : c->pk64, c->dsp, c->dsp_tot, mixed ? c->sdphi32 : c->sdphi,
+                               mixed ? c->shp32 : c->shp, c->dsp_tot_phy, c->fg, c->acc, c->status,
+                               c->var_defgrad[mixed]);
   if (r) return r;
-  if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->nsr32, c->nsc32, mixed, c->dsp, 0)))
-    return r;
+  if (c->nsni && !mixed && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, false, c->dsp, 0))) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[1], c->s));
   r = launch_stress(c->s, mixed, stress_args(c, dt, mode));
   if (r) return r;
-  if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, c->nsr32, c->nsc32, mixed, c->dsp, 1)))
-    return r;
+  if (c->nsni && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, mixed, c->dsp, 1))) return r;
+  if (c->nsni && !mixed && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, false, c->dsp, 2))) return r;
   if ((r = launch_fixity2(c, dt))) return r;
   if (ev) MEGA_TRY(cudaEventRecord(ev[2], c->s));
   r = launch_force_tiled(c->s, mixed, force_args(c, dt, mode, predict), c->var_force[mixed]);
@@ -1405,6 +1423,8 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     c->perm = c->iperm = nullptr;
     c->shp = c->sdphi = c->sdphi32 = c->tshp = c->tshp32 = c->shp32 = nullptr;
     c->pk64 = c->tpk64 = c->pk32 = c->tpk32 = nullptr;
+    c->ns_srow = c->ns_scol = nullptr;
+    c->ns_ssum = nullptr;
     c->searched = false;
     if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
   }
@@ -1565,13 +1585,6 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     for (int k = 0; k < 6; ++k)
       k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->csr.tpos, c->nsr.v[k], c->nsc.v[k]);
     MEGA_CHECK_LAUNCH();
-    if (c->prec_mask & 2) {
-      for (int k = 0; k < 6; ++k) {
-        MEGA_ALLOC(c->nbpool, c->nsr32.v[k], m);
-        MEGA_ALLOC(c->nbpool, c->nsc32.v[k], m);
-      }
-      if ((r = nsni_to_float(c->s, m, c->nsr, c->nsr32)) || (r = nsni_to_float(c->s, m, c->nsc, c->nsc32))) return r;
-    }
   }
   tr.mark("transpose");
   if (!packed) {
@@ -1638,6 +1651,15 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     MEGA_ALLOC(c->nbpool, c->shp32, m);
     k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, rpos, c->shp, c->shp32);
     MEGA_CHECK_LAUNCH();
+    if (c->nsni) {  // S in both float record orders, and its row sums
+      MEGA_ALLOC(c->nbpool, c->ns_srow, 6 * m);
+      MEGA_ALLOC(c->nbpool, c->ns_scol, 6 * m);
+      MEGA_ALLOC(c->nbpool, c->ns_ssum, 6 * (int64_t)n);
+      if ((r = nsni_records(c->s, m, rpos, c->nsr, c->ns_srow)) ||
+          (r = nsni_records(c->s, m, tpos32, c->nsr, c->ns_scol)) ||
+          (r = nsni_rowsum(c->s, n, c->csr.rowptr, c->nsr, c->ns_ssum)))
+        return r;
+    }
     MEGA_TRY(cudaStreamSynchronize(c->s));
     c->nbpool.release(c->pk32);
     c->pk32 = rec;
@@ -1993,10 +2015,12 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
   int r = 0;
   const StressArgs sa = stress_args(c, dt, mode & 0xff);
   for (int v = 0; v < nvar && !r; ++v) {
+    NsniTiles nt;
+    const NsniTiles* ns = nsni_tiles(c, mixed, nt);
     const auto def = [&]() {
-      return launch_defgrad_tiled(c->s, mixed, false, c->n, c->rt, c->csr.rowptr, mixed ? c->pk32 : c->pk64, c->dsp,
-                                  c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg, c->acc,
-                                  c->status, v);
+      return launch_defgrad_tiled(c->s, mixed, false, c->n, c->rt, ns, c->csr.rowptr, mixed ? c->pk32 : c->pk64,
+                                  c->dsp, c->dsp_tot, mixed ? c->sdphi32 : c->sdphi, c->shp, c->dsp_tot_phy, c->fg,
+                                  c->acc, c->status, v);
     };
     r = def();  // warm-up (twice: the first launch of a variant may also load its code)
     if (r == MEGA_ERR_UNSUPPORTED) {  // a streamed variant whose tiles do not fit shared memory
@@ -2129,6 +2153,8 @@ int mega_set_variants(int64_t h, int32_t mode, int32_t defgrad_variant, int32_t 
     return MEGA_ERR_ARG;
   if (!tiled_variant_fits(c->rt, mixed, defgrad_variant, false, c->has_body) ||
       !tiled_variant_fits(c->ct, mixed, force_variant, true, c->has_body))
+    return MEGA_ERR_UNSUPPORTED;
+  if (c->nsni && mixed && (defgrad_variant >= 4 || force_variant >= 4))  // the NSNI terms: register variants
     return MEGA_ERR_UNSUPPORTED;
   MEGA_TRY(cudaStreamSynchronize(c->s));
   drop_graph(c);
@@ -2573,7 +2599,6 @@ static int construct_fint_impl(const mega_params* p, const FintIO& io) {
   // NSNI: second derivatives (computed at LINIT, read otherwise) in CSR and
   // CSC order, stress gradients, per-call scratch
   NsniS nsr{}, nsc{};
-  NsniSF none{};
   double *sgrad = nullptr, *hq = nullptr, *nsw = nullptr, *fstab = nullptr, *sprev = nullptr;
   if (nsni) {
     for (int k = 0; k < 6; ++k) { MEGA_ALLOC(pool, nsr.v[k], m); MEGA_ALLOC(pool, nsc.v[k], m); }
@@ -2634,11 +2659,13 @@ static int construct_fint_impl(const mega_params* p, const FintIO& io) {
     na.n = n; na.fg = dfg; na.stress_old = sprev; na.stress_new = dsig; na.sml = dsml; na.vol = dv; na.matidx = midx;
     na.mats = dmat; na.hq = hq; na.sgrad = sgrad; na.w = nsw; na.fstab = fstab; na.finite_strain = p->finite_strain;
     na.inv3_exact = p->inv3_exact; na.acc = acc; na.status = st;
-    if ((r = nsni_step(s, na, csr, nsr, nsc, none, none, false, ddsp, 0))) return r;
+    if ((r = nsni_step(s, na, csr, nsr, nsc, false, ddsp, 0))) return r;
   }
   r = launch_stress(s, false, a);
   if (r) return r;
-  if (nsni && (r = nsni_step(s, na, csr, nsr, nsc, none, none, false, ddsp, 1))) return r;
+  if (nsni && ((r = nsni_step(s, na, csr, nsr, nsc, false, ddsp, 1)) || (r = nsni_step(s, na, csr, nsr, nsc, false,
+                                                                                       ddsp, 2))))
+    return r;
   DevCSR* dcsr;
   MEGA_ALLOC(pool, dcsr, 1);
   if ((r = upload(s, dcsr, &csr, 1))) return r;

@@ -302,11 +302,16 @@ struct NsniStepArgs {
 int nsni_combine(cudaStream_t s, int32_t n, int axis, const int64_t* rowptr, const double* sml, const double* gp[3],
                  const double* gm[3], const NsniS& out);
 // stage 0: the row gather of H (after the displacement increment is known);
-// stage 1: stress gradients, weights and the column gather of the force.
-// mixed: float second derivatives (rows32 / cols32) and float weights.
+// stage 1: stress gradients and weights (mixed: float weights);
+// stage 2: the column gather of the stabilisation force.
+// Stages 0 and 2 are the FP64 steps' own kernels: the mixed steps form H and
+// the stabilisation force in the tiled gathers (NsniTiles).
 int nsni_step(cudaStream_t s, const NsniStepArgs& a, const DevCSR& csr, const NsniS& rows, const NsniS& cols,
-              const NsniSF& rows32, const NsniSF& cols32, bool mixed, const double* du, int stage);
-int nsni_to_float(cudaStream_t s, int64_t m, const NsniS& src, const NsniSF& dst);
+              bool mixed, const double* du, int stage);
+// dst[6 e + q] = float S_q at list position pos[e]
+int nsni_records(cudaStream_t s, int64_t m, const int64_t* pos, const NsniS& src, float* dst);
+// dst[6 i + q] = sum over row i of the float-rounded S_q, in double
+int nsni_rowsum(cudaStream_t s, int32_t n, const int64_t* rowptr, const NsniS& src, double* dst);
 
 // surrogate network of the rate-dependent return mapping (mlp.cu)
 int mlp_nparams();

@@ -13,7 +13,8 @@
 //            mixed mode)
 //            k_nsni_h      (row gather) the gradients of the incremental
 //            displacement gradient, H_a(k,m) = sum_J S_(m a)(J) du_J,k
-//            (XLMAT/YLMAT/ZLMAT, FINT.F90:728-737);
+//            (XLMAT/YLMAT/ZLMAT, FINT.F90:728-737); the mixed steps form H
+//            in the tiled row gather instead (tiled.cu, NS);
 //            k_nsni_stress (node) the strain-gradient increments of
 //            D_HUGHES_WINGET (HUGHES_WINGET.F90:84-165), stress gradients
 //            sigma_,a rotated with the step's rotation and advanced with an
@@ -24,7 +25,7 @@
 //            M_a / V = (cell width_a)^2 / 12 (PRE_MODEL_SECOND_MOMENT.F90);
 //            k_nsni_force  (column gather) f_J += sum_a W_a S_(. a)(J)
 //            (FINT.F90:1127-1208), added by the force kernel before the
-//            corrector.
+//            corrector; the mixed steps sum it in the tiled column gather.
 #include "mega_internal.cuh"
 
 namespace mega {
@@ -342,11 +343,32 @@ __global__ void __launch_bounds__(256) k_nsni_force(int32_t n, const int64_t* __
   }
 }
 
-__global__ void k_nsni_narrow(int64_t m, NsniS src, NsniSF dst) {
+// dst[6 e + q] = float S_q at list position pos[e] (the record order of the
+// tiled gathers)
+__global__ void k_nsni_records(int64_t m, const int64_t* __restrict__ pos, NsniS src, float* __restrict__ dst) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= m) return;
+  const int64_t p = pos[e];
+  float v[6];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) dst.v[c][e] = (float)src.v[c][e];
+  for (int c = 0; c < 6; ++c) v[c] = (float)src.v[c][p];
+  float2* o = reinterpret_cast<float2*>(dst + 6 * e);
+  o[0] = make_float2(v[0], v[1]);
+  o[1] = make_float2(v[2], v[3]);
+  o[2] = make_float2(v[4], v[5]);
+}
+
+// dst[6 i + q] = sum over row i of the float-rounded S_q, in double (so that
+// the split sum of the tiled row gather is exact in exact arithmetic)
+__global__ void k_nsni_rowsum(int32_t n, const int64_t* __restrict__ rowptr, NsniS src, double* __restrict__ dst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double t[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int64_t p = rowptr[i]; p < rowptr[i + 1]; ++p)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) t[c] += (double)(float)src.v[c][p];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) dst[6 * i + c] = t[c];
 }
 
 }  // namespace
@@ -360,27 +382,32 @@ int nsni_combine(cudaStream_t s, int32_t n, int axis, const int64_t* rowptr, con
 }
 
 int nsni_step(cudaStream_t s, const NsniStepArgs& a, const DevCSR& csr, const NsniS& rows, const NsniS& cols,
-              const NsniSF& rows32, const NsniSF& cols32, bool mixed, const double* du, int stage) {
+              bool mixed, const double* du, int stage) {
   const unsigned gg = (unsigned)(((int64_t)a.n * kNL + 255) / 256);
   const unsigned gn = (unsigned)((a.n + 127) / 128);
+  if (mixed && stage != 1) return MEGA_ERR_UNSUPPORTED;  // the tiled gathers carry those terms
   if (stage == 0) {
-    if (mixed) k_nsni_h<float><<<gg, 256, 0, s>>>(a.n, csr.rowptr, csr.col, rows32, du, a.hq);
-    else k_nsni_h<double><<<gg, 256, 0, s>>>(a.n, csr.rowptr, csr.col, rows, du, a.hq);
-  } else if (mixed) {
-    k_nsni_stress<float><<<gn, 128, 0, s>>>(a);
-    MEGA_CHECK_LAUNCH();
-    k_nsni_force<float><<<gg, 256, 0, s>>>(a.n, csr.colptr, csr.trow, cols32, (const float*)a.w, a.fstab);
+    k_nsni_h<double><<<gg, 256, 0, s>>>(a.n, csr.rowptr, csr.col, rows, du, a.hq);
+  } else if (stage == 1) {
+    if (mixed) k_nsni_stress<float><<<gn, 128, 0, s>>>(a);
+    else k_nsni_stress<double><<<gn, 128, 0, s>>>(a);
   } else {
-    k_nsni_stress<double><<<gn, 128, 0, s>>>(a);
-    MEGA_CHECK_LAUNCH();
     k_nsni_force<double><<<gg, 256, 0, s>>>(a.n, csr.colptr, csr.trow, cols, (const double*)a.w, a.fstab);
   }
   MEGA_CHECK_LAUNCH();
   return 0;
 }
 
-int nsni_to_float(cudaStream_t s, int64_t m, const NsniS& src, const NsniSF& dst) {
-  k_nsni_narrow<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(m, src, dst);
+int nsni_records(cudaStream_t s, int64_t m, const int64_t* pos, const NsniS& src, float* dst) {
+  if (m <= 0) return 0;
+  k_nsni_records<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(m, pos, src, dst);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int nsni_rowsum(cudaStream_t s, int32_t n, const int64_t* rowptr, const NsniS& src, double* dst) {
+  if (n <= 0) return 0;
+  k_nsni_rowsum<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, rowptr, src, dst);
   MEGA_CHECK_LAUNCH();
   return 0;
 }

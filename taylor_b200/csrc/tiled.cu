@@ -21,8 +21,8 @@ namespace mega {
 namespace {
 
 // Launch variants of the two gathers (picked per context by the autotuner):
-// KG lanes per row / column (4 or 8), KU packed records in flight per lane
-// (2 or 4).  A block serves one tile of R rows with R * KG threads.
+// KG lanes per row / column (4, 8 or 16), KU packed records in flight per
+// lane (1, 2 or 4).  A block serves one tile of R rows with R * KG threads.
 template <int KG>
 __device__ __forceinline__ unsigned group_mask() {
   return ((1u << KG) - 1u) << (threadIdx.x & (32 - KG));
@@ -243,8 +243,21 @@ __device__ __forceinline__ void load_entry64(const void* pk, int64_t p, double& 
   g0 = a.x; g1 = a.y; g2 = b.x; l = (int)__double_as_longlong(b.y);
 }
 
-template <typename A, bool F64, bool INTERP, int KG, int KU>
-__global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int32_t n, int32_t R, int32_t jmax,
+// The six float S values of one NSNI record (three 8-byte loads).
+struct SRec {
+  float2 a, b, c;
+};
+__device__ __forceinline__ SRec load_srec(const float* base, int64_t p) {
+  const float2* sp = reinterpret_cast<const float2*>(base) + 3 * p;
+  return SRec{__ldg(sp), __ldg(sp + 1), __ldg(sp + 2)};
+}
+
+// NS: the NSNI gradients of the incremental displacement gradient ride
+// along, H_i(k, q) = sum_J S_q(i, J) du_J,k, formed like L as
+// sum_J S_q (du_J - du_i) + du_i,k sum_J S_q (FINT.F90:728-737 layout).
+template <typename A, bool F64, bool INTERP, int KG, int KU, bool NS = false>
+__global__ void __launch_bounds__(64 * KG, (F64 ? 12 : (NS ? 8 : 16)) / KG > 0 ? (F64 ? 12 : (NS ? 8 : 16)) / KG : 1) k_defgrad_t(int32_t n, int32_t R, int32_t jmax,
+                                                   NsniTiles ns,
                                                    const int64_t* __restrict__ rowptr, const void* __restrict__ pk,
                                                    const int32_t* __restrict__ jset, const int32_t* __restrict__ jcnt,
                                                    const double* __restrict__ dsp, const double* __restrict__ dsp_tot,
@@ -279,6 +292,7 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
   bool pre = false;
   float4 pf[KU];
   double2 pfa[KU], pfb[KU];
+  SRec psr[NS ? KU : 1];
   if (valid) {
     p = rowptr[i] + q;
     pend = rowptr[i + 1];
@@ -292,6 +306,7 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
         } else {
           pf[u] = __ldg((const float4*)pk + p + u * KG);
         }
+        if constexpr (NS) psr[u] = load_srec(ns.srow, p + u * KG);
       }
     }
   }
@@ -318,12 +333,15 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
   const double di0 = dsp[3 * i], di1 = dsp[3 * i + 1], di2 = dsp[3 * i + 2];
   const float fu0 = (float)(ui0 - ur0), fu1 = (float)(ui1 - ur1), fu2 = (float)(ui2 - ur2);
   const float fd0 = (float)(di0 - dr0), fd1 = (float)(di1 - dr1), fd2 = (float)(di2 - dr2);
-  A F[9], L[9];
+  A F[9], L[9], H[NS ? 18 : 1];
 #pragma unroll
   for (int k = 0; k < 9; ++k) { F[k] = A(0); L[k] = A(0); }
+#pragma unroll
+  for (int k = 0; k < (NS ? 18 : 1); ++k) H[k] = A(0);
   double ph0 = 0.0, ph1 = 0.0, ph2 = 0.0;
-  // One entry: F += (u_J - u_i) (x) g, L += (d_J - d_i) (x) g (+ phi d_J).
-  auto body = [&](int64_t p, A g0, A g1, A g2, int l) {
+  // One entry: F += (u_J - u_i) (x) g, L += (d_J - d_i) (x) g (+ phi d_J),
+  // H(k, q) += S_q (d_J - d_i)_k.
+  auto body = [&](int64_t p, A g0, A g1, A g2, int l, const SRec& sr) {
     A u0, u1, u2, d0, d1, d2;
     double dj0, dj1, dj2;  // du_J itself, for the per-step interpolation
     if (F64) {
@@ -344,6 +362,11 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
     L[0] += d0 * g0; L[1] += d0 * g1; L[2] += d0 * g2;
     L[3] += d1 * g0; L[4] += d1 * g1; L[5] += d1 * g2;
     L[6] += d2 * g0; L[7] += d2 * g1; L[8] += d2 * g2;
+    if constexpr (NS) {
+      const A sq[6] = {(A)sr.a.x, (A)sr.a.y, (A)sr.b.x, (A)sr.b.y, (A)sr.c.x, (A)sr.c.y};
+#pragma unroll
+      for (int c = 0; c < 6; ++c) { H[c] += sq[c] * d0; H[6 + c] += sq[c] * d1; H[12 + c] += sq[c] * d2; }
+    }
     if (INTERP) {
       const double s = shp[p];
       ph0 += s * dj0; ph1 += s * dj1; ph2 += s * dj2;
@@ -351,13 +374,14 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
   };
   // KU records in flight per lane before any is used (the loop is bound by
   // DRAM latency otherwise); each lane still sums its entries in list order.
+  const SRec s0{};
   if (pre) {
 #pragma unroll
     for (int u = 0; u < KU; ++u) {
       if (F64)
-        body(p + u * KG, (A)pfa[u].x, (A)pfa[u].y, (A)pfb[u].x, (int)__double_as_longlong(pfb[u].y));
+        body(p + u * KG, (A)pfa[u].x, (A)pfa[u].y, (A)pfb[u].x, (int)__double_as_longlong(pfb[u].y), s0);
       else
-        body(p + u * KG, (A)pf[u].x, (A)pf[u].y, (A)pf[u].z, __float_as_int(pf[u].w));
+        body(p + u * KG, (A)pf[u].x, (A)pf[u].y, (A)pf[u].z, __float_as_int(pf[u].w), NS ? psr[NS ? u : 0] : s0);
     }
     p += KU * KG;
   }
@@ -371,15 +395,20 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
       }
 #pragma unroll
       for (int u = 0; u < KU; ++u)
-        body(p + u * KG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y));
+        body(p + u * KG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y), s0);
     }
   } else {
     for (; p + (KU - 1) * KG < pend; p += KU * KG) {
       float4 r[KU];
+      SRec sr[NS ? KU : 1];
 #pragma unroll
-      for (int u = 0; u < KU; ++u) r[u] = __ldg((const float4*)pk + p + u * KG);
+      for (int u = 0; u < KU; ++u) {
+        r[u] = __ldg((const float4*)pk + p + u * KG);
+        if constexpr (NS) sr[u] = load_srec(ns.srow, p + u * KG);
+      }
 #pragma unroll
-      for (int u = 0; u < KU; ++u) body(p + u * KG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w));
+      for (int u = 0; u < KU; ++u)
+        body(p + u * KG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w), NS ? sr[NS ? u : 0] : s0);
     }
   }
   for (; p < pend; p += KG) {
@@ -387,12 +416,12 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
       double a0, a1, a2;
       int l;
       load_entry64(pk, p, a0, a1, a2, l);
-      body(p, (A)a0, (A)a1, (A)a2, l);
+      body(p, (A)a0, (A)a1, (A)a2, l, s0);
     } else {
       float a0, a1, a2;
       int l;
       load_entry<false>(pk, p, a0, a1, a2, l);
-      body(p, (A)a0, (A)a1, (A)a2, l);
+      body(p, (A)a0, (A)a1, (A)a2, l, NS ? load_srec(ns.srow, p) : s0);
     }
   }
 #pragma unroll
@@ -402,6 +431,10 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
       F[k] += __shfl_xor_sync(gmask, F[k], o);
       L[k] += __shfl_xor_sync(gmask, L[k], o);
     }
+    if constexpr (NS) {
+#pragma unroll
+      for (int k = 0; k < 18; ++k) H[k] += __shfl_xor_sync(gmask, H[k], o);
+    }
     if (INTERP) {
       ph0 += __shfl_xor_sync(gmask, ph0, o);
       ph1 += __shfl_xor_sync(gmask, ph1, o);
@@ -410,6 +443,15 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : 16) / KG) k_defgrad_t(int
   }
   if (q == 0) {
     const double ui[3] = {ui0, ui1, ui2}, di[3] = {di0, di1, di2};
+    if constexpr (NS) {
+      double ss[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) ss[c] = ns.ssum[6 * i + c];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) ns.hq[18 * i + 6 * k + c] = (double)H[6 * k + c] + di[k] * ss[c];
+    }
     const double sd3[3] = {sdphi[3 * i], sdphi[3 * i + 1], sdphi[3 * i + 2]};
     double h[18];
 #pragma unroll
@@ -499,10 +541,13 @@ __device__ __forceinline__ void step_sums(const TiledForceArgs& a, double ke, do
 }
 
 // TS = storage of T_i (float / double), A = accumulation, F64 = record width
-template <typename TS, typename A, bool F64, int KG, int KU>
+// NS (mixed): the NSNI stabilisation force rides along,
+// f_J += sum_i sum_q W_i(k, q) S_q(i, J) (FINT.F90:1127-1208 layout), with the
+// row weights W_i staged beside T_i.
+template <typename TS, typename A, bool F64, int KG, int KU, bool NS = false>
 __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
   extern __shared__ double smx[];
-  __shared__ double red[16 * 8];  // eight sums per warp, up to 16 warps (KG = 8)
+  __shared__ double red[32 * 8];  // eight sums per warp, up to 32 warps (KG = 16)
   const int64_t t = blockIdx.x;
   const int cnt = a.jcnt[t];
   const int nv = a.has_body ? 12 : 9;
@@ -558,6 +603,16 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) sT[k * cnt + l] = v[k];
     if (nv == 12) { sT[9 * cnt + l] = v[9]; sT[10 * cnt + l] = v[10]; sT[11 * cnt + l] = v[11]; }
+    if constexpr (NS) {  // W_l: 18 of its 20 floats, as five 16-byte loads
+      const float4* w4 = reinterpret_cast<const float4*>(a.ns_w + 20 * (int64_t)js[l]);
+      TS* sW = sT + nv * cnt;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const float4 x = __ldg(w4 + k);
+        sW[(4 * k) * cnt + l] = x.x; sW[(4 * k + 1) * cnt + l] = x.y;
+        if (4 * k + 2 < 18) { sW[(4 * k + 2) * cnt + l] = x.z; sW[(4 * k + 3) * cnt + l] = x.w; }
+      }
+    }
   }
   __syncthreads();
   if (!F64 && valid) {
@@ -569,23 +624,34 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
   if (valid) {
     A f0 = A(0), f1 = A(0), f2 = A(0);
     double e0 = 0.0, e1 = 0.0, e2 = 0.0;
-    auto body = [&](int64_t e, A g0, A g1, A g2, int l) {
+    auto body = [&](int64_t e, A g0, A g1, A g2, int l, const SRec& sr) {
       const TS* T = sT + l;  // component k of T_l at T[k * cnt]
       f0 += (A)T[0] * g0 + (A)T[cnt] * g1 + (A)T[2 * cnt] * g2;
       f1 += (A)T[3 * cnt] * g0 + (A)T[4 * cnt] * g1 + (A)T[5 * cnt] * g2;
       f2 += (A)T[6 * cnt] * g0 + (A)T[7 * cnt] * g1 + (A)T[8 * cnt] * g2;
+      if constexpr (NS) {
+        const A sq[6] = {(A)sr.a.x, (A)sr.a.y, (A)sr.b.x, (A)sr.b.y, (A)sr.c.x, (A)sr.c.y};
+        const TS* W = T + nv * cnt;  // W_l(k, q) at W[(6 k + q) * cnt]
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          f0 += (A)W[c * cnt] * sq[c];
+          f1 += (A)W[(6 + c) * cnt] * sq[c];
+          f2 += (A)W[(12 + c) * cnt] * sq[c];
+        }
+      }
       if (a.has_body) {
         const double s = a.tshp[e];
         e0 += s * (double)T[9 * cnt]; e1 += s * (double)T[10 * cnt]; e2 += s * (double)T[11 * cnt];
       }
     };
-    if (pre) {
+    const SRec s0{};
+    if (pre) {  // (FP64 only)
 #pragma unroll
       for (int u = 0; u < KU; ++u) {
         if (F64)
-          body(e + u * KG, (A)pfa[u].x, (A)pfa[u].y, (A)pfb[u].x, (int)__double_as_longlong(pfb[u].y));
+          body(e + u * KG, (A)pfa[u].x, (A)pfa[u].y, (A)pfb[u].x, (int)__double_as_longlong(pfb[u].y), s0);
         else
-          body(e + u * KG, (A)pf[u].x, (A)pf[u].y, (A)pf[u].z, __float_as_int(pf[u].w));
+          body(e + u * KG, (A)pf[u].x, (A)pf[u].y, (A)pf[u].z, __float_as_int(pf[u].w), s0);
       }
       e += KU * KG;
     }
@@ -599,15 +665,20 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
         }
 #pragma unroll
         for (int u = 0; u < KU; ++u)
-          body(e + u * KG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y));
+          body(e + u * KG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y), s0);
       }
     } else {
       for (; e + (KU - 1) * KG < c1; e += KU * KG) {
         float4 r[KU];
+        SRec sr[NS ? KU : 1];
 #pragma unroll
-        for (int u = 0; u < KU; ++u) r[u] = __ldg((const float4*)a.pk + e + u * KG);
+        for (int u = 0; u < KU; ++u) {
+          r[u] = __ldg((const float4*)a.pk + e + u * KG);
+          if constexpr (NS) sr[u] = load_srec(a.ns_scol, e + u * KG);
+        }
 #pragma unroll
-        for (int u = 0; u < KU; ++u) body(e + u * KG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w));
+        for (int u = 0; u < KU; ++u)
+          body(e + u * KG, (A)r[u].x, (A)r[u].y, (A)r[u].z, __float_as_int(r[u].w), NS ? sr[NS ? u : 0] : s0);
       }
     }
     for (; e < c1; e += KG) {
@@ -615,12 +686,12 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
         double b0, b1, b2;
         int l;
         load_entry64(a.pk, e, b0, b1, b2, l);
-        body(e, (A)b0, (A)b1, (A)b2, l);
+        body(e, (A)b0, (A)b1, (A)b2, l, s0);
       } else {
         float b0, b1, b2;
         int l;
         load_entry<false>(a.pk, e, b0, b1, b2, l);
-        body(e, (A)b0, (A)b1, (A)b2, l);
+        body(e, (A)b0, (A)b1, (A)b2, l, NS ? load_srec(a.ns_scol, e) : s0);
       }
     }
 #pragma unroll
@@ -832,7 +903,7 @@ __global__ void __launch_bounds__(64 * KG) k_force_b(TiledForceArgs a) {
   constexpr int RB = F64 ? 32 : 16;
   extern __shared__ __align__(128) unsigned char smb[];
   __shared__ uint64_t bar[kChunks];
-  __shared__ double red[16 * 8];  // eight sums per warp, up to 16 warps (KG = 8)
+  __shared__ double red[32 * 8];  // eight sums per warp, up to 32 warps (KG = 16)
   const int64_t t = blockIdx.x;
   const int64_t c0 = t * a.R, c1 = min((int64_t)a.n, c0 + a.R);
   const int64_t e0 = a.colptr[c0], ne = a.colptr[c1] - e0;
@@ -1028,7 +1099,9 @@ int gather_records32(cudaStream_t s, int64_t m, const int64_t* pos, const float4
 
 // The launch variants, in the order the autotuner tries them:
 // (KG, KU) = (4, 4), (4, 2), (4, 1), (8, 2) with register-held record
-// streams, then KG = 4, 8 with the records streamed into shared memory.
+// streams, then KG = 4, 8 with the records streamed into shared memory, then
+// (16, 1), (16, 2) with register-held streams (four times the threads per
+// staged neighbour of KG = 4: the NSNI force gather stages 27 values a node).
 constexpr int kVariants = kTiledVariants;
 // dynamic shared memory a streamed-variant block may ask for: sm_100's 227 KB
 // per block less room for the kernels' static shared memory (under 1 KB)
@@ -1045,9 +1118,12 @@ static int configure_variant(int lim) {
   int r = 0;
   if ((r = raise_smem(k_defgrad_t<float, false, true, KG, KU>, lim))) return r;
   if ((r = raise_smem(k_defgrad_t<float, false, false, KG, KU>, lim))) return r;
+  if ((r = raise_smem(k_defgrad_t<float, false, true, KG, KU, true>, lim))) return r;
+  if ((r = raise_smem(k_defgrad_t<float, false, false, KG, KU, true>, lim))) return r;
   if ((r = raise_smem(k_defgrad_t<double, true, true, KG, KU>, lim))) return r;
   if ((r = raise_smem(k_defgrad_t<double, true, false, KG, KU>, lim))) return r;
   if ((r = raise_smem(k_force_t<float, float, false, KG, KU>, lim))) return r;
+  if ((r = raise_smem(k_force_t<float, float, false, KG, KU, true>, lim))) return r;
   return raise_smem(k_force_t<double, double, true, KG, KU>, lim);
 }
 
@@ -1079,15 +1155,16 @@ static int configure_bulk(int lim) {
 
 // Raise the dynamic shared-memory limit of the tiled kernels once (outside
 // any stream capture): a tile stages at most 1024 neighbours, 96 KB for the
-// double-precision T_i of the force kernel; the streamed variants add the
-// tile's records.
+// double-precision T_i of the force kernel (120 KB for the float T_i and
+// NSNI weights); the streamed variants add the tile's records.
 int configure_tiled_kernels() {
   static bool done = false;
   if (done) return 0;
-  const int lim = 12 * 8 * 1024 + 1024;
+  const int lim = 30 * 4 * 1024 + 1024;
   int r = 0;
   if ((r = configure_variant<4, 4>(lim)) || (r = configure_variant<4, 2>(lim)) ||
       (r = configure_variant<4, 1>(lim)) || (r = configure_variant<8, 2>(lim)) ||
+      (r = configure_variant<16, 1>(lim)) || (r = configure_variant<16, 2>(lim)) ||
       (r = configure_bulk<4>(kBulkSmemMax)) || (r = configure_bulk<8>(kBulkSmemMax)))
     return r;
   done = true;
@@ -1098,7 +1175,7 @@ int tiled_variants() { return kVariants; }
 
 bool tiled_variant_fits(const TileSet& ts, bool mixed, int variant, bool force, bool has_body) {
   if (variant < 0 || variant >= kVariants) return false;
-  if (variant < 4) return true;
+  if (variant < 4 || variant > 5) return true;  // register variants
   const size_t stage = force ? (mixed ? sizeof(float) : sizeof(double)) * (has_body ? 12 : 9) : (mixed ? 24 : 48);
   return (size_t)ts.recmax * (mixed ? 16 : 32) + stage * (size_t)ts.maxcnt <= (size_t)g_bulk_lim;
 }
@@ -1126,28 +1203,31 @@ static int defgrad_bulk(cudaStream_t s, bool mixed, bool interp, int32_t n, cons
 
 template <int KG, int KU>
 static void defgrad_variant(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
-                            const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
-                            const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg,
-                            StepAccum* acc) {
+                            const NsniTiles* ns, const int64_t* rowptr, const void* pk, const double* dsp,
+                            const double* dsp_tot, const double* sdphi, const double* shp, double* dsp_tot_phy,
+                            double* fg, StepAccum* acc) {
   const size_t smem = (mixed ? 24 : 48) * (size_t)ts.maxcnt;
   const unsigned grid = (unsigned)ts.ntiles;
   const int block = ts.R * KG;
+  const NsniTiles nz = ns ? *ns : NsniTiles();
   if (mixed) {
-    auto k = interp ? k_defgrad_t<float, false, true, KG, KU> : k_defgrad_t<float, false, false, KG, KU>;
-    k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
+    auto k = ns ? (interp ? k_defgrad_t<float, false, true, KG, KU, true> : k_defgrad_t<float, false, false, KG, KU, true>)
+                : (interp ? k_defgrad_t<float, false, true, KG, KU> : k_defgrad_t<float, false, false, KG, KU>);
+    k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, nz, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
                                 dsp_tot_phy, fg, acc);
   } else {
     auto k = interp ? k_defgrad_t<double, true, true, KG, KU> : k_defgrad_t<double, true, false, KG, KU>;
-    k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
+    k<<<grid, block, smem, s>>>(n, ts.R, ts.jmax, nz, rowptr, pk, ts.jset, ts.jcnt, dsp, dsp_tot, sdphi, shp,
                                 dsp_tot_phy, fg, acc);
   }
 }
 
 int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
-                         const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
-                         const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc,
-                         unsigned* status, int variant) {
+                         const NsniTiles* ns, const int64_t* rowptr, const void* pk, const double* dsp,
+                         const double* dsp_tot, const double* sdphi, const double* shp, double* dsp_tot_phy,
+                         double* fg, StepAccum* acc, unsigned* status, int variant) {
   int r = 0;
+  if (ns && (!mixed || variant == 4 || variant == 5)) return MEGA_ERR_UNSUPPORTED;  // NSNI: register variants
   switch (variant) {
     case 4: r = defgrad_bulk<4>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc,
                                 status);
@@ -1155,13 +1235,19 @@ int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, con
     case 5: r = defgrad_bulk<8>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc,
                                 status);
       break;
-    case 1: defgrad_variant<4, 2>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
+    case 1: defgrad_variant<4, 2>(s, mixed, interp, n, ts, ns, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
       break;
-    case 2: defgrad_variant<4, 1>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
+    case 2: defgrad_variant<4, 1>(s, mixed, interp, n, ts, ns, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
       break;
-    case 3: defgrad_variant<8, 2>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
+    case 3: defgrad_variant<8, 2>(s, mixed, interp, n, ts, ns, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg, acc);
       break;
-    default: defgrad_variant<4, 4>(s, mixed, interp, n, ts, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg,
+    case 6: defgrad_variant<16, 1>(s, mixed, interp, n, ts, ns, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg,
+                                   acc);
+      break;
+    case 7: defgrad_variant<16, 2>(s, mixed, interp, n, ts, ns, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg,
+                                   acc);
+      break;
+    default: defgrad_variant<4, 4>(s, mixed, interp, n, ts, ns, rowptr, pk, dsp, dsp_tot, sdphi, shp, dsp_tot_phy, fg,
                                    acc);
   }
   if (r) return r;
@@ -1184,20 +1270,24 @@ static int force_bulk(cudaStream_t s, bool mixed, const TiledForceArgs& a) {
 
 template <int KG, int KU>
 static void force_variant(cudaStream_t s, bool mixed, const TiledForceArgs& a) {
-  const int nv = a.has_body ? 12 : 9;
+  const int nv = (a.has_body ? 12 : 9) + (a.ns_scol ? 18 : 0);
   const size_t smem = (mixed ? sizeof(float) : sizeof(double)) * nv * (size_t)a.maxcnt;
   const unsigned grid = (unsigned)a.ntiles;
   const int block = a.R * KG;
-  if (mixed) k_force_t<float, float, false, KG, KU><<<grid, block, smem, s>>>(a);
+  if (mixed && a.ns_scol) k_force_t<float, float, false, KG, KU, true><<<grid, block, smem, s>>>(a);
+  else if (mixed) k_force_t<float, float, false, KG, KU><<<grid, block, smem, s>>>(a);
   else k_force_t<double, double, true, KG, KU><<<grid, block, smem, s>>>(a);
 }
 
 int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a, int variant) {
   int r = 0;
+  if (a.ns_scol && (!mixed || variant == 4 || variant == 5)) return MEGA_ERR_UNSUPPORTED;  // NSNI: register variants
   switch (variant) {
     case 1: force_variant<4, 2>(s, mixed, a); break;
     case 2: force_variant<4, 1>(s, mixed, a); break;
     case 3: force_variant<8, 2>(s, mixed, a); break;
+    case 6: force_variant<16, 1>(s, mixed, a); break;
+    case 7: force_variant<16, 2>(s, mixed, a); break;
     case 4: r = force_bulk<4>(s, mixed, a); break;
     case 5: r = force_bulk<8>(s, mixed, a); break;
     default: force_variant<4, 4>(s, mixed, a);

@@ -16,6 +16,17 @@ struct TileSet {
   uint16_t* lidx = nullptr;  // per entry: rank of its neighbour in the tile's set
 };
 
+// NSNI terms carried by the mixed-precision tiled gathers: the smoothed
+// second derivatives S_q (XX, YY, ZZ, XY, YZ, XZ) of every list entry as six
+// floats in the order of the float row records (srow) and of the float
+// column records (scol), their row sums, and the per-node H output (row
+// gather) and force weights (column gather)
+struct NsniTiles {
+  const float* srow = nullptr;   // 6 per row record
+  const double* ssum = nullptr;  // 6 per node: sum_J S_q(i, J) in double
+  double* hq = nullptr;          // 18 per node out: sum_J S_q(i, J) du_J,k at [18 i + 6 k + q]
+};
+
 struct TiledForceArgs {
   int32_t n;
   int32_t R;
@@ -44,6 +55,8 @@ struct TiledForceArgs {
   double* dsp_tot;
   double* prforce;
   const double* fadd;     // 3 per node added to the internal force (NSNI), or null
+  const float* ns_scol;   // NSNI (mixed): 6 S values per column record, or null
+  const float* ns_w;      // NSNI (mixed): force weights, 20 floats per node (18 used)
   const double* vel2;     // prescribed velocities of fixity code 2 for this step (3), or null
   const double* ndt;      // per-node step of independent instances, or null (dt for all)
   double dt;
@@ -73,15 +86,18 @@ int iota64(cudaStream_t s, int64_t m, int64_t* out);
 int gather_records32(cudaStream_t s, int64_t m, const int64_t* pos, const float4* in, float4* out);
 int configure_tiled_kernels();
 // launch variants of the two gathers: lanes per row x records in flight
-// (register streams, variants 0-3), and lanes per row with the tile's
-// records streamed into shared memory by the copy engine (variants 4, 5)
-constexpr int kTiledVariants = 6;
+// (register streams, variants 0-3 and 6, 7), and lanes per row with the
+// tile's records streamed into shared memory by the copy engine (variants
+// 4, 5)
+constexpr int kTiledVariants = 8;
 int tiled_variants();
 // whether a variant's shared memory fits the row (defgrad) or column (force) tiles
 bool tiled_variant_fits(const TileSet& ts, bool mixed, int variant, bool force, bool has_body);
 // MEGA_ERR_UNSUPPORTED when the variant's shared memory does not fit the tiles
+// ns (mixed only, register variants 0-3): the NSNI H gather rides along
 int launch_defgrad_tiled(cudaStream_t s, bool mixed, bool interp, int32_t n, const TileSet& ts,
-                         const int64_t* rowptr, const void* pk, const double* dsp, const double* dsp_tot,
+                         const NsniTiles* ns, const int64_t* rowptr, const void* pk, const double* dsp,
+                         const double* dsp_tot,
                          const double* sdphi, const double* shp, double* dsp_tot_phy, double* fg, StepAccum* acc,
                          unsigned* status, int variant = 0);
 int launch_force_tiled(cudaStream_t s, bool mixed, const TiledForceArgs& a, int variant = 0);

@@ -1,7 +1,8 @@
 """The gathers' launch variants: the copy-engine streamed ones (4, 5) sum
 every row and column in the same order as the register-streamed ones with
-the same lanes per row (0 and 3), so a resident run gives bit-identical
-results in both precisions; a pinned choice repeats a run bit for bit."""
+the same lanes per row (0 and 3), and the two 16-lane ones (6, 7) agree with
+each other, so a resident run gives bit-identical results in both
+precisions; a pinned choice repeats a run bit for bit."""
 import numpy as np
 import pytest
 
@@ -24,7 +25,7 @@ def _run(case, mode, variants, steps=40):
 
 
 @pytest.mark.parametrize("mode", ["mixed", "fp64"])
-@pytest.mark.parametrize("pair", [((0, 0), (4, 4)), ((3, 3), (5, 5)), ((0, 4), (4, 0))])
+@pytest.mark.parametrize("pair", [((0, 0), (4, 4)), ((3, 3), (5, 5)), ((0, 4), (4, 0)), ((6, 6), (7, 7))])
 def test_streamed_variants_are_bit_identical(bar16k, mode, pair):
     a, sa = _run(bar16k, mode, pair[0])
     b, sb = _run(bar16k, mode, pair[1])
@@ -47,5 +48,5 @@ def test_set_variants_arguments(bar16k):
         m.set_variants(0, 0)          # before the search
     m.search_and_shapes()
     with pytest.raises(_lib.MegaError):
-        m.set_variants(6, 0)          # no such variant
+        m.set_variants(8, 0)          # no such variant
     m.close()
