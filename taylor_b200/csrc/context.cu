@@ -1619,7 +1619,10 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     MEGA_ALLOC(tmp1, tpos32, m);
     MEGA_TRY(cudaMemcpyAsync(lidx32, c->ct.lidx, sizeof(uint16_t) * m, cudaMemcpyDeviceToDevice, c->s));
     MEGA_TRY(cudaMemcpyAsync(tpos32, c->csr.tpos, sizeof(int64_t) * m, cudaMemcpyDeviceToDevice, c->s));
-    if ((r = bank_order(c->s, n, c->ct, c->csr.colptr, lidx32, tpos32, false))) return r;
+    // (for the lanes per column of the variant the force gather takes: 8 with
+    // the NSNI terms, whose 27 staged values a node favour more threads per
+    // staged node, else 4)
+    if ((r = bank_order(c->s, n, c->ct, c->csr.colptr, lidx32, tpos32, c->nsni ? 8 : 4))) return r;
     float4* b = nullptr;
     MEGA_ALLOC(c->nbpool, b, m);
     c->tpk32 = b;
@@ -1645,7 +1648,7 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     MEGA_ALLOC(tmp1, rl, m);
     MEGA_ALLOC(tmp1, rpos, m);
     MEGA_TRY(cudaMemcpyAsync(rl, c->rt.lidx, sizeof(uint16_t) * m, cudaMemcpyDeviceToDevice, c->s));
-    if ((r = iota64(c->s, m, rpos)) || (r = bank_order(c->s, n, c->rt, c->csr.rowptr, rl, rpos, false))) return r;
+    if ((r = iota64(c->s, m, rpos)) || (r = bank_order(c->s, n, c->rt, c->csr.rowptr, rl, rpos, 4))) return r;
     MEGA_ALLOC(c->nbpool, rec, m);
     if ((r = gather_records32(c->s, m, rpos, (const float4*)c->pk32, rec))) return r;
     MEGA_ALLOC(c->nbpool, c->shp32, m);

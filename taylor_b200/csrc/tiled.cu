@@ -1072,13 +1072,13 @@ int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* 
 }
 
 int bank_order(cudaStream_t s, int32_t n, const TileSet& ts, const int64_t* ptr, uint16_t* lidx, int64_t* pos,
-               bool f64) {
+               int lanes) {
   if (n <= 0) return 0;
-  constexpr int KG = 4;  // the lanes per row (column) of the gathers' first variant
-  const int64_t nwarps = ts.ntiles * (int64_t)(ts.R * KG / 32);
+  if ((lanes != 4 && lanes != 8) || ts.R * lanes < 32) return MEGA_ERR_UNSUPPORTED;
+  const int64_t nwarps = ts.ntiles * (int64_t)(ts.R * lanes / 32);
   const unsigned grid = (unsigned)((nwarps * 32 + 127) / 128);
-  if (f64) k_bank_order<KG, 16, 16><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos);  // double words
-  else k_bank_order<KG, 32, 32><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos);
+  if (lanes == 4) k_bank_order<4, 32, 32><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos);
+  else k_bank_order<8, 32, 32><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos);
   MEGA_CHECK_LAUNCH();
   return 0;
 }

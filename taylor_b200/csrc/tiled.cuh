@@ -76,11 +76,12 @@ int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* 
 int pack_transposed32(cudaStream_t s, int64_t m, const uint16_t* lidx, const float4* in, const int64_t* pos,
                       float4* out);
 // Reorder the entries within each row (column) of the tiles ts so that the
-// lanes of a warp of the gathers read distinct shared-memory banks of the
-// staged neighbour data where possible (f64: double-word layout); pos, when
-// not null, is permuted with lidx.
+// lanes of a warp of a gather with `lanes` (4 or 8) lanes per row read
+// distinct shared-memory banks of the staged neighbour data (one 32-bit
+// word per rank and value) where possible; pos, when not null, is permuted
+// with lidx.
 int bank_order(cudaStream_t s, int32_t n, const TileSet& ts, const int64_t* ptr, uint16_t* lidx, int64_t* pos,
-               bool f64);
+               int lanes);
 // out[e] = e;  out[e] = in[pos[e]]
 int iota64(cudaStream_t s, int64_t m, int64_t* out);
 int gather_records32(cudaStream_t s, int64_t m, const int64_t* pos, const float4* in, float4* out);
