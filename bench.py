@@ -368,6 +368,7 @@ def nsni_run(case, dt, args):
         m = mega.Mega(case, p)
         res = m.search_and_shapes()
         setup_s = time.perf_counter() - t0
+        m.autotune(dt, mode=mode, reps=3)
         m.step(args.warmup, dt, mode=mode)
         clk = Clocks()
         clk.start()

@@ -1688,6 +1688,9 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   c->csr.tpos = nullptr;
   tmp1.free_all();
   tr.mark("pack_and_release");
+  // the mixed NSNI force gather stages 27 values a node: its measured best is
+  // 8 lanes per column (variant 3); mega_autotune may pick another
+  if (c->nsni) c->var_force[1] = 3;
   c->searched = true;
   if (nnz) *nnz = m;
   if (gmaxn) *gmaxn = c->csr.gmaxn;
