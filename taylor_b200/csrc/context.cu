@@ -433,7 +433,8 @@ struct Ctx {
   int32_t* iperm = nullptr;  // original node i = new node iperm[i]
   TileSet rt, ct;            // row tiles (deformation gradient), column tiles (force)
   double *shp = nullptr, *sdphi = nullptr, *sdphi32 = nullptr, *tshp = nullptr, *tshp32 = nullptr;
-  double* shp32 = nullptr;   // shp in the order of the float row records (pk32)
+  double* shp32 = nullptr;   // shp in the order of the float row records once reordered (else shp)
+  bool banked = false;       // the float records reordered for the gathers' banks (bank_layout)
   void *pk64 = nullptr, *tpk64 = nullptr, *pk32 = nullptr, *tpk32 = nullptr;
   // state
   double *dsp = nullptr, *dsp_tot = nullptr, *dsp_tot_phy = nullptr, *vel = nullptr, *acl = nullptr;
@@ -659,7 +660,7 @@ static int step_once(Ctx* c, double dt, int mode, int predict, cudaEvent_t* ev) 
   NsniTiles nt;
   int r = launch_defgrad_tiled(c->s, mixed, interp, c->n, c->rt, nsni_tiles(c, mixed, nt), c->csr.rowptr,
                                mixed ? c->pk32 : c->pk64, c->dsp, c->dsp_tot, mixed ? c->sdphi32 : c->sdphi,
-                               mixed ? c->shp32 : c->shp, c->dsp_tot_phy, c->fg, c->acc, c->status,
+                               (mixed && c->shp32) ? c->shp32 : c->shp, c->dsp_tot_phy, c->fg, c->acc, c->status,
                                c->var_defgrad[mixed]);
   if (r) return r;
   if (c->nsni && !mixed && (r = nsni_step(c->s, nsni_args(c), c->csr, c->nsr, c->nsc, false, c->dsp, 0))) return r;
@@ -1425,6 +1426,7 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     c->pk64 = c->tpk64 = c->pk32 = c->tpk32 = nullptr;
     c->ns_srow = c->ns_scol = nullptr;
     c->ns_ssum = nullptr;
+    c->banked = false;
     c->searched = false;
     if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
   }
@@ -1609,63 +1611,35 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
     k_rowsum3<double><<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, g1x, g1y, g1z, c->sdphi);
     MEGA_CHECK_LAUNCH();
   }
-  // The float column records take their own entry order, chosen for the
-  // force gather's shared-memory banks (bank_order); the double records keep
-  // the column order of the list (ascending rows), the oracle's scatter order.
-  int64_t* tpos32 = nullptr;
+  // The float records are packed in list order here (rows in CSR order,
+  // columns ascending rows); mega_autotune in mixed precision reorders them
+  // once for the gathers' shared-memory banks (bank_layout).
   if (c->prec_mask & 2) {
-    uint16_t* lidx32 = nullptr;
-    MEGA_ALLOC(tmp1, lidx32, m);
-    MEGA_ALLOC(tmp1, tpos32, m);
-    MEGA_TRY(cudaMemcpyAsync(lidx32, c->ct.lidx, sizeof(uint16_t) * m, cudaMemcpyDeviceToDevice, c->s));
-    MEGA_TRY(cudaMemcpyAsync(tpos32, c->csr.tpos, sizeof(int64_t) * m, cudaMemcpyDeviceToDevice, c->s));
-    // (for the lanes per column of the variant the force gather takes: 8 with
-    // the NSNI terms, whose 27 staged values a node favour more threads per
-    // staged node, else 4)
-    if ((r = bank_order(c->s, n, c->ct, c->csr.colptr, lidx32, tpos32, c->nsni ? 8 : 4))) return r;
     float4* b = nullptr;
     MEGA_ALLOC(c->nbpool, b, m);
     c->tpk32 = b;
     if (packed) {
-      if ((r = pack_transposed32(c->s, m, lidx32, (const float4*)c->pk32, tpos32, b))) return r;
+      if ((r = pack_transposed32(c->s, m, c->ct.lidx, (const float4*)c->pk32, c->csr.tpos, b))) return r;
     } else {
       float4* a = nullptr;
       MEGA_ALLOC(c->nbpool, a, m);
       c->pk32 = a;
       if ((r = pack_entries(c->s, m, c->rt.lidx, g1x, g1y, g1z, nullptr, false, c->pk32)) ||
-          (r = pack_entries(c->s, m, lidx32, g1x, g1y, g1z, tpos32, false, c->tpk32)))
+          (r = pack_entries(c->s, m, c->ct.lidx, g1x, g1y, g1z, c->csr.tpos, false, c->tpk32)))
         return r;
     }
     MEGA_ALLOC(c->nbpool, c->sdphi32, 3 * (int64_t)n);
     k_rowsum_pk32<<<grid_for(n, 256), 256, 0, c->s>>>(n, c->csr.rowptr, (const float4*)c->pk32, c->sdphi32);
     MEGA_CHECK_LAUNCH();
-    // the float row records take their own entry order too, chosen for the
-    // deformation-gradient gather's banks (after every copy made from them in
-    // list order above); shp32 follows them for the per-step interpolation
-    uint16_t* rl = nullptr;
-    int64_t* rpos = nullptr;
-    float4* rec = nullptr;
-    MEGA_ALLOC(tmp1, rl, m);
-    MEGA_ALLOC(tmp1, rpos, m);
-    MEGA_TRY(cudaMemcpyAsync(rl, c->rt.lidx, sizeof(uint16_t) * m, cudaMemcpyDeviceToDevice, c->s));
-    if ((r = iota64(c->s, m, rpos)) || (r = bank_order(c->s, n, c->rt, c->csr.rowptr, rl, rpos, 4))) return r;
-    MEGA_ALLOC(c->nbpool, rec, m);
-    if ((r = gather_records32(c->s, m, rpos, (const float4*)c->pk32, rec))) return r;
-    MEGA_ALLOC(c->nbpool, c->shp32, m);
-    k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, rpos, c->shp, c->shp32);
-    MEGA_CHECK_LAUNCH();
     if (c->nsni) {  // S in both float record orders, and its row sums
       MEGA_ALLOC(c->nbpool, c->ns_srow, 6 * m);
       MEGA_ALLOC(c->nbpool, c->ns_scol, 6 * m);
       MEGA_ALLOC(c->nbpool, c->ns_ssum, 6 * (int64_t)n);
-      if ((r = nsni_records(c->s, m, rpos, c->nsr, c->ns_srow)) ||
-          (r = nsni_records(c->s, m, tpos32, c->nsr, c->ns_scol)) ||
+      if ((r = nsni_records(c->s, m, nullptr, c->nsr, c->ns_srow)) ||
+          (r = nsni_records(c->s, m, c->csr.tpos, c->nsr, c->ns_scol)) ||
           (r = nsni_rowsum(c->s, n, c->csr.rowptr, c->nsr, c->ns_ssum)))
         return r;
     }
-    MEGA_TRY(cudaStreamSynchronize(c->s));
-    c->nbpool.release(c->pk32);
-    c->pk32 = rec;
   }
   if (c->has_body && (c->prec_mask & 1)) {
     MEGA_ALLOC(c->nbpool, c->tshp, m);
@@ -1674,7 +1648,7 @@ int mega_search_and_shapes(int64_t h, int32_t* gn, int32_t* gstart, int32_t* gst
   }
   if (c->has_body && (c->prec_mask & 2)) {
     MEGA_ALLOC(c->nbpool, c->tshp32, m);
-    k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, tpos32, c->shp, c->tshp32);
+    k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, c->csr.tpos, c->shp, c->tshp32);
     MEGA_CHECK_LAUNCH();
   }
   MEGA_TRY(cudaStreamSynchronize(c->s));
@@ -1985,6 +1959,70 @@ int64_t mega_kernel_launches(int64_t h) {
 // Autotuner: time every launch variant of the two gathers on this context's
 // own lists (reps launches each, CUDA events), keep the fastest, and put the
 // state back as it was (the force kernel integrates when it runs).
+// One-time reordering of a context's float records (at its first mixed
+// autotune): the entries of each row and column take the order in which a
+// warp's lanes read distinct shared-memory banks of the staged data
+// (bank_order), and what travels with the records follows them (the
+// interpolation and body-force shape values, the NSNI S values).  About 6 ms
+// per gather on a 1 M-node bar; it pays back over a few hundred steps.
+static void drop_graph(Ctx* c);
+
+static int bank_layout(Ctx* c) {
+  if (c->banked || !(c->prec_mask & 2) || !c->pk32 || !c->tpk32) return 0;
+  const int64_t m = c->csr.nnz;
+  const int32_t n = c->n;
+  DevPool tmp(c->s);
+  uint16_t* l = nullptr;
+  int64_t* pos = nullptr;
+  MEGA_ALLOC(tmp, l, m);
+  MEGA_ALLOC(tmp, pos, m);
+  int r = 0;
+  // columns (the lanes per column of the force variant the context favours)
+  if ((r = record_ranks(c->s, m, (const float4*)c->tpk32, l)) || (r = iota64(c->s, m, pos)) ||
+      (r = bank_order(c->s, n, c->ct, c->csr.colptr, l, nullptr, pos, c->nsni ? 8 : 4)))
+    return r;
+  float4* tp = nullptr;
+  MEGA_ALLOC(c->nbpool, tp, m);
+  if ((r = gather_records32(c->s, m, pos, (const float4*)c->tpk32, tp))) return r;
+  double* ts = nullptr;
+  if (c->tshp32) {
+    MEGA_ALLOC(c->nbpool, ts, m);
+    k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, pos, c->tshp32, ts);
+    MEGA_CHECK_LAUNCH();
+  }
+  float* sc = nullptr;
+  if (c->ns_scol) {
+    MEGA_ALLOC(c->nbpool, sc, 6 * m);
+    if ((r = gather_f6(c->s, m, pos, c->ns_scol, sc))) return r;
+  }
+  // rows
+  if ((r = record_ranks(c->s, m, (const float4*)c->pk32, l)) || (r = iota64(c->s, m, pos)) ||
+      (r = bank_order(c->s, n, c->rt, c->csr.rowptr, l, nullptr, pos, 4)))
+    return r;
+  float4* rp = nullptr;
+  double* sh = nullptr;
+  MEGA_ALLOC(c->nbpool, rp, m);
+  MEGA_ALLOC(c->nbpool, sh, m);
+  if ((r = gather_records32(c->s, m, pos, (const float4*)c->pk32, rp))) return r;
+  k_gather_pos<<<grid_for(m, 256), 256, 0, c->s>>>(m, pos, c->shp, sh);
+  MEGA_CHECK_LAUNCH();
+  float* sr = nullptr;
+  if (c->ns_srow) {
+    MEGA_ALLOC(c->nbpool, sr, 6 * m);
+    if ((r = gather_f6(c->s, m, pos, c->ns_srow, sr))) return r;
+  }
+  MEGA_TRY(cudaStreamSynchronize(c->s));
+  drop_graph(c);  // captured steps hold the old arrays
+  c->nbpool.release(c->tpk32); c->tpk32 = tp;
+  if (ts) { c->nbpool.release(c->tshp32); c->tshp32 = ts; }
+  if (sc) { c->nbpool.release(c->ns_scol); c->ns_scol = sc; }
+  c->nbpool.release(c->pk32); c->pk32 = rp;
+  c->shp32 = sh;
+  if (sr) { c->nbpool.release(c->ns_srow); c->ns_srow = sr; }
+  c->banked = true;
+  return 0;
+}
+
 int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* choice, float* times_ms) {
   Ctx* c = get_ctx(h);
   if (!c) return MEGA_ERR_HANDLE;
@@ -1993,6 +2031,7 @@ int mega_autotune(int64_t h, double dt, int32_t mode, int32_t reps, int32_t* cho
   if (reps <= 0) return MEGA_ERR_ARG;
   const bool mixed = (mode & 0xff) == MEGA_MODE_MIXED;
   { int r = mixed ? ensure_mixed(c) : ensure_fp64(c); if (r) return r; }
+  if (mixed) { int r = bank_layout(c); if (r) return r; }
   const int nvar = tiled_variants();
   const size_t n = (size_t)c->n, n3 = 3 * n;
   // snapshot of everything a step writes

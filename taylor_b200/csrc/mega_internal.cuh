@@ -308,7 +308,7 @@ int nsni_combine(cudaStream_t s, int32_t n, int axis, const int64_t* rowptr, con
 // the stabilisation force in the tiled gathers (NsniTiles).
 int nsni_step(cudaStream_t s, const NsniStepArgs& a, const DevCSR& csr, const NsniS& rows, const NsniS& cols,
               bool mixed, const double* du, int stage);
-// dst[6 e + q] = float S_q at list position pos[e]
+// dst[6 e + q] = float S_q at list position pos[e] (e when pos is null)
 int nsni_records(cudaStream_t s, int64_t m, const int64_t* pos, const NsniS& src, float* dst);
 // dst[6 i + q] = sum over row i of the float-rounded S_q, in double
 int nsni_rowsum(cudaStream_t s, int32_t n, const int64_t* rowptr, const NsniS& src, double* dst);

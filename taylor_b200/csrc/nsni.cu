@@ -344,11 +344,11 @@ __global__ void __launch_bounds__(256) k_nsni_force(int32_t n, const int64_t* __
 }
 
 // dst[6 e + q] = float S_q at list position pos[e] (the record order of the
-// tiled gathers)
+// tiled gathers; list order without pos)
 __global__ void k_nsni_records(int64_t m, const int64_t* __restrict__ pos, NsniS src, float* __restrict__ dst) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= m) return;
-  const int64_t p = pos[e];
+  const int64_t p = pos ? pos[e] : e;
   float v[6];
 #pragma unroll
   for (int c = 0; c < 6; ++c) v[c] = (float)src.v[c][p];

@@ -179,49 +179,103 @@ __global__ void k_pack_f64(int64_t m, const uint16_t* __restrict__ lidx, const d
 // the same rank); a row keeps all its entries, only their order changes.
 // pos, when given, is permuted with lidx.  One warp per warp of the gather's
 // blocks, four warps per block.
+constexpr int kBankCap = 2048;  // entries of one warp's rows that its pass stages in shared memory
+
 template <int KG, int NC, int GL>
 __global__ void __launch_bounds__(128) k_bank_order(int32_t n, int32_t R, int64_t nwarps,
-                                                    const int64_t* __restrict__ ptr, uint16_t* lidx, int64_t* pos) {
+                                                    const int64_t* __restrict__ ptr, uint16_t* lidx,
+                                                    const int64_t* __restrict__ pos_src, int64_t* pos) {
   __shared__ int held_s[4][32];
+  __shared__ uint16_t sl_s[4][kBankCap], so_s[4][kBankCap];  // ranks, and offsets in the row before
   const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   if (w >= nwarps) return;  // whole warps leave together
-  const int lane = threadIdx.x & 31;
-  int* held = held_s[threadIdx.x >> 5] + (lane / GL) * NC;  // this lane's group: the rank held per class
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  int* held = held_s[wi] + (lane / GL) * NC;  // this lane's group: the rank held per class
   const int wpt = R * KG / 32;  // warps per tile
   const int64_t c = (w / wpt) * R + (w % wpt) * (32 / KG) + lane / KG;
   const int q = lane & (KG - 1);
   int64_t b = 0, e = 0;
   if (c < n) { b = ptr[c]; e = ptr[c + 1]; }
-  int steps = (int)((e - b + KG - 1) / KG);
+  const int len = (int)(e - b);
+  // the warp's rows one after another in shared memory, where they fit
+  int x = q == 0 ? len : 0;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  const int total = __shfl_sync(0xffffffffu, x, 31);
+  const int off = __shfl_sync(0xffffffffu, x - (q == 0 ? len : 0), lane & ~(KG - 1));
+  const bool fast = total <= kBankCap;  // warp-uniform
+  uint16_t* sl = sl_s[wi] + off;
+  uint16_t* so = so_s[wi] + off;
+  if (fast)
+    for (int k = q; k < len; k += KG) { sl[k] = lidx[b + k]; so[k] = (uint16_t)k; }
+  __syncwarp();
+  int steps = (len + KG - 1) / KG;
 #pragma unroll
   for (int o = 16; o; o >>= 1) steps = max(steps, __shfl_xor_sync(0xffffffffu, steps, o));
   for (int s = 0; s < steps; ++s) {
-    const int64_t slot = b + (int64_t)s * KG + q;
-    held_s[threadIdx.x >> 5][lane] = -1;
+    const int slot = s * KG + q;
+    held_s[wi][lane] = -1;
     __syncwarp();
     for (int turn = 0; turn < 32; ++turn) {
-      if (lane == turn && slot < e) {
-        int64_t pick = slot;
-        for (int64_t k = slot; k < e; ++k) {
-          const int l = lidx[k], h = held[l & (NC - 1)];
-          if (h < 0 || h == l) { pick = k; break; }
+      if (lane == turn && slot < len) {
+        if (fast) {
+          int pick = slot;
+          for (int k = slot; k < len; ++k) {
+            const int l = sl[k], h = held[l & (NC - 1)];
+            if (h < 0 || h == l) { pick = k; break; }
+          }
+          if (pick != slot) {
+            const uint16_t t1 = sl[pick]; sl[pick] = sl[slot]; sl[slot] = t1;
+            const uint16_t t2 = so[pick]; so[pick] = so[slot]; so[slot] = t2;
+          }
+          const int l = sl[slot];
+          if (held[l & (NC - 1)] < 0) held[l & (NC - 1)] = l;
+        } else {  // rows too long for shared memory: the same pass in place
+          int64_t pick = b + slot;
+          for (int64_t k = b + slot; k < e; ++k) {
+            const int l = lidx[k], h = held[l & (NC - 1)];
+            if (h < 0 || h == l) { pick = k; break; }
+          }
+          if (pick != b + slot) {
+            const uint16_t t1 = lidx[pick]; lidx[pick] = lidx[b + slot]; lidx[b + slot] = t1;
+            const int64_t t2 = pos[pick]; pos[pick] = pos[b + slot]; pos[b + slot] = t2;
+          }
+          const int l = lidx[b + slot];
+          if (held[l & (NC - 1)] < 0) held[l & (NC - 1)] = l;
         }
-        if (pick != slot) {
-          const uint16_t x = lidx[pick]; lidx[pick] = lidx[slot]; lidx[slot] = x;
-          if (pos) { const int64_t y = pos[pick]; pos[pick] = pos[slot]; pos[slot] = y; }
-        }
-        const int l = lidx[slot];
-        if (held[l & (NC - 1)] < 0) held[l & (NC - 1)] = l;
       }
       __syncwarp();
     }
   }
+  if (fast)
+    for (int k = q; k < len; k += KG) {
+      lidx[b + k] = sl[k];
+      pos[b + k] = pos_src ? pos_src[b + so[k]] : b + so[k];
+    }
 }
 
 __global__ void k_gather_rec32(int64_t m, const int64_t* __restrict__ pos, const float4* __restrict__ in,
                                float4* __restrict__ out) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e < m) out[e] = in[pos[e]];
+}
+
+// the tile rank carried by each float record
+__global__ void k_rec_ranks(int64_t m, const float4* __restrict__ rec, uint16_t* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e < m) out[e] = (uint16_t)__float_as_int(rec[e].w);
+}
+
+// out[6 e + k] = in[6 pos[e] + k]
+__global__ void k_gather_f6(int64_t m, const int64_t* __restrict__ pos, const float2* __restrict__ in,
+                            float2* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= m) return;
+  const int64_t p = pos[e];
+  out[3 * e] = in[3 * p]; out[3 * e + 1] = in[3 * p + 1]; out[3 * e + 2] = in[3 * p + 2];
 }
 
 __global__ void k_iota64(int64_t m, int64_t* __restrict__ out) {
@@ -1071,14 +1125,14 @@ int pack_entries(cudaStream_t s, int64_t m, const uint16_t* lidx, const double* 
   return 0;
 }
 
-int bank_order(cudaStream_t s, int32_t n, const TileSet& ts, const int64_t* ptr, uint16_t* lidx, int64_t* pos,
-               int lanes) {
+int bank_order(cudaStream_t s, int32_t n, const TileSet& ts, const int64_t* ptr, uint16_t* lidx,
+               const int64_t* pos_src, int64_t* pos, int lanes) {
   if (n <= 0) return 0;
   if ((lanes != 4 && lanes != 8) || ts.R * lanes < 32) return MEGA_ERR_UNSUPPORTED;
   const int64_t nwarps = ts.ntiles * (int64_t)(ts.R * lanes / 32);
   const unsigned grid = (unsigned)((nwarps * 32 + 127) / 128);
-  if (lanes == 4) k_bank_order<4, 32, 32><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos);
-  else k_bank_order<8, 32, 32><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos);
+  if (lanes == 4) k_bank_order<4, 32, 32><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos_src, pos);
+  else k_bank_order<8, 32, 32><<<grid, 128, 0, s>>>(n, ts.R, nwarps, ptr, lidx, pos_src, pos);
   MEGA_CHECK_LAUNCH();
   return 0;
 }
@@ -1086,6 +1140,20 @@ int bank_order(cudaStream_t s, int32_t n, const TileSet& ts, const int64_t* ptr,
 int iota64(cudaStream_t s, int64_t m, int64_t* out) {
   if (m <= 0) return 0;
   k_iota64<<<grid_for(m, 256), 256, 0, s>>>(m, out);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int record_ranks(cudaStream_t s, int64_t m, const float4* rec, uint16_t* out) {
+  if (m <= 0) return 0;
+  k_rec_ranks<<<grid_for(m, 256), 256, 0, s>>>(m, rec, out);
+  MEGA_CHECK_LAUNCH();
+  return 0;
+}
+
+int gather_f6(cudaStream_t s, int64_t m, const int64_t* pos, const float* in, float* out) {
+  if (m <= 0) return 0;
+  k_gather_f6<<<grid_for(m, 256), 256, 0, s>>>(m, pos, (const float2*)in, (float2*)out);
   MEGA_CHECK_LAUNCH();
   return 0;
 }

@@ -78,13 +78,17 @@ int pack_transposed32(cudaStream_t s, int64_t m, const uint16_t* lidx, const flo
 // Reorder the entries within each row (column) of the tiles ts so that the
 // lanes of a warp of a gather with `lanes` (4 or 8) lanes per row read
 // distinct shared-memory banks of the staged neighbour data (one 32-bit
-// word per rank and value) where possible; pos, when not null, is permuted
-// with lidx.
-int bank_order(cudaStream_t s, int32_t n, const TileSet& ts, const int64_t* ptr, uint16_t* lidx, int64_t* pos,
-               int lanes);
+// word per rank and value) where possible.  lidx is reordered in place;
+// pos[e] receives pos_src (or, when null, the identity) at the entry's
+// position before, and must hold that same array on entry.
+int bank_order(cudaStream_t s, int32_t n, const TileSet& ts, const int64_t* ptr, uint16_t* lidx,
+               const int64_t* pos_src, int64_t* pos, int lanes);
 // out[e] = e;  out[e] = in[pos[e]]
 int iota64(cudaStream_t s, int64_t m, int64_t* out);
 int gather_records32(cudaStream_t s, int64_t m, const int64_t* pos, const float4* in, float4* out);
+// out[e] = the tile rank of float record e;  out[6 e + k] = in[6 pos[e] + k]
+int record_ranks(cudaStream_t s, int64_t m, const float4* rec, uint16_t* out);
+int gather_f6(cudaStream_t s, int64_t m, const int64_t* pos, const float* in, float* out);
 int configure_tiled_kernels();
 // launch variants of the two gathers: lanes per row x records in flight
 // (register streams, variants 0-3 and 6, 7), and lanes per row with the
