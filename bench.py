@@ -573,11 +573,11 @@ def batch_run(args):
     ms = m.step_timed(K_steps, float(dts.min()), mode="mixed", allow_status=True)
     clocks = clk.stop()
     status = int(m.last_status)
-    eps = m.download(_lib.F_EPS)
+    xb = m.download(_lib.F_COO_CURRENT)
     dev_bytes = m.device_bytes()
     m.close()
     off = np.concatenate([[0], np.cumsum(b["counts"])])
-    finite_bars = int(sum(np.all(np.isfinite(eps[off[k]:off[k + 1]])) for k in range(len(b["bars"]))))
+    finite_bars = int(sum(np.all(np.isfinite(xb[off[k]:off[k + 1]])) for k in range(len(b["bars"]))))
     seq_ms = 0.0
     t0 = time.perf_counter()
     for k, bar in enumerate(b["bars"]):

@@ -178,10 +178,12 @@ def batch_bars(nbars=256, seed=5, h_range=(0.15e-3, 0.6e-3), v0_range=(100.0, 30
     return out
 
 
-def lattice_dt(bar, cfl=0.5):
+def lattice_dt(bar, cfl=0.2):
     """A stable step of a jittered lattice bar without its neighbour lists:
     cfl x (0.9 h, the closest two nodes of a +-5 % jitter can be) over the
-    dilatational wave speed."""
+    dilatational wave speed.  cfl = 0.2 keeps the impact of every bar of
+    batch_bars finite through 1,500 steps (with 0.5 the fast bars' nodes
+    close in at the wall and their steps go non-finite after 400-1,200)."""
     p = bar["props"][0]
     E, nu, rho = p[1], p[0], p[2]
     K, G = E / (3.0 * (1.0 - 2.0 * nu)), E / (2.0 * (1.0 + nu))
