@@ -387,11 +387,12 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : (NS ? 8 : 16)) / KG > 0 ?
   const double di0 = dsp[3 * i], di1 = dsp[3 * i + 1], di2 = dsp[3 * i + 2];
   const float fu0 = (float)(ui0 - ur0), fu1 = (float)(ui1 - ur1), fu2 = (float)(ui2 - ur2);
   const float fd0 = (float)(di0 - dr0), fd1 = (float)(di1 - dr1), fd2 = (float)(di2 - dr2);
-  A F[9], L[9], H[NS ? 18 : 1];
+  A F[9], L[9];
+  double H[NS ? 18 : 1];  // NSNI: exact products of the float S and differences, summed in double
 #pragma unroll
   for (int k = 0; k < 9; ++k) { F[k] = A(0); L[k] = A(0); }
 #pragma unroll
-  for (int k = 0; k < (NS ? 18 : 1); ++k) H[k] = A(0);
+  for (int k = 0; k < (NS ? 18 : 1); ++k) H[k] = 0.0;
   double ph0 = 0.0, ph1 = 0.0, ph2 = 0.0;
   // One entry: F += (u_J - u_i) (x) g, L += (d_J - d_i) (x) g (+ phi d_J),
   // H(k, q) += S_q (d_J - d_i)_k.
@@ -417,9 +418,11 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : (NS ? 8 : 16)) / KG > 0 ?
     L[3] += d1 * g0; L[4] += d1 * g1; L[5] += d1 * g2;
     L[6] += d2 * g0; L[7] += d2 * g1; L[8] += d2 * g2;
     if constexpr (NS) {
-      const A sq[6] = {(A)sr.a.x, (A)sr.a.y, (A)sr.b.x, (A)sr.b.y, (A)sr.c.x, (A)sr.c.y};
+      const double sq[6] = {(double)sr.a.x, (double)sr.a.y, (double)sr.b.x, (double)sr.b.y, (double)sr.c.x,
+                            (double)sr.c.y};
+      const double e0 = (double)d0, e1 = (double)d1, e2 = (double)d2;
 #pragma unroll
-      for (int c = 0; c < 6; ++c) { H[c] += sq[c] * d0; H[6 + c] += sq[c] * d1; H[12 + c] += sq[c] * d2; }
+      for (int c = 0; c < 6; ++c) { H[c] += sq[c] * e0; H[6 + c] += sq[c] * e1; H[12 + c] += sq[c] * e2; }
     }
     if (INTERP) {
       const double s = shp[p];
@@ -504,7 +507,7 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : (NS ? 8 : 16)) / KG > 0 ?
 #pragma unroll
       for (int k = 0; k < 3; ++k)
 #pragma unroll
-        for (int c = 0; c < 6; ++c) ns.hq[18 * i + 6 * k + c] = (double)H[6 * k + c] + di[k] * ss[c];
+        for (int c = 0; c < 6; ++c) ns.hq[18 * i + 6 * k + c] = H[6 * k + c] + di[k] * ss[c];
     }
     const double sd3[3] = {sdphi[3 * i], sdphi[3 * i + 1], sdphi[3 * i + 2]};
     double h[18];
