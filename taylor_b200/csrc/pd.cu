@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
   const int cnt = a.jcnt[t];
   const int32_t* js = a.jset + t * (int64_t)a.jmax;
   const bool f64 = sizeof(T) == sizeof(double);
-  // staged set: FP64 8 doubles per particle (X, u, vol, pad); float: X as
+  // staged set: FP64 7 arrays of one double per rank (X, u, vol); float: X as
   // 3 doubles (the bond vector is rounded from the exact difference, as the
   // FP64 path forms it: float offsets of X put 1e-6 of the bond length into
   // the stretch and move the break of near-critical bonds), one array per
@@ -340,10 +340,9 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
     const double x0 = a.X[3 * g], x1 = a.X[3 * g + 1], x2 = a.X[3 * g + 2];
     const double u0 = a.u_in[3 * g], u1 = a.u_in[3 * g + 1], u2 = a.u_in[3 * g + 2];
     const double v = a.vol[g];
-    if (f64) {
-      double2* d = reinterpret_cast<double2*>(sd + 8 * l);
-      d[0] = make_double2(x0, x1); d[1] = make_double2(x2, u0); d[2] = make_double2(u1, u2);
-      d[3] = make_double2(v, 0.0);
+    if (f64) {  // one array per value: lanes with distinct ranks mod 16 read distinct bank pairs
+      sd[l] = x0; sd[cnt + l] = x1; sd[2 * cnt + l] = x2;
+      sd[3 * cnt + l] = u0; sd[4 * cnt + l] = u1; sd[5 * cnt + l] = u2; sd[6 * cnt + l] = v;
     } else {
       sd[l] = x0; sd[cnt + l] = x1; sd[2 * cnt + l] = x2;
       sf[l] = make_float4((float)(u0 - ur0), (float)(u1 - ur1), (float)(u2 - ur2), (float)v);
@@ -392,18 +391,17 @@ __global__ void __launch_bounds__(512) k_pmb_step(PmbArgs a) {
         T s, e0, e1, e2, l, vj;
         if (f64) {
           // the oracle's arithmetic: xi from X, eta = xi + (u_j - u_i), s = (|eta| - |xi|)/|xi|
-          const double2* d = reinterpret_cast<const double2*>(sd + 8 * lj);
-          const double2 q0 = d[0], q1 = d[1], q2 = d[2], q3 = d[3];
-          const double x0 = q0.x - Xi0, x1 = q0.y - Xi1, x2 = q1.x - Xi2;
+          const double* d = sd + lj;  // value k of rank lj at d[k cnt]
+          const double x0 = d[0] - Xi0, x1 = d[cnt] - Xi1, x2 = d[2 * cnt] - Xi2;
           const double L0d = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
           if (L0d == 0.0) continue;  // the particle itself
-          e0 = (T)(x0 + (q1.y - ui0));
-          e1 = (T)(x1 + (q2.x - ui1));
-          e2 = (T)(x2 + (q2.y - ui2));
+          e0 = (T)(x0 + (d[3 * cnt] - ui0));
+          e1 = (T)(x1 + (d[4 * cnt] - ui1));
+          e2 = (T)(x2 + (d[5 * cnt] - ui2));
           const T L0 = (T)L0d;
           l = (T)sqrt((double)(e0 * e0 + e1 * e1 + e2 * e2));
           s = (l - L0) / L0;
-          vj = (T)q3.x;
+          vj = (T)d[6 * cnt];
         } else {
           const float4 ua = sf[lj];
           const float x0 = (float)(sd[lj] - Xi0), x1 = (float)(sd[cnt + lj] - Xi1), x2 = (float)(sd[2 * cnt + lj] - Xi2);
