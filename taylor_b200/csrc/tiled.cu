@@ -454,6 +454,29 @@ __global__ void __launch_bounds__(64 * KG, (F64 ? 12 : (NS ? 8 : 16)) / KG > 0 ?
       for (int u = 0; u < KU; ++u)
         body(p + u * KG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y), s0);
     }
+  } else if constexpr (!NS) {
+    // software-pipelined: the next KU records are requested before this
+    // KU's sums, so a lane keeps loads in flight while it computes
+    float4 cur[KU];
+    bool have = p + (KU - 1) * KG < pend;
+    if (have) {
+#pragma unroll
+      for (int u = 0; u < KU; ++u) cur[u] = __ldg((const float4*)pk + p + u * KG);
+    }
+    while (have) {
+      const int64_t pn = p + KU * KG;
+      const bool hn = pn + (KU - 1) * KG < pend;
+      float4 nxt[KU];
+#pragma unroll
+      for (int u = 0; u < KU; ++u) nxt[u] = hn ? __ldg((const float4*)pk + pn + u * KG) : cur[u];
+#pragma unroll
+      for (int u = 0; u < KU; ++u)
+        body(p + u * KG, (A)cur[u].x, (A)cur[u].y, (A)cur[u].z, __float_as_int(cur[u].w), s0);
+#pragma unroll
+      for (int u = 0; u < KU; ++u) cur[u] = nxt[u];
+      p = pn;
+      have = hn;
+    }
   } else {
     for (; p + (KU - 1) * KG < pend; p += KU * KG) {
       float4 r[KU];
@@ -723,6 +746,29 @@ __global__ void __launch_bounds__(64 * KG) k_force_t(TiledForceArgs a) {
 #pragma unroll
         for (int u = 0; u < KU; ++u)
           body(e + u * KG, (A)ra[u].x, (A)ra[u].y, (A)rb[u].x, (int)__double_as_longlong(rb[u].y), s0);
+      }
+    } else if constexpr (!NS) {
+      // software-pipelined: the next KU records are requested before this
+      // KU's sums, so a lane keeps loads in flight while it computes
+      float4 cur[KU];
+      bool have = e + (KU - 1) * KG < c1;
+      if (have) {
+#pragma unroll
+        for (int u = 0; u < KU; ++u) cur[u] = __ldg((const float4*)a.pk + e + u * KG);
+      }
+      while (have) {
+        const int64_t en = e + KU * KG;
+        const bool hn = en + (KU - 1) * KG < c1;
+        float4 nxt[KU];
+#pragma unroll
+        for (int u = 0; u < KU; ++u) nxt[u] = hn ? __ldg((const float4*)a.pk + en + u * KG) : cur[u];
+#pragma unroll
+        for (int u = 0; u < KU; ++u)
+          body(e + u * KG, (A)cur[u].x, (A)cur[u].y, (A)cur[u].z, __float_as_int(cur[u].w), s0);
+#pragma unroll
+        for (int u = 0; u < KU; ++u) cur[u] = nxt[u];
+        e = en;
+        have = hn;
       }
     } else {
       for (; e + (KU - 1) * KG < c1; e += KU * KG) {
