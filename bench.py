@@ -465,6 +465,7 @@ def learned_runs(args, rank):
             nb = m.search_and_shapes(download=True)
             dt = cases.stable_dt(case, nb["gn"], nb["gstart"], nb["gstack"])
             del nb
+        m.autotune(dt, mode=mode, reps=3)  # as every timed run: variants and (mixed) the banked record layout
         info = {}
         if learn:
             m.log_rate_samples(cap=10_000_000, stride=4, seed=3)
