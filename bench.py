@@ -200,17 +200,19 @@ def kernel_bytes(n, nnz, mixed):
 def nsni_step_bytes(n, nnz, mixed):
     """Algorithmic bytes of one NSNI step (every array touched once): the
     DNI kernels on the seven-point lists (kernel_bytes), the six second
-    derivatives S of every entry in both NSNI gathers with their row / column
-    index (4 + 6 s bytes each, s = 4 mixed or 8), the increment gathered by
-    k_nsni_h (24 per node), H (18 doubles written, read), the stress
-    gradients (18 doubles read and written), the force weights (18 floats /
-    doubles written, read), the stress before the step (6 doubles copied and
-    read) and the stabilisation force (3 doubles written, read)."""
+    derivatives S of every entry in both gathers (6 s bytes each, s = 4
+    mixed or 8; the FP64 NSNI gathers also read each entry's row / column
+    index, 4 bytes, and k_nsni_h gathers the increment, 24 per node, which
+    the mixed gathers have staged already), H (18 doubles written, read),
+    the stress gradients (18 doubles read and written), the force weights
+    (18 floats / doubles written, read), the stress before the step (6
+    doubles copied and read) and, in FP64, the stabilisation force (3
+    doubles written, read)."""
     kb = kernel_bytes(n, nnz, mixed)
     s = 4 if mixed else 8
     w = 80 if mixed else 144
-    per_entry = 2 * (4 + 6 * s)
-    per_node = 24 + 2 * 144 + 2 * 144 + 2 * w + 3 * 48 + 2 * 24
+    per_entry = 2 * (6 * s) if mixed else 2 * (4 + 6 * s)
+    per_node = 2 * 144 + 2 * 144 + 2 * w + 3 * 48 + (0 if mixed else 24 + 2 * 24)
     return kb["defgrad"] + kb["stress"] + kb["force"] + nnz * per_entry + n * per_node
 
 
